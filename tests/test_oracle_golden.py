@@ -1,0 +1,71 @@
+"""The CPU oracle (oracle/front_oracle.c) against the reference's golden outputs: bit for bit.
+
+This pins the oracle before it is used as the checker of the device path."""
+import numpy as np
+import pytest
+
+from oracle import front_oracle as O
+from tests import _golden as G
+
+
+@pytest.fixture(scope="module", params=G.CASES)
+def case(request):
+    return request.param, G.load_case(request.param)
+
+
+def test_detect_matches_reference(case):
+    name, c = case
+    cal = G.calib_of(c)
+    for img, kp_ref, desc_ref in ((c["left0"], c["kp0"], c["desc0"]), (c["left1"], c["kp1"], c["desc1"])):
+        kp = O.detect(img, int(c["budget"]), cal["q99"], cal["dy_vend"], cal["dx_vend"], cap=int(c["budget"]))
+        assert G.same_bits(kp, kp_ref), name
+        pat = G.pattern()
+        desc = O.orb(O.blur(img, cal["kf"], cal["blur_vr"], cal["blur_vc"]), kp, pat)
+        assert np.array_equal(desc, desc_ref), name
+
+
+def test_noise_floor_matches_reference(case):
+    name, c = case
+    cal = G.calib_of(c)
+    for img, ref in ((c["left0"], c["floor0"]), (c["left1"], c["floor1"])):
+        fl, _ff = O.noise_floor(img, cal["q99"])
+        assert np.isfinite(ref) and fl == float(ref), name
+
+
+def test_stereo_matches_reference(case):
+    name, c = case
+    kp = c["kp0"].astype(np.float64)
+    for tag, dlo, dhi, dy, band in G.stereo_variants(c):
+        lo = None if dlo is None else np.full(len(kp), dlo, np.int64)
+        hi = None if dhi is None else np.full(len(kp), dhi, np.int64)
+        d, s, ok, zn, ody = O.stereo(c["left0"], c["right0"], kp, lo, hi, dy=dy, band=band, half=5)
+        assert G.same_bits(d, c["st_%s_d" % tag]), (name, tag)
+        assert G.same_bits(s, c["st_%s_sig" % tag]), (name, tag)
+        assert np.array_equal(ok, c["st_%s_ok" % tag]), (name, tag)
+        assert G.same_bits(zn, c["st_%s_zn" % tag]), (name, tag)
+        assert G.same_bits(np.nan_to_num(ody, nan=-1e300), np.nan_to_num(c["st_%s_dy" % tag], nan=-1e300)), (name, tag)
+
+
+def test_match_matches_reference(case):
+    name, c = case
+    i0, i1 = O.match_desc(c["desc0"], c["desc1"])
+    assert np.array_equal(i0, c["m_i0"]) and np.array_equal(i1, c["m_i1"]), name
+
+
+def test_lk_solver_matches_numba_lapack():
+    z = np.load(G.GOLDEN + "/lk_solver.npz")
+    X, Inv = O.lk_solve_inv(z["As"], z["gs"])
+    assert G.same_bits(X, z["X"]) and G.same_bits(Inv, z["Inv"])
+
+
+def test_edge_cases_oracle():
+    """Empty inputs, off-image and non-finite keypoints, flat images (no positive response)."""
+    flat = np.full((64, 80), 77, np.uint8)
+    assert len(O.detect(flat, 50, 1.0, 64, 80)) == 0
+    d, s, ok, zn, ody = O.stereo(flat, flat, np.zeros((0, 2)))
+    assert len(d) == 0
+    kp = np.array([[np.nan, 5.0], [np.inf, 3.0], [1e300, 2.0], [-3.0, 10.0], [40.0, 30.0]])
+    d, s, ok, zn, ody = O.stereo(flat, flat, kp)
+    assert not ok.any() and (zn == -2.0).all() and np.isinf(s).all()
+    e0, e1 = O.match_desc(np.zeros((1, 32), np.uint8), np.zeros((5, 32), np.uint8))
+    assert len(e0) == 0 and len(e1) == 0

@@ -1,0 +1,97 @@
+"""ctypes binding of libxcb200.so (the sm_100a kernels behind include/xcb200.h).
+
+The library is built in-tree (xclean_b200/build.py).  There is no fallback: if it is missing, or no CUDA device is
+visible, every entry point that needs it raises RuntimeError."""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libxcb200.so")
+
+XCB_OK = 0
+XCB_ERR_ARG = -1
+XCB_ERR_CUDA = -2
+XCB_ERR_CAPACITY = -3
+XCB_ERR_NOT_CALIBRATED = -4
+XCB_ERR_DEVICE = -5
+
+_lock = threading.Lock()
+_LIB = None
+
+c_int, c_double, c_float, c_void_p, c_size_t = ctypes.c_int, ctypes.c_double, ctypes.c_float, ctypes.c_void_p, \
+    ctypes.c_size_t
+P = c_void_p
+
+
+class FrontBufs(ctypes.Structure):
+    _fields_ = [(n, c_void_p) for n in ("counts", "kp", "desc", "d", "sig", "ok", "zn", "dy", "m0", "m1", "nmatch",
+                                         "floor", "anypos")]
+
+
+# name -> (restype, argtypes)
+_SIGS = {
+    "xcb_last_error": (ctypes.c_char_p, []),
+    "xcb_version": (c_int, []),
+    "xcb_front_create": (c_int, [c_int, c_int, c_int, c_int, ctypes.POINTER(c_void_p)]),
+    "xcb_front_destroy": (None, [P]),
+    "xcb_front_last_error": (ctypes.c_char_p, [P]),
+    "xcb_front_device_bytes": (c_size_t, [P]),
+    "xcb_front_set_calibration": (c_int, [P, c_int, c_int, c_int, c_int, P, P, c_double]),
+    "xcb_front_response_host": (c_int, [P, P, c_int, c_int, P]),
+    "xcb_front_noise_floor_host": (c_int, [P, P, P]),
+    "xcb_front_blur_host": (c_int, [P, P, c_int, c_int, P]),
+    "xcb_front_detect_host": (c_int, [P, P, c_int, c_int, P, P, P, P, P]),
+    "xcb_front_describe_host": (c_int, [P, P, P, c_int, P]),
+    "xcb_front_stereo_host": (c_int, [P, P, P, P, P, P, c_int, c_double, c_int, c_int, P, P, P, P, P]),
+    "xcb_front_hamming_host": (c_int, [P, P, c_int, P, c_int, P, P, P, P]),
+    "xcb_front_match_host": (c_int, [P, P, c_int, P, c_int, c_int, c_double, P, P, P]),
+    "xcb_front_lk_check_host": (c_int, [P, P, P, c_int, P, P]),
+    "xcb_front_pipeline_dev": (c_int, [P, P, P, c_int, c_int, c_int, c_int, c_int, c_int, P]),
+    "xcb_front_buffers": (c_int, [P, ctypes.POINTER(FrontBufs)]),
+    "xcb_front_pipeline_host": (c_int, [P, P, P, c_int, c_int, c_int, c_int, c_int, c_int, ctypes.POINTER(FrontBufs)]),
+    "xcb_front_last_launches": (c_int, [P]),
+    "xcb_front_sync_check": (c_int, [P, P]),
+}
+
+
+def declared_symbols():
+    """Every entry point the header declares (the loader binds exactly these)."""
+    return sorted(_SIGS)
+
+
+def lib():
+    """The loaded library; RuntimeError when it is not built."""
+    global _LIB
+    with _lock:
+        if _LIB is None:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError("xclean_b200: %s is not built (run python -m xclean_b200.build or "
+                                   "__graft_entry__.build())" % LIB_PATH)
+            L = ctypes.CDLL(LIB_PATH)
+            for name, (res, args) in _SIGS.items():
+                fn = getattr(L, name)
+                fn.restype = res
+                fn.argtypes = args
+            _LIB = L
+    return _LIB
+
+
+def check(rc, handle=None, what="xcb"):
+    if rc == XCB_OK:
+        return
+    L = lib()
+    msg = (L.xcb_front_last_error(handle) if handle else L.xcb_last_error()) or b""
+    msg = msg.decode(errors="replace")
+    if rc == XCB_ERR_CAPACITY:
+        raise ValueError("%s: %s" % (what, msg))
+    raise RuntimeError("%s failed (%d): %s" % (what, rc, msg))
+
+
+def ptr(a):
+    """Data pointer of a numpy array (or None)."""
+    if a is None:
+        return None
+    return ctypes.c_void_p(a.ctypes.data)

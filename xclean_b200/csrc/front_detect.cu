@@ -1,0 +1,472 @@
+// front_detect.cu -- Shi-Tomasi response, noise floor, cell-scope candidates and the exact greedy pick (sm_100a).
+//
+// Bit-exactness contract (compiled with --fmad=false; every rounding step is an explicit intrinsic):
+//   response  = cv2.cornerMinEigenVal(gray, 3, 3)          (src/xclean/stages/features.py:299; the reference's device
+//               form is gpu_front.py:99-202).  OpenCV's arithmetic: separable Sobel with a fused multiply-add chain in
+//               the SIMD body of the smoothing row filter (x < dy_vend) and of the derivative column filter
+//               (x < dx_vend), float32 products, 3x3 box sum in double with ColumnSum's running sum per column, the
+//               min eigenvalue in float32.  The split points are calibrated against cv2 at start-up.
+//   floor     = features.noise_floor_8u (features.py:57-73), numpy's float32 pairwise summation tree.
+//   picks     = Frontend._response cell scope + Frontend._detect greedy + _subpix (features.py:288-403).
+//
+// B200 layout: frames are batched along grid.y; the response is ONE kernel per batch (u8 in, float32 R out: the
+// reference's dx/dy/row-sum/cov intermediates, ~100 B/px, never touch HBM).  Candidates are gathered one warp per
+// greedy cell straight into per-cell lists sorted by rank, so the greedy kernel advances a list head instead of
+// rescanning; the greedy state, the ranking (a bitonic sort of the picks) and the sub-pixel step share one CTA per
+// frame in shared memory.
+#include "common.cuh"
+#include "front_kernels.h"
+
+// ------------------------------------------------------------------------------------------------------------------
+// 1. response: one thread per (frame, column); the column walk reproduces ColumnSum's running double sums exactly.
+// ------------------------------------------------------------------------------------------------------------------
+struct SobelRow {
+    float rx, ry;
+};
+
+// row-filter outputs of OpenCV's Sobel at column c of one image row: rx = derivative taps (-1 0 1), ry = smoothing
+// taps (1 2 1) * scale, fused for c < dy_vend
+__device__ __forceinline__ SobelRow sobel_row(const u8* row, int W, int c, float ks, float k2s, int dy_vend)
+{
+    int cm = XCB_REFL(c - 1, W), cp = XCB_REFL(c + 1, W);
+    float a = (float)row[cm], b = (float)row[c], d = (float)row[cp];
+    SobelRow o;
+    o.rx = __fsub_rn(d, a);
+    if (c < dy_vend) {
+        float s = __fmul_rn(a, ks);
+        s = __fmaf_rn(b, k2s, s);
+        s = __fmaf_rn(d, ks, s);
+        o.ry = s;
+    } else {
+        float s = __fmul_rn(ks, a);
+        s = __fadd_rn(s, __fmul_rn(k2s, b));
+        s = __fadd_rn(s, __fmul_rn(ks, d));
+        o.ry = s;
+    }
+    return o;
+}
+
+// Sobel (dx, dy) at (y, c) -> the three products dx*dx, dx*dy, dy*dy (float32)
+__device__ __forceinline__ void sobel_products(const u8* I, int H, int W, int y, int c, float ks, float k2s,
+                                               int dy_vend, int dx_vend, float p[3])
+{
+    SobelRow r0 = sobel_row(I + (size_t)XCB_REFL(y - 1, H) * W, W, c, ks, k2s, dy_vend);
+    SobelRow r1 = sobel_row(I + (size_t)y * W, W, c, ks, k2s, dy_vend);
+    SobelRow r2 = sobel_row(I + (size_t)XCB_REFL(y + 1, H) * W, W, c, ks, k2s, dy_vend);
+    float t = __fadd_rn(r0.rx, r2.rx);
+    float dx = (c < dx_vend) ? __fmaf_rn(t, ks, __fmul_rn(r1.rx, k2s))
+                             : __fadd_rn(__fmul_rn(t, ks), __fmul_rn(r1.rx, k2s));
+    float dy = __fsub_rn(r2.ry, r0.ry);
+    p[0] = __fmul_rn(dx, dx);
+    p[1] = __fmul_rn(dx, dy);
+    p[2] = __fmul_rn(dy, dy);
+}
+
+// box-filter row sums (double) of the three products at row y, column x
+__device__ __forceinline__ void row_sums(const u8* I, int H, int W, int y, int x, float ks, float k2s, int dy_vend,
+                                         int dx_vend, double rs[3])
+{
+    float pm[3], p0[3], pp[3];
+    sobel_products(I, H, W, y, XCB_REFL(x - 1, W), ks, k2s, dy_vend, dx_vend, pm);
+    sobel_products(I, H, W, y, x, ks, k2s, dy_vend, dx_vend, p0);
+    sobel_products(I, H, W, y, XCB_REFL(x + 1, W), ks, k2s, dy_vend, dx_vend, pp);
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch) rs[ch] = __dadd_rn(__dadd_rn((double)pm[ch], (double)p0[ch]), (double)pp[ch]);
+}
+
+__global__ void __launch_bounds__(128) k_response(const u8* __restrict__ imgs, int H, int W, int dy_vend,
+                                                  int dx_vend, float* __restrict__ Rall, int* __restrict__ anypos)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int f = blockIdx.y;
+    const u8* I = imgs + (size_t)f * H * W;
+    float* R = Rall + (size_t)f * H * W;
+    const float ks = (float)(1.0 / (4 * 3 * 255.0));
+    const float k2s = (float)(2.0 * (1.0 / (4 * 3 * 255.0)));
+    int pos = 0;
+    if (x < W) {
+        double a[3], b[3], S[3], c[3];
+        row_sums(I, H, W, XCB_REFL(-1, H), x, ks, k2s, dy_vend, dx_vend, a);
+        row_sums(I, H, W, 0, x, ks, k2s, dy_vend, dx_vend, b);
+#pragma unroll
+        for (int ch = 0; ch < 3; ++ch) S[ch] = __dadd_rn(__dadd_rn(0.0, a[ch]), b[ch]);
+        for (int y = 0; y < H; ++y) {
+            row_sums(I, H, W, XCB_REFL(y + 1, H), x, ks, k2s, dy_vend, dx_vend, c);
+            float cov[3];
+#pragma unroll
+            for (int ch = 0; ch < 3; ++ch) {
+                double s0 = __dadd_rn(S[ch], c[ch]);
+                cov[ch] = __double2float_rn(s0);
+                S[ch] = __dsub_rn(s0, a[ch]);
+                a[ch] = b[ch];
+                b[ch] = c[ch];
+            }
+            float ea = __fmul_rn(cov[0], 0.5f), eb = cov[1], ec = __fmul_rn(cov[2], 0.5f);
+            float t = __fsub_rn(ea, ec);
+            float v = __fadd_rn(__fmul_rn(t, t), __fmul_rn(eb, eb));
+            float r = __fsub_rn(__fadd_rn(ea, ec), __fsqrt_rn(v));
+            R[(size_t)y * W + x] = r;
+            pos |= r > 0.0f;
+        }
+    }
+    if (__any_sync(0xffffffffu, pos) && (threadIdx.x & 31) == 0) atomicOr(anypos + f, 1);
+}
+
+cudaError_t xcb_launch_response(const uint8_t* img, int F, int H, int W, int dy_vend, int dx_vend, float* R,
+                                int* anypos, cudaStream_t st)
+{
+    dim3 grid((W + 127) / 128, F);
+    k_response<<<grid, 128, 0, st>>>(img, H, W, dy_vend, dx_vend, R, anypos);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------------------------------------
+// 2. noise floor: leaves of numpy's pairwise tree in parallel, then the tree level by level (one CTA per frame)
+// ------------------------------------------------------------------------------------------------------------------
+__device__ __forceinline__ float lap_abs(const u8* I, int W, long long k)
+{
+    int Wi = W - 2;
+    int y = 1 + (int)(k / Wi), x = 1 + (int)(k % Wi);
+    const u8* r0 = I + (size_t)(y - 1) * W + x;
+    const u8* r1 = r0 + W;
+    const u8* r2 = r1 + W;
+    int v = (int)r0[-1] - 2 * (int)r0[0] + (int)r0[1] - 2 * (int)r1[-1] + 4 * (int)r1[0] - 2 * (int)r1[1] + (int)r2[-1]
+            - 2 * (int)r2[0] + (int)r2[1];
+    return (float)(v < 0 ? -v : v);
+}
+
+__global__ void k_noise_leaves(const u8* __restrict__ imgs, int H, int W, const long long* __restrict__ lstart,
+                               const int* __restrict__ llen, int nleaf, int nnode, float* __restrict__ nodeval)
+{
+    int l = blockIdx.x * blockDim.x + threadIdx.x;
+    int f = blockIdx.y;
+    if (l >= nleaf) return;
+    const u8* I = imgs + (size_t)f * H * W;
+    long long st = lstart[l];
+    int n = llen[l];
+    float res;
+    if (n < 8) {
+        res = -0.0f;
+        for (int i = 0; i < n; ++i) res = __fadd_rn(res, lap_abs(I, W, st + i));
+    } else {
+        float r[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) r[j] = lap_abs(I, W, st + j);
+        int i = 8, lim = n - (n % 8);
+        for (; i < lim; i += 8) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) r[j] = __fadd_rn(r[j], lap_abs(I, W, st + i + j));
+        }
+        res = __fadd_rn(__fadd_rn(__fadd_rn(r[0], r[1]), __fadd_rn(r[2], r[3])),
+                        __fadd_rn(__fadd_rn(r[4], r[5]), __fadd_rn(r[6], r[7])));
+        for (; i < n; ++i) res = __fadd_rn(res, lap_abs(I, W, st + i));
+    }
+    nodeval[(size_t)f * nnode + l] = res;
+}
+
+__global__ void k_noise_tree(float* __restrict__ nodeval, int nnode, const int* __restrict__ left,
+                             const int* __restrict__ right, const int* __restrict__ lvl, int nlvl, int root, double K,
+                             double Q, double* __restrict__ floor_d, float* __restrict__ floor_f)
+{
+    int f = blockIdx.x;
+    float* val = nodeval + (size_t)f * nnode;
+    for (int h = 0; h < nlvl; ++h) {
+        for (int i = lvl[h] + threadIdx.x; i < lvl[h + 1]; i += blockDim.x) val[i] = __fadd_rn(val[left[i]], val[right[i]]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        double sn = __dmul_rn(K, (double)val[root]);
+        double fl = __ddiv_rn(__dmul_rn(__dmul_rn(Q, sn), sn), 65025.0);
+        floor_d[f] = fl;
+        floor_f[f] = __double2float_rn(fl);
+    }
+}
+
+cudaError_t xcb_launch_noise(const uint8_t* img, int F, int H, int W, const XcbNoiseTree& t, float* nodeval,
+                             double K, double Q, double* floor_d, float* floor_f, cudaStream_t st)
+{
+    dim3 g1((t.nleaf + 127) / 128, F);
+    k_noise_leaves<<<g1, 128, 0, st>>>(img, H, W, t.lstart, t.llen, t.nleaf, t.nnode, nodeval);
+    k_noise_tree<<<F, 1024, 0, st>>>(nodeval, t.nnode, t.left, t.right, t.lvl, t.nlvl, t.root, K, Q, floor_d, floor_f);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------------------------------------
+// 3. thresholds (0.01 x the c x c cell max of the zero-padded response) and the per-cell candidate lists
+// ------------------------------------------------------------------------------------------------------------------
+__global__ void k_cellmax(const float* __restrict__ Rall, int H, int W, int c, int gwc, int ghc,
+                          float* __restrict__ thr)
+{
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    const int f = blockIdx.y;
+    if (warp >= gwc * ghc) return;
+    const float* R = Rall + (size_t)f * H * W;
+    int gy = warp / gwc, gx = warp % gwc;
+    int y0 = gy * c, x0 = gx * c;
+    float m = -CUDART_INF_F;
+    int pad = 0;
+    for (int p = lane; p < c * c; p += 32) {
+        int y = y0 + p / c, x = x0 + p % c;
+        if (y < H && x < W) m = fmaxf(m, R[(size_t)y * W + x]);
+        else pad = 1;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+        pad |= __shfl_xor_sync(0xffffffffu, pad, o);
+    }
+    if (lane == 0) {
+        if (pad) m = fmaxf(m, 0.0f);
+        thr[(size_t)f * gwc * ghc + warp] = __fmul_rn(0.01f, m);
+    }
+}
+
+// one warp per greedy cell: candidates (3x3 local max, >= cell threshold, >= noise floor, inside the border) into the
+// cell's list, then ranked (keys are unique) into the sorted list
+__global__ void k_cell_candidates(const float* __restrict__ Rall, int H, int W, int b, int ncx, int ncell,
+                                  const int* __restrict__ ybeg, const int* __restrict__ xbeg,
+                                  const int* __restrict__ coff, int c, int gwc, int ghc, const float* __restrict__ thr,
+                                  const float* __restrict__ floor_f, const int* __restrict__ anypos, u64* raw,
+                                  u64* __restrict__ sorted, int* __restrict__ ccount, long long list_stride)
+{
+    const int cell = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    const int f = blockIdx.y;
+    if (cell >= ncell) return;
+    int* cnt_out = ccount + (size_t)f * ncell + cell;
+    if (!anypos[f]) {               // rmax <= 0: no candidates (Frontend._response)
+        if (lane == 0) *cnt_out = 0;
+        return;
+    }
+    const float* R = Rall + (size_t)f * H * W;
+    const float* T = thr + (size_t)f * gwc * ghc;
+    const float fl = floor_f[f];
+    int cy = cell / ncx, cx = cell % ncx;
+    int ya = max(ybeg[cy], b), yb = min(ybeg[cy + 1], H - b);
+    int xa = max(xbeg[cx], b), xb = min(xbeg[cx + 1], W - b);
+    u64* lraw = raw + (size_t)f * list_stride + coff[cell];
+    u64* lsorted = sorted + (size_t)f * list_stride + coff[cell];
+    int n = 0;
+    if (ya < yb && xa < xb) {
+        int w = xb - xa, np = w * (yb - ya);
+        for (int p0 = 0; p0 < np; p0 += 32) {
+            int p = p0 + lane;
+            bool cand = false;
+            u64 key = 0;
+            if (p < np) {
+                int y = ya + p / w, x = xa + p % w;
+                const float* q = R + (size_t)y * W + x;
+                float v = q[0];
+                float m = v;
+#pragma unroll
+                for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+                    for (int dx = -1; dx <= 1; ++dx) m = fmaxf(m, q[dy * W + dx]);
+                cand = (v >= m) && (v >= T[(y / c) * gwc + x / c]) && (v >= fl);
+                key = xcb_key(v, y, x);
+            }
+            unsigned bal = __ballot_sync(0xffffffffu, cand);
+            if (cand) lraw[n + __popc(bal & ((1u << lane) - 1u))] = key;
+            n += __popc(bal);
+        }
+    }
+    __syncwarp();
+    for (int i = lane; i < n; i += 32) {
+        u64 k = lraw[i];
+        int rank = 0;
+        for (int j = 0; j < n; ++j) rank += lraw[j] > k;
+        lsorted[rank] = k;
+    }
+    if (lane == 0) *cnt_out = n;
+}
+
+cudaError_t xcb_launch_candidates(const float* R, int F, int H, int W, const XcbDetectGeom& g, const float* floor_f,
+                                  const int* anypos, float* thr, unsigned long long* raw, unsigned long long* sorted,
+                                  int* ccount, cudaStream_t st)
+{
+    int nthr = g.gwc * g.ghc;
+    dim3 g1((nthr * 32 + 127) / 128, F);
+    k_cellmax<<<g1, 128, 0, st>>>(R, H, W, g.c, g.gwc, g.ghc, thr);
+    dim3 g2((g.ncell * 32 + 127) / 128, F);
+    k_cell_candidates<<<g2, 128, 0, st>>>(R, H, W, g.border, g.ncx, g.ncell, g.ybeg, g.xbeg, g.coff, g.c, g.gwc, g.ghc,
+                                          thr, floor_f, anypos, raw, sorted, ccount, (long long)H * W);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------------------------------------
+// 4. the exact greedy (one CTA per frame): strongest first, one pick per cell, none within r (strict <) of a
+//    higher-ranked pick.  Each cell holds its best unskipped candidate; a cell commits when no neighbouring undecided
+//    cell holds a higher-ranked candidate, and skips a candidate within r of a committed higher-ranked neighbour pick.
+//    The globally highest undecided candidate is never waiting, so every round decides something and the committed
+//    set equals the sequential loop's; ranking the picks and keeping the first n gives its first n picks.
+// ------------------------------------------------------------------------------------------------------------------
+#define ST_UNDECIDED 0
+#define ST_PICK 1
+#define ST_NONE 2
+#define GREEDY_THREADS 1024
+
+// shared-memory layout of k_greedy: key u64 [ncell] | head int [ncell] | state u8 [ncell] | picks u64 [p2]
+__host__ __device__ __forceinline__ size_t greedy_picks_offset(int ncell)
+{
+    return ((size_t)ncell * 13 + 15) & ~(size_t)15;
+}
+
+size_t xcb_greedy_smem(int ncell)
+{
+    int p2 = 1;
+    while (p2 < ncell) p2 <<= 1;
+    return greedy_picks_offset(ncell) + (size_t)p2 * 8;
+}
+
+// the B200 opt-in maximum is 227 KB per block including the kernel's static shared variables
+int xcb_greedy_smem_limit() { return 226 * 1024; }
+
+__global__ void __launch_bounds__(GREEDY_THREADS) k_greedy(const float* __restrict__ Rall, int H, int W, int ncx,
+                                                           int gh, int ncell, double r2,
+                                                           const int* __restrict__ coff,
+                                                           const u64* __restrict__ sorted_all,
+                                                           const int* __restrict__ ccount_all, long long list_stride,
+                                                           int budget, int cap, int max_rounds, float* __restrict__ kp,
+                                                           int* __restrict__ counts, int* __restrict__ rounds_out,
+                                                           unsigned int* __restrict__ err)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    int p2 = 1;
+    while (p2 < ncell) p2 <<= 1;
+    volatile u64* key = (volatile u64*)smem;
+    volatile int* head = (volatile int*)(smem + (size_t)ncell * 8);
+    volatile u8* state = (volatile u8*)(smem + (size_t)ncell * 12);
+    u64* picks = (u64*)(smem + greedy_picks_offset(ncell));
+    __shared__ int unresolved, npick;
+
+    const int f = blockIdx.x, tid = threadIdx.x;
+    const u64* lists = sorted_all + (size_t)f * list_stride;
+    const int* cnt = ccount_all + (size_t)f * ncell;
+
+    for (int c = tid; c < ncell; c += GREEDY_THREADS) {
+        head[c] = 0;
+        if (cnt[c] > 0) { key[c] = lists[coff[c]]; state[c] = ST_UNDECIDED; }
+        else { key[c] = 0; state[c] = ST_NONE; }
+    }
+    if (tid == 0) npick = 0;
+    __syncthreads();
+
+    int round = 0;
+    for (;;) {
+        if (tid == 0) unresolved = 0;
+        __syncthreads();
+        for (int c = tid; c < ncell; c += GREEDY_THREADS) {
+            if (state[c] != ST_UNDECIDED) continue;
+            const int gx = c % ncx, gy = c / ncx;
+            for (;;) {
+                const u64 kk = key[c];
+                const int qx = xcb_key_x(kk), qy = xcb_key_y(kk);
+                bool blocked = false, wait = false;
+                for (int ny = gy - 1; ny <= gy + 1 && !blocked; ++ny) {
+                    if (ny < 0 || ny >= gh) continue;
+                    for (int nx = gx - 1; nx <= gx + 1; ++nx) {
+                        if (nx < 0 || nx >= ncx) continue;
+                        const int nb = ny * ncx + nx;
+                        if (nb == c) continue;
+                        const int s = state[nb];
+                        if (s == ST_PICK) {
+                            __threadfence_block();
+                            const u64 pk = key[nb];
+                            if (pk > kk) {
+                                long long ddx = (long long)xcb_key_x(pk) - qx, ddy = (long long)xcb_key_y(pk) - qy;
+                                if ((double)(ddx * ddx + ddy * ddy) < r2) { blocked = true; break; }
+                            }
+                        } else if (s == ST_UNDECIDED) {
+                            if (key[nb] > kk) wait = true;
+                        }
+                    }
+                }
+                if (blocked) {
+                    const int h = head[c] + 1;
+                    head[c] = h;
+                    if (h >= cnt[c]) { __threadfence_block(); state[c] = ST_NONE; break; }
+                    key[c] = lists[coff[c] + h];
+                    continue;
+                }
+                if (wait) { atomicAdd(&unresolved, 1); break; }
+                __threadfence_block();
+                state[c] = ST_PICK;
+                break;
+            }
+        }
+        __syncthreads();
+        ++round;
+        const int u = unresolved;
+        if (u == 0) break;
+        if (round >= max_rounds) {
+            if (tid == 0) atomicOr(err, XCB_DEVERR_GREEDY_ROUNDS);
+            break;
+        }
+        __syncthreads();
+    }
+    __syncthreads();
+    // picks -> power-of-two buffer, zero padded; bitonic sort descending (keys are unique and non-zero)
+    for (int c = tid; c < ncell; c += GREEDY_THREADS)
+        if (state[c] == ST_PICK) picks[atomicAdd(&npick, 1)] = key[c];
+    __syncthreads();
+    const int P = npick;
+    for (int i = P + tid; i < p2; i += GREEDY_THREADS) picks[i] = 0ull;
+    __syncthreads();
+    for (int k = 2; k <= p2; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = tid; i < p2; i += GREEDY_THREADS) {
+                int ixj = i ^ j;
+                if (ixj > i) {
+                    u64 a = picks[i], bb = picks[ixj];
+                    bool desc = (i & k) == 0;
+                    if (desc ? (a < bb) : (a > bb)) { picks[i] = bb; picks[ixj] = a; }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    int n_out = P < budget ? P : budget;
+    if (n_out > cap) n_out = cap;
+    const float* R = Rall + (size_t)f * H * W;
+    float* kpo = kp + (size_t)f * cap * 2;
+    for (int i = tid; i < n_out; i += GREEDY_THREADS) {
+        const u64 k = picks[i];
+        const int x = xcb_key_x(k), y = xcb_key_y(k);
+        double fx = (double)x, fy = (double)y;
+        if (x > 0 && x < W - 1 && y > 0 && y < H - 1) {
+            const float* q = R + (size_t)y * W + x;
+            double cc = q[0], l = q[-1], rr = q[1], u = q[-W], d = q[W];
+            double c2 = __dmul_rn(2.0, cc);
+            double denx = __dadd_rn(__dsub_rn(l, c2), rr);
+            double deny = __dadd_rn(__dsub_rn(u, c2), d);
+            double dx = denx < 0.0 ? __ddiv_rn(__dmul_rn(0.5, __dsub_rn(l, rr)), denx) : 0.0;
+            double dy = deny < 0.0 ? __ddiv_rn(__dmul_rn(0.5, __dsub_rn(u, d)), deny) : 0.0;
+            dx = fmin(fmax(dx, -0.5), 0.5);
+            dy = fmin(fmax(dy, -0.5), 0.5);
+            fx = __dadd_rn(fx, dx);
+            fy = __dadd_rn(fy, dy);
+        }
+        kpo[2 * i] = __double2float_rn(fx);
+        kpo[2 * i + 1] = __double2float_rn(fy);
+    }
+    if (tid == 0) {
+        counts[f] = n_out;
+        if (rounds_out) rounds_out[f] = round;
+    }
+}
+
+cudaError_t xcb_greedy_init_attrs()
+{
+    return cudaFuncSetAttribute(k_greedy, cudaFuncAttributeMaxDynamicSharedMemorySize, xcb_greedy_smem_limit());
+}
+
+cudaError_t xcb_launch_greedy(const float* R, int F, int H, int W, const XcbDetectGeom& g,
+                              const unsigned long long* sorted, const int* ccount, int budget, int cap, float* kp,
+                              int* counts, int* rounds, unsigned int* err, cudaStream_t st)
+{
+    size_t sm = xcb_greedy_smem(g.ncell);
+    // every round decides at least one candidate: the bound is the candidate count, at most H * W
+    int max_rounds = H * W + 1;
+    k_greedy<<<F, GREEDY_THREADS, sm, st>>>(R, H, W, g.ncx, g.gh, g.ncell, g.r2, g.coff, sorted, ccount,
+                                            (long long)H * W, budget, cap, max_rounds, kp, counts, rounds, err);
+    return cudaGetLastError();
+}

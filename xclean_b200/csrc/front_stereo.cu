@@ -1,0 +1,614 @@
+// front_stereo.cu -- 1-D ZNCC epipolar stereo with the affine-LK sub-pixel step (sm_100a).
+//
+// Contract: front/stereo1d.stereo_points_band (src/xclean/front/stereo1d.py:335-472) bit for bit at HALF = 5 (the
+// reference's patch, stereo/epipolar.py:35); the same arithmetic with HALF = 3 or 4 for the 7x7 / 9x9 windows.
+// Every float64 sum whose rounding depends on order keeps the CPU's sequential order (the ZNCC cross term, the LK's
+// ten sums); sums of integers (the u8 patch sums and sums of squares, exact in float64) are taken in any order.  The
+// 3x3 solve / inverse replay OpenBLAS getf2 / getrs / trti2 + dgetri as numba's np.linalg.solve / inv run them on the
+// reference's CPU (the reference's device form: gpu_front.py:607-922).
+//
+// B200 layout: ONE WARP PER POINT (the reference uses a 128-thread block and thread-0 serial sections).  The right
+// image window of the point (all disparities, all band rows) is staged once in shared memory; each lane evaluates
+// four disparities at a time, so four independent float64 dependency chains hide the DADD latency; argmax, second
+// peak and left-right argmax are warp shuffles; the LK's ten sequential sums run on ten lanes that each resample the
+// patch themselves (no shared-memory term table, no block barrier).  Points of many frames share one launch.
+#include "common.cuh"
+#include "front_kernels.h"
+
+#define LK_ITERS 6
+#define MAXD 128
+#define ST_WARPS 4
+#define BAND_MAX 16
+
+static __host__ __device__ __forceinline__ int win_w(int half) { return ((MAXD + 2 * half) + 3) & ~3; }
+
+size_t xcb_stereo_smem_per_warp(int half, int band)
+{
+    int pw = 2 * half + 1, npix = pw * pw;
+    size_t rows = (size_t)(pw + 2 * band);
+    return (size_t)npix * 8 * 2 + MAXD * 8 + MAXD + rows * win_w(half) * 4;
+}
+
+// ---------------------------------------------------------------- OpenBLAS 3x3 arithmetic (as the oracle restates it)
+__device__ __forceinline__ void ob_getf2(double a[3][3], int piv[3])
+{
+    for (int j = 0; j < 3; ++j) {
+        for (int i = 0; i < j; ++i) {
+            int ip = piv[i];
+            if (ip != i) { double t = a[i][j]; a[i][j] = a[ip][j]; a[ip][j] = t; }
+        }
+        for (int i = 1; i < j; ++i) {
+            double s = 0.0;
+            for (int k = 0; k < i; ++k) s = __fma_rn(a[i][k], a[k][j], s);
+            a[i][j] = __dsub_rn(a[i][j], s);
+        }
+        if (j > 0)
+            for (int i = j; i < 3; ++i) {
+                double s = 0.0;
+                for (int k = 0; k < j; ++k) s = __fma_rn(a[i][k], a[k][j], s);
+                a[i][j] = __dsub_rn(a[i][j], s);
+            }
+        int jp = j;
+        double mx = fabs(a[j][j]);
+        for (int i = j + 1; i < 3; ++i)
+            if (fabs(a[i][j]) > mx) { mx = fabs(a[i][j]); jp = i; }
+        piv[j] = jp;
+        double t = a[jp][j];
+        if (t != 0.0) {
+            t = __ddiv_rn(1.0, t);
+            if (jp != j)
+                for (int k = 0; k <= j; ++k) { double u = a[j][k]; a[j][k] = a[jp][k]; a[jp][k] = u; }
+            for (int i = j + 1; i < 3; ++i) a[i][j] = __dmul_rn(a[i][j], t);
+        }
+    }
+}
+
+__device__ __forceinline__ void ob_getrs(const double a[3][3], const int piv[3], double y[3])
+{
+    for (int j = 0; j < 3; ++j) { int p = piv[j]; if (p != j) { double t = y[j]; y[j] = y[p]; y[p] = t; } }
+    for (int j = 0; j < 3; ++j)
+        for (int i = j + 1; i < 3; ++i) y[i] = __fma_rn(-y[j], a[i][j], y[i]);
+    for (int j = 2; j >= 0; --j) {
+        y[j] = __ddiv_rn(y[j], a[j][j]);
+        for (int i = 0; i < j; ++i) y[i] = __fma_rn(-y[j], a[i][j], y[i]);
+    }
+}
+
+__device__ __forceinline__ void ob_getri(double a[3][3], const int piv[3])
+{
+    for (int j = 0; j < 3; ++j) {
+        double ajj = __ddiv_rn(1.0, a[j][j]);
+        a[j][j] = ajj;
+        double x[3];
+        for (int i = 0; i < j; ++i) x[i] = a[i][j];
+        for (int i = 0; i < j; ++i) {
+            for (int q = 0; q < i; ++q) x[q] = __fma_rn(x[i], a[q][i], x[q]);
+            x[i] = __dmul_rn(x[i], a[i][i]);
+        }
+        for (int i = 0; i < j; ++i) a[i][j] = __dmul_rn(x[i], -ajj);
+    }
+    double work[3] = {0.0, 0.0, 0.0};
+    for (int j = 2; j >= 0; --j) {
+        for (int i = j + 1; i < 3; ++i) { work[i] = a[i][j]; a[i][j] = 0.0; }
+        if (j < 2)
+            for (int r = 0; r < 3; ++r) {
+                double s = 0.0;
+                for (int k = j + 1; k < 3; ++k) s = __fma_rn(a[r][k], work[k], s);
+                a[r][j] = __dsub_rn(a[r][j], s);
+            }
+    }
+    for (int j = 1; j >= 0; --j) {
+        int jp = piv[j];
+        if (jp != j)
+            for (int r = 0; r < 3; ++r) { double t = a[r][j]; a[r][j] = a[r][jp]; a[r][jp] = t; }
+    }
+}
+
+__global__ void k_lkcheck(const double* __restrict__ As, const double* __restrict__ gs, int n, double* __restrict__ X,
+                          double* __restrict__ Inv)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    double a[3][3], b[3][3];
+    int piv[3], piv2[3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) a[i][j] = b[i][j] = As[9 * k + 3 * i + j];
+    ob_getf2(a, piv);
+    double y[3] = {gs[3 * k], gs[3 * k + 1], gs[3 * k + 2]};
+    ob_getrs(a, piv, y);
+    for (int i = 0; i < 3; ++i) X[3 * k + i] = y[i];
+    ob_getf2(b, piv2);
+    ob_getri(b, piv2);
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) Inv[9 * k + 3 * i + j] = b[i][j];
+}
+
+cudaError_t xcb_launch_lkcheck(const double* As, const double* gs, int n, double* X, double* Inv, cudaStream_t st)
+{
+    k_lkcheck<<<(n + 127) / 128, 128, 0, st>>>(As, gs, n, X, Inv);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- shift_rows (stereo1d.py:478-489), float32
+__global__ void k_shift(const u8* __restrict__ R, int H, int W, double dy, float* __restrict__ Rs)
+{
+    int x = blockIdx.x * blockDim.x + threadIdx.x;
+    int y = blockIdx.y, f = blockIdx.z;
+    if (x >= W) return;
+    const u8* Rf = R + (size_t)f * H * W;
+    double yy = __dadd_rn((double)y, dy);
+    double y0d = floor(yy);
+    float fr = __double2float_rn(__dsub_rn(yy, y0d));
+    long long y0 = (long long)y0d;
+    long long ya = y0 < 0 ? 0 : (y0 > H - 1 ? H - 1 : y0);
+    long long yb = y0 + 1 < 0 ? 0 : (y0 + 1 > H - 1 ? H - 1 : y0 + 1);
+    float a = (float)Rf[(size_t)ya * W + x], b = (float)Rf[(size_t)yb * W + x];
+    Rs[(size_t)f * H * W + (size_t)y * W + x] = __fadd_rn(a, __fmul_rn(fr, __fsub_rn(b, a)));
+}
+
+cudaError_t xcb_launch_shift(const uint8_t* R, int F, int H, int W, double dy, float* Rs, cudaStream_t st)
+{
+    dim3 grid((W + 127) / 128, H, F);
+    k_shift<<<grid, 128, 0, st>>>(R, H, W, dy, Rs);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- helpers
+template <bool FLT>
+struct RightImg {
+    const u8* r8;
+    const float* rf;
+    __device__ __forceinline__ float at(size_t o) const { return FLT ? rf[o] : (float)r8[o]; }
+};
+
+// bilinear sample (stereo1d._bil) of float32-valued pixels: differences in float32 (exact for u8 data)
+template <typename TP>
+__device__ __forceinline__ void bil(const TP& img, int H, int W, double x, double y, double* val, double* gx)
+{
+    int x0 = (int)floor(x), y0 = (int)floor(y);
+    double ax = __dsub_rn(x, (double)x0), ay = __dsub_rn(y, (double)y0);
+    if (x0 < 0) x0 = 0;
+    if (x0 > W - 2) x0 = W - 2;
+    if (y0 < 0) y0 = 0;
+    if (y0 > H - 2) y0 = H - 2;
+    float fa = img.at((size_t)y0 * W + x0), fb = img.at((size_t)y0 * W + x0 + 1);
+    float fc = img.at((size_t)(y0 + 1) * W + x0), fd = img.at((size_t)(y0 + 1) * W + x0 + 1);
+    double a = (double)fa, c = (double)fc;
+    double ba = (double)__fsub_rn(fb, fa), dc = (double)__fsub_rn(fd, fc);
+    double top = __dadd_rn(a, __dmul_rn(ax, ba));
+    double bot = __dadd_rn(c, __dmul_rn(ax, dc));
+    *val = __dadd_rn(top, __dmul_rn(ay, __dsub_rn(bot, top)));
+    *gx = __dadd_rn(__dmul_rn(ba, __dsub_rn(1.0, ay)), __dmul_rn(dc, ay));
+}
+
+struct LeftImg {
+    const u8* p;
+    __device__ __forceinline__ float at(size_t o) const { return (float)p[o]; }
+};
+
+__device__ __forceinline__ double zncc_finish(double s, double s2, double sx, double ts, int npix)
+{
+    double m = __ddiv_rn(s, (double)npix);
+    double var = __dsub_rn(__ddiv_rn(s2, (double)npix), __dmul_rn(m, m));
+    double sd = __dsqrt_rn(var > 0.0 ? var : 0.0);
+    double den = __dmul_rn(__dmul_rn(ts, sd), (double)npix);
+    return den > 1e-6 ? __ddiv_rn(sx, den) : -2.0;
+}
+
+// Q ZNCCs at once on a shared-memory window: patch q's top-left at (row0, col0[q]); T = template minus its mean.
+// FLT: pixel sums in sequential float64 (shifted float32 image); else exact integer sums.
+template <int HALF, bool FLT, int Q>
+__device__ __forceinline__ void zncc_q(const float* win, int ww, int row0, const int col0[Q], const bool valid[Q],
+                                       const double* T, double ts, double out[Q])
+{
+    constexpr int PW = 2 * HALF + 1, NPIX = PW * PW;
+    double sx[Q], s[Q], s2[Q];
+    int si[Q], s2i[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) { sx[q] = 0.0; s[q] = 0.0; s2[q] = 0.0; si[q] = 0; s2i[q] = 0; }
+    int cb[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) cb[q] = valid[q] ? col0[q] : 0;
+    for (int dy = 0; dy < PW; ++dy) {
+        const float* row = win + (size_t)(row0 + dy) * ww;
+#pragma unroll
+        for (int dx = 0; dx < PW; ++dx) {
+            const double tk = T[dy * PW + dx];
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                const float v = row[cb[q] + dx];
+                const double r = (double)v;
+                if (FLT) {
+                    s[q] = __dadd_rn(s[q], r);
+                    s2[q] = __dadd_rn(s2[q], (double)__fmul_rn(v, v));
+                } else {
+                    const int iv = (int)v;
+                    si[q] += iv;
+                    s2i[q] += iv * iv;
+                }
+                sx[q] = __dadd_rn(sx[q], __dmul_rn(r, tk));
+            }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        if (!FLT) { s[q] = (double)si[q]; s2[q] = (double)s2i[q]; }
+        out[q] = valid[q] ? zncc_finish(s[q], s2[q], sx[q], ts, NPIX) : -2.0;
+    }
+}
+
+// warp argmax, first maximum in increasing index (strict '>' scan): ties keep the smaller index
+__device__ __forceinline__ void warp_argmax(double& v, int& idx)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        double v2 = __shfl_xor_sync(0xffffffffu, v, o);
+        int i2 = __shfl_xor_sync(0xffffffffu, idx, o);
+        if (v2 > v || (v2 == v && i2 < idx)) { v = v2; idx = i2; }
+    }
+}
+
+// ---------------------------------------------------------------- the stereo kernel
+template <int HALF, bool FLT>
+__global__ void __launch_bounds__(ST_WARPS * 32) k_stereo(
+    const u8* __restrict__ Lall, const u8* __restrict__ R8all, const float* __restrict__ Rsall, int H, int W,
+    const double* __restrict__ kpd, const long long* __restrict__ dlo_a, const long long* __restrict__ dhi_a, int n,
+    const float* __restrict__ kpf, const int* __restrict__ counts, int cap, int dlo_s, int dhi_s, int band,
+    double* __restrict__ od, double* __restrict__ osig, u8* __restrict__ ook, double* __restrict__ ozn,
+    double* __restrict__ ody)
+{
+    constexpr int PW = 2 * HALF + 1, NPIX = PW * PW;
+    const double ZMIN = 0.5, UNIQ1 = 1.0 + 0.05, LRT = 1.0;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int ww = win_w(HALF);
+    const size_t per_warp = (size_t)NPIX * 16 + MAXD * 8 + MAXD + (size_t)(PW + 2 * band) * ww * 4;
+    unsigned char* base = smem_raw + (size_t)wid * ((per_warp + 15) & ~(size_t)15);
+    double* Td = (double*)base;
+    double* T2d = Td + NPIX;
+    double* sc = T2d + NPIX;
+    float* win = (float*)(sc + MAXD);
+    signed char* jb = (signed char*)(win + (size_t)(PW + 2 * band) * ww);
+
+    const long long p = (long long)blockIdx.x * ST_WARPS + wid;
+    int f = 0;
+    size_t oi;
+    double u, v;
+    long long lo, hi;
+    if (kpd) {
+        if (p >= n) return;
+        oi = (size_t)p;
+        u = kpd[2 * p]; v = kpd[2 * p + 1];
+        lo = dlo_a[p]; hi = dhi_a[p];
+    } else {
+        f = (int)(p / cap);
+        int i = (int)(p % cap);
+        if (f >= n || i >= counts[f]) return;
+        oi = (size_t)f * cap + i;
+        u = (double)kpf[2 * oi]; v = (double)kpf[2 * oi + 1];
+        lo = dlo_s; hi = dhi_s;
+    }
+    const u8* L = Lall + (size_t)f * H * W;
+    RightImg<FLT> R;
+    R.r8 = R8all ? R8all + (size_t)f * H * W : nullptr;
+    R.rf = Rsall ? Rsall + (size_t)f * H * W : nullptr;
+    if (lane == 0) { ook[oi] = 0; od[oi] = 0.0; osig[oi] = XCB_INF; ozn[oi] = -2.0; ody[oi] = XCB_NAN; }
+
+    const int ui = (int)floor(__dadd_rn(u, 0.5)), vi = (int)floor(__dadd_rn(v, 0.5));
+    if (ui - HALF - 2 < 0 || ui + HALF + 2 >= W || vi - HALF - 2 - band < 0 || vi + HALF + 2 + band >= H) return;
+    if (lo < 0) lo = 0;
+    if (hi > MAXD - 1) hi = MAXD - 1;
+    if (hi > ui - HALF - 2) hi = ui - HALF - 2;
+    if (hi < lo) return;
+
+    // template statistics (_patch_stats on u8: integer sums, exact) and T - mean
+    int s = 0, s2 = 0;
+    for (int k = lane; k < NPIX; k += 32) {
+        int t = L[(size_t)(vi + k / PW - HALF) * W + ui + k % PW - HALF];
+        s += t; s2 += t * t;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) { s += __shfl_xor_sync(0xffffffffu, s, o); s2 += __shfl_xor_sync(0xffffffffu, s2, o); }
+    const double tm = __ddiv_rn((double)s, (double)NPIX);
+    const double tvar = __dsub_rn(__ddiv_rn((double)s2, (double)NPIX), __dmul_rn(tm, tm));
+    const double ts = __dsqrt_rn(tvar > 0.0 ? tvar : 0.0);
+    if (ts <= 1e-6) return;
+    for (int k = lane; k < NPIX; k += 32)
+        Td[k] = __dsub_rn((double)L[(size_t)(vi + k / PW - HALF) * W + ui + k % PW - HALF], tm);
+
+    // right-image window: rows vi-band-HALF .. vi+band+HALF, columns ui-hi-HALF .. ui-lo+HALF
+    const int wr0 = vi - band - HALF, wc0 = ui - (int)hi - HALF;
+    const int nrows = PW + 2 * band, ncols = (int)(hi - lo) + PW;
+    for (int idx = lane; idx < nrows * ncols; idx += 32) {
+        int rr = idx / ncols, cc = idx % ncols;
+        win[rr * ww + cc] = R.at((size_t)(wr0 + rr) * W + wc0 + cc);
+    }
+    __syncwarp();
+
+    // ZNCC over d in [lo, hi] (best row of the band), four disparities per lane
+    double lbest = -2.0;
+    int lbd = -1;
+#pragma unroll 1
+    for (int q0 = 0; q0 < 4; q0 += 4) {
+        int dq[4], col[4];
+        bool val[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            dq[q] = (int)lo + lane + 32 * q;
+            val[q] = dq[q] <= hi;
+            col[q] = (int)hi - dq[q];
+        }
+        double best[4];
+        int bj[4] = {0, 0, 0, 0};
+        zncc_q<HALF, FLT, 4>(win, ww, band, col, val, Td, ts, best);
+        for (int j = 1; j <= band; ++j) {
+            double z[4];
+            zncc_q<HALF, FLT, 4>(win, ww, band - j, col, val, Td, ts, z);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) if (z[q] > best[q]) { best[q] = z[q]; bj[q] = -j; }
+            zncc_q<HALF, FLT, 4>(win, ww, band + j, col, val, Td, ts, z);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) if (z[q] > best[q]) { best[q] = z[q]; bj[q] = j; }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (val[q]) {
+                sc[dq[q]] = best[q];
+                jb[dq[q]] = (signed char)bj[q];
+                if (best[q] > lbest) { lbest = best[q]; lbd = dq[q]; }
+            }
+        }
+    }
+    double bs = lbest;
+    int bestd = lbd;
+    warp_argmax(bs, bestd);
+    if (lane == 0) ozn[oi] = bs;
+    if (bestd < 0 || bs < ZMIN) return;
+    __syncwarp();
+    double sec = -2.0;
+    for (int d = (int)lo + lane; d <= hi; d += 32)
+        if (abs(d - bestd) > 1 && sc[d] > sec) sec = sc[d];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sec = fmax(sec, __shfl_xor_sync(0xffffffffu, sec, o));
+    if (!(__dsub_rn(1.0, sec) > __dmul_rn(__dsub_rn(1.0, bs), UNIQ1))) return;
+
+    // left-right check: the right patch at the peak searched back along the left row
+    const int js = jb[bestd];
+    const int xr = ui - bestd;
+    double rm, rsd;
+    if (FLT) {
+        // float32 patch: the CPU's sequential float64 sums (x * x a float32 product)
+        double a = 0.0, a2 = 0.0;
+        if (lane == 0)
+            for (int k = 0; k < NPIX; ++k) {
+                float x = R.at((size_t)(vi + js + k / PW - HALF) * W + xr + k % PW - HALF);
+                a = __dadd_rn(a, (double)x);
+                a2 = __dadd_rn(a2, (double)__fmul_rn(x, x));
+            }
+        a = __shfl_sync(0xffffffffu, a, 0);
+        a2 = __shfl_sync(0xffffffffu, a2, 0);
+        rm = __ddiv_rn(a, (double)NPIX);
+        double var = __dsub_rn(__ddiv_rn(a2, (double)NPIX), __dmul_rn(rm, rm));
+        rsd = __dsqrt_rn(var > 0.0 ? var : 0.0);
+    } else {
+        int a = 0, a2 = 0;
+        for (int k = lane; k < NPIX; k += 32) {
+            int x = (int)R.at((size_t)(vi + js + k / PW - HALF) * W + xr + k % PW - HALF);
+            a += x; a2 += x * x;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) { a += __shfl_xor_sync(0xffffffffu, a, o); a2 += __shfl_xor_sync(0xffffffffu, a2, o); }
+        rm = __ddiv_rn((double)a, (double)NPIX);
+        double var = __dsub_rn(__ddiv_rn((double)a2, (double)NPIX), __dmul_rn(rm, rm));
+        rsd = __dsqrt_rn(var > 0.0 ? var : 0.0);
+    }
+    if (rsd <= 1e-6) return;
+    for (int k = lane; k < NPIX; k += 32)
+        T2d[k] = __dsub_rn((double)R.at((size_t)(vi + js + k / PW - HALF) * W + xr + k % PW - HALF), rm);
+    int dmax = MAXD - 1;
+    if (xr + dmax + HALF >= W) dmax = W - 1 - HALF - xr;
+    const int lc0 = xr - HALF, lcols = dmax + PW;
+    __syncwarp();
+    for (int idx = lane; idx < PW * lcols; idx += 32) {
+        int rr = idx / lcols, cc = idx % lcols;
+        win[rr * ww + cc] = (float)L[(size_t)(vi - HALF + rr) * W + lc0 + cc];
+    }
+    __syncwarp();
+    double lrb = -2.0;
+    int lrd = -1;
+    {
+        int col[4];
+        bool val[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) { col[q] = lane + 32 * q; val[q] = col[q] <= dmax; }
+        double z[4];
+        zncc_q<HALF, false, 4>(win, ww, 0, col, val, T2d, rsd, z);
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (val[q] && z[q] > lrb) { lrb = z[q]; lrd = col[q]; }
+    }
+    warp_argmax(lrb, lrd);
+    if (lrd < 0 || fabs((double)(lrd - bestd)) > LRT) return;
+
+    // parabola seed, then the affine LK from the sub-pixel keypoint position
+    double off = 0.0;
+    if (bestd > lo && bestd < hi) {
+        double y0 = sc[bestd - 1], y2 = sc[bestd + 1];
+        double den = __dadd_rn(__dsub_rn(y0, __dmul_rn(2.0, bs)), y2);
+        if (den < -1e-9) {
+            off = __ddiv_rn(__dmul_rn(0.5, __dsub_rn(y0, y2)), den);
+            if (off > 0.5) off = 0.5;
+            if (off < -0.5) off = -0.5;
+        }
+    }
+    const double seed = __dadd_rn(__dadd_rn((double)bestd, off), __dsub_rn(u, (double)ui));
+    const double voff = (double)js;
+    double* Tl = T2d;     // the LK template (bilinear left samples) reuses T2d
+    __syncwarp();
+    LeftImg Li;
+    Li.p = L;
+    for (int k = lane; k < NPIX; k += 32) {
+        double g_;
+        bil(Li, H, W, __dadd_rn(u, (double)(k % PW - HALF)), __dadd_rn(v, (double)(k / PW - HALF)), &Tl[k], &g_);
+    }
+    __syncwarp();
+    double d = seed, a = 1.0, b = 0.0;
+    bool okk = false;
+    double sig = 0.0;
+    for (int it = 0; it <= LK_ITERS; ++it) {
+        double S = 0.0;
+        if (lane < 10) {
+            for (int k = 0; k < NPIX; ++k) {
+                double rv, rg;
+                double px = __dadd_rn(u, (double)(k % PW - HALF)), py = __dadd_rn(v, (double)(k / PW - HALF));
+                bil(R, H, W, __dsub_rn(px, d), __dadd_rn(py, voff), &rv, &rg);
+                double r = __dsub_rn(Tl[k], __dadd_rn(__dmul_rn(a, rv), b));
+                double J0 = __dmul_rn(-a, rg), J1 = rv;
+                double term;
+                switch (lane) {
+                    case 0: term = __dmul_rn(J0, r); break;
+                    case 1: term = __dmul_rn(J1, r); break;
+                    case 2: term = r; break;
+                    case 3: term = __dmul_rn(J0, J0); break;
+                    case 4: term = __dmul_rn(J0, J1); break;
+                    case 5: term = J0; break;
+                    case 6: term = __dmul_rn(J1, J1); break;
+                    case 7: term = J1; break;
+                    case 8: term = 1.0; break;
+                    default: term = __dmul_rn(r, r); break;
+                }
+                S = __dadd_rn(S, term);
+            }
+        }
+        double Sv[10];
+#pragma unroll
+        for (int q = 0; q < 10; ++q) Sv[q] = __shfl_sync(0xffffffffu, S, q);
+        int go = 1;
+        if (lane == 0) {
+            double A[3][3] = {{Sv[3], Sv[4], Sv[5]}, {Sv[4], Sv[6], Sv[7]}, {Sv[5], Sv[7], Sv[8]}};
+            for (int i = 0; i < 3; ++i) A[i][i] = __dadd_rn(A[i][i], 1e-9);
+            int piv[3];
+            ob_getf2(A, piv);
+            if (it < LK_ITERS) {
+                double dl[3] = {Sv[0], Sv[1], Sv[2]};
+                ob_getrs(A, piv, dl);
+                d = __dadd_rn(d, dl[0]);
+                a = __dadd_rn(a, dl[1]);
+                b = __dadd_rn(b, dl[2]);
+                if (!(isfinite(d) && isfinite(a))) go = 0;
+            } else {
+                double s2v = __ddiv_rn(Sv[9], (double)(NPIX - 3));
+                ob_getri(A, piv);
+                double var = __dmul_rn(s2v, A[0][0]);
+                sig = var > 0.0 ? __dsqrt_rn(var) : 0.0;
+                bool conv = isfinite(d) && fabs(__dsub_rn(d, seed)) <= 1.0 && a > 0.5 && a < 2.0;
+                okk = conv && !(d < 0.5);
+            }
+        }
+        go = __shfl_sync(0xffffffffu, go, 0);
+        d = __shfl_sync(0xffffffffu, d, 0);
+        a = __shfl_sync(0xffffffffu, a, 0);
+        b = __shfl_sync(0xffffffffu, b, 0);
+        if (!go) return;
+    }
+    okk = __shfl_sync(0xffffffffu, (int)okk, 0);
+    if (!okk) return;
+    if (lane == 0) { od[oi] = d; osig[oi] = sig; ook[oi] = 1; }
+
+    // the point's own vertical offset: column scan of the ZNCC at the matched integer disparity
+    if (vi - 2 * HALF - 1 >= 0 && vi + 2 * HALF + 1 < H) {
+        double z = -2.0;
+        if (lane < PW) {
+            const int vy = vi + lane - HALF;
+            double zs = 0.0, zs2 = 0.0, sx = 0.0;
+            int zi = 0, zi2 = 0;
+            for (int k = 0; k < NPIX; ++k) {
+                float rf = R.at((size_t)(vy + k / PW - HALF) * W + xr + k % PW - HALF);
+                double r = (double)rf;
+                if (FLT) {
+                    zs = __dadd_rn(zs, r);
+                    zs2 = __dadd_rn(zs2, (double)__fmul_rn(rf, rf));
+                } else {
+                    int iv = (int)rf;
+                    zi += iv; zi2 += iv * iv;
+                }
+                sx = __dadd_rn(sx, __dmul_rn(r, Td[k]));
+            }
+            if (!FLT) { zs = (double)zi; zs2 = (double)zi2; }
+            z = zncc_finish(zs, zs2, sx, ts, NPIX);
+        }
+        double col[PW];
+#pragma unroll
+        for (int j = 0; j < PW; ++j) col[j] = __shfl_sync(0xffffffffu, z, j);
+        if (lane == 0) {
+            int jp = 0;
+            double cs = -2.0;
+            for (int j = -HALF; j <= HALF; ++j)
+                if (col[j + HALF] > cs) { cs = col[j + HALF]; jp = j; }
+            double offy = 0.0;
+            if (jp > -HALF && jp < HALF) {
+                double y0 = col[jp - 1 + HALF], y2 = col[jp + 1 + HALF];
+                double den = __dadd_rn(__dsub_rn(y0, __dmul_rn(2.0, cs)), y2);
+                if (den < -1e-9) {
+                    offy = __ddiv_rn(__dmul_rn(0.5, __dsub_rn(y0, y2)), den);
+                    if (offy > 0.5) offy = 0.5;
+                    if (offy < -0.5) offy = -0.5;
+                }
+            }
+            ody[oi] = __dadd_rn((double)jp, offy);
+        }
+    }
+}
+
+template <int HALF, bool FLT>
+static cudaError_t launch_stereo_t(const uint8_t* L, const uint8_t* R8, const float* Rs, int H, int W,
+                                   const double* kpd, const long long* dlo_a, const long long* dhi_a, int n,
+                                   const float* kpf, const int* counts, int cap, int dlo, int dhi, int band,
+                                   double* od, double* osig, uint8_t* ook, double* ozn, double* ody, long long npts,
+                                   cudaStream_t st)
+{
+    size_t pw = (xcb_stereo_smem_per_warp(HALF, band) + 15) & ~(size_t)15;
+    size_t sm = pw * ST_WARPS;
+    long long nb = (npts + ST_WARPS - 1) / ST_WARPS;
+    if (nb <= 0) return cudaSuccess;
+    k_stereo<HALF, FLT><<<(unsigned)nb, ST_WARPS * 32, sm, st>>>(L, R8, Rs, H, W, kpd, dlo_a, dhi_a, n, kpf, counts,
+                                                                  cap, dlo, dhi, band, od, osig, ook, ozn, ody);
+    return cudaGetLastError();
+}
+
+// the largest window (band BAND_MAX) of every instantiation, set once before any launch or graph capture
+cudaError_t xcb_stereo_init_attrs()
+{
+    cudaError_t e = cudaSuccess;
+#define XCB_SA(HH, FF)                                                                                            \
+    if (e == cudaSuccess)                                                                                         \
+        e = cudaFuncSetAttribute(k_stereo<HH, FF>, cudaFuncAttributeMaxDynamicSharedMemorySize,                   \
+                                 (int)(((xcb_stereo_smem_per_warp(HH, BAND_MAX) + 15) & ~(size_t)15) * ST_WARPS));
+    XCB_SA(3, false) XCB_SA(3, true) XCB_SA(4, false) XCB_SA(4, true) XCB_SA(5, false) XCB_SA(5, true)
+#undef XCB_SA
+    return e;
+}
+
+cudaError_t xcb_launch_stereo(const uint8_t* L, const uint8_t* R8, const float* Rs, int F, int H, int W,
+                              const double* kpd, const long long* dlo_a, const long long* dhi_a, int n,
+                              const float* kpf, const int* counts, int cap, int dlo, int dhi, int band, int half,
+                              double* od, double* osig, uint8_t* ook, double* ozn, double* ody, unsigned int* err,
+                              cudaStream_t st)
+{
+    if (band < 0 || band > BAND_MAX) return cudaErrorInvalidValue;
+    long long npts = kpd ? (long long)n : (long long)F * cap;
+    int nn = kpd ? n : F;
+    bool flt = Rs != nullptr;
+#define XCB_ST(HH)                                                                                                  \
+    return flt ? launch_stereo_t<HH, true>(L, nullptr, Rs, H, W, kpd, dlo_a, dhi_a, nn, kpf, counts, cap, dlo, dhi,  \
+                                           band, od, osig, ook, ozn, ody, npts, st)                                 \
+               : launch_stereo_t<HH, false>(L, R8, nullptr, H, W, kpd, dlo_a, dhi_a, nn, kpf, counts, cap, dlo, dhi, \
+                                            band, od, osig, ook, ozn, ody, npts, st);
+    switch (half) {
+        case 3: XCB_ST(3)
+        case 4: XCB_ST(4)
+        case 5: XCB_ST(5)
+        default: return cudaErrorInvalidValue;
+    }
+#undef XCB_ST
+}

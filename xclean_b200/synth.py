@@ -1,0 +1,197 @@
+"""Seeded synthetic stereo scenes (stand-ins for the datasets the reference is run on, which are not available here).
+
+Textured planes rendered by ray-plane intersection (no graphics API: plain tensor arithmetic on the CPU or the GPU),
+rectified pinhole stereo, Gaussian sensor noise, uint8 output.
+
+  scene_planes(seed, ...)           N random planes at depths [z0, z1] plus a background plane (the small-frame case)
+  scene_road(seed, length)          a driving corridor: road, two facades, roadside boards, a far backdrop
+  render_pair(scene, cam, pose)     -> (left, right) uint8 (H, W)
+  sequence(...)                     a forward-driving sequence of stereo pairs, [F, H, W] uint8 tensors
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+
+@dataclass
+class Camera:
+    W: int
+    H: int
+    fx: float
+    fy: float
+    cx: float
+    cy: float
+    baseline: float
+
+
+CAM_SMALL = Camera(752, 480, 458.0, 458.0, 367.0, 248.0, 0.11)        # 752x480, disparities 0-64 at 2 m +
+CAM_KITTI = Camera(1241, 376, 718.0, 718.0, 607.0, 185.0, 0.54)       # 1241x376, disparities 0-96
+CAM_HD = Camera(1280, 720, 640.0, 640.0, 640.0, 360.0, 0.075)         # 1280x720, disparities 0-128
+
+
+def fractal_texture(seed, n=1024, beta=1.0):
+    """1/f^beta noise (FFT-shaped), normalised to [0, 1]."""
+    rng = np.random.default_rng(seed)
+    fy = np.fft.fftfreq(n)[:, None]
+    fx = np.fft.rfftfreq(n)[None, :]
+    f = np.sqrt(fx * fx + fy * fy)
+    f[0, 0] = 1.0
+    spec = (rng.normal(size=f.shape) + 1j * rng.normal(size=f.shape)) / f ** beta
+    spec[0, 0] = 0.0
+    t = np.fft.irfftn(spec, s=(n, n))
+    t = (t - t.min()) / max(t.max() - t.min(), 1e-12)
+    return t.astype(np.float32)
+
+
+@dataclass
+class Scene:
+    centers: np.ndarray          # (P, 3)
+    axes_u: np.ndarray           # (P, 3)
+    axes_v: np.ndarray           # (P, 3)
+    half: np.ndarray             # (P, 2) half extents (m)
+    tex_id: np.ndarray           # (P,)
+    tex_scale: np.ndarray        # (P,) texels per metre
+    tex_off: np.ndarray          # (P, 2)
+    gain: np.ndarray             # (P,) brightness
+    textures: np.ndarray = field(repr=False)   # (K, n, n)
+
+
+def _rot(ax, ay, az):
+    cx, sx, cy, sy, cz, sz = math.cos(ax), math.sin(ax), math.cos(ay), math.sin(ay), math.cos(az), math.sin(az)
+    Rx = np.array([[1, 0, 0], [0, cx, -sx], [0, sx, cx]])
+    Ry = np.array([[cy, 0, sy], [0, 1, 0], [-sy, 0, cy]])
+    Rz = np.array([[cz, -sz, 0], [sz, cz, 0], [0, 0, 1]])
+    return Rz @ Ry @ Rx
+
+
+def scene_planes(seed, cam, n_planes=6, z0=2.0, z1=15.0, n_tex=4):
+    """n_planes - 1 random tilted planes at depths U(z0, z1) in the view, and a background plane behind them."""
+    rng = np.random.default_rng(seed)
+    tex = np.stack([fractal_texture(seed * 131 + k) for k in range(n_tex)])
+    C, U, V, Hx, T, S, O, G = [], [], [], [], [], [], [], []
+    C.append([0.0, 0.0, z1 + 1.0]); U.append([1.0, 0, 0]); V.append([0, 1.0, 0]); Hx.append([1e3, 1e3])
+    for _ in range(n_planes - 1):
+        z = rng.uniform(z0, z1)
+        x = rng.uniform(-0.4, 0.4) * z * cam.W / cam.fx
+        y = rng.uniform(-0.4, 0.4) * z * cam.H / cam.fy
+        R = _rot(rng.uniform(-0.5, 0.5), rng.uniform(-0.5, 0.5), rng.uniform(-0.3, 0.3))
+        C.append([x, y, z]); U.append(R[:, 0]); V.append(R[:, 1])
+        Hx.append([rng.uniform(0.15, 0.45) * z * cam.W / cam.fx, rng.uniform(0.15, 0.45) * z * cam.H / cam.fy])
+    P = len(C)
+    for _ in range(P):
+        T.append(rng.integers(0, n_tex)); S.append(rng.uniform(60.0, 200.0)); O.append(rng.uniform(0, 1024, 2))
+        G.append(rng.uniform(0.55, 1.0))
+    return Scene(np.array(C, float), np.array(U, float), np.array(V, float), np.array(Hx, float), np.array(T),
+                 np.array(S), np.array(O), np.array(G), tex)
+
+
+def scene_road(seed, length=600.0, n_tex=6):
+    """A driving corridor along +z: road (y = 1.65), facades at x = -7.5 and +8.5, boards every ~12 m, backdrop."""
+    rng = np.random.default_rng(seed)
+    tex = np.stack([fractal_texture(seed * 131 + k) for k in range(n_tex)])
+    C, U, V, Hx = [], [], [], []
+    ex, ey, ez = np.array([1.0, 0, 0]), np.array([0, 1.0, 0]), np.array([0, 0, 1.0])
+    C.append([0, 1.65, length / 2]); U.append(ex); V.append(ez); Hx.append([20.0, length])          # road
+    C.append([-7.5, -2.0, length / 2]); U.append(ez); V.append(ey); Hx.append([length, 6.0])       # left facade
+    C.append([8.5, -2.0, length / 2]); U.append(ez); V.append(ey); Hx.append([length, 6.0])        # right facade
+    C.append([0, -3.0, length + 50]); U.append(ex); V.append(ey); Hx.append([1e3, 1e3])           # backdrop
+    z = 6.0
+    while z < length:
+        side = rng.choice([-1.0, 1.0])
+        x = side * rng.uniform(2.5, 6.0)
+        R = _rot(0.0, rng.uniform(-0.6, 0.6), 0.0)
+        C.append([x, rng.uniform(-1.0, 0.8), z]); U.append(R[:, 0]); V.append(R[:, 1])
+        Hx.append([rng.uniform(0.6, 1.8), rng.uniform(0.6, 1.6)])
+        z += rng.uniform(6.0, 18.0)
+    P = len(C)
+    T = rng.integers(0, n_tex, P)
+    S = rng.uniform(40.0, 160.0, P)
+    O = rng.uniform(0, 1024, (P, 2))
+    G = rng.uniform(0.55, 1.0, P)
+    return Scene(np.array(C, float), np.array(U, float), np.array(V, float), np.array(Hx, float), T, S, O, G, tex)
+
+
+class Renderer:
+    """Holds a scene on a device and renders grey images for camera poses (R_wc, t_wc) of the LEFT camera."""
+
+    def __init__(self, scene, cam, device="cpu"):
+        self.cam = cam
+        self.dev = torch.device(device)
+        d = dict(dtype=torch.float32, device=self.dev)
+        self.C = torch.tensor(scene.centers, **d)
+        self.U = torch.tensor(scene.axes_u, **d)
+        self.V = torch.tensor(scene.axes_v, **d)
+        self.N = torch.cross(self.U, self.V, dim=1)
+        self.half = torch.tensor(scene.half, **d)
+        self.tid = torch.tensor(scene.tex_id, dtype=torch.long, device=self.dev)
+        self.tscale = torch.tensor(scene.tex_scale, **d)
+        self.toff = torch.tensor(scene.tex_off, **d)
+        self.gain = torch.tensor(scene.gain, **d)
+        self.tex = torch.tensor(scene.textures, **d)
+        v, u = torch.meshgrid(torch.arange(cam.H, **d), torch.arange(cam.W, **d), indexing="ij")
+        self.rays = torch.stack([(u - cam.cx) / cam.fx, (v - cam.cy) / cam.fy, torch.ones_like(u)], -1).reshape(-1, 3)
+
+    def _render(self, R, t, gen, noise):
+        d = (self.rays @ R.T)                                     # world directions (z-depth parametrised)
+        P = self.C.shape[0]
+        best = torch.full((d.shape[0],), float("inf"), device=self.dev)
+        val = torch.zeros(d.shape[0], device=self.dev)
+        n_tex = self.tex.shape[-1]
+        for p in range(P):
+            n = self.N[p]
+            den = d @ n
+            tt = ((self.C[p] - t) @ n) / torch.where(den.abs() < 1e-9, torch.full_like(den, 1e-9), den)
+            hit = t + tt[:, None] * d
+            rel = hit - self.C[p]
+            s1, s2 = rel @ self.U[p], rel @ self.V[p]
+            ok = (tt > 0.2) & (s1.abs() <= self.half[p, 0]) & (s2.abs() <= self.half[p, 1]) & (tt < best)
+            if not bool(ok.any()):
+                continue
+            tx = torch.remainder(s1 * self.tscale[p] + self.toff[p, 0], n_tex - 1)
+            ty = torch.remainder(s2 * self.tscale[p] + self.toff[p, 1], n_tex - 1)
+            x0, y0 = tx.floor().long().clamp(0, n_tex - 2), ty.floor().long().clamp(0, n_tex - 2)
+            ax, ay = tx - x0, ty - y0
+            T = self.tex[self.tid[p]]
+            a = T[y0, x0]; b = T[y0, x0 + 1]; c = T[y0 + 1, x0]; e = T[y0 + 1, x0 + 1]
+            g = (a + ax * (b - a)) * (1 - ay) + (c + ax * (e - c)) * ay
+            g = 20.0 + 215.0 * g * self.gain[p]
+            best = torch.where(ok, tt, best)
+            val = torch.where(ok, g, val)
+        if noise > 0:
+            val = val + noise * torch.randn(val.shape, generator=gen, device=self.dev)
+        img = torch.clamp(torch.round(val), 0, 255).to(torch.uint8).reshape(self.cam.H, self.cam.W)
+        return img
+
+    def pair(self, R_wc, t_wc, seed=0, noise=2.0):
+        """-> (left, right) uint8 tensors for the left camera pose (R_wc (3,3), t_wc (3,))."""
+        R = torch.as_tensor(np.asarray(R_wc), dtype=torch.float32, device=self.dev)
+        t = torch.as_tensor(np.asarray(t_wc), dtype=torch.float32, device=self.dev)
+        gen = torch.Generator(device=self.dev)
+        gen.manual_seed(int(seed))
+        left = self._render(R, t, gen, noise)
+        right = self._render(R, t + R[:, 0] * self.cam.baseline, gen, noise)
+        return left, right
+
+
+def yaw(a):
+    c, s = math.cos(a), math.sin(a)
+    return np.array([[c, 0, s], [0, 1, 0], [-s, 0, c]])
+
+
+def sequence(cam, n_frames, seed=0, device="cpu", step=1.0, yaw_sigma_deg=0.5, noise=2.0, scene=None):
+    """A forward-driving stereo sequence (step metres per frame, yaw noise): -> (left [F,H,W], right [F,H,W])."""
+    scene = scene if scene is not None else scene_road(seed, length=step * n_frames + 120.0)
+    rd = Renderer(scene, cam, device)
+    rng = np.random.default_rng(seed + 7)
+    L = torch.empty((n_frames, cam.H, cam.W), dtype=torch.uint8, device=rd.dev)
+    R = torch.empty_like(L)
+    for k in range(n_frames):
+        Rw = yaw(math.radians(rng.normal(0.0, yaw_sigma_deg)))
+        l, r = rd.pair(Rw, np.array([0.0, 0.0, step * k]), seed=seed * 100003 + k, noise=noise)
+        L[k] = l
+        R[k] = r
+    return L, R
