@@ -104,13 +104,22 @@ int xcb_front_lk_check_host(xcb_front* f, const double* As, const double* gs, in
 int xcb_front_pipeline_dev(xcb_front* f, const uint8_t* left, const uint8_t* right, int nframes, int budget, int half,
                            int dlo, int dhi, int match_prev, void* stream);
 int xcb_front_buffers(xcb_front* f, xcb_front_bufs* out);
-/* the same from host memory (H2D, pipeline, D2H of every result array into the host arrays of `out`) */
+/* the same from host memory (H2D, pipeline, D2H of every non-NULL result array into the host arrays of `out`, then a
+   wait on `stream`); host buffers in page-locked memory make the copies asynchronous */
 int xcb_front_pipeline_host(xcb_front* f, const uint8_t* left, const uint8_t* right, int nframes, int budget,
-                            int half, int dlo, int dhi, int match_prev, const xcb_front_bufs* out);
+                            int half, int dlo, int dhi, int match_prev, const xcb_front_bufs* out, void* stream);
 /* number of kernel launches the last pipeline call issued */
 int xcb_front_last_launches(const xcb_front* f);
 /* wait for `stream` (NULL = the front's own) and read the device error word -> XCB_OK or XCB_ERR_DEVICE */
 int xcb_front_sync_check(xcb_front* f, void* stream);
+/* Stage timing of the batched pipeline (no reference counterpart; the reference times stages on the host with
+   obs/latency.Ledger, latency.py:177-212): when on, every captured pipeline graph records an event at each stage
+   boundary.  xcb_front_stage_times sums, over the graphs replayed since the last read, the device time of each stage:
+   0 response, 1 noise floor, 2 thresholds + candidate lists, 3 greedy + rank + sub-pixel, 4 blur + ORB,
+   5 stereo, 6 Hamming + match.  Call after the stream has been synchronised. */
+#define XCB_FRONT_STAGES 7
+int xcb_front_set_stage_timing(xcb_front* f, int on);
+int xcb_front_stage_times(xcb_front* f, float* ms, int* ngraphs);
 
 #ifdef __cplusplus
 }

@@ -77,14 +77,40 @@ struct xcb_front {
     // pinned staging
     u8* h_stage;
     size_t h_stage_bytes;
-    // graph cache of the batched pipeline
-    cudaGraphExec_t gexec;
-    bool have_graph;
-    const void *g_left, *g_right;
-    int g_F, g_budget, g_half, g_dlo, g_dhi, g_match_prev;
-    cudaStream_t g_stream;
+    // graph cache of the batched pipeline: one executable graph per (inputs, sizes, options, stream)
+    struct GraphEntry {
+        cudaGraphExec_t exec;
+        const void *left, *right;
+        int F, budget, half, dlo, dhi, match_prev;
+        cudaStream_t stream;
+        unsigned long long used;
+        bool timed, fresh;
+        cudaEvent_t ev[XCB_FRONT_STAGES + 1];   // stage boundaries, recorded inside the graph when timed
+    };
+    std::vector<GraphEntry> graphs;
+    unsigned long long graph_clock;
+    bool stage_timing;
     int last_launches;
 };
+
+static void drop_graph(xcb_front::GraphEntry& g)
+{
+    cudaGraphExecDestroy(g.exec);
+    if (g.timed)
+        for (int i = 0; i <= XCB_FRONT_STAGES; ++i) cudaEventDestroy(g.ev[i]);
+}
+
+static void drop_graphs(xcb_front* f)
+{
+    for (auto& g : f->graphs) drop_graph(g);
+    f->graphs.clear();
+}
+
+// an event-record node of the graph being captured (External: replayed with the graph, readable by the host)
+static inline cudaError_t mark(const cudaEvent_t* ev, int i, cudaStream_t st)
+{
+    return ev ? cudaEventRecordWithFlags(ev[i], st, cudaEventRecordExternal) : cudaSuccess;
+}
 
 static int fail(xcb_front* f, int code, const std::string& msg)
 {
@@ -266,7 +292,7 @@ static int set_geometry(xcb_front* f, int budget)
         return fail(f, XCB_ERR_CAPACITY, "detect: budget " + std::to_string(budget) + " needs more cells than the front was created for");
     if (xcb_greedy_smem(g.ncell) > (size_t)xcb_greedy_smem_limit())
         return fail(f, XCB_ERR_CAPACITY, "detect: " + std::to_string(g.ncell) + " cells exceed the greedy kernel's shared memory");
-    CK(cudaStreamSynchronize(f->stream), "geometry sync");
+    CK(cudaDeviceSynchronize(), "geometry sync");
     CK(cudaMemcpy(f->d_ybeg, g.ybeg.data(), g.ybeg.size() * sizeof(int), cudaMemcpyHostToDevice), "upload geometry");
     CK(cudaMemcpy(f->d_xbeg, g.xbeg.data(), g.xbeg.size() * sizeof(int), cudaMemcpyHostToDevice), "upload geometry");
     CK(cudaMemcpy(f->d_coff, g.coff.data(), g.coff.size() * sizeof(int), cudaMemcpyHostToDevice), "upload geometry");
@@ -284,7 +310,7 @@ static int set_geometry(xcb_front* f, int budget)
     f->geom.coff = f->d_coff;
     f->geom.max_cell_px = g.max_px;
     f->geom_budget = budget;
-    f->have_graph = false;
+    drop_graphs(f);
     return XCB_OK;
 }
 
@@ -300,8 +326,8 @@ extern "C" int xcb_front_create(int width, int height, int cap, int max_frames, 
     f->dev_bytes = 0;
     f->calibrated = false;
     f->geom_budget = -1;
-    f->have_graph = false;
-    f->gexec = nullptr;
+    f->graph_clock = 0;
+    f->stage_timing = false;
     f->pts_cap = 0;
     f->ham_capL = f->ham_capN = 0;
     f->h_stage = nullptr;
@@ -381,7 +407,7 @@ extern "C" void xcb_front_destroy(xcb_front* f)
 {
     if (!f) return;
     if (f->stream) cudaStreamSynchronize(f->stream);
-    if (f->have_graph && f->gexec) cudaGraphExecDestroy(f->gexec);
+    drop_graphs(f);
     for (void* p : f->allocs) cudaFree(p);
     if (f->h_stage) cudaFreeHost(f->h_stage);
     if (f->stream) cudaStreamDestroy(f->stream);
@@ -398,13 +424,13 @@ extern "C" int xcb_front_set_calibration(xcb_front* f, int dy_vend, int dx_vend,
     if (!f || !kf7 || !pattern) return fail(f, XCB_ERR_ARG, "set_calibration: null argument");
     for (int i = 0; i < 1024; ++i)
         if (pattern[i] < -15 || pattern[i] > 15) return fail(f, XCB_ERR_ARG, "set_calibration: ORB pattern out of the 31-px patch");
-    CK(cudaStreamSynchronize(f->stream), "calibration sync");
+    CK(cudaDeviceSynchronize(), "calibration sync");
     CK(cudaMemcpy(f->d_kf, kf7, 7 * sizeof(float), cudaMemcpyHostToDevice), "upload kf");
     CK(cudaMemcpy(f->d_pat, pattern, 1024, cudaMemcpyHostToDevice), "upload pattern");
     f->dy_vend = dy_vend; f->dx_vend = dx_vend; f->blur_vr = blur_vr; f->blur_vc = blur_vc;
     f->Q = noise_q99;
     f->calibrated = true;
-    f->have_graph = false;
+    drop_graphs(f);
     return XCB_OK;
 }
 
@@ -468,20 +494,27 @@ extern "C" int xcb_front_blur_host(xcb_front* f, const uint8_t* gray, int blur_v
 }
 
 // detection + description of F frames already in d_left (results in slots 1..F of the chains); -> launches issued
-static int enqueue_detect(xcb_front* f, const u8* left, int F, int budget, cudaStream_t st, int* nl)
+static int enqueue_detect(xcb_front* f, const u8* left, int F, int budget, cudaStream_t st, int* nl,
+                          const cudaEvent_t* ev = nullptr)
 {
     const int H = f->H, W = f->W;
     int* counts = f->d_counts_chain + 1;
     u8* desc = f->d_desc_chain + (size_t)f->cap * 32;
     CK(cudaMemsetAsync(f->d_anypos, 0, F * sizeof(int), st), "memset");
+    CK(mark(ev, 0, st), "event");
     CK(xcb_launch_response(left, F, H, W, f->dy_vend, f->dx_vend, f->d_R, f->d_anypos, st), "response");
+    CK(mark(ev, 1, st), "event");
     CK(xcb_launch_noise(left, F, H, W, f->tree, f->d_nodeval, f->K, f->Q, f->d_floor, f->d_floorf, st), "noise");
+    CK(mark(ev, 2, st), "event");
     CK(xcb_launch_candidates(f->d_R, F, H, W, f->geom, f->d_floorf, f->d_anypos, f->d_thr, f->d_raw, f->d_sorted,
                              f->d_ccount, st), "candidates");
+    CK(mark(ev, 3, st), "event");
     CK(xcb_launch_greedy(f->d_R, F, H, W, f->geom, f->d_sorted, f->d_ccount, budget, f->cap, f->d_kp, counts,
                          f->d_rounds, f->d_err, st), "greedy");
+    CK(mark(ev, 4, st), "event");
     CK(xcb_launch_blur(left, F, H, W, f->d_kf, f->blur_vr, f->blur_vc, f->d_blur, st), "blur");
     CK(xcb_launch_orb(f->d_blur, F, f->Hp, f->Wp, f->d_kp, counts, f->cap, f->d_pat, desc, st), "orb");
+    CK(mark(ev, 5, st), "event");
     *nl += 9;
     return XCB_OK;
 }
@@ -703,13 +736,14 @@ extern "C" int xcb_front_lk_check_host(xcb_front* f, const double* As, const dou
 
 // ----------------------------------------------------------------------------------------------- batched pipeline
 static int enqueue_pipeline(xcb_front* f, const u8* left, const u8* right, int F, int budget, int half, int dlo,
-                            int dhi, int match_prev, cudaStream_t st, int* nl)
+                            int dhi, int match_prev, cudaStream_t st, int* nl, const cudaEvent_t* ev)
 {
-    int rc = enqueue_detect(f, left, F, budget, st, nl);
+    int rc = enqueue_detect(f, left, F, budget, st, nl, ev);
     if (rc) return rc;
     int* counts = f->d_counts_chain + 1;
     CK(xcb_launch_stereo(left, right, nullptr, F, f->H, f->W, nullptr, nullptr, nullptr, F, f->d_kp, counts, f->cap,
                          dlo, dhi, 0, half, f->d_d, f->d_sig, f->d_ok, f->d_zn, f->d_dy, f->d_err, st), "stereo");
+    CK(mark(ev, 6, st), "event");
     if (!match_prev) CK(cudaMemsetAsync(f->d_counts_chain, 0, sizeof(int), st), "memset");
     XcbHamPairs p;
     p.A = f->d_desc_chain;
@@ -722,6 +756,7 @@ static int enqueue_pipeline(xcb_front* f, const u8* left, const u8* right, int F
     CK(xcb_launch_hamming(p, f->d_b1, f->d_b2, f->d_bi, f->d_ci, st), "hamming");
     CK(xcb_launch_match_epilogue(p, f->d_b1, f->d_b2, f->d_bi, f->d_ci, 104, 0.8, f->d_m0, f->d_m1, f->cap,
                                  f->d_nmatch, st), "match");
+    CK(mark(ev, 7, st), "event");
     // carry the last frame's descriptors to slot 0 for the next call
     CK(cudaMemcpyAsync(f->d_desc_chain, f->d_desc_chain + (size_t)F * f->cap * 32, (size_t)f->cap * 32,
                        cudaMemcpyDeviceToDevice, st), "carry desc");
@@ -741,27 +776,73 @@ extern "C" int xcb_front_pipeline_dev(xcb_front* f, const uint8_t* left, const u
     int rc = set_geometry(f, budget);
     if (rc) return rc;
     cudaStream_t st = stream ? (cudaStream_t)stream : f->stream;
-    bool same = f->have_graph && f->g_left == left && f->g_right == right && f->g_F == nframes &&
-                f->g_budget == budget && f->g_half == half && f->g_dlo == dlo && f->g_dhi == dhi &&
-                f->g_match_prev == match_prev && f->g_stream == st;
-    if (!same) {
-        if (f->have_graph) { cudaGraphExecDestroy(f->gexec); f->have_graph = false; }
+    xcb_front::GraphEntry* hit = nullptr;
+    for (auto& g : f->graphs)
+        if (g.left == left && g.right == right && g.F == nframes && g.budget == budget && g.half == half &&
+            g.dlo == dlo && g.dhi == dhi && g.match_prev == match_prev && g.stream == st) { hit = &g; break; }
+    if (!hit) {
+        if (f->graphs.size() >= 16) {   // evict the least recently used graph
+            size_t lru = 0;
+            for (size_t i = 1; i < f->graphs.size(); ++i) if (f->graphs[i].used < f->graphs[lru].used) lru = i;
+            drop_graph(f->graphs[lru]);
+            f->graphs.erase(f->graphs.begin() + lru);
+        }
         int nl = 0;
         cudaGraph_t g;
+        xcb_front::GraphEntry e;
+        e.timed = f->stage_timing;
+        if (e.timed)
+            for (int i = 0; i <= XCB_FRONT_STAGES; ++i) CK(cudaEventCreate(&e.ev[i]), "event create");
         CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
-        rc = enqueue_pipeline(f, left, right, nframes, budget, half, dlo, dhi, match_prev, st, &nl);
+        rc = enqueue_pipeline(f, left, right, nframes, budget, half, dlo, dhi, match_prev, st, &nl,
+                              e.timed ? e.ev : nullptr);
         cudaError_t ec = cudaStreamEndCapture(st, &g);
-        if (rc) return rc;
-        if (ec != cudaSuccess) return cuda_fail(f, ec, "end capture");
-        ec = cudaGraphInstantiate(&f->gexec, g, 0);
+        if (rc || ec != cudaSuccess) {
+            if (e.timed)
+                for (int i = 0; i <= XCB_FRONT_STAGES; ++i) cudaEventDestroy(e.ev[i]);
+            if (rc) return rc;
+            return cuda_fail(f, ec, "end capture");
+        }
+        ec = cudaGraphInstantiate(&e.exec, g, 0);
         cudaGraphDestroy(g);
         if (ec != cudaSuccess) return cuda_fail(f, ec, "graph instantiate");
-        f->have_graph = true;
-        f->g_left = left; f->g_right = right; f->g_F = nframes; f->g_budget = budget; f->g_half = half;
-        f->g_dlo = dlo; f->g_dhi = dhi; f->g_match_prev = match_prev; f->g_stream = st;
+        e.left = left; e.right = right; e.F = nframes; e.budget = budget; e.half = half; e.dlo = dlo; e.dhi = dhi;
+        e.match_prev = match_prev; e.stream = st; e.used = 0;
+        f->graphs.push_back(e);
+        hit = &f->graphs.back();
         f->last_launches = nl;
     }
-    CK(cudaGraphLaunch(f->gexec, st), "graph launch");
+    hit->used = ++f->graph_clock;
+    hit->fresh = true;
+    CK(cudaGraphLaunch(hit->exec, st), "graph launch");
+    return XCB_OK;
+}
+
+extern "C" int xcb_front_set_stage_timing(xcb_front* f, int on)
+{
+    if (!f) return fail(f, XCB_ERR_ARG, "set_stage_timing: null handle");
+    CK(cudaDeviceSynchronize(), "sync");
+    if ((bool)on != f->stage_timing) drop_graphs(f);
+    f->stage_timing = on != 0;
+    return XCB_OK;
+}
+
+extern "C" int xcb_front_stage_times(xcb_front* f, float* ms, int* ngraphs)
+{
+    if (!f || !ms) return fail(f, XCB_ERR_ARG, "stage_times: null argument");
+    for (int i = 0; i < XCB_FRONT_STAGES; ++i) ms[i] = 0.0f;
+    int n = 0;
+    for (auto& g : f->graphs) {
+        if (!g.timed || !g.fresh) continue;
+        for (int i = 0; i < XCB_FRONT_STAGES; ++i) {
+            float t = 0.0f;
+            CK(cudaEventElapsedTime(&t, g.ev[i], g.ev[i + 1]), "elapsed");
+            ms[i] += t;
+        }
+        g.fresh = false;
+        ++n;
+    }
+    if (ngraphs) *ngraphs = n;
     return XCB_OK;
 }
 
@@ -785,12 +866,13 @@ extern "C" int xcb_front_buffers(xcb_front* f, xcb_front_bufs* o)
 }
 
 extern "C" int xcb_front_pipeline_host(xcb_front* f, const uint8_t* left, const uint8_t* right, int nframes,
-                                       int budget, int half, int dlo, int dhi, int match_prev, const xcb_front_bufs* out)
+                                       int budget, int half, int dlo, int dhi, int match_prev, const xcb_front_bufs* out,
+                                       void* stream)
 {
     if (!f || !left || !right || !out) return fail(f, XCB_ERR_ARG, "pipeline_host: null argument");
     if (nframes < 1 || nframes > f->maxF) return fail(f, XCB_ERR_CAPACITY, "pipeline_host: frame count out of range");
     size_t bytes = (size_t)nframes * f->W * f->H;
-    cudaStream_t st = f->stream;
+    cudaStream_t st = stream ? (cudaStream_t)stream : f->stream;
     // host -> device straight from the caller's (ideally pinned) buffers
     CK(cudaMemcpyAsync(f->d_left, left, bytes, cudaMemcpyHostToDevice, st), "H2D left");
     CK(cudaMemcpyAsync(f->d_right, right, bytes, cudaMemcpyHostToDevice, st), "H2D right");

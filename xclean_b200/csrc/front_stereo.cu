@@ -22,12 +22,25 @@
 
 static __host__ __device__ __forceinline__ int win_w(int half) { return ((MAXD + 2 * half) + 3) & ~3; }
 
-size_t xcb_stereo_smem_per_warp(int half, int band)
+#define LK_TERMS 9      // the LK's sums except sum(1 * 1) = NPIX, which is exact
+
+// per-warp shared memory: Td [NPIX] f64 | T2d [NPIX] f64 | sc [MAXD] f64 | jb [MAXD] i8 | U, where U holds the image
+// window (float32, rows x win_w) during the two searches and the LK term table (LK_TERMS x NPIX f64) afterwards
+static __host__ __device__ __forceinline__ size_t stereo_off_u(int half)
 {
     int pw = 2 * half + 1, npix = pw * pw;
-    size_t rows = (size_t)(pw + 2 * band);
-    return (size_t)npix * 8 * 2 + MAXD * 8 + MAXD + rows * win_w(half) * 4;
+    return ((size_t)npix * 16 + MAXD * 8 + MAXD + 15) & ~(size_t)15;
 }
+
+static __host__ __device__ __forceinline__ size_t stereo_warp_bytes(int half, int band)
+{
+    int pw = 2 * half + 1, npix = pw * pw;
+    size_t win = (size_t)(pw + 2 * band) * win_w(half) * 4;
+    size_t terms = (size_t)LK_TERMS * npix * 8;
+    return (stereo_off_u(half) + (win > terms ? win : terms) + 15) & ~(size_t)15;
+}
+
+size_t xcb_stereo_smem_per_warp(int half, int band) { return stereo_warp_bytes(half, band); }
 
 // ---------------------------------------------------------------- OpenBLAS 3x3 arithmetic (as the oracle restates it)
 __device__ __forceinline__ void ob_getf2(double a[3][3], int piv[3])
@@ -237,6 +250,20 @@ __device__ __forceinline__ void zncc_q(const float* win, int ww, int row0, const
     }
 }
 
+// zncc_q with the chain count nq (1..4, uniform across the warp) chosen at run time
+template <int HALF, bool FLT>
+__device__ __forceinline__ void zncc_n(int nq, const float* win, int ww, int row0, const int col0[4],
+                                       const bool valid[4], const double* T, double ts, double out[4])
+{
+    out[0] = out[1] = out[2] = out[3] = -2.0;
+    switch (nq) {
+        case 1: zncc_q<HALF, FLT, 1>(win, ww, row0, col0, valid, T, ts, out); break;
+        case 2: zncc_q<HALF, FLT, 2>(win, ww, row0, col0, valid, T, ts, out); break;
+        case 3: zncc_q<HALF, FLT, 3>(win, ww, row0, col0, valid, T, ts, out); break;
+        default: zncc_q<HALF, FLT, 4>(win, ww, row0, col0, valid, T, ts, out); break;
+    }
+}
+
 // warp argmax, first maximum in increasing index (strict '>' scan): ties keep the smaller index
 __device__ __forceinline__ void warp_argmax(double& v, int& idx)
 {
@@ -262,13 +289,13 @@ __global__ void __launch_bounds__(ST_WARPS * 32) k_stereo(
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int ww = win_w(HALF);
-    const size_t per_warp = (size_t)NPIX * 16 + MAXD * 8 + MAXD + (size_t)(PW + 2 * band) * ww * 4;
-    unsigned char* base = smem_raw + (size_t)wid * ((per_warp + 15) & ~(size_t)15);
+    unsigned char* base = smem_raw + (size_t)wid * stereo_warp_bytes(HALF, band);
     double* Td = (double*)base;
     double* T2d = Td + NPIX;
     double* sc = T2d + NPIX;
-    float* win = (float*)(sc + MAXD);
-    signed char* jb = (signed char*)(win + (size_t)(PW + 2 * band) * ww);
+    signed char* jb = (signed char*)(sc + MAXD);
+    float* win = (float*)(base + stereo_off_u(HALF));
+    double* terms = (double*)(base + stereo_off_u(HALF));     // the LK term table, after the searches
 
     const long long p = (long long)blockIdx.x * ST_WARPS + wid;
     int f = 0;
@@ -340,13 +367,14 @@ __global__ void __launch_bounds__(ST_WARPS * 32) k_stereo(
         }
         double best[4];
         int bj[4] = {0, 0, 0, 0};
-        zncc_q<HALF, FLT, 4>(win, ww, band, col, val, Td, ts, best);
+        const int nq = (int)(hi - lo) / 32 + 1;
+        zncc_n<HALF, FLT>(nq, win, ww, band, col, val, Td, ts, best);
         for (int j = 1; j <= band; ++j) {
             double z[4];
-            zncc_q<HALF, FLT, 4>(win, ww, band - j, col, val, Td, ts, z);
+            zncc_n<HALF, FLT>(nq, win, ww, band - j, col, val, Td, ts, z);
 #pragma unroll
             for (int q = 0; q < 4; ++q) if (z[q] > best[q]) { best[q] = z[q]; bj[q] = -j; }
-            zncc_q<HALF, FLT, 4>(win, ww, band + j, col, val, Td, ts, z);
+            zncc_n<HALF, FLT>(nq, win, ww, band + j, col, val, Td, ts, z);
 #pragma unroll
             for (int q = 0; q < 4; ++q) if (z[q] > best[q]) { best[q] = z[q]; bj[q] = j; }
         }
@@ -422,7 +450,7 @@ __global__ void __launch_bounds__(ST_WARPS * 32) k_stereo(
 #pragma unroll
         for (int q = 0; q < 4; ++q) { col[q] = lane + 32 * q; val[q] = col[q] <= dmax; }
         double z[4];
-        zncc_q<HALF, false, 4>(win, ww, 0, col, val, T2d, rsd, z);
+        zncc_n<HALF, false>(dmax / 32 + 1, win, ww, 0, col, val, T2d, rsd, z);
 #pragma unroll
         for (int q = 0; q < 4; ++q)
             if (val[q] && z[q] > lrb) { lrb = z[q]; lrd = col[q]; }
@@ -456,33 +484,37 @@ __global__ void __launch_bounds__(ST_WARPS * 32) k_stereo(
     bool okk = false;
     double sig = 0.0;
     for (int it = 0; it <= LK_ITERS; ++it) {
-        double S = 0.0;
-        if (lane < 10) {
-            for (int k = 0; k < NPIX; ++k) {
-                double rv, rg;
-                double px = __dadd_rn(u, (double)(k % PW - HALF)), py = __dadd_rn(v, (double)(k / PW - HALF));
-                bil(R, H, W, __dsub_rn(px, d), __dadd_rn(py, voff), &rv, &rg);
-                double r = __dsub_rn(Tl[k], __dadd_rn(__dmul_rn(a, rv), b));
-                double J0 = __dmul_rn(-a, rg), J1 = rv;
-                double term;
-                switch (lane) {
-                    case 0: term = __dmul_rn(J0, r); break;
-                    case 1: term = __dmul_rn(J1, r); break;
-                    case 2: term = r; break;
-                    case 3: term = __dmul_rn(J0, J0); break;
-                    case 4: term = __dmul_rn(J0, J1); break;
-                    case 5: term = J0; break;
-                    case 6: term = __dmul_rn(J1, J1); break;
-                    case 7: term = J1; break;
-                    case 8: term = 1.0; break;
-                    default: term = __dmul_rn(r, r); break;
-                }
-                S = __dadd_rn(S, term);
-            }
+        // every patch pixel's residual and Jacobian terms, all lanes in parallel (terms[t][k]); then lane t sums term
+        // t over k = 0..NPIX-1 in the CPU's order.  Table rows: J0 r, J1 r, r, J0 J0, J0 J1, J0, J1 J1, J1, r r.
+        for (int k = lane; k < NPIX; k += 32) {
+            double rv, rg;
+            double px = __dadd_rn(u, (double)(k % PW - HALF)), py = __dadd_rn(v, (double)(k / PW - HALF));
+            bil(R, H, W, __dsub_rn(px, d), __dadd_rn(py, voff), &rv, &rg);
+            double r = __dsub_rn(Tl[k], __dadd_rn(__dmul_rn(a, rv), b));
+            double J0 = __dmul_rn(-a, rg), J1 = rv;
+            terms[0 * NPIX + k] = __dmul_rn(J0, r);
+            terms[1 * NPIX + k] = __dmul_rn(J1, r);
+            terms[2 * NPIX + k] = r;
+            terms[3 * NPIX + k] = __dmul_rn(J0, J0);
+            terms[4 * NPIX + k] = __dmul_rn(J0, J1);
+            terms[5 * NPIX + k] = J0;
+            terms[6 * NPIX + k] = __dmul_rn(J1, J1);
+            terms[7 * NPIX + k] = J1;
+            terms[8 * NPIX + k] = __dmul_rn(r, r);
         }
+        __syncwarp();
+        double S = 0.0;
+        if (lane < LK_TERMS && (lane < 8 || it == LK_ITERS)) {
+            const double* tr = terms + lane * NPIX;
+#pragma unroll 9
+            for (int k = 0; k < NPIX; ++k) S = __dadd_rn(S, tr[k]);
+        }
+        __syncwarp();
         double Sv[10];
 #pragma unroll
-        for (int q = 0; q < 10; ++q) Sv[q] = __shfl_sync(0xffffffffu, S, q);
+        for (int q = 0; q < 8; ++q) Sv[q] = __shfl_sync(0xffffffffu, S, q);
+        Sv[9] = __shfl_sync(0xffffffffu, S, 8);
+        Sv[8] = (double)NPIX;      // sum of 1 x 1 over the patch: exact
         int go = 1;
         if (lane == 0) {
             double A[3][3] = {{Sv[3], Sv[4], Sv[5]}, {Sv[4], Sv[6], Sv[7]}, {Sv[5], Sv[7], Sv[8]}};

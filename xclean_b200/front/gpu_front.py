@@ -505,7 +505,18 @@ class GpuFront:
     def last_launches(self):
         return int(self.L.xcb_front_last_launches(self._h))
 
-    def pipeline(self, left, right, budget, half=HALF, dlo=0, dhi=MAX_DISP - 1, match_prev=True, out=None):
+    def set_stage_timing(self, on):
+        """Record device events at the stage boundaries of every (re)captured pipeline graph."""
+        self._chk(self.L.xcb_front_set_stage_timing(self._h, int(bool(on))), "stage timing")
+
+    def stage_times(self):
+        """-> ({stage: ms summed over the graphs replayed since the last read}, number of graphs); sync first."""
+        ms = np.zeros(len(_lib.FRONT_STAGES), np.float32)
+        n = ctypes.c_int(0)
+        self._chk(self.L.xcb_front_stage_times(self._h, _lib.ptr(ms), ctypes.byref(n)), "stage times")
+        return dict(zip(_lib.FRONT_STAGES, (float(x) for x in ms))), int(n.value)
+
+    def pipeline(self, left, right, budget, half=HALF, dlo=0, dhi=MAX_DISP - 1, match_prev=True, out=None, stream=0):
         """The batched per-frame path from host arrays: left/right [F,H,W] -> dict of host arrays (frame-major)."""
         self._own()
         self._require()
@@ -519,8 +530,8 @@ class GpuFront:
             a = out.get(n)
             setattr(b, n, a.ctypes.data if a is not None else None)
         self._chk(self.L.xcb_front_pipeline_host(self._h, _lib.ptr(Lh), _lib.ptr(Rh), F, int(budget), int(half),
-                                                 int(dlo), int(dhi), int(bool(match_prev)), ctypes.byref(b)),
-                  "pipeline")
+                                                 int(dlo), int(dhi), int(bool(match_prev)), ctypes.byref(b),
+                                                 ctypes.c_void_p(int(stream) or None)), "pipeline")
         return out
 
     def alloc_outputs(self, F):

@@ -42,7 +42,7 @@ def fractal_texture(seed, n=1024, beta=1.0):
     f[0, 0] = 1.0
     spec = (rng.normal(size=f.shape) + 1j * rng.normal(size=f.shape)) / f ** beta
     spec[0, 0] = 0.0
-    t = np.fft.irfftn(spec, s=(n, n))
+    t = np.fft.irfftn(spec, s=(n, n), axes=(0, 1))
     t = (t - t.min()) / max(t.max() - t.min(), 1e-12)
     return t.astype(np.float32)
 
@@ -135,13 +135,20 @@ class Renderer:
         v, u = torch.meshgrid(torch.arange(cam.H, **d), torch.arange(cam.W, **d), indexing="ij")
         self.rays = torch.stack([(u - cam.cx) / cam.fx, (v - cam.cy) / cam.fy, torch.ones_like(u)], -1).reshape(-1, 3)
 
+    def _visible(self, R, t, max_depth=250.0):
+        """planes not entirely behind the camera nor (small ones) beyond max_depth"""
+        Cn = self.C.cpu().numpy()
+        rad = np.linalg.norm(self.half.cpu().numpy(), axis=1)
+        fwd = R[:, 2].cpu().numpy()
+        dz = (Cn - t.cpu().numpy()) @ fwd
+        return [p for p in range(len(Cn)) if dz[p] + rad[p] > 0.2 and (dz[p] - rad[p] < max_depth or rad[p] > 100)]
+
     def _render(self, R, t, gen, noise):
         d = (self.rays @ R.T)                                     # world directions (z-depth parametrised)
-        P = self.C.shape[0]
         best = torch.full((d.shape[0],), float("inf"), device=self.dev)
         val = torch.zeros(d.shape[0], device=self.dev)
         n_tex = self.tex.shape[-1]
-        for p in range(P):
+        for p in self._visible(R, t):
             n = self.N[p]
             den = d @ n
             tt = ((self.C[p] - t) @ n) / torch.where(den.abs() < 1e-9, torch.full_like(den, 1e-9), den)
