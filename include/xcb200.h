@@ -121,6 +121,48 @@ int xcb_front_sync_check(xcb_front* f, void* stream);
 int xcb_front_set_stage_timing(xcb_front* f, int on);
 int xcb_front_stage_times(xcb_front* f, float* ms, int* ngraphs);
 
+/* ============================================== sliding-window bundle adjustment ============================================== */
+/* A batch of windows of the reference's stereo window solve (src/xclean/vio/window.py: Problem :768-792, solve
+   :889-982), concatenated: window w owns slots [slot_off[w], slot_off[w] + P[w]) and landmarks [lm_off[w],
+   lm_off[w] + L[w]); landmark l's observation rows are [lm_ob[l], lm_ob[l + 1]) (at most 32), its host and the
+   rows' poses are window-local slot indices.  All pointers are device memory. */
+typedef struct {
+    int nw;                     /* windows */
+    const int32_t* P;           /* [nw] slots (<= 20) */
+    const int32_t* L;           /* [nw] landmarks */
+    const int32_t* slot_off;    /* [nw] */
+    const int32_t* lm_off;      /* [nw] */
+    const int32_t* hold;        /* [nw] slot held fixed (-1 none), or NULL */
+    const int32_t* order;       /* [nw] processing order (largest first), or NULL */
+    const double* cam;          /* [nw][6] fx fy cx cy B huber_k */
+    const double* ext;          /* [nw][12] Rbc (row-major) pbc */
+    double* Rwb;                /* [S][9] in / out */
+    double* pwb;                /* [S][3] in / out */
+    double* lmp;                /* [Lt][3] (a, b, rho) in / out */
+    const int32_t* lm_host;     /* [Lt] */
+    const uint8_t* lm_mask;     /* [Lt] */
+    const double* rho_meas;     /* [Lt] */
+    const double* rho_isig;     /* [Lt] */
+    const int32_t* lm_ob;       /* [Lt + 1] */
+    const int32_t* ob_pose;     /* [Mt] */
+    const uint8_t* ob_cam;      /* [Mt] 0 = left (u, v), 1 = right u_R */
+    const double* ob_z;         /* [Mt][2] */
+    const double* ob_isig;      /* [Mt] */
+    const uint8_t* ob_valid;    /* [Mt] */
+} xcb_ba_windows;
+
+#define XCB_BA_FP64 0           /* everything in float64: the plain form */
+#define XCB_BA_MIXED 1          /* FP32 linearisation + Schur, FP64 Cholesky, one FP64 refinement step */
+
+/* Device scratch the batched solve needs for `Lt` landmarks (trial landmark states and the work counter). */
+size_t xcb_ba_scratch_bytes(int nw, int Lt);
+/* window.solve (window.py:889-982, purely visual, fixed `iters` LM iterations from lam0) for every window of the batch
+   in ONE persistent launch (no reference counterpart as one call; the reference solves one window per call on the
+   CPU).  stats [nw][8] = cost0, cost, accepted, lam, status (0 ok, -1 window too large), iters, -, -;
+   dx0 [nw][dx0_stride] (optional) = the first iteration's pose step.  grid = 0: one CTA per SM. */
+int xcb_ba_solve_windows_dev(const xcb_ba_windows* w, int max_slots, int iters, double lam0, int mode, double* stats,
+                             double* dx0, int dx0_stride, void* scratch, size_t scratch_bytes, int grid, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

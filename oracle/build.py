@@ -1,4 +1,4 @@
-"""Build recipe for the CPU oracle (test infrastructure): oracle/front_oracle.c -> oracle/liboracle.so.
+"""Build recipe for the CPU oracle (test infrastructure): oracle/{front,ba}_oracle.c -> oracle/liboracle.so.
 
 Strict IEEE: -ffp-contract=off and no fast-math, so every fused multiply-add in the oracle is an explicit fma()."""
 import os
@@ -6,15 +6,15 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SRC = os.path.join(HERE, "front_oracle.c")
+SRCS = [os.path.join(HERE, f) for f in ("front_oracle.c", "ba_oracle.c")]
 OUT = os.path.join(HERE, "liboracle.so")
 
 
 def build(force=False):
-    if not force and os.path.exists(OUT) and os.path.getmtime(OUT) >= os.path.getmtime(SRC):
+    if not force and os.path.exists(OUT) and all(os.path.getmtime(OUT) >= os.path.getmtime(s) for s in SRCS):
         return OUT
     cmd = ["gcc", "-O2", "-march=x86-64-v2", "-mfma", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-shared",
-           "-fPIC", "-o", OUT + ".tmp", SRC, "-lm"]
+           "-fPIC", "-o", OUT + ".tmp"] + SRCS + ["-lm"]
     subprocess.check_call(cmd)
     os.replace(OUT + ".tmp", OUT)
     return OUT

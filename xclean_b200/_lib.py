@@ -61,6 +61,21 @@ _SIGS = {
 FRONT_STAGES = ("response", "noise_floor", "candidates", "greedy", "orb", "stereo", "match")
 
 
+class BaWindows(ctypes.Structure):
+    _fields_ = [("nw", c_int)] + [(n, c_void_p) for n in (
+        "P", "L", "slot_off", "lm_off", "hold", "order", "cam", "ext", "Rwb", "pwb", "lmp", "lm_host", "lm_mask",
+        "rho_meas", "rho_isig", "lm_ob", "ob_pose", "ob_cam", "ob_z", "ob_isig", "ob_valid")]
+
+
+XCB_BA_FP64 = 0
+XCB_BA_MIXED = 1
+_SIGS.update({
+    "xcb_ba_scratch_bytes": (c_size_t, [c_int, c_int]),
+    "xcb_ba_solve_windows_dev": (c_int, [ctypes.POINTER(BaWindows), c_int, c_int, c_double, c_int, P, P, c_int, P,
+                                         c_size_t, c_int, P]),
+})
+
+
 def declared_symbols():
     """Every entry point the header declares (the loader binds exactly these)."""
     return sorted(_SIGS)

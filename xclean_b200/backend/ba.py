@@ -1,0 +1,131 @@
+"""Bundle adjustment on the device: the batched sliding-window solve (the reference's window.solve model) and, in
+backend/ba_id.py, the drop-in _solve_gpu / _solve_gpu_id of src/xclean/backend/ba.py.
+
+    res = solve_batch(windows, iters=5, lam0=1e-4, precision="mixed", hold=0)
+    # windows: synth_ba.Window objects (the fields of vio/window.Problem); solved in place
+    # res: dict(cost0, cost, accepted, lam, status (per window), dx0 (the first pose step per window))
+
+    bs = BatchSolver(windows, device)       # pack once, keep resident on the device
+    bs.solve(iters, lam0, precision)        # one persistent launch for every window; results stay on the device
+
+Every call goes through libxcb200.so's C ABI (xcb_ba_solve_windows_dev); there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from .. import _lib
+
+PRECISIONS = {"fp64": _lib.XCB_BA_FP64, "mixed": _lib.XCB_BA_MIXED}
+MAX_SLOTS = 20
+MAX_ROWS_PER_LANDMARK = 32
+
+
+def pack_windows(windows, hold=0):
+    """Concatenate windows into the batch layout of xcb_ba_windows (host numpy arrays)."""
+    nw = len(windows)
+    P = np.array([w.Rwb.shape[0] for w in windows], np.int32)
+    L = np.array([w.lmp.shape[0] for w in windows], np.int32)
+    M = np.array([w.ob_pose.shape[0] for w in windows], np.int64)
+    if P.max(initial=0) > MAX_SLOTS:
+        raise ValueError("solve_batch: a window has %d slots (at most %d)" % (P.max(), MAX_SLOTS))
+    slot_off = np.zeros(nw, np.int32)
+    lm_off = np.zeros(nw, np.int32)
+    if nw:
+        slot_off[1:] = np.cumsum(P)[:-1]
+        lm_off[1:] = np.cumsum(L)[:-1]
+    ob_base = np.zeros(nw + 1, np.int64)
+    ob_base[1:] = np.cumsum(M)
+    lm_ob = np.concatenate([w.ob_start[:-1].astype(np.int64) + ob_base[i] for i, w in enumerate(windows)]
+                           + [np.array([ob_base[-1]], np.int64)])
+    rows = np.diff(lm_ob)
+    if len(rows) and rows.max() > MAX_ROWS_PER_LANDMARK:
+        raise ValueError("solve_batch: a landmark has %d observation rows (at most %d)" % (rows.max(),
+                                                                                       MAX_ROWS_PER_LANDMARK))
+    cat = lambda name, dt: np.ascontiguousarray(np.concatenate([np.asarray(getattr(w, name)).reshape(
+        len(getattr(w, name)), -1) for w in windows]).astype(dt)) if nw else np.zeros(0, dt)
+    hold_a = np.full(nw, -1 if hold is None else int(hold), np.int32)
+    cam = np.array([[w.fx, w.fy, w.cx, w.cy, w.B, w.huber_k] for w in windows], np.float64).reshape(nw, 6)
+    ext = np.array([np.concatenate([np.asarray(w.Rbc, np.float64).ravel(), np.asarray(w.pbc, np.float64).ravel()])
+                    for w in windows], np.float64).reshape(nw, 12)
+    work = P.astype(np.int64) ** 2 * 36 + M.astype(np.int64) * 64
+    order = np.argsort(-work, kind="stable").astype(np.int32)
+    return dict(P=P, L=L, slot_off=slot_off, lm_off=lm_off, hold=hold_a, order=order, cam=cam, ext=ext,
+                Rwb=cat("Rwb", np.float64).reshape(-1, 9), pwb=cat("pwb", np.float64).reshape(-1, 3),
+                lmp=cat("lmp", np.float64).reshape(-1, 3), lm_host=cat("lm_host", np.int32).ravel(),
+                lm_mask=cat("lm_mask", np.uint8).ravel(), rho_meas=cat("rho_meas", np.float64).ravel(),
+                rho_isig=cat("rho_isig", np.float64).ravel(), lm_ob=lm_ob.astype(np.int32),
+                ob_pose=cat("ob_pose", np.int32).ravel(), ob_cam=cat("ob_cam", np.uint8).ravel(),
+                ob_z=cat("ob_z", np.float64).reshape(-1, 2), ob_isig=cat("ob_isig", np.float64).ravel(),
+                ob_valid=cat("ob_valid", np.uint8).ravel(), max_slots=int(P.max(initial=1)), nw=nw)
+
+
+class BatchSolver:
+    """A packed batch resident on the device (torch tensors for the memory; the kernels are libxcb200's)."""
+
+    FIELDS = ("P", "L", "slot_off", "lm_off", "hold", "order", "cam", "ext", "Rwb", "pwb", "lmp", "lm_host",
+              "lm_mask", "rho_meas", "rho_isig", "lm_ob", "ob_pose", "ob_cam", "ob_z", "ob_isig", "ob_valid")
+
+    def __init__(self, windows, device="cuda", hold=0, packed=None):
+        import torch
+        self.torch = torch
+        self.dev = torch.device(device)
+        self.host = packed if packed is not None else pack_windows(windows, hold)
+        self.nw = self.host["nw"]
+        self.max_slots = self.host["max_slots"]
+        self.t = {k: torch.from_numpy(np.ascontiguousarray(self.host[k])).to(self.dev) for k in self.FIELDS}
+        self.init = {k: self.t[k].clone() for k in ("Rwb", "pwb", "lmp")}
+        self.stats = torch.zeros((max(self.nw, 1), 8), dtype=torch.float64, device=self.dev)
+        self.dx0 = torch.zeros((max(self.nw, 1), 6 * MAX_SLOTS), dtype=torch.float64, device=self.dev)
+        Lt = int(self.host["lmp"].shape[0])
+        L = _lib.lib()
+        nb = int(L.xcb_ba_scratch_bytes(self.nw, Lt))
+        self.scratch = torch.zeros(nb, dtype=torch.uint8, device=self.dev)
+        self.desc = _lib.BaWindows()
+        self.desc.nw = self.nw
+        for k in self.FIELDS:
+            setattr(self.desc, k, self.t[k].data_ptr())
+
+    def reset(self):
+        for k in ("Rwb", "pwb", "lmp"):
+            self.t[k].copy_(self.init[k])
+
+    def solve(self, iters=5, lam0=1e-4, precision="mixed", stream=None, grid=0):
+        """One persistent launch over every window (asynchronous on `stream`, torch's current stream by default)."""
+        torch = self.torch
+        s = stream if stream is not None else torch.cuda.current_stream(self.dev)
+        rc = _lib.lib().xcb_ba_solve_windows_dev(ctypes.byref(self.desc), self.max_slots, int(iters), float(lam0),
+                                                 PRECISIONS[precision], self.stats.data_ptr(), self.dx0.data_ptr(),
+                                                 6 * MAX_SLOTS, self.scratch.data_ptr(), self.scratch.numel(),
+                                                 int(grid), ctypes.c_void_p(s.cuda_stream or None))
+        _lib.check(rc, None, "xcb_ba_solve_windows_dev")
+
+    def results(self):
+        st = self.stats.cpu().numpy()[:self.nw]
+        return {"cost0": st[:, 0], "cost": st[:, 1], "accepted": st[:, 2].astype(np.int64), "lam": st[:, 3],
+                "status": st[:, 4].astype(np.int64), "dx0": self.dx0.cpu().numpy()[:self.nw]}
+
+    def unpack_into(self, windows):
+        Rwb = self.t["Rwb"].cpu().numpy()
+        pwb = self.t["pwb"].cpu().numpy()
+        lmp = self.t["lmp"].cpu().numpy()
+        so, lo = self.host["slot_off"], self.host["lm_off"]
+        for i, w in enumerate(windows):
+            P, L = w.Rwb.shape[0], w.lmp.shape[0]
+            w.Rwb[:] = Rwb[so[i]:so[i] + P].reshape(P, 3, 3)
+            w.pwb[:] = pwb[so[i]:so[i] + P]
+            w.lmp[:] = lmp[lo[i]:lo[i] + L]
+
+
+def solve_batch(windows, iters=5, lam0=1e-4, precision="mixed", hold=0, device="cuda"):
+    """window.solve for every window in one persistent device launch; windows are updated in place."""
+    bs = BatchSolver(windows, device, hold)
+    bs.solve(iters, lam0, precision)
+    bs.torch.cuda.synchronize(bs.dev)
+    bs.unpack_into(windows)
+    res = bs.results()
+    for i, w in enumerate(windows):
+        res.setdefault("dx0_list", []).append(res["dx0"][i][:6 * w.Rwb.shape[0]])
+    return res

@@ -1,0 +1,13 @@
+// ba_kernels.h -- host-side launchers of the bundle-adjustment kernels (ba_*.cu), used by ba_api.cu.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "xcb200.h"
+
+typedef xcb_ba_windows XcbBaWindows;
+
+size_t xcb_ba_smem_bytes(int maxP);
+int xcb_ba_max_slots();
+cudaError_t xcb_launch_ba_windows(const XcbBaWindows& d, int max_slots, int iters, double lam0, int mode,
+                                  double* stats, double* dx0, int dx0_stride, double* lmp_trial, int* counter,
+                                  int grid, cudaStream_t st);

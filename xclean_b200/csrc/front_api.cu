@@ -19,6 +19,7 @@
 static thread_local std::string g_last_error;
 
 extern "C" const char* xcb_last_error(void) { return g_last_error.c_str(); }
+void xcb_set_last_error(const std::string& m) { g_last_error = m; }
 extern "C" int xcb_version(void) { return 1; }
 
 struct xcb_front {

@@ -211,8 +211,8 @@ __device__ __forceinline__ double zncc_finish(double s, double s2, double sx, do
 // Q ZNCCs at once on a shared-memory window: patch q's top-left at (row0, col0[q]); T = template minus its mean.
 // FLT: pixel sums in sequential float64 (shifted float32 image); else exact integer sums.
 template <int HALF, bool FLT, int Q>
-__device__ __forceinline__ void zncc_q(const float* win, int ww, int row0, const int col0[Q], const bool valid[Q],
-                                       const double* T, double ts, double out[Q])
+__device__ __forceinline__ void zncc_q(const float* win, int ww, int row0, const int* col0, const bool* valid,
+                                       const double* T, double ts, double* out)
 {
     constexpr int PW = 2 * HALF + 1, NPIX = PW * PW;
     double sx[Q], s[Q], s2[Q];
@@ -222,6 +222,7 @@ __device__ __forceinline__ void zncc_q(const float* win, int ww, int row0, const
     int cb[Q];
 #pragma unroll
     for (int q = 0; q < Q; ++q) cb[q] = valid[q] ? col0[q] : 0;
+#pragma unroll 1
     for (int dy = 0; dy < PW; ++dy) {
         const float* row = win + (size_t)(row0 + dy) * ww;
 #pragma unroll
@@ -250,20 +251,6 @@ __device__ __forceinline__ void zncc_q(const float* win, int ww, int row0, const
     }
 }
 
-// zncc_q with the chain count nq (1..4, uniform across the warp) chosen at run time
-template <int HALF, bool FLT>
-__device__ __forceinline__ void zncc_n(int nq, const float* win, int ww, int row0, const int col0[4],
-                                       const bool valid[4], const double* T, double ts, double out[4])
-{
-    out[0] = out[1] = out[2] = out[3] = -2.0;
-    switch (nq) {
-        case 1: zncc_q<HALF, FLT, 1>(win, ww, row0, col0, valid, T, ts, out); break;
-        case 2: zncc_q<HALF, FLT, 2>(win, ww, row0, col0, valid, T, ts, out); break;
-        case 3: zncc_q<HALF, FLT, 3>(win, ww, row0, col0, valid, T, ts, out); break;
-        default: zncc_q<HALF, FLT, 4>(win, ww, row0, col0, valid, T, ts, out); break;
-    }
-}
-
 // warp argmax, first maximum in increasing index (strict '>' scan): ties keep the smaller index
 __device__ __forceinline__ void warp_argmax(double& v, int& idx)
 {
@@ -277,7 +264,7 @@ __device__ __forceinline__ void warp_argmax(double& v, int& idx)
 
 // ---------------------------------------------------------------- the stereo kernel
 template <int HALF, bool FLT>
-__global__ void __launch_bounds__(ST_WARPS * 32) k_stereo(
+__global__ void __launch_bounds__(ST_WARPS * 32, 5) k_stereo(
     const u8* __restrict__ Lall, const u8* __restrict__ R8all, const float* __restrict__ Rsall, int H, int W,
     const double* __restrict__ kpd, const long long* __restrict__ dlo_a, const long long* __restrict__ dhi_a, int n,
     const float* __restrict__ kpf, const int* __restrict__ counts, int cap, int dlo_s, int dhi_s, int band,
@@ -367,16 +354,15 @@ __global__ void __launch_bounds__(ST_WARPS * 32) k_stereo(
         }
         double best[4];
         int bj[4] = {0, 0, 0, 0};
-        const int nq = (int)(hi - lo) / 32 + 1;
-        zncc_n<HALF, FLT>(nq, win, ww, band, col, val, Td, ts, best);
-        for (int j = 1; j <= band; ++j) {
+        // rows in the CPU's order: vi, then vi - j, vi + j for j = 1..band; a later row wins only if strictly better
+#pragma unroll 1
+        for (int t = 0; t <= 2 * band; ++t) {
+            const int j = t == 0 ? 0 : ((t & 1) ? -((t + 1) >> 1) : (t >> 1));
             double z[4];
-            zncc_n<HALF, FLT>(nq, win, ww, band - j, col, val, Td, ts, z);
+            zncc_q<HALF, FLT, 4>(win, ww, band + j, col, val, Td, ts, z);
 #pragma unroll
-            for (int q = 0; q < 4; ++q) if (z[q] > best[q]) { best[q] = z[q]; bj[q] = -j; }
-            zncc_n<HALF, FLT>(nq, win, ww, band + j, col, val, Td, ts, z);
-#pragma unroll
-            for (int q = 0; q < 4; ++q) if (z[q] > best[q]) { best[q] = z[q]; bj[q] = j; }
+            for (int q = 0; q < 4; ++q)
+                if (t == 0 || z[q] > best[q]) { best[q] = z[q]; bj[q] = j; }
         }
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
@@ -450,7 +436,7 @@ __global__ void __launch_bounds__(ST_WARPS * 32) k_stereo(
 #pragma unroll
         for (int q = 0; q < 4; ++q) { col[q] = lane + 32 * q; val[q] = col[q] <= dmax; }
         double z[4];
-        zncc_n<HALF, false>(dmax / 32 + 1, win, ww, 0, col, val, T2d, rsd, z);
+        zncc_q<HALF, false, 4>(win, ww, 0, col, val, T2d, rsd, z);
 #pragma unroll
         for (int q = 0; q < 4; ++q)
             if (val[q] && z[q] > lrb) { lrb = z[q]; lrd = col[q]; }
