@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--batch", type=int, default=100)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-ba", action="store_true")
     return ap.parse_args()
 
 
@@ -160,6 +161,19 @@ def run_reference(args, ws, rank):
             "cpu_baseline": {"value": fps, "unit": "frames/s", "cores": cores, "kind": "port",
                              "sample": "%d frames of the sequence per step, OpenMP over frames" % sample},
             "e2e": {"value": fps, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if not args.no_ba:
+        from oracle import ba_oracle as BO
+        from xclean_b200.backend import synth_ba as S
+        wins = S.config2_windows(BA_WINDOWS, seed=1)
+        sample = wins[:max(8, min(BA_WINDOWS, 4 * cores))]
+        BO.solve_batch([w.copy() for w in sample[:cores]], iters=BA_ITERS, lam0=BA_LAM0, hold=0, nthreads=cores)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            BO.solve_batch([w.copy() for w in sample], iters=BA_ITERS, lam0=BA_LAM0, hold=0, nthreads=cores)
+        dt = (time.perf_counter() - t0) / args.steps
+        line["ba"] = {"metric": "BA windows/s (plain per-window float64, the reference's window.solve restated)",
+                      "value": len(sample) / dt, "unit": "windows/s", "cores": cores,
+                      "sample": "%d of the 256 windows per step" % len(sample)}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -321,6 +335,8 @@ def run_ours(args, ws, rank, local):
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         cpu = cpu_baseline(L, R, args)
+    del L, R
+    ba = None if args.no_ba else run_ba(args, dev, stream, rank, ws, cpu=(rank == 0 and ws == 1 and not args.no_cpu))
     line = {"metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u8/f32/f64",
@@ -330,13 +346,96 @@ def run_ours(args, ws, rank, local):
                        "half": HALF, "l2": "inputs (467 MB/GPU) larger than L2, no flush"},
             "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
             "gpu_launches": launches_per_step * args.steps,
-            "kp_per_frame_last_batch": float(np.mean(counts)) if len(counts) else None}
+            "kp_per_frame_last_batch": float(np.mean(counts)) if len(counts) else None, "ba": ba}
     if rank == 0:
         print(json.dumps(line), flush=True)
     gf.close()
     if ws > 1:
         dist.destroy_process_group()
     return 0
+
+
+BA_WINDOWS = 256
+BA_ITERS = 5
+BA_LAM0 = 1e-4
+
+
+def run_ba(args, dev, stream, rank, ws_world, cpu=True):
+    """Batched mixed-precision window BA (256 uneven windows: K ~ U{5..20}, L ~ U{300..3000}, 2-12 observing
+    keyframes per landmark, 1 px noise, 5 % outliers, 5 LM iterations) vs the plain per-window FP64 form, with the
+    first pose step's error against the FP64 oracle."""
+    import torch
+    from oracle import ba_oracle as BO
+    from xclean_b200.backend import synth_ba as S
+    from xclean_b200.backend.ba import BatchSolver
+    wins = S.config2_windows(BA_WINDOWS, seed=1 + rank)
+    with torch.cuda.stream(stream):
+        bs = BatchSolver(wins, dev, hold=0)
+        singles = [BatchSolver([w], dev, hold=0) for w in wins]
+    torch.cuda.synchronize()
+
+    def timed(fn, steps):
+        for _ in range(max(1, args.warmup)):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    def step_batched(prec):
+        def f():
+            bs.reset()
+            bs.solve(BA_ITERS, BA_LAM0, prec, stream=stream)
+        return f
+
+    def step_single():
+        for s in singles:
+            s.reset()
+            s.solve(BA_ITERS, BA_LAM0, "fp64", stream=stream, grid=1)
+
+    with torch.cuda.stream(stream):
+        ms_mixed = timed(step_batched("mixed"), args.steps)
+        res_mixed = bs.results()
+        ms_fp64b = timed(step_batched("fp64"), args.steps)
+        res_fp64 = bs.results()
+        ms_single = timed(step_single, 1)
+    # error of the first pose step against the FP64 oracle (the reference's window.solve restated), all windows
+    errs_m, errs_f = [], []
+    for i, w in enumerate(wins):
+        dx_o, _c, ok = BO.step(w.copy(), BA_LAM0, hold=0)
+        n = 6 * w.Rwb.shape[0]
+        den = max(np.linalg.norm(dx_o), 1e-300)
+        errs_m.append(np.linalg.norm(res_mixed["dx0"][i][:n] - dx_o) / den)
+        errs_f.append(np.linalg.norm(res_fp64["dx0"][i][:n] - dx_o) / den)
+    n_land = int(sum(w.lmp.shape[0] for w in wins))
+    n_rows = int(sum(w.ob_pose.shape[0] for w in wins))
+    out = {"metric": "BA windows/s (batched mixed precision)", "unit": "windows/s",
+           "value": ws_world * BA_WINDOWS / (ms_mixed / 1e3),
+           "fp64_batched_value": ws_world * BA_WINDOWS / (ms_fp64b / 1e3),
+           "fp64_per_window_value": ws_world * BA_WINDOWS / (ms_single / 1e3),
+           "speedup_vs_fp64_per_window": ms_single / ms_mixed,
+           "ms_per_step": {"mixed_batched": ms_mixed, "fp64_batched": ms_fp64b, "fp64_per_window": ms_single},
+           "pose_step_rel_err_vs_fp64_oracle": {"mixed_max": float(np.max(errs_m)),
+                                                "mixed_median": float(np.median(errs_m)),
+                                                "fp64_max": float(np.max(errs_f))},
+           "accepted_mean": float(np.mean(res_mixed["accepted"])),
+           "config": {"workload": "256 uneven windows, K~U{5..20}, L~U{300..3000}, 2-12 obs/landmark (geometric), "
+                                  "stereo rows, 5% outliers, 5 LM iterations, keyframe 0 held",
+                      "landmarks": n_land, "observation_rows": n_rows}}
+    if cpu:
+        cores = os.cpu_count() or 1
+        sample = [w.copy() for w in wins[:max(8, min(BA_WINDOWS, 4 * cores))]]
+        BO.solve_batch([w.copy() for w in sample[:cores]], iters=BA_ITERS, lam0=BA_LAM0, hold=0, nthreads=cores)
+        t0 = time.perf_counter()
+        BO.solve_batch(sample, iters=BA_ITERS, lam0=BA_LAM0, hold=0, nthreads=cores)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": len(sample) / dt, "unit": "windows/s", "cores": cores, "kind": "port",
+                               "sample": "%d of the windows, float64 window.solve, OpenMP over windows" % len(sample)}
+    return out
 
 
 def cpu_baseline(L, R, args):

@@ -86,56 +86,54 @@ def make_window(seed, K=10, L=1500, obs_min=2, obs_max=6, z0=2.0, z1=20.0, step_
     vs = rng.uniform(0.05 * H, 0.95 * H, L)
     Pc0 = np.stack([(us - cx) / fx * zs, (vs - cy) / fy * zs, zs], 1)
     Pw = Pc0 @ Rwb_t[0].T + pwb_t[0]
-    lm_host, lmp_true, lmp0, obs = [], [], [], []
-    for l in range(L):
-        vis = []
-        for k in range(K):
-            Pc = Rwb_t[k].T @ (Pw[l] - pwb_t[k])
-            if Pc[2] < 0.5:
-                continue
-            ul = fx * Pc[0] / Pc[2] + cx
-            vl = fy * Pc[1] / Pc[2] + cy
-            ur = fx * (Pc[0] - B) / Pc[2] + cx
-            if 0 <= ul < W and 0 <= vl < H and 0 <= ur < W:
-                vis.append((k, ul, vl, ur))
-        if len(vis) < obs_min:
-            continue
-        if geometric:
-            n = int(min(obs_max, obs_min + rng.geometric(0.35) - 1))
-        else:
-            n = int(rng.integers(obs_min, obs_max + 1))
-        n = min(n, len(vis))
-        pick = sorted(rng.choice(len(vis), n, replace=False))
-        sel = [vis[i] for i in pick]
-        h = sel[0][0]
-        Ph = Rwb_t[h].T @ (Pw[l] - pwb_t[h])
-        a_t, b_t, rho_t = Ph[0] / Ph[2], Ph[1] / Ph[2], 1.0 / Ph[2]
-        rows = []
-        for (k, ul, vl, ur) in sel:
-            zl = np.array([ul, vl]) + rng.normal(0.0, px_noise, 2)
-            zr = ur + rng.normal(0.0, px_noise)
-            if rng.random() < outlier_frac:
-                zl = np.array([rng.uniform(0, W), rng.uniform(0, H)])
-            if rng.random() < outlier_frac:
-                zr = rng.uniform(0, W)
-            rows.append((k, 0, zl[0], zl[1]))
-            rows.append((k, 1, zr, 0.0))
-        # initial landmark: the host's noisy left ray, depth off by depth_frac
-        zl_h = rows[0][2:4]
-        a0 = (zl_h[0] - cx) / fx
-        b0 = (zl_h[1] - cy) / fy
-        rho0 = rho_t / (1.0 + rng.normal(0.0, depth_frac))
-        lm_host.append(h)
-        lmp_true.append((a_t, b_t, rho_t))
-        lmp0.append((a0, b0, rho0))
-        obs.append(rows)
-    Lk = len(lm_host)
+    # every (keyframe, landmark) projection at once
+    Pc = np.einsum("kji,klj->kli", Rwb_t, Pw[None, :, :] - pwb_t[:, None, :])        # (K, L, 3)
+    z = Pc[:, :, 2]
+    with np.errstate(divide="ignore", invalid="ignore"):
+        ul = fx * Pc[:, :, 0] / z + cx
+        vl = fy * Pc[:, :, 1] / z + cy
+        ur = fx * (Pc[:, :, 0] - B) / z + cx
+    vis = (z >= 0.5) & (ul >= 0) & (ul < W) & (vl >= 0) & (vl < H) & (ur >= 0) & (ur < W)
+    nvis = vis.sum(0)
+    if geometric:
+        n = np.minimum(obs_max, obs_min + rng.geometric(0.35, L) - 1)
+    else:
+        n = rng.integers(obs_min, obs_max + 1, L)
+    n = np.minimum(n, nvis)
+    keep = nvis >= obs_min
+    keys = rng.random((K, L))
+    keys[~vis] = np.inf
+    rank = np.argsort(np.argsort(keys, axis=0), axis=0)                                  # rank of each keyframe
+    sel = (rank < n[None, :]) & vis & keep[None, :]                                       # (K, L)
+    lidx = np.nonzero(keep)[0]
+    Lk = len(lidx)
+    selT = sel[:, lidx].T                                                                 # (Lk, K), keyframe order
+    cnt = selT.sum(1)
     ob_start = np.zeros(Lk + 1, np.int64)
-    ob_start[1:] = np.cumsum([len(r) for r in obs])
-    flat = [r for rows in obs for r in rows]
-    ob_pose = np.array([r[0] for r in flat], np.int64)
-    ob_cam = np.array([r[1] for r in flat], np.int64)
-    ob_z = np.array([[r[2], r[3]] for r in flat], np.float64)
+    ob_start[1:] = np.cumsum(2 * cnt)
+    li, ki = np.nonzero(selT)                                                             # landmark-major, k ascending
+    lg = lidx[li]
+    nr = len(li)
+    zl = np.stack([ul[ki, lg], vl[ki, lg]], 1) + rng.normal(0.0, px_noise, (nr, 2))
+    zr = ur[ki, lg] + rng.normal(0.0, px_noise, nr)
+    ol = rng.random(nr) < outlier_frac
+    zl[ol] = np.stack([rng.uniform(0, W, int(ol.sum())), rng.uniform(0, H, int(ol.sum()))], 1)
+    orr = rng.random(nr) < outlier_frac
+    zr[orr] = rng.uniform(0, W, int(orr.sum()))
+    ob_pose = np.repeat(ki, 2).astype(np.int64)
+    ob_cam = np.tile(np.array([0, 1], np.int64), nr)
+    ob_z = np.zeros((2 * nr, 2))
+    ob_z[0::2] = zl
+    ob_z[1::2, 0] = zr
+    first = ob_start[:-1] // 2                                                            # each landmark's first row
+    host = ki[first] if Lk else np.zeros(0, np.int64)
+    Ph = np.einsum("lji,lj->li", Rwb_t[host], Pw[lidx] - pwb_t[host])
+    lmp_true = np.stack([Ph[:, 0] / Ph[:, 2], Ph[:, 1] / Ph[:, 2], 1.0 / Ph[:, 2]], 1) if Lk else np.zeros((0, 3))
+    zh = zl[first] if Lk else np.zeros((0, 2))
+    rho0 = lmp_true[:, 2] / (1.0 + rng.normal(0.0, depth_frac, Lk))
+    lmp0 = np.stack([(zh[:, 0] - cx) / fx, (zh[:, 1] - cy) / fy, rho0], 1) if Lk else np.zeros((0, 3))
+    lm_host = host.astype(np.int64)
+    flat_n = 2 * nr
     # initial poses: keyframe 0 at the truth (held), the others perturbed
     Rwb0 = Rwb_t.copy()
     pwb0 = pwb_t.copy()
@@ -146,13 +144,12 @@ def make_window(seed, K=10, L=1500, obs_min=2, obs_max=6, z0=2.0, z1=20.0, step_
         d = rng.normal(0.0, 1.0, 3)
         pwb0[k] = pwb_t[k] + pose_m * d / np.linalg.norm(d)
     return Window(Rwb=np.ascontiguousarray(Rwb0), pwb=np.ascontiguousarray(pwb0), Rbc=Rbc, pbc=pbc,
-                  lmp=np.ascontiguousarray(np.array(lmp0, np.float64).reshape(-1, 3)),
-                  lm_host=np.array(lm_host, np.int64), lm_mask=np.ones(Lk, np.bool_), rho_meas=np.zeros(Lk),
-                  rho_isig=np.zeros(Lk), ob_start=ob_start, ob_pose=ob_pose, ob_cam=ob_cam,
-                  ob_z=np.ascontiguousarray(ob_z.reshape(-1, 2)), ob_isig=np.full(len(flat), 1.0 / px_noise),
-                  ob_valid=np.ones(len(flat), np.bool_), fx=float(fx), fy=float(fy), cx=float(cx), cy=float(cy),
+                  lmp=np.ascontiguousarray(lmp0.reshape(-1, 3)), lm_host=lm_host, lm_mask=np.ones(Lk, np.bool_),
+                  rho_meas=np.zeros(Lk), rho_isig=np.zeros(Lk), ob_start=ob_start, ob_pose=ob_pose, ob_cam=ob_cam,
+                  ob_z=np.ascontiguousarray(ob_z), ob_isig=np.full(flat_n, 1.0 / px_noise),
+                  ob_valid=np.ones(flat_n, np.bool_), fx=float(fx), fy=float(fy), cx=float(cx), cy=float(cy),
                   B=float(B), huber_k=HUBER_K, Rwb_true=Rwb_t, pwb_true=pwb_t,
-                  lmp_true=np.array(lmp_true, np.float64).reshape(-1, 3))
+                  lmp_true=np.ascontiguousarray(lmp_true.reshape(-1, 3)))
 
 
 def config0_window(seed=0):
