@@ -163,6 +163,20 @@ size_t xcb_ba_scratch_bytes(int nw, int Lt);
 int xcb_ba_solve_windows_dev(const xcb_ba_windows* w, int max_slots, int iters, double lam0, int mode, double* stats,
                              double* dx0, int dx0_stride, void* scratch, size_t scratch_bytes, int grid, void* stream);
 
+/* Allocation-free form of xcb_ba_solve_windows_dev.  No counterpart in the reference.  It is for callers that cannot
+   call cudaMalloc while running: a real-time loop whose latency budget rules out an allocation (which may synchronise
+   the device), or a plugin whose host owns the device memory through its own allocator.  The caller passes inputs and
+   outputs as for xcb_ba_solve_windows_dev but no scratch: the scratch is a static device array of
+   XCB_BA_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until exit, which limits one call to
+   xcb_ba_noalloc_max_landmarks() landmarks in total (`Lt`, the batch's landmark count; more -> XCB_ERR_CAPACITY).
+   The first call on a device looks up the array's device address (call it before any stream capture).  Calls share
+   the array: calls that overlap on the GPU race.  No cudaMalloc, cudaFree or allocating library call is made. */
+#define XCB_BA_NOALLOC_SCRATCH_BYTES ((size_t)4 << 20)
+#define XCB_NOALLOC_MAX_DEVICES 64
+int xcb_ba_noalloc_max_landmarks(void);
+int xcb_ba_solve_windows_noalloc(const xcb_ba_windows* w, int Lt, int max_slots, int iters, double lam0, int mode,
+                                 double* stats, double* dx0, int dx0_stride, int grid, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

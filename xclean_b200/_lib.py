@@ -73,6 +73,9 @@ _SIGS.update({
     "xcb_ba_scratch_bytes": (c_size_t, [c_int, c_int]),
     "xcb_ba_solve_windows_dev": (c_int, [ctypes.POINTER(BaWindows), c_int, c_int, c_double, c_int, P, P, c_int, P,
                                          c_size_t, c_int, P]),
+    "xcb_ba_noalloc_max_landmarks": (c_int, []),
+    "xcb_ba_solve_windows_noalloc": (c_int, [ctypes.POINTER(BaWindows), c_int, c_int, c_int, c_double, c_int, P, P,
+                                             c_int, c_int, P]),
 })
 
 

@@ -1,4 +1,5 @@
 // ba_api.cu -- C ABI of the bundle-adjustment kernels (include/xcb200.h).
+#include <mutex>
 #include <string>
 
 #include "ba_kernels.h"
@@ -47,4 +48,61 @@ static int ba_fail(int code, const char* msg)
 {
     xcb_set_last_error(std::string(msg));
     return code;
+}
+
+// ------------------------------------------------------------------------------------------------------------------
+// Allocation-free batched window solve.
+//
+// Some callers cannot call cudaMalloc once they are running: a real-time frame loop, whose latency budget does not
+// allow an allocation that may synchronise the device and take unbounded time, and a plugin whose host application
+// owns the device memory budget through its own allocator.  xcb_ba_solve_windows_dev needs a scratch buffer from the
+// caller; this variant needs none.  Its scratch (the work counter and the trial landmark states) lives in the
+// file-scope device array below, XCB_BA_NOALLOC_SCRATCH_BYTES (4 MiB) that every GPU which loads libxcb200.so holds
+// until the process exits.  That bounds one call to xcb_ba_noalloc_max_landmarks() landmarks in total.
+//
+// In host code g_ba_noalloc_scratch is only a host-side stand-in for the device array, not a device address: its
+// device address is looked up once per device (cudaGetSymbolAddress, with that device current) by the first call on
+// that device, so that first call should come before any stream capture.  All calls share the one array and it keeps
+// the last call's contents: the work counter is cleared at the start of every call (the trial states are written
+// before they are read), and calls that overlap on the GPU (two streams, or two threads) race on it.
+// ------------------------------------------------------------------------------------------------------------------
+static __device__ __align__(256) unsigned char g_ba_noalloc_scratch[XCB_BA_NOALLOC_SCRATCH_BYTES];
+
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_addr[XCB_NOALLOC_MAX_DEVICES];
+
+extern "C" int xcb_ba_noalloc_max_landmarks(void)
+{
+    return (int)((XCB_BA_NOALLOC_SCRATCH_BYTES - 256) / (3 * sizeof(double)));
+}
+
+extern "C" int xcb_ba_solve_windows_noalloc(const xcb_ba_windows* w, int Lt, int max_slots, int iters, double lam0,
+                                            int mode, double* stats, double* dx0, int dx0_stride, int grid,
+                                            void* stream)
+{
+    if (!w || !stats) return ba_fail(XCB_ERR_ARG, "ba_solve_windows_noalloc: null argument");
+    if (Lt < 0) return ba_fail(XCB_ERR_ARG, "ba_solve_windows_noalloc: negative landmark count");
+    if (Lt > xcb_ba_noalloc_max_landmarks())
+        return ba_fail(XCB_ERR_CAPACITY, ("ba_solve_windows_noalloc: " + std::to_string(Lt) + " landmarks exceed the "
+                                          "static scratch (at most " + std::to_string(xcb_ba_noalloc_max_landmarks()) +
+                                          " per call); split the batch or use xcb_ba_solve_windows_dev").c_str());
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return ba_fail(XCB_ERR_CUDA, cudaGetErrorString(e));
+    if (dev < 0 || dev >= XCB_NOALLOC_MAX_DEVICES) return ba_fail(XCB_ERR_ARG, "ba_solve_windows_noalloc: device ordinal");
+    void* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_addr[dev]) {
+            void* p = nullptr;
+            e = cudaGetSymbolAddress(&p, g_ba_noalloc_scratch);
+            if (e != cudaSuccess || !p)
+                return ba_fail(XCB_ERR_CUDA, (std::string("ba_solve_windows_noalloc: cudaGetSymbolAddress: ") +
+                                              cudaGetErrorString(e)).c_str());
+            g_noalloc_addr[dev] = p;
+        }
+        base = g_noalloc_addr[dev];
+    }
+    return xcb_ba_solve_windows_dev(w, max_slots, iters, lam0, mode, stats, dx0, dx0_stride, base,
+                                    XCB_BA_NOALLOC_SCRATCH_BYTES, grid, stream);
 }
