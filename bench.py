@@ -51,6 +51,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ba", action="store_true")
+    ap.add_argument("--ba-only", action="store_true",
+                    help="run only the batched window BA part and print its JSON object (profiling)")
+    ap.add_argument("--ba-windows", type=int, default=None, help="BA windows per step (default 256)")
     return ap.parse_args()
 
 
@@ -216,6 +219,15 @@ def run_ours(args, ws, rank, local):
     dev = torch.device("cuda", local)
     if ws > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    if args.ba_only:
+        stream = torch.cuda.Stream(device=dev)
+        torch.cuda.set_stream(stream)
+        ba = run_ba(args, dev, stream, rank, ws, cpu=(rank == 0 and ws == 1 and not args.no_cpu))
+        if rank == 0:
+            print(json.dumps(ba), flush=True)
+        if ws > 1:
+            dist.destroy_process_group()
+        return 0
     F, Bt = args.frames, args.batch
     nb = (F + Bt - 1) // Bt
     L, R = synth.sequence(synth.CAM_KITTI, F, seed=rank, device=dev)
@@ -368,7 +380,8 @@ def run_ba(args, dev, stream, rank, ws_world, cpu=True):
     from oracle import ba_oracle as BO
     from xclean_b200.backend import synth_ba as S
     from xclean_b200.backend.ba import BatchSolver
-    wins = S.config2_windows(BA_WINDOWS, seed=1 + rank)
+    nwin = args.ba_windows or BA_WINDOWS
+    wins = S.config2_windows(BA_WINDOWS, seed=1 + rank)[:nwin]
     with torch.cuda.stream(stream):
         bs = BatchSolver(wins, dev, hold=0)
         singles = [BatchSolver([w], dev, hold=0) for w in wins]
@@ -414,9 +427,9 @@ def run_ba(args, dev, stream, rank, ws_world, cpu=True):
     n_land = int(sum(w.lmp.shape[0] for w in wins))
     n_rows = int(sum(w.ob_pose.shape[0] for w in wins))
     out = {"metric": "BA windows/s (batched mixed precision)", "unit": "windows/s",
-           "value": ws_world * BA_WINDOWS / (ms_mixed / 1e3),
-           "fp64_batched_value": ws_world * BA_WINDOWS / (ms_fp64b / 1e3),
-           "fp64_per_window_value": ws_world * BA_WINDOWS / (ms_single / 1e3),
+           "value": ws_world * nwin / (ms_mixed / 1e3),
+           "fp64_batched_value": ws_world * nwin / (ms_fp64b / 1e3),
+           "fp64_per_window_value": ws_world * nwin / (ms_single / 1e3),
            "speedup_vs_fp64_per_window": ms_single / ms_mixed,
            "ms_per_step": {"mixed_batched": ms_mixed, "fp64_batched": ms_fp64b, "fp64_per_window": ms_single},
            "pose_step_rel_err_vs_fp64_oracle": {"mixed_max": float(np.max(errs_m)),
@@ -428,7 +441,7 @@ def run_ba(args, dev, stream, rank, ws_world, cpu=True):
                       "landmarks": n_land, "observation_rows": n_rows}}
     if cpu:
         cores = os.cpu_count() or 1
-        sample = [w.copy() for w in wins[:max(8, min(BA_WINDOWS, 4 * cores))]]
+        sample = [w.copy() for w in wins[:max(8, min(nwin, 4 * cores))]]
         BO.solve_batch([w.copy() for w in sample[:cores]], iters=BA_ITERS, lam0=BA_LAM0, hold=0, nthreads=cores)
         t0 = time.perf_counter()
         BO.solve_batch(sample, iters=BA_ITERS, lam0=BA_LAM0, hold=0, nthreads=cores)

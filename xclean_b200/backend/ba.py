@@ -21,6 +21,7 @@ from .. import _lib
 PRECISIONS = {"fp64": _lib.XCB_BA_FP64, "mixed": _lib.XCB_BA_MIXED}
 MAX_SLOTS = 20
 MAX_ROWS_PER_LANDMARK = 32
+MAX_TOUCHED_SLOTS = 16      # host + observing keyframes per landmark (the kernel's per-warp scratch)
 
 
 def pack_windows(windows, hold=0):
@@ -44,6 +45,18 @@ def pack_windows(windows, hold=0):
     if len(rows) and rows.max() > MAX_ROWS_PER_LANDMARK:
         raise ValueError("solve_batch: a landmark has %d observation rows (at most %d)" % (rows.max(),
                                                                                        MAX_ROWS_PER_LANDMARK))
+    for i, w in enumerate(windows):
+        host, pose = np.asarray(w.lm_host, np.int64), np.asarray(w.ob_pose, np.int64)
+        if (host < 0).any() or (host >= P[i]).any() or (pose < 0).any() or (pose >= P[i]).any():
+            raise ValueError("solve_batch: window %d has a host or observing slot outside 0..%d" % (i, P[i] - 1))
+        if len(pose):
+            # distinct slots a landmark touches: its observing keyframes and its host
+            lm_of = np.repeat(np.arange(len(host)), np.diff(np.asarray(w.ob_start, np.int64)))
+            keys = np.unique(np.concatenate([lm_of * MAX_SLOTS + pose, np.arange(len(host)) * MAX_SLOTS + host]))
+            touched = np.bincount(keys // MAX_SLOTS, minlength=len(host))
+            if touched.max() > MAX_TOUCHED_SLOTS:
+                raise ValueError("solve_batch: a landmark of window %d touches %d keyframes (at most %d)"
+                                 % (i, touched.max(), MAX_TOUCHED_SLOTS))
     cat = lambda name, dt: np.ascontiguousarray(np.concatenate([np.asarray(getattr(w, name)).reshape(
         len(getattr(w, name)), -1) for w in windows]).astype(dt)) if nw else np.zeros(0, dt)
     hold_a = np.full(nw, -1 if hold is None else int(hold), np.int32)
