@@ -152,13 +152,14 @@ typedef struct {
 } xcb_ba_windows;
 
 #define XCB_BA_FP64 0           /* everything in float64: the plain form */
-#define XCB_BA_MIXED 1          /* FP32 linearisation + Schur, FP64 Cholesky, one FP64 refinement step */
+#define XCB_BA_MIXED 1          /* FP32 linearisation + Schur, FP64 Cholesky, FP64 refinement (to 1e-9, <= 3 steps) */
 
 /* Device scratch the batched solve needs for `Lt` landmarks (trial landmark states and the work counter). */
 size_t xcb_ba_scratch_bytes(int nw, int Lt);
 /* window.solve (window.py:889-982, purely visual, fixed `iters` LM iterations from lam0) for every window of the batch
    in ONE persistent launch (no reference counterpart as one call; the reference solves one window per call on the
-   CPU).  stats [nw][8] = cost0, cost, accepted, lam, status (0 ok, -1 window too large), iters, -, -;
+   CPU).  stats [nw][8] = cost0, cost, accepted, lam, status (0 ok, -1 window too large, -2 a landmark touches more
+   than 16 keyframes), iters, -, -;
    dx0 [nw][dx0_stride] (optional) = the first iteration's pose step.  grid = 0: one CTA per SM. */
 int xcb_ba_solve_windows_dev(const xcb_ba_windows* w, int max_slots, int iters, double lam0, int mode, double* stats,
                              double* dx0, int dx0_stride, void* scratch, size_t scratch_bytes, int grid, void* stream);
@@ -176,6 +177,105 @@ int xcb_ba_solve_windows_dev(const xcb_ba_windows* w, int max_slots, int iters, 
 int xcb_ba_noalloc_max_landmarks(void);
 int xcb_ba_solve_windows_noalloc(const xcb_ba_windows* w, int Lt, int max_slots, int iters, double lam0, int mode,
                                  double* stats, double* dx0, int dx0_stride, int grid, void* stream);
+
+/* ----------------------------------------------------------------------------------------------------------------
+   Local-BA stage kernels: one entry point per kernel of src/xclean/backend/kernels.py, same argument order and
+   meaning, device pointers (float32 / int32, the reference's layouts), enqueued on `stream` (NULL = the legacy default
+   stream).  Sums into Hll, bl, Hred and g are accumulated (the caller zeroes them), in an unspecified order.
+   -> XCB_OK or XCB_ERR_ARG / XCB_ERR_CUDA (message in xcb_last_error()).
+   ---------------------------------------------------------------------------------------------------------------- */
+/* kernels.py:45-114 build_blocks: Euclidean points, T_cw (nk,12) row-major 3x4; Jpose (N,2,6), Jlm (N,2,3),
+   resw (N,2), Hll (nl,9) +=, bl (nl,3) +=, Hpl (N,6,3) */
+int xcb_bk_build_blocks(const float* Tcw, const float* pts, const int* okf, const int* olm, const float* ouv,
+                        float* Jpose, float* Jlm, float* resw, float* Hll, float* bl, float* Hpl, int N, float fx,
+                        float cx, float cy, float huber, void* stream);
+/* kernels.py:135-166 depth_prior: inverse-range prior on Euclidean points */
+int xcb_bk_depth_prior(const float* pts, const float* chost, const float* rho0, const float* invsig,
+                       const float* valid, float* Hll, float* bl, int nl, float huber, void* stream);
+/* kernels.py:169-191 inv3_damped: (Hll + lam max(tr/3, 1e-9) I)^-1 */
+int xcb_bk_inv3_damped(const float* Hll, float* Hlli, int nl, float lam, void* stream);
+/* kernels.py:203-232 schur_pairs: Hred[ki][kj] -= Hpl_i Hlli Hpl_j^T over the ordered pair list (pa, pb) */
+int xcb_bk_schur_pairs(const float* Hpl, const float* Hlli, const int* okf, const int* olm, const int* pa,
+                       const int* pb, float* Hred, long long npair, int d, int n, void* stream);
+/* kernels.py:235-258 schur_grad: g[k] -= Hpl Hlli bl */
+int xcb_bk_schur_grad(const float* Hpl, const float* Hlli, const float* bl, const int* okf, const int* olm, float* g,
+                      int N, int d, void* stream);
+/* kernels.py:261-285 pose_blocks: Hred[k][k] += J^T J, g[k] -= J^T res (kf < 0: skipped); J (N,r,d) */
+int xcb_bk_pose_blocks(const float* Jp, const float* res, const int* kf, float* Hred, float* g, int N, int r, int d,
+                       int n, void* stream);
+/* kernels.py:291-346 chol_solve: H (n,n) overwritten by its lower Cholesky factor, x = H^-1 b, one CTA of `nthreads`;
+   status (int32 on the device) is cleared, then set to k+1 for a non-positive pivot k (the pivot is then 1e-8) */
+int xcb_bk_chol_solve(float* H, const float* b, float* x, int n, int* status, int nthreads, void* stream);
+/* kernels.py:349-374 backsub: dxl = Hlli (bl - sum_obs Hpl^T dxp[okf]), observations sorted by landmark (offs) */
+int xcb_bk_backsub(const float* Hpl, const float* Hlli, const float* bl, const float* dxp, const int* okf,
+                   const int* offs, float* dxl, int nl, int d, void* stream);
+/* kernels.py:417-580 build_blocks_id: host-anchored (x_n, y_n, rho) landmarks; in-window host slot hidx >= 0 (its
+   pose inverted from Tcw), else hpose (nl,12) T_wc; Jp (N,2,2,6) [observer, host], resw (N,2), kslot (N,2),
+   Hll (nl,9) +=, bl (nl,3) +=, Hpl (N,2,6,3) */
+int xcb_bk_build_blocks_id(const float* Tcw, const float* hpose, const int* hidx, const float* mbear, const float* rhov,
+                           const int* okf, const int* olm, const float* ouv, float* Jp, float* resw, int* kslot,
+                           float* Hll, float* bl, float* Hpl, int N, float fx, float cx, float cy, float huber,
+                           void* stream);
+/* kernels.py:599-643 landmark_prior_id: bearing (not robustified) and inverse-depth (Huber) priors */
+int xcb_bk_landmark_prior_id(const float* mb, const float* rhov, const float* m0, const float* rho0,
+                             const float* invsig, const float* wbear, const float* valid, float* Hll, float* bl,
+                             int nl, float huber, void* stream);
+/* kernels.py:646-680 pose_blocks_id: both slot pairs of every observation */
+int xcb_bk_pose_blocks_id(const float* Jp, const float* res, const int* kslot, float* Hred, float* g, int N, int d,
+                          int n, void* stream);
+/* kernels.py:683-717 schur_pairs_id */
+int xcb_bk_schur_pairs_id(const float* Hpl, const float* Hlli, const int* kslot, const int* olm, const int* pa,
+                          const int* pb, float* Hred, long long npair, int d, int n, void* stream);
+/* kernels.py:720-745 schur_grad_id */
+int xcb_bk_schur_grad_id(const float* Hpl, const float* Hlli, const float* bl, const int* kslot, const int* olm,
+                         float* g, int N, int d, void* stream);
+/* kernels.py:748-775 backsub_id */
+int xcb_bk_backsub_id(const float* Hpl, const float* Hlli, const float* bl, const float* dxp, const int* kslot,
+                      const int* offs, float* dxl, int nl, int d, void* stream);
+
+/* ----------------------------------------------------------------------------------------------------------------
+   Local BA solve on the device: the LM loop of src/xclean/backend/ba.py _solve_gpu (ba.py:930-1089, Euclidean
+   points) and _solve_gpu_id (ba.py:1345-1497, host-anchored inverse depth), every iteration enqueued on `stream` with
+   the LM decisions (reject -> restore the best state and lam x 4, non-finite step -> lam x 10, accept -> lam / 2) taken
+   by device kernels: no host round trip until the end.  Jacobians and landmark blocks are float32 (the reference's
+   stage kernels above), the reduced system, its Cholesky, the landmark back-substitution and the state are float64.
+   Observations must be sorted by landmark (offs = CSR starts, nl + 1).  All pointers are device pointers.
+   ---------------------------------------------------------------------------------------------------------------- */
+#define XCB_LBA_EUCLID 0
+#define XCB_LBA_INVDEPTH 1
+#define XCB_LBA_MAX_SLOTS 64        /* keyframes per problem */
+#define XCB_LBA_MAX_TOUCHED 32      /* distinct keyframes one landmark touches (observers + in-window host) */
+typedef struct {
+    int model;                      /* XCB_LBA_EUCLID / XCB_LBA_INVDEPTH */
+    int nk, nl, N;                  /* keyframes, landmarks, observations */
+    double fx, cx, cy, huber, rho_floor;
+    double* Tcw;                    /* (nk,12) in/out: rows of T_cw's 3x4, float64 */
+    double* lm;                     /* (nl,3) in/out: Euclidean points, or bearings (x_n, y_n, 1) */
+    double* rho;                    /* (nl) in/out: inverse depths (XCB_LBA_INVDEPTH) */
+    const int* okf;                 /* (N) observing keyframe slot */
+    const int* olm;                 /* (N) landmark */
+    const float* ouv;               /* (N,2) pixels */
+    const int* offs;                /* (nl+1) observation range of each landmark */
+    const int* hidx;                /* (nl) in-window host slot or -1 (XCB_LBA_INVDEPTH) */
+    const float* hpose;             /* (nl,12) T_wc of out-of-window hosts (XCB_LBA_INVDEPTH) */
+    const unsigned char* free_mask; /* (nk) 1 = the keyframe is updated */
+    /* optional priors (NULL = none), float32:
+       Euclidean (kernels.py depth_prior): p0 = host centre (nl,3), p1 = rho0, p2 = invsig, p3 = valid;
+       inverse depth (kernels.py landmark_prior_id): p0 = m0 (nl,2), p1 = rho0, p2 = invsig, p3 = valid, p4 = wbear */
+    const float *p0, *p1, *p2, *p3, *p4;
+    /* optional gyro relative-rotation factors (ba.py _rot_factor_blocks): a, b slots, M (nrot,9), sigma */
+    int nrot;
+    const int* rot_a;
+    const int* rot_b;
+    const double* rot_M;
+    const double* rot_sig;
+} xcb_lba_problem;
+size_t xcb_lba_workspace_bytes(const xcb_lba_problem* p);
+/* stats (device, 10 doubles): chi2_0 (chi of the last accepted state), chi2_n, rms_0, rms_n, lam, accepted steps,
+   rejected steps, non-finite steps, landmarks that touched more than XCB_LBA_MAX_TOUCHED keyframes (their surplus
+   slots were left out; the Python driver rejects such problems first), - */
+int xcb_lba_solve(const xcb_lba_problem* p, int iters, double lam0, double* stats, void* workspace,
+                  size_t workspace_bytes, void* stream);
 
 #ifdef __cplusplus
 }

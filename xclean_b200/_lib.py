@@ -78,6 +78,45 @@ _SIGS.update({
                                              c_int, c_int, P]),
 })
 
+# local-BA stage kernels (src/xclean/backend/kernels.py): device pointers, float32 scalars, stream last
+c_ll = ctypes.c_longlong
+_SIGS.update({
+    "xcb_bk_build_blocks": (c_int, [P] * 11 + [c_int, c_float, c_float, c_float, c_float, P]),
+    "xcb_bk_depth_prior": (c_int, [P] * 7 + [c_int, c_float, P]),
+    "xcb_bk_inv3_damped": (c_int, [P, P, c_int, c_float, P]),
+    "xcb_bk_schur_pairs": (c_int, [P] * 7 + [c_ll, c_int, c_int, P]),
+    "xcb_bk_schur_grad": (c_int, [P] * 6 + [c_int, c_int, P]),
+    "xcb_bk_pose_blocks": (c_int, [P] * 5 + [c_int, c_int, c_int, c_int, P]),
+    "xcb_bk_chol_solve": (c_int, [P, P, P, c_int, P, c_int, P]),
+    "xcb_bk_backsub": (c_int, [P] * 7 + [c_int, c_int, P]),
+    "xcb_bk_build_blocks_id": (c_int, [P] * 14 + [c_int, c_float, c_float, c_float, c_float, P]),
+    "xcb_bk_landmark_prior_id": (c_int, [P] * 9 + [c_int, c_float, P]),
+    "xcb_bk_pose_blocks_id": (c_int, [P] * 5 + [c_int, c_int, c_int, P]),
+    "xcb_bk_schur_pairs_id": (c_int, [P] * 7 + [c_ll, c_int, c_int, P]),
+    "xcb_bk_schur_grad_id": (c_int, [P] * 6 + [c_int, c_int, P]),
+    "xcb_bk_backsub_id": (c_int, [P] * 7 + [c_int, c_int, P]),
+})
+
+XCB_LBA_EUCLID = 0
+XCB_LBA_INVDEPTH = 1
+XCB_LBA_MAX_SLOTS = 64
+XCB_LBA_MAX_TOUCHED = 32
+LBA_STATS = 10
+
+
+class LbaProblem(ctypes.Structure):
+    _fields_ = ([("model", c_int), ("nk", c_int), ("nl", c_int), ("N", c_int)]
+                + [(k, c_double) for k in ("fx", "cx", "cy", "huber", "rho_floor")]
+                + [(k, c_void_p) for k in ("Tcw", "lm", "rho", "okf", "olm", "ouv", "offs", "hidx", "hpose",
+                                           "free_mask", "p0", "p1", "p2", "p3", "p4")]
+                + [("nrot", c_int)] + [(k, c_void_p) for k in ("rot_a", "rot_b", "rot_M", "rot_sig")])
+
+
+_SIGS.update({
+    "xcb_lba_workspace_bytes": (c_size_t, [ctypes.POINTER(LbaProblem)]),
+    "xcb_lba_solve": (c_int, [ctypes.POINTER(LbaProblem), c_int, c_double, P, P, c_size_t, P]),
+})
+
 
 def declared_symbols():
     """Every entry point the header declares (the loader binds exactly these)."""

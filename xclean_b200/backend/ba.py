@@ -1,5 +1,6 @@
 """Bundle adjustment on the device: the batched sliding-window solve (the reference's window.solve model) and, in
-backend/ba_id.py, the drop-in _solve_gpu / _solve_gpu_id of src/xclean/backend/ba.py.
+backend/local_ba.py, the drop-in _solve_gpu / _solve_gpu_id of src/xclean/backend/ba.py (with backend/kernels.py,
+the drop-in of its stage kernels).
 
     res = solve_batch(windows, iters=5, lam0=1e-4, precision="mixed", hold=0)
     # windows: synth_ba.Window objects (the fields of vio/window.Problem); solved in place
