@@ -32,6 +32,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from xclean_b200 import dist as D  # noqa: E402
+
 W, H = 1241, 376
 FRAMES = 500
 BUDGET = 2000
@@ -57,11 +59,6 @@ def parse():
     return ap.parse_args()
 
 
-def dist_env():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
 
 
 # ------------------------------------------------------------------------------------------------ clocks sampler
@@ -273,10 +270,7 @@ def run_ours(args, ws, rank, local):
     clk = clocks.stop()
     ms = ev0.elapsed_time(ev1)
     gf.sync_check(sptr)
-    if ws > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = D.max_over_ranks(ms, device=dev)            # the slowest rank defines the step time
     value = ws * F * args.steps / (ms / 1e3)
     out = gf.device_buffers()
     # per-frame results for the report: keypoints, stereo acceptance, matches (last step)
@@ -313,10 +307,7 @@ def run_ours(args, ws, rank, local):
         e1.record(stream)
         torch.cuda.synchronize()
         ems = e0.elapsed_time(e1)
-        if ws > 1:
-            t = torch.tensor([ems], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
+        ems = D.max_over_ranks(ems, device=dev)
         d2h = sum(sum(a.nbytes for a in o.values()) for o in outs)
         e2e = {"value": ws * F * args.steps / (ems / 1e3), "unit": "frames/s", "h2d_bytes_per_step": 2 * F * W * H,
                "d2h_bytes_per_step": d2h}
@@ -416,6 +407,7 @@ def run_ba(args, dev, stream, rank, ws_world, cpu=True):
         ms_fp64b = timed(step_batched("fp64"), args.steps)
         res_fp64 = bs.results()
         ms_single = timed(step_single, 1)
+    ms_mixed, ms_fp64b, ms_single = (D.max_over_ranks(v, device=dev) for v in (ms_mixed, ms_fp64b, ms_single))
     # error of the first pose step against the FP64 oracle (the reference's window.solve restated), all windows
     errs_m, errs_f = [], []
     for i, w in enumerate(wins):
@@ -471,7 +463,7 @@ def cpu_baseline(L, R, args):
 
 def main():
     args = parse()
-    ws, rank, local = dist_env()
+    ws, rank, local = D.env()
     if args.impl == "reference":
         return run_reference(args, ws, rank)
     return run_ours(args, ws, rank, local)

@@ -37,6 +37,24 @@ def test_batch_matches_oracle(precision, tol_dx):
         assert np.abs(w.lmp - r.lmp).max() < 1e-5 * max(1.0, np.abs(r.lmp).max())
 
 
+@pytest.mark.parametrize("precision,tol_dx", [("fp64", 1e-8), ("mixed", 1e-6)])
+def test_batch_with_extrinsic_and_depth_prior(precision, tol_dx):
+    """Non-identity body-to-camera extrinsic and the inverse-depth prior (the paths the golden windows pin)."""
+    from xclean_b200.backend.ba import solve_batch
+    ext = dict(Rbc=S.so3_exp(np.array([0.02, -0.03, 0.01])), pbc=np.array([0.05, -0.02, 0.1]), depth_prior=0.05)
+    ws = [S.make_window(None, K=k, L=l, obs_min=2, obs_max=8, rng=np.random.default_rng(100 + k), **ext)
+          for k, l in ((5, 120), (9, 350), (14, 600))]
+    ref = [w.copy() for w in ws]
+    outs = [BO.solve(r, iters=5, lam0=1e-4, hold=0) for r in ref]
+    res = solve_batch(ws, iters=5, lam0=1e-4, precision=precision, hold=0)
+    for i, (w, r, o) in enumerate(zip(ws, ref, outs)):
+        assert res["status"][i] == 0
+        assert rel(res["dx0_list"][i], o["dx0"]) < tol_dx, (i, rel(res["dx0_list"][i], o["dx0"]))
+        assert abs(res["cost0"][i] - o["cost0"]) <= 1e-9 * abs(o["cost0"])
+        assert res["accepted"][i] == o["accepted"], i
+        assert np.abs(w.pwb - r.pwb).max() < 1e-6 and np.abs(w.Rwb - r.Rwb).max() < 1e-6
+
+
 def test_config0_window_mixed_step_error():
     from xclean_b200.backend.ba import solve_batch
     w = S.config0_window(1)

@@ -2,8 +2,9 @@
 
 Subpackages mirror the reference modules they replace:
     xclean_b200.front.gpu_front   <- xclean.front.gpu_front
-    xclean_b200.backend.kernels   <- xclean.backend.kernels
-    xclean_b200.backend.ba        <- xclean.backend.ba (_solve_gpu, _solve_gpu_id) + the batched solve
+    xclean_b200.backend.kernels   <- xclean.backend.kernels (the local-BA stage kernels)
+    xclean_b200.backend.local_ba  <- xclean.backend.ba (_solve_gpu, _solve_gpu_id, build_pairs, warmup)
+    xclean_b200.backend.ba        <- xclean.vio.window.solve, batched over many windows in one launch
 The device code is libxcb200.so (xclean_b200/csrc, include/xcb200.h), called through ctypes."""
 
 __version__ = "0.1.0"

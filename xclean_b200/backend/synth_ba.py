@@ -61,12 +61,14 @@ class Window:
 
 def make_window(seed, K=10, L=1500, obs_min=2, obs_max=6, z0=2.0, z1=20.0, step_m=0.2, step_deg=5.0, px_noise=1.0,
                 outlier_frac=0.05, pose_m=0.05, pose_deg=1.0, depth_frac=0.05, fx=458.0, fy=458.0, cx=367.0,
-                cy=248.0, W=752, H=480, B=0.11, geometric=False, rng=None):
-    """-> Window (initial state in Rwb / pwb / lmp; truth in Rwb_true / pwb_true / lmp_true)."""
+                cy=248.0, W=752, H=480, B=0.11, geometric=False, rng=None, Rbc=None, pbc=None, depth_prior=0.0):
+    """-> Window (initial state in Rwb / pwb / lmp; truth in Rwb_true / pwb_true / lmp_true).  Rbc / pbc: the
+    body-to-camera extrinsic (identity by default); depth_prior > 0: an inverse-depth prior on every landmark with
+    that relative noise (none by default).  The defaults draw the same random sequence as without these options."""
     rng = np.random.default_rng(seed) if rng is None else rng
     # camera = body (identity extrinsic), smooth path: each step a random direction of norm step_m and a random axis
-    Rbc = np.eye(3)
-    pbc = np.zeros(3)
+    Rbc = np.eye(3) if Rbc is None else np.asarray(Rbc, np.float64)
+    pbc = np.zeros(3) if pbc is None else np.asarray(pbc, np.float64)
     Rs = [np.eye(3)]
     ps = [np.zeros(3)]
     v = np.array([0.3, 0.0, 1.0])
@@ -78,16 +80,16 @@ def make_window(seed, K=10, L=1500, obs_min=2, obs_max=6, z0=2.0, z1=20.0, step_
         ax /= np.linalg.norm(ax)
         Rs.append(Rs[-1] @ so3_exp(ax * math.radians(step_deg)))
         ps.append(ps[-1] + step_m * v)
-    Rwb_t = np.stack(Rs)
-    pwb_t = np.stack(ps)
+    Rwc_t = np.stack(Rs)                      # camera poses; the body poses follow from the extrinsic
+    pwc_t = np.stack(ps)
     # landmarks in keyframe 0's frustum
     zs = rng.uniform(z0, z1, L)
     us = rng.uniform(0.05 * W, 0.95 * W, L)
     vs = rng.uniform(0.05 * H, 0.95 * H, L)
     Pc0 = np.stack([(us - cx) / fx * zs, (vs - cy) / fy * zs, zs], 1)
-    Pw = Pc0 @ Rwb_t[0].T + pwb_t[0]
+    Pw = Pc0 @ Rwc_t[0].T + pwc_t[0]
     # every (keyframe, landmark) projection at once
-    Pc = np.einsum("kji,klj->kli", Rwb_t, Pw[None, :, :] - pwb_t[:, None, :])        # (K, L, 3)
+    Pc = np.einsum("kji,klj->kli", Rwc_t, Pw[None, :, :] - pwc_t[:, None, :])        # (K, L, 3)
     z = Pc[:, :, 2]
     with np.errstate(divide="ignore", invalid="ignore"):
         ul = fx * Pc[:, :, 0] / z + cx
@@ -127,13 +129,15 @@ def make_window(seed, K=10, L=1500, obs_min=2, obs_max=6, z0=2.0, z1=20.0, step_
     ob_z[1::2, 0] = zr
     first = ob_start[:-1] // 2                                                            # each landmark's first row
     host = ki[first] if Lk else np.zeros(0, np.int64)
-    Ph = np.einsum("lji,lj->li", Rwb_t[host], Pw[lidx] - pwb_t[host])
+    Ph = np.einsum("lji,lj->li", Rwc_t[host], Pw[lidx] - pwc_t[host])
     lmp_true = np.stack([Ph[:, 0] / Ph[:, 2], Ph[:, 1] / Ph[:, 2], 1.0 / Ph[:, 2]], 1) if Lk else np.zeros((0, 3))
     zh = zl[first] if Lk else np.zeros((0, 2))
     rho0 = lmp_true[:, 2] / (1.0 + rng.normal(0.0, depth_frac, Lk))
     lmp0 = np.stack([(zh[:, 0] - cx) / fx, (zh[:, 1] - cy) / fy, rho0], 1) if Lk else np.zeros((0, 3))
     lm_host = host.astype(np.int64)
     flat_n = 2 * nr
+    Rwb_t = Rwc_t @ Rbc.T
+    pwb_t = pwc_t - Rwb_t @ pbc
     # initial poses: keyframe 0 at the truth (held), the others perturbed
     Rwb0 = Rwb_t.copy()
     pwb0 = pwb_t.copy()
@@ -143,9 +147,13 @@ def make_window(seed, K=10, L=1500, obs_min=2, obs_max=6, z0=2.0, z1=20.0, step_
         Rwb0[k] = Rwb_t[k] @ so3_exp(ax * math.radians(pose_deg))
         d = rng.normal(0.0, 1.0, 3)
         pwb0[k] = pwb_t[k] + pose_m * d / np.linalg.norm(d)
+    rho_meas, rho_isig = np.zeros(Lk), np.zeros(Lk)
+    if depth_prior > 0 and Lk:
+        rho_meas = lmp_true[:, 2] * (1.0 + depth_prior * rng.normal(0.0, 1.0, Lk))
+        rho_isig = 1.0 / (depth_prior * lmp_true[:, 2])
     return Window(Rwb=np.ascontiguousarray(Rwb0), pwb=np.ascontiguousarray(pwb0), Rbc=Rbc, pbc=pbc,
                   lmp=np.ascontiguousarray(lmp0.reshape(-1, 3)), lm_host=lm_host, lm_mask=np.ones(Lk, np.bool_),
-                  rho_meas=np.zeros(Lk), rho_isig=np.zeros(Lk), ob_start=ob_start, ob_pose=ob_pose, ob_cam=ob_cam,
+                  rho_meas=rho_meas, rho_isig=rho_isig, ob_start=ob_start, ob_pose=ob_pose, ob_cam=ob_cam,
                   ob_z=np.ascontiguousarray(ob_z), ob_isig=np.full(flat_n, 1.0 / px_noise),
                   ob_valid=np.ones(flat_n, np.bool_), fx=float(fx), fy=float(fy), cx=float(cx), cy=float(cy),
                   B=float(B), huber_k=HUBER_K, Rwb_true=Rwb_t, pwb_true=pwb_t,
