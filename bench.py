@@ -40,6 +40,9 @@ BUDGET = 2000
 HALF = 4            # 9x9 ZNCC
 DLO, DHI = 0, 96
 METRIC = "frontend frames/s"
+# ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_stereo launch over 8 frames (9.549 MB + 0.222 MB),
+# per frame; traffic grows with the frame count, so a launch of F frames moves F times this
+TRAFFIC_PER_FRAME = {"stereo": (9.549312e6 + 0.221952e6) / 8}
 
 
 def parse():
@@ -59,8 +62,6 @@ def parse():
     return ap.parse_args()
 
 
-
-
 # ------------------------------------------------------------------------------------------------ clocks sampler
 class Clocks:
     """nvidia-smi samples during the timed region: median SM MHz under load and the throttle reasons seen."""
@@ -77,7 +78,7 @@ class Clocks:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -267,7 +268,6 @@ def run_ours(args, ws, rank, local):
             stage_sum[k] += v
     ev1.record(stream)
     torch.cuda.synchronize()
-    clk = clocks.stop()
     ms = ev0.elapsed_time(ev1)
     gf.sync_check(sptr)
     ms = D.max_over_ranks(ms, device=dev)            # the slowest rank defines the step time
@@ -312,6 +312,7 @@ def run_ours(args, ws, rank, local):
         e2e = {"value": ws * F * args.steps / (ems / 1e3), "unit": "frames/s", "h2d_bytes_per_step": 2 * F * W * H,
                "d2h_bytes_per_step": d2h}
         counts = outs[-1]["counts"]
+    clk = clocks.stop()                 # sampled over the device-resident and the end-to-end timed regions
     # ---------------------------------------------------------------- roofline of the dominant stage
     per_step = {k: v / args.steps for k, v in stage_sum.items()}
     dom = max(per_step, key=per_step.get)
@@ -332,7 +333,11 @@ def run_ours(args, ws, rank, local):
     frame_bytes = 2 * W * H + BUDGET * (8 + 32 + 33) + BUDGET * 32 + 16 * BUDGET
     roof = {"bound": "hbm", "kernel": "stage:%s" % dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_kind": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_kind if peak_kind == "measured"
-            else "fallback 6650 GB/s", "traffic": None, "algorithmic_bytes_per_launch": bytes_launch,
+            else "fallback 6650 GB/s",
+            "traffic": (TRAFFIC_PER_FRAME[dom] * (F / nb)) if dom in TRAFFIC_PER_FRAME else None,
+            "traffic_note": "DRAM read+write per launch, ncu capture of 8 frames scaled by frames "
+                            "(profiles/k_stereo_kitti1241_8frames.md)" if dom in TRAFFIC_PER_FRAME else None,
+            "algorithmic_bytes_per_launch": bytes_launch,
             "whole_path_frac": frame_bytes * value / ws / 1e9 / peak,
             "stage_ms_per_step": per_step}
     cpu = None
