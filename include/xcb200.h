@@ -178,6 +178,24 @@ int xcb_ba_noalloc_max_landmarks(void);
 int xcb_ba_solve_windows_noalloc(const xcb_ba_windows* w, int Lt, int max_slots, int iters, double lam0, int mode,
                                  double* stats, double* dx0, int dx0_stride, int grid, void* stream);
 
+/* Exact second-order steps on the window cost (no reference counterpart: the differentiable BA of the north-star API).
+   XCB_BA_NEWTON_POLISH: `steps` Newton steps with the exact Hessian (window.solve's LM converges only linearly when
+   Huber weights are active), the state updated in place.  XCB_BA_NEWTON_ADJOINT: at the converged state, solves
+   H x = dL/dstate (gpose: [slots][6] = dL/d(dphi, dp) per slot of the batch, landmarks 0) and writes
+   dL/dtheta = -(d2C / dtheta dstate) x: gtheta [nw][11] = fx, fy, cx, cy, B, omega (3), t (3) of the left-to-right
+   extrinsic at the rectified rig; gisig [M] = per-row weight 1/sigma; gz [M][2] = per-row pixels.  H is applied
+   exactly (dual numbers) and the system solved by conjugate gradients preconditioned with the Gauss-Newton Schur
+   system until the relative residual is below `tol` (at most `maxit` iterations).  stats [nw][4] = iterations,
+   final relative residual, final gradient max-norm (polish), status (0 ok, 1 Gauss-Newton system not positive
+   definite, 2 non-positive curvature met: the state is not at a strict minimum, so no step is taken, -1 window too
+   large, -2 a landmark touches more than 16 keyframes). */
+#define XCB_BA_NEWTON_POLISH 0
+#define XCB_BA_NEWTON_ADJOINT 1
+size_t xcb_ba_newton_scratch_bytes(int nw, int Lt);
+int xcb_ba_newton_windows_dev(const xcb_ba_windows* w, int max_slots, int mode, int steps, int maxit, double tol,
+                              const double* gpose, double* gtheta, double* gisig, double* gz, double* stats,
+                              void* scratch, size_t scratch_bytes, int grid, void* stream);
+
 /* ----------------------------------------------------------------------------------------------------------------
    Local-BA stage kernels: one entry point per kernel of src/xclean/backend/kernels.py, same argument order and
    meaning, device pointers (float32 / int32, the reference's layouts), enqueued on `stream` (NULL = the legacy default

@@ -1,0 +1,115 @@
+"""The implicit adjoint of the window solve (BAAdjoint) against the float64 autodiff reference and float64 central
+finite differences (oracle/ba_adjoint_ref.py: the window cost in torch, Newton-converged, exact Hessians by autograd).
+
+Tolerance (the differentiable-BA target): 1e-5 relative, group-wise (max-norm of the error over max-norm of the
+reference gradient) for the window parameters (fx, fy, cx, cy, B, the left-to-right extrinsic), the per-row weights
+and the pixels.  The windows carry a non-identity body-to-camera extrinsic, an inverse-depth prior and 5 % outliers
+(so Huber weights are active)."""
+import copy
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+
+def _ext():
+    from xclean_b200.backend import synth_ba as S
+    return dict(Rbc=S.so3_exp(np.array([0.02, -0.03, 0.01])), pbc=np.array([0.05, -0.02, 0.1]), depth_prior=0.05)
+
+
+def _windows():
+    from xclean_b200.backend import synth_ba as S
+    return [S.make_window(None, K=k, L=l, obs_min=2, obs_max=4, rng=np.random.default_rng(s), **_ext())
+            for k, l, s in ((4, 30, 9), (5, 40, 8))]
+
+
+def _rel(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+@pytest.fixture(scope="module")
+def run():
+    import torch
+    from oracle import ba_adjoint_ref as AR
+    from xclean_b200.backend.adjoint import BAAdjoint, inputs_of
+    from xclean_b200.backend.ba import BatchSolver
+    ws = _windows()
+    solver = BatchSolver(ws, "cuda", hold=0)
+    inp = inputs_of(solver)
+    p = BAAdjoint.apply(*inp, solver, 100, 4)
+    torch.cuda.synchronize()
+    so = solver.host["slot_off"]
+    ptrue = torch.as_tensor(np.concatenate([w.pwb_true for w in ws]), device="cuda")
+    loss = ((p - ptrue) ** 2).sum()
+    loss.backward()
+    Rwb = solver.t["Rwb"].cpu().numpy().reshape(-1, 3, 3)
+    pwb = solver.t["pwb"].cpu().numpy()
+    lmp = solver.t["lmp"].cpu().numpy()
+    lo, ro = solver.host["lm_off"], np.concatenate([[0], np.cumsum([w.ob_pose.shape[0] for w in ws])])
+    refs = []
+    for i, w in enumerate(ws):
+        c = w.copy()
+        P, L = w.Rwb.shape[0], w.lmp.shape[0]
+        c.Rwb, c.pwb, c.lmp = Rwb[so[i]:so[i] + P].copy(), pwb[so[i]:so[i] + P].copy(), lmp[lo[i]:lo[i] + L].copy()
+        W = AR.Window(c, hold=0)
+        AR.solve(W, W.theta0, W.isig0, W.z0)
+        dLdp = 2 * (W.p0.numpy() - w.pwb_true)
+        refs.append((W, dLdp, AR.implicit_grad(W, W.theta0, W.isig0, W.z0, dLdp), ro[i], ro[i + 1]))
+    return dict(ws=ws, solver=solver, inp=inp, p=p.detach().cpu().numpy(), refs=refs, so=so)
+
+
+def test_forward_converges_to_the_reference_stationary_point(run):
+    st = run["solver"].newton(0)          # no step: just the gradient at the state
+    assert float(st[:, 2].max()) < 1e-6, st
+    assert int(st[:, 3].abs().max()) == 0
+    for i, (W, _, _, _, _) in enumerate(run["refs"]):
+        P = W.P
+        dev = run["p"][run["so"][i]:run["so"][i] + P]
+        assert np.abs(dev - W.p0.numpy()).max() < 1e-9
+
+
+def test_adjoint_matches_the_autodiff_reference(run):
+    gi, gb, ge, gw, gp = (x.grad.detach().cpu().numpy() for x in run["inp"])
+    for i, (W, _, (gth, gis, gz), r0, r1) in enumerate(run["refs"]):
+        dev_theta = np.concatenate([gi[i], [gb[i]], ge[i]])
+        assert _rel(dev_theta, gth) < TOL, (i, dev_theta, gth)
+        assert _rel(gw[r0:r1], gis) < TOL
+        assert _rel(gp[r0:r1], gz) < TOL
+
+
+def test_newton_reports_a_state_that_is_not_a_strict_minimum():
+    """A window whose LM solve stalls (this seed: window.solve stops where the Hessian is indefinite) gets status 2
+    and no Newton step."""
+    import torch
+    from xclean_b200.backend import synth_ba as S
+    from xclean_b200.backend.ba import BatchSolver
+    w = S.make_window(None, K=4, L=30, obs_min=2, obs_max=4, rng=np.random.default_rng(7), **_ext())
+    solver = BatchSolver([w], "cuda", hold=0)
+    solver.solve(100, 1e-4, "fp64")
+    before = solver.t["pwb"].clone()
+    st = solver.newton(2)
+    torch.cuda.synchronize()
+    assert int(st[0, 3]) == 2
+    assert torch.equal(before, solver.t["pwb"])
+
+
+def test_adjoint_matches_central_finite_differences(run):
+    import torch
+    from oracle import ba_adjoint_ref as AR
+    gi, gb, ge, gw, gp = (x.grad.detach().cpu().numpy() for x in run["inp"])
+    W, _dLdp, _g, r0, r1 = run["refs"][0]
+    ptrue = torch.as_tensor(run["ws"][0].pwb_true)
+    loss = lambda p: ((p - ptrue) ** 2).sum()
+    rows = np.nonzero(np.abs(gw[r0:r1]) > 1e-3 * np.abs(gw[r0:r1]).max())[0][:4].tolist()
+    zi = np.nonzero(np.abs(gp[r0:r1].reshape(-1)) > 1e-3 * np.abs(gp[r0:r1]).max())[0][:4].tolist()
+    fd = AR.fd_grad(copy.deepcopy(W), W.theta0, W.isig0, W.z0, loss, step=1e-6, idx={"isig": rows, "z": zi})
+    dev_theta = np.concatenate([gi[0], [gb[0]], ge[0]])
+    assert _rel(dev_theta, fd["theta"]) < TOL, (dev_theta, fd["theta"])
+    scale_w = np.abs(gw[r0:r1]).max()
+    scale_z = np.abs(gp[r0:r1]).max()
+    assert np.abs(gw[r0:r1][rows] - fd["isig"][rows]).max() < TOL * scale_w
+    assert np.abs(gp[r0:r1].reshape(-1)[zi] - fd["z"].reshape(-1)[zi]).max() < TOL * scale_z

@@ -69,10 +69,15 @@ class BaWindows(ctypes.Structure):
 
 XCB_BA_FP64 = 0
 XCB_BA_MIXED = 1
+XCB_BA_NEWTON_POLISH = 0
+XCB_BA_NEWTON_ADJOINT = 1
 _SIGS.update({
     "xcb_ba_scratch_bytes": (c_size_t, [c_int, c_int]),
     "xcb_ba_solve_windows_dev": (c_int, [ctypes.POINTER(BaWindows), c_int, c_int, c_double, c_int, P, P, c_int, P,
                                          c_size_t, c_int, P]),
+    "xcb_ba_newton_scratch_bytes": (c_size_t, [c_int, c_int]),
+    "xcb_ba_newton_windows_dev": (c_int, [ctypes.POINTER(BaWindows), c_int, c_int, c_int, c_int, c_double, P, P, P,
+                                          P, P, P, c_size_t, c_int, P]),
     "xcb_ba_noalloc_max_landmarks": (c_int, []),
     "xcb_ba_solve_windows_noalloc": (c_int, [ctypes.POINTER(BaWindows), c_int, c_int, c_int, c_double, c_int, P, P,
                                              c_int, c_int, P]),

@@ -116,6 +116,41 @@ class BatchSolver:
                                                  int(grid), ctypes.c_void_p(s.cuda_stream or None))
         _lib.check(rc, None, "xcb_ba_solve_windows_dev")
 
+    def newton(self, steps=3, maxit=60, tol=1e-12, stream=None, grid=0):
+        """Exact-Hessian Newton steps on every window (in place): the converged state the adjoint differentiates.
+        -> per-window stats tensor [nw, 4] (CG iterations, relative residual, final gradient max-norm, status)."""
+        return self._newton(_lib.XCB_BA_NEWTON_POLISH, steps, maxit, tol, None, stream, grid)[0]
+
+    def adjoint(self, gpose, maxit=60, tol=1e-12, stream=None, grid=0):
+        """dL/dtheta at the current (converged) state for dL/d(dphi, dp) = gpose [slots, 6] (float64 CUDA tensor)
+        -> (stats [nw, 4], gtheta [nw, 11], gisig [M], gz [M, 2])."""
+        return self._newton(_lib.XCB_BA_NEWTON_ADJOINT, 0, maxit, tol, gpose, stream, grid)
+
+    def _newton(self, mode, steps, maxit, tol, gpose, stream, grid):
+        torch = self.torch
+        s = stream if stream is not None else torch.cuda.current_stream(self.dev)
+        M = int(self.host["ob_isig"].shape[0])
+        if not hasattr(self, "nscratch"):
+            nb = int(_lib.lib().xcb_ba_newton_scratch_bytes(self.nw, int(self.host["lmp"].shape[0])))
+            self.nscratch = torch.zeros(nb, dtype=torch.uint8, device=self.dev)
+        stats = torch.zeros((max(self.nw, 1), 4), dtype=torch.float64, device=self.dev)
+        gtheta = torch.zeros((max(self.nw, 1), 11), dtype=torch.float64, device=self.dev)
+        gisig = torch.zeros(max(M, 1), dtype=torch.float64, device=self.dev)
+        gz = torch.zeros((max(M, 1), 2), dtype=torch.float64, device=self.dev)
+        gp = None
+        if gpose is not None:
+            gp = gpose.to(self.dev, torch.float64).contiguous()
+            if tuple(gp.shape) != (int(self.host["Rwb"].shape[0]), 6):
+                raise ValueError("adjoint: gpose must be [slots, 6]")
+        rc = _lib.lib().xcb_ba_newton_windows_dev(
+            ctypes.byref(self.desc), self.max_slots, int(mode), int(steps), int(maxit), float(tol),
+            ctypes.c_void_p(gp.data_ptr() if gp is not None else None), ctypes.c_void_p(gtheta.data_ptr()),
+            ctypes.c_void_p(gisig.data_ptr()), ctypes.c_void_p(gz.data_ptr()), ctypes.c_void_p(stats.data_ptr()),
+            ctypes.c_void_p(self.nscratch.data_ptr()), self.nscratch.numel(), int(grid),
+            ctypes.c_void_p(s.cuda_stream or None))
+        _lib.check(rc, None, "xcb_ba_newton_windows_dev")
+        return stats[:self.nw], gtheta[:self.nw], gisig[:M], gz[:M]
+
     def results(self):
         st = self.stats.cpu().numpy()[:self.nw]
         return {"cost0": st[:, 0], "cost": st[:, 1], "accepted": st[:, 2].astype(np.int64), "lam": st[:, 3],

@@ -50,6 +50,43 @@ static int ba_fail(int code, const char* msg)
     return code;
 }
 
+extern "C" size_t xcb_ba_newton_scratch_bytes(int nw, int Lt)
+{
+    (void)nw;
+    return ((size_t)(Lt > 0 ? Lt : 1) * 18 * sizeof(double) + 255) / 256 * 256 + 256;
+}
+
+extern "C" int xcb_ba_newton_windows_dev(const xcb_ba_windows* w, int max_slots, int mode, int steps, int maxit,
+                                         double tol, const double* gpose, double* gtheta, double* gisig, double* gz,
+                                         double* stats, void* scratch, size_t scratch_bytes, int grid, void* stream)
+{
+    if (!w || !stats || !scratch) return ba_fail(XCB_ERR_ARG, "ba_newton: null argument");
+    if (w->nw <= 0) return XCB_OK;
+    if (max_slots < 1 || max_slots > xcb_ba_max_slots())
+        return ba_fail(XCB_ERR_CAPACITY, "ba_newton: max_slots out of range (1..20)");
+    if (mode != XCB_BA_NEWTON_POLISH && mode != XCB_BA_NEWTON_ADJOINT) return ba_fail(XCB_ERR_ARG, "ba_newton: mode");
+    if (mode == XCB_BA_NEWTON_ADJOINT && (!gpose || !gtheta)) return ba_fail(XCB_ERR_ARG, "ba_newton: adjoint outputs");
+    if (steps < 0 || maxit < 1) return ba_fail(XCB_ERR_ARG, "ba_newton: steps / maxit");
+    cudaStream_t st = (cudaStream_t)stream;
+    // scratch: [counter (256 B)][18 doubles per landmark]
+    int* counter = (int*)scratch;
+    double* lsc = (double*)((char*)scratch + 256);
+    (void)scratch_bytes;
+    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), st);
+    if (e != cudaSuccess) return ba_fail(XCB_ERR_CUDA, cudaGetErrorString(e));
+    if (grid <= 0) {
+        int dev = 0, sms = XCB_B200_SMS;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        grid = sms;
+    }
+    if (grid > w->nw) grid = w->nw;
+    e = xcb_launch_ba_newton(*w, max_slots, mode, steps, maxit, tol, gpose, gtheta, gisig, gz, stats, lsc, counter,
+                             grid, st);
+    if (e != cudaSuccess) return ba_fail(XCB_ERR_CUDA, cudaGetErrorString(e));
+    return XCB_OK;
+}
+
 // ------------------------------------------------------------------------------------------------------------------
 // Allocation-free batched window solve.
 //

@@ -11,3 +11,7 @@ int xcb_ba_max_slots();
 cudaError_t xcb_launch_ba_windows(const XcbBaWindows& d, int max_slots, int iters, double lam0, int mode,
                                   double* stats, double* dx0, int dx0_stride, double* lmp_trial, int* counter,
                                   int grid, cudaStream_t st);
+size_t xcb_ba_newton_smem_bytes(int maxP);
+cudaError_t xcb_launch_ba_newton(const XcbBaWindows& d, int max_slots, int mode, int steps, int maxit, double tol,
+                                 const double* gpose, double* gtheta, double* gisig, double* gz, double* stats,
+                                 double* lsc, int* counter, int grid, cudaStream_t st);

@@ -854,6 +854,619 @@ __global__ void __launch_bounds__(BA_THREADS, 1) k_ba_windows(XcbBaWindows d, in
     }
 }
 
+// =====================================================================================================================
+// Exact second derivatives of the window cost: Newton polish and the implicit adjoint.
+//
+// The cost C(x, theta) = sum_k huber(|e_k|) + sum_l huber(|r_l|) (the same terms as above).  Its exact Hessian H is
+// never formed: H p comes from evaluating the analytic gradient (w J^T e, the Jacobians of obs_lin) in dual numbers
+// along p, which also gives the mixed derivative (d2C / dtheta dx) p when the analytic theta-gradient is evaluated the
+// same way.  At a stationary point (the converged solve) this equals the Hessian of C in the pose charts used here
+// (R <- R Exp(dphi), p <- p + dp), the terms of the chart's connection being proportional to the gradient.
+// H x = b is solved by conjugate gradients preconditioned with the Gauss-Newton system: its Schur complement is built
+// and Cholesky-factored once per linearisation, each preconditioner application is two landmark passes and one
+// triangular solve with that factor, each CG iteration one dual pass for H p.
+// =====================================================================================================================
+struct Dual {
+    double v, e;
+    __host__ __device__ Dual() : v(0.0), e(0.0) {}
+    __host__ __device__ Dual(double x) : v(x), e(0.0) {}
+    __host__ __device__ Dual(double x, double y) : v(x), e(y) {}
+    __device__ Dual& operator+=(const Dual& o) { v += o.v; e += o.e; return *this; }
+    __device__ Dual& operator-=(const Dual& o) { v -= o.v; e -= o.e; return *this; }
+};
+__device__ __forceinline__ Dual operator+(Dual a, Dual b) { return Dual(a.v + b.v, a.e + b.e); }
+__device__ __forceinline__ Dual operator-(Dual a, Dual b) { return Dual(a.v - b.v, a.e - b.e); }
+__device__ __forceinline__ Dual operator-(Dual a) { return Dual(-a.v, -a.e); }
+__device__ __forceinline__ Dual operator*(Dual a, Dual b) { return Dual(a.v * b.v, a.e * b.v + a.v * b.e); }
+__device__ __forceinline__ Dual operator/(Dual a, Dual b)
+{
+    const double iv = 1.0 / b.v;
+    return Dual(a.v * iv, (a.e - a.v * iv * b.e) * iv);
+}
+__device__ __forceinline__ bool operator<=(Dual a, Dual b) { return a.v <= b.v; }
+__device__ __forceinline__ bool operator<(Dual a, Dual b) { return a.v < b.v; }
+__device__ __forceinline__ bool operator>(Dual a, Dual b) { return a.v > b.v; }
+__device__ __forceinline__ Dual sqrt(Dual a)
+{
+    const double s = ::sqrt(a.v);
+    return Dual(s, s > 0.0 ? 0.5 * a.e / s : 0.0);
+}
+__device__ __forceinline__ Dual fabs(Dual a) { return a.v < 0.0 ? -a : a; }
+
+#define NT_MODE_GRAD 0          // value parts: the exact gradient
+#define NT_MODE_HV 1            // dual parts: H p
+#define NT_MODE_THETA 2         // dual parts of the theta-gradient: (d2C / dtheta dx) p
+#define NT_THETA 11             // fx, fy, cx, cy, B, omega (3), t (3)
+
+// per-landmark scratch of the exact solves (global memory): b (rhs), r (residual), p (direction, the dual pass's
+// tangent), x (solution), z (preconditioned residual), Hp
+#define NT_LM_STRIDE 18
+#define NT_B 0
+#define NT_R 3
+#define NT_P 6
+#define NT_X 9
+#define NT_Z 12
+#define NT_HP 15
+
+struct NtShared {
+    double gp[BA_MAXN];         // value accumulators of the pose gradient
+    double hp[BA_MAXN];         // dual accumulators (H p)
+    double th[NT_THETA];
+    double red2;
+};
+
+__device__ __forceinline__ bool held(const BaShared& sh, int q) { return sh.w.hold >= 0 && q / 6 == sh.w.hold; }
+
+// geometry of the state moved along p: Rwb (I + eps hat(p_phi)), pwb + eps p_p (p = zp per slot)
+__device__ void slot_geo_dual(const BaShared& sh, const double* zp, SlotGeo<Dual>& G)
+{
+    const int P = sh.w.P;
+    for (int s = threadIdx.x; s < P; s += blockDim.x) {
+        const double* R0 = sh.Rwb + 9 * s;
+        const double w0 = zp[6 * s], w1 = zp[6 * s + 1], w2 = zp[6 * s + 2];
+        const double K[9] = {0.0, -w2, w1, w2, 0.0, -w0, -w1, w0, 0.0};
+        Dual R[9], p[3];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+                R[i * 3 + j] = Dual(R0[i * 3 + j],
+                                    R0[i * 3] * K[j] + R0[i * 3 + 1] * K[3 + j] + R0[i * 3 + 2] * K[6 + j]);
+        for (int i = 0; i < 3; ++i) p[i] = Dual(sh.pwb[3 * s + i], zp[6 * s + 3 + i]);
+        Dual Rwc[9], N[9];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                Dual a = Dual(0.0), b = Dual(0.0);
+                for (int k = 0; k < 3; ++k) {
+                    a = a + R[i * 3 + k] * Dual(sh.w.Rbc[3 * k + j]);
+                    b = b + R[i * 3 + k] * Dual(sh.w.Px[3 * k + j]);
+                }
+                Rwc[i * 3 + j] = a;
+                N[i * 3 + j] = b;
+            }
+        for (int i = 0; i < 3; ++i) {
+            Dual a = p[i];
+            for (int k = 0; k < 3; ++k) a = a + R[i * 3 + k] * Dual(sh.w.pbc[k]);
+            G.pwc[3 * s + i] = a;
+        }
+        for (int i = 0; i < 9; ++i) { G.Rwc[9 * s + i] = Rwc[i]; G.N[9 * s + i] = N[i]; }
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                Dual a = Dual(0.0);
+                for (int k = 0; k < 3; ++k) a = a + Rwc[3 * k + i] * N[3 * k + j];
+                G.M[9 * s + i * 3 + j] = a;
+            }
+    }
+    if (threadIdx.x < 9) G.Rcb[threadIdx.x] = Dual(sh.w.Rcb[threadIdx.x]);
+    __syncthreads();
+}
+
+// d e / d theta of one observation row group (whitened residual e): columns fx, fy, cx, cy, B, omega (3), t (3) of
+// the left-to-right extrinsic at the rectified rig (q_r = Exp(omega) q + rho (t - B e_x)), the row's weight 1/sigma,
+// and its pixel (z0, z1).  -> 0 when not evaluable.
+template <typename T>
+__device__ __forceinline__ int obs_theta(const BaWin& w, const SlotGeo<T>& G, const T lm[3], int h, int t, int cam,
+                                         const double* z, double isgd, T de[2][14])
+{
+    const T a = lm[0], b = lm[1], rho = lm[2];
+    const T* Rh = G.Rwc + 9 * h;
+    const T* Rt = G.Rwc + 9 * t;
+    const T d0 = G.pwc[3 * h] - G.pwc[3 * t], d1 = G.pwc[3 * h + 1] - G.pwc[3 * t + 1],
+            d2 = G.pwc[3 * h + 2] - G.pwc[3 * t + 2];
+    const T Y0 = Rh[0] * a + Rh[1] * b + Rh[2] + rho * d0;
+    const T Y1 = Rh[3] * a + Rh[4] * b + Rh[5] + rho * d1;
+    const T Y2 = Rh[6] * a + Rh[7] * b + Rh[8] + rho * d2;
+    const T q0 = Rt[0] * Y0 + Rt[3] * Y1 + Rt[6] * Y2;
+    const T q1 = Rt[1] * Y0 + Rt[4] * Y1 + Rt[7] * Y2;
+    const T q2 = Rt[2] * Y0 + Rt[5] * Y1 + Rt[8] * Y2;
+    if (q2 <= (T)1e-9) return 0;
+    const T s = (T)isgd, fx = (T)w.fx, fy = (T)w.fy, B = (T)w.B;
+    for (int r = 0; r < 2; ++r)
+        for (int j = 0; j < 14; ++j) de[r][j] = (T)0.0;
+    const T iq = (T)1.0 / q2;
+    if (cam == 0) {
+        de[0][0] = q0 * iq * s;
+        de[1][1] = q1 * iq * s;
+        de[0][2] = s;
+        de[1][3] = s;
+        de[0][11] = fx * q0 * iq + (T)w.cx - (T)z[0];
+        de[1][11] = fy * q1 * iq + (T)w.cy - (T)z[1];
+        de[0][12] = -s;
+        de[1][13] = -s;
+    } else {
+        const T qr0 = q0 - rho * B;
+        de[0][0] = qr0 * iq * s;
+        de[0][2] = s;
+        de[0][4] = -fx * rho * iq * s;
+        const T D0 = fx * iq * s, D2 = -fx * qr0 * iq * iq * s;          // d e_R / d q_r (its u row)
+        de[0][5] = D2 * q1;                                              // D (-hat(q))
+        de[0][6] = D0 * q2 - D2 * q0;
+        de[0][7] = -D0 * q1;
+        de[0][8] = D0 * rho;
+        de[0][10] = D2 * rho;
+        de[0][11] = fx * qr0 * iq + (T)w.cx - (T)z[0];
+        de[0][12] = -s;
+    }
+    return 1;
+}
+
+// One pass over the window's landmarks with the state moved along p (sh.dx for the poses, scratch NT_P for the
+// landmarks): value parts = the exact gradient, dual parts = H p; in NT_MODE_THETA the theta-gradient's dual parts.
+// Outputs: nt.gp / nt.hp (pose accumulators, atomics), per landmark: -gradient -> NT_B (GRAD), (H p)_l -> NT_HP (HV);
+// THETA: nt.th and the per-row outputs.  Landmarks that are not variables get zeros.
+__device__ void pass_dual(BaShared& sh, NtShared& nt, const XcbBaWindows& d, const SlotGeo<Dual>& G, int mode,
+                          double* lsc, double* gisig, double* gz)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int l = wid; l < sh.w.L; l += BA_WARPS) {
+        const int gl = sh.w.lm0 + l;
+        if (!d.lm_mask[gl]) continue;
+        const int h = d.lm_host[gl];
+        if ((unsigned)h >= (unsigned)sh.w.P) continue;
+        double* sc = lsc + (size_t)gl * NT_LM_STRIDE;
+        const int k0 = d.lm_ob[gl], nob = lm_rows(d, gl);
+        // the landmark moves along p only if it is a variable (its Gauss-Newton block passes the conditioning test,
+        // judged below on the same sums; a landmark that is not a variable has p_l = 0 in the scratch)
+        const Dual lm[3] = {Dual(d.lmp[3 * gl], sc[NT_P]), Dual(d.lmp[3 * gl + 1], sc[NT_P + 1]),
+                            Dual(d.lmp[3 * gl + 2], sc[NT_P + 2])};
+        Dual gl3[3] = {Dual(0.0), Dual(0.0), Dual(0.0)}, gh[6];
+        double hv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        int nobs = 0;
+        for (int i = 0; i < 6; ++i) gh[i] = Dual(0.0);
+        if (lane < nob) {
+            const int k = k0 + lane;
+            const int t = d.ob_pose[k];
+            Dual ob[33];
+            if (d.ob_valid[k] && (unsigned)t < (unsigned)sh.w.P &&
+                obs_lin<Dual>(sh.w, G, lm, h, t, d.ob_cam[k], d.ob_z + 2 * k, Dual(d.ob_isig[k]), ob, true)) {
+                const Dual en = sqrt(ob[OB_E] * ob[OB_E] + ob[OB_E + 1] * ob[OB_E + 1]);
+                Dual wt, cc;
+                huber_w<Dual>(en, Dual(sh.w.hk), &wt, &cc);
+                nobs = 1;
+                for (int i = 0; i < 3; ++i) {
+                    gl3[i] = wt * (ob[OB_JL + i] * ob[OB_E] + ob[OB_JL + 3 + i] * ob[OB_E + 1]);
+                    for (int j = 0; j < 3; ++j)
+                        hv[i * 3 + j] = wt.v * (ob[OB_JL + i].v * ob[OB_JL + j].v + ob[OB_JL + 3 + i].v * ob[OB_JL + 3 + j].v);
+                }
+                if (t != h) {
+                    for (int i = 0; i < 6; ++i) {
+                        const Dual gt = wt * (ob[OB_JT + i] * ob[OB_E] + ob[OB_JT + 6 + i] * ob[OB_E + 1]);
+                        gh[i] = wt * (ob[OB_JH + i] * ob[OB_E] + ob[OB_JH + 6 + i] * ob[OB_E + 1]);
+                        if (mode != NT_MODE_THETA) {
+                            atomicAdd(&nt.gp[6 * t + i], gt.v);
+                            atomicAdd(&nt.hp[6 * t + i], gt.e);
+                        }
+                    }
+                }
+                if (mode == NT_MODE_THETA) {
+                    Dual de[2][14];
+                    if (obs_theta<Dual>(sh.w, G, lm, h, t, d.ob_cam[k], d.ob_z + 2 * k, d.ob_isig[k], de)) {
+                        Dual gth[14];
+                        for (int j = 0; j < 14; ++j) gth[j] = wt * (ob[OB_E] * de[0][j] + ob[OB_E + 1] * de[1][j]);
+                        for (int j = 0; j < NT_THETA; ++j) atomicAdd(&nt.th[j], -gth[j].e);
+                        if (gisig) gisig[k] = -gth[11].e;
+                        if (gz) { gz[2 * k] = -gth[12].e; gz[2 * k + 1] = -gth[13].e; }
+                    }
+                }
+            }
+        }
+        // landmark sums (all lanes), the inverse-depth prior, the variable test
+        for (int i = 0; i < 9; ++i) hv[i] = warp_sum(hv[i]);
+        nobs = __popc(__ballot_sync(0xffffffffu, nobs != 0));
+        for (int i = 0; i < 3; ++i) {
+            gl3[i].v = warp_sum(gl3[i].v);
+            gl3[i].e = warp_sum(gl3[i].e);
+        }
+        for (int i = 0; i < 6; ++i) {
+            gh[i].v = warp_sum(gh[i].v);
+            gh[i].e = warp_sum(gh[i].e);
+        }
+        if (d.rho_isig[gl] > 0.0) {
+            const Dual ris = Dual(d.rho_isig[gl]);
+            const Dual r0 = (lm[2] - Dual(d.rho_meas[gl])) * ris;
+            Dual wt, cc;
+            huber_w<Dual>(fabs(r0), Dual(sh.w.hk), &wt, &cc);
+            gl3[2] = gl3[2] + wt * ris * r0;
+            hv[8] += wt.v * d.rho_isig[gl] * d.rho_isig[gl];
+        }
+        for (int i = 0; i < 3; ++i) hv[i * 4] += 1e-12;
+        const double det = hv[0] * (hv[4] * hv[8] - hv[5] * hv[7]) - hv[1] * (hv[3] * hv[8] - hv[5] * hv[6]) +
+                           hv[2] * (hv[3] * hv[7] - hv[4] * hv[6]);
+        const double tr = hv[0] + hv[4] + hv[8];
+        const bool var = nobs > 0 && det > 1e-18 * tr * tr * tr && isfinite(det);
+        if (lane == 0) {
+            if (mode != NT_MODE_THETA)
+                for (int i = 0; i < 6; ++i) {
+                    atomicAdd(&nt.gp[6 * h + i], gh[i].v);
+                    atomicAdd(&nt.hp[6 * h + i], gh[i].e);
+                }
+            if (mode == NT_MODE_GRAD)
+                for (int i = 0; i < 3; ++i) sc[NT_B + i] = var ? -gl3[i].v : 0.0;
+            else if (mode == NT_MODE_HV)
+                for (int i = 0; i < 3; ++i) sc[NT_HP + i] = var ? gl3[i].e : 0.0;
+        }
+        __syncwarp();
+    }
+}
+
+// Gauss-Newton preconditioner, part 1: y = r_p - sum_l Hpl Hll^-1 r_l (r_p = sh.g, r_l = NT_R) -> sh.y
+__device__ void pass_pre_a(BaShared& sh, const XcbBaWindows& d, WarpLm<double>* wls, const double* lsc)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int n = sh.w.n;
+    WarpLm<double>& wl = wls[wid];
+    for (int q = lane; q < BA_MAXN; q += 32) wl.acc[q] = 0.0;
+    __syncwarp();
+    double cdummy = 0.0;
+    for (int l = wid; l < sh.w.L; l += BA_WARPS) {
+        const int gl = sh.w.lm0 + l;
+        if (!d.lm_mask[gl]) continue;
+        double Hll[9], bl[3];
+        int nt;
+        const bool ok = lin_landmark<double>(sh, d, sh.g64, l, 0.0, d.lmp, wl, Hll, bl, &nt, &cdummy);
+        if (ok && nt) {
+            double Hi[9];
+            inv3<double>(Hll, Hi);
+            const double* r = lsc + (size_t)gl * NT_LM_STRIDE + NT_R;
+            double u[3];
+            for (int i = 0; i < 3; ++i) u[i] = Hi[i * 3] * r[0] + Hi[i * 3 + 1] * r[1] + Hi[i * 3 + 2] * r[2];
+            for (int q = lane; q < nt * 6; q += 32) {
+                const int a = q / 6, j = q % 6;
+                wl.acc[6 * wl.ts[a] + j] -= wl.Hlp[a][j] * u[0] + wl.Hlp[a][6 + j] * u[1] + wl.Hlp[a][12 + j] * u[2];
+            }
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < n; q += blockDim.x) {
+        double s = sh.g[q];
+        for (int k = 0; k < BA_WARPS; ++k) s += wls[k].acc[q];
+        sh.y[q] = s;
+    }
+    __syncthreads();
+}
+
+// part 2: z_l = Hll^-1 (r_l - Hlp delta_p) (delta_p = sh.y) -> NT_Z (zero for landmarks that are not variables)
+__device__ void pass_pre_b(BaShared& sh, const XcbBaWindows& d, WarpLm<double>* wls, double* lsc)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    WarpLm<double>& wl = wls[wid];
+    double cdummy = 0.0;
+    for (int l = wid; l < sh.w.L; l += BA_WARPS) {
+        const int gl = sh.w.lm0 + l;
+        if (!d.lm_mask[gl]) continue;
+        double Hll[9], bl[3];
+        int nt;
+        const bool ok = lin_landmark<double>(sh, d, sh.g64, l, 0.0, d.lmp, wl, Hll, bl, &nt, &cdummy);
+        if (lane == 0) {
+            double* sc = lsc + (size_t)gl * NT_LM_STRIDE;
+            if (!ok) {
+                sc[NT_Z] = sc[NT_Z + 1] = sc[NT_Z + 2] = 0.0;
+            } else {
+                double Hi[9];
+                inv3<double>(Hll, Hi);
+                double v[3] = {sc[NT_R], sc[NT_R + 1], sc[NT_R + 2]};
+                for (int a = 0; a < nt; ++a) {
+                    const int s = wl.ts[a];
+                    for (int i = 0; i < 3; ++i) {
+                        double acc = 0.0;
+                        for (int j = 0; j < 6; ++j) acc += wl.Hlp[a][i * 6 + j] * sh.y[6 * s + j];
+                        v[i] -= acc;
+                    }
+                }
+                for (int i = 0; i < 3; ++i) sc[NT_Z + i] = Hi[i * 3] * v[0] + Hi[i * 3 + 1] * v[1] + Hi[i * 3 + 2] * v[2];
+            }
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+}
+
+// the Gauss-Newton reduced system at the current state (no damping but 1e-12 / 1e-9 regularisation), held slot
+// identity, Cholesky in S64 -> 0 or -1 (not positive definite)
+__device__ int nt_gn_factor(BaShared& sh, const XcbBaWindows& d, double* S64, WarpLm<double>* wl64)
+{
+    const int n = sh.w.n, tid = threadIdx.x;
+    if (tid == 0) sh.lam = 0.0;
+    for (int q = tid; q < n * n; q += blockDim.x) S64[q] = 0.0;
+    for (int q = tid; q < n; q += blockDim.x) sh.y[q] = 0.0;
+    __syncthreads();
+    pass_build<double, false>(sh, d, sh.g64, S64, sh.y, wl64, nullptr);
+    __syncthreads();
+    const int hs = sh.w.hold;
+    if (hs >= 0 && hs < sh.w.P) {
+        for (int q = tid; q < 6 * n; q += blockDim.x) {
+            const int i = 6 * hs + q / n, j = q % n;
+            S64[i * n + j] = 0.0;
+            S64[j * n + i] = 0.0;
+        }
+        __syncthreads();
+        for (int q = tid; q < 6; q += blockDim.x) S64[(6 * hs + q) * n + 6 * hs + q] = 1.0;
+        __syncthreads();
+    }
+    for (int q = tid; q < n; q += blockDim.x) S64[q * n + q] += 1e-9;
+    __syncthreads();
+    return chol_factor(S64, n);
+}
+
+// sum over the window's variables of a_p b_p (poses, the held slot excluded) + a_l b_l (scratch offsets oa, ob)
+__device__ double nt_dot(BaShared& sh, NtShared& nt, const double* pa, const double* pb, const double* lsc, int oa,
+                         int ob)
+{
+    const int tid = threadIdx.x, n = sh.w.n;
+    double s = 0.0;
+    for (int q = tid; q < n; q += blockDim.x)
+        if (!held(sh, q)) s += pa[q] * pb[q];
+    for (int l = tid; l < sh.w.L; l += blockDim.x) {
+        const double* sc = lsc + (size_t)(sh.w.lm0 + l) * NT_LM_STRIDE;
+        s += sc[oa] * sc[ob] + sc[oa + 1] * sc[ob + 1] + sc[oa + 2] * sc[ob + 2];
+    }
+    s = warp_sum(s);
+    __syncthreads();
+    if (tid == 0) nt.red2 = 0.0;
+    __syncthreads();
+    if ((tid & 31) == 0) atomicAdd(&nt.red2, s);
+    __syncthreads();
+    return nt.red2;
+}
+
+// Gauss-Newton preconditioner: z = M^-1 r (r: sh.g, NT_R -> z: sh.y, NT_Z)
+__device__ void nt_precond(BaShared& sh, const XcbBaWindows& d, double* S64, WarpLm<double>* wl64, double* lsc)
+{
+    pass_pre_a(sh, d, wl64, lsc);
+    for (int q = threadIdx.x; q < sh.w.n; q += blockDim.x)
+        if (held(sh, q)) sh.y[q] = 0.0;
+    __syncthreads();
+    chol_solve(S64, sh.w.n, sh.y);
+    pass_pre_b(sh, d, wl64, lsc);
+}
+
+// H x = b (b_p = sh.rhs, b_l = NT_B) by conjugate gradients preconditioned with the Gauss-Newton system (its factor
+// in S64).  -> x (sh.dmp, NT_X); the final relative residual; *iters_out the iterations; *neg set if a non-positive
+// curvature p^T H p was met (the state is not a strict minimum).
+__device__ double nt_solve_exact(BaShared& sh, NtShared& nt, const XcbBaWindows& d, double* S64, unsigned char* dsm,
+                                 double* lsc, int maxit, double tol, int* iters_out, int* neg)
+{
+    const int n = sh.w.n, tid = threadIdx.x;
+    WarpLm<double>* wl64 = (WarpLm<double>*)(dsm + ba_off_x(n));
+    SlotGeo<Dual>* Gd = (SlotGeo<Dual>*)(dsm + ba_off_x(n));
+    for (int q = tid; q < n; q += blockDim.x) { sh.dmp[q] = 0.0; sh.g[q] = held(sh, q) ? 0.0 : sh.rhs[q]; }
+    for (int l = tid; l < sh.w.L; l += blockDim.x) {
+        double* sc = lsc + (size_t)(sh.w.lm0 + l) * NT_LM_STRIDE;
+        for (int i = 0; i < 3; ++i) { sc[NT_X + i] = 0.0; sc[NT_R + i] = sc[NT_B + i]; }
+    }
+    __syncthreads();
+    const double bnorm = sqrt(nt_dot(sh, nt, sh.g, sh.g, lsc, NT_R, NT_R));
+    *neg = 0;
+    double rel = 0.0;
+    int it = 0;
+    if (bnorm > 0.0) {
+        nt_precond(sh, d, S64, wl64, lsc);
+        for (int q = tid; q < n; q += blockDim.x) sh.dx[q] = sh.y[q];
+        for (int l = tid; l < sh.w.L; l += blockDim.x) {
+            double* sc = lsc + (size_t)(sh.w.lm0 + l) * NT_LM_STRIDE;
+            for (int i = 0; i < 3; ++i) sc[NT_P + i] = sc[NT_Z + i];
+        }
+        __syncthreads();
+        double rz = nt_dot(sh, nt, sh.g, sh.y, lsc, NT_R, NT_Z);
+        rel = 1.0;
+        for (it = 0; it < maxit; ++it) {
+            for (int q = tid; q < n; q += blockDim.x) { nt.gp[q] = 0.0; nt.hp[q] = 0.0; }
+            __syncthreads();
+            slot_geo_dual(sh, sh.dx, *Gd);
+            pass_dual(sh, nt, d, *Gd, NT_MODE_HV, lsc, nullptr, nullptr);
+            __syncthreads();
+            const double pAp = nt_dot(sh, nt, sh.dx, nt.hp, lsc, NT_P, NT_HP);
+            if (!(pAp > 0.0)) { *neg = 1; break; }
+            const double alpha = rz / pAp;
+            for (int q = tid; q < n; q += blockDim.x) {
+                if (held(sh, q)) continue;
+                sh.dmp[q] += alpha * sh.dx[q];
+                sh.g[q] -= alpha * nt.hp[q];
+            }
+            for (int l = tid; l < sh.w.L; l += blockDim.x) {
+                double* sc = lsc + (size_t)(sh.w.lm0 + l) * NT_LM_STRIDE;
+                for (int i = 0; i < 3; ++i) {
+                    sc[NT_X + i] += alpha * sc[NT_P + i];
+                    sc[NT_R + i] -= alpha * sc[NT_HP + i];
+                }
+            }
+            __syncthreads();
+            rel = sqrt(nt_dot(sh, nt, sh.g, sh.g, lsc, NT_R, NT_R)) / bnorm;
+            if (!(rel > tol)) { ++it; break; }
+            nt_precond(sh, d, S64, wl64, lsc);
+            const double rz_new = nt_dot(sh, nt, sh.g, sh.y, lsc, NT_R, NT_Z);
+            const double beta = rz_new / rz;
+            rz = rz_new;
+            for (int q = tid; q < n; q += blockDim.x) sh.dx[q] = held(sh, q) ? 0.0 : sh.y[q] + beta * sh.dx[q];
+            for (int l = tid; l < sh.w.L; l += blockDim.x) {
+                double* sc = lsc + (size_t)(sh.w.lm0 + l) * NT_LM_STRIDE;
+                for (int i = 0; i < 3; ++i) sc[NT_P + i] = sc[NT_Z + i] + beta * sc[NT_P + i];
+            }
+            __syncthreads();
+        }
+    }
+    *iters_out = it;
+    return rel;
+}
+
+// the exact gradient at the current state: -gradient -> sh.rhs (poses, held slot 0) and NT_B (landmarks)
+__device__ void nt_grad(BaShared& sh, NtShared& nt, const XcbBaWindows& d, unsigned char* dsm, double* lsc)
+{
+    const int n = sh.w.n, tid = threadIdx.x;
+    SlotGeo<Dual>* Gd = (SlotGeo<Dual>*)(dsm + ba_off_x(n));
+    for (int q = tid; q < n; q += blockDim.x) { sh.dx[q] = 0.0; nt.gp[q] = 0.0; nt.hp[q] = 0.0; }
+    for (int l = tid; l < sh.w.L; l += blockDim.x)
+        for (int i = 0; i < NT_LM_STRIDE; ++i) lsc[(size_t)(sh.w.lm0 + l) * NT_LM_STRIDE + i] = 0.0;
+    __syncthreads();
+    slot_geo_dual(sh, sh.dx, *Gd);
+    pass_dual(sh, nt, d, *Gd, NT_MODE_GRAD, lsc, nullptr, nullptr);
+    __syncthreads();
+    for (int q = tid; q < n; q += blockDim.x) sh.rhs[q] = held(sh, q) ? 0.0 : -nt.gp[q];
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(BA_THREADS, 1) k_ba_newton(XcbBaWindows d, int mode, int steps, int maxit,
+                                                             double tol, const double* gpose, double* gtheta,
+                                                             double* gisig, double* gz, double* stats, double* lsc,
+                                                             int* counter)
+{
+    extern __shared__ __align__(16) unsigned char dsm[];
+    __shared__ BaShared sh;
+    __shared__ NtShared nt;
+    const int tid = threadIdx.x;
+    for (;;) {
+        if (tid == 0) sh.win = atomicAdd(counter, 1);
+        __syncthreads();
+        const int wi = sh.win;
+        if (wi >= d.nw) break;
+        const int w = d.order ? d.order[wi] : wi;
+        if (tid == 0) {
+            BaWin& W = sh.w;
+            W.P = d.P[w]; W.L = d.L[w]; W.n = 6 * W.P; W.hold = d.hold ? d.hold[w] : -1;
+            W.lm0 = d.lm_off[w]; W.s0 = d.slot_off[w];
+            W.fx = d.cam[6 * w]; W.fy = d.cam[6 * w + 1]; W.cx = d.cam[6 * w + 2]; W.cy = d.cam[6 * w + 3];
+            W.B = d.cam[6 * w + 4]; W.hk = d.cam[6 * w + 5];
+            for (int i = 0; i < 9; ++i) W.Rbc[i] = d.ext[12 * w + i];
+            for (int i = 0; i < 3; ++i) W.pbc[i] = d.ext[12 * w + 9 + i];
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) W.Rcb[i * 3 + j] = W.Rbc[j * 3 + i];
+            double px[9] = {0.0, -W.pbc[2], W.pbc[1], W.pbc[2], 0.0, -W.pbc[0], -W.pbc[1], W.pbc[0], 0.0};
+            for (int i = 0; i < 9; ++i) W.Px[i] = px[i];
+            sh.lam = 0.0; sh.overflow = 0;
+            for (int i = 0; i < NT_THETA; ++i) nt.th[i] = 0.0;
+        }
+        __syncthreads();
+        const int P = sh.w.P, n = sh.w.n, s0 = sh.w.s0;
+        if (P > BA_MAXP || P < 1) {
+            if (tid == 0) stats[4 * w + 3] = -1.0;
+            __syncthreads();
+            continue;
+        }
+        for (int q = tid; q < P * 9; q += blockDim.x) sh.Rwb[q] = d.Rwb[9 * s0 + q];
+        for (int q = tid; q < P * 3; q += blockDim.x) sh.pwb[q] = d.pwb[3 * s0 + q];
+        __syncthreads();
+        double* S64 = (double*)dsm;
+        WarpLm<double>* wl64 = (WarpLm<double>*)(dsm + ba_off_x(n));
+        int iters = 0, status = 0, neg = 0;
+        double rel = 0.0, gmax = 0.0;
+        if (mode == XCB_BA_NEWTON_POLISH) {
+            for (int st = 0; st < steps; ++st) {
+                slot_geo(sh, sh.Rwb, sh.pwb);
+                if (nt_gn_factor(sh, d, S64, wl64)) { status = 1; break; }
+                nt_grad(sh, nt, d, dsm, lsc);
+                rel = nt_solve_exact(sh, nt, d, S64, dsm, lsc, maxit, tol, &iters, &neg);
+                if (neg) { status = 2; break; }            // not in the basin of a strict minimum: no step
+                // apply the Newton step x: poses R <- R Exp(dphi), p <- p + dp; landmarks that are variables += x_l
+                for (int s = tid; s < P; s += blockDim.x) {
+                    if (sh.w.hold == s) continue;
+                    double Re[9], R[9];
+                    so3_exp(sh.dmp + 6 * s, Re);
+                    for (int i = 0; i < 9; ++i) R[i] = sh.Rwb[9 * s + i];
+                    for (int i = 0; i < 3; ++i)
+                        for (int j = 0; j < 3; ++j)
+                            sh.Rwb[9 * s + 3 * i + j] = R[3 * i] * Re[j] + R[3 * i + 1] * Re[3 + j] + R[3 * i + 2] * Re[6 + j];
+                    for (int i = 0; i < 3; ++i) sh.pwb[3 * s + i] += sh.dmp[6 * s + 3 + i];
+                }
+                for (int l = tid; l < sh.w.L; l += blockDim.x) {
+                    const int gl = sh.w.lm0 + l;
+                    const double* sc = lsc + (size_t)gl * NT_LM_STRIDE;
+                    for (int i = 0; i < 3; ++i) d.lmp[3 * gl + i] += sc[NT_X + i];
+                }
+                __syncthreads();
+            }
+            // the gradient at the final state
+            slot_geo(sh, sh.Rwb, sh.pwb);
+            nt_grad(sh, nt, d, dsm, lsc);
+            double gm = 0.0;
+            for (int q = tid; q < n; q += blockDim.x) gm = fmax(gm, fabs(sh.rhs[q]));
+            for (int l = tid; l < sh.w.L; l += blockDim.x)
+                for (int i = 0; i < 3; ++i) gm = fmax(gm, fabs(lsc[(size_t)(sh.w.lm0 + l) * NT_LM_STRIDE + NT_B + i]));
+            for (int o = 16; o > 0; o >>= 1) gm = fmax(gm, __shfl_xor_sync(0xffffffffu, gm, o));
+            if (tid == 0) nt.red2 = 0.0;
+            __syncthreads();
+            if ((tid & 31) == 0) atomicMax((unsigned long long*)&nt.red2, (unsigned long long)__double_as_longlong(gm));
+            __syncthreads();
+            gmax = nt.red2;
+            for (int q = tid; q < P * 9; q += blockDim.x) d.Rwb[9 * s0 + q] = sh.Rwb[q];
+            for (int q = tid; q < P * 3; q += blockDim.x) d.pwb[3 * s0 + q] = sh.pwb[q];
+        } else {
+            // implicit adjoint: H x = dL/dx (poses from gpose, landmarks 0), then -(d2C / dtheta dx) x
+            slot_geo(sh, sh.Rwb, sh.pwb);
+            if (nt_gn_factor(sh, d, S64, wl64)) status = 1;
+            else {
+                for (int q = tid; q < n; q += blockDim.x) sh.rhs[q] = held(sh, q) ? 0.0 : gpose[6 * (size_t)s0 + q];
+                for (int l = tid; l < sh.w.L; l += blockDim.x)
+                    for (int i = 0; i < NT_LM_STRIDE; ++i) lsc[(size_t)(sh.w.lm0 + l) * NT_LM_STRIDE + i] = 0.0;
+                __syncthreads();
+                rel = nt_solve_exact(sh, nt, d, S64, dsm, lsc, maxit, tol, &iters, &neg);
+                if (neg) status = 2;
+                // the theta pass moves the state along the solution x
+                for (int q = tid; q < n; q += blockDim.x) sh.dx[q] = sh.dmp[q];
+                for (int l = tid; l < sh.w.L; l += blockDim.x) {
+                    double* sc = lsc + (size_t)(sh.w.lm0 + l) * NT_LM_STRIDE;
+                    for (int i = 0; i < 3; ++i) sc[NT_P + i] = sc[NT_X + i];
+                }
+                __syncthreads();
+                SlotGeo<Dual>* Gd = (SlotGeo<Dual>*)(dsm + ba_off_x(n));
+                slot_geo_dual(sh, sh.dx, *Gd);
+                pass_dual(sh, nt, d, *Gd, NT_MODE_THETA, lsc, gisig, gz);
+                __syncthreads();
+                if (tid < NT_THETA) gtheta[(size_t)w * NT_THETA + tid] = nt.th[tid];
+            }
+        }
+        if (tid == 0) {
+            stats[4 * w + 0] = iters;
+            stats[4 * w + 1] = rel;
+            stats[4 * w + 2] = gmax;
+            stats[4 * w + 3] = status ? (double)status : (sh.overflow ? -2.0 : 0.0);
+        }
+        __syncthreads();
+    }
+}
+
+size_t xcb_ba_newton_smem_bytes(int maxP)
+{
+    const int n = 6 * maxP;
+    size_t x = ba_x_bytes(n);
+    if (sizeof(SlotGeo<Dual>) > x) x = sizeof(SlotGeo<Dual>);
+    return ba_off_x(n) + x;
+}
+
+cudaError_t xcb_launch_ba_newton(const XcbBaWindows& d, int max_slots, int mode, int steps, int maxit, double tol,
+                                 const double* gpose, double* gtheta, double* gisig, double* gz, double* stats,
+                                 double* lsc, int* counter, int grid, cudaStream_t st)
+{
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(k_ba_newton, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)xcb_ba_newton_smem_bytes(BA_MAXP));
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    k_ba_newton<<<grid, BA_THREADS, xcb_ba_newton_smem_bytes(max_slots), st>>>(d, mode, steps, maxit, tol, gpose,
+                                                                               gtheta, gisig, gz, stats, lsc, counter);
+    return cudaGetLastError();
+}
+
 cudaError_t xcb_launch_ba_windows(const XcbBaWindows& d, int max_slots, int iters, double lam0, int mode,
                                   double* stats, double* dx0, int dx0_stride, double* lmp_trial, int* counter,
                                   int grid, cudaStream_t st)
