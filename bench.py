@@ -59,6 +59,7 @@ def parse():
     ap.add_argument("--ba-only", action="store_true",
                     help="run only the batched window BA part and print its JSON object (profiling)")
     ap.add_argument("--ba-windows", type=int, default=None, help="BA windows per step (default 256)")
+    ap.add_argument("--no-ba-large", action="store_true", help="skip the 20-keyframe windows and the adjoint")
     return ap.parse_args()
 
 
@@ -445,7 +446,92 @@ def run_ba(args, dev, stream, rank, ws_world, cpu=True):
         dt = time.perf_counter() - t0
         out["cpu_baseline"] = {"value": len(sample) / dt, "unit": "windows/s", "cores": cores, "kind": "port",
                                "sample": "%d of the windows, float64 window.solve, OpenMP over windows" % len(sample)}
+    if not args.no_ba_large:
+        out["large_windows"] = run_ba_large(args, dev, stream, ws_world, rank)
+        out["adjoint"] = run_adjoint(args, dev, stream, ws_world, rank)
     return out
+
+
+def run_ba_large(args, dev, stream, ws_world, rank):
+    """32 windows of 20 keyframes and 6,000 landmarks (3-15 observing keyframes, 10 % outliers), mixed precision,
+    5 LM iterations, one launch; the first pose step's error against the FP64 oracle."""
+    import torch
+    from oracle import ba_oracle as BO
+    from xclean_b200.backend import synth_ba as S
+    from xclean_b200.backend.ba import BatchSolver
+    wins = S.config4_windows(32, seed=4 + rank)
+    with torch.cuda.stream(stream):
+        bs = BatchSolver(wins, dev, hold=0)
+    torch.cuda.synchronize()
+    res = {}
+    for prec in ("mixed", "fp64"):
+        for _ in range(max(1, args.warmup)):
+            bs.reset()
+            bs.solve(BA_ITERS, BA_LAM0, prec, stream=stream)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            bs.reset()
+            bs.solve(BA_ITERS, BA_LAM0, prec, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        res[prec] = (D.max_over_ranks(e0.elapsed_time(e1) / args.steps, device=dev), bs.results())
+    errs = []
+    for i, w in enumerate(wins):
+        dx_o, _c, _ok = BO.step(w.copy(), BA_LAM0, hold=0)
+        n = 6 * w.Rwb.shape[0]
+        errs.append(float(np.linalg.norm(res["mixed"][1]["dx0"][i][:n] - dx_o) / max(np.linalg.norm(dx_o), 1e-300)))
+    return {"value": ws_world * len(wins) / (res["mixed"][0] / 1e3), "unit": "windows/s",
+            "fp64_batched_value": ws_world * len(wins) / (res["fp64"][0] / 1e3),
+            "ms_per_step": {"mixed_batched": res["mixed"][0], "fp64_batched": res["fp64"][0]},
+            "pose_step_rel_err_vs_fp64_oracle": {"mixed_max": max(errs), "mixed_median": float(np.median(errs))},
+            "config": {"workload": "32 windows x (20 keyframes, 6000 landmarks, 3-15 obs, 10% outliers), 5 LM "
+                                   "iterations", "landmarks": int(sum(w.lmp.shape[0] for w in wins)),
+                       "observation_rows": int(sum(w.ob_pose.shape[0] for w in wins))}}
+
+
+ADJ_NEWTON = 30
+
+
+def run_adjoint(args, dev, stream, ws_world, rank):
+    """Differentiable BA: 64 windows of 10 keyframes and 2,000 landmarks; forward = 20 LM iterations + up to 30
+    trust-region Newton steps on the exact Hessian, loss = sum of squared translation errors against the ground truth, backward = the implicit adjoint
+    (gradients to fx, fy, cx, cy, baseline, left-right extrinsic, per-row weights and pixels)."""
+    import torch
+    from xclean_b200.backend import synth_ba as S
+    from xclean_b200.backend.adjoint import BAAdjoint, inputs_of
+    from xclean_b200.backend.ba import BatchSolver
+    wins = S.config3_windows(64, seed=3 + rank)
+    with torch.cuda.stream(stream):
+        solver = BatchSolver(wins, dev, hold=0)
+        ptrue = torch.as_tensor(np.concatenate([w.pwb_true for w in wins]), device=dev)
+    torch.cuda.synchronize()
+    fwd, bwd = [], []
+    with torch.cuda.stream(stream):
+        n_warm, n_timed = 1, min(2, args.steps)          # bounded: a step is seconds long
+        for it in range(n_warm + n_timed):
+            inp = inputs_of(solver)
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            ev[0].record(stream)
+            p = BAAdjoint.apply(*inp, solver, 20, ADJ_NEWTON)
+            ev[1].record(stream)
+            ((p - ptrue) ** 2).sum().backward()
+            ev[2].record(stream)
+            torch.cuda.synchronize()
+            if it >= n_warm:
+                fwd.append(ev[0].elapsed_time(ev[1]))
+                bwd.append(ev[1].elapsed_time(ev[2]))
+        st = solver.newton(0).cpu().numpy()
+    f_ms = D.max_over_ranks(float(np.mean(fwd)), device=dev)
+    b_ms = D.max_over_ranks(float(np.mean(bwd)), device=dev)
+    return {"value": ws_world * len(wins) / ((f_ms + b_ms) / 1e3), "unit": "windows/s (forward + backward)",
+            "ms_per_step": {"forward": f_ms, "backward": b_ms},
+            "windows_stationary": int(((st[:, 3] == 0) & (st[:, 2] < 1e-6)).sum()),
+            "final_gradient_max_median": float(np.median(st[:, 2])),
+            "config": {"workload": "64 windows x (10 keyframes, 2000 landmarks, 2-6 obs, 5%% outliers); forward 20 LM "
+                                   "iterations + up to %d trust-region Newton steps; implicit adjoint of "
+                                   "sum |t - t_gt|^2" % ADJ_NEWTON}}
 
 
 def cpu_baseline(L, R, args):

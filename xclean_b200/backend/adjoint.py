@@ -11,14 +11,15 @@ converged poses to de-rectifying it), weights [M] (the per-row weight 1/sigma in
 [M, 2] (observed pixels per row; the right rows use column 0).  Output: the converged body translations [slots, 3]
 (float64; the batch's slots in window order).
 
-Forward: `iters` LM iterations of window.solve (float64, batched, one launch), then `newton_steps` exact-Hessian
-Newton steps (window.solve alone converges only linearly where Huber weights are active, and the adjoint is exact
-only at a stationary point).  Backward: one solve H x = dL/dstate (H applied exactly through dual numbers, conjugate
-gradients preconditioned with the Gauss-Newton Cholesky factor, Jacobians recomputed from the state rather than
-stored), then dL/dtheta = -(d2C / dtheta dstate) x, scattered to the window parameters and to every observation row.
+Forward: `iters` LM iterations of window.solve (float64, batched, one launch), then at most `newton_steps`
+trust-region Newton steps on the exact Hessian (window.solve alone converges only linearly where Huber weights are
+active, can stall where its positive-depth rule rejects a landmark's step, and the adjoint is exact only at a
+stationary point).  Backward: one solve H x = dL/dstate (H applied exactly through dual numbers, conjugate gradients
+preconditioned with the Gauss-Newton Cholesky factor, Jacobians recomputed from the state rather than stored), then dL/dtheta = -(d2C / dtheta dstate) x, scattered to the window parameters and to every observation row.
 The solver keeps the converged state between forward and backward: do not reuse it for another forward before
-backward.  ctx.newton_stats / ctx.adjoint_stats keep the per-window status (2 = the state is not a strict minimum,
-e.g. an LM solve that stalled; its gradient is then not meaningful).
+backward.  ctx.newton_stats / ctx.adjoint_stats keep the per-window stats (column 2: the gradient max-norm at the
+returned state; a window that did not reach a stationary point within `newton_steps` has an approximate gradient).
+Landmarks that window.solve cannot move (its step would take the inverse depth to <= 1e-9) are constants.
 """
 from __future__ import annotations
 
@@ -27,7 +28,7 @@ import torch
 
 class BAAdjoint(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, intrinsics, baseline, extrinsic, weights, pixels, solver, iters=20, newton_steps=3,
+    def forward(ctx, intrinsics, baseline, extrinsic, weights, pixels, solver, iters=20, newton_steps=40,
                 lam0=1e-4, tol=1e-12):
         if float(extrinsic.detach().abs().max()) != 0.0:
             raise ValueError("BAAdjoint: the left-to-right extrinsic is the rectified rig (zero); only its gradient "

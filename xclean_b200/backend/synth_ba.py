@@ -177,6 +177,12 @@ def config2_windows(n=256, seed=1):
     return out
 
 
+def config3_windows(n=64, seed=3):
+    """Differentiable-BA batch: 10 keyframes, 2,000 landmarks seen by 2-6 keyframes, 1 px noise, 5 % outliers."""
+    return [make_window(None, K=10, L=2000, obs_min=2, obs_max=6, rng=np.random.default_rng([seed, i]))
+            for i in range(n)]
+
+
 def config4_windows(n=32, seed=4):
     """Large windows: 20 keyframes, 6,000 landmarks seen by 3-15 keyframes, 10 % outliers."""
     return [make_window(None, K=20, L=6000, obs_min=3, obs_max=15, outlier_frac=0.10, step_m=0.15,

@@ -53,7 +53,7 @@ static int ba_fail(int code, const char* msg)
 extern "C" size_t xcb_ba_newton_scratch_bytes(int nw, int Lt)
 {
     (void)nw;
-    return ((size_t)(Lt > 0 ? Lt : 1) * 18 * sizeof(double) + 255) / 256 * 256 + 256;
+    return ((size_t)(Lt > 0 ? Lt : 1) * 19 * sizeof(double) + 255) / 256 * 256 + 256;
 }
 
 extern "C" int xcb_ba_newton_windows_dev(const xcb_ba_windows* w, int max_slots, int mode, int steps, int maxit,
@@ -68,7 +68,7 @@ extern "C" int xcb_ba_newton_windows_dev(const xcb_ba_windows* w, int max_slots,
     if (mode == XCB_BA_NEWTON_ADJOINT && (!gpose || !gtheta)) return ba_fail(XCB_ERR_ARG, "ba_newton: adjoint outputs");
     if (steps < 0 || maxit < 1) return ba_fail(XCB_ERR_ARG, "ba_newton: steps / maxit");
     cudaStream_t st = (cudaStream_t)stream;
-    // scratch: [counter (256 B)][18 doubles per landmark]
+    // scratch: [counter (256 B)][19 doubles per landmark]
     int* counter = (int*)scratch;
     double* lsc = (double*)((char*)scratch + 256);
     (void)scratch_bytes;

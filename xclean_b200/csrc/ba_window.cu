@@ -899,8 +899,11 @@ __device__ __forceinline__ Dual fabs(Dual a) { return a.v < 0.0 ? -a : a; }
 #define NT_THETA 11             // fx, fy, cx, cy, B, omega (3), t (3)
 
 // per-landmark scratch of the exact solves (global memory): b (rhs), r (residual), p (direction, the dual pass's
-// tangent), x (solution), z (preconditioned residual), Hp
-#define NT_LM_STRIDE 18
+// tangent), x (solution), z (preconditioned residual), Hp, and the frozen flag: a landmark whose Gauss-Newton step
+// would take its inverse depth to <= 1e-9 is never moved by window.solve (apply_update's positive-depth rule), so the
+// state it converges to is stationary in every variable but those landmarks, which are constants here
+#define NT_LM_STRIDE 19
+#define NT_FROZEN 18
 #define NT_B 0
 #define NT_R 3
 #define NT_P 6
@@ -1013,7 +1016,7 @@ __device__ __forceinline__ int obs_theta(const BaWin& w, const SlotGeo<T>& G, co
 // Outputs: nt.gp / nt.hp (pose accumulators, atomics), per landmark: -gradient -> NT_B (GRAD), (H p)_l -> NT_HP (HV);
 // THETA: nt.th and the per-row outputs.  Landmarks that are not variables get zeros.
 __device__ void pass_dual(BaShared& sh, NtShared& nt, const XcbBaWindows& d, const SlotGeo<Dual>& G, int mode,
-                          double* lsc, double* gisig, double* gz)
+                          double* lsc, double* gisig, double* gz, double mu = 0.0)
 {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     for (int l = wid; l < sh.w.L; l += BA_WARPS) {
@@ -1029,6 +1032,7 @@ __device__ void pass_dual(BaShared& sh, NtShared& nt, const XcbBaWindows& d, con
                             Dual(d.lmp[3 * gl + 2], sc[NT_P + 2])};
         Dual gl3[3] = {Dual(0.0), Dual(0.0), Dual(0.0)}, gh[6];
         double hv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        double gnl[3] = {0.0, 0.0, 0.0}, gnh[6] = {0, 0, 0, 0, 0, 0};      // Gauss-Newton products w J^T (J p)
         int nobs = 0;
         for (int i = 0; i < 6; ++i) gh[i] = Dual(0.0);
         if (lane < nob) {
@@ -1041,8 +1045,10 @@ __device__ void pass_dual(BaShared& sh, NtShared& nt, const XcbBaWindows& d, con
                 Dual wt, cc;
                 huber_w<Dual>(en, Dual(sh.w.hk), &wt, &cc);
                 nobs = 1;
+                const double jp0 = ob[OB_E].e, jp1 = ob[OB_E + 1].e;             // J p (the dual part of e)
                 for (int i = 0; i < 3; ++i) {
                     gl3[i] = wt * (ob[OB_JL + i] * ob[OB_E] + ob[OB_JL + 3 + i] * ob[OB_E + 1]);
+                    gnl[i] = wt.v * (ob[OB_JL + i].v * jp0 + ob[OB_JL + 3 + i].v * jp1);
                     for (int j = 0; j < 3; ++j)
                         hv[i * 3 + j] = wt.v * (ob[OB_JL + i].v * ob[OB_JL + j].v + ob[OB_JL + 3 + i].v * ob[OB_JL + 3 + j].v);
                 }
@@ -1050,9 +1056,11 @@ __device__ void pass_dual(BaShared& sh, NtShared& nt, const XcbBaWindows& d, con
                     for (int i = 0; i < 6; ++i) {
                         const Dual gt = wt * (ob[OB_JT + i] * ob[OB_E] + ob[OB_JT + 6 + i] * ob[OB_E + 1]);
                         gh[i] = wt * (ob[OB_JH + i] * ob[OB_E] + ob[OB_JH + 6 + i] * ob[OB_E + 1]);
+                        gnh[i] = wt.v * (ob[OB_JH + i].v * jp0 + ob[OB_JH + 6 + i].v * jp1);
                         if (mode != NT_MODE_THETA) {
+                            const double gnt = wt.v * (ob[OB_JT + i].v * jp0 + ob[OB_JT + 6 + i].v * jp1);
                             atomicAdd(&nt.gp[6 * t + i], gt.v);
-                            atomicAdd(&nt.hp[6 * t + i], gt.e);
+                            atomicAdd(&nt.hp[6 * t + i], gt.e + mu * gnt);
                         }
                     }
                 }
@@ -1074,10 +1082,12 @@ __device__ void pass_dual(BaShared& sh, NtShared& nt, const XcbBaWindows& d, con
         for (int i = 0; i < 3; ++i) {
             gl3[i].v = warp_sum(gl3[i].v);
             gl3[i].e = warp_sum(gl3[i].e);
+            gnl[i] = warp_sum(gnl[i]);
         }
         for (int i = 0; i < 6; ++i) {
             gh[i].v = warp_sum(gh[i].v);
             gh[i].e = warp_sum(gh[i].e);
+            gnh[i] = warp_sum(gnh[i]);
         }
         if (d.rho_isig[gl] > 0.0) {
             const Dual ris = Dual(d.rho_isig[gl]);
@@ -1085,23 +1095,38 @@ __device__ void pass_dual(BaShared& sh, NtShared& nt, const XcbBaWindows& d, con
             Dual wt, cc;
             huber_w<Dual>(fabs(r0), Dual(sh.w.hk), &wt, &cc);
             gl3[2] = gl3[2] + wt * ris * r0;
+            gnl[2] += wt.v * ris.v * r0.e;
             hv[8] += wt.v * d.rho_isig[gl] * d.rho_isig[gl];
         }
         for (int i = 0; i < 3; ++i) hv[i * 4] += 1e-12;
         const double det = hv[0] * (hv[4] * hv[8] - hv[5] * hv[7]) - hv[1] * (hv[3] * hv[8] - hv[5] * hv[6]) +
                            hv[2] * (hv[3] * hv[7] - hv[4] * hv[6]);
         const double tr = hv[0] + hv[4] + hv[8];
-        const bool var = nobs > 0 && det > 1e-18 * tr * tr * tr && isfinite(det);
+        bool var = nobs > 0 && det > 1e-18 * tr * tr * tr && isfinite(det);
+        if (mode == NT_MODE_GRAD) {
+            bool frozen = false;
+            if (var) {      // the Gauss-Newton landmark step at this state, decoupled from the poses
+                const double id = 1.0 / det;
+                const double i2[3] = {(hv[3] * hv[7] - hv[4] * hv[6]) * id, (hv[1] * hv[6] - hv[0] * hv[7]) * id,
+                                      (hv[0] * hv[4] - hv[1] * hv[3]) * id};
+                const double step = -(i2[0] * gl3[0].v + i2[1] * gl3[1].v + i2[2] * gl3[2].v);
+                frozen = !(lm[2].v + step > 1e-9);
+            }
+            if (lane == 0) sc[NT_FROZEN] = frozen ? 1.0 : 0.0;
+            var = var && !frozen;
+        } else {
+            var = var && sc[NT_FROZEN] == 0.0;
+        }
         if (lane == 0) {
             if (mode != NT_MODE_THETA)
                 for (int i = 0; i < 6; ++i) {
                     atomicAdd(&nt.gp[6 * h + i], gh[i].v);
-                    atomicAdd(&nt.hp[6 * h + i], gh[i].e);
+                    atomicAdd(&nt.hp[6 * h + i], gh[i].e + mu * gnh[i]);
                 }
             if (mode == NT_MODE_GRAD)
                 for (int i = 0; i < 3; ++i) sc[NT_B + i] = var ? -gl3[i].v : 0.0;
             else if (mode == NT_MODE_HV)
-                for (int i = 0; i < 3; ++i) sc[NT_HP + i] = var ? gl3[i].e : 0.0;
+                for (int i = 0; i < 3; ++i) sc[NT_HP + i] = var ? gl3[i].e + mu * gnl[i] : 0.0;
         }
         __syncwarp();
     }
@@ -1122,7 +1147,7 @@ __device__ void pass_pre_a(BaShared& sh, const XcbBaWindows& d, WarpLm<double>* 
         double Hll[9], bl[3];
         int nt;
         const bool ok = lin_landmark<double>(sh, d, sh.g64, l, 0.0, d.lmp, wl, Hll, bl, &nt, &cdummy);
-        if (ok && nt) {
+        if (ok && nt && lsc[(size_t)gl * NT_LM_STRIDE + NT_FROZEN] == 0.0) {
             double Hi[9];
             inv3<double>(Hll, Hi);
             const double* r = lsc + (size_t)gl * NT_LM_STRIDE + NT_R;
@@ -1158,7 +1183,7 @@ __device__ void pass_pre_b(BaShared& sh, const XcbBaWindows& d, WarpLm<double>* 
         const bool ok = lin_landmark<double>(sh, d, sh.g64, l, 0.0, d.lmp, wl, Hll, bl, &nt, &cdummy);
         if (lane == 0) {
             double* sc = lsc + (size_t)gl * NT_LM_STRIDE;
-            if (!ok) {
+            if (!ok || sc[NT_FROZEN] != 0.0) {
                 sc[NT_Z] = sc[NT_Z + 1] = sc[NT_Z + 2] = 0.0;
             } else {
                 double Hi[9];
@@ -1239,11 +1264,32 @@ __device__ void nt_precond(BaShared& sh, const XcbBaWindows& d, double* S64, War
     pass_pre_b(sh, d, wl64, lsc);
 }
 
-// H x = b (b_p = sh.rhs, b_l = NT_B) by conjugate gradients preconditioned with the Gauss-Newton system (its factor
-// in S64).  -> x (sh.dmp, NT_X); the final relative residual; *iters_out the iterations; *neg set if a non-positive
+// (H + mu H_GN) x = b (b_p = sh.rhs, b_l = NT_B) by conjugate gradients preconditioned with the Gauss-Newton system
+// (its factor in S64; H_GN p comes from the same dual pass: the dual part of e is J p).  delta > 0: Steihaug's
+// truncated CG for the trust region |x|_M <= delta (M the Gauss-Newton preconditioner): a step that would leave the
+// region, or a direction of non-positive curvature, ends at its boundary (*boundary = 1).  -> x (sh.dmp, NT_X); the final relative residual; *iters_out the iterations; *neg set if a non-positive
 // curvature p^T H p was met (the state is not a strict minimum).
+__device__ void nt_axpy_p(BaShared& sh, double* lsc, double a)        // x += a p (poses sh.dmp / sh.dx, NT_X / NT_P)
+{
+    for (int q = threadIdx.x; q < sh.w.n; q += blockDim.x)
+        if (!held(sh, q)) sh.dmp[q] += a * sh.dx[q];
+    for (int l = threadIdx.x; l < sh.w.L; l += blockDim.x) {
+        double* sc = lsc + (size_t)(sh.w.lm0 + l) * NT_LM_STRIDE;
+        for (int i = 0; i < 3; ++i) sc[NT_X + i] += a * sc[NT_P + i];
+    }
+    __syncthreads();
+}
+
+// tau >= 0 with |x + tau p|_M = delta, from x^T M x, x^T M p, p^T M p
+__device__ __forceinline__ double nt_to_boundary(double xMx, double xMp, double pMp, double delta)
+{
+    const double disc = fmax(xMp * xMp + pMp * (delta * delta - xMx), 0.0);
+    return (-xMp + sqrt(disc)) / fmax(pMp, 1e-300);
+}
+
 __device__ double nt_solve_exact(BaShared& sh, NtShared& nt, const XcbBaWindows& d, double* S64, unsigned char* dsm,
-                                 double* lsc, int maxit, double tol, int* iters_out, int* neg)
+                                 double* lsc, int maxit, double tol, int* iters_out, int* neg, double mu = 0.0,
+                                 double delta = 0.0, int* boundary = nullptr, double* xMx_out = nullptr)
 {
     const int n = sh.w.n, tid = threadIdx.x;
     WarpLm<double>* wl64 = (WarpLm<double>*)(dsm + ba_off_x(n));
@@ -1256,7 +1302,8 @@ __device__ double nt_solve_exact(BaShared& sh, NtShared& nt, const XcbBaWindows&
     __syncthreads();
     const double bnorm = sqrt(nt_dot(sh, nt, sh.g, sh.g, lsc, NT_R, NT_R));
     *neg = 0;
-    double rel = 0.0;
+    if (boundary) *boundary = 0;
+    double rel = 0.0, pMp = 0.0, xMp = 0.0, xMx = 0.0;
     int it = 0;
     if (bnorm > 0.0) {
         nt_precond(sh, d, S64, wl64, lsc);
@@ -1267,16 +1314,29 @@ __device__ double nt_solve_exact(BaShared& sh, NtShared& nt, const XcbBaWindows&
         }
         __syncthreads();
         double rz = nt_dot(sh, nt, sh.g, sh.y, lsc, NT_R, NT_Z);
+        pMp = rz;                                       // M-norm terms of the iterates (CG recursions)
+        if (delta >= 1e100) delta = 10.0 * sqrt(fmax(rz, 0.0));   // unbounded: 10x the Gauss-Newton step's M-norm
         rel = 1.0;
         for (it = 0; it < maxit; ++it) {
             for (int q = tid; q < n; q += blockDim.x) { nt.gp[q] = 0.0; nt.hp[q] = 0.0; }
             __syncthreads();
             slot_geo_dual(sh, sh.dx, *Gd);
-            pass_dual(sh, nt, d, *Gd, NT_MODE_HV, lsc, nullptr, nullptr);
+            pass_dual(sh, nt, d, *Gd, NT_MODE_HV, lsc, nullptr, nullptr, mu);
             __syncthreads();
             const double pAp = nt_dot(sh, nt, sh.dx, nt.hp, lsc, NT_P, NT_HP);
+            if (delta > 0.0) {
+                const double a0 = pAp > 0.0 ? rz / pAp : 0.0;
+                if (!(pAp > 0.0) || xMx + 2.0 * a0 * xMp + a0 * a0 * pMp >= delta * delta) {
+                    nt_axpy_p(sh, lsc, nt_to_boundary(xMx, xMp, pMp, delta));
+                    xMx = delta * delta;
+                    if (boundary) *boundary = 1;
+                    ++it;
+                    break;
+                }
+            }
             if (!(pAp > 0.0)) { *neg = 1; break; }
             const double alpha = rz / pAp;
+            xMx += 2.0 * alpha * xMp + alpha * alpha * pMp;
             for (int q = tid; q < n; q += blockDim.x) {
                 if (held(sh, q)) continue;
                 sh.dmp[q] += alpha * sh.dx[q];
@@ -1296,6 +1356,8 @@ __device__ double nt_solve_exact(BaShared& sh, NtShared& nt, const XcbBaWindows&
             const double rz_new = nt_dot(sh, nt, sh.g, sh.y, lsc, NT_R, NT_Z);
             const double beta = rz_new / rz;
             rz = rz_new;
+            xMp = beta * (xMp + alpha * pMp);
+            pMp = rz_new + beta * beta * pMp;
             for (int q = tid; q < n; q += blockDim.x) sh.dx[q] = held(sh, q) ? 0.0 : sh.y[q] + beta * sh.dx[q];
             for (int l = tid; l < sh.w.L; l += blockDim.x) {
                 double* sc = lsc + (size_t)(sh.w.lm0 + l) * NT_LM_STRIDE;
@@ -1305,6 +1367,7 @@ __device__ double nt_solve_exact(BaShared& sh, NtShared& nt, const XcbBaWindows&
         }
     }
     *iters_out = it;
+    if (xMx_out) *xMx_out = xMx;
     return rel;
 }
 
@@ -1369,30 +1432,89 @@ __global__ void __launch_bounds__(BA_THREADS, 1) k_ba_newton(XcbBaWindows d, int
         int iters = 0, status = 0, neg = 0;
         double rel = 0.0, gmax = 0.0;
         if (mode == XCB_BA_NEWTON_POLISH) {
-            for (int st = 0; st < steps; ++st) {
-                slot_geo(sh, sh.Rwb, sh.pwb);
+            // Trust-region Newton on the exact Hessian: Steihaug's truncated CG in the Gauss-Newton metric, the step
+            // kept when the cost decreases by more than 1e-4 of the model's prediction (or the prediction is at
+            // rounding level: a converged state); the radius shrinks x4 on a poor step and doubles on a good step that
+            // reached it.  The first radius is unbounded, so a state in the Newton basin takes pure Newton steps.
+            // `steps` bounds the linear solves.
+            double delta = 1e300;
+            slot_geo(sh, sh.Rwb, sh.pwb);
+            pass_cost(sh, d, sh.g64, d.lmp);
+            double c0 = block_sum_red(sh);
+            bool last_ok = true;
+            int st = 0;
+            SlotGeo<Dual>* Gd = (SlotGeo<Dual>*)(dsm + ba_off_x(n));
+            while (st < steps) {
                 if (nt_gn_factor(sh, d, S64, wl64)) { status = 1; break; }
                 nt_grad(sh, nt, d, dsm, lsc);
-                rel = nt_solve_exact(sh, nt, d, S64, dsm, lsc, maxit, tol, &iters, &neg);
-                if (neg) { status = 2; break; }            // not in the basin of a strict minimum: no step
-                // apply the Newton step x: poses R <- R Exp(dphi), p <- p + dp; landmarks that are variables += x_l
-                for (int s = tid; s < P; s += blockDim.x) {
-                    if (sh.w.hold == s) continue;
-                    double Re[9], R[9];
-                    so3_exp(sh.dmp + 6 * s, Re);
-                    for (int i = 0; i < 9; ++i) R[i] = sh.Rwb[9 * s + i];
-                    for (int i = 0; i < 3; ++i)
-                        for (int j = 0; j < 3; ++j)
-                            sh.Rwb[9 * s + 3 * i + j] = R[3 * i] * Re[j] + R[3 * i + 1] * Re[3 + j] + R[3 * i + 2] * Re[6 + j];
-                    for (int i = 0; i < 3; ++i) sh.pwb[3 * s + i] += sh.dmp[6 * s + 3 + i];
+                bool moved = false;
+                while (st < steps && !moved) {
+                    ++st;
+                    int bnd = 0;
+                    double xMx = 0.0;
+                    rel = nt_solve_exact(sh, nt, d, S64, dsm, lsc, maxit, tol, &iters, &neg, 0.0, delta, &bnd, &xMx);
+                    // the model's decrease b.x - x.Hx / 2 (b = -gradient), H x from one more dual pass
+                    for (int q = tid; q < n; q += blockDim.x) { sh.dx[q] = sh.dmp[q]; nt.gp[q] = 0.0; nt.hp[q] = 0.0; }
+                    for (int l = tid; l < sh.w.L; l += blockDim.x) {
+                        double* sc = lsc + (size_t)(sh.w.lm0 + l) * NT_LM_STRIDE;
+                        for (int i = 0; i < 3; ++i) sc[NT_P + i] = sc[NT_X + i];
+                    }
+                    __syncthreads();
+                    slot_geo_dual(sh, sh.dx, *Gd);
+                    pass_dual(sh, nt, d, *Gd, NT_MODE_HV, lsc, nullptr, nullptr);
+                    __syncthreads();
+                    const double xHx = nt_dot(sh, nt, sh.dmp, nt.hp, lsc, NT_X, NT_HP);
+                    const double bx = nt_dot(sh, nt, sh.rhs, sh.dmp, lsc, NT_B, NT_X);
+                    const double pred = bx - 0.5 * xHx;
+                    // the trial state: poses R Exp(dphi), p + dp (held slot unchanged), landmarks + x_l
+                    for (int s = tid; s < P; s += blockDim.x) {
+                        double Re[9], R[9];
+                        for (int i = 0; i < 9; ++i) R[i] = sh.Rwb[9 * s + i];
+                        if (sh.w.hold == s) {
+                            for (int i = 0; i < 9; ++i) sh.R2[9 * s + i] = R[i];
+                            for (int i = 0; i < 3; ++i) sh.p2[3 * s + i] = sh.pwb[3 * s + i];
+                            continue;
+                        }
+                        so3_exp(sh.dmp + 6 * s, Re);
+                        for (int i = 0; i < 3; ++i)
+                            for (int j = 0; j < 3; ++j)
+                                sh.R2[9 * s + 3 * i + j] = R[3 * i] * Re[j] + R[3 * i + 1] * Re[3 + j] + R[3 * i + 2] * Re[6 + j];
+                        for (int i = 0; i < 3; ++i) sh.p2[3 * s + i] = sh.pwb[3 * s + i] + sh.dmp[6 * s + 3 + i];
+                    }
+                    for (int l = tid; l < sh.w.L; l += blockDim.x) {
+                        const int gl = sh.w.lm0 + l;
+                        const double* sc = lsc + (size_t)gl * NT_LM_STRIDE;
+                        for (int i = 0; i < 3; ++i) d.lmp[3 * gl + i] += sc[NT_X + i];
+                    }
+                    __syncthreads();
+                    slot_geo(sh, sh.R2, sh.p2);
+                    pass_cost(sh, d, sh.g64, d.lmp);
+                    const double c1 = block_sum_red(sh);
+                    const bool tiny = fabs(pred) <= 1e-13 * fabs(c0);
+                    const double ratio = pred > 0.0 ? (c0 - c1) / pred : -1.0;
+                    if ((tiny && c1 <= c0 + 1e-12 * fabs(c0)) || ratio > 1e-4) {
+                        for (int q = tid; q < P * 9; q += blockDim.x) sh.Rwb[q] = sh.R2[q];
+                        for (int q = tid; q < P * 3; q += blockDim.x) sh.pwb[q] = sh.p2[q];
+                        c0 = c1;
+                        moved = true;
+                        last_ok = true;
+                        if (ratio > 0.75 && bnd) delta *= 2.0;
+                        else if (ratio < 0.25 && !tiny) delta = 0.25 * sqrt(xMx);
+                    } else {
+                        for (int l = tid; l < sh.w.L; l += blockDim.x) {
+                            const int gl = sh.w.lm0 + l;
+                            const double* sc = lsc + (size_t)gl * NT_LM_STRIDE;
+                            for (int i = 0; i < 3; ++i) d.lmp[3 * gl + i] -= sc[NT_X + i];
+                        }
+                        delta = 0.25 * sqrt(xMx);
+                        last_ok = false;
+                    }
+                    __syncthreads();
+                    slot_geo(sh, sh.Rwb, sh.pwb);
+                    if (!(delta > 0.0)) { status = 2; st = steps; }
                 }
-                for (int l = tid; l < sh.w.L; l += blockDim.x) {
-                    const int gl = sh.w.lm0 + l;
-                    const double* sc = lsc + (size_t)gl * NT_LM_STRIDE;
-                    for (int i = 0; i < 3; ++i) d.lmp[3 * gl + i] += sc[NT_X + i];
-                }
-                __syncthreads();
             }
+            if (!last_ok && status == 0) status = 2;
             // the gradient at the final state
             slot_geo(sh, sh.Rwb, sh.pwb);
             nt_grad(sh, nt, d, dsm, lsc);
@@ -1413,9 +1535,10 @@ __global__ void __launch_bounds__(BA_THREADS, 1) k_ba_newton(XcbBaWindows d, int
             slot_geo(sh, sh.Rwb, sh.pwb);
             if (nt_gn_factor(sh, d, S64, wl64)) status = 1;
             else {
+                nt_grad(sh, nt, d, dsm, lsc);              // the frozen flags of this state
                 for (int q = tid; q < n; q += blockDim.x) sh.rhs[q] = held(sh, q) ? 0.0 : gpose[6 * (size_t)s0 + q];
                 for (int l = tid; l < sh.w.L; l += blockDim.x)
-                    for (int i = 0; i < NT_LM_STRIDE; ++i) lsc[(size_t)(sh.w.lm0 + l) * NT_LM_STRIDE + i] = 0.0;
+                    for (int i = 0; i < NT_FROZEN; ++i) lsc[(size_t)(sh.w.lm0 + l) * NT_LM_STRIDE + i] = 0.0;
                 __syncthreads();
                 rel = nt_solve_exact(sh, nt, d, S64, dsm, lsc, maxit, tol, &iters, &neg);
                 if (neg) status = 2;
