@@ -23,7 +23,7 @@
 #include "common.cuh"
 #include "ba_kernels.h"
 
-#define BA_WARPS 6
+#define BA_WARPS 10
 #define BA_THREADS (BA_WARPS * 32)
 #define BA_MAXP 20
 #define BA_MAXN (6 * BA_MAXP)
@@ -37,10 +37,26 @@ struct BaWin {
     double Rbc[9], pbc[3], Rcb[9], Px[9];
 };
 
+#define OB_E 0
+#define OB_W 2
+#define OB_JL 3
+#define OB_JT 9
+#define OB_JH 21
+#define OB_N 27
+
+// the pose Jacobian of a staged observation row group: row r, column i of the target (off = OB_JT) or host
+// (off = OB_JH) block; the host block's translation columns are minus the target block's
+template <typename T>
+__device__ __forceinline__ T obj(const T* ob, int off, int r, int i)
+{
+    if (off == OB_JT) return ob[OB_JT + 6 * r + i];
+    return i < 3 ? ob[OB_JH + 3 * r + i] : -ob[OB_JT + 6 * r + i];
+}
+
 // per-warp scratch for one landmark
 template <typename T>
 struct WarpLm {
-    T ob[BA_OBS][33];       // e0 e1 w | Jl[2][3] | Jt[2][6] | Jh[2][6]  (whitened)
+    T ob[BA_OBS][OB_N];     // e0 e1 w | Jl[2][3] | Jt[2][6] | Jh[2][0..2]  (whitened; Jh[r][3..5] = -Jt[r][3..5])
     T ux[BA_OBS][2];        // refinement: w (Jt dx_t + Jh dx_h)
     T Hlp[BA_MAXT][18];
     T Tb[BA_MAXT][18];
@@ -48,14 +64,7 @@ struct WarpLm {
     int obt[BA_OBS];        // target slot, -1 = not evaluable
     int ts[BA_MAXT];
     unsigned om[BA_MAXT];   // observations contributing to touched slot a
-    double acc[2 * BA_MAXN];
 };
-
-#define OB_E 0
-#define OB_W 2
-#define OB_JL 3
-#define OB_JT 9
-#define OB_JH 21
 
 // -------------------------------------------------------------------------------------------- small math
 template <typename T>
@@ -120,8 +129,12 @@ struct BaShared {
     int win;
 };
 
-// dynamic shared memory: [S64 n*n doubles][region: FP32 packed lower S + FP32 warp scratch | FP64 warp scratch]
-static __host__ __device__ __forceinline__ size_t ba_off_x(int n) { return ((size_t)n * n * 8 + 15) & ~(size_t)15; }
+// dynamic shared memory: [S64, packed lower, n(n+1)/2 doubles][region: FP32 packed lower S + FP32 warp scratch |
+// FP64 warp scratch]
+static __host__ __device__ __forceinline__ size_t ba_off_x(int n)
+{
+    return (((size_t)n * (n + 1) / 2) * 8 + 15) & ~(size_t)15;
+}
 static __host__ __device__ __forceinline__ size_t ba_s32_bytes(int n)
 {
     return (((size_t)n * (n + 1) / 2) * 4 + 15) & ~(size_t)15;
@@ -192,7 +205,7 @@ __device__ __forceinline__ int obs_lin(const BaWin& w, const SlotGeo<T>& G, cons
     }
     if (t == h) {
 #pragma unroll
-        for (int j = 0; j < 24; ++j) ob[OB_JT + j] = 0;
+        for (int j = 0; j < 18; ++j) ob[OB_JT + j] = 0;
         return 1;
     }
     // target: T1 = [q]x Rcb + rho R_ct Rwb_t Px ; host: T2 = -(RcR [m]x Rcb) - rho R_ct Rwb_h Px
@@ -220,11 +233,10 @@ __device__ __forceinline__ int obs_lin(const BaWin& w, const SlotGeo<T>& G, cons
                 t2[i] = -MR[i * 3 + j] - rho * rn;
             }
             ob[OB_JT + 6 * r + j] = Dp[r][0] * t1[0] + Dp[r][1] * t1[1] + Dp[r][2] * t1[2];
-            ob[OB_JH + 6 * r + j] = Dp[r][0] * t2[0] + Dp[r][1] * t2[1] + Dp[r][2] * t2[2];
+            ob[OB_JH + 3 * r + j] = Dp[r][0] * t2[0] + Dp[r][1] * t2[1] + Dp[r][2] * t2[2];
             // d q / d p (world): -rho R_ct, row j of Rwc_t
             T v = Dp[r][0] * Rt[3 * j] + Dp[r][1] * Rt[3 * j + 1] + Dp[r][2] * Rt[3 * j + 2];
             ob[OB_JT + 6 * r + 3 + j] = -rho * v;
-            ob[OB_JH + 6 * r + 3 + j] = rho * v;
         }
     return 1;
 }
@@ -311,7 +323,7 @@ __device__ __forceinline__ bool lin_landmark(BaShared& sh, const XcbBaWindows& d
         T acc = 0;
         for (unsigned m = wl.om[a]; m; m &= m - 1) {
             const T* ob = wl.ob[__ffs(m) - 1];
-            acc += ob[OB_W] * (ob[OB_JL + i] * ob[off + j] + ob[OB_JL + 3 + i] * ob[off + 6 + j]);
+            acc += ob[OB_W] * (ob[OB_JL + i] * obj(ob, off, 0, j) + ob[OB_JL + 3 + i] * obj(ob, off, 1, j));
         }
         wl.Hlp[a][e] = acc;
     }
@@ -394,7 +406,7 @@ __device__ void pass_build(BaShared& sh, const XcbBaWindows& d, const SlotGeo<T>
             T acc = 0;
             for (unsigned m = wl.om[a]; m; m &= m - 1) {
                 const T* ob = wl.ob[__ffs(m) - 1];
-                acc += ob[OB_W] * (ob[off + i] * ob[OB_E] + ob[off + 6 + i] * ob[OB_E + 1]);
+                acc += ob[OB_W] * (obj(ob, off, 0, i) * ob[OB_E] + obj(ob, off, 1, i) * ob[OB_E + 1]);
             }
             if (ok) acc -= wl.Hlp[a][i] * HiB[0] + wl.Hlp[a][6 + i] * HiB[1] + wl.Hlp[a][12 + i] * HiB[2];
             atomicAdd(&gb[6 * s + i], acc);
@@ -415,14 +427,14 @@ __device__ void pass_build(BaShared& sh, const XcbBaWindows& d, const SlotGeo<T>
                 const int off = sa == h ? OB_JH : OB_JT;
                 for (unsigned m = wl.om[a]; m; m &= m - 1) {
                     const T* ob = wl.ob[__ffs(m) - 1];
-                    acc += ob[OB_W] * (ob[off + i] * ob[off + j] + ob[off + 6 + i] * ob[off + 6 + j]);
+                    acc += ob[OB_W] * (obj(ob, off, 0, i) * obj(ob, off, 0, j) + obj(ob, off, 1, i) * obj(ob, off, 1, j));
                 }
             } else if (sa == h || sb == h) {
                 const int at = sa == h ? b : a;           // the target slot's index
                 const int offa = sa == h ? OB_JH : OB_JT, offb = sb == h ? OB_JH : OB_JT;
                 for (unsigned m = wl.om[at]; m; m &= m - 1) {
                     const T* ob = wl.ob[__ffs(m) - 1];
-                    acc += ob[OB_W] * (ob[offa + i] * ob[offb + j] + ob[offa + 6 + i] * ob[offb + 6 + j]);
+                    acc += ob[OB_W] * (obj(ob, offa, 0, i) * obj(ob, offb, 0, j) + obj(ob, offa, 1, i) * obj(ob, offb, 1, j));
                 }
             }
             if (ok) acc -= wl.Hlp[a][i] * wl.Tb[b][j] + wl.Hlp[a][6 + i] * wl.Tb[b][6 + j] + wl.Hlp[a][12 + i] * wl.Tb[b][12 + j];
@@ -443,10 +455,11 @@ __device__ void pass_refine(BaShared& sh, const XcbBaWindows& d, WarpLm<double>*
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int n = sh.w.n;
     WarpLm<double>& wl = wls[wid];
-    double* gacc = wl.acc;
-    double* yacc = wl.acc + BA_MAXN;
-    for (int q = lane; q < 2 * BA_MAXN; q += 32) wl.acc[q] = 0.0;
-    __syncwarp();
+    for (int q = threadIdx.x; q < n; q += blockDim.x) {
+        if (want_g) sh.g[q] = 0.0;
+        sh.y[q] = 0.0;
+    }
+    __syncthreads();
     double c_local = 0.0;
     for (int l = wid; l < sh.w.L; l += BA_WARPS) {
         const int gl = sh.w.lm0 + l;
@@ -465,7 +478,7 @@ __device__ void pass_refine(BaShared& sh, const XcbBaWindows& d, WarpLm<double>*
             for (int r = 0; r < 2; ++r) {
                 double a = 0.0;
 #pragma unroll
-                for (int j = 0; j < 6; ++j) a += ob[OB_JT + 6 * r + j] * sh.dx[6 * t + j] + ob[OB_JH + 6 * r + j] * sh.dx[6 * h + j];
+                for (int j = 0; j < 6; ++j) a += ob[OB_JT + 6 * r + j] * sh.dx[6 * t + j] + obj(ob, OB_JH, r, j) * sh.dx[6 * h + j];
                 wl.ux[lane][r] = ob[OB_W] * a;
             }
         }
@@ -494,27 +507,20 @@ __device__ void pass_refine(BaShared& sh, const XcbBaWindows& d, WarpLm<double>*
             for (unsigned m = wl.om[a]; m; m &= m - 1) {
                 const int k = __ffs(m) - 1;
                 const double* ob = wl.ob[k];
-                ga += ob[OB_W] * (ob[off + i] * ob[OB_E] + ob[off + 6 + i] * ob[OB_E + 1]);
-                ya += ob[off + i] * wl.ux[k][0] + ob[off + 6 + i] * wl.ux[k][1];
+                ga += ob[OB_W] * (obj(ob, off, 0, i) * ob[OB_E] + obj(ob, off, 1, i) * ob[OB_E + 1]);
+                ya += obj(ob, off, 0, i) * wl.ux[k][0] + obj(ob, off, 1, i) * wl.ux[k][1];
             }
             if (ok) {
                 ga -= wl.Hlp[a][i] * HiB[0] + wl.Hlp[a][6 + i] * HiB[1] + wl.Hlp[a][12 + i] * HiB[2];
                 ya -= wl.Hlp[a][i] * u[0] + wl.Hlp[a][6 + i] * u[1] + wl.Hlp[a][12 + i] * u[2];
             }
-            gacc[6 * s + i] += ga;
-            yacc[6 * s + i] += ya;
+            if (want_g) atomicAdd(&sh.g[6 * s + i], ga);
+            atomicAdd(&sh.y[6 * s + i], ya);
         }
         __syncwarp();
     }
     c_local = warp_sum(c_local);
     if (lane == 0) sh.red[wid] = c_local;
-    __syncthreads();
-    for (int q = threadIdx.x; q < n; q += blockDim.x) {
-        double gs = 0.0, ys = 0.0;
-        for (int k = 0; k < BA_WARPS; ++k) { gs += wls[k].acc[q]; ys += wls[k].acc[BA_MAXN + q]; }
-        if (want_g) sh.g[q] = gs;
-        sh.y[q] = ys;
-    }
     __syncthreads();
 }
 
@@ -571,7 +577,7 @@ __device__ void pass_cost(BaShared& sh, const XcbBaWindows& d, const SlotGeo<dou
         const double lm[3] = {lmp[3 * gl], lmp[3 * gl + 1], lmp[3 * gl + 2]};
         for (int k = d.lm_ob[gl] + lane; k < d.lm_ob[gl + 1]; k += 32) {
             if (!d.ob_valid[k] || (unsigned)d.ob_pose[k] >= (unsigned)sh.w.P) continue;
-            double ob[33];
+            double ob[OB_N];
             if (!obs_lin<double>(sh.w, G, lm, h, d.ob_pose[k], d.ob_cam[k], d.ob_z + 2 * k, d.ob_isig[k], ob, false)) {
                 c += 1e6;
                 continue;
@@ -599,18 +605,19 @@ __device__ int chol_factor(double* S, int n)
     __syncthreads();
     for (int j = 0; j < n; ++j) {
         if (threadIdx.x == 0) {
-            double dj = S[j * n + j];
+            double dj = S[tri(j, j)];
             if (!(dj > 0.0) || !isfinite(dj)) { bad = 1; dj = 1.0; }
-            S[j * n + j] = sqrt(dj);
+            S[tri(j, j)] = sqrt(dj);
         }
         __syncthreads();
-        const double dj = S[j * n + j];
-        for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) S[i * n + j] /= dj;
+        const double dj = S[tri(j, j)];
+        for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) S[tri(i, j)] /= dj;
         __syncthreads();
         // trailing update of the lower triangle: row i, columns j+1..i
         for (int i = j + 1 + threadIdx.x / 32; i < n; i += blockDim.x / 32) {
-            const double lij = S[i * n + j];
-            for (int c = j + 1 + (threadIdx.x & 31); c <= i; c += 32) S[i * n + c] -= lij * S[c * n + j];
+            double* row = S + tri(i, 0);
+            const double lij = row[j];
+            for (int c = j + 1 + (threadIdx.x & 31); c <= i; c += 32) row[c] -= lij * S[tri(c, j)];
         }
         __syncthreads();
     }
@@ -621,17 +628,18 @@ __device__ int chol_factor(double* S, int n)
 __device__ void chol_solve(const double* Lc, int n, double* x)
 {
     for (int j = 0; j < n; ++j) {
-        if (threadIdx.x == 0) x[j] /= Lc[j * n + j];
+        if (threadIdx.x == 0) x[j] /= Lc[tri(j, j)];
         __syncthreads();
         const double xj = x[j];
-        for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) x[i] -= Lc[i * n + j] * xj;
+        for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) x[i] -= Lc[tri(i, j)] * xj;
         __syncthreads();
     }
     for (int j = n - 1; j >= 0; --j) {
-        if (threadIdx.x == 0) x[j] /= Lc[j * n + j];
+        if (threadIdx.x == 0) x[j] /= Lc[tri(j, j)];
         __syncthreads();
         const double xj = x[j];
-        for (int i = threadIdx.x; i < j; i += blockDim.x) x[i] -= Lc[j * n + i] * xj;
+        const double* row = Lc + tri(j, 0);
+        for (int i = threadIdx.x; i < j; i += blockDim.x) x[i] -= row[i] * xj;
         __syncthreads();
     }
 }
@@ -737,15 +745,12 @@ __global__ void __launch_bounds__(BA_THREADS, 1) k_ba_windows(XcbBaWindows d, in
                 __syncthreads();
                 pass_build<float, true>(sh, d, sh.g32, S32, sh.bf, wl32, nullptr);
                 __syncthreads();
-                for (int q = tid; q < n * n; q += blockDim.x) {
-                    const int i = q / n, j = q % n;
-                    S64[q] = j <= i ? (double)S32[tri(i, j)] : 0.0;
-                }
+                for (int q = tid; q < n * (n + 1) / 2; q += blockDim.x) S64[q] = (double)S32[q];
                 for (int q = tid; q < n; q += blockDim.x) sh.rhs[q] = (double)sh.bf[q];
             } else {
-                for (int q = tid; q < n * n; q += blockDim.x) S64[q] = 0.0;
+                for (int q = tid; q < n * (n + 1) / 2; q += blockDim.x) S64[q] = 0.0;
                 __syncthreads();
-                pass_build<double, false>(sh, d, sh.g64, S64, sh.g, wl64, &c_tot);
+                pass_build<double, true>(sh, d, sh.g64, S64, sh.g, wl64, &c_tot);
                 c_tot = block_sum_red(sh);
                 for (int q = tid; q < n; q += blockDim.x) sh.rhs[q] = sh.g[q];
             }
@@ -755,17 +760,16 @@ __global__ void __launch_bounds__(BA_THREADS, 1) k_ba_windows(XcbBaWindows d, in
             if (hs >= 0 && hs < P) {
                 for (int q = tid; q < 6 * n; q += blockDim.x) {
                     const int i = 6 * hs + q / n, j = q % n;
-                    S64[i * n + j] = 0.0;
-                    S64[j * n + i] = 0.0;
+                    S64[i >= j ? tri(i, j) : tri(j, i)] = 0.0;
                 }
                 __syncthreads();
-                for (int q = tid; q < 6; q += blockDim.x) { S64[(6 * hs + q) * n + 6 * hs + q] = 1.0; sh.rhs[6 * hs + q] = 0.0; }
+                for (int q = tid; q < 6; q += blockDim.x) { S64[tri(6 * hs + q, 6 * hs + q)] = 1.0; sh.rhs[6 * hs + q] = 0.0; }
                 __syncthreads();
             }
             for (int q = tid; q < n; q += blockDim.x) {
-                const double dg = S64[q * n + q];
+                const double dg = S64[tri(q, q)];
                 sh.dmp[q] = sh.lam * dg + 1e-9;
-                S64[q * n + q] = dg + sh.dmp[q];
+                S64[tri(q, q)] = dg + sh.dmp[q];
                 sh.dx[q] = -sh.rhs[q];
             }
             __syncthreads();
@@ -1038,7 +1042,7 @@ __device__ void pass_dual(BaShared& sh, NtShared& nt, const XcbBaWindows& d, con
         if (lane < nob) {
             const int k = k0 + lane;
             const int t = d.ob_pose[k];
-            Dual ob[33];
+            Dual ob[OB_N];
             if (d.ob_valid[k] && (unsigned)t < (unsigned)sh.w.P &&
                 obs_lin<Dual>(sh.w, G, lm, h, t, d.ob_cam[k], d.ob_z + 2 * k, Dual(d.ob_isig[k]), ob, true)) {
                 const Dual en = sqrt(ob[OB_E] * ob[OB_E] + ob[OB_E + 1] * ob[OB_E + 1]);
@@ -1055,8 +1059,9 @@ __device__ void pass_dual(BaShared& sh, NtShared& nt, const XcbBaWindows& d, con
                 if (t != h) {
                     for (int i = 0; i < 6; ++i) {
                         const Dual gt = wt * (ob[OB_JT + i] * ob[OB_E] + ob[OB_JT + 6 + i] * ob[OB_E + 1]);
-                        gh[i] = wt * (ob[OB_JH + i] * ob[OB_E] + ob[OB_JH + 6 + i] * ob[OB_E + 1]);
-                        gnh[i] = wt.v * (ob[OB_JH + i].v * jp0 + ob[OB_JH + 6 + i].v * jp1);
+                        const Dual jh0 = obj(ob, OB_JH, 0, i), jh1 = obj(ob, OB_JH, 1, i);
+                        gh[i] = wt * (jh0 * ob[OB_E] + jh1 * ob[OB_E + 1]);
+                        gnh[i] = wt.v * (jh0.v * jp0 + jh1.v * jp1);
                         if (mode != NT_MODE_THETA) {
                             const double gnt = wt.v * (ob[OB_JT + i].v * jp0 + ob[OB_JT + 6 + i].v * jp1);
                             atomicAdd(&nt.gp[6 * t + i], gt.v);
@@ -1138,8 +1143,8 @@ __device__ void pass_pre_a(BaShared& sh, const XcbBaWindows& d, WarpLm<double>* 
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int n = sh.w.n;
     WarpLm<double>& wl = wls[wid];
-    for (int q = lane; q < BA_MAXN; q += 32) wl.acc[q] = 0.0;
-    __syncwarp();
+    for (int q = threadIdx.x; q < n; q += blockDim.x) sh.y[q] = sh.g[q];
+    __syncthreads();
     double cdummy = 0.0;
     for (int l = wid; l < sh.w.L; l += BA_WARPS) {
         const int gl = sh.w.lm0 + l;
@@ -1155,16 +1160,11 @@ __device__ void pass_pre_a(BaShared& sh, const XcbBaWindows& d, WarpLm<double>* 
             for (int i = 0; i < 3; ++i) u[i] = Hi[i * 3] * r[0] + Hi[i * 3 + 1] * r[1] + Hi[i * 3 + 2] * r[2];
             for (int q = lane; q < nt * 6; q += 32) {
                 const int a = q / 6, j = q % 6;
-                wl.acc[6 * wl.ts[a] + j] -= wl.Hlp[a][j] * u[0] + wl.Hlp[a][6 + j] * u[1] + wl.Hlp[a][12 + j] * u[2];
+                atomicAdd(&sh.y[6 * wl.ts[a] + j],
+                          -(wl.Hlp[a][j] * u[0] + wl.Hlp[a][6 + j] * u[1] + wl.Hlp[a][12 + j] * u[2]));
             }
         }
         __syncwarp();
-    }
-    __syncthreads();
-    for (int q = threadIdx.x; q < n; q += blockDim.x) {
-        double s = sh.g[q];
-        for (int k = 0; k < BA_WARPS; ++k) s += wls[k].acc[q];
-        sh.y[q] = s;
     }
     __syncthreads();
 }
@@ -1211,23 +1211,22 @@ __device__ int nt_gn_factor(BaShared& sh, const XcbBaWindows& d, double* S64, Wa
 {
     const int n = sh.w.n, tid = threadIdx.x;
     if (tid == 0) sh.lam = 0.0;
-    for (int q = tid; q < n * n; q += blockDim.x) S64[q] = 0.0;
+    for (int q = tid; q < n * (n + 1) / 2; q += blockDim.x) S64[q] = 0.0;
     for (int q = tid; q < n; q += blockDim.x) sh.y[q] = 0.0;
     __syncthreads();
-    pass_build<double, false>(sh, d, sh.g64, S64, sh.y, wl64, nullptr);
+    pass_build<double, true>(sh, d, sh.g64, S64, sh.y, wl64, nullptr);
     __syncthreads();
     const int hs = sh.w.hold;
     if (hs >= 0 && hs < sh.w.P) {
         for (int q = tid; q < 6 * n; q += blockDim.x) {
             const int i = 6 * hs + q / n, j = q % n;
-            S64[i * n + j] = 0.0;
-            S64[j * n + i] = 0.0;
+            S64[i >= j ? tri(i, j) : tri(j, i)] = 0.0;
         }
         __syncthreads();
-        for (int q = tid; q < 6; q += blockDim.x) S64[(6 * hs + q) * n + 6 * hs + q] = 1.0;
+        for (int q = tid; q < 6; q += blockDim.x) S64[tri(6 * hs + q, 6 * hs + q)] = 1.0;
         __syncthreads();
     }
-    for (int q = tid; q < n; q += blockDim.x) S64[q * n + q] += 1e-9;
+    for (int q = tid; q < n; q += blockDim.x) S64[tri(q, q)] += 1e-9;
     __syncthreads();
     return chol_factor(S64, n);
 }
