@@ -25,7 +25,8 @@ static __host__ __device__ __forceinline__ int win_w(int half) { return ((MAXD +
 #define LK_TERMS 9      // the LK's sums except sum(1 * 1) = NPIX, which is exact
 
 // per-warp shared memory: Td [NPIX] f64 | T2d [NPIX] f64 | sc [MAXD] f64 | jb [MAXD] i8 | U, where U holds the image
-// window (float32, rows x win_w) during the two searches and the LK term table (LK_TERMS x NPIX f64) afterwards
+// window (float32 rows of win_w, or u8 rows of U8Win::WWB) during the two searches, then the LK term table
+// (LK_TERMS x NPIX f64) and the LK's staged right-image block ((PW + 2) x (PW + 10) f64)
 static __host__ __device__ __forceinline__ size_t stereo_off_u(int half)
 {
     int pw = 2 * half + 1, npix = pw * pw;
@@ -36,7 +37,7 @@ static __host__ __device__ __forceinline__ size_t stereo_warp_bytes(int half, in
 {
     int pw = 2 * half + 1, npix = pw * pw;
     size_t win = (size_t)(pw + 2 * band) * win_w(half) * 4;
-    size_t terms = (size_t)LK_TERMS * npix * 8;
+    size_t terms = (size_t)LK_TERMS * npix * 8 + (size_t)(pw + 2) * (pw + 2 * 4 + 2) * 8;   // + the LK's staged block
     return (stereo_off_u(half) + (win > terms ? win : terms) + 15) & ~(size_t)15;
 }
 
@@ -251,6 +252,103 @@ __device__ __forceinline__ void zncc_q(const float* win, int ww, int row0, const
     }
 }
 
+// u8 image windows (the unshifted right image in the search, the left image in the left-right check): each lane scores
+// four ADJACENT patches (top-left columns cb .. cb + 3), so one row of PW + 3 bytes, read as aligned 32-bit words,
+// feeds 4 x PW products.  Pixel sums and sums of squares are exact integers (dp4a over whole words, then a sliding
+// update per patch); the cross term keeps the CPU's sequential float64 order per patch.
+template <int HALF>
+struct U8Win {
+    static constexpr int PW = 2 * HALF + 1;
+    static constexpr int NV = PW + 3;                 // bytes a lane reads per row
+    static constexpr int NWD = (NV + 3) / 4;          // ... as 32-bit words
+    static constexpr int PAD = 8;                     // left pad bytes: 4 + the alignment shift (0..3)
+    static constexpr int WWB = (MAXD + 4 * NWD + PAD + 3) & ~3;    // row stride in bytes
+};
+
+// z[k] = ZNCC of the patch whose top-left is byte `p` + k (rows WWB bytes apart); p is 4-byte aligned
+template <int HALF>
+__device__ __forceinline__ void zncc4_u8(const unsigned char* p, const double* T, double ts, double z[4])
+{
+    using G = U8Win<HALF>;
+    constexpr int PW = G::PW, NPIX = PW * PW, NV = G::NV, NWD = G::NWD;
+    double sx[4] = {0.0, 0.0, 0.0, 0.0};
+    unsigned S[4] = {0u, 0u, 0u, 0u}, SQ[4] = {0u, 0u, 0u, 0u};
+#pragma unroll 1
+    for (int dy = 0; dy < PW; ++dy) {
+        const unsigned* rp = (const unsigned*)(p + dy * G::WWB);
+        unsigned w[NWD];
+#pragma unroll
+        for (int i = 0; i < NWD; ++i) w[i] = rp[i];
+        unsigned b[NV];
+#pragma unroll
+        for (int i = 0; i < NV; ++i) b[i] = (w[i >> 2] >> (8 * (i & 3))) & 0xffu;
+        unsigned s = 0u, sq = 0u;
+#pragma unroll
+        for (int i = 0; i < PW / 4; ++i) { s = __dp4a(w[i], 0x01010101u, s); sq = __dp4a(w[i], w[i], sq); }
+#pragma unroll
+        for (int i = (PW / 4) * 4; i < PW; ++i) { s += b[i]; sq += b[i] * b[i]; }
+        S[0] += s; SQ[0] += sq;
+#pragma unroll
+        for (int k = 1; k < 4; ++k) {
+            s += b[k - 1 + PW] - b[k - 1];
+            sq += b[k - 1 + PW] * b[k - 1 + PW] - b[k - 1] * b[k - 1];
+            S[k] += s; SQ[k] += sq;
+        }
+        double v[NV];
+#pragma unroll
+        for (int i = 0; i < NV; ++i) v[i] = (double)b[i];
+        const double* Tr = T + dy * PW;
+#pragma unroll
+        for (int dx = 0; dx < PW; ++dx) {
+            const double tk = Tr[dx];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) sx[k] = __dadd_rn(sx[k], __dmul_rn(v[k + dx], tk));
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) z[k] = zncc_finish((double)S[k], (double)SQ[k], sx[k], ts, NPIX);
+}
+
+// stage image rows r0 .. r0 + nrows - 1, columns c0 .. c0 + ncols - 1 of a u8 image into WWB-byte rows (column c at
+// byte pad + c, zero bytes around it).  Each shared-memory word comes from two aligned 32-bit global words joined by a
+// funnel shift, eight words per lane in flight.  The aligned words reach at most 6 bytes before column c0 and 7 bytes
+// after the last column, i.e. into the rows just above and below the window: callers keep a row of the frame on either
+// side of every window (and column c0 >= 2).
+template <int HALF>
+__device__ __forceinline__ void stage_u8(unsigned char* wb, const u8* __restrict__ img, int W, int r0, int nrows, int c0,
+                                         int ncols, int pad, int lane)
+{
+    constexpr int NWW = U8Win<HALF>::WWB / 4;
+    constexpr int UB = 8;
+    unsigned* ws = (unsigned*)wb;
+    const int total = nrows * NWW;
+    for (int i0 = 0; i0 < total; i0 += 32 * UB) {
+        unsigned lo[UB], hi[UB], msk[UB];
+        int sh[UB];
+#pragma unroll
+        for (int u = 0; u < UB; ++u) {
+            const int idx = i0 + 32 * u + lane;
+            const int rr = idx / NWW, m = idx - rr * NWW;
+            const int c = 4 * m - pad;                       // column of the word's first byte
+            lo[u] = 0u; hi[u] = 0u; sh[u] = 0; msk[u] = 0u;
+            if (idx < total && c + 3 >= 0 && c < ncols) {
+                const size_t ga = (size_t)(img + (size_t)(r0 + rr) * W + c0) + (size_t)(ptrdiff_t)c;
+                const unsigned* a4 = (const unsigned*)(ga & ~(size_t)3);
+                sh[u] = (int)(ga & 3) * 8;
+                lo[u] = __ldg(a4);
+                hi[u] = __ldg(a4 + 1);
+                msk[u] = (c >= 0 ? 0xffffffffu : (0xffffffffu << (8 * -c))) &
+                         (c + 4 <= ncols ? 0xffffffffu : (0xffffffffu >> (8 * (c + 4 - ncols))));
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < UB; ++u) {
+            const int idx = i0 + 32 * u + lane;
+            if (idx < total) ws[idx] = __funnelshift_r(lo[u], hi[u], sh[u]) & msk[u];
+        }
+    }
+}
+
 // warp argmax, first maximum in increasing index (strict '>' scan): ties keep the smaller index
 __device__ __forceinline__ void warp_argmax(double& v, int& idx)
 {
@@ -272,6 +370,7 @@ __global__ void __launch_bounds__(ST_WARPS * 32, 5) k_stereo(
     double* __restrict__ ody)
 {
     constexpr int PW = 2 * HALF + 1, NPIX = PW * PW;
+    static_assert(U8Win<HALF>::WWB <= 4 * (((MAXD + 2 * HALF) + 3) & ~3), "u8 rows fit the float32 window rows");
     const double ZMIN = 0.5, UNIQ1 = 1.0 + 0.05, LRT = 1.0;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -282,6 +381,7 @@ __global__ void __launch_bounds__(ST_WARPS * 32, 5) k_stereo(
     double* sc = T2d + NPIX;
     signed char* jb = (signed char*)(sc + MAXD);
     float* win = (float*)(base + stereo_off_u(HALF));
+    unsigned char* winb = base + stereo_off_u(HALF);          // the u8 windows (U8Win row stride)
     double* terms = (double*)(base + stereo_off_u(HALF));     // the LK term table, after the searches
 
     const long long p = (long long)blockIdx.x * ST_WARPS + wid;
@@ -316,44 +416,48 @@ __global__ void __launch_bounds__(ST_WARPS * 32, 5) k_stereo(
     if (hi < lo) return;
 
     // template statistics (_patch_stats on u8: integer sums, exact) and T - mean
-    int s = 0, s2 = 0;
-    for (int k = lane; k < NPIX; k += 32) {
-        int t = L[(size_t)(vi + k / PW - HALF) * W + ui + k % PW - HALF];
-        s += t; s2 += t * t;
+    constexpr int KP = (NPIX + 31) / 32;      // patch pixels per lane
+    int tv[KP];
+#pragma unroll
+    for (int i = 0; i < KP; ++i) {
+        const int k = lane + 32 * i;
+        tv[i] = k < NPIX ? (int)L[(size_t)(vi + k / PW - HALF) * W + ui + k % PW - HALF] : 0;
     }
+    int s = 0, s2 = 0;
+#pragma unroll
+    for (int i = 0; i < KP; ++i) { s += tv[i]; s2 += tv[i] * tv[i]; }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) { s += __shfl_xor_sync(0xffffffffu, s, o); s2 += __shfl_xor_sync(0xffffffffu, s2, o); }
     const double tm = __ddiv_rn((double)s, (double)NPIX);
     const double tvar = __dsub_rn(__ddiv_rn((double)s2, (double)NPIX), __dmul_rn(tm, tm));
     const double ts = __dsqrt_rn(tvar > 0.0 ? tvar : 0.0);
     if (ts <= 1e-6) return;
-    for (int k = lane; k < NPIX; k += 32)
-        Td[k] = __dsub_rn((double)L[(size_t)(vi + k / PW - HALF) * W + ui + k % PW - HALF], tm);
+#pragma unroll
+    for (int i = 0; i < KP; ++i)
+        if (lane + 32 * i < NPIX) Td[lane + 32 * i] = __dsub_rn((double)tv[i], tm);
 
-    // right-image window: rows vi-band-HALF .. vi+band+HALF, columns ui-hi-HALF .. ui-lo+HALF
+    // right-image window: rows vi-band-HALF .. vi+band+HALF, columns ui-hi-HALF .. ui-lo+HALF (window column = hi - d)
     const int wr0 = vi - band - HALF, wc0 = ui - (int)hi - HALF;
-    const int nrows = PW + 2 * band, ncols = (int)(hi - lo) + PW;
-    for (int idx = lane; idx < nrows * ncols; idx += 32) {
-        int rr = idx / ncols, cc = idx % ncols;
-        win[rr * ww + cc] = R.at((size_t)(wr0 + rr) * W + wc0 + cc);
-    }
-    __syncwarp();
-
-    // ZNCC over d in [lo, hi] (best row of the band), four disparities per lane
+    const int nrows = PW + 2 * band, span = (int)(hi - lo), ncols = span + PW;
     double lbest = -2.0;
     int lbd = -1;
-#pragma unroll 1
-    for (int q0 = 0; q0 < 4; q0 += 4) {
-        int dq[4], col[4];
-        bool val[4];
+    double best[4];
+    int bj[4] = {0, 0, 0, 0}, dq[4];
+    bool val[4];
+    if (FLT) {
+        // shifted float32 right image: disparities lo + lane + 32 q
+        for (int idx = lane; idx < nrows * ncols; idx += 32) {
+            int rr = idx / ncols, cc = idx % ncols;
+            win[rr * ww + cc] = R.at((size_t)(wr0 + rr) * W + wc0 + cc);
+        }
+        __syncwarp();
+        int col[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             dq[q] = (int)lo + lane + 32 * q;
             val[q] = dq[q] <= hi;
             col[q] = (int)hi - dq[q];
         }
-        double best[4];
-        int bj[4] = {0, 0, 0, 0};
         // rows in the CPU's order: vi, then vi - j, vi + j for j = 1..band; a later row wins only if strictly better
 #pragma unroll 1
         for (int t = 0; t <= 2 * band; ++t) {
@@ -364,13 +468,38 @@ __global__ void __launch_bounds__(ST_WARPS * 32, 5) k_stereo(
             for (int q = 0; q < 4; ++q)
                 if (t == 0 || z[q] > best[q]) { best[q] = z[q]; bj[q] = j; }
         }
+    } else {
+        // u8 right image: lane's disparities lo + 4 lane + q (q = 0..3) are window columns span - 4 lane - q, a block of
+        // four adjacent patches starting at column cb = span - 4 lane - 3.  The pad makes every block start on a 32-bit
+        // word; a lane whose four disparities all exceed hi starts at the lowest column >= -3 of the same residue
+        // mod 4 (pad bytes, results unused).
+        const int pad = 4 + ((3 - span) & 3);
+        stage_u8<HALF>(winb, R.r8, W, wr0, nrows, wc0, ncols, pad, lane);
+        __syncwarp();
+        int cb = span - 4 * lane - 3;
+        if (cb < -3) cb += (-cb) & ~3;
+        const unsigned char* pb = winb + pad + cb;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            if (val[q]) {
-                sc[dq[q]] = best[q];
-                jb[dq[q]] = (signed char)bj[q];
-                if (best[q] > lbest) { lbest = best[q]; lbd = dq[q]; }
-            }
+            dq[q] = (int)lo + 4 * lane + q;
+            val[q] = dq[q] <= hi;
+        }
+#pragma unroll 1
+        for (int t = 0; t <= 2 * band; ++t) {
+            const int j = t == 0 ? 0 : ((t & 1) ? -((t + 1) >> 1) : (t >> 1));
+            double z[4];
+            zncc4_u8<HALF>(pb + (band + j) * U8Win<HALF>::WWB, Td, ts, z);
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (t == 0 || z[3 - q] > best[q]) { best[q] = z[3 - q]; bj[q] = j; }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        if (val[q]) {
+            sc[dq[q]] = best[q];
+            jb[dq[q]] = (signed char)bj[q];
+            if (best[q] > lbest) { lbest = best[q]; lbd = dq[q]; }
         }
     }
     double bs = lbest;
@@ -390,6 +519,12 @@ __global__ void __launch_bounds__(ST_WARPS * 32, 5) k_stereo(
     const int js = jb[bestd];
     const int xr = ui - bestd;
     double rm, rsd;
+    float rv[KP];
+#pragma unroll
+    for (int i = 0; i < KP; ++i) {
+        const int k = lane + 32 * i;
+        rv[i] = k < NPIX ? R.at((size_t)(vi + js + k / PW - HALF) * W + xr + k % PW - HALF) : 0.f;
+    }
     if (FLT) {
         // float32 patch: the CPU's sequential float64 sums (x * x a float32 product)
         double a = 0.0, a2 = 0.0;
@@ -406,10 +541,8 @@ __global__ void __launch_bounds__(ST_WARPS * 32, 5) k_stereo(
         rsd = __dsqrt_rn(var > 0.0 ? var : 0.0);
     } else {
         int a = 0, a2 = 0;
-        for (int k = lane; k < NPIX; k += 32) {
-            int x = (int)R.at((size_t)(vi + js + k / PW - HALF) * W + xr + k % PW - HALF);
-            a += x; a2 += x * x;
-        }
+#pragma unroll
+        for (int i = 0; i < KP; ++i) { const int x = (int)rv[i]; a += x; a2 += x * x; }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) { a += __shfl_xor_sync(0xffffffffu, a, o); a2 += __shfl_xor_sync(0xffffffffu, a2, o); }
         rm = __ddiv_rn((double)a, (double)NPIX);
@@ -417,29 +550,24 @@ __global__ void __launch_bounds__(ST_WARPS * 32, 5) k_stereo(
         rsd = __dsqrt_rn(var > 0.0 ? var : 0.0);
     }
     if (rsd <= 1e-6) return;
-    for (int k = lane; k < NPIX; k += 32)
-        T2d[k] = __dsub_rn((double)R.at((size_t)(vi + js + k / PW - HALF) * W + xr + k % PW - HALF), rm);
+#pragma unroll
+    for (int i = 0; i < KP; ++i)
+        if (lane + 32 * i < NPIX) T2d[lane + 32 * i] = __dsub_rn((double)rv[i], rm);
     int dmax = MAXD - 1;
     if (xr + dmax + HALF >= W) dmax = W - 1 - HALF - xr;
     const int lc0 = xr - HALF, lcols = dmax + PW;
     __syncwarp();
-    for (int idx = lane; idx < PW * lcols; idx += 32) {
-        int rr = idx / lcols, cc = idx % lcols;
-        win[rr * ww + cc] = (float)L[(size_t)(vi - HALF + rr) * W + lc0 + cc];
-    }
+    // left-image window, candidate c at column c: lane scores c = 4 lane .. 4 lane + 3 (pad 4: word-aligned blocks)
+    stage_u8<HALF>(winb, L, W, vi - HALF, PW, lc0, lcols, 4, lane);
     __syncwarp();
     double lrb = -2.0;
     int lrd = -1;
     {
-        int col[4];
-        bool val[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) { col[q] = lane + 32 * q; val[q] = col[q] <= dmax; }
         double z[4];
-        zncc_q<HALF, false, 4>(win, ww, 0, col, val, T2d, rsd, z);
+        zncc4_u8<HALF>(winb + 4 + 4 * lane, T2d, rsd, z);
 #pragma unroll
-        for (int q = 0; q < 4; ++q)
-            if (val[q] && z[q] > lrb) { lrb = z[q]; lrd = col[q]; }
+        for (int k = 0; k < 4; ++k)
+            if (4 * lane + k <= dmax && z[k] > lrb) { lrb = z[k]; lrd = 4 * lane + k; }
     }
     warp_argmax(lrb, lrd);
     if (lrd < 0 || fabs((double)(lrd - bestd)) > LRT) return;
@@ -466,16 +594,74 @@ __global__ void __launch_bounds__(ST_WARPS * 32, 5) k_stereo(
         bil(Li, H, W, __dadd_rn(u, (double)(k % PW - HALF)), __dadd_rn(v, (double)(k / PW - HALF)), &Tl[k], &g_);
     }
     __syncwarp();
+    // the LK's right-image samples: x = u + dx - d moves with d, y = v + dy + voff does not (its row and weight are
+    // fixed).  u8 right image: the rows the samples can touch and the columns of d within LK_MG of the integer peak are
+    // staged once as float64 after the term table; a sample outside them (a diverging LK) reads the image.
+    constexpr int LK_MG = 4, LKW = PW + 2 * LK_MG + 2, LKR = PW + 2;
+    double* lks = terms + LK_TERMS * NPIX;
+    const int xs0 = xr - HALF - LK_MG - 1, ys0 = vi + js - HALF - 1;
+    const int xa = xs0 > 0 ? xs0 : 0, xb = xs0 + LKW - 1 < W - 1 ? xs0 + LKW - 1 : W - 1;
+    double lpx[KP], lay[KP];
+    int lyr[KP];
+#pragma unroll
+    for (int i = 0; i < KP; ++i) {
+        const int k = lane + 32 * i < NPIX ? lane + 32 * i : NPIX - 1;
+        lpx[i] = __dadd_rn(u, (double)(k % PW - HALF));
+        const double y = __dadd_rn(__dadd_rn(v, (double)(k / PW - HALF)), voff);
+        int y0 = (int)floor(y);
+        lay[i] = __dsub_rn(y, (double)y0);
+        if (y0 < 0) y0 = 0;
+        if (y0 > H - 2) y0 = H - 2;
+        lyr[i] = y0;
+    }
+    if (!FLT) {
+#pragma unroll
+        for (int i = 0; i < (LKR * LKW + 31) / 32; ++i) {
+            const int idx = lane + 32 * i;
+            if (idx < LKR * LKW) {
+                const int rr = idx / LKW, col = xs0 + idx - rr * LKW;
+                lks[idx] = (col >= 0 && col < W) ? (double)R.r8[(size_t)(ys0 + rr) * W + col] : 0.0;
+            }
+        }
+    }
+    __syncwarp();
     double d = seed, a = 1.0, b = 0.0;
     bool okk = false;
     double sig = 0.0;
     for (int it = 0; it <= LK_ITERS; ++it) {
         // every patch pixel's residual and Jacobian terms, all lanes in parallel (terms[t][k]); then lane t sums term
         // t over k = 0..NPIX-1 in the CPU's order.  Table rows: J0 r, J1 r, r, J0 J0, J0 J1, J0, J1 J1, J1, r r.
-        for (int k = lane; k < NPIX; k += 32) {
+#pragma unroll
+        for (int i = 0; i < KP; ++i) {
+            const int k = lane + 32 * i;
+            if (k >= NPIX) break;
             double rv, rg;
-            double px = __dadd_rn(u, (double)(k % PW - HALF)), py = __dadd_rn(v, (double)(k / PW - HALF));
-            bil(R, H, W, __dsub_rn(px, d), __dadd_rn(py, voff), &rv, &rg);
+            if (FLT) {
+                double px = __dadd_rn(u, (double)(k % PW - HALF)), py = __dadd_rn(v, (double)(k / PW - HALF));
+                bil(R, H, W, __dsub_rn(px, d), __dadd_rn(py, voff), &rv, &rg);
+            } else {
+                // bil() on u8 values held as float64 (their float32 differences are exact, so are these)
+                const double x = __dsub_rn(lpx[i], d);
+                int x0 = (int)floor(x);
+                const double ax = __dsub_rn(x, (double)x0);
+                if (x0 < 0) x0 = 0;
+                if (x0 > W - 2) x0 = W - 2;
+                const int y0 = lyr[i];
+                double fa, fb, fc, fd;
+                if (x0 >= xa && x0 + 1 <= xb && y0 >= ys0 && y0 + 1 < ys0 + LKR) {
+                    const double* sp = lks + (y0 - ys0) * LKW + (x0 - xs0);
+                    fa = sp[0]; fb = sp[1]; fc = sp[LKW]; fd = sp[LKW + 1];
+                } else {
+                    const u8* gp = R.r8 + (size_t)y0 * W + x0;
+                    fa = (double)gp[0]; fb = (double)gp[1]; fc = (double)gp[W]; fd = (double)gp[W + 1];
+                }
+                const double ay = lay[i];
+                const double ba = __dsub_rn(fb, fa), dc = __dsub_rn(fd, fc);
+                const double top = __dadd_rn(fa, __dmul_rn(ax, ba));
+                const double bot = __dadd_rn(fc, __dmul_rn(ax, dc));
+                rv = __dadd_rn(top, __dmul_rn(ay, __dsub_rn(bot, top)));
+                rg = __dadd_rn(__dmul_rn(ba, __dsub_rn(1.0, ay)), __dmul_rn(dc, ay));
+            }
             double r = __dsub_rn(Tl[k], __dadd_rn(__dmul_rn(a, rv), b));
             double J0 = __dmul_rn(-a, rg), J1 = rv;
             terms[0 * NPIX + k] = __dmul_rn(J0, r);
@@ -535,24 +721,31 @@ __global__ void __launch_bounds__(ST_WARPS * 32, 5) k_stereo(
 
     // the point's own vertical offset: column scan of the ZNCC at the matched integer disparity
     if (vi - 2 * HALF - 1 >= 0 && vi + 2 * HALF + 1 < H) {
+        // image rows vi - 2 HALF .. vi + 2 HALF, columns xr - HALF .. xr + HALF, staged once (the LK table is done)
+        float* vsf = (float*)(base + stereo_off_u(HALF));
+        __syncwarp();
+#pragma unroll
+        for (int i = 0; i < ((2 * PW - 1) * PW + 31) / 32; ++i) {
+            const int idx = lane + 32 * i;
+            if (idx < (2 * PW - 1) * PW) {
+                const int rr = idx / PW, cc = idx - rr * PW;
+                vsf[idx] = R.at((size_t)(vi - 2 * HALF + rr) * W + xr - HALF + cc);
+            }
+        }
+        __syncwarp();
         double z = -2.0;
         if (lane < PW) {
-            const int vy = vi + lane - HALF;
+            // lane j scores rows vi + j - 2 HALF .. vi + j (staged rows j .. j + PW - 1).  Sums of u8 values and of
+            // their squares are exact in float64 in any order; the shifted float32 image keeps the CPU's float32 square.
             double zs = 0.0, zs2 = 0.0, sx = 0.0;
-            int zi = 0, zi2 = 0;
+#pragma unroll
             for (int k = 0; k < NPIX; ++k) {
-                float rf = R.at((size_t)(vy + k / PW - HALF) * W + xr + k % PW - HALF);
-                double r = (double)rf;
-                if (FLT) {
-                    zs = __dadd_rn(zs, r);
-                    zs2 = __dadd_rn(zs2, (double)__fmul_rn(rf, rf));
-                } else {
-                    int iv = (int)rf;
-                    zi += iv; zi2 += iv * iv;
-                }
+                const float rf = vsf[(lane + k / PW) * PW + k % PW];
+                const double r = (double)rf;
+                zs = __dadd_rn(zs, r);
+                zs2 = __dadd_rn(zs2, FLT ? (double)__fmul_rn(rf, rf) : __dmul_rn(r, r));
                 sx = __dadd_rn(sx, __dmul_rn(r, Td[k]));
             }
-            if (!FLT) { zs = (double)zi; zs2 = (double)zi2; }
             z = zncc_finish(zs, zs2, sx, ts, NPIX);
         }
         double col[PW];
