@@ -89,6 +89,27 @@ def test_hamming_and_match(setup):
     assert np.array_equal(i0, c["m_i0"]) and np.array_equal(i1, c["m_i1"]), name
 
 
+@pytest.mark.parametrize("L,N", [(1, 1), (1, 9), (7, 1), (17, 130), (129, 257), (300, 1025), (5000, 2049)])
+def test_hamming_ties_and_ragged_sizes(L, N):
+    """Distances drawn from a few repeated descriptors (many exact ties, between and within rows), sizes that are not
+    multiples of the device tiles: best / second / first index and the column first index equal the CPU scan."""
+    from xclean_b200.front.gpu_front import GpuFront
+    rng = np.random.default_rng(L * 7919 + N)
+    pool = rng.integers(0, 256, (6, 32), dtype=np.uint8)
+    pool[1] = pool[0]
+    pool[2, :4] ^= 1                                      # near-duplicates: distances 0..few
+    A = np.where(rng.random((L, 1)) < 0.5, pool[rng.integers(0, 6, L)], rng.integers(0, 256, (L, 32), dtype=np.uint8))
+    B = np.where(rng.random((N, 1)) < 0.5, pool[rng.integers(0, 6, N)], rng.integers(0, 256, (N, 32), dtype=np.uint8))
+    gf = GpuFront(64, 64, cap=4096, max_frames=1)
+    try:
+        got = gf.hamming(A.astype(np.uint8), B.astype(np.uint8))
+    finally:
+        gf.close()
+    ref = O.hamming(A.astype(np.uint8), B.astype(np.uint8))
+    for g, r, nm in zip(got, ref, ("best", "second", "index", "column index")):
+        assert np.array_equal(g, r), nm
+
+
 def test_lk_solver_bitexact():
     from xclean_b200.front.gpu_front import GpuFront
     z = np.load(G.GOLDEN + "/lk_solver.npz")

@@ -686,6 +686,10 @@ extern "C" int xcb_front_hamming_host(xcb_front* f, const uint8_t* A, int L, con
     }
     if (N) CK(cudaMemcpyAsync(ci, f->d_hci, (size_t)N * 4, cudaMemcpyDeviceToHost, st), "D2H");
     CK(cudaStreamSynchronize(st), "hamming sync");
+    for (int j = 0; j < N; ++j) {          // device: (distance << 16 | query) column minima, all ones if no query
+        const uint32_t v = (uint32_t)ci[j];
+        ci[j] = v == 0xffffffffu ? -1 : (int32_t)(v & 0xffffu);
+    }
     return XCB_OK;
 }
 

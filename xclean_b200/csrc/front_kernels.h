@@ -67,6 +67,8 @@ struct XcbHamPairs {
     const int* NB;                // [npair] train counts
     int npair, maxL, maxN;
 };
+// rows: b1 / b2 / bi [npair x maxL] (best, second, first index of the best); columns: ci [npair x maxN] holds
+// (distance << 16 | first-minimum query) as unsigned, all ones where the pair has no query (set by this call)
 cudaError_t xcb_launch_hamming(const XcbHamPairs& p, int* b1, int* b2, int* bi, int* ci, cudaStream_t st);
 cudaError_t xcb_launch_match_epilogue(const XcbHamPairs& p, const int* b1, const int* b2, const int* bi,
                                       const int* ci, int ham_max, double ratio, long long* i0, long long* i1,

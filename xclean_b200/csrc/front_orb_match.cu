@@ -122,10 +122,15 @@ cudaError_t xcb_launch_orb(const uint8_t* blur, int F, int Hp, int Wp, const flo
 }
 
 // ------------------------------------------------------------------------------------------------------------------
-// Hamming: rows (query best / second / index, first minimum) and columns (train first-minimum query index)
+// Hamming, one pass over the distance matrix: a thread owns a query row and scans the train descriptors (staged in
+// shared memory, read as broadcasts) in increasing index with the CPU's update (strictly smaller replaces the best),
+// which gives best / second / first index directly.  The column side (each train descriptor's first-minimum query)
+// reuses the same distances: (distance << 16 | query) packed so that an unsigned minimum picks the smallest distance
+// and, among equal distances, the smallest query index; a warp reduces its 32 rows with redux.sync, the CTA in
+// shared memory, the row blocks of a pair with one global atomicMin per column and block.
 // ------------------------------------------------------------------------------------------------------------------
 #define HAM_T 128
-#define HAM_CHUNK 256
+#define HAM_CHUNK 1024
 
 __device__ __forceinline__ int ham4(const ulonglong2 a0, const ulonglong2 a1, const ulonglong2 b0,
                                     const ulonglong2 b1)
@@ -133,79 +138,59 @@ __device__ __forceinline__ int ham4(const ulonglong2 a0, const ulonglong2 a1, co
     return __popcll(a0.x ^ b0.x) + __popcll(a0.y ^ b0.y) + __popcll(a1.x ^ b1.x) + __popcll(a1.y ^ b1.y);
 }
 
-__global__ void __launch_bounds__(HAM_T) k_ham_rows(const u8* __restrict__ A, const u8* __restrict__ B,
+__global__ void __launch_bounds__(HAM_T) k_hamming(const u8* __restrict__ A, const u8* __restrict__ B,
                                                    long long strideA, long long strideB, const int* __restrict__ LA,
-                                                   const int* __restrict__ NB, int maxL, int* __restrict__ o1,
-                                                   int* __restrict__ o2, int* __restrict__ oi)
+                                                   const int* __restrict__ NB, int maxL, int maxN,
+                                                   int* __restrict__ o1, int* __restrict__ o2, int* __restrict__ oi,
+                                                   unsigned* __restrict__ colmin)
 {
     __shared__ ulonglong2 sb[HAM_CHUNK][2];
+    __shared__ unsigned cm[HAM_CHUNK];
     const int p = blockIdx.y;
     const int L = LA[p], N = NB[p];
-    const int i = blockIdx.x * HAM_T + threadIdx.x;
     if (blockIdx.x * HAM_T >= L) return;
+    const int i = blockIdx.x * HAM_T + threadIdx.x, lane = threadIdx.x & 31;
+    const bool act = i < L;
     const ulonglong2* Ap = (const ulonglong2*)(A + p * strideA);
     const ulonglong2* Bp = (const ulonglong2*)(B + p * strideB);
     ulonglong2 a0 = make_ulonglong2(0, 0), a1 = a0;
-    if (i < L) { a0 = Ap[2 * i]; a1 = Ap[2 * i + 1]; }
+    if (act) { a0 = Ap[2 * i]; a1 = Ap[2 * i + 1]; }
     int b1 = 1 << 30, b2 = 1 << 30, bi = -1;
+    unsigned* cg = colmin + (size_t)p * maxN;
     for (int j0 = 0; j0 < N; j0 += HAM_CHUNK) {
-        int nj = min(HAM_CHUNK, N - j0);
+        const int nj = min(HAM_CHUNK, N - j0);
         __syncthreads();
         for (int t = threadIdx.x; t < 2 * nj; t += HAM_T) sb[t >> 1][t & 1] = Bp[2 * j0 + t];
+        for (int t = threadIdx.x; t < nj; t += HAM_T) cm[t] = 0xffffffffu;
         __syncthreads();
-        if (i < L) {
-            for (int j = 0; j < nj; ++j) {
-                int d = ham4(a0, a1, sb[j][0], sb[j][1]);
-                if (d < b1) { b2 = b1; b1 = d; bi = j0 + j; }
-                else if (d < b2) b2 = d;
-            }
+        for (int j = 0; j < nj; ++j) {
+            const int d = ham4(a0, a1, sb[j][0], sb[j][1]);
+            if (d < b1) { b2 = b1; b1 = d; bi = j0 + j; }
+            else if (d < b2) b2 = d;
+            const unsigned wm = __reduce_min_sync(0xffffffffu, act ? ((unsigned)d << 16) | (unsigned)i : 0xffffffffu);
+            if (lane == 0 && wm != 0xffffffffu) atomicMin(&cm[j], wm);
         }
+        __syncthreads();
+        for (int t = threadIdx.x; t < nj; t += HAM_T)
+            if (cm[t] != 0xffffffffu) atomicMin(&cg[j0 + t], cm[t]);
     }
-    if (i < L) {
-        size_t o = (size_t)p * maxL + i;
+    if (act) {
+        const size_t o = (size_t)p * maxL + i;
         o1[o] = b1; o2[o] = b2; oi[o] = bi;
     }
-}
-
-__global__ void __launch_bounds__(HAM_T) k_ham_cols(const u8* __restrict__ A, const u8* __restrict__ B,
-                                                   long long strideA, long long strideB, const int* __restrict__ LA,
-                                                   const int* __restrict__ NB, int maxN, int* __restrict__ ci)
-{
-    __shared__ ulonglong2 sa[HAM_CHUNK][2];
-    const int p = blockIdx.y;
-    const int L = LA[p], N = NB[p];
-    const int j = blockIdx.x * HAM_T + threadIdx.x;
-    if (blockIdx.x * HAM_T >= N) return;
-    const ulonglong2* Ap = (const ulonglong2*)(A + p * strideA);
-    const ulonglong2* Bp = (const ulonglong2*)(B + p * strideB);
-    ulonglong2 b0 = make_ulonglong2(0, 0), b1 = b0;
-    if (j < N) { b0 = Bp[2 * j]; b1 = Bp[2 * j + 1]; }
-    int best = 1 << 30, idx = -1;
-    for (int i0 = 0; i0 < L; i0 += HAM_CHUNK) {
-        int ni = min(HAM_CHUNK, L - i0);
-        __syncthreads();
-        for (int t = threadIdx.x; t < 2 * ni; t += HAM_T) sa[t >> 1][t & 1] = Ap[2 * i0 + t];
-        __syncthreads();
-        if (j < N) {
-            for (int i = 0; i < ni; ++i) {
-                int d = ham4(sa[i][0], sa[i][1], b0, b1);
-                if (d < best) { best = d; idx = i0 + i; }
-            }
-        }
-    }
-    if (j < N) ci[(size_t)p * maxN + j] = idx;
 }
 
 cudaError_t xcb_launch_hamming(const XcbHamPairs& p, int* b1, int* b2, int* bi, int* ci, cudaStream_t st)
 {
     if (p.npair <= 0) return cudaSuccess;
+    if (p.maxN > 0) {
+        cudaError_t e = cudaMemsetAsync(ci, 0xff, (size_t)p.npair * p.maxN * sizeof(unsigned), st);
+        if (e != cudaSuccess) return e;
+    }
     if (p.maxL > 0) {
         dim3 gr((p.maxL + HAM_T - 1) / HAM_T, p.npair);
-        k_ham_rows<<<gr, HAM_T, 0, st>>>(p.A, p.B, p.strideA, p.strideB, p.LA, p.NB, p.maxL, b1, b2, bi);
-    }
-    if (p.maxN > 0) {
-        dim3 gc((p.maxN + HAM_T - 1) / HAM_T, p.npair);
-        k_ham_cols<<<gc, HAM_T, 0, st>>>(p.A, p.B, p.strideA, p.strideB, p.LA, p.NB, p.maxN, ci);
+        k_hamming<<<gr, HAM_T, 0, st>>>(p.A, p.B, p.strideA, p.strideB, p.LA, p.NB, p.maxL, p.maxN, b1, b2, bi,
+                                        (unsigned*)ci);
     }
     return cudaGetLastError();
 }
@@ -238,7 +223,8 @@ __global__ void __launch_bounds__(1024) k_match_epilogue(const int* __restrict__
             j = bi[o];
             if (j >= 0) {
                 int d1 = b1[o], d2 = b2[o];
-                ok = d1 <= ham_max && (double)d1 < ratio * (double)d2 && ci[(size_t)p * maxN + j] == q;
+                ok = d1 <= ham_max && (double)d1 < ratio * (double)d2 &&
+                     (ci[(size_t)p * maxN + j] & 0xffff) == q;
             }
         }
         unsigned bal = __ballot_sync(0xffffffffu, ok);
