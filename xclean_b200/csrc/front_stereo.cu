@@ -44,34 +44,51 @@ static __host__ __device__ __forceinline__ size_t stereo_warp_bytes(int half, in
 size_t xcb_stereo_smem_per_warp(int half, int band) { return stereo_warp_bytes(half, band); }
 
 // ---------------------------------------------------------------- OpenBLAS 3x3 arithmetic (as the oracle restates it)
+// Every loop has constant bounds and the pivot rows are applied by comparisons, so the matrix stays in registers (a
+// pivot used as an index would put it in local memory); the arithmetic and its order are OpenBLAS getf2 / getrs /
+// trti2 + getri's.
 __device__ __forceinline__ void ob_getf2(double a[3][3], int piv[3])
 {
+#pragma unroll
     for (int j = 0; j < 3; ++j) {
-        for (int i = 0; i < j; ++i) {
-            int ip = piv[i];
-            if (ip != i) { double t = a[i][j]; a[i][j] = a[ip][j]; a[ip][j] = t; }
-        }
+#pragma unroll
+        for (int i = 0; i < j; ++i)
+#pragma unroll
+            for (int r = i + 1; r < 3; ++r)
+                if (piv[i] == r) { double t = a[i][j]; a[i][j] = a[r][j]; a[r][j] = t; }
+#pragma unroll
         for (int i = 1; i < j; ++i) {
             double s = 0.0;
+#pragma unroll
             for (int k = 0; k < i; ++k) s = __fma_rn(a[i][k], a[k][j], s);
             a[i][j] = __dsub_rn(a[i][j], s);
         }
         if (j > 0)
+#pragma unroll
             for (int i = j; i < 3; ++i) {
                 double s = 0.0;
+#pragma unroll
                 for (int k = 0; k < j; ++k) s = __fma_rn(a[i][k], a[k][j], s);
                 a[i][j] = __dsub_rn(a[i][j], s);
             }
         int jp = j;
         double mx = fabs(a[j][j]);
+#pragma unroll
         for (int i = j + 1; i < 3; ++i)
             if (fabs(a[i][j]) > mx) { mx = fabs(a[i][j]); jp = i; }
         piv[j] = jp;
-        double t = a[jp][j];
+        double t = a[j][j];
+#pragma unroll
+        for (int r = j + 1; r < 3; ++r)
+            if (jp == r) t = a[r][j];
         if (t != 0.0) {
             t = __ddiv_rn(1.0, t);
-            if (jp != j)
-                for (int k = 0; k <= j; ++k) { double u = a[j][k]; a[j][k] = a[jp][k]; a[jp][k] = u; }
+#pragma unroll
+            for (int r = j + 1; r < 3; ++r)
+                if (jp == r)
+#pragma unroll
+                    for (int k = 0; k <= j; ++k) { double u = a[j][k]; a[j][k] = a[r][k]; a[r][k] = u; }
+#pragma unroll
             for (int i = j + 1; i < 3; ++i) a[i][j] = __dmul_rn(a[i][j], t);
         }
     }
@@ -79,43 +96,62 @@ __device__ __forceinline__ void ob_getf2(double a[3][3], int piv[3])
 
 __device__ __forceinline__ void ob_getrs(const double a[3][3], const int piv[3], double y[3])
 {
-    for (int j = 0; j < 3; ++j) { int p = piv[j]; if (p != j) { double t = y[j]; y[j] = y[p]; y[p] = t; } }
+#pragma unroll
     for (int j = 0; j < 3; ++j)
+#pragma unroll
+        for (int r = j + 1; r < 3; ++r)
+            if (piv[j] == r) { double t = y[j]; y[j] = y[r]; y[r] = t; }
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
         for (int i = j + 1; i < 3; ++i) y[i] = __fma_rn(-y[j], a[i][j], y[i]);
+#pragma unroll
     for (int j = 2; j >= 0; --j) {
         y[j] = __ddiv_rn(y[j], a[j][j]);
+#pragma unroll
         for (int i = 0; i < j; ++i) y[i] = __fma_rn(-y[j], a[i][j], y[i]);
     }
 }
 
 __device__ __forceinline__ void ob_getri(double a[3][3], const int piv[3])
 {
+#pragma unroll
     for (int j = 0; j < 3; ++j) {
         double ajj = __ddiv_rn(1.0, a[j][j]);
         a[j][j] = ajj;
         double x[3];
+#pragma unroll
         for (int i = 0; i < j; ++i) x[i] = a[i][j];
+#pragma unroll
         for (int i = 0; i < j; ++i) {
+#pragma unroll
             for (int q = 0; q < i; ++q) x[q] = __fma_rn(x[i], a[q][i], x[q]);
             x[i] = __dmul_rn(x[i], a[i][i]);
         }
+#pragma unroll
         for (int i = 0; i < j; ++i) a[i][j] = __dmul_rn(x[i], -ajj);
     }
     double work[3] = {0.0, 0.0, 0.0};
+#pragma unroll
     for (int j = 2; j >= 0; --j) {
+#pragma unroll
         for (int i = j + 1; i < 3; ++i) { work[i] = a[i][j]; a[i][j] = 0.0; }
         if (j < 2)
+#pragma unroll
             for (int r = 0; r < 3; ++r) {
                 double s = 0.0;
+#pragma unroll
                 for (int k = j + 1; k < 3; ++k) s = __fma_rn(a[r][k], work[k], s);
                 a[r][j] = __dsub_rn(a[r][j], s);
             }
     }
-    for (int j = 1; j >= 0; --j) {
-        int jp = piv[j];
-        if (jp != j)
-            for (int r = 0; r < 3; ++r) { double t = a[r][j]; a[r][j] = a[r][jp]; a[r][jp] = t; }
-    }
+#pragma unroll
+    for (int j = 1; j >= 0; --j)
+#pragma unroll
+        for (int c = j + 1; c < 3; ++c)
+            if (piv[j] == c)
+#pragma unroll
+                for (int r = 0; r < 3; ++r) { double t = a[r][j]; a[r][j] = a[r][c]; a[r][c] = t; }
 }
 
 __global__ void k_lkcheck(const double* __restrict__ As, const double* __restrict__ gs, int n, double* __restrict__ X,
@@ -738,7 +774,7 @@ __global__ void __launch_bounds__(ST_WARPS * 32, 5) k_stereo(
             // lane j scores rows vi + j - 2 HALF .. vi + j (staged rows j .. j + PW - 1).  Sums of u8 values and of
             // their squares are exact in float64 in any order; the shifted float32 image keeps the CPU's float32 square.
             double zs = 0.0, zs2 = 0.0, sx = 0.0;
-#pragma unroll
+#pragma unroll 9
             for (int k = 0; k < NPIX; ++k) {
                 const float rf = vsf[(lane + k / PW) * PW + k % PW];
                 const double r = (double)rf;
