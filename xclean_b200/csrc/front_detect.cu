@@ -24,12 +24,10 @@ struct SobelRow {
     float rx, ry;
 };
 
-// row-filter outputs of OpenCV's Sobel at column c of one image row: rx = derivative taps (-1 0 1), ry = smoothing
-// taps (1 2 1) * scale, fused for c < dy_vend
-__device__ __forceinline__ SobelRow sobel_row(const u8* row, int W, int c, float ks, float k2s, int dy_vend)
+// row-filter outputs of OpenCV's Sobel at column c of one image row from its pixels a = row[c - 1], b = row[c],
+// d = row[c + 1] (reflected): rx = derivative taps (-1 0 1), ry = smoothing taps (1 2 1) * scale, fused for c < dy_vend
+__device__ __forceinline__ SobelRow sobel_row_v(float a, float b, float d, int c, float ks, float k2s, int dy_vend)
 {
-    int cm = XCB_REFL(c - 1, W), cp = XCB_REFL(c + 1, W);
-    float a = (float)row[cm], b = (float)row[c], d = (float)row[cp];
     SobelRow o;
     o.rx = __fsub_rn(d, a);
     if (c < dy_vend) {
@@ -46,13 +44,17 @@ __device__ __forceinline__ SobelRow sobel_row(const u8* row, int W, int c, float
     return o;
 }
 
-// Sobel (dx, dy) at (y, c) -> the three products dx*dx, dx*dy, dy*dy (float32)
-__device__ __forceinline__ void sobel_products(const u8* I, int H, int W, int y, int c, float ks, float k2s,
-                                               int dy_vend, int dx_vend, float p[3])
+__device__ __forceinline__ SobelRow sobel_row(const u8* row, int W, int c, float ks, float k2s, int dy_vend)
 {
-    SobelRow r0 = sobel_row(I + (size_t)XCB_REFL(y - 1, H) * W, W, c, ks, k2s, dy_vend);
-    SobelRow r1 = sobel_row(I + (size_t)y * W, W, c, ks, k2s, dy_vend);
-    SobelRow r2 = sobel_row(I + (size_t)XCB_REFL(y + 1, H) * W, W, c, ks, k2s, dy_vend);
+    return sobel_row_v((float)row[XCB_REFL(c - 1, W)], (float)row[c], (float)row[XCB_REFL(c + 1, W)], c, ks, k2s,
+                       dy_vend);
+}
+
+// Sobel (dx, dy) at column c from the row-filter outputs of the rows above, at and below -> the three products
+// dx*dx, dx*dy, dy*dy (float32)
+__device__ __forceinline__ void sobel_products3(const SobelRow& r0, const SobelRow& r1, const SobelRow& r2, int c,
+                                                float ks, float k2s, int dx_vend, float p[3])
+{
     float t = __fadd_rn(r0.rx, r2.rx);
     float dx = (c < dx_vend) ? __fmaf_rn(t, ks, __fmul_rn(r1.rx, k2s))
                              : __fadd_rn(__fmul_rn(t, ks), __fmul_rn(r1.rx, k2s));
@@ -60,6 +62,16 @@ __device__ __forceinline__ void sobel_products(const u8* I, int H, int W, int y,
     p[0] = __fmul_rn(dx, dx);
     p[1] = __fmul_rn(dx, dy);
     p[2] = __fmul_rn(dy, dy);
+}
+
+// Sobel products at (y, c)
+__device__ __forceinline__ void sobel_products(const u8* I, int H, int W, int y, int c, float ks, float k2s,
+                                               int dy_vend, int dx_vend, float p[3])
+{
+    SobelRow r0 = sobel_row(I + (size_t)XCB_REFL(y - 1, H) * W, W, c, ks, k2s, dy_vend);
+    SobelRow r1 = sobel_row(I + (size_t)y * W, W, c, ks, k2s, dy_vend);
+    SobelRow r2 = sobel_row(I + (size_t)XCB_REFL(y + 1, H) * W, W, c, ks, k2s, dy_vend);
+    sobel_products3(r0, r1, r2, c, ks, k2s, dx_vend, p);
 }
 
 // box-filter row sums (double) of the three products at row y, column x
@@ -74,7 +86,7 @@ __device__ __forceinline__ void row_sums(const u8* I, int H, int W, int y, int x
     for (int ch = 0; ch < 3; ++ch) rs[ch] = __dadd_rn(__dadd_rn((double)pm[ch], (double)p0[ch]), (double)pp[ch]);
 }
 
-__global__ void __launch_bounds__(128) k_response(const u8* __restrict__ imgs, int H, int W, int dy_vend,
+__global__ void __launch_bounds__(128, 7) k_response(const u8* __restrict__ imgs, int H, int W, int dy_vend,
                                                   int dx_vend, float* __restrict__ Rall, int* __restrict__ anypos)
 {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -90,8 +102,58 @@ __global__ void __launch_bounds__(128) k_response(const u8* __restrict__ imgs, i
         row_sums(I, H, W, 0, x, ks, k2s, dy_vend, dx_vend, b);
 #pragma unroll
         for (int ch = 0; ch < 3; ++ch) S[ch] = __dadd_rn(__dadd_rn(0.0, a[ch]), b[ch]);
+        // the row-filter outputs of image rows y and y + 1 at columns x - 1, x, x + 1 roll down with y, so each step
+        // filters one new row, whose nine pixels were loaded a step earlier (the last step, whose rows reflect back
+        // up, is computed in full)
+        const int cols[3] = {XCB_REFL(x - 1, W), x, XCB_REFL(x + 1, W)};
+        int po[3][3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            po[k][0] = XCB_REFL(cols[k] - 1, W); po[k][1] = cols[k]; po[k][2] = XCB_REFL(cols[k] + 1, W);
+        }
+        SobelRow q0[3], q1[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            q0[k] = sobel_row(I, W, cols[k], ks, k2s, dy_vend);
+            q1[k] = sobel_row(I + (size_t)XCB_REFL(1, H) * W, W, cols[k], ks, k2s, dy_vend);
+        }
+        u8 nb[3][3];
+        {
+            const u8* rn = I + (size_t)XCB_REFL(2, H) * W;
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+#pragma unroll
+                for (int e = 0; e < 3; ++e) nb[k][e] = rn[po[k][e]];
+        }
         for (int y = 0; y < H; ++y) {
-            row_sums(I, H, W, XCB_REFL(y + 1, H), x, ks, k2s, dy_vend, dx_vend, c);
+            if (y < H - 1 && H >= 3) {
+                u8 cb[3][3];
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+#pragma unroll
+                    for (int e = 0; e < 3; ++e) cb[k][e] = nb[k][e];
+                if (y + 1 < H - 1) {
+                    const u8* rn = I + (size_t)XCB_REFL(y + 3, H) * W;
+#pragma unroll
+                    for (int k = 0; k < 3; ++k)
+#pragma unroll
+                        for (int e = 0; e < 3; ++e) nb[k][e] = rn[po[k][e]];
+                }
+                float pr[3][3];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    const SobelRow q2 = sobel_row_v((float)cb[k][0], (float)cb[k][1], (float)cb[k][2], cols[k], ks,
+                                                    k2s, dy_vend);
+                    sobel_products3(q0[k], q1[k], q2, cols[k], ks, k2s, dx_vend, pr[k]);
+                    q0[k] = q1[k];
+                    q1[k] = q2;
+                }
+#pragma unroll
+                for (int ch = 0; ch < 3; ++ch)
+                    c[ch] = __dadd_rn(__dadd_rn((double)pr[0][ch], (double)pr[1][ch]), (double)pr[2][ch]);
+            } else {
+                row_sums(I, H, W, XCB_REFL(y + 1, H), x, ks, k2s, dy_vend, dx_vend, c);
+            }
             float cov[3];
 #pragma unroll
             for (int ch = 0; ch < 3; ++ch) {

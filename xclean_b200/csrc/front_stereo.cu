@@ -26,7 +26,8 @@ static __host__ __device__ __forceinline__ int win_w(int half) { return ((MAXD +
 
 // per-warp shared memory: Td [NPIX] f64 | T2d [NPIX] f64 | sc [MAXD] f64 | jb [MAXD] i8 | U, where U holds the image
 // window (float32 rows of win_w, or u8 rows of U8Win::WWB) during the two searches, then the LK term table
-// (LK_TERMS x NPIX f64) and the LK's staged right-image block ((PW + 2) x (PW + 10) f64)
+// (LK_TERMS rows of NPIX f64, rows NPIXP = NPIX rounded up to even apart) and the LK's staged right-image block
+// ((PW + 2) x (PW + 10) f64)
 static __host__ __device__ __forceinline__ size_t stereo_off_u(int half)
 {
     int pw = 2 * half + 1, npix = pw * pw;
@@ -37,7 +38,7 @@ static __host__ __device__ __forceinline__ size_t stereo_warp_bytes(int half, in
 {
     int pw = 2 * half + 1, npix = pw * pw;
     size_t win = (size_t)(pw + 2 * band) * win_w(half) * 4;
-    size_t terms = (size_t)LK_TERMS * npix * 8 + (size_t)(pw + 2) * (pw + 2 * 4 + 2) * 8;   // + the LK's staged block
+    size_t terms = (size_t)LK_TERMS * ((npix + 1) & ~1) * 8 + (size_t)(pw + 2) * (pw + 2 * 4 + 2) * 8;   // + LK block
     return (stereo_off_u(half) + (win > terms ? win : terms) + 15) & ~(size_t)15;
 }
 
@@ -405,7 +406,7 @@ __global__ void __launch_bounds__(ST_WARPS * 32, 5) k_stereo(
     double* __restrict__ od, double* __restrict__ osig, u8* __restrict__ ook, double* __restrict__ ozn,
     double* __restrict__ ody)
 {
-    constexpr int PW = 2 * HALF + 1, NPIX = PW * PW;
+    constexpr int PW = 2 * HALF + 1, NPIX = PW * PW, NPIXP = (NPIX + 1) & ~1;
     static_assert(U8Win<HALF>::WWB <= 4 * (((MAXD + 2 * HALF) + 3) & ~3), "u8 rows fit the float32 window rows");
     const double ZMIN = 0.5, UNIQ1 = 1.0 + 0.05, LRT = 1.0;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -634,7 +635,7 @@ __global__ void __launch_bounds__(ST_WARPS * 32, 5) k_stereo(
     // fixed).  u8 right image: the rows the samples can touch and the columns of d within LK_MG of the integer peak are
     // staged once as float64 after the term table; a sample outside them (a diverging LK) reads the image.
     constexpr int LK_MG = 4, LKW = PW + 2 * LK_MG + 2, LKR = PW + 2;
-    double* lks = terms + LK_TERMS * NPIX;
+    double* lks = terms + LK_TERMS * NPIXP;
     const int xs0 = xr - HALF - LK_MG - 1, ys0 = vi + js - HALF - 1;
     const int xa = xs0 > 0 ? xs0 : 0, xb = xs0 + LKW - 1 < W - 1 ? xs0 + LKW - 1 : W - 1;
     double lpx[KP], lay[KP];
@@ -700,22 +701,26 @@ __global__ void __launch_bounds__(ST_WARPS * 32, 5) k_stereo(
             }
             double r = __dsub_rn(Tl[k], __dadd_rn(__dmul_rn(a, rv), b));
             double J0 = __dmul_rn(-a, rg), J1 = rv;
-            terms[0 * NPIX + k] = __dmul_rn(J0, r);
-            terms[1 * NPIX + k] = __dmul_rn(J1, r);
-            terms[2 * NPIX + k] = r;
-            terms[3 * NPIX + k] = __dmul_rn(J0, J0);
-            terms[4 * NPIX + k] = __dmul_rn(J0, J1);
-            terms[5 * NPIX + k] = J0;
-            terms[6 * NPIX + k] = __dmul_rn(J1, J1);
-            terms[7 * NPIX + k] = J1;
-            terms[8 * NPIX + k] = __dmul_rn(r, r);
+            terms[0 * NPIXP + k] = __dmul_rn(J0, r);
+            terms[1 * NPIXP + k] = __dmul_rn(J1, r);
+            terms[2 * NPIXP + k] = r;
+            terms[3 * NPIXP + k] = __dmul_rn(J0, J0);
+            terms[4 * NPIXP + k] = __dmul_rn(J0, J1);
+            terms[5 * NPIXP + k] = J0;
+            terms[6 * NPIXP + k] = __dmul_rn(J1, J1);
+            terms[7 * NPIXP + k] = J1;
+            terms[8 * NPIXP + k] = __dmul_rn(r, r);
         }
         __syncwarp();
         double S = 0.0;
         if (lane < LK_TERMS && (lane < 8 || it == LK_ITERS)) {
-            const double* tr = terms + lane * NPIX;
-#pragma unroll 9
-            for (int k = 0; k < NPIX; ++k) S = __dadd_rn(S, tr[k]);
+            const double2* tr = (const double2*)(terms + lane * NPIXP);     // rows are 16-byte aligned
+#pragma unroll 8
+            for (int k2 = 0; k2 < NPIX / 2; ++k2) {
+                const double2 t2 = tr[k2];
+                S = __dadd_rn(__dadd_rn(S, t2.x), t2.y);
+            }
+            if (NPIX & 1) S = __dadd_rn(S, terms[lane * NPIXP + NPIX - 1]);
         }
         __syncwarp();
         double Sv[10];
