@@ -191,10 +191,22 @@ int xcb_ba_solve_windows_noalloc(const xcb_ba_windows* w, int Lt, int max_slots,
    large, -2 a landmark touches more than 16 keyframes). */
 #define XCB_BA_NEWTON_POLISH 0
 #define XCB_BA_NEWTON_ADJOINT 1
+#define XCB_BA_NEWTON_POLISH_FIXED 2      /* as XCB_BA_NEWTON_POLISH, flagging no new constant landmarks */
 size_t xcb_ba_newton_scratch_bytes(int nw, int Lt);
 int xcb_ba_newton_windows_dev(const xcb_ba_windows* w, int max_slots, int mode, int steps, int maxit, double tol,
                               const double* gpose, double* gtheta, double* gisig, double* gz, double* stats,
                               void* scratch, size_t scratch_bytes, int grid, void* stream);
+
+/* window.solve's LM (as xcb_ba_solve_windows_dev, float64) with the landmarks that the Newton calls on `scratch` found
+   frozen held constant (no reference counterpart; the differentiable BA's forward).  window.solve keeps a landmark
+   whose step would take its inverse depth to <= 1e-9 where it is, but its Schur complement assumes every landmark
+   moves, so its fixed point is not a stationary point of the cost when such landmarks exist; holding them constant
+   (their rows stay in the pose blocks and the gradient) makes the LM converge to one.  A landmark is flagged by
+   XCB_BA_NEWTON_POLISH calls (whose Gauss-Newton step, decoupled from the poses, would take its inverse depth to
+   <= 1e-9; a flag stays until the scratch is cleared).  scratch: the Newton scratch, at least
+   xcb_ba_newton_scratch_bytes(nw, Lt) bytes (Lt: the batch's landmarks).  stats [nw][8] as xcb_ba_solve_windows_dev. */
+int xcb_ba_solve_windows_free_dev(const xcb_ba_windows* w, int Lt, int max_slots, int iters, double lam0,
+                                  double* stats, void* scratch, size_t scratch_bytes, int grid, void* stream);
 
 /* ----------------------------------------------------------------------------------------------------------------
    Local-BA stage kernels: one entry point per kernel of src/xclean/backend/kernels.py, same argument order and

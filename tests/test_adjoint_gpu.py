@@ -40,7 +40,7 @@ def run():
     ws = _windows()
     solver = BatchSolver(ws, "cuda", hold=0)
     inp = inputs_of(solver)
-    p = BAAdjoint.apply(*inp, solver, 100, 4)
+    p = BAAdjoint.apply(*inp, solver, 100, 10)
     torch.cuda.synchronize()
     so = solver.host["slot_off"]
     ptrue = torch.as_tensor(np.concatenate([w.pwb_true for w in ws]), device="cuda")

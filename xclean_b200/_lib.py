@@ -71,6 +71,7 @@ XCB_BA_FP64 = 0
 XCB_BA_MIXED = 1
 XCB_BA_NEWTON_POLISH = 0
 XCB_BA_NEWTON_ADJOINT = 1
+XCB_BA_NEWTON_POLISH_FIXED = 2
 _SIGS.update({
     "xcb_ba_scratch_bytes": (c_size_t, [c_int, c_int]),
     "xcb_ba_solve_windows_dev": (c_int, [ctypes.POINTER(BaWindows), c_int, c_int, c_double, c_int, P, P, c_int, P,
@@ -78,6 +79,8 @@ _SIGS.update({
     "xcb_ba_newton_scratch_bytes": (c_size_t, [c_int, c_int]),
     "xcb_ba_newton_windows_dev": (c_int, [ctypes.POINTER(BaWindows), c_int, c_int, c_int, c_int, c_double, P, P, P,
                                           P, P, P, c_size_t, c_int, P]),
+    "xcb_ba_solve_windows_free_dev": (c_int, [ctypes.POINTER(BaWindows), c_int, c_int, c_int, c_double, P, P,
+                                              c_size_t, c_int, P]),
     "xcb_ba_noalloc_max_landmarks": (c_int, []),
     "xcb_ba_solve_windows_noalloc": (c_int, [ctypes.POINTER(BaWindows), c_int, c_int, c_int, c_double, c_int, P, P,
                                              c_int, c_int, P]),

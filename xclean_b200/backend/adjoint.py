@@ -11,15 +11,17 @@ converged poses to de-rectifying it), weights [M] (the per-row weight 1/sigma in
 [M, 2] (observed pixels per row; the right rows use column 0).  Output: the converged body translations [slots, 3]
 (float64; the batch's slots in window order).
 
-Forward: `iters` LM iterations of window.solve (float64, batched, one launch), then at most `newton_steps`
-trust-region Newton steps on the exact Hessian (window.solve alone converges only linearly where Huber weights are
-active, can stall where its positive-depth rule rejects a landmark's step, and the adjoint is exact only at a
-stationary point).  Backward: one solve H x = dL/dstate (H applied exactly through dual numbers, conjugate gradients
+Forward: `iters` LM iterations of window.solve (float64, batched, one launch); then the landmarks whose
+Gauss-Newton step would take the inverse depth to <= 1e-9 (window.solve keeps them where they are, while its Schur
+complement assumes they move, so its fixed point is not stationary) are flagged constant and two rounds of
+`free_iters` LM iterations run with them held; then at most `newton_steps` trust-region Newton steps on the exact
+Hessian (the LM converges only linearly where Huber weights are active, and the adjoint is exact only at a stationary
+point).  Backward: one solve H x = dL/dstate (H applied exactly through dual numbers, conjugate gradients
 preconditioned with the Gauss-Newton Cholesky factor, Jacobians recomputed from the state rather than stored), then dL/dtheta = -(d2C / dtheta dstate) x, scattered to the window parameters and to every observation row.
 The solver keeps the converged state between forward and backward: do not reuse it for another forward before
 backward.  ctx.newton_stats / ctx.adjoint_stats keep the per-window stats (column 2: the gradient max-norm at the
 returned state; a window that did not reach a stationary point within `newton_steps` has an approximate gradient).
-Landmarks that window.solve cannot move (its step would take the inverse depth to <= 1e-9) are constants.
+The flagged landmarks are constants of the forward and of the adjoint.
 """
 from __future__ import annotations
 
@@ -29,7 +31,7 @@ import torch
 class BAAdjoint(torch.autograd.Function):
     @staticmethod
     def forward(ctx, intrinsics, baseline, extrinsic, weights, pixels, solver, iters=20, newton_steps=40,
-                lam0=1e-4, tol=1e-12):
+                lam0=1e-4, tol=1e-12, free_iters=40):
         if float(extrinsic.detach().abs().max()) != 0.0:
             raise ValueError("BAAdjoint: the left-to-right extrinsic is the rectified rig (zero); only its gradient "
                              "is returned")
@@ -46,7 +48,10 @@ class BAAdjoint(torch.autograd.Function):
             t["ob_z"].copy_(pixels.detach().to(torch.float64))
             solver.reset()
             solver.solve(int(iters), float(lam0), "fp64")
-            st = solver.newton(int(newton_steps), tol=float(tol))
+            for _ in range(2):
+                solver.newton(0)                                    # flag the landmarks the LM cannot move
+                solver.solve_free(int(free_iters), float(lam0))
+            st = solver.newton(int(newton_steps), tol=float(tol), flag=False)
         ctx.solver = solver
         ctx.tol = float(tol)
         ctx.dtypes = (intrinsics.dtype, baseline.dtype, extrinsic.dtype, weights.dtype, pixels.dtype)
@@ -62,7 +67,7 @@ class BAAdjoint(torch.autograd.Function):
         ctx.adjoint_stats = stats
         di, db, de, dw, dp = ctx.dtypes
         return (gtheta[:, 0:4].to(di), gtheta[:, 4].to(db), gtheta[:, 5:11].to(de), gisig.to(dw), gz.to(dp),
-                None, None, None, None, None)
+                None, None, None, None, None, None)
 
 
 def inputs_of(solver, requires_grad=True):

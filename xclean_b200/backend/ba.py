@@ -105,6 +105,33 @@ class BatchSolver:
     def reset(self):
         for k in ("Rwb", "pwb", "lmp"):
             self.t[k].copy_(self.init[k])
+        self.clear_frozen()
+
+    def clear_frozen(self):
+        """Forget the constant-landmark flags of the Newton calls (they belong to the state they were found at)."""
+        if hasattr(self, "nscratch"):
+            self.nscratch.zero_()
+
+    def _nscratch(self):
+        if not hasattr(self, "nscratch"):
+            nb = int(_lib.lib().xcb_ba_newton_scratch_bytes(self.nw, int(self.host["lmp"].shape[0])))
+            self.nscratch = self.torch.zeros(nb, dtype=self.torch.uint8, device=self.dev)
+        return self.nscratch
+
+    def solve_free(self, iters=20, lam0=1e-4, stream=None, grid=0):
+        """window.solve (float64) with the landmarks that earlier newton() calls found frozen held constant, so that
+        the LM converges to a stationary point of the cost in the other variables.  -> stats [nw, 8] (cost0, cost,
+        accepted, lam, status, iters, -, -)."""
+        torch = self.torch
+        s = stream if stream is not None else torch.cuda.current_stream(self.dev)
+        sc = self._nscratch()
+        stats = torch.zeros((max(self.nw, 1), 8), dtype=torch.float64, device=self.dev)
+        rc = _lib.lib().xcb_ba_solve_windows_free_dev(ctypes.byref(self.desc), int(self.host["lmp"].shape[0]),
+                                                      self.max_slots, int(iters), float(lam0), stats.data_ptr(),
+                                                      sc.data_ptr(), sc.numel(), int(grid),
+                                                      ctypes.c_void_p(s.cuda_stream or None))
+        _lib.check(rc, None, "xcb_ba_solve_windows_free_dev")
+        return stats[:self.nw]
 
     def solve(self, iters=5, lam0=1e-4, precision="mixed", stream=None, grid=0):
         """One persistent launch over every window (asynchronous on `stream`, torch's current stream by default)."""
@@ -116,10 +143,13 @@ class BatchSolver:
                                                  int(grid), ctypes.c_void_p(s.cuda_stream or None))
         _lib.check(rc, None, "xcb_ba_solve_windows_dev")
 
-    def newton(self, steps=3, maxit=60, tol=1e-12, stream=None, grid=0):
+    def newton(self, steps=3, maxit=60, tol=1e-12, stream=None, grid=0, flag=True):
         """Exact-Hessian Newton steps on every window (in place): the converged state the adjoint differentiates.
+        flag: landmarks whose decoupled Gauss-Newton step would take the inverse depth to <= 1e-9 at an evaluated
+        state are flagged constant (flags persist until clear_frozen / reset); False keeps the flags as they are.
         -> per-window stats tensor [nw, 4] (CG iterations, relative residual, final gradient max-norm, status)."""
-        return self._newton(_lib.XCB_BA_NEWTON_POLISH, steps, maxit, tol, None, stream, grid)[0]
+        mode = _lib.XCB_BA_NEWTON_POLISH if flag else _lib.XCB_BA_NEWTON_POLISH_FIXED
+        return self._newton(mode, steps, maxit, tol, None, stream, grid)[0]
 
     def adjoint(self, gpose, maxit=60, tol=1e-12, stream=None, grid=0):
         """dL/dtheta at the current (converged) state for dL/d(dphi, dp) = gpose [slots, 6] (float64 CUDA tensor)
@@ -130,9 +160,7 @@ class BatchSolver:
         torch = self.torch
         s = stream if stream is not None else torch.cuda.current_stream(self.dev)
         M = int(self.host["ob_isig"].shape[0])
-        if not hasattr(self, "nscratch"):
-            nb = int(_lib.lib().xcb_ba_newton_scratch_bytes(self.nw, int(self.host["lmp"].shape[0])))
-            self.nscratch = torch.zeros(nb, dtype=torch.uint8, device=self.dev)
+        self._nscratch()
         stats = torch.zeros((max(self.nw, 1), 4), dtype=torch.float64, device=self.dev)
         gtheta = torch.zeros((max(self.nw, 1), 11), dtype=torch.float64, device=self.dev)
         gisig = torch.zeros(max(M, 1), dtype=torch.float64, device=self.dev)

@@ -50,10 +50,45 @@ static int ba_fail(int code, const char* msg)
     return code;
 }
 
+// Newton / adjoint scratch: [counter (256 B)][19 doubles per landmark][3 doubles per landmark: trial states of the
+// constant-landmark window solve]
 extern "C" size_t xcb_ba_newton_scratch_bytes(int nw, int Lt)
 {
     (void)nw;
-    return ((size_t)(Lt > 0 ? Lt : 1) * 19 * sizeof(double) + 255) / 256 * 256 + 256;
+    return ((size_t)(Lt > 0 ? Lt : 1) * 22 * sizeof(double) + 255) / 256 * 256 + 256;
+}
+
+static int ba_grid(int grid, int nw)
+{
+    if (grid <= 0) {
+        int dev = 0, sms = XCB_B200_SMS;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        grid = sms;
+    }
+    return grid > nw ? nw : grid;
+}
+
+extern "C" int xcb_ba_solve_windows_free_dev(const xcb_ba_windows* w, int Lt, int max_slots, int iters, double lam0,
+                                             double* stats, void* scratch, size_t scratch_bytes, int grid,
+                                             void* stream)
+{
+    if (!w || !stats || !scratch) return ba_fail(XCB_ERR_ARG, "ba_solve_windows_free: null argument");
+    if (w->nw <= 0) return XCB_OK;
+    if (max_slots < 1 || max_slots > xcb_ba_max_slots())
+        return ba_fail(XCB_ERR_CAPACITY, "ba_solve_windows_free: max_slots out of range (1..20)");
+    if (Lt < 0 || scratch_bytes < xcb_ba_newton_scratch_bytes(w->nw, Lt))
+        return ba_fail(XCB_ERR_CAPACITY, "ba_solve_windows_free: scratch smaller than xcb_ba_newton_scratch_bytes");
+    cudaStream_t st = (cudaStream_t)stream;
+    int* counter = (int*)scratch;
+    double* lsc = (double*)((char*)scratch + 256);
+    double* trial = lsc + (size_t)(Lt > 0 ? Lt : 1) * 19;
+    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), st);
+    if (e != cudaSuccess) return ba_fail(XCB_ERR_CUDA, cudaGetErrorString(e));
+    e = xcb_launch_ba_windows(*w, max_slots, iters, lam0, XCB_BA_FP64, stats, nullptr, 0, trial, counter,
+                              ba_grid(grid, w->nw), st, lsc);
+    if (e != cudaSuccess) return ba_fail(XCB_ERR_CUDA, cudaGetErrorString(e));
+    return XCB_OK;
 }
 
 extern "C" int xcb_ba_newton_windows_dev(const xcb_ba_windows* w, int max_slots, int mode, int steps, int maxit,
@@ -64,7 +99,8 @@ extern "C" int xcb_ba_newton_windows_dev(const xcb_ba_windows* w, int max_slots,
     if (w->nw <= 0) return XCB_OK;
     if (max_slots < 1 || max_slots > xcb_ba_max_slots())
         return ba_fail(XCB_ERR_CAPACITY, "ba_newton: max_slots out of range (1..20)");
-    if (mode != XCB_BA_NEWTON_POLISH && mode != XCB_BA_NEWTON_ADJOINT) return ba_fail(XCB_ERR_ARG, "ba_newton: mode");
+    if (mode != XCB_BA_NEWTON_POLISH && mode != XCB_BA_NEWTON_ADJOINT && mode != XCB_BA_NEWTON_POLISH_FIXED)
+        return ba_fail(XCB_ERR_ARG, "ba_newton: mode");
     if (mode == XCB_BA_NEWTON_ADJOINT && (!gpose || !gtheta)) return ba_fail(XCB_ERR_ARG, "ba_newton: adjoint outputs");
     if (steps < 0 || maxit < 1) return ba_fail(XCB_ERR_ARG, "ba_newton: steps / maxit");
     cudaStream_t st = (cudaStream_t)stream;
