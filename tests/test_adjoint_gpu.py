@@ -104,6 +104,36 @@ def test_newton_polish_reaches_a_stationary_point_where_the_lm_solve_stalls():
     assert BO.visual_cost(c) < cost_lm
 
 
+def test_constant_landmark_lm_holds_flagged_landmarks_and_reaches_a_lower_gradient():
+    """window.solve stalls on this seed (its positive-depth rule keeps a landmark in place while the Schur complement
+    assumes it moves); solve_free holds the flagged landmarks exactly and brings the gradient in the other variables
+    down, with a cost no higher than the LM's."""
+    import torch
+    from oracle import ba_oracle as BO
+    from xclean_b200.backend import synth_ba as S
+    from xclean_b200.backend.ba import BatchSolver
+    w = S.make_window(None, K=4, L=30, obs_min=2, obs_max=4, rng=np.random.default_rng(7), **_ext())
+    solver = BatchSolver([w], "cuda", hold=0)
+    solver.solve(100, 1e-4, "fp64")
+    st0 = solver.newton(0)
+    flags = solver.frozen()
+    assert bool(flags.any())
+    c = w.copy()
+    solver.unpack_into([c])
+    cost_lm = BO.visual_cost(c)
+    held = solver.t["lmp"][flags].clone()
+    fs = solver.solve_free(40)
+    torch.cuda.synchronize()
+    assert int(fs[0, 4]) == 0
+    assert torch.equal(solver.t["lmp"][flags], held)
+    st1 = solver.newton(0, flag=False)
+    assert float(st1[0, 2]) < 1e-3 * float(st0[0, 2]), (st0, st1)
+    solver.unpack_into([c])
+    assert BO.visual_cost(c) <= cost_lm
+    solver.reset()
+    assert not bool(solver.frozen().any())
+
+
 def test_adjoint_matches_central_finite_differences(run):
     import torch
     from oracle import ba_adjoint_ref as AR

@@ -112,6 +112,14 @@ class BatchSolver:
         if hasattr(self, "nscratch"):
             self.nscratch.zero_()
 
+    def frozen(self):
+        """-> bool tensor [Lt]: the landmarks flagged constant by newton() calls (all False before any)."""
+        Lt = int(self.host["lmp"].shape[0])
+        if not hasattr(self, "nscratch"):
+            return self.torch.zeros(Lt, dtype=self.torch.bool, device=self.dev)
+        lsc = self.nscratch[256:256 + 8 * 19 * Lt].view(self.torch.float64).view(Lt, 19)
+        return lsc[:, 18] != 0.0
+
     def _nscratch(self):
         if not hasattr(self, "nscratch"):
             nb = int(_lib.lib().xcb_ba_newton_scratch_bytes(self.nw, int(self.host["lmp"].shape[0])))
