@@ -185,45 +185,67 @@ cudaError_t xcb_launch_response(const uint8_t* img, int F, int H, int W, int dy_
 // ------------------------------------------------------------------------------------------------------------------
 // 2. noise floor: leaves of numpy's pairwise tree in parallel, then the tree level by level (one CTA per frame)
 // ------------------------------------------------------------------------------------------------------------------
-__device__ __forceinline__ float lap_abs(const u8* I, int W, long long k)
+// |Laplacian-like filter| at the pixel p points to (an integer, exact in float32)
+__device__ __forceinline__ float lap_abs_at(const u8* p, int W)
 {
-    int Wi = W - 2;
-    int y = 1 + (int)(k / Wi), x = 1 + (int)(k % Wi);
-    const u8* r0 = I + (size_t)(y - 1) * W + x;
-    const u8* r1 = r0 + W;
-    const u8* r2 = r1 + W;
-    int v = (int)r0[-1] - 2 * (int)r0[0] + (int)r0[1] - 2 * (int)r1[-1] + 4 * (int)r1[0] - 2 * (int)r1[1] + (int)r2[-1]
+    const u8* r0 = p - W;
+    const u8* r2 = p + W;
+    int v = (int)r0[-1] - 2 * (int)r0[0] + (int)r0[1] - 2 * (int)p[-1] + 4 * (int)p[0] - 2 * (int)p[1] + (int)r2[-1]
             - 2 * (int)r2[0] + (int)r2[1];
     return (float)(v < 0 ? -v : v);
 }
 
-__global__ void k_noise_leaves(const u8* __restrict__ imgs, int H, int W, const long long* __restrict__ lstart,
-                               const int* __restrict__ llen, int nleaf, int nnode, float* __restrict__ nodeval)
+#define NOISE_LEAF 128      // numpy's pairwise block: a leaf holds at most 128 elements
+#define NOISE_WARPS 8
+
+// one warp per leaf: the lanes evaluate the leaf's elements (consecutive interior pixels: coalesced rows) into shared
+// memory, then numpy's order inside a leaf: eight running sums over elements j, j + 8, ... (lane j), combined as
+// ((r0 + r1) + (r2 + r3)) + ((r4 + r5) + (r6 + r7)), then the tail; fewer than 8 elements: one sequential sum
+__global__ void __launch_bounds__(NOISE_WARPS * 32) k_noise_leaves(const u8* __restrict__ imgs, int H, int W,
+                                                                   const long long* __restrict__ lstart,
+                                                                   const int* __restrict__ llen, int nleaf,
+                                                                   int nnode, float* __restrict__ nodeval)
 {
-    int l = blockIdx.x * blockDim.x + threadIdx.x;
-    int f = blockIdx.y;
+    __shared__ float ev[NOISE_WARPS][NOISE_LEAF];
+    const int wl = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int l = blockIdx.x * NOISE_WARPS + wl;
+    const int f = blockIdx.y;
     if (l >= nleaf) return;
     const u8* I = imgs + (size_t)f * H * W;
-    long long st = lstart[l];
-    int n = llen[l];
-    float res;
-    if (n < 8) {
-        res = -0.0f;
-        for (int i = 0; i < n; ++i) res = __fadd_rn(res, lap_abs(I, W, st + i));
-    } else {
-        float r[8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) r[j] = lap_abs(I, W, st + j);
-        int i = 8, lim = n - (n % 8);
-        for (; i < lim; i += 8) {
-#pragma unroll
-            for (int j = 0; j < 8; ++j) r[j] = __fadd_rn(r[j], lap_abs(I, W, st + i + j));
-        }
-        res = __fadd_rn(__fadd_rn(__fadd_rn(r[0], r[1]), __fadd_rn(r[2], r[3])),
-                        __fadd_rn(__fadd_rn(r[4], r[5]), __fadd_rn(r[6], r[7])));
-        for (; i < n; ++i) res = __fadd_rn(res, lap_abs(I, W, st + i));
+    const long long st = lstart[l];
+    const int n = min(llen[l], NOISE_LEAF);
+    const int wi = W - 2;
+    const int y0 = 1 + (int)(st / wi), x0 = (int)(st % wi);
+    float* e = ev[wl];
+    for (int i = lane; i < n; i += 32) {
+        int xx = x0 + i, y = y0;
+        while (xx >= wi) { xx -= wi; ++y; }
+        e[i] = lap_abs_at(I + (size_t)y * W + 1 + xx, W);
     }
-    nodeval[(size_t)f * nnode + l] = res;
+    __syncwarp();
+    float res = 0.0f;
+    if (n < 8) {
+        if (lane == 0) {
+            res = -0.0f;
+            for (int i = 0; i < n; ++i) res = __fadd_rn(res, e[i]);
+        }
+    } else {
+        const int lim = n - (n % 8);
+        float r = 0.0f;
+        if (lane < 8) {
+            r = e[lane];
+            for (int i = 8 + lane; i < lim; i += 8) r = __fadd_rn(r, e[i]);
+        }
+        float q[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) q[j] = __shfl_sync(0xffffffffu, r, j);
+        if (lane == 0) {
+            res = __fadd_rn(__fadd_rn(__fadd_rn(q[0], q[1]), __fadd_rn(q[2], q[3])),
+                            __fadd_rn(__fadd_rn(q[4], q[5]), __fadd_rn(q[6], q[7])));
+            for (int i = lim; i < n; ++i) res = __fadd_rn(res, e[i]);
+        }
+    }
+    if (lane == 0) nodeval[(size_t)f * nnode + l] = res;
 }
 
 __global__ void k_noise_tree(float* __restrict__ nodeval, int nnode, const int* __restrict__ left,
@@ -247,8 +269,8 @@ __global__ void k_noise_tree(float* __restrict__ nodeval, int nnode, const int* 
 cudaError_t xcb_launch_noise(const uint8_t* img, int F, int H, int W, const XcbNoiseTree& t, float* nodeval,
                              double K, double Q, double* floor_d, float* floor_f, cudaStream_t st)
 {
-    dim3 g1((t.nleaf + 127) / 128, F);
-    k_noise_leaves<<<g1, 128, 0, st>>>(img, H, W, t.lstart, t.llen, t.nleaf, t.nnode, nodeval);
+    dim3 g1((t.nleaf + NOISE_WARPS - 1) / NOISE_WARPS, F);
+    k_noise_leaves<<<g1, NOISE_WARPS * 32, 0, st>>>(img, H, W, t.lstart, t.llen, t.nleaf, t.nnode, nodeval);
     k_noise_tree<<<F, 1024, 0, st>>>(nodeval, t.nnode, t.left, t.right, t.lvl, t.nlvl, t.root, K, Q, floor_d, floor_f);
     return cudaGetLastError();
 }
