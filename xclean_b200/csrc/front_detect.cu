@@ -305,62 +305,67 @@ __global__ void k_cellmax(const float* __restrict__ Rall, int H, int W, int c, i
     }
 }
 
-// one warp per greedy cell: candidates (3x3 local max, >= cell threshold, >= noise floor, inside the border) into the
-// cell's list, then ranked (keys are unique) into the sorted list
-__global__ void k_cell_candidates(const float* __restrict__ Rall, int H, int W, int b, int ncx, int ncell,
-                                  const int* __restrict__ ybeg, const int* __restrict__ xbeg,
-                                  const int* __restrict__ coff, int c, int gwc, int ghc, const float* __restrict__ thr,
-                                  const float* __restrict__ floor_f, const int* __restrict__ anypos, u64* raw,
-                                  u64* __restrict__ sorted, int* __restrict__ ccount, long long list_stride)
+// candidates (3x3 local max of the response, >= its threshold cell's 0.01 max, >= the noise floor, inside the border):
+// one CTA per (greedy cell row, frame), threads over columns so every row is read coalesced; a candidate is appended
+// to its cell's list through a shared-memory counter, then each cell's list (keys are unique) is ranked into the
+// sorted list (one warp per cell)
+#define CAND_T 256
+#define CAND_MAXCX 1024
+__global__ void __launch_bounds__(CAND_T) k_cell_candidates(const float* __restrict__ Rall, int H, int W, int b, int ncx,
+                                                            int ncell, const int* __restrict__ ybeg,
+                                                            const int* __restrict__ xbeg, const int* __restrict__ coff,
+                                                            int c, int gwc, int ghc, const float* __restrict__ thr,
+                                                            const float* __restrict__ floor_f,
+                                                            const int* __restrict__ anypos, u64* raw,
+                                                            u64* __restrict__ sorted, int* __restrict__ ccount,
+                                                            long long list_stride)
 {
-    const int cell = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    const int f = blockIdx.y;
-    if (cell >= ncell) return;
-    int* cnt_out = ccount + (size_t)f * ncell + cell;
-    if (!anypos[f]) {               // rmax <= 0: no candidates (Frontend._response)
-        if (lane == 0) *cnt_out = 0;
-        return;
-    }
-    const float* R = Rall + (size_t)f * H * W;
-    const float* T = thr + (size_t)f * gwc * ghc;
-    const float fl = floor_f[f];
-    int cy = cell / ncx, cx = cell % ncx;
-    int ya = max(ybeg[cy], b), yb = min(ybeg[cy + 1], H - b);
-    int xa = max(xbeg[cx], b), xb = min(xbeg[cx + 1], W - b);
-    u64* lraw = raw + (size_t)f * list_stride + coff[cell];
-    u64* lsorted = sorted + (size_t)f * list_stride + coff[cell];
-    int n = 0;
-    if (ya < yb && xa < xb) {
-        int w = xb - xa, np = w * (yb - ya);
-        for (int p0 = 0; p0 < np; p0 += 32) {
-            int p = p0 + lane;
-            bool cand = false;
-            u64 key = 0;
-            if (p < np) {
-                int y = ya + p / w, x = xa + p % w;
+    __shared__ int cnt[CAND_MAXCX];
+    __shared__ int sxb[CAND_MAXCX + 1];
+    const int cy = blockIdx.x, f = blockIdx.y, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    for (int i = tid; i < ncx; i += CAND_T) cnt[i] = 0;
+    for (int i = tid; i <= ncx; i += CAND_T) sxb[i] = xbeg[i];
+    __syncthreads();
+    const int c0 = cy * ncx;
+    u64* fraw = raw + (size_t)f * list_stride;
+    if (anypos[f]) {               // rmax <= 0: no candidates (Frontend._response)
+        const float* R = Rall + (size_t)f * H * W;
+        const float* T = thr + (size_t)f * gwc * ghc;
+        const float fl = floor_f[f];
+        const int ya = max(ybeg[cy], b), yb = min(ybeg[cy + 1], H - b);
+        for (int x = b + tid; x < W - b; x += CAND_T) {
+            int lo = 0, hi = ncx - 1;            // the cell column holding x: the last start <= x
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (sxb[mid] <= x) lo = mid; else hi = mid - 1;
+            }
+            const int tx = x / c;
+            u64* lraw = fraw + coff[c0 + lo];
+            for (int y = ya; y < yb; ++y) {
                 const float* q = R + (size_t)y * W + x;
-                float v = q[0];
+                const float v = q[0];
                 float m = v;
 #pragma unroll
                 for (int dy = -1; dy <= 1; ++dy)
 #pragma unroll
                     for (int dx = -1; dx <= 1; ++dx) m = fmaxf(m, q[dy * W + dx]);
-                cand = (v >= m) && (v >= T[(y / c) * gwc + x / c]) && (v >= fl);
-                key = xcb_key(v, y, x);
+                if (v >= m && v >= T[(y / c) * gwc + tx] && v >= fl) lraw[atomicAdd(&cnt[lo], 1)] = xcb_key(v, y, x);
             }
-            unsigned bal = __ballot_sync(0xffffffffu, cand);
-            if (cand) lraw[n + __popc(bal & ((1u << lane) - 1u))] = key;
-            n += __popc(bal);
         }
     }
-    __syncwarp();
-    for (int i = lane; i < n; i += 32) {
-        u64 k = lraw[i];
-        int rank = 0;
-        for (int j = 0; j < n; ++j) rank += lraw[j] > k;
-        lsorted[rank] = k;
+    __syncthreads();
+    for (int cx = wid; cx < ncx; cx += CAND_T / 32) {
+        const int cell = c0 + cx, n = cnt[cx];
+        const u64* lraw = fraw + coff[cell];
+        u64* ls = sorted + (size_t)f * list_stride + coff[cell];
+        for (int i = lane; i < n; i += 32) {
+            const u64 k = lraw[i];
+            int rank = 0;
+            for (int j = 0; j < n; ++j) rank += lraw[j] > k;
+            ls[rank] = k;
+        }
+        if (lane == 0) ccount[(size_t)f * ncell + cell] = n;
     }
-    if (lane == 0) *cnt_out = n;
 }
 
 cudaError_t xcb_launch_candidates(const float* R, int F, int H, int W, const XcbDetectGeom& g, const float* floor_f,
@@ -370,9 +375,10 @@ cudaError_t xcb_launch_candidates(const float* R, int F, int H, int W, const Xcb
     int nthr = g.gwc * g.ghc;
     dim3 g1((nthr * 32 + 127) / 128, F);
     k_cellmax<<<g1, 128, 0, st>>>(R, H, W, g.c, g.gwc, g.ghc, thr);
-    dim3 g2((g.ncell * 32 + 127) / 128, F);
-    k_cell_candidates<<<g2, 128, 0, st>>>(R, H, W, g.border, g.ncx, g.ncell, g.ybeg, g.xbeg, g.coff, g.c, g.gwc, g.ghc,
-                                          thr, floor_f, anypos, raw, sorted, ccount, (long long)H * W);
+    if (g.ncx > CAND_MAXCX) return cudaErrorInvalidValue;
+    dim3 g2(g.gh, F);
+    k_cell_candidates<<<g2, CAND_T, 0, st>>>(R, H, W, g.border, g.ncx, g.ncell, g.ybeg, g.xbeg, g.coff, g.c, g.gwc,
+                                             g.ghc, thr, floor_f, anypos, raw, sorted, ccount, (long long)H * W);
     return cudaGetLastError();
 }
 
