@@ -56,7 +56,7 @@ typedef struct {
 } xcb_front_bufs;
 
 /* GpuFront.__init__ (gpu_front.py:1076-1198): all device and pinned buffers for W x H frames, `cap` keypoints per
-   frame, up to `max_frames` frames per batched call; one stream. */
+   frame, up to `max_frames` frames per batched call; one stream.  48 <= width <= 8192, 48 <= height <= 65535. */
 int xcb_front_create(int width, int height, int cap, int max_frames, xcb_front** out);
 /* GpuFront teardown / release_device (gpu_front.py:1653-1686): frees every buffer; the CUDA context is kept. */
 void xcb_front_destroy(xcb_front* f);

@@ -319,8 +319,8 @@ extern "C" int xcb_front_create(int width, int height, int cap, int max_frames, 
 {
     if (!out) return fail(nullptr, XCB_ERR_ARG, "create: out is NULL");
     *out = nullptr;
-    if (width < 48 || height < 48 || width > 0xFFFF || height > 0xFFFF || cap < 1 || cap > 65536 || max_frames < 1)
-        return fail(nullptr, XCB_ERR_ARG, "create: bad size");
+    if (width < 48 || height < 48 || width > 8192 || height > 0xFFFF || cap < 1 || cap > 65536 || max_frames < 1)
+        return fail(nullptr, XCB_ERR_ARG, "create: bad size (48 <= width <= 8192, 48 <= height <= 65535)");
     xcb_front* f = new xcb_front();
     f->W = width; f->H = height; f->cap = cap; f->maxF = max_frames;
     f->Hp = height + 64; f->Wp = width + 64;

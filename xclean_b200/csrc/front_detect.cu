@@ -278,30 +278,29 @@ cudaError_t xcb_launch_noise(const uint8_t* img, int F, int H, int W, const XcbN
 // ------------------------------------------------------------------------------------------------------------------
 // 3. thresholds (0.01 x the c x c cell max of the zero-padded response) and the per-cell candidate lists
 // ------------------------------------------------------------------------------------------------------------------
-__global__ void k_cellmax(const float* __restrict__ Rall, int H, int W, int c, int gwc, int ghc,
-                          float* __restrict__ thr)
+// one CTA per threshold-cell row: column maxima over the row's c image rows (coalesced), then one thread per cell;
+// a cell reaching past the image (the zero pad) also takes max(., 0)
+#define CMAX_T 256
+#define CMAX_MAXW 8192
+__global__ void __launch_bounds__(CMAX_T) k_cellmax(const float* __restrict__ Rall, int H, int W, int c, int gwc,
+                                                    int ghc, float* __restrict__ thr)
 {
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    const int f = blockIdx.y;
-    if (warp >= gwc * ghc) return;
+    __shared__ float colmax[CMAX_MAXW];
+    const int gy = blockIdx.x, f = blockIdx.y, tid = threadIdx.x;
     const float* R = Rall + (size_t)f * H * W;
-    int gy = warp / gwc, gx = warp % gwc;
-    int y0 = gy * c, x0 = gx * c;
-    float m = -CUDART_INF_F;
-    int pad = 0;
-    for (int p = lane; p < c * c; p += 32) {
-        int y = y0 + p / c, x = x0 + p % c;
-        if (y < H && x < W) m = fmaxf(m, R[(size_t)y * W + x]);
-        else pad = 1;
+    const int y0 = gy * c, y1 = min(y0 + c, H);
+    for (int x = tid; x < W; x += CMAX_T) {
+        float m = -CUDART_INF_F;
+        for (int y = y0; y < y1; ++y) m = fmaxf(m, R[(size_t)y * W + x]);
+        colmax[x] = m;
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-        pad |= __shfl_xor_sync(0xffffffffu, pad, o);
-    }
-    if (lane == 0) {
-        if (pad) m = fmaxf(m, 0.0f);
-        thr[(size_t)f * gwc * ghc + warp] = __fmul_rn(0.01f, m);
+    __syncthreads();
+    for (int gx = tid; gx < gwc; gx += CMAX_T) {
+        const int x0 = gx * c, x1 = min(x0 + c, W);
+        float m = -CUDART_INF_F;
+        for (int x = x0; x < x1; ++x) m = fmaxf(m, colmax[x]);
+        if (y0 + c > H || x0 + c > W) m = fmaxf(m, 0.0f);
+        thr[(size_t)f * gwc * ghc + (size_t)gy * gwc + gx] = __fmul_rn(0.01f, m);
     }
 }
 
@@ -372,9 +371,9 @@ cudaError_t xcb_launch_candidates(const float* R, int F, int H, int W, const Xcb
                                   const int* anypos, float* thr, unsigned long long* raw, unsigned long long* sorted,
                                   int* ccount, cudaStream_t st)
 {
-    int nthr = g.gwc * g.ghc;
-    dim3 g1((nthr * 32 + 127) / 128, F);
-    k_cellmax<<<g1, 128, 0, st>>>(R, H, W, g.c, g.gwc, g.ghc, thr);
+    if (W > CMAX_MAXW) return cudaErrorInvalidValue;
+    dim3 g1(g.ghc, F);
+    k_cellmax<<<g1, CMAX_T, 0, st>>>(R, H, W, g.c, g.gwc, g.ghc, thr);
     if (g.ncx > CAND_MAXCX) return cudaErrorInvalidValue;
     dim3 g2(g.gh, F);
     k_cell_candidates<<<g2, CAND_T, 0, st>>>(R, H, W, g.border, g.ncx, g.ncell, g.ybeg, g.xbeg, g.coff, g.c, g.gwc,
