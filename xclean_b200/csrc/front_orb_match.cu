@@ -12,8 +12,8 @@
 //
 // B200 layout: the blur is one tiled kernel (u8 tile + halo staged in shared memory, the row pass kept in shared
 // memory as float32, only the u8 result written), so the reference's (H+64) x (W+64) float32 intermediate never
-// reaches HBM.  Descriptors are read as 16-byte vectors; each Hamming CTA streams the train descriptors through shared
-// memory once for 128 query rows.
+// reaches HBM.  The Hamming distances are int8 tensor-core products of +-1 expanded descriptors; each CTA expands the
+// train descriptors into shared memory once for 128 query rows, and the row and column minima come from one pass.
 #include "common.cuh"
 #include "front_kernels.h"
 
@@ -122,61 +122,133 @@ cudaError_t xcb_launch_orb(const uint8_t* blur, int F, int Hp, int Wp, const flo
 }
 
 // ------------------------------------------------------------------------------------------------------------------
-// Hamming, one pass over the distance matrix: a thread owns a query row and scans the train descriptors (staged in
-// shared memory, read as broadcasts) in increasing index with the CPU's update (strictly smaller replaces the best),
-// which gives best / second / first index directly.  The column side (each train descriptor's first-minimum query)
-// reuses the same distances: (distance << 16 | query) packed so that an unsigned minimum picks the smallest distance
-// and, among equal distances, the smallest query index; a warp reduces its 32 rows with redux.sync, the CTA in
-// shared memory, the row blocks of a pair with one global atomicMin per column and block.
+// Hamming, one pass over the distance matrix: per query row the best / second / first index of the best (the CPU's
+// sequential scan), per train column the first-minimum query, both from the same distances.
 // ------------------------------------------------------------------------------------------------------------------
-#define HAM_T 128
-#define HAM_CHUNK 1024
+// The distance is a dot product of +-1 vectors, hamming = (256 - a.b) / 2, so
+// legacy int8 mma.m16n8k32 (native on this part, unlike the single-bit XOR-popc form) gives a 16 x 8 block of
+// distances per 8 instructions.  A warp owns 16 query rows (their +-1 expansion held in registers); a CTA expands a
+// chunk of 128 train descriptors once into shared memory for its 8 warps.  Fragments (PTX ISA, m16n8k32 .s8): a0 / a2
+// = row g, k = 4q.. / 16 + 4q..; a1 / a3 = row g + 8; b0 / b1 = column g, k = 4q.. / 16 + 4q..; d0, d1 = row g,
+// columns 2q, 2q + 1; d2, d3 = row g + 8 (g = lane / 4, q = lane % 4).  In k-step ks, descriptor nibble 8 ks + q feeds
+// the first half and nibble 8 ks + 4 + q the second, in the same order for queries and trains.  Rows: each lane scans
+// its columns in increasing order with the CPU's update, then the four lanes of a row merge (ties to the smaller
+// index).  Columns: packed (distance << 16 | query) minima over the warp's 16 rows by shuffles, over the CTA in shared
+// memory, over the row blocks by global atomicMin.
+#define HTC_WARPS 8
+#define HTC_CHUNK 128
+#define HTC_BSTRIDE 272     // bytes per expanded train descriptor: word 8 ks + q of column g hits bank (4 g + q + 8 ks) % 32
 
-__device__ __forceinline__ int ham4(const ulonglong2 a0, const ulonglong2 a1, const ulonglong2 b0,
-                                    const ulonglong2 b1)
+// 4 descriptor bits -> 4 int8: +1 where the bit is set, -1 elsewhere
+__device__ __forceinline__ unsigned pm1_nibble(unsigned nib)
 {
-    return __popcll(a0.x ^ b0.x) + __popcll(a0.y ^ b0.y) + __popcll(a1.x ^ b1.x) + __popcll(a1.y ^ b1.y);
+    return ~(((nib * 0x00204081u) & 0x01010101u) * 0xFEu);
 }
 
-__global__ void __launch_bounds__(HAM_T) k_hamming(const u8* __restrict__ A, const u8* __restrict__ B,
-                                                   long long strideA, long long strideB, const int* __restrict__ LA,
-                                                   const int* __restrict__ NB, int maxL, int maxN,
-                                                   int* __restrict__ o1, int* __restrict__ o2, int* __restrict__ oi,
-                                                   unsigned* __restrict__ colmin)
+__device__ __forceinline__ void ham_take(int d, int j, int& b1, int& bi, int& b2)
 {
-    __shared__ ulonglong2 sb[HAM_CHUNK][2];
-    __shared__ unsigned cm[HAM_CHUNK];
+    if (d < b1) { b2 = b1; b1 = d; bi = j; }
+    else if (d < b2) b2 = d;
+}
+
+// merge the (best, index, second) of lane ^ off: the smaller best wins, ties to the smaller index
+__device__ __forceinline__ void ham_merge(int& b1, int& bi, int& b2, int off)
+{
+    const int c1 = __shfl_xor_sync(0xffffffffu, b1, off);
+    const int ci = __shfl_xor_sync(0xffffffffu, bi, off);
+    const int c2 = __shfl_xor_sync(0xffffffffu, b2, off);
+    if (c1 < b1 || (c1 == b1 && ci >= 0 && (bi < 0 || ci < bi))) {
+        b2 = min(b1, c2); b1 = c1; bi = ci;
+    } else {
+        b2 = min(b2, c1);
+    }
+}
+
+__global__ void __launch_bounds__(HTC_WARPS * 32) k_hamming_tc(const u8* __restrict__ A, const u8* __restrict__ B,
+                                                              long long strideA, long long strideB,
+                                                              const int* __restrict__ LA, const int* __restrict__ NB,
+                                                              int maxL, int maxN, int* __restrict__ o1,
+                                                              int* __restrict__ o2, int* __restrict__ oi,
+                                                              unsigned* __restrict__ colmin)
+{
+    __shared__ __align__(16) unsigned char sB[HTC_CHUNK * HTC_BSTRIDE];
+    __shared__ unsigned cm[HTC_CHUNK];
     const int p = blockIdx.y;
     const int L = LA[p], N = NB[p];
-    if (blockIdx.x * HAM_T >= L) return;
-    const int i = blockIdx.x * HAM_T + threadIdx.x, lane = threadIdx.x & 31;
-    const bool act = i < L;
-    const ulonglong2* Ap = (const ulonglong2*)(A + p * strideA);
-    const ulonglong2* Bp = (const ulonglong2*)(B + p * strideB);
-    ulonglong2 a0 = make_ulonglong2(0, 0), a1 = a0;
-    if (act) { a0 = Ap[2 * i]; a1 = Ap[2 * i + 1]; }
-    int b1 = 1 << 30, b2 = 1 << 30, bi = -1;
+    const int rb = blockIdx.x * 16 * HTC_WARPS;
+    if (rb >= L) return;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, g = lane >> 2, q = lane & 3;
+    const int r0 = rb + 16 * w + g, r1 = r0 + 8;
+    // the warp's 16 query rows as +-1 fragments (rows past L: any values, never reported)
+    unsigned a0[8], a1[8], a2[8], a3[8];
+    {
+        const uint4* Ap = (const uint4*)(A + p * strideA);
+        uint4 x0 = make_uint4(0u, 0u, 0u, 0u), x1 = x0, y0 = x0, y1 = x0;
+        if (r0 < L) { x0 = __ldg(Ap + 2 * r0); x1 = __ldg(Ap + 2 * r0 + 1); }
+        if (r1 < L) { y0 = __ldg(Ap + 2 * r1); y1 = __ldg(Ap + 2 * r1 + 1); }
+        const unsigned xr[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+        const unsigned yr[8] = {y0.x, y0.y, y0.z, y0.w, y1.x, y1.y, y1.z, y1.w};
+#pragma unroll
+        for (int ks = 0; ks < 8; ++ks) {       // descriptor word ks holds nibbles 8 ks .. 8 ks + 7
+            a0[ks] = pm1_nibble((xr[ks] >> (4 * q)) & 0xFu);
+            a2[ks] = pm1_nibble((xr[ks] >> (4 * q + 16)) & 0xFu);
+            a1[ks] = pm1_nibble((yr[ks] >> (4 * q)) & 0xFu);
+            a3[ks] = pm1_nibble((yr[ks] >> (4 * q + 16)) & 0xFu);
+        }
+    }
+    int b1r0 = 1 << 30, b2r0 = 1 << 30, bir0 = -1, b1r1 = 1 << 30, b2r1 = 1 << 30, bir1 = -1;
+    const unsigned pk0 = r0 < L ? (unsigned)r0 : 0xffffffffu, pk1 = r1 < L ? (unsigned)r1 : 0xffffffffu;
+    const unsigned* Bw = (const unsigned*)(B + p * strideB);
     unsigned* cg = colmin + (size_t)p * maxN;
-    for (int j0 = 0; j0 < N; j0 += HAM_CHUNK) {
-        const int nj = min(HAM_CHUNK, N - j0);
+    for (int j0 = 0; j0 < N; j0 += HTC_CHUNK) {
+        const int nj = min(HTC_CHUNK, N - j0), njp = (nj + 7) & ~7;
         __syncthreads();
-        for (int t = threadIdx.x; t < 2 * nj; t += HAM_T) sb[t >> 1][t & 1] = Bp[2 * j0 + t];
-        for (int t = threadIdx.x; t < nj; t += HAM_T) cm[t] = 0xffffffffu;
+        for (int t = tid; t < njp * 64; t += HTC_WARPS * 32) {      // (descriptor, nibble) -> one expanded word
+            const int jj = t >> 6, nb = t & 63;
+            const unsigned word = jj < nj ? __ldg(Bw + 8 * (j0 + jj) + (nb >> 3)) : 0u;
+            ((unsigned*)(sB + jj * HTC_BSTRIDE))[nb] = pm1_nibble((word >> (4 * (nb & 7))) & 0xFu);
+        }
+        for (int t = tid; t < HTC_CHUNK; t += HTC_WARPS * 32) cm[t] = 0xffffffffu;
         __syncthreads();
-        for (int j = 0; j < nj; ++j) {
-            const int d = ham4(a0, a1, sb[j][0], sb[j][1]);
-            if (d < b1) { b2 = b1; b1 = d; bi = j0 + j; }
-            else if (d < b2) b2 = d;
-            const unsigned wm = __reduce_min_sync(0xffffffffu, act ? ((unsigned)d << 16) | (unsigned)i : 0xffffffffu);
-            if (lane == 0 && wm != 0xffffffffu) atomicMin(&cm[j], wm);
+        for (int jt = 0; jt < njp; jt += 8) {
+            const unsigned* bw = (const unsigned*)(sB + (jt + g) * HTC_BSTRIDE);
+            int d0 = 0, d1 = 0, d2 = 0, d3 = 0;
+#pragma unroll
+            for (int ks = 0; ks < 8; ++ks) {
+                const unsigned b0 = bw[8 * ks + q], bb1 = bw[8 * ks + 4 + q];
+                asm("mma.sync.aligned.m16n8k32.row.col.s32.s8.s8.s32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+                    "{%0,%1,%2,%3};"
+                    : "+r"(d0), "+r"(d1), "+r"(d2), "+r"(d3)
+                    : "r"(a0[ks]), "r"(a1[ks]), "r"(a2[ks]), "r"(a3[ks]), "r"(b0), "r"(bb1));
+            }
+            d0 = (256 - d0) >> 1; d1 = (256 - d1) >> 1; d2 = (256 - d2) >> 1; d3 = (256 - d3) >> 1;
+            const int jA = j0 + jt + 2 * q;
+            const bool vA = jA < N, vB = jA + 1 < N;
+            if (vA) { ham_take(d0, jA, b1r0, bir0, b2r0); ham_take(d2, jA, b1r1, bir1, b2r1); }
+            if (vB) { ham_take(d1, jA + 1, b1r0, bir0, b2r0); ham_take(d3, jA + 1, b1r1, bir1, b2r1); }
+            unsigned mA = min(pk0 == 0xffffffffu ? pk0 : ((unsigned)d0 << 16) | pk0,
+                              pk1 == 0xffffffffu ? pk1 : ((unsigned)d2 << 16) | pk1);
+            unsigned mB = min(pk0 == 0xffffffffu ? pk0 : ((unsigned)d1 << 16) | pk0,
+                              pk1 == 0xffffffffu ? pk1 : ((unsigned)d3 << 16) | pk1);
+#pragma unroll
+            for (int o = 4; o < 32; o <<= 1) {
+                mA = min(mA, __shfl_xor_sync(0xffffffffu, mA, o));
+                mB = min(mB, __shfl_xor_sync(0xffffffffu, mB, o));
+            }
+            if (g == 0) {
+                if (vA && mA != 0xffffffffu) atomicMin(&cm[jt + 2 * q], mA);
+                if (vB && mB != 0xffffffffu) atomicMin(&cm[jt + 2 * q + 1], mB);
+            }
         }
         __syncthreads();
-        for (int t = threadIdx.x; t < nj; t += HAM_T)
+        for (int t = tid; t < nj; t += HTC_WARPS * 32)
             if (cm[t] != 0xffffffffu) atomicMin(&cg[j0 + t], cm[t]);
     }
-    if (act) {
-        const size_t o = (size_t)p * maxL + i;
-        o1[o] = b1; o2[o] = b2; oi[o] = bi;
+    ham_merge(b1r0, bir0, b2r0, 1); ham_merge(b1r0, bir0, b2r0, 2);
+    ham_merge(b1r1, bir1, b2r1, 1); ham_merge(b1r1, bir1, b2r1, 2);
+    if (q == 0) {
+        if (r0 < L) { const size_t o = (size_t)p * maxL + r0; o1[o] = b1r0; o2[o] = b2r0; oi[o] = bir0; }
+        if (r1 < L) { const size_t o = (size_t)p * maxL + r1; o1[o] = b1r1; o2[o] = b2r1; oi[o] = bir1; }
     }
 }
 
@@ -188,9 +260,9 @@ cudaError_t xcb_launch_hamming(const XcbHamPairs& p, int* b1, int* b2, int* bi, 
         if (e != cudaSuccess) return e;
     }
     if (p.maxL > 0) {
-        dim3 gr((p.maxL + HAM_T - 1) / HAM_T, p.npair);
-        k_hamming<<<gr, HAM_T, 0, st>>>(p.A, p.B, p.strideA, p.strideB, p.LA, p.NB, p.maxL, p.maxN, b1, b2, bi,
-                                        (unsigned*)ci);
+        dim3 gr((p.maxL + 16 * HTC_WARPS - 1) / (16 * HTC_WARPS), p.npair);
+        k_hamming_tc<<<gr, HTC_WARPS * 32, 0, st>>>(p.A, p.B, p.strideA, p.strideB, p.LA, p.NB, p.maxL, p.maxN, b1, b2,
+                                                    bi, (unsigned*)ci);
     }
     return cudaGetLastError();
 }
