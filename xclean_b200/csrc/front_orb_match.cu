@@ -145,24 +145,29 @@ __device__ __forceinline__ unsigned pm1_nibble(unsigned nib)
     return ~(((nib * 0x00204081u) & 0x01010101u) * 0xFEu);
 }
 
-__device__ __forceinline__ void ham_take(int d, int j, int& b1, int& bi, int& b2)
+// the row state is kept on dot products (distance = (256 - dot) / 2 falls as the dot rises): the CPU's update
+// (a strictly smaller distance replaces the best) is a strictly larger dot
+#define HTC_NONE (-(1 << 30))
+__device__ __forceinline__ void ham_take(int dot, int j, int& b1, int& bi, int& b2)
 {
-    if (d < b1) { b2 = b1; b1 = d; bi = j; }
-    else if (d < b2) b2 = d;
+    if (dot > b1) { b2 = b1; b1 = dot; bi = j; }
+    else if (dot > b2) b2 = dot;
 }
 
-// merge the (best, index, second) of lane ^ off: the smaller best wins, ties to the smaller index
+// merge the (best, index, second) of lane ^ off: the larger best dot wins, ties to the smaller index
 __device__ __forceinline__ void ham_merge(int& b1, int& bi, int& b2, int off)
 {
     const int c1 = __shfl_xor_sync(0xffffffffu, b1, off);
     const int ci = __shfl_xor_sync(0xffffffffu, bi, off);
     const int c2 = __shfl_xor_sync(0xffffffffu, b2, off);
-    if (c1 < b1 || (c1 == b1 && ci >= 0 && (bi < 0 || ci < bi))) {
-        b2 = min(b1, c2); b1 = c1; bi = ci;
+    if (c1 > b1 || (c1 == b1 && ci >= 0 && (bi < 0 || ci < bi))) {
+        b2 = max(b1, c2); b1 = c1; bi = ci;
     } else {
-        b2 = min(b2, c1);
+        b2 = max(b2, c1);
     }
 }
+
+__device__ __forceinline__ int ham_of_dot(int dot) { return dot == HTC_NONE ? 1 << 30 : (256 - dot) >> 1; }
 
 __global__ void __launch_bounds__(HTC_WARPS * 32) k_hamming_tc(const u8* __restrict__ A, const u8* __restrict__ B,
                                                               long long strideA, long long strideB,
@@ -196,7 +201,8 @@ __global__ void __launch_bounds__(HTC_WARPS * 32) k_hamming_tc(const u8* __restr
             a3[ks] = pm1_nibble((yr[ks] >> (4 * q + 16)) & 0xFu);
         }
     }
-    int b1r0 = 1 << 30, b2r0 = 1 << 30, bir0 = -1, b1r1 = 1 << 30, b2r1 = 1 << 30, bir1 = -1;
+    int b1r0 = HTC_NONE, b2r0 = HTC_NONE, bir0 = -1, b1r1 = HTC_NONE, b2r1 = HTC_NONE, bir1 = -1;
+    // column keys: distance << 16 | query = (256 - dot) << 15 | query; a row past L keys all ones (never the minimum)
     const unsigned pk0 = r0 < L ? (unsigned)r0 : 0xffffffffu, pk1 = r1 < L ? (unsigned)r1 : 0xffffffffu;
     const unsigned* Bw = (const unsigned*)(B + p * strideB);
     unsigned* cg = colmin + (size_t)p * maxN;
@@ -221,15 +227,12 @@ __global__ void __launch_bounds__(HTC_WARPS * 32) k_hamming_tc(const u8* __restr
                     : "+r"(d0), "+r"(d1), "+r"(d2), "+r"(d3)
                     : "r"(a0[ks]), "r"(a1[ks]), "r"(a2[ks]), "r"(a3[ks]), "r"(b0), "r"(bb1));
             }
-            d0 = (256 - d0) >> 1; d1 = (256 - d1) >> 1; d2 = (256 - d2) >> 1; d3 = (256 - d3) >> 1;
             const int jA = j0 + jt + 2 * q;
             const bool vA = jA < N, vB = jA + 1 < N;
             if (vA) { ham_take(d0, jA, b1r0, bir0, b2r0); ham_take(d2, jA, b1r1, bir1, b2r1); }
             if (vB) { ham_take(d1, jA + 1, b1r0, bir0, b2r0); ham_take(d3, jA + 1, b1r1, bir1, b2r1); }
-            unsigned mA = min(pk0 == 0xffffffffu ? pk0 : ((unsigned)d0 << 16) | pk0,
-                              pk1 == 0xffffffffu ? pk1 : ((unsigned)d2 << 16) | pk1);
-            unsigned mB = min(pk0 == 0xffffffffu ? pk0 : ((unsigned)d1 << 16) | pk0,
-                              pk1 == 0xffffffffu ? pk1 : ((unsigned)d3 << 16) | pk1);
+            unsigned mA = min(((unsigned)(256 - d0) << 15) | pk0, ((unsigned)(256 - d2) << 15) | pk1);
+            unsigned mB = min(((unsigned)(256 - d1) << 15) | pk0, ((unsigned)(256 - d3) << 15) | pk1);
 #pragma unroll
             for (int o = 4; o < 32; o <<= 1) {
                 mA = min(mA, __shfl_xor_sync(0xffffffffu, mA, o));
@@ -247,8 +250,14 @@ __global__ void __launch_bounds__(HTC_WARPS * 32) k_hamming_tc(const u8* __restr
     ham_merge(b1r0, bir0, b2r0, 1); ham_merge(b1r0, bir0, b2r0, 2);
     ham_merge(b1r1, bir1, b2r1, 1); ham_merge(b1r1, bir1, b2r1, 2);
     if (q == 0) {
-        if (r0 < L) { const size_t o = (size_t)p * maxL + r0; o1[o] = b1r0; o2[o] = b2r0; oi[o] = bir0; }
-        if (r1 < L) { const size_t o = (size_t)p * maxL + r1; o1[o] = b1r1; o2[o] = b2r1; oi[o] = bir1; }
+        if (r0 < L) {
+            const size_t o = (size_t)p * maxL + r0;
+            o1[o] = ham_of_dot(b1r0); o2[o] = ham_of_dot(b2r0); oi[o] = bir0;
+        }
+        if (r1 < L) {
+            const size_t o = (size_t)p * maxL + r1;
+            o1[o] = ham_of_dot(b1r1); o2[o] = ham_of_dot(b2r1); oi[o] = bir1;
+        }
     }
 }
 
