@@ -10,10 +10,10 @@
 //   picks     = Frontend._response cell scope + Frontend._detect greedy + _subpix (features.py:288-403).
 //
 // B200 layout: frames are batched along grid.y; the response is ONE kernel per batch (u8 in, float32 R out: the
-// reference's dx/dy/row-sum/cov intermediates, ~100 B/px, never touch HBM).  Candidates are gathered one warp per
-// greedy cell straight into per-cell lists sorted by rank, so the greedy kernel advances a list head instead of
-// rescanning; the greedy state, the ranking (a bitonic sort of the picks) and the sub-pixel step share one CTA per
-// frame in shared memory.
+// reference's dx/dy/row-sum/cov intermediates, ~100 B/px, never touch HBM).  Candidates are gathered one CTA per
+// greedy cell row (coalesced rows) into per-cell lists, each list then sorted by rank, so the greedy kernel advances a
+// list head instead of rescanning; the greedy state, the ranking (a bitonic sort of the picks) and the sub-pixel step
+// share one CTA per frame in shared memory.
 #include "common.cuh"
 #include "front_kernels.h"
 
