@@ -18,64 +18,71 @@
 #include "front_kernels.h"
 
 #define BLUR_TY 32
-#define BLUR_TX 64
+#define BLUR_TX 128
 
-__global__ void __launch_bounds__(256) k_blur(const u8* __restrict__ imgs, int H, int W, const float* __restrict__ kf,
-                                              int vr, int vc, u8* __restrict__ outs)
+// one thread per padded-image column of a 128 x 32 tile: the tile and its 3-pixel halo are staged once in shared
+// memory (float32), then each thread walks down its column: the row pass of each staged row (7 taps in OpenCV's
+// order, fused for x < vr), a 7-row window in registers, the symmetric column pass (fused for x < vc), rounding half
+// to even and saturation to u8
+__global__ void __launch_bounds__(BLUR_TX) k_blur(const u8* __restrict__ imgs, int H, int W, const float* __restrict__ kf,
+                                                 int vr, int vc, u8* __restrict__ outs)
 {
     const int Hp = H + 64, Wp = W + 64;
-    const int f = blockIdx.z;
+    const int f = blockIdx.z, tx = threadIdx.x;
     const u8* I = imgs + (size_t)f * H * W;
     u8* out = outs + (size_t)f * Hp * Wp;
     const int y0 = blockIdx.y * BLUR_TY, x0 = blockIdx.x * BLUR_TX;
     __shared__ float src[BLUR_TY + 6][BLUR_TX + 6];
-    __shared__ float rb[BLUR_TY + 6][BLUR_TX];
-    __shared__ float k[7];
-    if (threadIdx.x < 7) k[threadIdx.x] = kf[threadIdx.x];
     // stage: virtual padded rows y0-3 .. y0+BLUR_TY+2 and columns x0-3 .. x0+BLUR_TX+2, each reflected at the padded
     // image's border and then mapped to the source image by the reflect-101 pad of 32
-    for (int i = threadIdx.x; i < (BLUR_TY + 6) * (BLUR_TX + 6); i += blockDim.x) {
-        int vy = i / (BLUR_TX + 6), vx = i % (BLUR_TX + 6);
-        int py = XCB_REFL(y0 - 3 + vy, Hp), px = XCB_REFL(x0 - 3 + vx, Wp);
-        int sy = XCB_REFL(py - 32, H), sx = XCB_REFL(px - 32, W);
-        src[vy][vx] = (float)I[(size_t)sy * W + sx];
+    const int sxa = XCB_REFL(XCB_REFL(x0 - 3 + tx, Wp) - 32, W);
+    const int sxb = tx < 6 ? XCB_REFL(XCB_REFL(x0 - 3 + BLUR_TX + tx, Wp) - 32, W) : 0;
+    for (int vy = 0; vy < BLUR_TY + 6; ++vy) {
+        const u8* row = I + (size_t)XCB_REFL(XCB_REFL(y0 - 3 + vy, Hp) - 32, H) * W;
+        src[vy][tx] = (float)row[sxa];
+        if (tx < 6) src[vy][BLUR_TX + tx] = (float)row[sxb];
     }
+    float k[7];
+#pragma unroll
+    for (int q = 0; q < 7; ++q) k[q] = kf[q];
     __syncthreads();
-    for (int i = threadIdx.x; i < (BLUR_TY + 6) * BLUR_TX; i += blockDim.x) {
-        int vy = i / BLUR_TX, tx = i % BLUR_TX;
-        int x = x0 + tx;
-        const float* p = &src[vy][tx];
-        float s;
-        if (x < vr) {
-            s = __fmul_rn(p[0], k[0]);
+    const int x = x0 + tx;
+    if (x >= Wp) return;
+    const bool fr = x < vr, fc = x < vc;
+    float h[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-            for (int q = 1; q < 7; ++q) s = __fmaf_rn(p[q], k[q], s);
+    for (int vy = 0; vy < BLUR_TY + 6; ++vy) {
+        const float* pp = &src[vy][tx];
+        float sr;
+        if (fr) {
+            sr = __fmul_rn(pp[0], k[0]);
+#pragma unroll
+            for (int q = 1; q < 7; ++q) sr = __fmaf_rn(pp[q], k[q], sr);
         } else {
-            s = __fmul_rn(k[0], p[0]);
+            sr = __fmul_rn(k[0], pp[0]);
 #pragma unroll
-            for (int q = 1; q < 7; ++q) s = __fadd_rn(s, __fmul_rn(k[q], p[q]));
+            for (int q = 1; q < 7; ++q) sr = __fadd_rn(sr, __fmul_rn(k[q], pp[q]));
         }
-        rb[vy][tx] = s;
-    }
-    __syncthreads();
-    for (int i = threadIdx.x; i < BLUR_TY * BLUR_TX; i += blockDim.x) {
-        int ty = i / BLUR_TX, tx = i % BLUR_TX;
-        int y = y0 + ty, x = x0 + tx;
-        if (y >= Hp || x >= Wp) continue;
-        int vy = ty + 3;
-        float s;
-        if (x < vc) {
-            s = __fmul_rn(k[3], rb[vy][tx]);
 #pragma unroll
-            for (int q = 1; q <= 3; ++q) s = __fmaf_rn(k[3 + q], __fadd_rn(rb[vy + q][tx], rb[vy - q][tx]), s);
-        } else {
-            s = __fadd_rn(__fmul_rn(k[3], rb[vy][tx]), 0.0f);
+        for (int i = 0; i < 6; ++i) h[i] = h[i + 1];
+        h[6] = sr;
+        if (vy >= 6) {
+            const int y = y0 + vy - 6;        // output row: h[3] is its row pass, h[3 -+ q] the rows above / below
+            float sc;
+            if (fc) {
+                sc = __fmul_rn(k[3], h[3]);
 #pragma unroll
-            for (int q = 1; q <= 3; ++q)
-                s = __fadd_rn(s, __fmul_rn(k[3 + q], __fadd_rn(rb[vy + q][tx], rb[vy - q][tx])));
+                for (int q = 1; q <= 3; ++q) sc = __fmaf_rn(k[3 + q], __fadd_rn(h[3 + q], h[3 - q]), sc);
+            } else {
+                sc = __fadd_rn(__fmul_rn(k[3], h[3]), 0.0f);
+#pragma unroll
+                for (int q = 1; q <= 3; ++q) sc = __fadd_rn(sc, __fmul_rn(k[3 + q], __fadd_rn(h[3 + q], h[3 - q])));
+            }
+            if (y < Hp) {
+                const int v = __float2int_rn(sc);
+                out[(size_t)y * Wp + x] = (u8)(v < 0 ? 0 : (v > 255 ? 255 : v));
+            }
         }
-        int v = __float2int_rn(s);
-        out[(size_t)y * Wp + x] = (u8)(v < 0 ? 0 : (v > 255 ? 255 : v));
     }
 }
 
@@ -84,7 +91,7 @@ cudaError_t xcb_launch_blur(const uint8_t* img, int F, int H, int W, const float
 {
     int Hp = H + 64, Wp = W + 64;
     dim3 grid((Wp + BLUR_TX - 1) / BLUR_TX, (Hp + BLUR_TY - 1) / BLUR_TY, F);
-    k_blur<<<grid, 256, 0, st>>>(img, H, W, kf, vr, vc, out);
+    k_blur<<<grid, BLUR_TX, 0, st>>>(img, H, W, kf, vr, vc, out);
     return cudaGetLastError();
 }
 
