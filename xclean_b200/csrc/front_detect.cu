@@ -125,6 +125,7 @@ __global__ void __launch_bounds__(128, 7) k_response(const u8* __restrict__ imgs
 #pragma unroll
                 for (int e = 0; e < 3; ++e) nb[k][e] = rn[po[k][e]];
         }
+#pragma unroll 2
         for (int y = 0; y < H; ++y) {
             if (y < H - 1 && H >= 3) {
                 u8 cb[3][3];
