@@ -42,7 +42,7 @@ DLO, DHI = 0, 96
 METRIC = "frontend frames/s"
 # ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_stereo launch over 8 frames (9.549 MB + 0.222 MB),
 # per frame; traffic grows with the frame count, so a launch of F frames moves F times this
-TRAFFIC_PER_FRAME = {"stereo": (12.47872e6 + 0.418816e6) / 8}      # ncu dram read + write, 8-frame capture
+TRAFFIC_PER_FRAME = {"stereo": (8.183552e6 + 0.163584e6) / 8}      # ncu dram read + write, 8-frame capture
 
 
 def parse():
