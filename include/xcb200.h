@@ -154,7 +154,10 @@ typedef struct {
 #define XCB_BA_FP64 0           /* everything in float64: the plain form */
 #define XCB_BA_MIXED 1          /* FP32 linearisation + Schur, FP64 Cholesky, FP64 refinement (to 1e-9, <= 3 steps) */
 
-/* Device scratch the batched solve needs for `Lt` landmarks (trial landmark states and the work counter). */
+/* Device scratch the batched solve needs for `Lt` landmarks: the work counter, the trial landmark states and, for the
+   float64 mode, each landmark's back-substitution record (118 doubles: ~0.95 kB per landmark).  A smaller scratch
+   that still holds the trial states (3 doubles per landmark) works too: the float64 mode then re-linearises the
+   landmarks for the back-substitution. */
 size_t xcb_ba_scratch_bytes(int nw, int Lt);
 /* window.solve (window.py:889-982, purely visual, fixed `iters` LM iterations from lam0) for every window of the batch
    in ONE persistent launch (no reference counterpart as one call; the reference solves one window per call on the

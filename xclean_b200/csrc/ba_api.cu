@@ -5,10 +5,13 @@
 #include "ba_kernels.h"
 #include "common.cuh"
 
+// scratch: [counter (256 B)][3 doubles per landmark: trial states, rounded to 32 doubles][118 doubles per landmark:
+// the float64 back-substitution records]
 extern "C" size_t xcb_ba_scratch_bytes(int nw, int Lt)
 {
     (void)nw;
-    return ((size_t)(Lt > 0 ? Lt : 1) * 3 * sizeof(double) + 255) / 256 * 256 + 256;
+    const size_t L = (size_t)(Lt > 0 ? Lt : 1);
+    return ((3 * L + 31) / 32 * 32 + 118 * L) * sizeof(double) + 256;
 }
 
 static int ba_fail(int code, const char* msg);
@@ -36,8 +39,8 @@ extern "C" int xcb_ba_solve_windows_dev(const xcb_ba_windows* w, int max_slots, 
         grid = sms;
     }
     if (grid > w->nw) grid = w->nw;
-    (void)scratch_bytes;
-    e = xcb_launch_ba_windows(*w, max_slots, iters, lam0, mode, stats, dx0, dx0_stride, trial, counter, grid, st);
+    e = xcb_launch_ba_windows(*w, max_slots, iters, lam0, mode, stats, dx0, dx0_stride, trial, counter, grid, st,
+                              nullptr, scratch_bytes > 256 ? (scratch_bytes - 256) / sizeof(double) : 0);
     if (e != cudaSuccess) return ba_fail(XCB_ERR_CUDA, cudaGetErrorString(e));
     return XCB_OK;
 }
@@ -86,7 +89,7 @@ extern "C" int xcb_ba_solve_windows_free_dev(const xcb_ba_windows* w, int Lt, in
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), st);
     if (e != cudaSuccess) return ba_fail(XCB_ERR_CUDA, cudaGetErrorString(e));
     e = xcb_launch_ba_windows(*w, max_slots, iters, lam0, XCB_BA_FP64, stats, nullptr, 0, trial, counter,
-                              ba_grid(grid, w->nw), st, lsc);
+                              ba_grid(grid, w->nw), st, lsc, (size_t)(Lt > 0 ? Lt : 1) * 3);
     if (e != cudaSuccess) return ba_fail(XCB_ERR_CUDA, cudaGetErrorString(e));
     return XCB_OK;
 }

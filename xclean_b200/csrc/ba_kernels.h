@@ -10,9 +10,11 @@ size_t xcb_ba_smem_bytes(int maxP);
 int xcb_ba_max_slots();
 // frz (optional): the Newton scratch's per-landmark flags (19 doubles per landmark, entry 18); flagged landmarks are
 // held constant
+// trial_doubles: doubles available from lmp_trial on; when they also hold 118 per landmark after the trial states
+// (rounded to 32), the float64 mode keeps each landmark's back-substitution record there instead of re-linearising
 cudaError_t xcb_launch_ba_windows(const XcbBaWindows& d, int max_slots, int iters, double lam0, int mode,
                                   double* stats, double* dx0, int dx0_stride, double* lmp_trial, int* counter,
-                                  int grid, cudaStream_t st, const double* frz = nullptr);
+                                  int grid, cudaStream_t st, const double* frz = nullptr, size_t trial_doubles = 0);
 size_t xcb_ba_newton_smem_bytes(int maxP);
 cudaError_t xcb_launch_ba_newton(const XcbBaWindows& d, int max_slots, int mode, int steps, int maxit, double tol,
                                  const double* gpose, double* gtheta, double* gisig, double* gz, double* stats,

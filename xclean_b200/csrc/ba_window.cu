@@ -33,6 +33,11 @@
 // per-landmark scratch of the Newton / adjoint kernel (19 doubles); entry 18 flags a landmark held constant
 #define BA_LSC_STRIDE 19
 #define BA_LSC_FROZEN 18
+// per-landmark back-substitution record, written by the float64 build and read by the back-substitution of the same
+// LM iteration (the state and the damping are the same): [0] = touched slots nt (-1: more than BA_BSC_NT, recompute;
+// -2: no step), [1..3] Hll^-1 bl, [4..4+nt) the slots, [10 + 18 a + 6 i + j] (Hll^-1 Hlp_a)[i][j]
+#define BA_BSC_NT 6
+#define BA_BSC 118
 
 struct BaWin {
     int P, L, n, hold, lm0, s0;
@@ -384,7 +389,7 @@ __device__ __forceinline__ void inv3(const T H[9], T Hi[9])
 // S: packed lower triangle (FP32, mixed) or full n x n (FP64 plain form, lower triangle used); gb: gradient
 template <typename T, bool PACKED>
 __device__ void pass_build(BaShared& sh, const XcbBaWindows& d, const SlotGeo<T>& G, T* S, T* gb, WarpLm<T>* wls,
-                           double* cost_out, const double* frz = nullptr)
+                           double* cost_out, const double* frz = nullptr, double* bsc = nullptr)
 {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int n = sh.w.n;
@@ -408,6 +413,16 @@ __device__ void pass_build(BaShared& sh, const XcbBaWindows& d, const SlotGeo<T>
                 wl.Tb[a][e] = Hi[i * 3] * wl.Hlp[a][j] + Hi[i * 3 + 1] * wl.Hlp[a][6 + j] + Hi[i * 3 + 2] * wl.Hlp[a][12 + j];
             }
             __syncwarp();
+        }
+        if (bsc) {
+            double* rec = bsc + (size_t)gl * BA_BSC;
+            const bool keep = ok && nt <= BA_BSC_NT;
+            if (lane == 0) rec[0] = !ok ? -2.0 : (keep ? (double)nt : -1.0);
+            if (keep) {
+                if (lane < 3) rec[1 + lane] = (double)HiB[lane];
+                if (lane < nt) rec[4 + lane] = (double)wl.ts[lane];
+                for (int q = lane; q < nt * 18; q += 32) rec[10 + q] = (double)wl.Tb[q / 18][q % 18];
+            }
         }
         // gradient: sum_obs w Jx^T e - Hlp^T Hll^-1 bl
         for (int q = lane; q < nt * 6; q += 32) {
@@ -538,7 +553,7 @@ __device__ void pass_refine(BaShared& sh, const XcbBaWindows& d, WarpLm<double>*
 
 // ------------------------------------------------------------------ pass C: back-substitution (FP64) -> trial lmp
 __device__ void pass_backsub(BaShared& sh, const XcbBaWindows& d, WarpLm<double>* wls, double* lmp_trial,
-                             const double* frz = nullptr)
+                             const double* frz = nullptr, const double* bsc = nullptr)
 {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     WarpLm<double>& wl = wls[wid];
@@ -548,6 +563,31 @@ __device__ void pass_backsub(BaShared& sh, const XcbBaWindows& d, WarpLm<double>
         if (!d.lm_mask[gl]) {
             if (lane < 3) lmp_trial[3 * gl + lane] = d.lmp[3 * gl + lane];
             continue;
+        }
+        if (bsc) {
+            // the build's record: dl = -(Hll^-1 bl + sum_a (Hll^-1 Hlp_a) dx_{slot a})
+            const double* rec = bsc + (size_t)gl * BA_BSC;
+            const int nt = (int)rec[0];
+            if (nt >= -2 && nt != -1) {
+                if (lane < 3) {
+                    double out = d.lmp[3 * gl + lane];
+                    if (nt >= 0) {
+                        double v = rec[1 + lane];
+                        for (int a = 0; a < nt; ++a) {
+                            const int sl = (int)rec[4 + a];
+                            const double* tb = rec + 10 + 18 * a + 6 * lane;
+#pragma unroll
+                            for (int j = 0; j < 6; ++j) v += tb[j] * sh.dx[6 * sl + j];
+                        }
+                        const double dl2 = __shfl_sync(0x7u, -v, 2);
+                        const double r = d.lmp[3 * gl + 2] + dl2;
+                        if (r > 1e-9 && isfinite(r)) out = lane == 2 ? r : d.lmp[3 * gl + lane] - v;
+                    }
+                    lmp_trial[3 * gl + lane] = out;
+                }
+                __syncwarp();
+                continue;
+            }
         }
         double Hll[9], bl[3];
         int nt;
@@ -709,11 +749,22 @@ __device__ double block_sum_red(BaShared& sh)
 // ------------------------------------------------------------------------------------------------- the kernel
 __global__ void __launch_bounds__(BA_THREADS, 1) k_ba_windows(XcbBaWindows d, int iters, double lam0, int mode,
                                                               double* stats, double* dx0, int dx0_stride,
-                                                              double* lmp_trial, int* counter, const double* frz)
+                                                              double* lmp_trial, int* counter, const double* frz,
+                                                              size_t trial_doubles)
 {
     extern __shared__ __align__(16) unsigned char dsm[];
     __shared__ BaShared sh;
     __shared__ double s_norm[2];
+    __shared__ double* s_bsc;
+    // the back-substitution records follow the trial states when the scratch holds them (float64 mode)
+    if (threadIdx.x == 0) {
+        long long Lt = 0;
+        for (int w = 0; w < d.nw; ++w) Lt = max(Lt, (long long)d.lm_off[w] + d.L[w]);
+        const size_t off = ((size_t)3 * Lt + 31) / 32 * 32;
+        s_bsc = (mode == XCB_BA_FP64 && off + (size_t)Lt * BA_BSC <= trial_doubles) ? lmp_trial + off : nullptr;
+    }
+    __syncthreads();
+    double* const bsc = s_bsc;
     const int tid = threadIdx.x;
     for (;;) {
         if (tid == 0) sh.win = atomicAdd(counter, 1);
@@ -764,7 +815,7 @@ __global__ void __launch_bounds__(BA_THREADS, 1) k_ba_windows(XcbBaWindows d, in
             } else {
                 for (int q = tid; q < n * (n + 1) / 2; q += blockDim.x) S64[q] = 0.0;
                 __syncthreads();
-                pass_build<double, true>(sh, d, sh.g64, S64, sh.g, wl64, &c_tot, frz);
+                pass_build<double, true>(sh, d, sh.g64, S64, sh.g, wl64, &c_tot, frz, bsc);
                 c_tot = block_sum_red(sh);
                 for (int q = tid; q < n; q += blockDim.x) sh.rhs[q] = sh.g[q];
             }
@@ -830,7 +881,7 @@ __global__ void __launch_bounds__(BA_THREADS, 1) k_ba_windows(XcbBaWindows d, in
                     for (int q = tid; q < n; q += blockDim.x) dx0[(size_t)w * dx0_stride + q] = sh.dx[q];
             }
             // trial state: landmarks (back-substitution), poses
-            pass_backsub(sh, d, wl64, lmp_trial, frz);
+            pass_backsub(sh, d, wl64, lmp_trial, frz, bsc);
             for (int s = tid; s < P; s += blockDim.x) {
                 double Re[9], R[9];
                 so3_exp(sh.dx + 6 * s, Re);
@@ -1631,7 +1682,7 @@ cudaError_t xcb_launch_ba_newton(const XcbBaWindows& d, int max_slots, int mode,
 
 cudaError_t xcb_launch_ba_windows(const XcbBaWindows& d, int max_slots, int iters, double lam0, int mode,
                                   double* stats, double* dx0, int dx0_stride, double* lmp_trial, int* counter,
-                                  int grid, cudaStream_t st, const double* frz)
+                                  int grid, cudaStream_t st, const double* frz, size_t trial_doubles)
 {
     size_t sm = xcb_ba_smem_bytes(max_slots);
     static bool attr = false;
@@ -1642,7 +1693,7 @@ cudaError_t xcb_launch_ba_windows(const XcbBaWindows& d, int max_slots, int iter
         attr = true;
     }
     k_ba_windows<<<grid, BA_THREADS, sm, st>>>(d, iters, lam0, mode, stats, dx0, dx0_stride, lmp_trial, counter,
-                                               frz);
+                                               frz, trial_doubles);
     return cudaGetLastError();
 }
 
