@@ -476,7 +476,7 @@ __device__ void pass_build(BaShared& sh, const XcbBaWindows& d, const SlotGeo<T>
 // ------------------------------------------------------------------------ pass B: FP64 gradient and S_true dx
 // warp-private g and y = S dx (matrix-free from FP64 Jacobians), then summed over warps into sh.g / sh.y
 __device__ void pass_refine(BaShared& sh, const XcbBaWindows& d, WarpLm<double>* wls, bool want_g,
-                            const double* frz = nullptr)
+                            const double* frz = nullptr, double* bsc = nullptr)
 {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int n = sh.w.n;
@@ -495,7 +495,11 @@ __device__ void pass_refine(BaShared& sh, const XcbBaWindows& d, WarpLm<double>*
         int nt;
         const bool ok = lin_landmark<double>(sh, d, sh.g64, l, sh.lam, d.lmp, wl, Hll, bl, &nt, &c_local) &&
                         !lm_const(frz, gl);
-        if (nt == 0) { __syncwarp(); continue; }
+        if (nt == 0) {
+            if (bsc && lane == 0) bsc[(size_t)gl * BA_BSC] = -1.0;     // the back-substitution re-linearises it
+            __syncwarp();
+            continue;
+        }
         // w (J dx) per observation row
         const int nob = lm_rows(d, gl);
         if (lane < nob && wl.obt[lane] >= 0 && wl.obt[lane] != h) {
@@ -525,7 +529,17 @@ __device__ void pass_refine(BaShared& sh, const XcbBaWindows& d, WarpLm<double>*
                 u[i] = Hi[i * 3] * v[0] + Hi[i * 3 + 1] * v[1] + Hi[i * 3 + 2] * v[2];
                 HiB[i] = Hi[i * 3] * bl[0] + Hi[i * 3 + 1] * bl[1] + Hi[i * 3 + 2] * bl[2];
             }
+            if (bsc && nt <= BA_BSC_NT) {     // the back-substitution record, from these float64 blocks
+                double* rec = bsc + (size_t)gl * BA_BSC;
+                if (lane < 3) rec[1 + lane] = HiB[lane];
+                if (lane < nt) rec[4 + lane] = (double)wl.ts[lane];
+                for (int q = lane; q < nt * 18; q += 32) {
+                    const int a = q / 18, e = q % 18, i = e / 6, j = e % 6;
+                    rec[10 + q] = Hi[i * 3] * wl.Hlp[a][j] + Hi[i * 3 + 1] * wl.Hlp[a][6 + j] + Hi[i * 3 + 2] * wl.Hlp[a][12 + j];
+                }
+            }
         }
+        if (bsc && lane == 0) bsc[(size_t)gl * BA_BSC] = !ok ? -2.0 : (nt <= BA_BSC_NT ? (double)nt : -1.0);
         __syncwarp();
         for (int q = lane; q < nt * 6; q += 32) {
             const int a = q / 6, i = q % 6, s = wl.ts[a];
@@ -761,7 +775,7 @@ __global__ void __launch_bounds__(BA_THREADS, 1) k_ba_windows(XcbBaWindows d, in
         long long Lt = 0;
         for (int w = 0; w < d.nw; ++w) Lt = max(Lt, (long long)d.lm_off[w] + d.L[w]);
         const size_t off = ((size_t)3 * Lt + 31) / 32 * 32;
-        s_bsc = (mode == XCB_BA_FP64 && off + (size_t)Lt * BA_BSC <= trial_doubles) ? lmp_trial + off : nullptr;
+        s_bsc = off + (size_t)Lt * BA_BSC <= trial_doubles ? lmp_trial + off : nullptr;
     }
     __syncthreads();
     double* const bsc = s_bsc;
@@ -855,7 +869,7 @@ __global__ void __launch_bounds__(BA_THREADS, 1) k_ba_windows(XcbBaWindows d, in
                 // FP64 refinement: rho = -g - (S + D) dx with S dx matrix-free from FP64 Jacobians; repeated while the
                 // correction exceeds 1e-9 of the step
                 for (int rf = 0; rf < BA_REFINE_MAX; ++rf) {
-                    pass_refine(sh, d, wl64, rf == 0, frz);
+                    pass_refine(sh, d, wl64, rf == 0, frz, rf == 0 ? bsc : nullptr);
                     if (rf == 0) c_tot = block_sum_red(sh);
                     for (int q = tid; q < n; q += blockDim.x) {
                         double r = -sh.g[q] - sh.y[q] - sh.dmp[q] * sh.dx[q];
