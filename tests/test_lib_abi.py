@@ -28,3 +28,17 @@ def test_binding_covers_the_header():
 def test_loader_binds_without_a_device():
     L = _lib.lib()
     assert L.xcb_version() >= 1
+
+
+def test_host_side_size_rules_without_a_device():
+    """Scratch sizes and argument checks that run on the host before any device call."""
+    L = _lib.lib()
+    for nw, Lt in ((1, 1), (4, 1000), (256, 412517)):
+        need = ((3 * Lt + 31) // 32 * 32 + 118 * Lt) * 8 + 256        # counter, trial states, back-substitution records
+        assert int(L.xcb_ba_scratch_bytes(nw, Lt)) >= need
+        assert int(L.xcb_ba_newton_scratch_bytes(nw, Lt)) >= 22 * 8 * Lt + 256
+    h = ctypes.c_void_p()
+    for w, hgt in ((8193, 376), (47, 376), (1241, 47)):      # outside 48 <= width <= 8192, 48 <= height
+        rc = L.xcb_front_create(w, hgt, 2048, 4, ctypes.byref(h))
+        assert rc == _lib.XCB_ERR_ARG and not h.value
+        assert b"bad size" in L.xcb_last_error()
