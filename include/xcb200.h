@@ -108,6 +108,15 @@ int xcb_front_buffers(xcb_front* f, xcb_front_bufs* out);
    wait on `stream`); host buffers in page-locked memory make the copies asynchronous */
 int xcb_front_pipeline_host(xcb_front* f, const uint8_t* left, const uint8_t* right, int nframes, int budget,
                             int half, int dlo, int dhi, int match_prev, const xcb_front_bufs* out, void* stream);
+/* xcb_front_pipeline_host over `nframes` frames in batches of `batch` (<= max_frames), the results of every batch
+   going to its frames' rows of `out` (arrays for all `nframes` frames); batch b's frames are matched as by
+   consecutive xcb_front_pipeline_host calls (batch 0 against the previous call's last frame when match_prev != 0).
+   No reference counterpart as one call: the reference uploads and processes frame by frame.  The next batch's
+   frames are copied in on a second stream into a second input buffer pair while the current batch computes (page-
+   locked `left` / `right` make that copy overlap); the first call allocates that buffer pair and the stream. */
+int xcb_front_pipeline_host_batches(xcb_front* f, const uint8_t* left, const uint8_t* right, int nframes, int batch,
+                                    int budget, int half, int dlo, int dhi, int match_prev, const xcb_front_bufs* out,
+                                    void* stream);
 /* number of kernel launches the last pipeline call issued */
 int xcb_front_last_launches(const xcb_front* f);
 /* wait for `stream` (NULL = the front's own) and read the device error word -> XCB_OK or XCB_ERR_DEVICE */

@@ -152,6 +152,43 @@ def test_pipeline_batched_vs_oracle():
     gf.close()
 
 
+def test_pipeline_batches_equals_consecutive_calls():
+    """One call over 7 frames in batches of 3 (inputs copied on a second stream into a second buffer pair while the
+    previous batch computes) gives the results of three consecutive pipeline() calls, bit for bit, including the
+    matches across batch boundaries."""
+    import torch
+    from xclean_b200 import synth
+    from xclean_b200.front.gpu_front import GpuFront
+    c = G.load_case("kitti1241")
+    L, R = synth.sequence(synth.CAM_KITTI, 7, seed=11)
+    L = L.numpy().copy()
+    R = R.numpy().copy()
+    Lp = torch.from_numpy(L).pin_memory().numpy()
+    Rp = torch.from_numpy(R).pin_memory().numpy()
+    fronts = []
+    for _ in range(2):
+        gf = GpuFront(1241, 376, cap=2048, max_frames=3)
+        gf.set_calibration(G.calib_of(c), G.pattern())
+        fronts.append(gf)
+    try:
+        got = fronts[0].pipeline_batches(Lp, Rp, 2000, batch=3, half=4, dlo=0, dhi=96, match_prev=False)
+        parts = [fronts[1].pipeline(L[a:a + 3], R[a:a + 3], 2000, half=4, dlo=0, dhi=96, match_prev=a > 0)
+                 for a in (0, 3, 6)]
+        want = {k: np.concatenate([p[k] for p in parts]) for k in got}
+        for k in ("counts", "nmatch", "floor", "anypos"):
+            assert np.array_equal(got[k].view(np.uint8), want[k].view(np.uint8)), k
+        for f in range(7):                       # per-keypoint rows past a frame's count are not written
+            n, m = int(want["counts"][f]), int(want["nmatch"][f])
+            for k in ("kp", "desc", "d", "sig", "ok", "zn", "dy"):
+                assert np.array_equal(got[k][f, :n].view(np.uint8), want[k][f, :n].view(np.uint8)), (f, k)
+            for k in ("m0", "m1"):
+                assert np.array_equal(got[k][f, :m], want[k][f, :m]), (f, k)
+        assert (want["nmatch"][3] > 0) and (want["nmatch"][6] > 0)        # matches across the batch boundaries
+    finally:
+        for gf in fronts:
+            gf.close()
+
+
 def test_errors_and_edges():
     from xclean_b200.front.gpu_front import GpuFront
     c = G.load_case("calib160")

@@ -52,6 +52,8 @@ _SIGS = {
     "xcb_front_pipeline_dev": (c_int, [P, P, P, c_int, c_int, c_int, c_int, c_int, c_int, P]),
     "xcb_front_buffers": (c_int, [P, ctypes.POINTER(FrontBufs)]),
     "xcb_front_pipeline_host": (c_int, [P, P, P, c_int, c_int, c_int, c_int, c_int, c_int, ctypes.POINTER(FrontBufs), P]),
+    "xcb_front_pipeline_host_batches": (c_int, [P, P, P, c_int, c_int, c_int, c_int, c_int, c_int, c_int,
+                                                ctypes.POINTER(FrontBufs), P]),
     "xcb_front_last_launches": (c_int, [P]),
     "xcb_front_sync_check": (c_int, [P, P]),
     "xcb_front_set_stage_timing": (c_int, [P, c_int]),

@@ -25,6 +25,10 @@ extern "C" int xcb_version(void) { return 1; }
 struct xcb_front {
     int W, H, cap, maxF, Hp, Wp;
     cudaStream_t stream;
+    // xcb_front_pipeline_host_batches: a copy stream and a second input buffer pair (made on first use)
+    cudaStream_t cstream;
+    cudaEvent_t ev_loaded[2], ev_free[2];
+    u8* d_in2[2];
     std::string err;
     size_t dev_bytes;
     std::vector<void*> allocs;
@@ -411,6 +415,11 @@ extern "C" void xcb_front_destroy(xcb_front* f)
     drop_graphs(f);
     for (void* p : f->allocs) cudaFree(p);
     if (f->h_stage) cudaFreeHost(f->h_stage);
+    if (f->cstream) {
+        cudaStreamSynchronize(f->cstream);
+        for (int k = 0; k < 2; ++k) { cudaEventDestroy(f->ev_loaded[k]); cudaEventDestroy(f->ev_free[k]); }
+        cudaStreamDestroy(f->cstream);
+    }
     if (f->stream) cudaStreamDestroy(f->stream);
     delete f;
 }
@@ -868,6 +877,89 @@ extern "C" int xcb_front_buffers(xcb_front* f, xcb_front_bufs* o)
     o->m0 = (int64_t*)f->d_m0; o->m1 = (int64_t*)f->d_m1; o->nmatch = f->d_nmatch;
     o->floor = f->d_floor; o->anypos = f->d_anypos;
     return XCB_OK;
+}
+
+// D2H of every non-NULL result array of `out` for the frames [f0, f0 + nframes) of a host result set
+static int d2h_results(xcb_front* f, const xcb_front_bufs* out, size_t f0, size_t nframes, cudaStream_t st)
+{
+    const size_t F = nframes, cap = f->cap;
+    xcb_front_bufs d;
+    xcb_front_buffers(f, &d);
+#define DLB(field, per_frame)                                                                                   \
+    if (out->field)                                                                                            \
+        CK(cudaMemcpyAsync((char*)out->field + f0 * (per_frame), d.field, F * (per_frame), cudaMemcpyDeviceToHost, \
+                           st), "D2H " #field);
+    DLB(counts, 4)
+    DLB(kp, cap * 8)
+    DLB(desc, cap * 32)
+    DLB(d, cap * 8)
+    DLB(sig, cap * 8)
+    DLB(ok, cap)
+    DLB(zn, cap * 8)
+    DLB(dy, cap * 8)
+    DLB(m0, cap * 8)
+    DLB(m1, cap * 8)
+    DLB(nmatch, 4)
+    DLB(floor, 8)
+    DLB(anypos, 4)
+#undef DLB
+    return XCB_OK;
+}
+
+extern "C" int xcb_front_pipeline_host_batches(xcb_front* f, const uint8_t* left, const uint8_t* right, int nframes,
+                                               int batch, int budget, int half, int dlo, int dhi, int match_prev,
+                                               const xcb_front_bufs* out, void* stream)
+{
+    if (!f || !left || !right || !out) return fail(f, XCB_ERR_ARG, "pipeline_host_batches: null argument");
+    if (nframes < 1 || batch < 1 || batch > f->maxF)
+        return fail(f, XCB_ERR_CAPACITY, "pipeline_host_batches: frame or batch count out of range");
+    const size_t npx = (size_t)f->W * f->H;
+    cudaStream_t st = stream ? (cudaStream_t)stream : f->stream;
+    if (!f->cstream) {
+        CK(cudaStreamCreateWithFlags(&f->cstream, cudaStreamNonBlocking), "copy stream");
+        for (int k = 0; k < 2; ++k) {
+            CK(cudaEventCreateWithFlags(&f->ev_loaded[k], cudaEventDisableTiming), "event");
+            CK(cudaEventCreateWithFlags(&f->ev_free[k], cudaEventDisableTiming), "event");
+        }
+        CK(dalloc(f, &f->d_in2[0], (size_t)f->maxF * npx), "alloc inputs");
+        CK(dalloc(f, &f->d_in2[1], (size_t)f->maxF * npx), "alloc inputs");
+        CK(cudaEventRecord(f->ev_free[0], st), "event");
+        CK(cudaEventRecord(f->ev_free[1], st), "event");
+    }
+    // input pairs: buffer 0 = the front's own (d_left, d_right), buffer 1 = d_in2
+    u8* inL[2] = {f->d_left, f->d_in2[0]};
+    u8* inR[2] = {f->d_right, f->d_in2[1]};
+    const int nb = (nframes + batch - 1) / batch;
+    auto load = [&](int b) -> int {
+        const int k = b & 1;
+        const size_t f0 = (size_t)b * batch, fn = (size_t)std::min(batch, nframes - b * batch);
+        CK(cudaStreamWaitEvent(f->cstream, f->ev_free[k], 0), "wait free");
+        CK(cudaMemcpyAsync(inL[k], left + f0 * npx, fn * npx, cudaMemcpyHostToDevice, f->cstream), "H2D left");
+        CK(cudaMemcpyAsync(inR[k], right + f0 * npx, fn * npx, cudaMemcpyHostToDevice, f->cstream), "H2D right");
+        CK(cudaEventRecord(f->ev_loaded[k], f->cstream), "loaded");
+        return XCB_OK;
+    };
+    int rc = load(0);
+    if (!rc && nb > 1) rc = load(1);
+    for (int b = 0; b < nb && !rc; ++b) {
+        const int k = b & 1;
+        const int fn = std::min(batch, nframes - b * batch);
+        CK(cudaStreamWaitEvent(st, f->ev_loaded[k], 0), "wait loaded");
+        rc = xcb_front_pipeline_dev(f, inL[k], inR[k], fn, budget, half, dlo, dhi, match_prev || b > 0, st);
+        if (rc) break;
+        CK(cudaEventRecord(f->ev_free[k], st), "free");
+        // the next load of this buffer is queued before the results are read back, so that a read into pageable
+        // host memory (which returns only when done) does not hold the copy stream back
+        if (b + 2 < nb) rc = load(b + 2);
+        if (!rc) rc = d2h_results(f, out, (size_t)b * batch, fn, st);
+    }
+    if (rc) {
+        cudaStreamSynchronize(f->cstream);
+        cudaStreamSynchronize(st);
+        return rc;
+    }
+    CK(cudaStreamSynchronize(st), "pipeline sync");
+    return check_dev_err(f);
 }
 
 extern "C" int xcb_front_pipeline_host(xcb_front* f, const uint8_t* left, const uint8_t* right, int nframes,

@@ -534,6 +534,28 @@ class GpuFront:
                                                  ctypes.c_void_p(int(stream) or None)), "pipeline")
         return out
 
+    def pipeline_batches(self, left, right, budget, batch, half=HALF, dlo=0, dhi=MAX_DISP - 1, match_prev=True,
+                         out=None, stream=0):
+        """pipeline() over any number of frames in batches of `batch` (<= max_frames), one call: the next batch's
+        frames are copied to the device while the current batch computes (page-locked `left` / `right` make the copy
+        overlap).  Results as consecutive pipeline() calls on the batches, in one dict of host arrays."""
+        self._own()
+        self._require()
+        Lh = np.ascontiguousarray(left, np.uint8).reshape(-1, self.H, self.W)
+        Rh = np.ascontiguousarray(right, np.uint8).reshape(-1, self.H, self.W)
+        F = len(Lh)
+        if out is None:
+            out = self.alloc_outputs(F)
+        b = _lib.FrontBufs()
+        for n, _ in _lib.FrontBufs._fields_:
+            a = out.get(n)
+            setattr(b, n, a.ctypes.data if a is not None else None)
+        self._chk(self.L.xcb_front_pipeline_host_batches(self._h, _lib.ptr(Lh), _lib.ptr(Rh), F, int(batch),
+                                                         int(budget), int(half), int(dlo), int(dhi),
+                                                         int(bool(match_prev)), ctypes.byref(b),
+                                                         ctypes.c_void_p(int(stream) or None)), "pipeline_batches")
+        return out
+
     def alloc_outputs(self, F):
         cap = self.cap
         return dict(counts=np.zeros(F, np.int32), kp=np.zeros((F, cap, 2), np.float32),
