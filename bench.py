@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ba", action="store_true")
+    ap.add_argument("--no-mm", action="store_true", help="skip the gated map matcher")
     ap.add_argument("--ba-only", action="store_true",
                     help="run only the batched window BA part and print its JSON object (profiling)")
     ap.add_argument("--ba-windows", type=int, default=None, help="BA windows per step (default 256)")
@@ -278,6 +279,7 @@ def run_ours(args, ws, rank, local):
     counts = torch.empty(0)
     # ---------------------------------------------------------------- end to end through the public API
     e2e = None
+    outs = None
     if not args.no_e2e:
         gf.set_stage_timing(False)
         Lh = L.cpu().pin_memory()
@@ -342,6 +344,8 @@ def run_ours(args, ws, rank, local):
         cpu = cpu_baseline(L, R, args)
     del L, R
     ba = None if args.no_ba else run_ba(args, dev, stream, rank, ws, cpu=(rank == 0 and ws == 1 and not args.no_cpu))
+    mm = None if (args.no_mm or outs is None) else run_mapmatch(args, dev, stream, ws, outs,
+                                                                  cpu=(rank == 0 and ws == 1 and not args.no_cpu))
     line = {"metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u8/f32/f64",
@@ -351,13 +355,114 @@ def run_ours(args, ws, rank, local):
                        "half": HALF, "l2": "inputs (467 MB/GPU) larger than L2, no flush"},
             "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
             "gpu_launches": launches_per_step * args.steps,
-            "kp_per_frame_last_batch": float(np.mean(counts)) if len(counts) else None, "ba": ba}
+            "kp_per_frame_last_batch": float(np.mean(counts)) if len(counts) else None, "ba": ba, "mapmatch": mm}
     if rank == 0:
         print(json.dumps(line), flush=True)
     gf.close()
     if ws > 1:
         dist.destroy_process_group()
     return 0
+
+
+MM_LANDMARKS = 1500     # window landmarks projected per frame (the 10-keyframe window's 1,500)
+MM_SLOTS = 3            # descriptors kept per landmark
+
+
+def run_mapmatch(args, dev, stream, ws_world, outs, cpu=True):
+    """Gated map matching of every frame of the sequence against MM_LANDMARKS landmarks made from the previous frame's
+    keypoints (synth.map_landmarks), with the frontend's own keypoints and descriptors.  Device-resident: the batched
+    xcb_mm_match_dev over all frames (batches of args.batch); end to end: MapMatcher.match per frame from host arrays,
+    as the engine calls it; CPU: the oracle's restatement of the reference's numba matcher."""
+    import torch
+    from xclean_b200 import synth
+    from xclean_b200.front.mapmatch import MapMatcher
+    F, Bt = args.frames, args.batch
+    kp, counts, desc = outs["kp"], outs["counts"], outs["desc"]
+    uv, S, lmd, lnd, nlm = synth.map_landmarks(kp, counts, desc, outs["m0"], outs["m1"], outs["nmatch"],
+                                               n_lm=MM_LANDMARKS, D=MM_SLOTS, seed=11)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    d = dict(kp=T(kp), nkp=T(counts.astype(np.int32)), desc=T(desc), uv=T(uv), S=T(S), lmd=T(lmd), lnd=T(lnd),
+             nlm=T(nlm))
+    cap = kp.shape[1]
+    mm = MapMatcher(W, H, max_frames=Bt, max_kp=cap, max_lm=MM_LANDMARKS)
+    out = dict(kp=torch.empty((F, MM_LANDMARKS), dtype=torch.int64, device=dev),
+               d=torch.empty((F, MM_LANDMARKS), dtype=torch.int64, device=dev),
+               d2=torch.empty((F, MM_LANDMARKS), dtype=torch.float64, device=dev))
+    sptr = stream.cuda_stream
+    nb = (F + Bt - 1) // Bt
+
+    def step():
+        for b in range(nb):
+            a, e = b * Bt, min(F, (b + 1) * Bt)
+            mm.match_dev(d["kp"][a:e], d["nkp"][a:e], d["desc"][a:e], d["uv"][a:e], d["S"][a:e], d["lmd"][a:e],
+                         d["lnd"][a:e], d["nlm"][a:e], out={k: v[a:e] for k, v in out.items()}, stream=sptr)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    if ws_world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = D.max_over_ranks(e0.elapsed_time(e1) / args.steps, device=dev)
+    got = {k: v.cpu().numpy() for k, v in out.items()}
+    # end to end: the public per-frame call from host arrays (H2D of the frame's inputs, D2H of its results)
+    n_e2e = min(F, 200)
+    frames = [(kp[f, :counts[f]].astype(np.float64), desc[f, :counts[f]], uv[f, :nlm[f]], S[f, :nlm[f]],
+               lmd[f, :nlm[f]], lnd[f, :nlm[f]]) for f in range(n_e2e)]
+    mm1 = MapMatcher(W, H)
+    for fr in frames[:5]:
+        mm1.match(*fr)
+    t0 = time.perf_counter()
+    for fr in frames:
+        mm1.match(*fr)
+    e2e_dt = (time.perf_counter() - t0) / n_e2e
+    h2d = sum(a.nbytes for fr in frames for a in fr) / n_e2e
+    d2h = float(np.mean([24 * len(fr[2]) for fr in frames]))
+    res = {"metric": "map-matching frames/s (%d landmarks x ~%d keypoints per frame)"
+                     % (MM_LANDMARKS, int(np.mean(counts))),
+           "value": F / (ms / 1e3), "unit": "frames/s", "ms_per_step": ms, "frames_per_step": F,
+           "matched_per_frame": float((got["kp"] >= 0).sum() / F),
+           "gpu_launches_per_step": 3 * nb,
+           "e2e": {"value": 1.0 / e2e_dt, "unit": "frames/s", "api": "MapMatcher.match per frame (host arrays)",
+                   "us_per_frame": 1e6 * e2e_dt, "h2d_bytes_per_frame": h2d, "d2h_bytes_per_frame": d2h}}
+    nk = float(np.mean(counts))
+    algo = nk * (8 + 32) + float(np.mean(nlm)) * (16 + 32 + MM_SLOTS * 32 + 8 + 24)
+    peak, peak_kind = peaks()
+    achieved = algo * F / (ms / 1e3) / 1e9
+    res["roofline"] = {"bound": "hbm", "kernel": "k_mm_grid + k_mm_gate + k_mm_mutual (one call)",
+                       "algorithmic_bytes_per_frame": algo, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                       "frac": achieved / peak, "peak_kind": peak_kind}
+    if cpu:
+        from oracle import front_oracle as O
+        # the checker on the timed data: every frame's results against the oracle (OpenMP over frames)
+        ref = O.mapmatch_frames(kp, counts, desc, uv, S, lmd, lnd, nlm, W, H)
+        res["bitexact_vs_oracle_all_frames"] = all(
+            np.array_equal(got["kp"][f, :nlm[f]], ref[0][f, :nlm[f]])
+            and np.array_equal(got["d"][f, :nlm[f]], ref[1][f, :nlm[f]])
+            and np.array_equal(got["d2"][f, :nlm[f]].view(np.uint64), ref[2][f, :nlm[f]].view(np.uint64))
+            for f in range(F))
+        ncores = os.cpu_count() or 1
+        sample = min(F, 100)
+        t0 = time.perf_counter()
+        O.mapmatch_frames(kp[:sample], counts[:sample], desc[:sample], uv[:sample], S[:sample], lmd[:sample],
+                          lnd[:sample], nlm[:sample], W, H, nthreads=ncores)
+        dt_all = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        O.mapmatch_frames(kp[:20], counts[:20], desc[:20], uv[:20], S[:20], lmd[:20], lnd[:20], nlm[:20], W, H,
+                          nthreads=1)
+        dt_one = time.perf_counter() - t0
+        res["cpu_baseline"] = {"value": sample / dt_all, "unit": "frames/s", "cores": ncores, "kind": "port",
+                               "sample": "%d frames of the same workload" % sample,
+                               "single_thread_frames_per_s": 20 / dt_one}
+    mm.close()
+    mm1.close()
+    return res
 
 
 BA_WINDOWS = 256

@@ -130,6 +130,41 @@ int xcb_front_sync_check(xcb_front* f, void* stream);
 int xcb_front_set_stage_timing(xcb_front* f, int on);
 int xcb_front_stage_times(xcb_front* f, float* ms, int* ngraphs);
 
+/* ================================================ gated map matching ================================================ */
+/* Landmarks of the window, projected with the predicted pose, matched to the frame's keypoints inside the chi2 ellipse
+   of their innovation covariance: minimum Hamming distance over the landmark's descriptors, chance bound 104, Lowe
+   ratio 0.8 against the second-best in-gate distance, then one landmark per keypoint (smaller distance, then smaller
+   Mahalanobis d2, then lower landmark index).  Outputs per landmark: keypoint index or -1, Hamming distance (9999 when
+   rejected at the gate), Mahalanobis d2 (inf when rejected at the gate); a landmark that loses the one-per-keypoint
+   step keeps its distance and d2 and gets index -1, as in the reference. */
+typedef struct xcb_mm xcb_mm;
+
+/* MapMatcher.__init__ (src/xclean/front/mapmatch.py:134-139, mapmatch_fast.py:164-170): a 16-px grid over a
+   width x height image (at most 49152 cells), device scratch for batches of up to max_frames frames of max_kp keypoints
+   and max_lm landmarks (xcb_mm_match_dev), one stream. */
+int xcb_mm_create(int width, int height, int max_frames, int max_kp, int max_lm, xcb_mm** out);
+int xcb_mm_destroy(xcb_mm* m);
+const char* xcb_mm_last_error(xcb_mm* m);
+int xcb_mm_grid_dims(xcb_mm* m, int* gw, int* gh);
+/* MapMatcher.match (mapmatch.py:148-169 + _gated :49-131; mapmatch_fast.py:172-184 + _match_fused :113-161) from host
+   arrays: kp (N x 2 float64), desc (N x 32), uv (L x 2 float64), S (L x 2 x 2 float64), lm_desc (L x D x 32),
+   lm_ndesc (L, int64, each <= D, else XCB_ERR_ARG: the reference would read past the landmark's slots), chi2 (the
+   reference's default is 13.815510557964274).  Outputs out_kp / out_d (int64) and out_d2 (float64), L each.  Grows
+   the device scratch when N or L exceed the handle's capacities; returns when the results are in the output arrays. */
+int xcb_mm_match_host(xcb_mm* m, const double* kp, int N, const uint8_t* desc, const double* uv, const double* S,
+                      const uint8_t* lm_desc, int D, const int64_t* lm_ndesc, int L, double chi2, int64_t* out_kp,
+                      int64_t* out_d, double* out_d2, void* stream);
+/* The same for F frames resident in device memory (no reference counterpart as one call: the reference matches one
+   frame per call on the CPU).  Frame f: nkp[f] keypoints of kp_stride in kp (float32, the frontend's layout) and desc,
+   nlm[f] landmarks of lm_stride in uv / S / lm_desc / lm_ndesc / outputs (counts read on the device, clamped to the
+   strides; lm_ndesc values above D read as D; output rows past nlm[f] are not written).  Three launches on `stream`
+   (NULL = the handle's own), nothing allocated, no synchronisation. */
+int xcb_mm_match_dev(xcb_mm* m, int F, const float* kp, const int32_t* nkp, int kp_stride, const uint8_t* desc,
+                     const double* uv, const double* S, const uint8_t* lm_desc, int D, const int64_t* lm_ndesc,
+                     const int32_t* nlm, int lm_stride, double chi2, int64_t* out_kp, int64_t* out_d, double* out_d2,
+                     void* stream);
+int xcb_mm_sync(xcb_mm* m, void* stream);
+
 /* ============================================== sliding-window bundle adjustment ============================================== */
 /* A batch of windows of the reference's stereo window solve (src/xclean/vio/window.py: Problem :768-792, solve
    :889-982), concatenated: window w owns slots [slot_off[w], slot_off[w] + P[w]) and landmarks [lm_off[w],

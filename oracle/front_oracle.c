@@ -20,6 +20,8 @@
  *                 the LAPACK calls numba makes (np.linalg.solve / inv -> OpenBLAS getf2/getrs, trti2 + dgetri),
  *                 the arithmetic the reference's device kernel reproduces (gpu_front.py:607-704).
  *   hamming       front/mapmatch_fast._bf_mutual (mapmatch_fast.py:46-90) = Frontend.match_desc (features.py:564-595).
+ *   mapmatch      front/mapmatch.MapMatcher.match (mapmatch.py:148-169) with its numba _gated (mapmatch.py:49-131) and
+ *                 grid (:141-146), = front/mapmatch_fast.MapMatcher.match (mapmatch_fast.py:113-184).
  *
  * Build: gcc -O2 -ffp-contract=off -fno-fast-math -fopenmp -shared -fPIC (see oracle/build.py).  Every floating-point
  * step is written out; fma() is used exactly where the restated library uses a fused multiply-add.
@@ -861,4 +863,151 @@ long xo_frames(const u8* left, const u8* right, int F, int H, int W, int budget,
                              m1 + (size_t)f * cap);
     if (F > 0) nmatch[0] = 0;
     return tot;
+}
+
+/* ================================================== gated map matching ================================================== */
+/* float64 -> int64 as x86-64 converts it (numpy astype(np.int64) and numba int() both compile to cvttsd2si there):
+   NaN and values outside the int64 range give INT64_MIN ("integer indefinite") */
+static i64 xo_f2i64(double v)
+{
+    if (!(v >= -9223372036854775808.0 && v < 9223372036854775808.0)) return INT64_MIN;
+    return (i64)v;
+}
+
+static int xo_ham4(const u64* a, const u64* b)
+{
+    return __builtin_popcountll(a[0] ^ b[0]) + __builtin_popcountll(a[1] ^ b[1]) + __builtin_popcountll(a[2] ^ b[2])
+           + __builtin_popcountll(a[3] ^ b[3]);
+}
+
+/* MapMatcher.match for one frame (the caller has already returned the defaults for L == 0 or N == 0).
+   kp (N x 2) float64, kd (N x 4 words), uvp (L x 2), S (L x 2 x 2), ld (L x D x 4 words), lnd (L).
+   Preamble (mapmatch.py:158-166): det, Sinv, half = sqrt(max(chi2 S_ii, 0)) with NaN kept, nd = lnd where det > 0.
+   Grid (mapmatch.py:141-146): cell = clip(x // 16) + gw clip(y // 16), stable counting sort.
+   Gated search (mapmatch.py:52-112): visit the cells of the gate's bounding box row by row, a cell's keypoints in
+   index order; keep the best (Hamming, then Mahalanobis d2) and the second-best distance; chance bound and ratio.
+   Mutual step (mapmatch.py:113-131): landmarks in index order claim their keypoint; a later claimant takes it only
+   with a smaller distance, or an equal distance and a smaller d2. */
+void xo_mapmatch(const double* kp, int N, const u64* kd, const double* uvp, const double* S, const u64* ld, int D,
+                 const i64* lnd, int L, int gw, int gh, double chi2, double ratio, int ham_max, i64* out_kp, i64* out_d,
+                 double* out_d2)
+{
+    const int grid = 16;
+    double* Sinv = (double*)calloc((size_t)L * 4 + 1, sizeof(double));
+    double* half = (double*)malloc(sizeof(double) * ((size_t)L * 2 + 1));
+    i64* nd = (i64*)calloc((size_t)L + 1, sizeof(i64));
+    for (int l = 0; l < L; ++l) {
+        const double* s = S + 4 * (size_t)l;
+        double det = s[0] * s[3] - s[1] * s[2];
+        if (det > 0) {
+            Sinv[4 * l + 0] = s[3] / det;
+            Sinv[4 * l + 3] = s[0] / det;
+            Sinv[4 * l + 1] = -s[1] / det;
+            Sinv[4 * l + 2] = -s[2] / det;
+            nd[l] = lnd[l];
+        }
+        for (int a = 0; a < 2; ++a) {
+            double h = chi2 * s[3 * a];
+            half[2 * l + a] = sqrt((h >= 0.0 || isnan(h)) ? h : 0.0);
+        }
+    }
+    const int ncell = gw * gh;
+    i64* cstart = (i64*)calloc((size_t)ncell + 1, sizeof(i64));
+    i64* cur = (i64*)malloc(sizeof(i64) * (size_t)ncell);
+    int* cell = (int*)malloc(sizeof(int) * (size_t)N);
+    int* cidx = (int*)malloc(sizeof(int) * (size_t)N);
+    for (int k = 0; k < N; ++k) {
+        i64 cx = xo_f2i64(floor(kp[2 * k] / grid)), cy = xo_f2i64(floor(kp[2 * k + 1] / grid));
+        cx = cx < 0 ? 0 : (cx > gw - 1 ? gw - 1 : cx);
+        cy = cy < 0 ? 0 : (cy > gh - 1 ? gh - 1 : cy);
+        cell[k] = (int)(cy * gw + cx);
+        cstart[cell[k] + 1] += 1;
+    }
+    for (int c = 0; c < ncell; ++c) cstart[c + 1] += cstart[c];
+    for (int c = 0; c < ncell; ++c) cur[c] = cstart[c];
+    for (int k = 0; k < N; ++k) cidx[cur[cell[k]]++] = k;
+    for (int l = 0; l < L; ++l) {
+        out_kp[l] = -1;
+        out_d[l] = 9999;
+        out_d2[l] = INFINITY;
+        const double u = uvp[2 * l], v = uvp[2 * l + 1];
+        if (nd[l] <= 0 || !(isfinite(u) && isfinite(v))) continue;
+        i64 x0 = xo_f2i64(floor((u - half[2 * l]) / grid)), x1 = xo_f2i64(floor((u + half[2 * l]) / grid));
+        i64 y0 = xo_f2i64(floor((v - half[2 * l + 1]) / grid)), y1 = xo_f2i64(floor((v + half[2 * l + 1]) / grid));
+        if (x0 < 0) x0 = 0;
+        if (y0 < 0) y0 = 0;
+        if (x1 > gw - 1) x1 = gw - 1;
+        if (y1 > gh - 1) y1 = gh - 1;
+        const double* si = Sinv + 4 * (size_t)l;
+        int best = 9999, second = 9999;
+        i64 bk = -1;
+        double bd2 = INFINITY;
+        for (i64 cy = y0; cy <= y1; ++cy)
+            for (i64 cx = x0; cx <= x1; ++cx) {
+                const i64 c = cy * gw + cx;
+                for (i64 t = cstart[c]; t < cstart[c + 1]; ++t) {
+                    const int k = cidx[t];
+                    const double dx = kp[2 * k] - u, dy = kp[2 * k + 1] - v;
+                    const double d2 = dx * (si[0] * dx + si[1] * dy) + dy * (si[2] * dx + si[3] * dy);
+                    if (d2 > chi2) continue;
+                    int h = 9999;
+                    for (i64 j = 0; j < nd[l]; ++j) {
+                        int hj = xo_ham4(kd + 4 * (size_t)k, ld + 4 * ((size_t)l * D + j));
+                        if (hj < h) h = hj;
+                    }
+                    if (h < best || (h == best && d2 < bd2)) {
+                        second = best;
+                        best = h;
+                        bk = k;
+                        bd2 = d2;
+                    } else if (h < second) {
+                        second = h;
+                    }
+                }
+            }
+        if (bk < 0 || best > ham_max) continue;
+        if (second < 9999 && !((double)best < ratio * (double)second)) continue;
+        out_kp[l] = bk;
+        out_d[l] = best;
+        out_d2[l] = bd2;
+    }
+    i64* owner = (i64*)malloc(sizeof(i64) * ((size_t)N + 1));
+    for (int k = 0; k < N; ++k) owner[k] = -1;
+    for (int l = 0; l < L; ++l) {
+        const i64 k = out_kp[l];
+        if (k < 0) continue;
+        const i64 o = owner[k];
+        if (o < 0) { owner[k] = l; continue; }
+        if (out_d[l] < out_d[o] || (out_d[l] == out_d[o] && out_d2[l] < out_d2[o])) {
+            owner[k] = l;
+            out_kp[o] = -1;
+        } else {
+            out_kp[l] = -1;
+        }
+    }
+    free(owner); free(cidx); free(cell); free(cur); free(cstart); free(nd); free(half); free(Sinv);
+}
+
+/* F frames of MapMatcher.match (frame f: counts_kp[f] keypoints of kp_stride, counts_lm[f] landmarks of lm_stride),
+   OpenMP over frames with nthreads threads; float32 keypoints as the frontend stores them (widened to float64 as
+   MapMatcher.match does). */
+void xo_mapmatch_frames(const float* kp32, const int* counts_kp, int kp_stride, const u8* desc, const double* uvp,
+                        const double* S, const u8* ld, int D, const i64* lnd, const int* counts_lm, int lm_stride, int F,
+                        int gw, int gh, double chi2, int nthreads, i64* out_kp, i64* out_d, double* out_d2)
+{
+    #pragma omp parallel for num_threads(nthreads) schedule(dynamic, 1)
+    for (int f = 0; f < F; ++f) {
+        const int N = counts_kp[f], L = counts_lm[f];
+        i64* ok = out_kp + (size_t)f * lm_stride;
+        i64* od = out_d + (size_t)f * lm_stride;
+        double* od2 = out_d2 + (size_t)f * lm_stride;
+        for (int l = 0; l < L; ++l) { ok[l] = -1; od[l] = 9999; od2[l] = INFINITY; }
+        if (L == 0 || N == 0) continue;
+        double* kp = (double*)malloc(sizeof(double) * 2 * (size_t)N);
+        for (int i = 0; i < 2 * N; ++i) kp[i] = (double)kp32[(size_t)f * kp_stride * 2 + i];
+        xo_mapmatch(kp, N, (const u64*)(desc + (size_t)f * kp_stride * 32), uvp + (size_t)f * lm_stride * 2,
+                    S + (size_t)f * lm_stride * 4, (const u64*)(ld + (size_t)f * lm_stride * D * 32), D,
+                    lnd + (size_t)f * lm_stride, L, gw, gh, chi2, 0.8, 104, ok, od, od2);
+        free(kp);
+    }
 }

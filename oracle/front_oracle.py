@@ -8,6 +8,7 @@ Thin numpy wrappers over oracle/liboracle.so (front_oracle.c), with the referenc
   blur(gray, kf, vr, vc) / orb(...)       = Frontend.describe                          (features.py:405-421)
   stereo(left, right, kp, ...)            = front/stereo1d.disparities                 (stereo1d.py:492-522)
   hamming(A, B) / match_desc(d0, d1)      = mapmatch_fast._bf_mutual / match_desc       (mapmatch_fast.py:46-111)
+  mapmatch(kp, desc, uv, S, lmd, lnd, W, H) = mapmatch.MapMatcher.match                  (mapmatch.py:148-169)
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import this module.
 """
@@ -24,6 +25,8 @@ HALF_REF = 5                    # the reference's patch half-size (stereo/epipol
 MAX_DISP = 128                  # stereo/sgm32.py:68
 HAMMING_CHANCE = 104            # features.py:50
 RATIO = 0.8                     # features.py:51
+CHI2_2_999 = 13.815510557964274  # mapmatch.py:29
+GRID = 16                       # mapmatch.py:30
 
 _LIB = None
 
@@ -149,6 +152,54 @@ def match_desc(d0, d1):
     m1 = np.empty(max(len(A), 1), np.int64)
     m = lib().xo_match(_p(A), len(A), _p(B), len(B), HAMMING_CHANCE, ctypes.c_double(RATIO), _p(m0), _p(m1))
     return m0[:m].copy(), m1[:m].copy()
+
+
+def mapmatch(kp, desc, uv_pred, S_uv, lm_desc, lm_ndesc, W, H, chi2=CHI2_2_999):
+    """MapMatcher(W, H).match(kp, desc, uv_pred, S_uv, lm_desc, lm_ndesc, chi2) -> (kp index per landmark or -1,
+    Hamming distance, Mahalanobis d2), the reference's dtypes (int64, int64, float64)."""
+    L = len(uv_pred)
+    out_kp = np.full(L, -1, np.int64)
+    out_d = np.full(L, 9999, np.int64)
+    out_d2 = np.full(L, np.inf)
+    if L == 0 or len(kp) == 0:
+        return out_kp, out_d, out_d2
+    kp = np.ascontiguousarray(kp, np.float64).reshape(-1, 2)
+    kd = np.ascontiguousarray(desc, np.uint8).reshape(len(kp), 32)
+    uv = np.ascontiguousarray(uv_pred, np.float64).reshape(L, 2)
+    S = np.ascontiguousarray(S_uv, np.float64).reshape(L, 2, 2)
+    D = lm_desc.shape[1]
+    ld = np.ascontiguousarray(lm_desc, np.uint8).reshape(L, D, 32)
+    lnd = np.ascontiguousarray(lm_ndesc, np.int64).reshape(L)
+    if (lnd > D).any():
+        raise ValueError("lm_ndesc above the descriptor slots of lm_desc")
+    gw, gh = -(-int(W) // GRID), -(-int(H) // GRID)
+    lib().xo_mapmatch(_p(kp), len(kp), _p(kd), _p(uv), _p(S), _p(ld), D, _p(lnd), L, gw, gh, ctypes.c_double(chi2),
+                      ctypes.c_double(RATIO), HAMMING_CHANCE, _p(out_kp), _p(out_d), _p(out_d2))
+    return out_kp, out_d, out_d2
+
+
+def mapmatch_frames(kp32, counts_kp, desc, uv, S, lm_desc, lm_ndesc, counts_lm, W, H, chi2=CHI2_2_999,
+                    nthreads=None):
+    """F frames of mapmatch with float32 keypoints (F, Nmax, 2), descriptors (F, Nmax, 32), landmark arrays
+    (F, Lmax, ...); OpenMP over frames.  -> (out_kp, out_d, out_d2) of shape (F, Lmax)."""
+    kp32 = np.ascontiguousarray(kp32, np.float32)
+    F, Nmax = kp32.shape[:2]
+    Lmax, D = lm_desc.shape[1], lm_desc.shape[2]
+    desc = np.ascontiguousarray(desc, np.uint8)
+    uv = np.ascontiguousarray(uv, np.float64)
+    S = np.ascontiguousarray(S, np.float64)
+    ld = np.ascontiguousarray(lm_desc, np.uint8)
+    lnd = np.ascontiguousarray(lm_ndesc, np.int64)
+    ck = np.ascontiguousarray(counts_kp, np.int32)
+    cl = np.ascontiguousarray(counts_lm, np.int32)
+    out_kp = np.full((F, Lmax), -1, np.int64)
+    out_d = np.full((F, Lmax), 9999, np.int64)
+    out_d2 = np.full((F, Lmax), np.inf)
+    gw, gh = -(-int(W) // GRID), -(-int(H) // GRID)
+    lib().xo_mapmatch_frames(_p(kp32), _p(ck), Nmax, _p(desc), _p(uv), _p(S), _p(ld), D, _p(lnd), _p(cl), Lmax, F, gw,
+                             gh, ctypes.c_double(chi2), int(nthreads or os.cpu_count() or 1), _p(out_kp), _p(out_d),
+                             _p(out_d2))
+    return out_kp, out_d, out_d2
 
 
 def lk_solve_inv(As, gs):

@@ -63,3 +63,20 @@ def same_bits(a, b):
         b = np.ascontiguousarray(b, np.float64)
         return np.array_equal(a.view(np.uint64), b.view(np.uint64))
     return np.array_equal(a, b)
+
+
+def mapmatch_cases():
+    """The gated map matcher fixture (tests/golden/make_golden_mapmatch.py): name -> dict of inputs and outputs."""
+    z = np.load(os.path.join(GOLDEN, "mapmatch_golden.npz"))
+    out = {}
+    for n in z["names"]:
+        n = str(n)
+        out[n] = {k.split("__", 1)[1]: z[k] for k in z.files if k.startswith(n + "__")}
+    return out
+
+
+def same_outputs(got, want):
+    """(kp index, distance, d2) triples equal bit for bit (NaN payloads included)."""
+    return (np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
+            and np.array_equal(np.asarray(got[2], np.float64).view(np.uint64),
+                               np.asarray(want[2], np.float64).view(np.uint64)))

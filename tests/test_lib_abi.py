@@ -42,3 +42,15 @@ def test_host_side_size_rules_without_a_device():
         rc = L.xcb_front_create(w, hgt, 2048, 4, ctypes.byref(h))
         assert rc == _lib.XCB_ERR_ARG and not h.value
         assert b"bad size" in L.xcb_last_error()
+
+
+def test_map_matcher_argument_checks_without_a_device():
+    """xcb_mm_create refuses bad sizes and grids larger than one CTA's shared memory before any device call."""
+    L = _lib.lib()
+    h = ctypes.c_void_p()
+    assert L.xcb_mm_create(0, 48, 1, 16, 16, ctypes.byref(h)) == _lib.XCB_ERR_ARG and not h.value
+    assert L.xcb_mm_create(64, 48, 0, 16, 16, ctypes.byref(h)) == _lib.XCB_ERR_ARG
+    assert L.xcb_mm_create(8192, 8192, 1, 16, 16, ctypes.byref(h)) == _lib.XCB_ERR_ARG
+    assert b"49152" in L.xcb_last_error()
+    assert L.xcb_mm_match_host(None, None, 0, None, None, None, None, 0, None, 0, 1.0, None, None, None,
+                               None) == _lib.XCB_ERR_ARG

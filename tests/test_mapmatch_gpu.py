@@ -1,0 +1,148 @@
+"""Device gated map matcher (libxcb200.so through the C ABI) against the reference's golden outputs and the CPU
+oracle: landmark -> keypoint index, Hamming distance and Mahalanobis d2, bit for bit (NaN payloads included)."""
+import numpy as np
+import pytest
+
+from oracle import front_oracle as O
+from tests import _golden as G
+
+pytestmark = pytest.mark.gpu
+
+
+def _mm(W, H, **kw):
+    from xclean_b200.front.mapmatch import MapMatcher
+    return MapMatcher(W, H, **kw)
+
+
+@pytest.mark.parametrize("name", sorted(G.mapmatch_cases()))
+def test_golden_bitexact(name):
+    c = G.mapmatch_cases()[name]
+    mm = _mm(int(c["W"]), int(c["H"]))
+    try:
+        got = mm.match(c["kp"], c["desc"], c["uv"], c["S"], c["lmd"], c["lnd"], chi2=float(c["chi2"]))
+    finally:
+        mm.close()
+    assert G.same_outputs(got, (c["out_kp"], c["out_d"], c["out_d2"])), name
+    assert mm.stats["matched"] == int((c["out_kp"] >= 0).sum())
+
+
+def _random_case(rng, W, H, N, L, D, dup=0.3):
+    pool = rng.integers(0, 256, (max(4, N // 8), 32), dtype=np.uint8)
+    kp = np.stack([rng.uniform(-12, W + 12, N), rng.uniform(-12, H + 12, N)], 1)
+    desc = np.where(rng.random((N, 1)) < dup, pool[rng.integers(0, len(pool), N)],
+                    rng.integers(0, 256, (N, 32), dtype=np.uint8)).astype(np.uint8)
+    src = rng.integers(0, N, L)
+    uv = kp[src] + rng.normal(0, 1.5, (L, 2))
+    sx, sy, rho = rng.uniform(0.5, 9.0, L), rng.uniform(0.5, 9.0, L), rng.uniform(-0.9, 0.9, L)
+    S = np.empty((L, 2, 2))
+    S[:, 0, 0], S[:, 1, 1] = sx * sx, sy * sy
+    S[:, 0, 1] = S[:, 1, 0] = rho * sx * sy
+    lmd = rng.integers(0, 256, (L, D, 32), dtype=np.uint8)
+    flips = np.packbits(rng.random((L, 256)) < rng.uniform(0, 0.3, (L, 1)), axis=1)
+    lmd[:, 0] = desc[src] ^ flips
+    lnd = rng.integers(0 if D > 1 else 1, D + 1, L).astype(np.int64)
+    return kp, desc, uv, S, lmd, lnd
+
+
+@pytest.mark.parametrize("W,H,N,L,D,chi2", [(752, 480, 1, 1, 1, 13.815510557964274),
+                                            (752, 480, 37, 500, 3, 13.815510557964274),
+                                            (1241, 376, 2000, 1500, 3, 13.815510557964274),
+                                            (1241, 376, 2000, 3000, 3, 50.0),
+                                            (1280, 720, 5000, 2500, 5, 13.815510557964274),
+                                            (1280, 720, 4000, 6000, 3, 5.0)])
+def test_random_vs_oracle(W, H, N, L, D, chi2):
+    """Random frames, sizes past the handle's initial capacities (its buffers grow), several descriptor slots, other
+    gate quantiles."""
+    rng = np.random.default_rng(W + N + L + D)
+    kp, desc, uv, S, lmd, lnd = _random_case(rng, W, H, N, L, D)
+    mm = _mm(W, H)
+    try:
+        got = mm.match(kp, desc, uv, S, lmd, lnd, chi2=chi2)
+        again = mm.match(kp[: N // 2 + 1], desc[: N // 2 + 1], uv, S, lmd, lnd, chi2=chi2)   # reused buffers
+    finally:
+        mm.close()
+    assert G.same_outputs(got, O.mapmatch(kp, desc, uv, S, lmd, lnd, W, H, chi2))
+    h = N // 2 + 1
+    assert G.same_outputs(again, O.mapmatch(kp[:h], desc[:h], uv, S, lmd, lnd, W, H, chi2))
+
+
+def test_crowded_keypoints_and_shared_claims():
+    """All keypoints in a few cells, many landmarks per keypoint: long cell ranges and long owner folds."""
+    rng = np.random.default_rng(7)
+    W, H, N, L = 320, 240, 3000, 4000
+    kp = np.concatenate([rng.normal(40, 3, (N // 2, 2)), rng.normal(200, 1, (N - N // 2, 2))])
+    desc = rng.integers(0, 256, (N, 32), dtype=np.uint8)
+    src = rng.integers(0, 50, L)                       # 50 keypoints claimed by 80 landmarks each
+    uv = kp[src] + rng.normal(0, 0.3, (L, 2))
+    S = np.tile(np.eye(2) * 9.0, (L, 1, 1))
+    lmd = desc[src][:, None, :].copy()
+    lnd = np.ones(L, np.int64)
+    mm = _mm(W, H)
+    try:
+        got = mm.match(kp, desc, uv, S, lmd, lnd)
+    finally:
+        mm.close()
+    want = O.mapmatch(kp, desc, uv, S, lmd, lnd, W, H)
+    assert G.same_outputs(got, want)
+    assert (want[0] >= 0).sum() > 0
+
+
+def test_empty_inputs_and_errors():
+    mm = _mm(64, 48)
+    try:
+        out = mm.match(np.zeros((0, 2)), np.zeros((0, 32), np.uint8), np.array([[10.0, 10.0]]), np.eye(2)[None],
+                       np.zeros((1, 3, 32), np.uint8), np.array([1]))
+        assert out[0].tolist() == [-1] and out[1].tolist() == [9999] and np.isinf(out[2]).all()
+        out = mm.match(np.array([[1.0, 1.0]]), np.zeros((1, 32), np.uint8), np.zeros((0, 2)), np.zeros((0, 2, 2)),
+                       np.zeros((0, 3, 32), np.uint8), np.zeros(0, np.int64))
+        assert all(len(o) == 0 for o in out)
+        with pytest.raises(ValueError):
+            mm.match(np.array([[1.0, 1.0]]), np.zeros((1, 32), np.uint8), np.array([[1.0, 1.0]]), np.eye(2)[None],
+                     np.zeros((1, 2, 32), np.uint8), np.array([3]))
+    finally:
+        mm.close()
+    with pytest.raises(ValueError):
+        _mm(8192, 8192)                                # more grid cells than one CTA's shared memory holds
+
+
+def test_match_dev_batched_vs_oracle():
+    """A batch of frames in device memory (float32 keypoints as the frontend stores them, ragged keypoint and
+    landmark counts): every frame's rows equal the oracle's; rows past a frame's landmark count are not written."""
+    import torch
+    from xclean_b200 import synth
+    rng = np.random.default_rng(3)
+    W, H, F, Nk, Nl = 1241, 376, 6, 2048, 1600
+    nkp = np.array([0, 1, 700, 2048, 1500, 1900], np.int32)
+    kp = np.zeros((F, Nk, 2), np.float32)
+    desc = np.zeros((F, Nk, 32), np.uint8)
+    for f in range(F):
+        kp[f] = np.stack([rng.uniform(-5, W + 5, Nk), rng.uniform(-5, H + 5, Nk)], 1).astype(np.float32)
+        desc[f] = rng.integers(0, 256, (Nk, 32), dtype=np.uint8)
+    m = np.tile(np.arange(Nk, dtype=np.int64), (F, 1))
+    nmatch = np.minimum(nkp, np.roll(nkp, 1)).astype(np.int32)
+    # frame f's landmarks from frame f-1; matches pair the same index (a keypoint that stayed in place)
+    kp_lm = kp.copy()
+    uv, S, lmd, lnd, nlm = synth.map_landmarks(kp_lm, nkp, desc, m, m, nmatch, n_lm=Nl, D=3, seed=5)
+    nlm[2] = 0
+    dev = torch.device("cuda", 0)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    mm = _mm(W, H, max_frames=F, max_kp=Nk, max_lm=Nl)
+    try:
+        out = dict(kp=torch.full((F, Nl), -7, dtype=torch.int64, device=dev),
+                   d=torch.full((F, Nl), -7, dtype=torch.int64, device=dev),
+                   d2=torch.full((F, Nl), -7.0, dtype=torch.float64, device=dev))
+        mm.match_dev(T(kp), T(nkp), T(desc), T(uv), T(S), T(lmd), T(lnd), T(nlm), out=out)
+        torch.cuda.synchronize()
+        got = {k: v.cpu().numpy() for k, v in out.items()}
+    finally:
+        mm.close()
+    for f in range(F):
+        L = int(nlm[f])
+        want = O.mapmatch(kp[f, :nkp[f]].astype(np.float64), desc[f, :nkp[f]], uv[f, :L], S[f, :L], lmd[f, :L],
+                          lnd[f, :L], W, H)
+        assert G.same_outputs((got["kp"][f, :L], got["d"][f, :L], got["d2"][f, :L]), want), f
+        assert (got["kp"][f, L:] == -7).all() and (got["d2"][f, L:] == -7.0).all()
+    want_all = O.mapmatch_frames(kp, nkp, desc, uv, S, lmd, lnd, nlm, W, H)
+    for f in range(F):
+        L = int(nlm[f])
+        assert np.array_equal(want_all[0][f, :L], got["kp"][f, :L])

@@ -69,3 +69,30 @@ def test_edge_cases_oracle():
     assert not ok.any() and (zn == -2.0).all() and np.isinf(s).all()
     e0, e1 = O.match_desc(np.zeros((1, 32), np.uint8), np.zeros((5, 32), np.uint8))
     assert len(e0) == 0 and len(e1) == 0
+
+
+@pytest.mark.parametrize("name", sorted(G.mapmatch_cases()))
+def test_mapmatch_matches_reference(name):
+    """The oracle's gated map matcher against xclean.front.mapmatch.MapMatcher's outputs (= mapmatch_fast's), bit for
+    bit: realistic frames, an inflated re-search, degenerate inputs (non-finite keypoints and covariances, NaN d2 on
+    accepted matches) and tie-heavy lattices."""
+    c = G.mapmatch_cases()[name]
+    with np.errstate(all="ignore"):
+        got = O.mapmatch(c["kp"], c["desc"], c["uv"], c["S"], c["lmd"], c["lnd"], int(c["W"]), int(c["H"]),
+                         float(c["chi2"]))
+    assert G.same_outputs(got, (c["out_kp"], c["out_d"], c["out_d2"]))
+
+
+def test_mapmatch_oracle_edges():
+    """Empty landmark / keypoint sets return the defaults; more valid descriptors than slots is refused."""
+    kp = np.array([[10.0, 10.0]])
+    d = np.zeros((1, 32), np.uint8)
+    out = O.mapmatch(np.zeros((0, 2)), np.zeros((0, 32), np.uint8), np.array([[10.0, 10.0]]), np.eye(2)[None],
+                     np.zeros((1, 3, 32), np.uint8), np.array([1]), 64, 64)
+    assert out[0].tolist() == [-1] and out[1].tolist() == [9999] and np.isinf(out[2]).all()
+    out = O.mapmatch(kp, d, np.zeros((0, 2)), np.zeros((0, 2, 2)), np.zeros((0, 3, 32), np.uint8),
+                     np.zeros(0, np.int64), 64, 64)
+    assert all(len(o) == 0 for o in out)
+    with pytest.raises(ValueError):
+        O.mapmatch(kp, d, np.array([[10.0, 10.0]]), np.eye(2)[None], np.zeros((1, 2, 32), np.uint8), np.array([3]),
+                   64, 64)

@@ -123,6 +123,16 @@ class LbaProblem(ctypes.Structure):
 
 
 _SIGS.update({
+    "xcb_mm_create": (c_int, [c_int, c_int, c_int, c_int, c_int, P]),
+    "xcb_mm_destroy": (c_int, [P]),
+    "xcb_mm_last_error": (ctypes.c_char_p, [P]),
+    "xcb_mm_grid_dims": (c_int, [P, P, P]),
+    "xcb_mm_match_host": (c_int, [P, P, c_int, P, P, P, P, c_int, P, c_int, c_double, P, P, P, P]),
+    "xcb_mm_match_dev": (c_int, [P, c_int, P, P, c_int, P, P, P, P, c_int, P, P, c_int, c_double, P, P, P, P]),
+    "xcb_mm_sync": (c_int, [P, P]),
+})
+
+_SIGS.update({
     "xcb_lba_workspace_bytes": (c_size_t, [ctypes.POINTER(LbaProblem)]),
     "xcb_lba_solve": (c_int, [ctypes.POINTER(LbaProblem), c_int, c_double, P, P, c_size_t, P]),
 })

@@ -23,6 +23,7 @@ SOURCES = {
     "front_orb_match.cu": STRICT,
     "front_stereo.cu": STRICT,
     "front_api.cu": STRICT,
+    "front_mapmatch.cu": STRICT,
     "ba_window.cu": [],
     "ba_api.cu": [],
 }

@@ -202,3 +202,44 @@ def sequence(cam, n_frames, seed=0, device="cpu", step=1.0, yaw_sigma_deg=0.5, n
         L[k] = l
         R[k] = r
     return L, R
+
+
+def map_landmarks(kp, counts, desc, m0, m1, nmatch, n_lm=1500, D=3, seed=0):
+    """Map-matching inputs for a frame sequence (the frontend's per-frame outputs): frame f's landmarks are the first
+    n_lm keypoints of frame f-1 (frame 0 takes the last frame's), predicted where frame f's matches put them (+0.7 px
+    noise) or, unmatched, at their old position shifted by the median flow (+3 px noise); innovation covariances with
+    sigmas in [0.8, 4] px and correlation in [-0.5, 0.5]; D descriptor slots (the keypoint's own, a copy with ~4 % of
+    the bits flipped, a random one) of which 1..D are valid.
+    -> uv (F,n_lm,2) float64, S (F,n_lm,2,2) float64, lm_desc (F,n_lm,D,32) uint8, lm_ndesc (F,n_lm) int64,
+    nlm (F,) int32."""
+    F = len(counts)
+    rng = np.random.default_rng(seed)
+    uv = np.zeros((F, n_lm, 2))
+    S = np.zeros((F, n_lm, 2, 2))
+    lmd = np.zeros((F, n_lm, D, 32), np.uint8)
+    lnd = np.zeros((F, n_lm), np.int64)
+    nlm = np.zeros(F, np.int32)
+    for f in range(F):
+        p = (f - 1) % F
+        L = min(int(counts[p]), n_lm)
+        nlm[f] = L
+        q, t = m0[f, :int(nmatch[f])], m1[f, :int(nmatch[f])]
+        keep = q < L
+        q, t = q[keep], t[keep]
+        base = kp[p, :L].astype(np.float64)
+        flow = np.median(kp[f, t].astype(np.float64) - base[q], axis=0) if len(q) else np.zeros(2)
+        u = base + flow + rng.normal(0, 3.0, (L, 2))
+        u[q] = kp[f, t].astype(np.float64) + rng.normal(0, 0.7, (len(q), 2))
+        uv[f, :L] = u
+        sx, sy, rho = rng.uniform(0.8, 4.0, L), rng.uniform(0.8, 4.0, L), rng.uniform(-0.5, 0.5, L)
+        S[f, :L, 0, 0] = sx * sx
+        S[f, :L, 1, 1] = sy * sy
+        S[f, :L, 0, 1] = S[f, :L, 1, 0] = rho * sx * sy
+        lmd[f, :L, 0] = desc[p, :L]
+        if D > 1:
+            flips = np.packbits(rng.random((L, 256)) < 0.04, axis=1)
+            lmd[f, :L, 1] = desc[p, :L] ^ flips
+        if D > 2:
+            lmd[f, :L, 2:] = rng.integers(0, 256, (L, D - 2, 32), dtype=np.uint8)
+        lnd[f, :L] = rng.integers(1, D + 1, L)
+    return uv, S, lmd, lnd, nlm
