@@ -431,6 +431,22 @@ def run_mapmatch(args, dev, stream, ws_world, outs, cpu=True):
            "gpu_launches_per_step": 3 * nb,
            "e2e": {"value": 1.0 / e2e_dt, "unit": "frames/s", "api": "MapMatcher.match per frame (host arrays)",
                    "us_per_frame": 1e6 * e2e_dt, "h2d_bytes_per_frame": h2d, "d2h_bytes_per_frame": d2h}}
+    # the engine's tracking step in one call: predict_projection of a 2,000-landmark window + the gated matching
+    tw = synth.tracking_window(13, n_lm=2000)
+    twa = (*tw["pose"], tw["kp"], tw["desc"], tw["lm_desc"], tw["lm_ndesc"])
+    mm2 = MapMatcher(tw["W"], tw["H"])
+    for _ in range(5):
+        r = mm2.predict_match(*twa)
+    t0 = time.perf_counter()
+    n_tr = 200
+    for _ in range(n_tr):
+        r = mm2.predict_match(*twa)
+    tr_dt = (time.perf_counter() - t0) / n_tr
+    res["tracking_step"] = {"api": "MapMatcher.predict_match (window.predict_projection + MapMatcher.match)",
+                            "landmarks": int(len(tw["lm_desc"])), "in_view": int(r[2].sum()),
+                            "keypoints": int(len(tw["kp"])), "matched": int((r[4] >= 0).sum()),
+                            "us_per_call": 1e6 * tr_dt, "calls_per_s": 1.0 / tr_dt}
+    mm2.close()
     nk = float(np.mean(counts))
     algo = nk * (8 + 32) + float(np.mean(nlm)) * (16 + 32 + MM_SLOTS * 32 + 8 + 24)
     peak, peak_kind = peaks()
@@ -460,6 +476,15 @@ def run_mapmatch(args, dev, stream, ws_world, outs, cpu=True):
         res["cpu_baseline"] = {"value": sample / dt_all, "unit": "frames/s", "cores": ncores, "kind": "port",
                                "sample": "%d frames of the same workload" % sample,
                                "single_thread_frames_per_s": 20 / dt_one}
+        L2 = len(tw["lm_desc"])
+        o = [np.full((L2, 2), np.nan), np.zeros((L2, 2, 2)), np.zeros(L2, np.bool_), np.zeros(L2)]
+        t0 = time.perf_counter()
+        for _ in range(50):
+            O.predict_projection(*tw["pose"], float(tw["W"]), float(tw["H"]), *o)
+            sel = np.nonzero(o[2])[0]
+            O.mapmatch(tw["kp"], tw["desc"], o[0][sel], o[1][sel], tw["lm_desc"][sel], tw["lm_ndesc"][sel],
+                       tw["W"], tw["H"])
+        res["tracking_step"]["cpu_oracle_us_per_call_1_thread"] = 1e6 * (time.perf_counter() - t0) / 50
     mm.close()
     mm1.close()
     return res

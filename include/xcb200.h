@@ -164,6 +164,29 @@ int xcb_mm_match_dev(xcb_mm* m, int F, const float* kp, const int32_t* nkp, int 
                      const int32_t* nlm, int lm_stride, double chi2, int64_t* out_kp, int64_t* out_d, double* out_d2,
                      void* stream);
 int xcb_mm_sync(xcb_mm* m, void* stream);
+/* window.predict_projection (src/xclean/vio/window.py:1032-1144): every landmark (host camera Rwc_h (L x 3 x 3) /
+   pwc_h (L x 3), inverse-depth state lmp (L x 3) = a, b, rho) projected into the predicted body pose Rwb_t (3 x 3) /
+   pwb_t (3) through the body-to-camera extrinsic Rbc / pbc, with the innovation covariance
+   S = Jp Spose Jp^T + Jl Sl Jl^T + sig_px^2 I (Spose 6 x 6 in [dphi, dp], Sl (L x 3 x 3)); all row-major float64.
+   Writes ok (L) for every landmark and, as the reference does, uv (L x 2) and depth (L) only where the point is in
+   front (q2 > 1e-9, rho > 0) and S (L x 2 x 2) only where it also projects inside W x H; other entries keep the
+   caller's values.  Bit-identical to the reference's float64 arithmetic. */
+int xcb_mm_predict_host(xcb_mm* m, const double* Rwb_t, const double* pwb_t, const double* Rbc, const double* pbc,
+                        const double* Rwc_h, const double* pwc_h, const double* lmp, const double* Spose,
+                        const double* Sl, double sig_px, double fx, double fy, double cx, double cy, double W, double H,
+                        int L, double* uv, double* S, uint8_t* ok, double* depth, void* stream);
+/* The engine's tracking step in one call (vio/engine_live.py:1580-1582 and :1618-1632: _project, then
+   MapMatcher.match on the landmarks predicted in view): xcb_mm_predict_host over the handle's W x H, then the gated
+   map matching of the in-view landmarks against kp (N x 2 float64) / desc (N x 32), one upload and one read-back.
+   out_kp / out_d / out_d2 have one entry per landmark (L); at the in-view landmarks sel = nonzero(ok) they equal
+   MapMatcher.match(kp, desc, uv[sel], S[sel], lm_desc[sel], lm_ndesc[sel]), elsewhere they hold the defaults
+   (-1, 9999, inf).  lm_ndesc is checked against D for every landmark. */
+int xcb_mm_predict_match_host(xcb_mm* m, const double* Rwb_t, const double* pwb_t, const double* Rbc, const double* pbc,
+                              const double* Rwc_h, const double* pwc_h, const double* lmp, const double* Spose,
+                              const double* Sl, double sig_px, double fx, double fy, double cx, double cy, int L,
+                              const double* kp, int N, const uint8_t* desc, const uint8_t* lm_desc, int D,
+                              const int64_t* lm_ndesc, double chi2, double* uv, double* S, uint8_t* ok, double* depth,
+                              int64_t* out_kp, int64_t* out_d, double* out_d2, void* stream);
 
 /* ============================================== sliding-window bundle adjustment ============================================== */
 /* A batch of windows of the reference's stereo window solve (src/xclean/vio/window.py: Problem :768-792, solve

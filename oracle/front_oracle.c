@@ -20,6 +20,8 @@
  *                 the LAPACK calls numba makes (np.linalg.solve / inv -> OpenBLAS getf2/getrs, trti2 + dgetri),
  *                 the arithmetic the reference's device kernel reproduces (gpu_front.py:607-704).
  *   hamming       front/mapmatch_fast._bf_mutual (mapmatch_fast.py:46-90) = Frontend.match_desc (features.py:564-595).
+ *   predict       vio/window.predict_projection (window.py:1032-1144), the map matcher's predicted pixels and
+ *                 innovation covariances.
  *   mapmatch      front/mapmatch.MapMatcher.match (mapmatch.py:148-169) with its numba _gated (mapmatch.py:49-131) and
  *                 grid (:141-146), = front/mapmatch_fast.MapMatcher.match (mapmatch_fast.py:113-184).
  *
@@ -1009,5 +1011,95 @@ void xo_mapmatch_frames(const float* kp32, const int* counts_kp, int kp_stride, 
                     S + (size_t)f * lm_stride * 4, (const u64*)(ld + (size_t)f * lm_stride * D * 32), D,
                     lnd + (size_t)f * lm_stride, L, gw, gh, chi2, 0.8, 104, ok, od, od2);
         free(kp);
+    }
+}
+
+/* ================================================ gating prediction ================================================ */
+/* window.predict_projection (src/xclean/vio/window.py:1032-1144): every landmark (host camera Rwc_h / pwc_h, inverse-
+   depth state a, b, rho) projected into the predicted body pose (Rwb_t, pwb_t) through the body-to-camera extrinsic
+   (Rbc, pbc); S = Jp Spose Jp^T + Jl Sl Jl^T + sig_px^2 I.  Writes ok for every landmark, uv and depth where the point
+   is in front (q2 > 1e-9, rho > 0), S where it also projects inside the image; other entries are left as they are.
+   Row-major 3x3 / 6x6 arrays; every sum in the reference's order. */
+static void xo_mm3(const double* A, const double* B, double* out)
+{
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) out[3 * i + j] = A[3 * i] * B[j] + A[3 * i + 1] * B[3 + j] + A[3 * i + 2] * B[6 + j];
+}
+
+void xo_predict_projection(const double* Rwb_t, const double* pwb_t, const double* Rbc, const double* pbc,
+                           const double* Rwc_h, const double* pwc_h, const double* lmp, const double* Spose,
+                           const double* Sl, double sig_px, double fx, double fy, double cx, double cy, double W,
+                           double H, int L, double* uv, double* S, u8* ok, double* depth)
+{
+    double Rwc_t[9], pwc_t[3], Rcb[9], Px[9] = {0}, Wt[9], Rct[9], RctWt[9];
+    xo_mm3(Rwb_t, Rbc, Rwc_t);
+    for (int i = 0; i < 3; ++i) pwc_t[i] = pwb_t[i] + Rwb_t[3 * i] * pbc[0] + Rwb_t[3 * i + 1] * pbc[1] + Rwb_t[3 * i + 2] * pbc[2];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) Rcb[3 * i + j] = Rbc[3 * j + i];
+    Px[1] = -pbc[2]; Px[2] = pbc[1]; Px[3] = pbc[2]; Px[5] = -pbc[0]; Px[6] = -pbc[1]; Px[7] = pbc[0];
+    xo_mm3(Rwb_t, Px, Wt);
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) Rct[3 * i + j] = Rwc_t[3 * j + i];
+    xo_mm3(Rct, Wt, RctWt);
+    double Qx[9] = {0}, QR[9], Jp[12], Jl[6], RcR[9], Dp[6], t6[12], t3[6];
+    for (int l = 0; l < L; ++l) {
+        ok[l] = 0;
+        const double* R = Rwc_h + 9 * (size_t)l;
+        const double a = lmp[3 * l], b = lmp[3 * l + 1], rho = lmp[3 * l + 2];
+        const double d0 = pwc_h[3 * l] - pwc_t[0], d1 = pwc_h[3 * l + 1] - pwc_t[1], d2 = pwc_h[3 * l + 2] - pwc_t[2];
+        const double Y0 = R[0] * a + R[1] * b + R[2] + rho * d0;
+        const double Y1 = R[3] * a + R[4] * b + R[5] + rho * d1;
+        const double Y2 = R[6] * a + R[7] * b + R[8] + rho * d2;
+        const double q0 = Rct[0] * Y0 + Rct[1] * Y1 + Rct[2] * Y2;
+        const double q1 = Rct[3] * Y0 + Rct[4] * Y1 + Rct[5] * Y2;
+        const double q2 = Rct[6] * Y0 + Rct[7] * Y1 + Rct[8] * Y2;
+        if (q2 <= 1e-9 || rho <= 0.0) continue;
+        depth[l] = q2 / rho;
+        const double iq = 1.0 / q2;
+        const double u = fx * q0 * iq + cx, v = fy * q1 * iq + cy;
+        uv[2 * l] = u;
+        uv[2 * l + 1] = v;
+        if (u < 0.0 || u >= W || v < 0.0 || v >= H) continue;
+        Dp[0] = fx * iq; Dp[1] = 0.0; Dp[2] = -fx * q0 * iq * iq;
+        Dp[3] = 0.0; Dp[4] = fy * iq; Dp[5] = -fy * q1 * iq * iq;
+        Qx[1] = -q2; Qx[2] = q1; Qx[3] = q2; Qx[5] = -q0; Qx[6] = -q1; Qx[7] = q0;
+        xo_mm3(Qx, Rcb, QR);
+        for (int r = 0; r < 2; ++r)
+            for (int j = 0; j < 3; ++j) {
+                Jp[6 * r + j] = Dp[3 * r] * (QR[j] + rho * RctWt[j]) + Dp[3 * r + 1] * (QR[3 + j] + rho * RctWt[3 + j])
+                                + Dp[3 * r + 2] * (QR[6 + j] + rho * RctWt[6 + j]);
+                Jp[6 * r + 3 + j] = -rho * (Dp[3 * r] * Rct[j] + Dp[3 * r + 1] * Rct[3 + j] + Dp[3 * r + 2] * Rct[6 + j]);
+            }
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) RcR[3 * i + j] = Rct[3 * i] * R[j] + Rct[3 * i + 1] * R[3 + j] + Rct[3 * i + 2] * R[6 + j];
+        const double e0 = Rct[0] * d0 + Rct[1] * d1 + Rct[2] * d2;
+        const double e1 = Rct[3] * d0 + Rct[4] * d1 + Rct[5] * d2;
+        const double e2 = Rct[6] * d0 + Rct[7] * d1 + Rct[8] * d2;
+        for (int r = 0; r < 2; ++r) {
+            Jl[3 * r] = Dp[3 * r] * RcR[0] + Dp[3 * r + 1] * RcR[3] + Dp[3 * r + 2] * RcR[6];
+            Jl[3 * r + 1] = Dp[3 * r] * RcR[1] + Dp[3 * r + 1] * RcR[4] + Dp[3 * r + 2] * RcR[7];
+            Jl[3 * r + 2] = Dp[3 * r] * e0 + Dp[3 * r + 1] * e1 + Dp[3 * r + 2] * e2;
+        }
+        const double* sl = Sl + 9 * (size_t)l;
+        for (int r = 0; r < 2; ++r) {
+            for (int j = 0; j < 6; ++j) {
+                double acc = 0.0;
+                for (int k = 0; k < 6; ++k) acc += Jp[6 * r + k] * Spose[6 * k + j];
+                t6[6 * r + j] = acc;
+            }
+            for (int j = 0; j < 3; ++j) {
+                double acc = 0.0;
+                for (int k = 0; k < 3; ++k) acc += Jl[3 * r + k] * sl[3 * k + j];
+                t3[3 * r + j] = acc;
+            }
+        }
+        for (int r = 0; r < 2; ++r)
+            for (int c = 0; c < 2; ++c) {
+                double acc = 0.0;
+                for (int k = 0; k < 6; ++k) acc += t6[6 * r + k] * Jp[6 * c + k];
+                for (int k = 0; k < 3; ++k) acc += t3[3 * r + k] * Jl[3 * c + k];
+                S[4 * (size_t)l + 2 * r + c] = acc + (r == c ? sig_px * sig_px : 0.0);
+            }
+        ok[l] = 1;
     }
 }

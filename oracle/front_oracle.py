@@ -9,6 +9,7 @@ Thin numpy wrappers over oracle/liboracle.so (front_oracle.c), with the referenc
   stereo(left, right, kp, ...)            = front/stereo1d.disparities                 (stereo1d.py:492-522)
   hamming(A, B) / match_desc(d0, d1)      = mapmatch_fast._bf_mutual / match_desc       (mapmatch_fast.py:46-111)
   mapmatch(kp, desc, uv, S, lmd, lnd, W, H) = mapmatch.MapMatcher.match                  (mapmatch.py:148-169)
+  predict_projection(...)                 = vio/window.predict_projection               (window.py:1032-1144)
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import this module.
 """
@@ -176,6 +177,19 @@ def mapmatch(kp, desc, uv_pred, S_uv, lm_desc, lm_ndesc, W, H, chi2=CHI2_2_999):
     lib().xo_mapmatch(_p(kp), len(kp), _p(kd), _p(uv), _p(S), _p(ld), D, _p(lnd), L, gw, gh, ctypes.c_double(chi2),
                       ctypes.c_double(RATIO), HAMMING_CHANCE, _p(out_kp), _p(out_d), _p(out_d2))
     return out_kp, out_d, out_d2
+
+
+def predict_projection(Rwb_t, pwb_t, Rbc, pbc, Rwc_h, pwc_h, lmp, Spose, Sl, sig_px, fx, fy, cx, cy, W, H, uv, S, ok,
+                       depth):
+    """window.predict_projection: writes ok, and uv / depth / S where the reference writes them (in place)."""
+    ins = [np.ascontiguousarray(a, np.float64) for a in (Rwb_t, pwb_t, Rbc, pbc, Rwc_h, pwc_h, lmp, Spose, Sl)]
+    L = len(ins[6])
+    for a, dt in ((uv, np.float64), (S, np.float64), (depth, np.float64), (ok, np.bool_)):
+        assert a.dtype == dt and a.flags.c_contiguous and len(a) == L
+    lib().xo_predict_projection(*[_p(a) for a in ins], ctypes.c_double(sig_px), ctypes.c_double(fx),
+                                ctypes.c_double(fy), ctypes.c_double(cx), ctypes.c_double(cy), ctypes.c_double(W),
+                                ctypes.c_double(H), L, _p(uv), _p(S), _p(ok.view(np.uint8)), _p(depth))
+    return 0
 
 
 def mapmatch_frames(kp32, counts_kp, desc, uv, S, lm_desc, lm_ndesc, counts_lm, W, H, chi2=CHI2_2_999,

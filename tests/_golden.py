@@ -80,3 +80,22 @@ def same_outputs(got, want):
     return (np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
             and np.array_equal(np.asarray(got[2], np.float64).view(np.uint64),
                                np.asarray(want[2], np.float64).view(np.uint64)))
+
+
+def predict_cases():
+    """The gating-prediction fixture (predict_golden.npz, made by tests/golden/make_golden_mapmatch.py)."""
+    z = np.load(os.path.join(GOLDEN, "predict_golden.npz"))
+    out = {}
+    for n in z["names"]:
+        n = str(n)
+        out[n] = {k.split("__", 1)[1]: z[k] for k in z.files if k.startswith(n + "__")}
+    return out
+
+
+PREDICT_ARGS = ("Rwb_t", "pwb_t", "Rbc", "pbc", "Rwc_h", "pwc_h", "lmp", "Spose", "Sl", "sig_px", "fx", "fy", "cx",
+                "cy", "W", "H")
+
+
+def predict_args(c):
+    """The positional inputs of predict_projection from a fixture case (scalars as Python floats)."""
+    return [float(c[k]) if np.ndim(c[k]) == 0 else c[k] for k in PREDICT_ARGS]

@@ -8,6 +8,10 @@ outputs (kp index per landmark, Hamming distance, Mahalanobis d2) from xclean.fr
 asserts that xclean.front.mapmatch_fast.MapMatcher returns the same arrays.  Keypoints and descriptors of the realistic
 cases are the frontend fixtures' (front_<case>.npz: two consecutive frames and their matches); the landmarks are the
 first frame's keypoints projected into the second frame with noise, with covariances drawn per landmark.
+
+predict_golden.npz: xclean.vio.window.predict_projection on engine-shaped inputs (its outputs pre-filled as the
+engine's _project fills them), then MapMatcher.match on the in-view landmarks, as the engine's tracking stage calls
+them one after the other.
 """
 import os
 import sys
@@ -132,6 +136,92 @@ def ties(seed):
     return dict(W=W, H=H, chi2=13.815510557964274, kp=kp, desc=desc, uv=uv, S=S, lmd=lmd, lnd=lnd)
 
 
+def _rot(rng, scale):
+    w = rng.normal(0, scale, 3)
+    th = np.linalg.norm(w)
+    k = w / th if th > 0 else np.array([1.0, 0.0, 0.0])
+    K = np.array([[0, -k[2], k[1]], [k[2], 0, -k[0]], [-k[1], k[0], 0]])
+    return np.eye(3) + np.sin(th) * K + (1 - np.cos(th)) * K @ K
+
+
+def predict_case(seed, L, zero_spose=False, sig_px=1.0, edges=False):
+    """window.predict_projection inputs shaped as the engine's _project builds them (host cameras of a few keyframes
+    along a forward path, inverse-depth landmarks, a predicted pose near the newest keyframe), then the map matcher
+    on the in-view landmarks (keypoints near their projections plus clutter)."""
+    rng = np.random.default_rng(seed)
+    W, H, fx, fy, cx, cy = 1241, 376, 718.0, 718.0, 607.0, 185.0
+    Rbc = np.array([[0.0, 0.0, 1.0], [-1.0, 0.0, 0.0], [0.0, -1.0, 0.0]]) @ _rot(rng, 0.01)   # camera z = body x
+    pbc = np.array([0.3, -0.1, 0.05])
+    nh = 8
+    Rwb_h = [_rot(rng, 0.02) for _ in range(nh)]
+    pwb_h = [np.array([1.0 * i, rng.normal(0, 0.05), rng.normal(0, 0.02)]) for i in range(nh)]
+    if edges:
+        Rwb_h[0] = Rwb_h[0] @ np.diag([-1.0, -1.0, 1.0])            # a host looking backwards: points behind
+    host = rng.integers(0, nh, L)
+    Rwc_h = np.stack([Rwb_h[h] @ Rbc for h in host])
+    pwc_h = np.stack([pwb_h[h] + Rwb_h[h] @ pbc for h in host])
+    lmp = np.stack([rng.uniform(-0.7, 0.7, L), rng.uniform(-0.22, 0.22, L), rng.uniform(0.03, 0.3, L)], 1)
+    R_t = Rwb_h[-1] @ _rot(rng, 0.01)
+    p_t = pwb_h[-1] + np.array([1.0, 0.0, 0.0]) + rng.normal(0, 0.02, 3)
+    A = rng.normal(0, 0.05, (6, 6))
+    Spose = np.zeros((6, 6)) if zero_spose else A @ A.T + np.diag([1e-4] * 3 + [1e-3] * 3)
+    B = rng.normal(0, 0.03, (L, 3, 3))
+    Sl = np.einsum("lij,lkj->lik", B, B)
+    Sl[rng.random(L) < 0.1] = 0.0
+    if edges:
+        lmp[0, 2] = 0.0
+        lmp[1, 2] = -0.1
+        lmp[2, 2] = np.nan
+        lmp[3, 0] = np.nan
+        lmp[4, 2] = 1e-12
+        Sl[5] = np.nan
+        pwc_h[6] = np.inf
+    uv = np.full((L, 2), np.nan)
+    S = np.zeros((L, 2, 2))
+    ok = np.zeros(L, np.bool_)
+    depth = np.zeros(L)
+    return dict(Rwb_t=R_t, pwb_t=p_t, Rbc=Rbc, pbc=pbc, Rwc_h=Rwc_h, pwc_h=pwc_h, lmp=lmp, Spose=Spose, Sl=Sl,
+                sig_px=sig_px, fx=fx, fy=fy, cx=cx, cy=cy, W=float(W), H=float(H), uv0=uv, S0=S, ok0=ok, depth0=depth)
+
+
+def predict_match_inputs(rng, c, uv, ok):
+    """Keypoints near 70 % of the in-view projections (and 400 clutter points), their landmarks' descriptors."""
+    L = len(uv)
+    sel = np.nonzero(ok)[0]
+    lmd = rng.integers(0, 256, (L, 3, 32), dtype=np.uint8)
+    lnd = rng.integers(1, 4, L).astype(np.int64)
+    seen = sel[rng.random(len(sel)) < 0.7]
+    kp = np.concatenate([uv[seen] + rng.normal(0, 1.0, (len(seen), 2)),
+                         np.stack([rng.uniform(0, c["W"], 400), rng.uniform(0, c["H"], 400)], 1)]).astype(np.float32)
+    flips = np.packbits(rng.random((len(seen), 256)) < 0.05, axis=1)
+    desc = np.concatenate([lmd[seen, 0] ^ flips, rng.integers(0, 256, (400, 32), dtype=np.uint8)])
+    perm = rng.permutation(len(kp))
+    return kp[perm], desc[perm], lmd, lnd
+
+
+def make_predict(ref_src, RM):
+    from xclean.vio import window as RW
+    cases = {"kitti": predict_case(6, 1500), "track": predict_case(7, 900, zero_spose=True, sig_px=2.3),
+             "edges": predict_case(8, 64, edges=True)}
+    out = {}
+    for ci, (name, c) in enumerate(cases.items()):
+        uv, S, ok, depth = c["uv0"].copy(), c["S0"].copy(), c["ok0"].copy(), c["depth0"].copy()
+        with np.errstate(all="ignore"):
+            RW.predict_projection(c["Rwb_t"], c["pwb_t"], c["Rbc"], c["pbc"], c["Rwc_h"], c["pwc_h"], c["lmp"],
+                                  c["Spose"], c["Sl"], c["sig_px"], c["fx"], c["fy"], c["cx"], c["cy"], c["W"],
+                                  c["H"], uv, S, ok, depth)
+        rng = np.random.default_rng(100 + ci)
+        kp, desc, lmd, lnd = predict_match_inputs(rng, c, uv, ok)
+        sel = np.nonzero(ok)[0]
+        with np.errstate(all="ignore"):
+            k, d, d2 = RM.MapMatcher(int(c["W"]), int(c["H"])).match(kp, desc, uv[sel], S[sel], lmd[sel], lnd[sel])
+        c.update(uv=uv, S=S, ok=ok, depth=depth, kp=kp, desc=desc, lmd=lmd, lnd=lnd, sel=sel, m_kp=k, m_d=d, m_d2=d2)
+        for key, v in c.items():
+            out["%s__%s" % (name, key)] = np.asarray(v)
+        print("predict", name, "landmarks", len(uv), "in view", len(sel), "matched", int((k >= 0).sum()))
+    np.savez_compressed(os.path.join(HERE, "predict_golden.npz"), names=np.array(list(cases)), **out)
+
+
 def main(ref_src):
     os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/nbcache")
     sys.path.insert(0, ref_src)
@@ -159,6 +249,7 @@ def main(ref_src):
         out["%s__out_kp" % name], out["%s__out_d" % name], out["%s__out_d2" % name] = a
         print(name, "landmarks", len(c["uv"]), "keypoints", len(c["kp"]), "matched", int((a[0] >= 0).sum()))
     np.savez_compressed(os.path.join(HERE, "mapmatch_golden.npz"), names=np.array(list(cases)), **out)
+    make_predict(ref_src, RM)
 
 
 if __name__ == "__main__":

@@ -146,3 +146,80 @@ def test_match_dev_batched_vs_oracle():
     for f in range(F):
         L = int(nlm[f])
         assert np.array_equal(want_all[0][f, :L], got["kp"][f, :L])
+
+
+@pytest.mark.parametrize("name", sorted(G.predict_cases()))
+def test_predict_projection_golden(name):
+    """window.predict_projection on the device against the reference's outputs, bit for bit; entries the reference
+    does not write keep the caller's values (checked with sentinels against the oracle)."""
+    from xclean_b200.front.mapmatch import predict_projection
+    c = G.predict_cases()[name]
+    uv, S, ok, depth = c["uv0"].copy(), c["S0"].copy(), c["ok0"].copy(), c["depth0"].copy()
+    assert predict_projection(*G.predict_args(c), uv, S, ok, depth) == 0
+    for got, k in ((uv, "uv"), (S, "S"), (depth, "depth")):
+        assert np.array_equal(got.view(np.uint64), c[k].view(np.uint64)), k
+    assert np.array_equal(ok, c["ok"])
+    L = len(ok)
+    sent = [np.full((L, 2), 7.0), np.full((L, 2, 2), 3.0), np.ones(L, np.bool_), np.full(L, -1.0)]
+    want = [a.copy() for a in sent]
+    predict_projection(*G.predict_args(c), *sent)
+    with np.errstate(all="ignore"):
+        O.predict_projection(*G.predict_args(c), *want)
+    for g, w in zip(sent, want):
+        assert np.array_equal(g.view(np.uint8), w.view(np.uint8))
+
+
+@pytest.mark.parametrize("name", sorted(G.predict_cases()))
+def test_predict_match_golden(name):
+    """The fused tracking step equals predict_projection followed by MapMatcher.match on the in-view landmarks."""
+    c = G.predict_cases()[name]
+    mm = _mm(int(c["W"]), int(c["H"]))
+    try:
+        args = G.predict_args(c)[:-2]                       # W, H come from the matcher
+        uv, S, ok, depth, k, d, d2 = mm.predict_match(*args, c["kp"], c["desc"], c["lmd"], c["lnd"])
+    finally:
+        mm.close()
+    for got, key in ((uv, "uv"), (S, "S"), (depth, "depth")):
+        assert np.array_equal(got.view(np.uint64), c[key].view(np.uint64)), key
+    assert np.array_equal(ok, c["ok"])
+    sel = c["sel"]
+    assert G.same_outputs((k[sel], d[sel], d2[sel]), (c["m_kp"], c["m_d"], c["m_d2"]))
+    rest = np.setdiff1d(np.arange(len(ok)), sel)
+    assert (k[rest] == -1).all() and (d[rest] == 9999).all() and np.isinf(d2[rest]).all()
+
+
+def test_predict_match_random_vs_oracle():
+    """A larger random window (5,000 landmarks, non-zero pose covariance) through the fused call, against the oracle's
+    predict_projection + map matcher."""
+    rng = np.random.default_rng(21)
+    L, W, H = 5000, 1280, 720
+    th = rng.normal(0, 0.05, 3)
+    K = np.array([[0, -th[2], th[1]], [th[2], 0, -th[0]], [-th[1], th[0], 0]])
+    Rwb = np.eye(3) + K + 0.5 * K @ K
+    args = dict(Rwb_t=Rwb, pwb_t=rng.normal(0, 0.1, 3), Rbc=np.array([[0.0, 0.0, 1.0], [-1.0, 0.0, 0.0],
+                                                                      [0.0, -1.0, 0.0]]),
+                pbc=np.array([0.1, 0.0, 0.02]), Rwc_h=np.tile(np.array([[0.0, 0.0, 1.0], [-1.0, 0.0, 0.0],
+                                                                        [0.0, -1.0, 0.0]]), (L, 1, 1)),
+                pwc_h=rng.normal(0, 0.5, (L, 3)) - np.array([2.0, 0.0, 0.0]),
+                lmp=np.stack([rng.uniform(-0.8, 0.8, L), rng.uniform(-0.5, 0.5, L), rng.uniform(0.05, 0.5, L)], 1),
+                Spose=np.diag([1e-6, 1e-6, 1e-6, 1e-4, 1e-4, 1e-4]), Sl=np.tile(np.eye(3) * 1e-6, (L, 1, 1)),
+                sig_px=1.5, fx=640.0, fy=640.0, cx=640.0, cy=360.0)
+    order = ("Rwb_t", "pwb_t", "Rbc", "pbc", "Rwc_h", "pwc_h", "lmp", "Spose", "Sl", "sig_px", "fx", "fy", "cx", "cy")
+    a = [args[k] for k in order]
+    uv0, S0, ok0, dep0 = np.full((L, 2), np.nan), np.zeros((L, 2, 2)), np.zeros(L, np.bool_), np.zeros(L)
+    O.predict_projection(*a, float(W), float(H), uv0, S0, ok0, dep0)
+    sel = np.nonzero(ok0)[0]
+    kp = np.concatenate([uv0[sel] + rng.normal(0, 1.0, (len(sel), 2)), rng.uniform(0, 700, (300, 2))])
+    lmd = rng.integers(0, 256, (L, 3, 32), dtype=np.uint8)
+    desc = np.concatenate([lmd[sel, 0], rng.integers(0, 256, (300, 32), dtype=np.uint8)])
+    lnd = rng.integers(1, 4, L).astype(np.int64)
+    mm = _mm(W, H)
+    try:
+        uv, S, ok, depth, k, d, d2 = mm.predict_match(*a, kp, desc, lmd, lnd)
+    finally:
+        mm.close()
+    assert np.array_equal(ok, ok0) and np.array_equal(uv.view(np.uint64), uv0.view(np.uint64))
+    assert np.array_equal(S.view(np.uint64), S0.view(np.uint64)) and np.array_equal(depth, dep0)
+    want = O.mapmatch(kp, desc, uv0[sel], S0[sel], lmd[sel], lnd[sel], W, H)
+    assert G.same_outputs((k[sel], d[sel], d2[sel]), want)
+    assert len(sel) > 1000 and (want[0] >= 0).sum() > 500

@@ -96,3 +96,21 @@ def test_mapmatch_oracle_edges():
     with pytest.raises(ValueError):
         O.mapmatch(kp, d, np.array([[10.0, 10.0]]), np.eye(2)[None], np.zeros((1, 2, 32), np.uint8), np.array([3]),
                    64, 64)
+
+
+@pytest.mark.parametrize("name", sorted(G.predict_cases()))
+def test_predict_projection_matches_reference(name):
+    """The oracle's window.predict_projection against the reference's numba function, bit for bit, with the outputs
+    pre-filled as the engine fills them (entries the reference leaves alone stay as they were); then the map matcher
+    on the in-view landmarks."""
+    c = G.predict_cases()[name]
+    uv, S, ok, depth = c["uv0"].copy(), c["S0"].copy(), c["ok0"].copy(), c["depth0"].copy()
+    with np.errstate(all="ignore"):
+        O.predict_projection(*G.predict_args(c), uv, S, ok, depth)
+    for got, k in ((uv, "uv"), (S, "S"), (depth, "depth")):
+        assert np.array_equal(got.view(np.uint64), c[k].view(np.uint64)), k
+    assert np.array_equal(ok, c["ok"])
+    sel = np.nonzero(ok)[0]
+    with np.errstate(all="ignore"):
+        got = O.mapmatch(c["kp"], c["desc"], uv[sel], S[sel], c["lmd"][sel], c["lnd"][sel], int(c["W"]), int(c["H"]))
+    assert G.same_outputs(got, (c["m_kp"], c["m_d"], c["m_d2"]))

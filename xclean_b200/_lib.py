@@ -130,6 +130,9 @@ _SIGS.update({
     "xcb_mm_match_host": (c_int, [P, P, c_int, P, P, P, P, c_int, P, c_int, c_double, P, P, P, P]),
     "xcb_mm_match_dev": (c_int, [P, c_int, P, P, c_int, P, P, P, P, c_int, P, P, c_int, c_double, P, P, P, P]),
     "xcb_mm_sync": (c_int, [P, P]),
+    "xcb_mm_predict_host": (c_int, [P, P, P, P, P, P, P, P, P, P] + [c_double] * 7 + [c_int, P, P, P, P, P]),
+    "xcb_mm_predict_match_host": (c_int, [P, P, P, P, P, P, P, P, P, P] + [c_double] * 5
+                                  + [c_int, P, c_int, P, P, c_int, P, c_double, P, P, P, P, P, P, P, P]),
 })
 
 _SIGS.update({

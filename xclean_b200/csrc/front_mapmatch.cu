@@ -495,54 +495,74 @@ static int mm_launch(xcb_mm* m, MMArgs& a, int F, bool kp_f32, cudaStream_t st)
 
 static size_t mm_al(size_t n) { return (n + 255) & ~(size_t)255; }
 
-extern "C" int xcb_mm_match_host(xcb_mm* m, const double* kp, int N, const uint8_t* desc, const double* uv,
-                                 const double* S, const uint8_t* lm_desc, int D, const int64_t* lm_ndesc, int L,
-                                 double chi2, int64_t* out_kp, int64_t* out_d, double* out_d2, void* stream)
+// scratch for N keypoints and L landmarks per frame (grown, never shrunk)
+static int mm_reserve(xcb_mm* m, int N, int L)
 {
-    if (!m) return mm_fail(nullptr, XCB_ERR_ARG, "mm_match_host: null handle");
-    if (N < 0 || L < 0 || D < 0) return mm_fail(m, XCB_ERR_ARG, "mm_match_host: negative size");
-    if (L > 0 && (!uv || !S || !lm_ndesc || !out_kp || !out_d || !out_d2 || (D > 0 && !lm_desc)))
-        return mm_fail(m, XCB_ERR_ARG, "mm_match_host: null landmark argument");
-    if (N > 0 && (!kp || !desc)) return mm_fail(m, XCB_ERR_ARG, "mm_match_host: null keypoint argument");
+    if (N <= m->cap_kp && L <= m->cap_lm) return XCB_OK;
+    MCK(cudaStreamSynchronize(m->stream), "mapmatch: sync");
+    return mm_alloc_scratch(m, std::max(N, m->cap_kp), std::max(L, m->cap_lm));
+}
+
+// page-locked staging blocks and their device twins for the host entries (grown, never shrunk); waits for `st`,
+// whose previous call may still read them
+static int mm_staging(xcb_mm* m, size_t in_bytes, size_t out_bytes, cudaStream_t st)
+{
+    MCK(cudaStreamSynchronize(st), "mapmatch: sync");
+    if (in_bytes > m->in_cap) {
+        MCK(cudaStreamSynchronize(m->stream), "mapmatch: sync");
+        cudaFreeHost(m->h_in);
+        cudaFree(m->d_in);
+        m->h_in = m->d_in = nullptr;
+        m->in_cap = 0;
+        MCK(cudaMallocHost(&m->h_in, in_bytes * 2), "mapmatch: staging");
+        MCK(cudaMalloc(&m->d_in, in_bytes * 2), "mapmatch: staging");
+        m->in_cap = in_bytes * 2;
+    }
+    if (out_bytes > m->out_cap) {
+        MCK(cudaStreamSynchronize(m->stream), "mapmatch: sync");
+        cudaFreeHost(m->h_out);
+        cudaFree(m->d_out);
+        m->h_out = m->d_out = nullptr;
+        m->out_cap = 0;
+        MCK(cudaMallocHost(&m->h_out, out_bytes * 2), "mapmatch: staging");
+        MCK(cudaMalloc(&m->d_out, out_bytes * 2), "mapmatch: staging");
+        m->out_cap = out_bytes * 2;
+    }
+    return XCB_OK;
+}
+
+static int mm_check_match_args(xcb_mm* m, const double* kp, int N, const uint8_t* desc, const uint8_t* lm_desc, int D,
+                               const int64_t* lm_ndesc, int L, int64_t* out_kp, int64_t* out_d, double* out_d2,
+                               const char* who)
+{
+    if (N < 0 || L < 0 || D < 0) return mm_fail(m, XCB_ERR_ARG, std::string(who) + ": negative size");
+    if (L > 0 && (!lm_ndesc || !out_kp || !out_d || !out_d2 || (D > 0 && !lm_desc)))
+        return mm_fail(m, XCB_ERR_ARG, std::string(who) + ": null landmark argument");
+    if (N > 0 && (!kp || !desc)) return mm_fail(m, XCB_ERR_ARG, std::string(who) + ": null keypoint argument");
     for (int l = 0; l < L; ++l)
-        if (lm_ndesc[l] > D) return mm_fail(m, XCB_ERR_ARG, "mm_match_host: lm_ndesc above the descriptor slots");
+        if (lm_ndesc[l] > D) return mm_fail(m, XCB_ERR_ARG, std::string(who) + ": lm_ndesc above the descriptor slots");
     for (int l = 0; l < L; ++l) {           // mapmatch.py:151-153 defaults; returned as they are when L or N is 0
         out_kp[l] = -1;
         out_d[l] = MM_NONE;
         out_d2[l] = INFINITY;
     }
-    if (L == 0 || N == 0) return XCB_OK;
-    if (N > m->cap_kp || L > m->cap_lm) {
-        MCK(cudaStreamSynchronize(m->stream), "mm_match_host: sync");
-        const int rc = mm_alloc_scratch(m, std::max(N, m->cap_kp), std::max(L, m->cap_lm));
-        if (rc) return rc;
-    }
+    return XCB_OK;
+}
+
+extern "C" int xcb_mm_match_host(xcb_mm* m, const double* kp, int N, const uint8_t* desc, const double* uv,
+                                 const double* S, const uint8_t* lm_desc, int D, const int64_t* lm_ndesc, int L,
+                                 double chi2, int64_t* out_kp, int64_t* out_d, double* out_d2, void* stream)
+{
+    if (!m) return mm_fail(nullptr, XCB_ERR_ARG, "mm_match_host: null handle");
+    if (L > 0 && (!uv || !S)) return mm_fail(m, XCB_ERR_ARG, "mm_match_host: null landmark argument");
+    int rc = mm_check_match_args(m, kp, N, desc, lm_desc, D, lm_ndesc, L, out_kp, out_d, out_d2, "mm_match_host");
+    if (rc || L == 0 || N == 0) return rc;
+    if ((rc = mm_reserve(m, N, L))) return rc;
     const size_t o_desc = mm_al((size_t)N * 16), o_uv = o_desc + mm_al((size_t)N * 32), o_S = o_uv + mm_al((size_t)L * 16);
     const size_t o_lmd = o_S + mm_al((size_t)L * 32), o_lnd = o_lmd + mm_al((size_t)L * D * 32);
     const size_t in_bytes = o_lnd + mm_al((size_t)L * 8), out_bytes = (size_t)L * 24;
-    if (in_bytes > m->in_cap || out_bytes > m->out_cap) {
-        MCK(cudaStreamSynchronize(m->stream), "mm_match_host: sync");
-        if (in_bytes > m->in_cap) {
-            cudaFreeHost(m->h_in);
-            cudaFree(m->d_in);
-            m->h_in = m->d_in = nullptr;
-            m->in_cap = 0;
-            MCK(cudaMallocHost(&m->h_in, in_bytes * 2), "mm_match_host: staging");
-            MCK(cudaMalloc(&m->d_in, in_bytes * 2), "mm_match_host: staging");
-            m->in_cap = in_bytes * 2;
-        }
-        if (out_bytes > m->out_cap) {
-            cudaFreeHost(m->h_out);
-            cudaFree(m->d_out);
-            m->h_out = m->d_out = nullptr;
-            m->out_cap = 0;
-            MCK(cudaMallocHost(&m->h_out, out_bytes * 2), "mm_match_host: staging");
-            MCK(cudaMalloc(&m->d_out, out_bytes * 2), "mm_match_host: staging");
-            m->out_cap = out_bytes * 2;
-        }
-    }
     cudaStream_t st = stream ? (cudaStream_t)stream : m->stream;
-    MCK(cudaStreamSynchronize(st), "mm_match_host: sync");      // the staging block may still feed a previous call
+    if ((rc = mm_staging(m, in_bytes, out_bytes, st))) return rc;
     std::memcpy(m->h_in, kp, (size_t)N * 16);
     std::memcpy(m->h_in + o_desc, desc, (size_t)N * 32);
     std::memcpy(m->h_in + o_uv, uv, (size_t)L * 16);
@@ -566,13 +586,319 @@ extern "C" int xcb_mm_match_host(xcb_mm* m, const double* kp, int N, const uint8
     a.out_kp = (i64*)m->d_out;
     a.out_d = (i64*)(m->d_out + (size_t)L * 8);
     a.out_d2 = (double*)(m->d_out + (size_t)L * 16);
-    int rc = mm_launch(m, a, 1, false, st);
-    if (rc) return rc;
+    if ((rc = mm_launch(m, a, 1, false, st))) return rc;
     MCK(cudaMemcpyAsync(m->h_out, m->d_out, out_bytes, cudaMemcpyDeviceToHost, st), "mm_match_host: D2H");
     MCK(cudaStreamSynchronize(st), "mm_match_host: kernels");
     std::memcpy(out_kp, m->h_out, (size_t)L * 8);
     std::memcpy(out_d, m->h_out + (size_t)L * 8, (size_t)L * 8);
     std::memcpy(out_d2, m->h_out + (size_t)L * 16, (size_t)L * 8);
+    return XCB_OK;
+}
+
+// ------------------------------------------------------------------------------------------------ gating prediction
+// window.predict_projection (src/xclean/vio/window.py:1032-1144) on the device, one thread per landmark.  The file is
+// built with --fmad=false, so every product and sum below is a separate IEEE round-to-nearest operation, evaluated
+// left to right in the reference's order (numba contracts nothing either).
+struct PredArgs {
+    double Rwb[9], pwb[3], Rbc[9], pbc[3], Spose[36];   // predicted body pose, body-to-camera extrinsic, pose covariance
+    const double* Rwc_h;      // [L][3][3] host camera rotations
+    const double* pwc_h;      // [L][3] host camera centres
+    const double* lmp;        // [L][3] (a, b, rho)
+    const double* Sl;         // [L][3][3] landmark marginals
+    double sig_px, fx, fy, cx, cy, W, H;
+    int L;
+    double* uv;               // [L][2] written where the point is in front, else NaN
+    double* S;                // [L][2][2] written where it is also inside the image, else 0
+    double* depth;            // [L] written where the point is in front, else 0
+    u8* ok;                   // [L]
+    u8* wr;                   // [L] 0: nothing written, 1: uv + depth, 2: uv + depth + S (the reference's writes)
+    const i64* lnd_in;        // [L] descriptor counts, or NULL: no map matching follows
+    i64* lnd_eff;             // [L] lnd_in where ok, else 0 (the landmarks the map matcher then sees)
+};
+
+__device__ __forceinline__ void pp_mm3(const double* A, const double* B, double* o)
+{
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) o[3 * i + j] = A[3 * i] * B[j] + A[3 * i + 1] * B[3 + j] + A[3 * i + 2] * B[6 + j];
+}
+
+__global__ void __launch_bounds__(128) k_mm_predict(PredArgs a)
+{
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= a.L) return;
+    double Rwc_t[9], pwc_t[3], Rcb[9], Px[9], Wt[9], Rct[9], RctWt[9];
+    pp_mm3(a.Rwb, a.Rbc, Rwc_t);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) pwc_t[i] = a.pwb[i] + a.Rwb[3 * i] * a.pbc[0] + a.Rwb[3 * i + 1] * a.pbc[1] + a.Rwb[3 * i + 2] * a.pbc[2];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            Rcb[3 * i + j] = a.Rbc[3 * j + i];
+            Px[3 * i + j] = 0.0;
+        }
+    Px[1] = -a.pbc[2]; Px[2] = a.pbc[1]; Px[3] = a.pbc[2]; Px[5] = -a.pbc[0]; Px[6] = -a.pbc[1]; Px[7] = a.pbc[0];
+    pp_mm3(a.Rwb, Px, Wt);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) Rct[3 * i + j] = Rwc_t[3 * j + i];
+    pp_mm3(Rct, Wt, RctWt);
+    u8 wr = 0;
+    double u = XCB_NAN, v = XCB_NAN, dep = 0.0, Sv[4] = {0.0, 0.0, 0.0, 0.0};
+    const double* R = a.Rwc_h + 9 * (size_t)l;
+    const double la = a.lmp[3 * l], lb = a.lmp[3 * l + 1], rho = a.lmp[3 * l + 2];
+    const double d0 = a.pwc_h[3 * l] - pwc_t[0], d1 = a.pwc_h[3 * l + 1] - pwc_t[1], d2 = a.pwc_h[3 * l + 2] - pwc_t[2];
+    const double Y0 = R[0] * la + R[1] * lb + R[2] + rho * d0;
+    const double Y1 = R[3] * la + R[4] * lb + R[5] + rho * d1;
+    const double Y2 = R[6] * la + R[7] * lb + R[8] + rho * d2;
+    const double q0 = Rct[0] * Y0 + Rct[1] * Y1 + Rct[2] * Y2;
+    const double q1 = Rct[3] * Y0 + Rct[4] * Y1 + Rct[5] * Y2;
+    const double q2 = Rct[6] * Y0 + Rct[7] * Y1 + Rct[8] * Y2;
+    if (!(q2 <= 1e-9 || rho <= 0.0)) {
+        dep = q2 / rho;
+        const double iq = 1.0 / q2;
+        u = a.fx * q0 * iq + a.cx;
+        v = a.fy * q1 * iq + a.cy;
+        wr = 1;
+        if (!(u < 0.0 || u >= a.W || v < 0.0 || v >= a.H)) {
+            const double Dp[6] = {a.fx * iq, 0.0, -a.fx * q0 * iq * iq, 0.0, a.fy * iq, -a.fy * q1 * iq * iq};
+            const double Qx[9] = {0.0, -q2, q1, q2, 0.0, -q0, -q1, q0, 0.0};
+            double QR[9], Jp[12], Jl[6], RcR[9];
+            pp_mm3(Qx, Rcb, QR);
+#pragma unroll
+            for (int r = 0; r < 2; ++r)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    Jp[6 * r + j] = Dp[3 * r] * (QR[j] + rho * RctWt[j]) + Dp[3 * r + 1] * (QR[3 + j] + rho * RctWt[3 + j])
+                                    + Dp[3 * r + 2] * (QR[6 + j] + rho * RctWt[6 + j]);
+                    Jp[6 * r + 3 + j] = -rho * (Dp[3 * r] * Rct[j] + Dp[3 * r + 1] * Rct[3 + j] + Dp[3 * r + 2] * Rct[6 + j]);
+                }
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j)
+                    RcR[3 * i + j] = Rct[3 * i] * R[j] + Rct[3 * i + 1] * R[3 + j] + Rct[3 * i + 2] * R[6 + j];
+            const double e0 = Rct[0] * d0 + Rct[1] * d1 + Rct[2] * d2;
+            const double e1 = Rct[3] * d0 + Rct[4] * d1 + Rct[5] * d2;
+            const double e2 = Rct[6] * d0 + Rct[7] * d1 + Rct[8] * d2;
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+                Jl[3 * r] = Dp[3 * r] * RcR[0] + Dp[3 * r + 1] * RcR[3] + Dp[3 * r + 2] * RcR[6];
+                Jl[3 * r + 1] = Dp[3 * r] * RcR[1] + Dp[3 * r + 1] * RcR[4] + Dp[3 * r + 2] * RcR[7];
+                Jl[3 * r + 2] = Dp[3 * r] * e0 + Dp[3 * r + 1] * e1 + Dp[3 * r + 2] * e2;
+            }
+            const double* sl = a.Sl + 9 * (size_t)l;
+            double t6[12], t3[6];
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+#pragma unroll
+                for (int j = 0; j < 6; ++j) {
+                    double acc = 0.0;
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) acc += Jp[6 * r + k] * a.Spose[6 * k + j];
+                    t6[6 * r + j] = acc;
+                }
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    double acc = 0.0;
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) acc += Jl[3 * r + k] * sl[3 * k + j];
+                    t3[3 * r + j] = acc;
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < 2; ++r)
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    double acc = 0.0;
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) acc += t6[6 * r + k] * Jp[6 * c + k];
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) acc += t3[3 * r + k] * Jl[3 * c + k];
+                    Sv[2 * r + c] = acc + (r == c ? a.sig_px * a.sig_px : 0.0);
+                }
+            wr = 2;
+        }
+    }
+    a.uv[2 * l] = u;
+    a.uv[2 * l + 1] = v;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) a.S[4 * (size_t)l + i] = Sv[i];
+    a.depth[l] = dep;
+    a.ok[l] = wr == 2;
+    a.wr[l] = wr;
+    if (a.lnd_in) a.lnd_eff[l] = wr == 2 ? a.lnd_in[l] : 0;
+}
+
+// the reference's writes into the caller's arrays: ok everywhere, uv / depth / S only where it writes them
+static void pp_scatter(int L, const char* ho, double* uv, double* S, uint8_t* ok, double* depth)
+{
+    const double* duv = (const double*)ho;
+    const double* dS = (const double*)(ho + (size_t)L * 16);
+    const double* ddep = (const double*)(ho + (size_t)L * 48);
+    const u8* dok = (const u8*)(ho + (size_t)L * 56);
+    const u8* dwr = dok + L;
+    for (int l = 0; l < L; ++l) {
+        ok[l] = dok[l];
+        if (dwr[l] >= 1) {
+            uv[2 * l] = duv[2 * l];
+            uv[2 * l + 1] = duv[2 * l + 1];
+            depth[l] = ddep[l];
+        }
+        if (dwr[l] == 2)
+            for (int i = 0; i < 4; ++i) S[4 * (size_t)l + i] = dS[4 * (size_t)l + i];
+    }
+}
+
+static int pp_setup(xcb_mm* m, PredArgs& p, const double* Rwb_t, const double* pwb_t, const double* Rbc,
+                    const double* pbc, const double* Spose, double sig_px, double fx, double fy, double cx, double cy,
+                    double W, double H, int L, const char* who)
+{
+    if (!Rwb_t || !pwb_t || !Rbc || !pbc || !Spose) return mm_fail(m, XCB_ERR_ARG, std::string(who) + ": null pose");
+    if (L < 0) return mm_fail(m, XCB_ERR_ARG, std::string(who) + ": negative size");
+    std::memcpy(p.Rwb, Rwb_t, sizeof(p.Rwb));
+    std::memcpy(p.pwb, pwb_t, sizeof(p.pwb));
+    std::memcpy(p.Rbc, Rbc, sizeof(p.Rbc));
+    std::memcpy(p.pbc, pbc, sizeof(p.pbc));
+    std::memcpy(p.Spose, Spose, sizeof(p.Spose));
+    p.sig_px = sig_px;
+    p.fx = fx;
+    p.fy = fy;
+    p.cx = cx;
+    p.cy = cy;
+    p.W = W;
+    p.H = H;
+    p.L = L;
+    return XCB_OK;
+}
+
+// device layout of the prediction outputs (and the host copy): uv 16L, S 32L, depth 8L, ok L, wr L
+static size_t pp_out_bytes(int L) { return mm_al((size_t)L * 58); }
+
+static void pp_outputs(PredArgs& p, char* base, int L)
+{
+    p.uv = (double*)base;
+    p.S = (double*)(base + (size_t)L * 16);
+    p.depth = (double*)(base + (size_t)L * 48);
+    p.ok = (u8*)(base + (size_t)L * 56);
+    p.wr = p.ok + L;
+}
+
+extern "C" int xcb_mm_predict_host(xcb_mm* m, const double* Rwb_t, const double* pwb_t, const double* Rbc,
+                                   const double* pbc, const double* Rwc_h, const double* pwc_h, const double* lmp,
+                                   const double* Spose, const double* Sl, double sig_px, double fx, double fy,
+                                   double cx, double cy, double W, double H, int L, double* uv, double* S, uint8_t* ok,
+                                   double* depth, void* stream)
+{
+    if (!m) return mm_fail(nullptr, XCB_ERR_ARG, "mm_predict_host: null handle");
+    PredArgs p = {};
+    int rc = pp_setup(m, p, Rwb_t, pwb_t, Rbc, pbc, Spose, sig_px, fx, fy, cx, cy, W, H, L, "mm_predict_host");
+    if (rc || L == 0) return rc;
+    if (!Rwc_h || !pwc_h || !lmp || !Sl || !uv || !S || !ok || !depth)
+        return mm_fail(m, XCB_ERR_ARG, "mm_predict_host: null landmark argument");
+    const size_t o_p = mm_al((size_t)L * 72), o_l = o_p + mm_al((size_t)L * 24), o_s = o_l + mm_al((size_t)L * 24);
+    const size_t in_bytes = o_s + mm_al((size_t)L * 72), out_bytes = pp_out_bytes(L);
+    cudaStream_t st = stream ? (cudaStream_t)stream : m->stream;
+    if ((rc = mm_staging(m, in_bytes, out_bytes, st))) return rc;
+    std::memcpy(m->h_in, Rwc_h, (size_t)L * 72);
+    std::memcpy(m->h_in + o_p, pwc_h, (size_t)L * 24);
+    std::memcpy(m->h_in + o_l, lmp, (size_t)L * 24);
+    std::memcpy(m->h_in + o_s, Sl, (size_t)L * 72);
+    MCK(cudaMemcpyAsync(m->d_in, m->h_in, in_bytes, cudaMemcpyHostToDevice, st), "mm_predict_host: H2D");
+    p.Rwc_h = (const double*)m->d_in;
+    p.pwc_h = (const double*)(m->d_in + o_p);
+    p.lmp = (const double*)(m->d_in + o_l);
+    p.Sl = (const double*)(m->d_in + o_s);
+    pp_outputs(p, m->d_out, L);
+    k_mm_predict<<<(L + 127) / 128, 128, 0, st>>>(p);
+    MCK(cudaGetLastError(), "mm_predict_host: launch");
+    MCK(cudaMemcpyAsync(m->h_out, m->d_out, (size_t)L * 58, cudaMemcpyDeviceToHost, st), "mm_predict_host: D2H");
+    MCK(cudaStreamSynchronize(st), "mm_predict_host: kernel");
+    pp_scatter(L, m->h_out, uv, S, ok, depth);
+    return XCB_OK;
+}
+
+extern "C" int xcb_mm_predict_match_host(xcb_mm* m, const double* Rwb_t, const double* pwb_t, const double* Rbc,
+                                         const double* pbc, const double* Rwc_h, const double* pwc_h, const double* lmp,
+                                         const double* Spose, const double* Sl, double sig_px, double fx, double fy,
+                                         double cx, double cy, int L, const double* kp, int N, const uint8_t* desc,
+                                         const uint8_t* lm_desc, int D, const int64_t* lm_ndesc, double chi2,
+                                         double* uv, double* S, uint8_t* ok, double* depth, int64_t* out_kp,
+                                         int64_t* out_d, double* out_d2, void* stream)
+{
+    if (!m) return mm_fail(nullptr, XCB_ERR_ARG, "mm_predict_match_host: null handle");
+    PredArgs p = {};
+    int rc = pp_setup(m, p, Rwb_t, pwb_t, Rbc, pbc, Spose, sig_px, fx, fy, cx, cy, (double)m->W, (double)m->H, L,
+                      "mm_predict_match_host");
+    if (rc) return rc;
+    if (L > 0 && (!Rwc_h || !pwc_h || !lmp || !Sl || !uv || !S || !ok || !depth))
+        return mm_fail(m, XCB_ERR_ARG, "mm_predict_match_host: null landmark argument");
+    if ((rc = mm_check_match_args(m, kp, N, desc, lm_desc, D, lm_ndesc, L, out_kp, out_d, out_d2,
+                                  "mm_predict_match_host")))
+        return rc;
+    if (L == 0) return XCB_OK;
+    if ((rc = mm_reserve(m, N, L))) return rc;
+    const size_t o_p = mm_al((size_t)L * 72), o_l = o_p + mm_al((size_t)L * 24), o_s = o_l + mm_al((size_t)L * 24);
+    const size_t o_kp = o_s + mm_al((size_t)L * 72), o_desc = o_kp + mm_al((size_t)N * 16);
+    const size_t o_lmd = o_desc + mm_al((size_t)N * 32), o_lnd = o_lmd + mm_al((size_t)L * D * 32);
+    const size_t in_bytes = o_lnd + mm_al((size_t)L * 8);
+    const size_t o_mo = pp_out_bytes(L), o_eff = o_mo + mm_al((size_t)L * 24), out_bytes = o_eff + mm_al((size_t)L * 8);
+    cudaStream_t st = stream ? (cudaStream_t)stream : m->stream;
+    if ((rc = mm_staging(m, in_bytes, out_bytes, st))) return rc;
+    std::memcpy(m->h_in, Rwc_h, (size_t)L * 72);
+    std::memcpy(m->h_in + o_p, pwc_h, (size_t)L * 24);
+    std::memcpy(m->h_in + o_l, lmp, (size_t)L * 24);
+    std::memcpy(m->h_in + o_s, Sl, (size_t)L * 72);
+    if (N > 0) {
+        std::memcpy(m->h_in + o_kp, kp, (size_t)N * 16);
+        std::memcpy(m->h_in + o_desc, desc, (size_t)N * 32);
+    }
+    if (D > 0) std::memcpy(m->h_in + o_lmd, lm_desc, (size_t)L * D * 32);
+    std::memcpy(m->h_in + o_lnd, lm_ndesc, (size_t)L * 8);
+    MCK(cudaMemcpyAsync(m->d_in, m->h_in, in_bytes, cudaMemcpyHostToDevice, st), "mm_predict_match_host: H2D");
+    p.Rwc_h = (const double*)m->d_in;
+    p.pwc_h = (const double*)(m->d_in + o_p);
+    p.lmp = (const double*)(m->d_in + o_l);
+    p.Sl = (const double*)(m->d_in + o_s);
+    p.lnd_in = (const i64*)(m->d_in + o_lnd);
+    p.lnd_eff = (i64*)(m->d_out + o_eff);
+    pp_outputs(p, m->d_out, L);
+    k_mm_predict<<<(L + 127) / 128, 128, 0, st>>>(p);
+    MCK(cudaGetLastError(), "mm_predict_match_host: launch");
+    size_t d2h = o_mo;
+    if (N > 0) {
+        // the landmarks out of view carry no descriptors, so the gate skips them: the in-view ones are matched in
+        // landmark order exactly as MapMatcher.match on the in-view subset matches them
+        MMArgs a = {};
+        a.kp = m->d_in + o_kp;
+        a.nkp1 = N;
+        a.kp_stride = N;
+        a.desc = (const u8*)(m->d_in + o_desc);
+        a.uv = p.uv;
+        a.S = p.S;
+        a.lmd = (const u8*)(m->d_in + o_lmd);
+        a.lnd = p.lnd_eff;
+        a.nlm1 = L;
+        a.lm_stride = L;
+        a.D = D;
+        a.chi2 = chi2;
+        a.out_kp = (i64*)(m->d_out + o_mo);
+        a.out_d = a.out_kp + L;
+        a.out_d2 = (double*)(a.out_d + L);
+        if ((rc = mm_launch(m, a, 1, false, st))) return rc;
+        d2h = o_mo + (size_t)L * 24;
+    }
+    MCK(cudaMemcpyAsync(m->h_out, m->d_out, d2h, cudaMemcpyDeviceToHost, st), "mm_predict_match_host: D2H");
+    MCK(cudaStreamSynchronize(st), "mm_predict_match_host: kernels");
+    pp_scatter(L, m->h_out, uv, S, ok, depth);
+    if (N > 0) {
+        std::memcpy(out_kp, m->h_out + o_mo, (size_t)L * 8);
+        std::memcpy(out_d, m->h_out + o_mo + (size_t)L * 8, (size_t)L * 8);
+        std::memcpy(out_d2, m->h_out + o_mo + (size_t)L * 16, (size_t)L * 8);
+    }
     return XCB_OK;
 }
 

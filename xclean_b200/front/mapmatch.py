@@ -14,6 +14,12 @@ Same API and the same outputs as the reference (src/xclean/front/mapmatch.py:132
 Every call runs three kernels of libxcb200.so (xcb_mm_match_host, include/xcb200.h); there is no CPU path.
 `match_dev` (no reference counterpart) matches a batch of frames already in device memory, e.g. the frontend's
 keypoints and descriptors, in the same three launches.
+
+Also here, the gating prediction that feeds the matcher (src/xclean/vio/window.py:1032-1144):
+
+    predict_projection(Rwb_t, pwb_t, Rbc, pbc, Rwc_h, pwc_h, lmp, Spose, Sl, sig_px, fx, fy, cx, cy, W, H,
+                       uv, S, ok, depth)                 # = window.predict_projection, in place, bit-identical
+    uv, S, ok, depth, k, d, d2 = mm.predict_match(...)  # _project + match on the in-view landmarks, one call
 """
 from __future__ import annotations
 
@@ -103,6 +109,42 @@ class MapMatcher:
         self.stats["matched"] += int((out_kp >= 0).sum())
         return out_kp, out_d, out_d2
 
+    def predict_match(self, Rwb_t, pwb_t, Rbc, pbc, Rwc_h, pwc_h, lmp, Spose, Sl, sig_px, fx, fy, cx, cy, kp, desc,
+                      lm_desc, lm_ndesc, chi2=CHI2_2_999, stream=0):
+        """The engine's tracking step (engine_live.py:1580-1582): predict_projection of the L landmarks into the
+        predicted pose over this matcher's W x H (uv NaN / S 0 / depth 0 where the reference writes nothing, as
+        _project pre-fills them), then the gated matching of the in-view ones.  -> (uv, S, ok, depth, kp index,
+        distance, d2); the last three have one entry per landmark and equal match(kp, desc, uv[sel], S[sel],
+        lm_desc[sel], lm_ndesc[sel]) at sel = nonzero(ok), defaults elsewhere."""
+        self._own()
+        lmp = np.ascontiguousarray(lmp, np.float64).reshape(-1, 3)
+        L = len(lmp)
+        uv = np.full((L, 2), np.nan)
+        S = np.zeros((L, 2, 2))
+        ok = np.zeros(L, np.bool_)
+        depth = np.zeros(L)
+        out_kp = np.full(L, -1, np.int64)
+        out_d = np.full(L, 9999, np.int64)
+        out_d2 = np.full(L, np.inf)
+        kp64 = np.ascontiguousarray(kp, np.float64).reshape(-1, 2)
+        N = len(kp64)
+        kd = np.ascontiguousarray(desc, np.uint8).reshape(N, 32)
+        lm_desc = np.asarray(lm_desc)
+        D = int(lm_desc.shape[1]) if lm_desc.ndim == 3 else 0
+        ld = np.ascontiguousarray(lm_desc, np.uint8).reshape(L, D, 32)
+        lnd = np.ascontiguousarray(lm_ndesc, np.int64).reshape(L)
+        ins = _pred_inputs(Rwb_t, pwb_t, Rbc, pbc, Rwc_h, pwc_h, lmp, Spose, Sl, L)
+        p = _lib.ptr
+        self._chk(self.L.xcb_mm_predict_match_host(self._h, *[p(a) for a in ins], float(sig_px), float(fx), float(fy),
+                                                   float(cx), float(cy), L, p(kp64), N, p(kd), p(ld), D, p(lnd),
+                                                   float(chi2), p(uv), p(S), p(ok.view(np.uint8)), p(depth),
+                                                   p(out_kp), p(out_d), p(out_d2),
+                                                   ctypes.c_void_p(int(stream) or None)), "mapmatch.predict_match")
+        self.stats["calls"] += 1
+        self.stats["landmarks"] += int(ok.sum())
+        self.stats["matched"] += int((out_kp >= 0).sum())
+        return uv, S, ok, depth, out_kp, out_d, out_d2
+
     def match_dev(self, kp, nkp, desc, uv, S, lm_desc, lm_ndesc, nlm, chi2=CHI2_2_999, out=None, stream=0):
         """F frames in device memory (torch CUDA tensors): kp (F,Nk,2) float32, nkp (F,) int32, desc (F,Nk,32) uint8,
         uv (F,Nl,2) float64, S (F,Nl,2,2) float64, lm_desc (F,Nl,D,32) uint8, lm_ndesc (F,Nl) int64, nlm (F,) int32.
@@ -124,6 +166,44 @@ class MapMatcher:
                                           v(lm_ndesc), v(nlm), Nl, float(chi2), v(out["kp"]), v(out["d"]),
                                           v(out["d2"]), ctypes.c_void_p(int(stream) or None)), "mapmatch.match_dev")
         return out
+
+
+def _pred_inputs(Rwb_t, pwb_t, Rbc, pbc, Rwc_h, pwc_h, lmp, Spose, Sl, L):
+    f = lambda a, shape: np.ascontiguousarray(a, np.float64).reshape(shape)
+    return [f(Rwb_t, (3, 3)), f(pwb_t, (3,)), f(Rbc, (3, 3)), f(pbc, (3,)), f(Rwc_h, (L, 3, 3)), f(pwc_h, (L, 3)),
+            f(lmp, (L, 3)), f(Spose, (6, 6)), f(Sl, (L, 3, 3))]
+
+
+_tls = threading.local()
+
+
+def _pred_handle():
+    h = getattr(_tls, "mm", None)
+    if h is None:
+        h = _tls.mm = MapMatcher(16, 16, max_kp=1, max_lm=1)
+    return h
+
+
+def predict_projection(Rwb_t, pwb_t, Rbc, pbc, Rwc_h, pwc_h, lmp, Spose, Sl, sig_px, fx, fy, cx, cy, W, H, uv, S, ok,
+                       depth):
+    """window.predict_projection on the device: ok (L,) for every landmark, uv (L,2) / depth (L,) where the point is
+    in front, S (L,2,2) where it also projects inside W x H, written into the caller's arrays (float64 / bool,
+    C-contiguous) exactly where the reference writes them; bit-identical values.  Returns 0."""
+    lmp = np.ascontiguousarray(lmp, np.float64).reshape(-1, 3)
+    L = len(lmp)
+    for a, dt, shape in ((uv, np.float64, (L, 2)), (S, np.float64, (L, 2, 2)), (ok, np.bool_, (L,)),
+                         (depth, np.float64, (L,))):
+        if not (isinstance(a, np.ndarray) and a.dtype == dt and a.flags.c_contiguous and a.shape == shape):
+            raise ValueError("predict_projection: outputs must be C-contiguous arrays of the reference's shapes")
+    if L == 0:
+        return 0
+    mm = _pred_handle()
+    ins = _pred_inputs(Rwb_t, pwb_t, Rbc, pbc, Rwc_h, pwc_h, lmp, Spose, Sl, L)
+    p = _lib.ptr
+    mm._chk(mm.L.xcb_mm_predict_host(mm._h, *[p(a) for a in ins], float(sig_px), float(fx), float(fy), float(cx),
+                                     float(cy), float(W), float(H), L, p(uv), p(S), p(ok.view(np.uint8)), p(depth),
+                                     None), "predict_projection")
+    return 0
 
 
 def warmup():

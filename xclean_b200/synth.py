@@ -243,3 +243,55 @@ def map_landmarks(kp, counts, desc, m0, m1, nmatch, n_lm=1500, D=3, seed=0):
             lmd[f, :L, 2:] = rng.integers(0, 256, (L, D - 2, 32), dtype=np.uint8)
         lnd[f, :L] = rng.integers(1, D + 1, L)
     return uv, S, lmd, lnd, nlm
+
+
+def tracking_window(seed, n_lm=2000, cam=None, n_clutter=400):
+    """One tracking step's inputs: a window of n_lm inverse-depth landmarks hosted by 8 keyframes along a forward
+    path (camera z = body x), the predicted body pose one metre ahead of the newest keyframe, pose and landmark
+    covariances, and the frame's keypoints (the in-view projections with 1 px noise, 70 % of them, plus clutter)
+    with descriptors (the landmark's own with ~5 % of the bits flipped).
+    -> dict(pose=[Rwb_t, pwb_t, Rbc, pbc, Rwc_h, pwc_h, lmp, Spose, Sl, sig_px, fx, fy, cx, cy], W, H, kp, desc,
+    lm_desc, lm_ndesc); kp are placed from this module's own float64 projection."""
+    cam = cam or CAM_KITTI
+    rng = np.random.default_rng(seed)
+    Rbc = np.array([[0.0, 0.0, 1.0], [-1.0, 0.0, 0.0], [0.0, -1.0, 0.0]])
+    pbc = np.array([0.3, -0.1, 0.05])
+    nh = 8
+    def rz(a):                                          # body yaw (z up)
+        c, s = math.cos(a), math.sin(a)
+        return np.array([[c, -s, 0.0], [s, c, 0.0], [0.0, 0.0, 1.0]])
+
+    yaw_h = [rz(rng.normal(0, 0.01)) for _ in range(nh)]
+    pwb_h = [np.array([1.0 * i, rng.normal(0, 0.05), 0.0]) for i in range(nh)]
+    host = rng.integers(0, nh, n_lm)
+    Rwc_h = np.stack([yaw_h[h] @ Rbc for h in host])
+    pwc_h = np.stack([pwb_h[h] + yaw_h[h] @ pbc for h in host])
+    lmp = np.stack([rng.uniform(-0.6, 0.6, n_lm), rng.uniform(-0.2, 0.2, n_lm), rng.uniform(0.03, 0.3, n_lm)], 1)
+    Rwb_t = yaw_h[-1]
+    pwb_t = pwb_h[-1] + np.array([1.0, 0.0, 0.0])
+    A = rng.normal(0, 0.002, (6, 6))
+    Spose = A @ A.T
+    B = rng.normal(0, 0.002, (n_lm, 3, 3))
+    Sl = np.einsum("lij,lkj->lik", B, B)
+    fx, fy, cx, cy = cam.fx, cam.fy, cam.cx, cam.cy
+    # in-view projections (plain float64 pinhole; the exact values come from predict_projection itself)
+    Rwc_t = Rwb_t @ Rbc
+    pwc_t = pwb_t + Rwb_t @ pbc
+    m = np.stack([lmp[:, 0], lmp[:, 1], np.ones(n_lm)], 1)
+    Pw = pwc_h + np.einsum("nij,nj->ni", Rwc_h, m) / lmp[:, 2:3]
+    Xc = (Pw - pwc_t) @ Rwc_t
+    with np.errstate(all="ignore"):
+        u = fx * Xc[:, 0] / Xc[:, 2] + cx
+        v = fy * Xc[:, 1] / Xc[:, 2] + cy
+    vis = np.nonzero((Xc[:, 2] > 0.1) & (u >= 0) & (u < cam.W) & (v >= 0) & (v < cam.H))[0]
+    seen = vis[rng.random(len(vis)) < 0.7]
+    lm_desc = rng.integers(0, 256, (n_lm, 3, 32), dtype=np.uint8)
+    lm_ndesc = rng.integers(1, 4, n_lm).astype(np.int64)
+    kp = np.concatenate([np.stack([u[seen], v[seen]], 1) + rng.normal(0, 1.0, (len(seen), 2)),
+                         np.stack([rng.uniform(0, cam.W, n_clutter), rng.uniform(0, cam.H, n_clutter)], 1)])
+    flips = np.packbits(rng.random((len(seen), 256)) < 0.05, axis=1)
+    desc = np.concatenate([lm_desc[seen, 0] ^ flips, rng.integers(0, 256, (n_clutter, 32), dtype=np.uint8)])
+    perm = rng.permutation(len(kp))
+    return dict(pose=[Rwb_t, pwb_t, Rbc, pbc, Rwc_h, pwc_h, lmp, Spose, Sl, 1.0, float(fx), float(fy), float(cx),
+                      float(cy)], W=cam.W, H=cam.H, kp=kp[perm].astype(np.float32), desc=desc[perm],
+                lm_desc=lm_desc, lm_ndesc=lm_ndesc)
