@@ -277,6 +277,19 @@ int xcb_ba_newton_windows_dev(const xcb_ba_windows* w, int max_slots, int mode, 
    xcb_ba_newton_scratch_bytes(nw, Lt) bytes (Lt: the batch's landmarks).  stats [nw][8] as xcb_ba_solve_windows_dev. */
 int xcb_ba_solve_windows_free_dev(const xcb_ba_windows* w, int Lt, int max_slots, int iters, double lam0,
                                   double* stats, void* scratch, size_t scratch_bytes, int grid, void* stream);
+/* window.posefree_cost and window.posefree_step (src/xclean/vio/window.py:683-765): the pose-free landmarks of one
+   window (seen only in their host's left image; the batched solve carries them as ordinary landmarks with that one
+   observation).  Window: P slots Rwb (P x 3 x 3) / pwb (P x 3), extrinsic Rbc / pbc; block: n landmarks lmp (n x 3),
+   host (n, int64, in 0..P-1), rmeas / ris (n), z (n x 2), isg.  cost_out (may be NULL): the robust cost, terms added
+   in landmark order (behind != 0: 1e6 per point behind its host).  lmp_out (n x 3) / Hinv_out (n x 3 x 3) / ok_out
+   (n) (NULL together): the step at damping lam (lam = 0: final_linearisation's marginals, window.py:1003-1006);
+   Hinv_out is written only where ok, as the reference does.  Bit-identical to the reference's float64 arithmetic.
+   Host memory; waits for `stream` (NULL = the legacy default stream) before returning. */
+int xcb_ba_posefree_host(int P, const double* Rwb, const double* pwb, const double* Rbc, const double* pbc, int n,
+                         const double* lmp, const int64_t* host, const double* rmeas, const double* ris,
+                         const double* z, double isg, double fx, double fy, double cx, double cy, double huber_k,
+                         int behind, double lam, double* cost_out, double* lmp_out, double* Hinv_out, uint8_t* ok_out,
+                         void* stream);
 
 /* ----------------------------------------------------------------------------------------------------------------
    Local-BA stage kernels: one entry point per kernel of src/xclean/backend/kernels.py, same argument order and

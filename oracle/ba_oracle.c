@@ -5,7 +5,8 @@
  *   _cam_poses (:108-122), obs_residual (:126-146), obs_jacobians_ws (:165-263), _huber (:282-286),
  *   build_system (:292-463), visual_cost (:467-493), back_substitute (:497-519), apply_update (:523-547),
  *   so3_exp_nb (:43-62) and the fixed-iteration LM of solve (:889-982) for a purely visual window (no marginal
- *   prior, no IMU terms, no pose-free block: those are out of this path).  Loops and expression order follow the
+ *   prior, no IMU terms: those are out of this path), and the pose-free block's posefree_cost / posefree_step
+ *   (:550-765).  Loops and expression order follow the
  *   reference's numba code; the reduced system is factored by a plain float64 Cholesky (the reference calls
  *   np.linalg.cholesky + two np.linalg.solve, so the step agrees to rounding, not bit for bit).
  * Extension used by the synthetic windows: `hold` = a slot held fixed (its rows / columns of the reduced system
@@ -504,4 +505,162 @@ void xo_ba_solve_batch(XoWindow* ws, int nw, int iters, double lam0, int nthread
 {
     #pragma omp parallel for num_threads(nthreads) schedule(dynamic, 1)
     for (int i = 0; i < nw; ++i) xo_ba_solve(&ws[i], iters, lam0, out + 4 * i, NULL);
+}
+
+/* ============================================ pose-free landmarks ============================================ */
+/* window._pf_block_fast (window.py:550-680): the host left observation and the inverse-depth prior of one pose-free
+   landmark, damped by lam, its 3x3 inverse into Hi and the gradient into bl.  -> lm_ok. */
+static int pf_block(const double* Rwc, const double* pwc, const double* RcR, int h, double a, double b, double rho,
+                    double z0, double z1, double isg, double ris, double rmeas, double fx, double fy, double cx,
+                    double cy, double huber_k, double lam, double* Hll, double* bl, double* Hi)
+{
+    const double* R = Rwc + 9 * (size_t)h;
+    const double* p = pwc + 3 * (size_t)h;
+    const double d0 = p[0] - p[0], d1 = p[1] - p[1], d2 = p[2] - p[2];
+    const double Y0 = R[0] * a + R[1] * b + R[2] + rho * d0;
+    const double Y1 = R[3] * a + R[4] * b + R[5] + rho * d1;
+    const double Y2 = R[6] * a + R[7] * b + R[8] + rho * d2;
+    const double q0 = R[0] * Y0 + R[3] * Y1 + R[6] * Y2;
+    const double q1 = R[1] * Y0 + R[4] * Y1 + R[7] * Y2;
+    const double q2 = R[2] * Y0 + R[5] * Y1 + R[8] * Y2;
+    for (int i = 0; i < 9; ++i) Hll[i] = 0.0;
+    for (int i = 0; i < 3; ++i) bl[i] = 0.0;
+    int nobs = 0;
+    if (q2 > 1e-9) {
+        double e0 = fx * q0 / q2 + cx - z0, e1 = fy * q1 / q2 + cy - z1, en2 = 0.0;
+        e0 *= isg;
+        en2 += e0 * e0;
+        e1 *= isg;
+        en2 += e1 * e1;
+        const double en = sqrt(en2);
+        const double w = en <= huber_k ? 1.0 : huber_k / en;
+        const double iq = 1.0 / q2;
+        const double D[6] = {fx * iq, 0.0, -fx * q0 * iq * iq, 0.0, fy * iq, -fy * q1 * iq * iq};
+        const double r0 = R[0] * d0 + R[3] * d1 + R[6] * d2;
+        const double r1 = R[1] * d0 + R[4] * d1 + R[7] * d2;
+        const double r2 = R[2] * d0 + R[5] * d1 + R[8] * d2;
+        double J[2][3];
+        for (int r = 0; r < 2; ++r) {
+            J[r][0] = D[3 * r] * RcR[0] + D[3 * r + 1] * RcR[3] + D[3 * r + 2] * RcR[6];
+            J[r][1] = D[3 * r] * RcR[1] + D[3 * r + 1] * RcR[4] + D[3 * r + 2] * RcR[7];
+            J[r][2] = D[3 * r] * r0 + D[3 * r + 1] * r1 + D[3 * r + 2] * r2;
+        }
+        for (int r = 0; r < 2; ++r)
+            for (int j = 0; j < 3; ++j) J[r][j] *= isg;
+        nobs += 1;
+        const double e[2] = {e0, e1};
+        for (int i = 0; i < 3; ++i) {
+            for (int j = 0; j < 3; ++j) {
+                double acc = 0.0;
+                acc += J[0][i] * J[0][j];
+                acc += J[1][i] * J[1][j];
+                Hll[3 * i + j] += w * acc;
+            }
+            double acc = 0.0;
+            acc += J[0][i] * e[0];
+            acc += J[1][i] * e[1];
+            bl[i] += w * acc;
+        }
+    }
+    if (ris > 0.0) {
+        const double rr = (rho - rmeas) * ris, ar = fabs(rr);
+        const double wp = ar <= huber_k ? 1.0 : huber_k / ar;
+        Hll[8] += wp * ris * ris;
+        bl[2] += wp * ris * rr;
+    }
+    for (int i = 0; i < 3; ++i) Hll[4 * i] += lam * Hll[4 * i] + 1e-12;
+    const double det = Hll[0] * (Hll[4] * Hll[8] - Hll[5] * Hll[7]) - Hll[1] * (Hll[3] * Hll[8] - Hll[5] * Hll[6])
+                       + Hll[2] * (Hll[3] * Hll[7] - Hll[4] * Hll[6]);
+    const double tr = Hll[0] + Hll[4] + Hll[8];
+    if (nobs == 0 || !(det > 1e-18 * tr * tr * tr) || !isfinite(det)) return 0;
+    const double idet = 1.0 / det;
+    Hi[0] = (Hll[4] * Hll[8] - Hll[5] * Hll[7]) * idet;
+    Hi[1] = (Hll[2] * Hll[7] - Hll[1] * Hll[8]) * idet;
+    Hi[2] = (Hll[1] * Hll[5] - Hll[2] * Hll[4]) * idet;
+    Hi[3] = (Hll[5] * Hll[6] - Hll[3] * Hll[8]) * idet;
+    Hi[4] = (Hll[0] * Hll[8] - Hll[2] * Hll[6]) * idet;
+    Hi[5] = (Hll[2] * Hll[3] - Hll[0] * Hll[5]) * idet;
+    Hi[6] = (Hll[3] * Hll[7] - Hll[4] * Hll[6]) * idet;
+    Hi[7] = (Hll[1] * Hll[6] - Hll[0] * Hll[7]) * idet;
+    Hi[8] = (Hll[0] * Hll[4] - Hll[1] * Hll[3]) * idet;
+    return 1;
+}
+
+/* window.posefree_cost (window.py:683-710): the host left observation (q2 <= 1e-9: nothing, or 1e6 when `behind`)
+   and the inverse-depth prior of every pose-free landmark, added in landmark order. */
+double xo_ba_posefree_cost(int P, const double* Rwb, const double* pwb, const double* Rbc, const double* pbc, int n,
+                           const double* lmp, const int64_t* host, const double* rmeas, const double* ris,
+                           const double* z, double isg, double fx, double fy, double cx, double cy, double B,
+                           double huber_k, int behind)
+{
+    double* Rwc = (double*)malloc(sizeof(double) * 9 * (size_t)(P > 0 ? P : 1));
+    double* pwc = (double*)malloc(sizeof(double) * 3 * (size_t)(P > 0 ? P : 1));
+    cam_poses(P, Rwb, pwb, Rbc, pbc, Rwc, pwc);
+    double cost = 0.0, e[2], q2, w, c;
+    for (int l = 0; l < n; ++l) {
+        const int h = (int)host[l];
+        obs_residual(Rwc, pwc, lmp + 3 * (size_t)l, h, h, 0, z + 2 * (size_t)l, fx, fy, cx, cy, B, e, &q2);
+        if (q2 <= 1e-9) {
+            if (behind) cost += 1e6;
+        } else {
+            double en2 = 0.0;
+            const double e0 = e[0] * isg;
+            en2 += e0 * e0;
+            const double e1 = e[1] * isg;
+            en2 += e1 * e1;
+            huber(sqrt(en2), huber_k, &w, &c);
+            cost += c;
+        }
+        if (ris[l] > 0.0) {
+            const double r0 = (lmp[3 * l + 2] - rmeas[l]) * ris[l];
+            huber(fabs(r0), huber_k, &w, &c);
+            cost += c;
+        }
+    }
+    free(Rwc);
+    free(pwc);
+    return cost;
+}
+
+/* window.posefree_step (window.py:713-765): every pose-free landmark's damped 3x3 step at lam -> lmp_out (the trial
+   state, the input where the step is refused), Hinv_out (written where ok) and ok_out. */
+void xo_ba_posefree_step(int P, const double* Rwb, const double* pwb, const double* Rbc, const double* pbc, int n,
+                         const double* lmp_in, const int64_t* host, const double* rmeas, const double* ris,
+                         const double* z, double isg, double fx, double fy, double cx, double cy, double huber_k,
+                         double lam, double* lmp_out, double* Hinv_out, uint8_t* ok_out)
+{
+    double* Rwc = (double*)malloc(sizeof(double) * 9 * (size_t)(P > 0 ? P : 1));
+    double* pwc = (double*)malloc(sizeof(double) * 3 * (size_t)(P > 0 ? P : 1));
+    double* RcR = (double*)malloc(sizeof(double) * 9 * (size_t)(P > 0 ? P : 1));
+    cam_poses(P, Rwb, pwb, Rbc, pbc, Rwc, pwc);
+    for (int s = 0; s < P; ++s) mtm3(Rwc + 9 * s, Rwc + 9 * s, RcR + 9 * s);
+    double Hll[9], bl[3], Hi[9];
+    for (int l = 0; l < n; ++l) {
+        const int h = (int)host[l];
+        const double* li = lmp_in + 3 * (size_t)l;
+        for (int i = 0; i < 3; ++i) lmp_out[3 * l + i] = li[i];
+        const int ok = pf_block(Rwc, pwc, RcR + 9 * h, h, li[0], li[1], li[2], z[2 * l], z[2 * l + 1], isg, ris[l],
+                                rmeas[l], fx, fy, cx, cy, huber_k, lam, Hll, bl, Hi);
+        ok_out[l] = (uint8_t)ok;
+        if (!ok) continue;
+        for (int i = 0; i < 9; ++i) Hinv_out[9 * (size_t)l + i] = Hi[i];
+        double v[3], d[3];
+        for (int i = 0; i < 3; ++i) v[i] = bl[i] + 0.0;
+        for (int i = 0; i < 3; ++i) {
+            double acc = 0.0;
+            acc += Hi[3 * i] * v[0];
+            acc += Hi[3 * i + 1] * v[1];
+            acc += Hi[3 * i + 2] * v[2];
+            d[i] = -acc;
+        }
+        const double r = li[2] + d[2];
+        if (r > 1e-9 && isfinite(r)) {
+            lmp_out[3 * l] = li[0] + d[0];
+            lmp_out[3 * l + 1] = li[1] + d[1];
+            lmp_out[3 * l + 2] = r;
+        }
+    }
+    free(RcR);
+    free(pwc);
+    free(Rwc);
 }

@@ -117,3 +117,39 @@ def solve_batch(windows, iters=5, lam0=1e-4, hold=0, nthreads=None):
     _lib().xo_ba_solve_batch(arr_p, len(structs), int(iters), c_double(lam0), int(nthreads or os.cpu_count() or 1),
                              out.ctypes.data)
     return out
+
+
+def _pf_common(Rwb, pwb, Rbc, pbc, lmp, host, rmeas, ris, z):
+    f = lambda a: np.ascontiguousarray(a, np.float64)
+    Rwb, pwb, Rbc, pbc = f(Rwb).reshape(-1, 3, 3), f(pwb).reshape(-1, 3), f(Rbc).reshape(3, 3), f(pbc).reshape(3)
+    lmp = f(lmp).reshape(-1, 3)
+    host = np.ascontiguousarray(host, np.int64).reshape(-1)
+    return Rwb, pwb, Rbc, pbc, lmp, host, f(rmeas).reshape(-1), f(ris).reshape(-1), f(z).reshape(-1, 2)
+
+
+def posefree_cost(Rwb, pwb, Rbc, pbc, lmp, host, rmeas, ris, z, isg, fx, fy, cx, cy, B, huber_k, behind):
+    """window.posefree_cost (window.py:683-710)."""
+    L = _fo.lib()
+    L.xo_ba_posefree_cost.restype = c_double
+    a = _pf_common(Rwb, pwb, Rbc, pbc, lmp, host, rmeas, ris, z)
+    return L.xo_ba_posefree_cost(len(a[0]), *[ctypes.c_void_p(x.ctypes.data) for x in a[:4]], len(a[4]),
+                                 *[ctypes.c_void_p(x.ctypes.data) for x in a[4:]], c_double(isg), c_double(fx),
+                                 c_double(fy), c_double(cx), c_double(cy), c_double(B), c_double(huber_k),
+                                 int(bool(behind)))
+
+
+def posefree_step(Rwb, pwb, Rbc, pbc, lmp_in, host, rmeas, ris, z, isg, fx, fy, cx, cy, huber_k, lam, lmp_out,
+                  Hinv_out, ok_out):
+    """window.posefree_step (window.py:713-765): lmp_out, Hinv_out (where ok), ok_out in place."""
+    L = _fo.lib()
+    L.xo_ba_posefree_step.restype = None
+    a = _pf_common(Rwb, pwb, Rbc, pbc, lmp_in, host, rmeas, ris, z)
+    n = len(a[4])
+    for o, dt, shape in ((lmp_out, np.float64, (n, 3)), (Hinv_out, np.float64, (n, 3, 3)), (ok_out, np.bool_, (n,))):
+        assert o.dtype == dt and o.flags.c_contiguous and o.shape == shape
+    L.xo_ba_posefree_step(len(a[0]), *[ctypes.c_void_p(x.ctypes.data) for x in a[:4]], n,
+                          *[ctypes.c_void_p(x.ctypes.data) for x in a[4:]], c_double(isg), c_double(fx), c_double(fy),
+                          c_double(cx), c_double(cy), c_double(huber_k), c_double(lam),
+                          ctypes.c_void_p(lmp_out.ctypes.data), ctypes.c_void_p(Hinv_out.ctypes.data),
+                          ctypes.c_void_p(ok_out.ctypes.data))
+    return 0

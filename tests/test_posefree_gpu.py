@@ -1,0 +1,81 @@
+"""The pose-free landmark block on the device: window.posefree_cost / posefree_step bit for bit against the
+reference's outputs, and the batched window solve with the block attached against the reference's solve
+(tests/golden/posefree_golden.npz).  Tolerances of the solve as for the windows without a block: the first cost to
+1e-9 relative, the accepted count identical, the states to 1e-6 (float64 mode; atomics change the summation order)."""
+import numpy as np
+import pytest
+
+from oracle import ba_oracle as BO
+from tests.test_posefree_oracle import GOLD, pf_args, window
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def G():
+    return dict(np.load(GOLD))
+
+
+@pytest.mark.parametrize("c", [0, 1])
+def test_posefree_cost_and_step_bit_exact(G, c):
+    from xclean_b200.backend import ba
+    w = window(G, c)
+    a = pf_args(G, c, w)
+    for behind in (False, True):
+        got = ba.posefree_cost(*a, w.fx, w.fy, w.cx, w.cy, w.B, w.huber_k, behind)
+        ref = G["c%d_cost_%d" % (c, int(behind))][0]
+        assert np.array_equal(np.float64(got).view(np.uint64), np.float64(ref).view(np.uint64)), behind
+    n = len(a[4])
+    for tag, lam in (("d", 1e-3), ("u", 0.0)):
+        lo, Hi, ok = np.full((n, 3), 7.0), np.full((n, 3, 3), 5.0), np.zeros(n, np.bool_)
+        assert ba.posefree_step(*a, w.fx, w.fy, w.cx, w.cy, w.huber_k, lam, lo, Hi, ok) == 0
+        assert np.array_equal(ok, G["c%d_%s_ok" % (c, tag)])
+        for x, k in ((lo, "lmp"), (Hi, "Hinv")):
+            assert np.array_equal(x.view(np.uint64), G["c%d_%s_%s" % (c, tag, k)].view(np.uint64)), (tag, k)
+
+
+def test_batched_solve_with_posefree_block(G, precision="fp64", tol=1e-6):
+    """Both fixture windows with their pose-free blocks and one window without, in one float64 batch with the gauge
+    free (as the reference solves them): every window as the reference's solve leaves it; then final_linearisation's
+    pose-free marginals at the solution equal the oracle's."""
+    from xclean_b200.backend import ba
+    ws = [window(G, 0, "pfs"), window(G, 1, "pfs"), window(G, 1)]
+    plain_ref = BO.solve(window(G, 1), iters=5, lam0=1e-4, hold=None)
+    res = ba.solve_batch(ws, iters=5, lam0=1e-4, precision=precision, hold=None)
+    for i, c in enumerate((0, 1)):
+        ref = G["c%d_stats" % c]
+        w = ws[i]
+        assert res["status"][i] == 0
+        assert abs(res["cost0"][i] - ref[0]) <= 1e-9 * abs(ref[0])
+        assert res["accepted"][i] == int(ref[2])
+        assert np.abs(w.Rwb - G["c%d_Rwb_n" % c]).max() < tol and np.abs(w.pwb - G["c%d_pwb_n" % c]).max() < tol
+        for got, k in ((w.lmp, "lmp_n"), (w.pf.lmp, "pflmp_n")):
+            r = G["c%d_%s" % (c, k)]
+            assert np.abs(got - r).max() < 10 * tol * max(1.0, np.abs(r).max()), k
+        ba.posefree_marginals(w)
+        pf = w.pf
+        n = len(pf.host)
+        lo, Hi, ok = np.zeros((n, 3)), np.zeros((n, 3, 3)), np.zeros(n, np.bool_)
+        BO.posefree_step(w.Rwb, w.pwb, w.Rbc, w.pbc, pf.lmp, pf.host, pf.rmeas, pf.ris, pf.z, pf.isg, w.fx, w.fy,
+                         w.cx, w.cy, w.huber_k, 0.0, lo, Hi, ok)
+        assert np.array_equal(pf.ok, ok) and np.array_equal(pf.Hinv[ok], Hi[ok])
+    assert res["accepted"][2] == plain_ref["accepted"]
+    assert abs(res["cost0"][2] - plain_ref["cost0"]) <= 1e-9 * abs(plain_ref["cost0"])
+
+
+def test_mixed_solve_with_posefree_block(G):
+    """Mixed precision (its step target assumes a fixed gauge: slot 0 held, as the other mixed-precision tests) with
+    the blocks attached, against the oracle's float64 solve of the merged windows: the first pose step to 1e-6
+    relative, the same accepted count, the states to 1e-6."""
+    from xclean_b200.backend import ba
+    ws = [window(G, 0, "pfs"), window(G, 1, "pfs")]
+    refs = [ba.merge_posefree(window(G, c, "pfs")) for c in (0, 1)]
+    outs = [BO.solve(r, iters=5, lam0=1e-4, hold=0) for r in refs]
+    res = ba.solve_batch(ws, iters=5, lam0=1e-4, precision="mixed", hold=0)
+    for i, (w, r, o) in enumerate(zip(ws, refs, outs)):
+        dx = res["dx0_list"][i]
+        assert np.linalg.norm(dx - o["dx0"]) <= 1e-6 * np.linalg.norm(o["dx0"]), i
+        assert res["accepted"][i] == o["accepted"], i
+        assert np.abs(w.pwb - r.pwb).max() < 1e-6 and np.abs(w.Rwb - r.Rwb).max() < 1e-6
+        L = w.lmp.shape[0]
+        assert np.abs(w.pf.lmp - r.lmp[L:]).max() < 1e-5 * max(1.0, np.abs(r.lmp[L:]).max())

@@ -136,6 +136,11 @@ _SIGS.update({
 })
 
 _SIGS.update({
+    "xcb_ba_posefree_host": (c_int, [c_int, P, P, P, P, c_int, P, P, P, P, P] + [c_double] * 6
+                             + [c_int, c_double, P, P, P, P, P]),
+})
+
+_SIGS.update({
     "xcb_lba_workspace_bytes": (c_size_t, [ctypes.POINTER(LbaProblem)]),
     "xcb_lba_solve": (c_int, [ctypes.POINTER(LbaProblem), c_int, c_double, P, P, c_size_t, P]),
 })

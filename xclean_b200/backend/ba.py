@@ -3,11 +3,14 @@ backend/local_ba.py, the drop-in _solve_gpu / _solve_gpu_id of src/xclean/backen
 the drop-in of its stage kernels).
 
     res = solve_batch(windows, iters=5, lam0=1e-4, precision="mixed", hold=0)
-    # windows: synth_ba.Window objects (the fields of vio/window.Problem); solved in place
+    # windows: synth_ba.Window objects (the fields of vio/window.Problem, `pf` = PoseFree or None); solved in place
     # res: dict(cost0, cost, accepted, lam, status (per window), dx0 (the first pose step per window))
 
     bs = BatchSolver(windows, device)       # pack once, keep resident on the device
     bs.solve(iters, lam0, precision)        # one persistent launch for every window; results stay on the device
+
+    posefree_cost(...), posefree_step(...)  # window.py's pose-free block functions, bit-identical
+    posefree_marginals(w)                   # final_linearisation's pose-free marginals into w.pf.Hinv / w.pf.ok
 
 Every call goes through libxcb200.so's C ABI (xcb_ba_solve_windows_dev); there is no CPU fallback.
 """
@@ -25,8 +28,69 @@ MAX_ROWS_PER_LANDMARK = 32
 MAX_TOUCHED_SLOTS = 16      # host + observing keyframes per landmark (the kernel's per-warp scratch)
 
 
+class PoseFree:
+    """window.PoseFree (src/xclean/vio/window.py:795-810): landmarks kept out of the Schur system, seen only in their
+    host's left image.  host (n,) slot indices, z (n,2) the host left pixels, isg their whitening, rmeas / ris (n,)
+    the inverse-depth prior, lmp (n,3) the state (updated by the solve), Hinv (n,3,3) / ok (n,) the marginals
+    (posefree_marginals)."""
+
+    def __init__(self, host, z, isg, rmeas, ris, lmp):
+        self.host = np.ascontiguousarray(host, np.int64)
+        self.z = np.ascontiguousarray(np.asarray(z, np.float64).reshape(-1, 2))
+        self.isg = float(isg)
+        self.rmeas = np.ascontiguousarray(rmeas, np.float64)
+        self.ris = np.ascontiguousarray(ris, np.float64)
+        self.lmp = np.ascontiguousarray(np.asarray(lmp, np.float64).reshape(-1, 3)).copy()
+        n = len(self.host)
+        self.Hinv = np.zeros((n, 3, 3))
+        self.ok = np.zeros(n, np.bool_)
+
+
+def _pf_of(w):
+    pf = getattr(w, "pf", None)
+    return pf if (pf is not None and len(pf.host) > 0) else None
+
+
+class _Merged:
+    """A window with its pose-free landmarks appended as ordinary landmarks, each with its one observation (host
+    slot, left camera, its pixel and whitening) and its inverse-depth prior.  window.solve treats the pose-free block
+    exactly as build_system treats such a landmark (_pf_block_fast is build_system's landmark block with t == h,
+    window.py:550-680): the observation has no pose coupling, the block is damped and guarded the same way, its
+    cost joins the window's and its step is accepted with the poses' (window.py:934-975)."""
+
+    def __init__(self, w, pf):
+        n = len(pf.host)
+        for k in ("Rwb", "pwb", "Rbc", "pbc", "fx", "fy", "cx", "cy", "B", "huber_k"):
+            setattr(self, k, getattr(w, k))
+        M = int(np.asarray(w.ob_start)[-1])
+        self.lmp = np.concatenate([np.asarray(w.lmp, np.float64).reshape(-1, 3), pf.lmp])
+        self.lm_host = np.concatenate([np.asarray(w.lm_host, np.int64), pf.host])
+        self.lm_mask = np.concatenate([np.asarray(w.lm_mask, np.bool_), np.ones(n, np.bool_)])
+        self.rho_meas = np.concatenate([np.asarray(w.rho_meas, np.float64), pf.rmeas])
+        self.rho_isig = np.concatenate([np.asarray(w.rho_isig, np.float64), pf.ris])
+        self.ob_start = np.concatenate([np.asarray(w.ob_start, np.int64), M + 1 + np.arange(n, dtype=np.int64)])
+        self.ob_pose = np.concatenate([np.asarray(w.ob_pose, np.int64), pf.host])
+        self.ob_cam = np.concatenate([np.asarray(w.ob_cam, np.int64), np.zeros(n, np.int64)])
+        self.ob_z = np.concatenate([np.asarray(w.ob_z, np.float64).reshape(-1, 2), pf.z])
+        self.ob_isig = np.concatenate([np.asarray(w.ob_isig, np.float64), np.full(n, pf.isg)])
+        self.ob_valid = np.concatenate([np.asarray(w.ob_valid, np.bool_), np.ones(n, np.bool_)])
+
+
+def merge_posefree(w):
+    """The window as the batched solve sees it: `w` itself, or, with a pose-free block, a view with the block's
+    landmarks appended after w's own (their states follow w.lmp's rows in the packed batch)."""
+    pf = _pf_of(w)
+    if pf is None:
+        return w
+    if (pf.host < 0).any() or (pf.host >= w.Rwb.shape[0]).any():
+        raise ValueError("solve_batch: a pose-free landmark's host slot is outside the window")
+    return _Merged(w, pf)
+
+
 def pack_windows(windows, hold=0):
-    """Concatenate windows into the batch layout of xcb_ba_windows (host numpy arrays)."""
+    """Concatenate windows into the batch layout of xcb_ba_windows (host numpy arrays); pose-free blocks are
+    appended to their windows' landmarks (merge_posefree)."""
+    windows = [merge_posefree(w) for w in windows]
     nw = len(windows)
     P = np.array([w.Rwb.shape[0] for w in windows], np.int32)
     L = np.array([w.lmp.shape[0] for w in windows], np.int32)
@@ -202,6 +266,9 @@ class BatchSolver:
             w.Rwb[:] = Rwb[so[i]:so[i] + P].reshape(P, 3, 3)
             w.pwb[:] = pwb[so[i]:so[i] + P]
             w.lmp[:] = lmp[lo[i]:lo[i] + L]
+            pf = _pf_of(w)
+            if pf is not None:
+                pf.lmp[:] = lmp[lo[i] + L:lo[i] + L + len(pf.host)]
 
 
 def solve_batch(windows, iters=5, lam0=1e-4, precision="mixed", hold=0, device="cuda"):
@@ -214,3 +281,58 @@ def solve_batch(windows, iters=5, lam0=1e-4, precision="mixed", hold=0, device="
     for i, w in enumerate(windows):
         res.setdefault("dx0_list", []).append(res["dx0"][i][:6 * w.Rwb.shape[0]])
     return res
+
+
+def _pf_arrays(Rwb, pwb, Rbc, pbc, lmp, host, rmeas, ris, z):
+    f = lambda a, shape: np.ascontiguousarray(a, np.float64).reshape(shape)
+    Rwb = f(Rwb, (-1, 3, 3))
+    lmp = f(lmp, (-1, 3))
+    n = len(lmp)
+    return [Rwb, f(pwb, (len(Rwb), 3)), f(Rbc, (3, 3)), f(pbc, (3,)), lmp,
+            np.ascontiguousarray(host, np.int64).reshape(n), f(rmeas, (n,)), f(ris, (n,)), f(z, (n, 2))]
+
+
+def _pf_call(a, isg, fx, fy, cx, cy, huber_k, behind, lam, cost, lmp_out, Hinv_out, ok_out):
+    L = _lib.lib()
+    p = _lib.ptr
+    rc = L.xcb_ba_posefree_host(len(a[0]), p(a[0]), p(a[1]), p(a[2]), p(a[3]), len(a[4]), *[p(x) for x in a[4:]],
+                                float(isg), float(fx), float(fy), float(cx), float(cy), float(huber_k), int(bool(behind)),
+                                float(lam), p(cost), p(lmp_out), p(Hinv_out),
+                                None if ok_out is None else p(ok_out.view(np.uint8)), None)
+    if rc != _lib.XCB_OK:
+        msg = (L.xcb_last_error() or b"").decode(errors="replace")
+        raise (ValueError if rc == _lib.XCB_ERR_ARG else RuntimeError)("posefree: %s" % msg)
+
+
+def posefree_cost(Rwb, pwb, Rbc, pbc, lmp, host, rmeas, ris, z, isg, fx, fy, cx, cy, B, huber_k, behind):
+    """window.posefree_cost on the device (src/xclean/vio/window.py:683-710): the robust cost of the pose-free
+    landmarks (host observation + inverse-depth prior; behind=True adds 1e6 per point behind its host), the
+    reference's float64 value bit for bit.  B is unused, as in the reference (left observations only)."""
+    a = _pf_arrays(Rwb, pwb, Rbc, pbc, lmp, host, rmeas, ris, z)
+    cost = np.zeros(1)
+    _pf_call(a, isg, fx, fy, cx, cy, huber_k, behind, 0.0, cost, None, None, None)
+    return float(cost[0])
+
+
+def posefree_step(Rwb, pwb, Rbc, pbc, lmp_in, host, rmeas, ris, z, isg, fx, fy, cx, cy, huber_k, lam, lmp_out,
+                  Hinv_out, ok_out):
+    """window.posefree_step on the device (window.py:713-765): lmp_out = the trial state, Hinv_out (written where
+    ok) / ok_out = the damped 3x3 inverses and lm_ok (lam = 0: final_linearisation's marginals); in place, the
+    reference's bits.  Returns 0."""
+    a = _pf_arrays(Rwb, pwb, Rbc, pbc, lmp_in, host, rmeas, ris, z)
+    n = len(a[4])
+    for o, dt, shape in ((lmp_out, np.float64, (n, 3)), (Hinv_out, np.float64, (n, 3, 3)), (ok_out, np.bool_, (n,))):
+        if not (isinstance(o, np.ndarray) and o.dtype == dt and o.flags.c_contiguous and o.shape == shape):
+            raise ValueError("posefree_step: outputs must be C-contiguous arrays of the reference's shapes")
+    _pf_call(a, isg, fx, fy, cx, cy, huber_k, False, lam, None, lmp_out, Hinv_out, ok_out)
+    return 0
+
+
+def posefree_marginals(w):
+    """final_linearisation's pose-free part (window.py:1003-1006): the block's 3x3 marginals at lam = 0 at the
+    window's current state, into w.pf.Hinv / w.pf.ok (nothing when the window has no block)."""
+    pf = _pf_of(w)
+    if pf is None:
+        return
+    posefree_step(w.Rwb, w.pwb, w.Rbc, w.pbc, pf.lmp, pf.host, pf.rmeas, pf.ris, pf.z, pf.isg, w.fx, w.fy, w.cx, w.cy,
+                  w.huber_k, 0.0, np.zeros_like(pf.lmp), pf.Hinv, pf.ok)

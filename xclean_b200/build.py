@@ -24,6 +24,7 @@ SOURCES = {
     "front_stereo.cu": STRICT,
     "front_api.cu": STRICT,
     "front_mapmatch.cu": STRICT,
+    "ba_posefree.cu": STRICT,
     "ba_window.cu": [],
     "ba_api.cu": [],
 }
