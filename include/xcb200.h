@@ -220,6 +220,7 @@ typedef struct {
 
 #define XCB_BA_FP64 0           /* everything in float64: the plain form */
 #define XCB_BA_MIXED 1          /* FP32 linearisation + Schur, FP64 Cholesky, FP64 refinement (to 1e-9, <= 3 steps) */
+#define XCB_BA_LINEARISE 2      /* internal: one float64 linearisation, the reduced system exported (no step) */
 
 /* Device scratch the batched solve needs for `Lt` landmarks: the work counter, the trial landmark states and, for the
    float64 mode, each landmark's back-substitution record (118 doubles: ~0.95 kB per landmark).  A smaller scratch
@@ -277,6 +278,13 @@ int xcb_ba_newton_windows_dev(const xcb_ba_windows* w, int max_slots, int mode, 
    xcb_ba_newton_scratch_bytes(nw, Lt) bytes (Lt: the batch's landmarks).  stats [nw][8] as xcb_ba_solve_windows_dev. */
 int xcb_ba_solve_windows_free_dev(const xcb_ba_windows* w, int Lt, int max_slots, int iters, double lam0,
                                   double* stats, void* scratch, size_t scratch_bytes, int grid, void* stream);
+/* final_linearisation's visual system (src/xclean/vio/window.py:985-1008, build_system at lam = 0): for every window
+   of the batch, at its current state, the Schur-reduced H (6P x 6P, row-major) and b (6P), float64, written to
+   out + w * out_stride (out_stride >= 36 max_slots^2 + 6 max_slots doubles); stats [nw][8]: [0], [1] = the robust
+   cost.  No hold, no damping, the state unchanged.  The prior and IMU terms of the reference's _full_system are not
+   part of it (this path has neither).  scratch as xcb_ba_solve_windows_dev. */
+int xcb_ba_linearise_windows_dev(const xcb_ba_windows* w, int max_slots, double* out, int out_stride, double* stats,
+                                 void* scratch, size_t scratch_bytes, int grid, void* stream);
 /* window.posefree_cost and window.posefree_step (src/xclean/vio/window.py:683-765): the pose-free landmarks of one
    window (seen only in their host's left image; the batched solve carries them as ordinary landmarks with that one
    observation).  Window: P slots Rwb (P x 3 x 3) / pwb (P x 3), extrinsic Rbc / pbc; block: n landmarks lmp (n x 3),

@@ -79,3 +79,31 @@ def test_mixed_solve_with_posefree_block(G):
         assert np.abs(w.pwb - r.pwb).max() < 1e-6 and np.abs(w.Rwb - r.Rwb).max() < 1e-6
         L = w.lmp.shape[0]
         assert np.abs(w.pf.lmp - r.lmp[L:]).max() < 1e-5 * max(1.0, np.abs(r.lmp[L:]).max())
+
+
+def test_final_linearisation_systems(G):
+    """final_linearisation's reduced visual system (lam = 0) from the batched kernel against the oracle's
+    build_system (which the reference pins bit for bit): H and b to 1e-9 of their scale, the cost to 1e-12; a window's
+    pose-free block leaves its system unchanged (no pose coupling) and gets its marginals."""
+    from tests.test_window_oracle import GOLD as WGOLD, _window as wwindow
+    from xclean_b200.backend import ba
+    WG = dict(np.load(WGOLD))
+    ws = [wwindow(WG, c) for c in (0, 1, 2)] + [window(G, 1, "pfs"), window(G, 1)]
+    systems, cost = ba.final_linearisation(ws)
+    for i, w in enumerate(ws):
+        ref = w if getattr(w, "pf", None) is None else window(G, 1)
+        H, b, c, _Hi, _bl, _Hlp, _ok = BO.build_system(ref, 0.0)
+        Hd, bd = systems[i]
+        assert Hd.shape == H.shape and bd.shape == b.shape
+        assert np.abs(Hd - H).max() <= 1e-9 * np.abs(H).max(), i
+        assert np.abs(bd - b).max() <= 1e-9 * np.abs(b).max(), i
+        if getattr(w, "pf", None) is None:
+            assert abs(cost[i] - c) <= 1e-12 * abs(c), i
+    pf = ws[3].pf
+    n = len(pf.host)
+    lo, Hi, ok = np.zeros((n, 3)), np.zeros((n, 3, 3)), np.zeros(n, np.bool_)
+    w = ws[3]
+    BO.posefree_step(w.Rwb, w.pwb, w.Rbc, w.pbc, pf.lmp, pf.host, pf.rmeas, pf.ris, pf.z, pf.isg, w.fx, w.fy, w.cx,
+                     w.cy, w.huber_k, 0.0, lo, Hi, ok)
+    assert np.array_equal(pf.ok, ok) and np.array_equal(pf.Hinv[ok], Hi[ok])
+    assert cost[3] > cost[4]                             # the block's cost joins the window's

@@ -136,6 +136,7 @@ _SIGS.update({
 })
 
 _SIGS.update({
+    "xcb_ba_linearise_windows_dev": (c_int, [ctypes.POINTER(BaWindows), c_int, P, c_int, P, P, c_size_t, c_int, P]),
     "xcb_ba_posefree_host": (c_int, [c_int, P, P, P, P, c_int, P, P, P, P, P] + [c_double] * 6
                              + [c_int, c_double, P, P, P, P, P]),
 })

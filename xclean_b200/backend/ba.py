@@ -9,8 +9,10 @@ the drop-in of its stage kernels).
     bs = BatchSolver(windows, device)       # pack once, keep resident on the device
     bs.solve(iters, lam0, precision)        # one persistent launch for every window; results stay on the device
 
+    bs.linearise()                          # final_linearisation's reduced visual system per window
     posefree_cost(...), posefree_step(...)  # window.py's pose-free block functions, bit-identical
     posefree_marginals(w)                   # final_linearisation's pose-free marginals into w.pf.Hinv / w.pf.ok
+    systems, costs = final_linearisation(windows)
 
 Every call goes through libxcb200.so's C ABI (xcb_ba_solve_windows_dev); there is no CPU fallback.
 """
@@ -215,6 +217,29 @@ class BatchSolver:
                                                  int(grid), ctypes.c_void_p(s.cuda_stream or None))
         _lib.check(rc, None, "xcb_ba_solve_windows_dev")
 
+    def linearise(self, stream=None, grid=0):
+        """final_linearisation's visual system (window.py:985-1008, build_system at lam = 0) of every window at the
+        state on the device: -> (list of (H (6P,6P), b (6P)) float64 host arrays, robust cost per window).  No hold,
+        no damping; the state is unchanged."""
+        torch = self.torch
+        s = stream if stream is not None else torch.cuda.current_stream(self.dev)
+        nm = 6 * self.max_slots
+        stride = nm * nm + nm
+        out = torch.empty(max(self.nw, 1) * stride, dtype=torch.float64, device=self.dev)
+        rc = _lib.lib().xcb_ba_linearise_windows_dev(ctypes.byref(self.desc), self.max_slots, out.data_ptr(), stride,
+                                                     self.stats.data_ptr(), self.scratch.data_ptr(),
+                                                     self.scratch.numel(), int(grid),
+                                                     ctypes.c_void_p(s.cuda_stream or None))
+        _lib.check(rc, None, "xcb_ba_linearise_windows_dev")
+        s.synchronize()
+        o = out.cpu().numpy()
+        systems = []
+        for i in range(self.nw):
+            n = 6 * int(self.host["P"][i])
+            blk = o[i * stride:i * stride + n * n + n]
+            systems.append((blk[:n * n].reshape(n, n).copy(), blk[n * n:].copy()))
+        return systems, self.stats.cpu().numpy()[:self.nw, 0].copy()
+
     def newton(self, steps=3, maxit=60, tol=1e-12, stream=None, grid=0, flag=True):
         """Exact-Hessian Newton steps on every window (in place): the converged state the adjoint differentiates.
         flag: landmarks whose decoupled Gauss-Newton step would take the inverse depth to <= 1e-9 at an evaluated
@@ -336,3 +361,15 @@ def posefree_marginals(w):
         return
     posefree_step(w.Rwb, w.pwb, w.Rbc, w.pbc, pf.lmp, pf.host, pf.rmeas, pf.ris, pf.z, pf.isg, w.fx, w.fy, w.cx, w.cy,
                   w.huber_k, 0.0, np.zeros_like(pf.lmp), pf.Hinv, pf.ok)
+
+
+def final_linearisation(windows, device="cuda"):
+    """window.final_linearisation for a batch of purely visual windows (no prior, no IMU): per window (H, b) of the
+    Schur-reduced visual system at lam = 0 (the reference's H, bvec for such a window), its robust cost, and the
+    pose-free block's marginals into w.pf.Hinv / w.pf.ok.  -> (list of (H, b), costs).  The per-observation chi2
+    and the kept landmarks' Hll_inv are not exported."""
+    bs = BatchSolver(windows, device, hold=None)
+    systems, cost = bs.linearise()
+    for w in windows:
+        posefree_marginals(w)
+    return systems, cost

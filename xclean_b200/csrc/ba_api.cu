@@ -15,6 +15,7 @@ extern "C" size_t xcb_ba_scratch_bytes(int nw, int Lt)
 }
 
 static int ba_fail(int code, const char* msg);
+static int ba_grid(int grid, int nw);
 
 extern "C" int xcb_ba_solve_windows_dev(const xcb_ba_windows* w, int max_slots, int iters, double lam0, int mode,
                                         double* stats, double* dx0, int dx0_stride, void* scratch,
@@ -41,6 +42,27 @@ extern "C" int xcb_ba_solve_windows_dev(const xcb_ba_windows* w, int max_slots, 
     if (grid > w->nw) grid = w->nw;
     e = xcb_launch_ba_windows(*w, max_slots, iters, lam0, mode, stats, dx0, dx0_stride, trial, counter, grid, st,
                               nullptr, scratch_bytes > 256 ? (scratch_bytes - 256) / sizeof(double) : 0);
+    if (e != cudaSuccess) return ba_fail(XCB_ERR_CUDA, cudaGetErrorString(e));
+    return XCB_OK;
+}
+
+extern "C" int xcb_ba_linearise_windows_dev(const xcb_ba_windows* w, int max_slots, double* out, int out_stride,
+                                            double* stats, void* scratch, size_t scratch_bytes, int grid, void* stream)
+{
+    if (!w || !out || !stats || !scratch) return ba_fail(XCB_ERR_ARG, "ba_linearise_windows: null argument");
+    if (w->nw <= 0) return XCB_OK;
+    if (max_slots < 1 || max_slots > xcb_ba_max_slots())
+        return ba_fail(XCB_ERR_CAPACITY, "ba_linearise_windows: max_slots out of range (1..20)");
+    const long long nm = 6LL * max_slots;
+    if (out_stride < nm * nm + nm) return ba_fail(XCB_ERR_ARG, "ba_linearise_windows: out stride too small");
+    cudaStream_t st = (cudaStream_t)stream;
+    int* counter = (int*)scratch;
+    double* trial = (double*)((char*)scratch + 256);
+    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), st);
+    if (e != cudaSuccess) return ba_fail(XCB_ERR_CUDA, cudaGetErrorString(e));
+    e = xcb_launch_ba_windows(*w, max_slots, 1, 0.0, XCB_BA_LINEARISE, stats, out, out_stride, trial, counter,
+                              ba_grid(grid, w->nw), st, nullptr,
+                              scratch_bytes > 256 ? (scratch_bytes - 256) / sizeof(double) : 0);
     if (e != cudaSuccess) return ba_fail(XCB_ERR_CUDA, cudaGetErrorString(e));
     return XCB_OK;
 }

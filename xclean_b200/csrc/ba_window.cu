@@ -834,6 +834,20 @@ __global__ void __launch_bounds__(BA_THREADS, 1) k_ba_windows(XcbBaWindows d, in
                 for (int q = tid; q < n; q += blockDim.x) sh.rhs[q] = sh.g[q];
             }
             __syncthreads();
+            if (mode == XCB_BA_LINEARISE) {
+                // final_linearisation's visual part (window.py:985-1008): the reduced system at the current state, no
+                // hold, no step; dx0 receives H (n x n, row-major) and then b for each window
+                double* o = dx0 + (size_t)w * dx0_stride;
+                for (int q = tid; q < n * n; q += blockDim.x) {
+                    const int i = q / n, j = q % n;
+                    o[q] = S64[i >= j ? tri(i, j) : tri(j, i)];
+                }
+                for (int q = tid; q < n; q += blockDim.x) o[(size_t)n * n + q] = sh.g[q];
+                cost0 = c_tot;
+                cur = c_tot;
+                __syncthreads();
+                break;
+            }
             // hold, damping (D = lam diag + 1e-9, kept for the refinement residual), RHS = -b
             const int hs = sh.w.hold;
             if (hs >= 0 && hs < P) {
