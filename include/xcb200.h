@@ -278,11 +278,14 @@ int xcb_ba_newton_windows_dev(const xcb_ba_windows* w, int max_slots, int mode, 
    xcb_ba_newton_scratch_bytes(nw, Lt) bytes (Lt: the batch's landmarks).  stats [nw][8] as xcb_ba_solve_windows_dev. */
 int xcb_ba_solve_windows_free_dev(const xcb_ba_windows* w, int Lt, int max_slots, int iters, double lam0,
                                   double* stats, void* scratch, size_t scratch_bytes, int grid, void* stream);
-/* final_linearisation's visual system (src/xclean/vio/window.py:985-1008, build_system at lam = 0): for every window
-   of the batch, at its current state, the Schur-reduced H (6P x 6P, row-major) and b (6P), float64, written to
-   out + w * out_stride (out_stride >= 36 max_slots^2 + 6 max_slots doubles); stats [nw][8]: [0], [1] = the robust
-   cost.  No hold, no damping, the state unchanged.  The prior and IMU terms of the reference's _full_system are not
-   part of it (this path has neither).  scratch as xcb_ba_solve_windows_dev. */
+/* final_linearisation's visual outputs (src/xclean/vio/window.py:985-1008, build_system at lam = 0): for every
+   window of the batch, at its current state, written from out + w * out_stride (float64; out zero-filled by the
+   caller): the Schur-reduced H (6P x 6P, row-major), b (6P), then, when the row holds them (out_stride >=
+   36 P^2 + 6 P + 10 L + M for that window), per landmark [lm_ok, Hll_inv (3 x 3)] (10 L; masked-out landmarks stay
+   0, Hll_inv only where lm_ok) and per observation its whitened squared residual ob_chi2 (M; inf where invalid or
+   behind the camera, 0 for masked-out landmarks).  out_stride >= 36 max_slots^2 + 6 max_slots.  stats [nw][8]:
+   [0], [1] = the robust cost.  No hold, no damping, the state unchanged.  The prior and IMU terms of the reference's
+   _full_system are not part of it (this path has neither).  scratch as xcb_ba_solve_windows_dev. */
 int xcb_ba_linearise_windows_dev(const xcb_ba_windows* w, int max_slots, double* out, int out_stride, double* stats,
                                  void* scratch, size_t scratch_bytes, int grid, void* stream);
 /* window.posefree_cost and window.posefree_step (src/xclean/vio/window.py:683-765): the pose-free landmarks of one

@@ -62,8 +62,8 @@ def as_struct(w, hold=0):
     return s
 
 
-def build_system(w, lam):
-    """-> (H (6P,6P), b (6P,), cost, Hll_inv (L,3,3), bl (L,3), Hlp (L,P,3,6), lm_ok (L,))"""
+def build_system(w, lam, want_chi2=False):
+    """-> (H (6P,6P), b (6P,), cost, Hll_inv (L,3,3), bl (L,3), Hlp (L,P,3,6), lm_ok (L,)[, ob_chi2 (M,)])"""
     s = as_struct(w, None)
     Pn, L, M = s.P, s.L, s.M
     H = np.zeros((6 * Pn, 6 * Pn))
@@ -75,6 +75,8 @@ def build_system(w, lam):
     chi = np.zeros(max(M, 1))
     c = _lib().xo_ba_build_system(ctypes.byref(s), s.Rwb, s.pwb, s.lmp, c_double(lam), H.ctypes.data, b.ctypes.data,
                                   Hi.ctypes.data, bl.ctypes.data, Hlp.ctypes.data, ok.ctypes.data, chi.ctypes.data)
+    if want_chi2:
+        return H, b, c, Hi[:L], bl[:L], Hlp[:L], ok[:L].astype(bool), chi[:M]
     return H, b, c, Hi[:L], bl[:L], Hlp[:L], ok[:L].astype(bool)
 
 

@@ -82,9 +82,10 @@ def test_mixed_solve_with_posefree_block(G):
 
 
 def test_final_linearisation_systems(G):
-    """final_linearisation's reduced visual system (lam = 0) from the batched kernel against the oracle's
-    build_system (which the reference pins bit for bit): H and b to 1e-9 of their scale, the cost to 1e-12; a window's
-    pose-free block leaves its system unchanged (no pose coupling) and gets its marginals."""
+    """final_linearisation's visual outputs (lam = 0) from the batched kernel against the oracle's build_system (which
+    the reference pins bit for bit): H, b and the kept landmarks' Hll_inv to 1e-9 of their scale, lm_ok exactly, the
+    observations' chi2 to 1e-9 (inf at the same rows), the cost to 1e-12; a window's pose-free block leaves its system
+    unchanged (no pose coupling) and gets its marginals."""
     from tests.test_window_oracle import GOLD as WGOLD, _window as wwindow
     from xclean_b200.backend import ba
     WG = dict(np.load(WGOLD))
@@ -92,11 +93,18 @@ def test_final_linearisation_systems(G):
     systems, cost = ba.final_linearisation(ws)
     for i, w in enumerate(ws):
         ref = w if getattr(w, "pf", None) is None else window(G, 1)
-        H, b, c, _Hi, _bl, _Hlp, _ok = BO.build_system(ref, 0.0)
-        Hd, bd = systems[i]
+        H, b, c, Hi, _bl, _Hlp, ok, chi = BO.build_system(ref, 0.0, want_chi2=True)
+        sy = systems[i]
+        Hd, bd = sy["H"], sy["b"]
         assert Hd.shape == H.shape and bd.shape == b.shape
         assert np.abs(Hd - H).max() <= 1e-9 * np.abs(H).max(), i
         assert np.abs(bd - b).max() <= 1e-9 * np.abs(b).max(), i
+        assert np.array_equal(sy["lm_ok"], ok), i
+        assert np.abs(sy["Hll_inv"][ok] - Hi[ok]).max() <= 1e-9 * np.abs(Hi[ok]).max(), i
+        assert (sy["Hll_inv"][~ok] == 0).all()
+        fin = np.isfinite(chi)
+        assert np.array_equal(np.isfinite(sy["ob_chi2"]), fin), i
+        assert np.allclose(sy["ob_chi2"][fin], chi[fin], rtol=1e-9, atol=1e-12), i
         if getattr(w, "pf", None) is None:
             assert abs(cost[i] - c) <= 1e-12 * abs(c), i
     pf = ws[3].pf

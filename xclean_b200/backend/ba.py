@@ -218,14 +218,19 @@ class BatchSolver:
         _lib.check(rc, None, "xcb_ba_solve_windows_dev")
 
     def linearise(self, stream=None, grid=0):
-        """final_linearisation's visual system (window.py:985-1008, build_system at lam = 0) of every window at the
-        state on the device: -> (list of (H (6P,6P), b (6P)) float64 host arrays, robust cost per window).  No hold,
-        no damping; the state is unchanged."""
+        """final_linearisation's visual outputs (window.py:985-1008, build_system at lam = 0) of every window at the
+        state on the device: -> (list of dict(H (6P,6P), b (6P), lm_ok (L), Hll_inv (L,3,3), ob_chi2 (M)) float64
+        host arrays over the packed window (pose-free landmarks and their observations after the window's own),
+        robust cost per window).  No hold, no damping; the state is unchanged."""
         torch = self.torch
         s = stream if stream is not None else torch.cuda.current_stream(self.dev)
         nm = 6 * self.max_slots
-        stride = nm * nm + nm
-        out = torch.empty(max(self.nw, 1) * stride, dtype=torch.float64, device=self.dev)
+        Lw = self.host["L"].astype(np.int64)
+        lm_ob = self.host["lm_ob"].astype(np.int64)
+        lo = self.host["lm_off"].astype(np.int64)
+        Mw = lm_ob[lo + Lw] - lm_ob[lo]
+        stride = int(nm * nm + nm + 10 * Lw.max(initial=0) + Mw.max(initial=0))
+        out = torch.zeros(max(self.nw, 1) * stride, dtype=torch.float64, device=self.dev)
         rc = _lib.lib().xcb_ba_linearise_windows_dev(ctypes.byref(self.desc), self.max_slots, out.data_ptr(), stride,
                                                      self.stats.data_ptr(), self.scratch.data_ptr(),
                                                      self.scratch.numel(), int(grid),
@@ -235,9 +240,12 @@ class BatchSolver:
         o = out.cpu().numpy()
         systems = []
         for i in range(self.nw):
-            n = 6 * int(self.host["P"][i])
-            blk = o[i * stride:i * stride + n * n + n]
-            systems.append((blk[:n * n].reshape(n, n).copy(), blk[n * n:].copy()))
+            n, L, M = 6 * int(self.host["P"][i]), int(Lw[i]), int(Mw[i])
+            blk = o[i * stride:i * stride + n * n + n + 10 * L + M]
+            rec = blk[n * n + n:n * n + n + 10 * L].reshape(L, 10)
+            systems.append(dict(H=blk[:n * n].reshape(n, n).copy(), b=blk[n * n:n * n + n].copy(),
+                                lm_ok=rec[:, 0] != 0, Hll_inv=rec[:, 1:].reshape(L, 3, 3).copy(),
+                                ob_chi2=blk[n * n + n + 10 * L:].copy()))
         return systems, self.stats.cpu().numpy()[:self.nw, 0].copy()
 
     def newton(self, steps=3, maxit=60, tol=1e-12, stream=None, grid=0, flag=True):
@@ -364,12 +372,14 @@ def posefree_marginals(w):
 
 
 def final_linearisation(windows, device="cuda"):
-    """window.final_linearisation for a batch of purely visual windows (no prior, no IMU): per window (H, b) of the
-    Schur-reduced visual system at lam = 0 (the reference's H, bvec for such a window), its robust cost, and the
-    pose-free block's marginals into w.pf.Hinv / w.pf.ok.  -> (list of (H, b), costs).  The per-observation chi2
-    and the kept landmarks' Hll_inv are not exported."""
+    """window.final_linearisation for a batch of purely visual windows (no prior, no IMU): per window a dict of the
+    reference's outputs for such a window - H, b (the Schur-reduced visual system at lam = 0), ob_chi2 (M), lm_ok (L),
+    Hll_inv (L,3,3) of the window's own landmarks and observations - and the pose-free block's marginals into
+    w.pf.Hinv / w.pf.ok.  -> (list of dicts, robust costs (the block's cost included))."""
     bs = BatchSolver(windows, device, hold=None)
     systems, cost = bs.linearise()
-    for w in windows:
+    for w, sy in zip(windows, systems):
+        L, M = w.lmp.shape[0], int(np.asarray(w.ob_start)[-1])
+        sy["lm_ok"], sy["Hll_inv"], sy["ob_chi2"] = sy["lm_ok"][:L], sy["Hll_inv"][:L], sy["ob_chi2"][:M]
         posefree_marginals(w)
     return systems, cost

@@ -264,10 +264,12 @@ __device__ __forceinline__ int lm_rows(const XcbBaWindows& d, int gl)
 
 // Linearise one landmark into the warp scratch: observations, Hll (damped) and bl, touched slots and their Hlp
 // blocks.  -> whether the landmark enters the system (window.build_system's lm_ok); lane-local cost added to *cost.
+// exp_ob (optional): the window's per-observation whitened squared residuals (final_linearisation's ob_chi2), indexed
+// from the window's first observation: inf where the observation is invalid or its point is behind the camera.
 template <typename T>
 __device__ __forceinline__ bool lin_landmark(BaShared& sh, const XcbBaWindows& d, const SlotGeo<T>& G, int l,
                                              double lam, const double* lmp_src, WarpLm<T>& wl, T Hll[9], T bl[3],
-                                             int* nt_out, double* cost)
+                                             int* nt_out, double* cost, double* exp_ob = nullptr)
 {
     const int lane = threadIdx.x & 31;
     const BaWin& w = sh.w;
@@ -281,16 +283,20 @@ __device__ __forceinline__ bool lin_landmark(BaShared& sh, const XcbBaWindows& d
         const int k = k0 + lane;
         T* ob = wl.ob[lane];
         const int t = d.ob_pose[k];
+        double chi2 = XCB_INF;
         if (d.ob_valid[k] && h_ok && (unsigned)t < (unsigned)w.P) {
             if (obs_lin<T>(w, G, lm, h, t, d.ob_cam[k], d.ob_z + 2 * k, (T)d.ob_isig[k], ob, true)) {
-                T en = sqrt(ob[OB_E] * ob[OB_E] + ob[OB_E + 1] * ob[OB_E + 1]), wt, cc;
+                const T e2 = ob[OB_E] * ob[OB_E] + ob[OB_E + 1] * ob[OB_E + 1];
+                T en = sqrt(e2), wt, cc;
                 huber_w<T>(en, (T)w.hk, &wt, &cc);
                 ob[OB_W] = wt;
                 *cost += (double)cc;
                 mt = t;
+                chi2 = (double)e2;
             }
         }
         wl.obt[lane] = mt;
+        if (exp_ob) exp_ob[k - d.lm_ob[w.lm0]] = chi2;
     }
     // touched slots: observing keyframes other than the host, plus the host when any exists
     const bool pose = mt >= 0 && mt != h;
@@ -387,9 +393,12 @@ __device__ __forceinline__ void inv3(const T H[9], T Hi[9])
 
 // ---------------------------------------------------------------------------------------- pass A: build + Schur
 // S: packed lower triangle (FP32, mixed) or full n x n (FP64 plain form, lower triangle used); gb: gradient
+// exp_lm / exp_ob (optional, final_linearisation's exports): per landmark of the window [lm_ok, Hll^-1 (9)] (written
+// for the landmarks the mask admits; Hll^-1 only where lm_ok), per observation its chi2 (lin_landmark).
 template <typename T, bool PACKED>
 __device__ void pass_build(BaShared& sh, const XcbBaWindows& d, const SlotGeo<T>& G, T* S, T* gb, WarpLm<T>* wls,
-                           double* cost_out, const double* frz = nullptr, double* bsc = nullptr)
+                           double* cost_out, const double* frz = nullptr, double* bsc = nullptr,
+                           double* exp_lm = nullptr, double* exp_ob = nullptr)
 {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int n = sh.w.n;
@@ -401,11 +410,14 @@ __device__ void pass_build(BaShared& sh, const XcbBaWindows& d, const SlotGeo<T>
         const int h = d.lm_host[gl];
         T Hll[9], bl[3];
         int nt;
-        const bool ok = lin_landmark<T>(sh, d, G, l, sh.lam, d.lmp, wl, Hll, bl, &nt, &c_local) && !lm_const(frz, gl);
+        const bool ok = lin_landmark<T>(sh, d, G, l, sh.lam, d.lmp, wl, Hll, bl, &nt, &c_local, exp_ob)
+                        && !lm_const(frz, gl);
         // pose-pose blocks (always) and, for an entering landmark, minus the Schur term
         T Hi[9], HiB[3];
+        if (exp_lm && lane == 0) exp_lm[10 * (size_t)l] = ok ? 1.0 : 0.0;
         if (ok) {
             inv3<T>(Hll, Hi);
+            if (exp_lm && lane < 9) exp_lm[10 * (size_t)l + 1 + lane] = (double)Hi[lane];
 #pragma unroll
             for (int i = 0; i < 3; ++i) HiB[i] = Hi[i * 3] * bl[0] + Hi[i * 3 + 1] * bl[1] + Hi[i * 3 + 2] * bl[2];
             for (int q = lane; q < nt * 18; q += 32) {
@@ -829,14 +841,20 @@ __global__ void __launch_bounds__(BA_THREADS, 1) k_ba_windows(XcbBaWindows d, in
             } else {
                 for (int q = tid; q < n * (n + 1) / 2; q += blockDim.x) S64[q] = 0.0;
                 __syncthreads();
-                pass_build<double, true>(sh, d, sh.g64, S64, sh.g, wl64, &c_tot, frz, bsc);
+                // the landmark records and chi2 only when the window's row of dx0 holds them
+                const long long Mw = (long long)d.lm_ob[sh.w.lm0 + L] - d.lm_ob[sh.w.lm0];
+                double* exl = mode == XCB_BA_LINEARISE && (long long)n * n + n + 10LL * L + Mw <= dx0_stride
+                                  ? dx0 + (size_t)w * dx0_stride + (size_t)n * n + n : nullptr;
+                pass_build<double, true>(sh, d, sh.g64, S64, sh.g, wl64, &c_tot, frz, bsc, exl,
+                                         exl ? exl + 10 * (size_t)L : nullptr);
                 c_tot = block_sum_red(sh);
                 for (int q = tid; q < n; q += blockDim.x) sh.rhs[q] = sh.g[q];
             }
             __syncthreads();
             if (mode == XCB_BA_LINEARISE) {
                 // final_linearisation's visual part (window.py:985-1008): the reduced system at the current state, no
-                // hold, no step; dx0 receives H (n x n, row-major) and then b for each window
+                // hold, no step; dx0 receives, for each window, H (n x n, row-major), b (n), the landmark records
+                // [lm_ok, Hll^-1] (10 L, from pass_build) and the observations' chi2 (from lin_landmark)
                 double* o = dx0 + (size_t)w * dx0_stride;
                 for (int q = tid; q < n * n; q += blockDim.x) {
                     const int i = q / n, j = q % n;
