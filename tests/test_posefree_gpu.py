@@ -115,3 +115,18 @@ def test_final_linearisation_systems(G):
                      w.cy, w.huber_k, 0.0, lo, Hi, ok)
     assert np.array_equal(pf.ok, ok) and np.array_equal(pf.Hinv[ok], Hi[ok])
     assert cost[3] > cost[4]                             # the block's cost joins the window's
+
+
+def test_marg_system(G):
+    """window.marg_system: the masked landmarks' reduced system against the oracle's build_system with that mask
+    (lam = 0), H and b to 1e-9 of their scale; the offsets are 6 per slot."""
+    from xclean_b200.backend import ba
+    w = window(G, 1, "pfs")
+    rng = np.random.default_rng(4)
+    mask = rng.random(w.lmp.shape[0]) < 0.3
+    (H, b, off), = ba.marg_system([w], [mask])
+    ref = window(G, 1)
+    ref.lm_mask = mask
+    Hr, br = BO.build_system(ref, 0.0)[:2]
+    assert np.abs(H - Hr).max() <= 1e-9 * np.abs(Hr).max() and np.abs(b - br).max() <= 1e-9 * np.abs(br).max()
+    assert np.array_equal(off, np.arange(w.Rwb.shape[0] + 1) * 6)

@@ -383,3 +383,26 @@ def final_linearisation(windows, device="cuda"):
         sy["lm_ok"], sy["Hll_inv"], sy["ob_chi2"] = sy["lm_ok"][:L], sy["Hll_inv"][:L], sy["ob_chi2"][:M]
         posefree_marginals(w)
     return systems, cost
+
+
+def marg_system(windows, lm_masks, device="cuda"):
+    """window.marg_system (window.py:1011-1031) for a batch of purely visual windows: for each window and its
+    landmark mask, the linear system (H, b) of the masked landmarks' visual observations, Schur'd out, at the current
+    state (lam = 0; the reference adds the prior and IMU terms, which this path has none of), and the state offsets.
+    The pose-free block never enters (the reference's marg_system does not see it).  -> list of (H, b, off)."""
+    views = []
+    for w, m in zip(windows, lm_masks):
+        v = _Masked(w, np.ascontiguousarray(m, np.bool_).reshape(w.lmp.shape[0]))
+        views.append(v)
+    systems, _cost = BatchSolver(views, device, hold=None).linearise()
+    return [(s["H"], s["b"], np.arange(w.Rwb.shape[0] + 1, dtype=np.int64) * 6) for s, w in zip(systems, windows)]
+
+
+class _Masked:
+    """A window's arrays with another landmark mask and no pose-free block."""
+
+    def __init__(self, w, mask):
+        for k in ("Rwb", "pwb", "Rbc", "pbc", "lmp", "lm_host", "rho_meas", "rho_isig", "ob_start", "ob_pose", "ob_cam",
+                  "ob_z", "ob_isig", "ob_valid", "fx", "fy", "cx", "cy", "B", "huber_k"):
+            setattr(self, k, getattr(w, k))
+        self.lm_mask = mask
