@@ -112,8 +112,10 @@ int xcb_front_pipeline_host(xcb_front* f, const uint8_t* left, const uint8_t* ri
    going to its frames' rows of `out` (arrays for all `nframes` frames); batch b's frames are matched as by
    consecutive xcb_front_pipeline_host calls (batch 0 against the previous call's last frame when match_prev != 0).
    No reference counterpart as one call: the reference uploads and processes frame by frame.  The next batch's
-   frames are copied in on a second stream into a second input buffer pair while the current batch computes (page-
-   locked `left` / `right` make that copy overlap); the first call allocates that buffer pair and the stream. */
+   frames are copied in on a second stream into a second input buffer pair while the current batch computes, and
+   each batch's results are copied on the device into one of two staging blocks and read back on a third stream
+   while the next batch computes (page-locked `left` / `right` / `out` make the copies overlap); the first call
+   allocates the buffers, the streams and the events. */
 int xcb_front_pipeline_host_batches(xcb_front* f, const uint8_t* left, const uint8_t* right, int nframes, int batch,
                                     int budget, int half, int dlo, int dhi, int match_prev, const xcb_front_bufs* out,
                                     void* stream);

@@ -6,6 +6,7 @@
 // allocated at creation (nothing per call on the device path), and the batched pipeline's ~13 launches are captured
 // once into a CUDA graph and replayed.
 #include <algorithm>
+#include <cstddef>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -25,10 +26,13 @@ extern "C" int xcb_version(void) { return 1; }
 struct xcb_front {
     int W, H, cap, maxF, Hp, Wp;
     cudaStream_t stream;
-    // xcb_front_pipeline_host_batches: a copy stream and a second input buffer pair (made on first use)
-    cudaStream_t cstream;
-    cudaEvent_t ev_loaded[2], ev_free[2];
+    // xcb_front_pipeline_host_batches (made on first use): a copy stream and a second input buffer pair for the
+    // uploads; a read-back stream and two device staging blocks that each batch's results are copied into, so the
+    // read-back of batch b overlaps batch b+1's compute
+    cudaStream_t cstream, rstream;
+    cudaEvent_t ev_loaded[2], ev_free[2], ev_staged[2], ev_read[2];
     u8* d_in2[2];
+    char* d_stage[2];
     std::string err;
     size_t dev_bytes;
     std::vector<void*> allocs;
@@ -417,8 +421,15 @@ extern "C" void xcb_front_destroy(xcb_front* f)
     if (f->h_stage) cudaFreeHost(f->h_stage);
     if (f->cstream) {
         cudaStreamSynchronize(f->cstream);
-        for (int k = 0; k < 2; ++k) { cudaEventDestroy(f->ev_loaded[k]); cudaEventDestroy(f->ev_free[k]); }
+        cudaStreamSynchronize(f->rstream);
+        for (int k = 0; k < 2; ++k) {
+            cudaEventDestroy(f->ev_loaded[k]);
+            cudaEventDestroy(f->ev_free[k]);
+            cudaEventDestroy(f->ev_staged[k]);
+            cudaEventDestroy(f->ev_read[k]);
+        }
         cudaStreamDestroy(f->cstream);
+        cudaStreamDestroy(f->rstream);
     }
     if (f->stream) cudaStreamDestroy(f->stream);
     delete f;
@@ -880,29 +891,53 @@ extern "C" int xcb_front_buffers(xcb_front* f, xcb_front_bufs* o)
 }
 
 // D2H of every non-NULL result array of `out` for the frames [f0, f0 + nframes) of a host result set
-static int d2h_results(xcb_front* f, const xcb_front_bufs* out, size_t f0, size_t nframes, cudaStream_t st)
+// the result fields of xcb_front_bufs with their bytes per frame, in one table for the staging copies
+struct ResField {
+    size_t off;      // offset of the field in xcb_front_bufs (a pointer member)
+    size_t per;      // bytes per frame
+};
+
+static int result_fields(const xcb_front* f, ResField* rf)
 {
-    const size_t F = nframes, cap = f->cap;
+    const size_t cap = f->cap;
+    int n = 0;
+#define RF(field, per_frame) rf[n++] = ResField{offsetof(xcb_front_bufs, field), (per_frame)};
+    RF(counts, 4) RF(kp, cap * 8) RF(desc, cap * 32) RF(d, cap * 8) RF(sig, cap * 8) RF(ok, cap) RF(zn, cap * 8)
+    RF(dy, cap * 8) RF(m0, cap * 8) RF(m1, cap * 8) RF(nmatch, 4) RF(floor, 8) RF(anypos, 4)
+#undef RF
+    return n;
+}
+
+static void* field_ptr(const xcb_front_bufs* b, size_t off) { return *(void* const*)((const char*)b + off); }
+
+// device results of the last batch (fn frames) -> staging block `stage` (fields at maxF-frame strides), on st
+static int stage_results(xcb_front* f, const xcb_front_bufs* out, char* stage, size_t fn, cudaStream_t st)
+{
     xcb_front_bufs d;
     xcb_front_buffers(f, &d);
-#define DLB(field, per_frame)                                                                                   \
-    if (out->field)                                                                                            \
-        CK(cudaMemcpyAsync((char*)out->field + f0 * (per_frame), d.field, F * (per_frame), cudaMemcpyDeviceToHost, \
-                           st), "D2H " #field);
-    DLB(counts, 4)
-    DLB(kp, cap * 8)
-    DLB(desc, cap * 32)
-    DLB(d, cap * 8)
-    DLB(sig, cap * 8)
-    DLB(ok, cap)
-    DLB(zn, cap * 8)
-    DLB(dy, cap * 8)
-    DLB(m0, cap * 8)
-    DLB(m1, cap * 8)
-    DLB(nmatch, 4)
-    DLB(floor, 8)
-    DLB(anypos, 4)
-#undef DLB
+    ResField rf[16];
+    const int n = result_fields(f, rf);
+    size_t base = 0;
+    for (int i = 0; i < n; ++i) {
+        if (field_ptr(out, rf[i].off))
+            CK(cudaMemcpyAsync(stage + base, field_ptr(&d, rf[i].off), fn * rf[i].per, cudaMemcpyDeviceToDevice, st),
+               "stage results");
+        base += (size_t)f->maxF * rf[i].per;
+    }
+    return XCB_OK;
+}
+
+// staging block -> the host rows f0.. of `out`, on rs
+static int read_stage(xcb_front* f, const xcb_front_bufs* out, const char* stage, size_t f0, size_t fn, cudaStream_t rs)
+{
+    ResField rf[16];
+    const int n = result_fields(f, rf);
+    size_t base = 0;
+    for (int i = 0; i < n; ++i) {
+        char* h = (char*)field_ptr(out, rf[i].off);
+        if (h) CK(cudaMemcpyAsync(h + f0 * rf[i].per, stage + base, fn * rf[i].per, cudaMemcpyDeviceToHost, rs), "D2H");
+        base += (size_t)f->maxF * rf[i].per;
+    }
     return XCB_OK;
 }
 
@@ -917,14 +952,25 @@ extern "C" int xcb_front_pipeline_host_batches(xcb_front* f, const uint8_t* left
     cudaStream_t st = stream ? (cudaStream_t)stream : f->stream;
     if (!f->cstream) {
         CK(cudaStreamCreateWithFlags(&f->cstream, cudaStreamNonBlocking), "copy stream");
+        CK(cudaStreamCreateWithFlags(&f->rstream, cudaStreamNonBlocking), "read-back stream");
         for (int k = 0; k < 2; ++k) {
             CK(cudaEventCreateWithFlags(&f->ev_loaded[k], cudaEventDisableTiming), "event");
             CK(cudaEventCreateWithFlags(&f->ev_free[k], cudaEventDisableTiming), "event");
+            CK(cudaEventCreateWithFlags(&f->ev_staged[k], cudaEventDisableTiming), "event");
+            CK(cudaEventCreateWithFlags(&f->ev_read[k], cudaEventDisableTiming), "event");
         }
         CK(dalloc(f, &f->d_in2[0], (size_t)f->maxF * npx), "alloc inputs");
         CK(dalloc(f, &f->d_in2[1], (size_t)f->maxF * npx), "alloc inputs");
-        CK(cudaEventRecord(f->ev_free[0], st), "event");
-        CK(cudaEventRecord(f->ev_free[1], st), "event");
+        ResField rf[16];
+        const int nf = result_fields(f, rf);
+        size_t per = 0;
+        for (int i = 0; i < nf; ++i) per += rf[i].per;
+        CK(dalloc(f, &f->d_stage[0], (size_t)f->maxF * per), "alloc staging");
+        CK(dalloc(f, &f->d_stage[1], (size_t)f->maxF * per), "alloc staging");
+        for (int k = 0; k < 2; ++k) {
+            CK(cudaEventRecord(f->ev_free[k], st), "event");
+            CK(cudaEventRecord(f->ev_read[k], st), "event");
+        }
     }
     // input pairs: buffer 0 = the front's own (d_left, d_right), buffer 1 = d_in2
     u8* inL[2] = {f->d_left, f->d_in2[0]};
@@ -939,6 +985,15 @@ extern "C" int xcb_front_pipeline_host_batches(xcb_front* f, const uint8_t* left
         CK(cudaEventRecord(f->ev_loaded[k], f->cstream), "loaded");
         return XCB_OK;
     };
+    auto read = [&](int b) -> int {
+        const int k = b & 1;
+        const size_t f0 = (size_t)b * batch, fn = (size_t)std::min(batch, nframes - b * batch);
+        CK(cudaStreamWaitEvent(f->rstream, f->ev_staged[k], 0), "wait staged");
+        const int r = read_stage(f, out, f->d_stage[k], f0, fn, f->rstream);
+        if (r) return r;
+        CK(cudaEventRecord(f->ev_read[k], f->rstream), "read");
+        return XCB_OK;
+    };
     int rc = load(0);
     if (!rc && nb > 1) rc = load(1);
     for (int b = 0; b < nb && !rc; ++b) {
@@ -948,16 +1003,24 @@ extern "C" int xcb_front_pipeline_host_batches(xcb_front* f, const uint8_t* left
         rc = xcb_front_pipeline_dev(f, inL[k], inR[k], fn, budget, half, dlo, dhi, match_prev || b > 0, st);
         if (rc) break;
         CK(cudaEventRecord(f->ev_free[k], st), "free");
-        // the next load of this buffer is queued before the results are read back, so that a read into pageable
-        // host memory (which returns only when done) does not hold the copy stream back
-        if (b + 2 < nb) rc = load(b + 2);
-        if (!rc) rc = d2h_results(f, out, (size_t)b * batch, fn, st);
+        // the next upload into this buffer pair, then this batch's results into staging block k once batch b-2's
+        // read-back from it has finished
+        if (b + 2 < nb && (rc = load(b + 2))) break;
+        CK(cudaStreamWaitEvent(st, f->ev_read[k], 0), "wait read");
+        if ((rc = stage_results(f, out, f->d_stage[k], (size_t)fn, st))) break;
+        CK(cudaEventRecord(f->ev_staged[k], st), "staged");
+        // the previous batch's read-back is queued only now, so that a read into pageable host memory (which returns
+        // only when done) leaves this batch's work already queued on the device
+        if (b > 0 && (rc = read(b - 1))) break;
     }
+    if (!rc) rc = read(nb - 1);
     if (rc) {
         cudaStreamSynchronize(f->cstream);
+        cudaStreamSynchronize(f->rstream);
         cudaStreamSynchronize(st);
         return rc;
     }
+    CK(cudaStreamSynchronize(f->rstream), "read-back sync");
     CK(cudaStreamSynchronize(st), "pipeline sync");
     return check_dev_err(f);
 }
