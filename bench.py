@@ -10,6 +10,12 @@ stereo over d in [0, 96] with the affine-LK sub-pixel step, Hamming matching aga
 ratio 0.8, chance bound 104).  One step = the whole sequence, in graph-replayed batches of frames.  The inputs
 (467 MB) are larger than the 126 MB L2, so no flush is needed between steps.
 
+The end-to-end figure (`e2e`) goes through GpuFront.pipeline_batches from pinned host arrays: both images of every
+frame uploaded and every result read back inside the timed region.  Beside the headline line's frontend numbers:
+"ba" (the batched window solve of 256 uneven windows, mixed and float64, against the plain per-window form, the
+20-keyframe windows and the differentiable BA) and "mapmatch" (the gated map matcher over the sequence's frames,
+batched on the device and per frame from host arrays, and the fused predict + match tracking step).
+
 --impl reference times the reference's own CPU implementation of the path (its C restatement in oracle/, verified
 bit-exact against the reference's CPU modules) on all host cores, on a bounded sample of the same frames.
 Multi-GPU (torchrun): every rank runs its own 500-frame sequence (weak scaling, no collective on the data path);

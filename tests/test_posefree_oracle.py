@@ -93,3 +93,25 @@ def _bad_host(w):
     w.pf.host = w.pf.host.copy()
     w.pf.host[0] = w.Rwb.shape[0]
     return w
+
+
+def test_pack_windows_appends_the_posefree_block(G):
+    """The packed batch carries each pose-free landmark after the window's own, with one observation (host slot, left
+    camera, its pixel and whitening) and its prior; a window without a block packs as before."""
+    from xclean_b200.backend.ba import pack_windows
+    w = window(G, 1, "pfs")
+    plain = window(G, 1)
+    pk = pack_windows([w, plain], hold=None)
+    L, M, n = plain.lmp.shape[0], int(plain.ob_start[-1]), len(w.pf.host)
+    assert list(pk["L"]) == [L + n, L]
+    lo = pk["lm_off"]
+    assert np.array_equal(pk["lmp"][lo[0] + L:lo[0] + L + n], w.pf.lmp)
+    assert np.array_equal(pk["lm_host"][lo[0] + L:lo[0] + L + n], w.pf.host)
+    assert np.array_equal(pk["rho_isig"][lo[0] + L:lo[0] + L + n], w.pf.ris)
+    ob = pk["lm_ob"]
+    assert np.array_equal(np.diff(ob[lo[0] + L:lo[0] + L + n + 1]), np.ones(n))
+    k0 = ob[lo[0] + L]
+    assert k0 == M
+    assert np.array_equal(pk["ob_pose"][k0:k0 + n], w.pf.host) and (pk["ob_cam"][k0:k0 + n] == 0).all()
+    assert np.array_equal(pk["ob_z"][k0:k0 + n], w.pf.z) and (pk["ob_isig"][k0:k0 + n] == w.pf.isg).all()
+    assert np.array_equal(pk["lmp"][lo[1]:lo[1] + L], plain.lmp)
