@@ -5,10 +5,10 @@
 // Three launches per call (grid.y = frame):
 //   k_mm_grid    one CTA per frame builds the 16-px keypoint grid: cell counts by shared-memory atomics, a block scan
 //                into cell starts, then each keypoint's index stored in its cell's range (any order inside a cell).
-//   k_mm_gate    four lanes per landmark: the gate preamble (det, Sinv, half-widths, the box of cells under the
+//   k_mm_gate    two lanes per landmark: the gate preamble (det, Sinv, half-widths, the box of cells under the
 //                ellipse), then the lanes walk the box's cell rows side by side (one contiguous range of entries per
 //                row), apply the Mahalanobis gate, take the minimum Hamming distance over the landmark's descriptors and
-//                keep a lane-local best / second best, merged across the four lanes; chance bound and Lowe ratio; an
+//                keep a lane-local best / second best, merged across the two lanes; chance bound and Lowe ratio; an
 //                accepted landmark claims its keypoint, counts itself on it and leaves its id in one of the keypoint's
 //                four claimant slots.
 //   k_mm_mutual  one thread per landmark: a keypoint with a single claimant goes to it; the reference's owner fold
@@ -37,7 +37,7 @@ extern void xcb_set_last_error(const std::string& m);
 #define MM_GRID 16            // mapmatch.py:30
 #define MM_GRID_T 1024        // threads of k_mm_grid
 #define MM_WARPS 8            // warps per CTA of k_mm_gate / k_mm_mutual
-#define MM_GROUP 4            // lanes per landmark in k_mm_gate
+#define MM_GROUP 2            // lanes per landmark in k_mm_gate (2 measured faster than 4 and 8: more landmarks in flight)
 #define MM_SLOTS 4            // claimant ids kept per keypoint (more claimants: the ordered scan of all claims)
 #define MM_LPB (MM_WARPS * 32 / MM_GROUP)   // landmarks per CTA of k_mm_gate
 // x / 16 and x * 0.0625 are the same correctly rounded double for every x (scaling by a power of two)
@@ -168,7 +168,7 @@ __device__ __forceinline__ int mm_ham(const uint4* p, const uint4* q)
            + __popc(a1.x ^ b1.x) + __popc(a1.y ^ b1.y) + __popc(a1.z ^ b1.z) + __popc(a1.w ^ b1.w);
 }
 
-// ------------------------------------------------------------------------------ gate (4 lanes per landmark, 64 per CTA)
+// ----------------------------------------------------------------------------- gate (2 lanes per landmark, 128 per CTA)
 template <typename KT>
 __global__ void __launch_bounds__(MM_WARPS * 32, 4) k_mm_gate(MMArgs a)
 {
