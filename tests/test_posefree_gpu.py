@@ -90,7 +90,7 @@ def test_final_linearisation_systems(G):
     from xclean_b200.backend import ba
     WG = dict(np.load(WGOLD))
     ws = [wwindow(WG, c) for c in (0, 1, 2)] + [window(G, 1, "pfs"), window(G, 1)]
-    systems, cost = ba.final_linearisation(ws)
+    systems, cost = ba.final_linearisation_batch(ws)
     for i, w in enumerate(ws):
         ref = w if getattr(w, "pf", None) is None else window(G, 1)
         H, b, c, Hi, _bl, _Hlp, ok, chi = BO.build_system(ref, 0.0, want_chi2=True)
@@ -124,9 +124,31 @@ def test_marg_system(G):
     w = window(G, 1, "pfs")
     rng = np.random.default_rng(4)
     mask = rng.random(w.lmp.shape[0]) < 0.3
-    (H, b, off), = ba.marg_system([w], [mask])
+    (H, b, off), = ba.marg_system_batch([w], [mask])
     ref = window(G, 1)
     ref.lm_mask = mask
     Hr, br = BO.build_system(ref, 0.0)[:2]
     assert np.abs(H - Hr).max() <= 1e-9 * np.abs(Hr).max() and np.abs(b - br).max() <= 1e-9 * np.abs(br).max()
     assert np.array_equal(off, np.arange(w.Rwb.shape[0] + 1) * 6)
+
+
+def test_single_window_signatures(G):
+    """window.solve / final_linearisation / marg_system with the reference's signatures and return shapes: solve
+    equals the reference's solve with the block attached (float64, free gauge) and returns its stats dict; the
+    linearisation tuple matches the batched outputs; a prior or IMU terms are refused."""
+    from xclean_b200.backend import ba
+    w = window(G, 1, "pfs")
+    st = ba.solve(w, iters=5, lam0=1e-4)
+    ref = G["c1_stats"]
+    assert set(st) == {"cost0", "cost", "accepted", "iters", "lam"} and st["accepted"] == int(ref[2])
+    assert abs(st["cost0"] - ref[0]) <= 1e-9 * abs(ref[0])
+    assert np.abs(w.pwb - G["c1_pwb_n"]).max() < 1e-6
+    H, b, chi2, ok, Hi, imu, off = ba.final_linearisation(w)
+    (sy,), _c = ba.final_linearisation_batch([w])
+    assert np.array_equal(H, sy["H"]) and np.array_equal(chi2, sy["ob_chi2"]) and np.array_equal(ok, sy["lm_ok"])
+    assert imu == [] and np.array_equal(off, np.arange(w.Rwb.shape[0] + 1) * 6) and w.pf.ok.any()
+    Hm, bm, offm = ba.marg_system(w, np.asarray(w.lm_mask, np.bool_))      # the window's own mask: its H again
+    assert np.allclose(Hm, H, rtol=0, atol=1e-9 * np.abs(H).max())
+    w.prior = object()
+    with pytest.raises(NotImplementedError):
+        ba.solve(w)

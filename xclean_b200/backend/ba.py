@@ -12,7 +12,10 @@ the drop-in of its stage kernels).
     bs.linearise()                          # final_linearisation's reduced visual system per window
     posefree_cost(...), posefree_step(...)  # window.py's pose-free block functions, bit-identical
     posefree_marginals(w)                   # final_linearisation's pose-free marginals into w.pf.Hinv / w.pf.ok
-    systems, costs = final_linearisation(windows)
+    systems, costs = final_linearisation_batch(windows);  H, b, off = marg_system_batch(windows, masks)[i]
+
+    # window.py's own single-window signatures (visual windows; prior / IMU raise NotImplementedError)
+    st = solve(pb, iters=5, lam0=1e-4);  final_linearisation(pb);  marg_system(pb, lm_mask)
 
 Every call goes through libxcb200.so's C ABI (xcb_ba_solve_windows_dev); there is no CPU fallback.
 """
@@ -371,7 +374,7 @@ def posefree_marginals(w):
                   w.huber_k, 0.0, np.zeros_like(pf.lmp), pf.Hinv, pf.ok)
 
 
-def final_linearisation(windows, device="cuda"):
+def final_linearisation_batch(windows, device="cuda"):
     """window.final_linearisation for a batch of purely visual windows (no prior, no IMU): per window a dict of the
     reference's outputs for such a window - H, b (the Schur-reduced visual system at lam = 0), ob_chi2 (M), lm_ok (L),
     Hll_inv (L,3,3) of the window's own landmarks and observations - and the pose-free block's marginals into
@@ -385,7 +388,7 @@ def final_linearisation(windows, device="cuda"):
     return systems, cost
 
 
-def marg_system(windows, lm_masks, device="cuda"):
+def marg_system_batch(windows, lm_masks, device="cuda"):
     """window.marg_system (window.py:1011-1031) for a batch of purely visual windows: for each window and its
     landmark mask, the linear system (H, b) of the masked landmarks' visual observations, Schur'd out, at the current
     state (lam = 0; the reference adds the prior and IMU terms, which this path has none of), and the state offsets.
@@ -406,3 +409,38 @@ class _Masked:
                   "ob_z", "ob_isig", "ob_valid", "fx", "fy", "cx", "cy", "B", "huber_k"):
             setattr(self, k, getattr(w, k))
         self.lm_mask = mask
+
+
+# --------------------------------------------------------------------- window.py's single-window signatures
+def _visual_only(pb, what):
+    if getattr(pb, "prior", None) is not None or getattr(pb, "imu", None):
+        raise NotImplementedError("%s: the marginal prior and IMU terms are not on this path (visual windows only)"
+                                  % what)
+    if getattr(pb, "dims", None) is not None and (np.asarray(pb.dims) != 6).any():
+        raise NotImplementedError("%s: full-state slots (dims 15) are not on this path" % what)
+
+
+def solve(pb, iters=5, lam0=1e-4, device="cuda"):
+    """window.solve (src/xclean/vio/window.py:889-982) for one visual window, pose-free block included, in float64 on
+    the device; pb is updated in place.  -> dict(cost0, cost, accepted, iters, lam) as the reference returns."""
+    _visual_only(pb, "solve")
+    res = solve_batch([pb], iters=iters, lam0=lam0, precision="fp64", hold=None, device=device)
+    if int(res["status"][0]) != 0:
+        raise RuntimeError("solve: the window exceeds the device solver's limits (status %d)" % int(res["status"][0]))
+    return {"cost0": float(res["cost0"][0]), "cost": float(res["cost"][0]), "accepted": int(res["accepted"][0]),
+            "iters": int(iters), "lam": float(res["lam"][0])}
+
+
+def final_linearisation(pb, device="cuda"):
+    """window.final_linearisation (window.py:985-1008) for one visual window: -> (H, bvec, ob_chi2, lm_ok, Hll_inv,
+    imu_chi2 ([]: no IMU), off), the pose-free block's marginals into pb.pf.Hinv / pb.pf.ok."""
+    _visual_only(pb, "final_linearisation")
+    (sy,), _cost = final_linearisation_batch([pb], device=device)
+    P = pb.Rwb.shape[0]
+    return sy["H"], sy["b"], sy["ob_chi2"], sy["lm_ok"], sy["Hll_inv"], [], np.arange(P + 1, dtype=np.int64) * 6
+
+
+def marg_system(pb, lm_mask, device="cuda"):
+    """window.marg_system (window.py:1011-1031) for one visual window: -> (H, b, off)."""
+    _visual_only(pb, "marg_system")
+    return marg_system_batch([pb], [lm_mask], device=device)[0]
