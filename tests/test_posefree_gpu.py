@@ -145,7 +145,9 @@ def test_single_window_signatures(G):
     assert np.abs(w.pwb - G["c1_pwb_n"]).max() < 1e-6
     H, b, chi2, ok, Hi, imu, off = ba.final_linearisation(w)
     (sy,), _c = ba.final_linearisation_batch([w])
-    assert np.array_equal(H, sy["H"]) and np.array_equal(chi2, sy["ob_chi2"]) and np.array_equal(ok, sy["lm_ok"])
+    # two linearisations agree to rounding (the reduced system is accumulated by atomics in any order)
+    assert np.abs(H - sy["H"]).max() <= 1e-12 * np.abs(H).max()
+    assert np.array_equal(chi2, sy["ob_chi2"]) and np.array_equal(ok, sy["lm_ok"])
     assert imu == [] and np.array_equal(off, np.arange(w.Rwb.shape[0] + 1) * 6) and w.pf.ok.any()
     Hm, bm, offm = ba.marg_system(w, np.asarray(w.lm_mask, np.bool_))      # the window's own mask: its H again
     assert np.allclose(Hm, H, rtol=0, atol=1e-9 * np.abs(H).max())
