@@ -54,3 +54,22 @@ def test_map_matcher_argument_checks_without_a_device():
     assert b"49152" in L.xcb_last_error()
     assert L.xcb_mm_match_host(None, None, 0, None, None, None, None, 0, None, 0, 1.0, None, None, None,
                                None) == _lib.XCB_ERR_ARG
+
+
+def test_new_entry_points_refuse_bad_arguments_without_a_device():
+    """The prediction, pose-free, linearisation and batched-pipeline entries check their arguments on the host
+    before any device call."""
+    L = _lib.lib()
+    z = [None] * 9
+    assert L.xcb_mm_predict_host(None, *z, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0, 0, None, None, None, None,
+                                 None) == _lib.XCB_ERR_ARG
+    assert L.xcb_mm_predict_match_host(None, *z, 1.0, 1.0, 1.0, 1.0, 1.0, 0, None, 0, None, None, 0, None, 1.0,
+                                       None, None, None, None, None, None, None, None) == _lib.XCB_ERR_ARG
+    assert L.xcb_mm_match_dev(None, 1, None, None, 0, None, None, None, None, 1, None, None, 0, 1.0, None, None,
+                              None, None) == _lib.XCB_ERR_ARG
+    assert L.xcb_ba_linearise_windows_dev(None, 1, None, 0, None, None, 0, 0, None) == _lib.XCB_ERR_ARG
+    assert L.xcb_ba_posefree_host(0, None, None, None, None, 0, None, None, None, None, None, 1.0, 1.0, 1.0, 1.0, 1.0,
+                                  1.345, 0, 0.0, None, None, None, None, None) == _lib.XCB_ERR_ARG
+    assert b"bad window" in L.xcb_last_error()
+    assert L.xcb_front_pipeline_host_batches(None, None, None, 1, 1, 100, 4, 0, 96, 0, None,
+                                             None) == _lib.XCB_ERR_ARG
