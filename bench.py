@@ -63,6 +63,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ba", action="store_true")
     ap.add_argument("--no-mm", action="store_true", help="skip the gated map matcher")
+    ap.add_argument("--no-hd", action="store_true", help="skip the 64-frame 1280x720 frontend batch")
     ap.add_argument("--ba-only", action="store_true",
                     help="run only the batched window BA part and print its JSON object (profiling)")
     ap.add_argument("--ba-windows", type=int, default=None, help="BA windows per step (default 256)")
@@ -135,41 +136,44 @@ def peaks():
 # ------------------------------------------------------------------------------------------------ reference arm
 def run_reference(args, ws, rank):
     """The reference's CPU implementation of the path (oracle/, C restatement, OpenMP over frames, all host threads) on
-    a bounded sample of the same frames; one bounded sample per step."""
+    the same workload as our arm: every step runs all `--frames` frames of the same sequence (seed 0) at the same
+    budget, window and disparity range; the same config dict is printed.  Warm-up steps run a core-count sample."""
     if rank != 0:
         return 0
     import torch
     from oracle import front_oracle as O
     from xclean_b200 import synth
-    from xclean_b200.front.gpu_front import GpuFront, probe_orb_pattern
-    from xclean_b200.front.features import noise_q99
-    import cv2
+    from xclean_b200.front.gpu_front import probe_orb_pattern
     cores = os.cpu_count() or 1
-    sample = max(8, min(args.frames, 2 * cores))
+    F = args.frames
     dev = "cuda" if torch.cuda.is_available() else "cpu"
-    L, R = synth.sequence(synth.CAM_KITTI, sample, seed=0, device=dev)
+    L, R = synth.sequence(synth.CAM_KITTI, F, seed=0, device=dev)
     L, R = L.cpu().numpy(), R.cpu().numpy()
     cal = _cpu_calibration()
     pat = probe_orb_pattern()
     for _ in range(max(1, args.warmup)):
-        O.frames(L[:min(sample, cores)], R[:min(sample, cores)], BUDGET, cal["q99"], cal, pat, HALF, DLO, DHI,
-                 cap=2048, nthreads=cores)
+        O.frames(L[:cores], R[:cores], BUDGET, cal["q99"], cal, pat, HALF, DLO, DHI, cap=2048, nthreads=cores)
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
         O.frames(L, R, BUDGET, cal["q99"], cal, pat, HALF, DLO, DHI, cap=2048, nthreads=cores)
         times.append(time.perf_counter() - t0)
     dt = sum(times)
-    fps = sample * args.steps / dt
+    fps = F * args.steps / dt
+    t0 = time.perf_counter()
+    O.frames(L[:4], R[:4], BUDGET, cal["q99"], cal, pat, HALF, DLO, DHI, cap=2048, nthreads=1)
+    fps1 = 4 / (time.perf_counter() - t0)
     line = {"metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u8/f32/f64", "data": "synthetic",
-            "config": {"workload": "kitti-like 1241x376 stereo sequence, 2000 features, 9x9 ZNCC d 0-96, match to "
-                                   "previous frame", "frames_per_step": sample, "budget": BUDGET, "half": HALF},
+            "vs_baseline": None, "dtype": "u8/f32/f64",
+            "data": "synthetic (rendered textured-plane driving sequence, seeded)",
+            "config": headline_config(F, args.batch),
             "impl": "reference",
             "cpu_baseline": {"value": fps, "unit": "frames/s", "cores": cores, "kind": "port",
-                             "sample": "%d frames of the sequence per step, OpenMP over frames" % sample},
-            "e2e": {"value": fps, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+                             "sample": "all %d frames of the sequence per step, OpenMP over frames" % F,
+                             "single_thread_frames_per_s": fps1},
+            "e2e": {"value": fps, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "reference_cupy": cupy_status()}
     if not args.no_ba:
         from oracle import ba_oracle as BO
         from xclean_b200.backend import synth_ba as S
@@ -180,11 +184,30 @@ def run_reference(args, ws, rank):
         for _ in range(args.steps):
             BO.solve_batch([w.copy() for w in sample], iters=BA_ITERS, lam0=BA_LAM0, hold=0, nthreads=cores)
         dt = (time.perf_counter() - t0) / args.steps
+        t0 = time.perf_counter()
+        BO.solve_batch([w.copy() for w in sample[:4]], iters=BA_ITERS, lam0=BA_LAM0, hold=0, nthreads=1)
+        dt1 = (time.perf_counter() - t0) / 4
         line["ba"] = {"metric": "BA windows/s (plain per-window float64, the reference's window.solve restated)",
                       "value": len(sample) / dt, "unit": "windows/s", "cores": cores,
+                      "single_thread_windows_per_s": 1.0 / dt1,
                       "sample": "%d of the 256 windows per step" % len(sample)}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def headline_config(F, batch):
+    return {"workload": "kitti-like 1241x376 stereo sequence, 2000 features, 9x9 ZNCC d 0-96, match to previous frame",
+            "frames_per_step_per_gpu": F, "batch": batch, "budget": BUDGET, "half": HALF,
+            "l2": "inputs (467 MB/GPU) larger than L2, no flush"}
+
+
+def cupy_status():
+    """The reference's own CuPy path cannot run without CuPy; record why."""
+    try:
+        import cupy  # noqa: F401
+        return "importable (not timed: the reference's source does not travel with this benchmark)"
+    except Exception as e:           # noqa: BLE001
+        return "unavailable: %s: %s" % (type(e).__name__, e)
 
 
 def _cpu_calibration():
@@ -346,9 +369,13 @@ def run_ours(args, ws, rank, local):
             "whole_path_frac": frame_bytes * value / ws / 1e9 / peak,
             "stage_ms_per_step": per_step}
     cpu = None
+    recheck = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         cpu = cpu_baseline(L, R, args)
+        if outs is not None:
+            recheck = recheck_frames(L, R, outs, gf.calib, gf.pattern, BUDGET, HALF, DLO, DHI)
     del L, R
+    hd = None if (args.no_hd or ws > 1) else run_front_hd(args, dev, stream, rank, cpu=(rank == 0 and not args.no_cpu))
     ba = None if args.no_ba else run_ba(args, dev, stream, rank, ws, cpu=(rank == 0 and ws == 1 and not args.no_cpu))
     mm = None if (args.no_mm or outs is None) else run_mapmatch(args, dev, stream, ws, outs,
                                                                   cpu=(rank == 0 and ws == 1 and not args.no_cpu))
@@ -356,18 +383,152 @@ def run_ours(args, ws, rank, local):
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u8/f32/f64",
             "data": "synthetic (rendered textured-plane driving sequence, seeded)",
-            "config": {"workload": "kitti-like 1241x376 stereo sequence, 2000 features, 9x9 ZNCC d 0-96, match to "
-                                   "previous frame", "frames_per_step_per_gpu": F, "batch": Bt, "budget": BUDGET,
-                       "half": HALF, "l2": "inputs (467 MB/GPU) larger than L2, no flush"},
-            "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
+            "config": headline_config(F, Bt),
+            "e2e": e2e, "reference_cupy": cupy_status(),
+            "reference_numba": "not run by this benchmark: the reference's source is not on the benchmark host; "
+                               "oracle/time_reference_cpu.py times its numba / cv2 modules where the source is", "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
             "gpu_launches": launches_per_step * args.steps,
-            "kp_per_frame_last_batch": float(np.mean(counts)) if len(counts) else None, "ba": ba, "mapmatch": mm}
+            "kp_per_frame_last_batch": float(np.mean(counts)) if len(counts) else None,
+            "bitexact_vs_oracle_all_frames": recheck, "front_hd": hd, "ba": ba, "mapmatch": mm}
     if rank == 0:
         print(json.dumps(line), flush=True)
     gf.close()
     if ws > 1:
         dist.destroy_process_group()
     return 0
+
+
+def recheck_frames(L, R, outs, calib, pattern, budget, half, dlo, dhi):
+    """Every frame of the timed end-to-end run against the oracle (OpenMP over frames): counts, keypoints,
+    descriptors, stereo outputs and matches, bit for bit.  -> bool"""
+    from oracle import front_oracle as O
+    Ln, Rn = L.cpu().numpy(), R.cpu().numpy()
+    cap = outs["kp"].shape[1]
+    ref = O.frames(Ln, Rn, budget, calib["q99"], calib, pattern, half, dlo, dhi, cap=cap)
+    if not (np.array_equal(outs["counts"], ref["counts"]) and np.array_equal(outs["nmatch"], ref["nmatch"])):
+        return False
+    for f in range(len(Ln)):
+        n, m = int(ref["counts"][f]), int(ref["nmatch"][f])
+        for k in ("kp", "desc", "d", "sig", "zn", "ok"):
+            if not np.array_equal(np.ascontiguousarray(outs[k][f, :n]).view(np.uint8),
+                                  np.ascontiguousarray(ref[k][f, :n]).view(np.uint8)):
+                return False
+        if not np.array_equal(np.nan_to_num(outs["dy"][f, :n], nan=-1e300), np.nan_to_num(ref["dy"][f, :n], nan=-1e300)):
+            return False
+        if not (np.array_equal(outs["m0"][f, :m], ref["m0"][f, :m]) and np.array_equal(outs["m1"][f, :m],
+                                                                                     ref["m1"][f, :m])):
+            return False
+    return True
+
+
+HD_W, HD_H = 1280, 720
+HD_FRAMES = 64
+HD_BUDGET = 4000
+HD_CAP = 4096
+HD_HALF = 5             # the reference's 11x11 window (the stress configuration names none)
+HD_DLO, HD_DHI = 0, 127  # the reference's 128-disparity range
+
+
+def run_front_hd(args, dev, stream, rank, cpu=True):
+    """The stress shape: 64 frames of 1280x720 (fx 640, baseline 0.075 m, disparities 0-127), 4,000 features at
+    capacity 4,096, 11x11 ZNCC, matching to the previous frame; one step = the 64 frames in one graph-replayed batch.
+    Device-resident frames/s, end to end through GpuFront.pipeline_batches (batches of 16 from pinned host memory),
+    the dominant stage's roofline, every timed frame checked against the oracle, and the oracle on a bounded sample."""
+    import torch
+    from xclean_b200 import _lib, synth
+    from xclean_b200.front.gpu_front import GpuFront
+    F = HD_FRAMES
+    L, R = synth.sequence(synth.CAM_HD, F, seed=100 + rank, device=dev)
+    torch.cuda.synchronize()
+    gf = GpuFront(HD_W, HD_H, cap=HD_CAP, max_frames=F)
+    gf.calibrate()
+    sptr = stream.cuda_stream
+    gf.set_stage_timing(True)
+
+    def step():
+        gf.pipeline_dev(L.data_ptr(), R.data_ptr(), F, HD_BUDGET, HD_HALF, HD_DLO, HD_DHI, match_prev=False,
+                        stream=sptr)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    gf.sync_check(sptr)
+    gf.stage_times()
+    launches = gf.last_launches()
+    steps = max(args.steps, 5)
+    stage_sum = {k: 0.0 for k in _lib.FRONT_STAGES}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    gf.sync_check(sptr)
+    times, _n = gf.stage_times()
+    per_step = {k: v / steps for k, v in times.items()}
+    Lh, Rh = L.cpu().pin_memory(), R.cpu().pin_memory()
+    outs = gf.alloc_outputs(F)
+    for k in list(outs):
+        outs[k] = torch.from_numpy(outs[k]).pin_memory().numpy()
+    gf.set_stage_timing(False)
+
+    def step_e2e():
+        gf.pipeline_batches(Lh.numpy(), Rh.numpy(), HD_BUDGET, 16, HD_HALF, HD_DLO, HD_DHI, match_prev=False,
+                            out=outs, stream=sptr)
+
+    for _ in range(max(3, args.warmup)):
+        step_e2e()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        step_e2e()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ems = e0.elapsed_time(e1) / steps
+    peak, peak_kind = peaks()
+    n = HD_BUDGET
+    algo = {"response": HD_W * HD_H * 5, "noise_floor": HD_W * HD_H, "candidates": HD_W * HD_H * 4,
+            "greedy": HD_W * HD_H * 4 // 16 + n * 8, "orb": HD_W * HD_H + n * 40, "stereo": 2 * HD_W * HD_H + n * 41,
+            "match": 2 * n * 32 + 16 * n}
+    dom = max(per_step, key=per_step.get)
+    frame_bytes = 2 * HD_W * HD_H + n * (8 + 32 + 33) + n * 32 + 16 * n
+    ach = algo[dom] * F / (per_step[dom] / 1e3) / 1e9 if per_step[dom] > 0 else 0.0
+    res = {"metric": "frontend frames/s (64 x 1280x720, 4000 features, 11x11 ZNCC d 0-127)",
+           "value": F / (ms / 1e3), "unit": "frames/s", "ms_per_step": ms, "frames_per_step": F,
+           "gpu_launches_per_step": launches, "kp_per_frame": float(np.mean(outs["counts"])),
+           "stereo_ok_per_frame": float(np.mean([outs["ok"][f, :outs["counts"][f]].sum() for f in range(F)])),
+           "matches_per_frame": float(np.mean(outs["nmatch"][1:])),
+           "e2e": {"value": F / (ems / 1e3), "unit": "frames/s", "api": "GpuFront.pipeline_batches (batches of 16)",
+                   "h2d_bytes_per_step": 2 * F * HD_W * HD_H, "d2h_bytes_per_step": sum(a.nbytes for a in outs.values())},
+           "roofline": {"bound": "hbm", "kernel": "stage:%s" % dom, "achieved": ach, "peak": peak, "unit": "GB/s",
+                        "frac": ach / peak, "peak_kind": peak_kind, "algorithmic_bytes_per_launch": algo[dom] * F,
+                        "whole_path_frac": frame_bytes * F / (ms / 1e3) / 1e9 / peak,
+                        "algorithmic_bytes_per_frame": frame_bytes, "stage_ms_per_step": per_step},
+           "config": {"workload": "64-frame 1280x720 stereo sequence (fx 640, baseline 0.075 m, 1 m/frame), 4000 "
+                                  "features, cap 4096, 11x11 ZNCC d 0-127, match to the previous frame, one graph per "
+                                  "step", "l2": "inputs (118 MB) re-read each step; the per-frame intermediates "
+                                                "(~1.6 GB) exceed L2"}}
+    if cpu:
+        res["bitexact_vs_oracle_all_frames"] = recheck_frames(L, R, outs, gf.calib, gf.pattern, HD_BUDGET, HD_HALF,
+                                                              HD_DLO, HD_DHI)
+        from oracle import front_oracle as O
+        cores = os.cpu_count() or 1
+        sample = min(F, max(8, cores))
+        Ln, Rn = L[:sample].cpu().numpy(), R[:sample].cpu().numpy()
+        t0 = time.perf_counter()
+        O.frames(Ln, Rn, HD_BUDGET, gf.calib["q99"], gf.calib, gf.pattern, HD_HALF, HD_DLO, HD_DHI, cap=HD_CAP,
+                 nthreads=cores)
+        dt = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        O.frames(Ln[:2], Rn[:2], HD_BUDGET, gf.calib["q99"], gf.calib, gf.pattern, HD_HALF, HD_DLO, HD_DHI,
+                 cap=HD_CAP, nthreads=1)
+        dt1 = time.perf_counter() - t0
+        res["cpu_baseline"] = {"value": sample / dt, "unit": "frames/s", "cores": cores, "kind": "port",
+                               "sample": "%d frames of the same sequence, OpenMP over frames" % sample,
+                               "single_thread_frames_per_s": 2 / dt1}
+    gf.close()
+    return res
 
 
 MM_LANDMARKS = 1500     # window landmarks projected per frame (the 10-keyframe window's 1,500)
@@ -501,6 +662,61 @@ BA_ITERS = 5
 BA_LAM0 = 1e-4
 
 
+def ba_flops(w):
+    """Algorithmic flops of one LM iteration of window.solve on window `w`, counted from window.build_system's loop
+    structure (src/xclean/vio/window.py:292-463, :497-519): per valid observation with nd rows (2 left, 1 right)
+    12 nd, plus (36 + 108 + 12) nd when its keyframe is not the landmark's host; per landmark with k touched slots
+    72 k + 108 k^2 + 30; the reduced system's Cholesky n^3 / 6 + 2 n^2 (n = 6 P); back-substitution 18 P + 9 per
+    landmark."""
+    P, L = w.Rwb.shape[0], w.lmp.shape[0]
+    n = 6 * P
+    cnt = np.diff(w.ob_start)
+    lm = np.repeat(np.arange(L), cnt)
+    keep = w.lm_mask.astype(bool)
+    valid = w.ob_valid.astype(bool) & keep[lm]
+    nd = np.where(w.ob_cam == 0, 2, 1)
+    cross = w.ob_pose != w.lm_host[lm]
+    f = float((nd * (12 + 156 * cross))[valid].sum())
+    key = np.unique(np.concatenate([lm[valid] * 64 + w.ob_pose[valid], np.nonzero(keep)[0] * 64 + w.lm_host[keep]]))
+    k = np.bincount(key // 64, minlength=L).astype(np.float64)[keep]
+    f += float((72 * k + 108 * k * k + 30).sum())
+    f += n ** 3 / 6 + 2 * n * n + (18 * P + 9) * float(keep.sum())
+    return f
+
+
+_PEAK_CACHE = {}
+
+
+def fma_peak(fp64):
+    """The device's FP64 / FP32 FMA-loop peak (TFLOP/s) at the clocks of this run (xcb_peak_fma), median of 3."""
+    import ctypes
+    from xclean_b200 import _lib
+    if fp64 in _PEAK_CACHE:
+        return _PEAK_CACHE[fp64]
+    vals = []
+    for _ in range(3):
+        tf = ctypes.c_double(0.0)
+        _lib.check(_lib.lib().xcb_peak_fma(int(fp64), 65536 if fp64 else 262144, ctypes.byref(tf), None), None,
+                   "xcb_peak_fma")
+        vals.append(tf.value)
+    _PEAK_CACHE[fp64] = float(np.median(vals))
+    return _PEAK_CACHE[fp64]
+
+
+def ba_roofline(wins, iters, ms_fp64, ms_mixed, kernel):
+    """Compute roofline of the window BA: algorithmic flops (ba_flops x iterations) / event-timed ms, against the
+    FP64 FMA-loop peak for the float64 batch and the FP32 one for the mixed batch (its build and Schur are FP32)."""
+    total = sum(ba_flops(w) for w in wins) * iters
+    p64, p32 = fma_peak(True), fma_peak(False)
+    a64 = total / (ms_fp64 / 1e3) / 1e12
+    a32 = total / (ms_mixed / 1e3) / 1e12
+    return {"bound": "fp64", "kernel": kernel + " (float64 batch)", "achieved": a64, "peak": p64, "unit": "TFLOP/s",
+            "frac": a64 / p64, "peak_kind": "measured FP64 FMA loop on this GPU (xcb_peak_fma)",
+            "algorithmic_flops_per_step": total,
+            "mixed": {"achieved": a32, "peak": p32, "frac": a32 / p32,
+                      "peak_kind": "measured FP32 FMA loop on this GPU (xcb_peak_fma)"}}
+
+
 def run_ba(args, dev, stream, rank, ws_world, cpu=True):
     """Batched mixed-precision window BA (256 uneven windows: K ~ U{5..20}, L ~ U{300..3000}, 2-12 observing
     keyframes per landmark, 1 px noise, 5 % outliers, 5 LM iterations) vs the plain per-window FP64 form, with the
@@ -566,6 +782,7 @@ def run_ba(args, dev, stream, rank, ws_world, cpu=True):
                                                 "mixed_median": float(np.median(errs_m)),
                                                 "fp64_max": float(np.max(errs_f))},
            "accepted_mean": float(np.mean(res_mixed["accepted"])),
+           "roofline": ba_roofline(wins, BA_ITERS, ms_fp64b, ms_mixed, "k_ba_windows"),
            "config": {"workload": "256 uneven windows, K~U{5..20}, L~U{300..3000}, 2-12 obs/landmark (geometric), "
                                   "stereo rows, 5% outliers, 5 LM iterations, keyframe 0 held",
                       "landmarks": n_land, "observation_rows": n_rows}}
@@ -618,6 +835,7 @@ def run_ba_large(args, dev, stream, ws_world, rank):
             "fp64_batched_value": ws_world * len(wins) / (res["fp64"][0] / 1e3),
             "ms_per_step": {"mixed_batched": res["mixed"][0], "fp64_batched": res["fp64"][0]},
             "pose_step_rel_err_vs_fp64_oracle": {"mixed_max": max(errs), "mixed_median": float(np.median(errs))},
+            "roofline": ba_roofline(wins, BA_ITERS, res["fp64"][0], res["mixed"][0], "k_ba_windows"),
             "config": {"workload": "32 windows x (20 keyframes, 6000 landmarks, 3-15 obs, 10% outliers), 5 LM "
                                    "iterations", "landmarks": int(sum(w.lmp.shape[0] for w in wins)),
                        "observation_rows": int(sum(w.ob_pose.shape[0] for w in wins))}}

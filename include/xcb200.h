@@ -34,6 +34,11 @@ extern "C" {
 
 const char* xcb_last_error(void);
 int xcb_version(void);
+/* The FP64 (fp64 = 1) or FP32 FMA peak of this device at its current clocks: one timed launch of 8 independent FMA
+   chains per thread, 8 blocks of 256 threads per SM, `iters` steps per chain (65536 takes ~10 ms in FP64).  No
+   reference counterpart: the compute rooflines of the window BA and of the stereo's LK are quoted against it.
+   tflops: FLOP/s / 1e12 (an FMA counts 2); ms (may be NULL): the launch's duration.  Synchronises the device. */
+int xcb_peak_fma(int fp64, int iters, double* tflops, float* ms);
 
 /* ===================================================== frontend ===================================================== */
 typedef struct xcb_front xcb_front;
@@ -223,6 +228,10 @@ typedef struct {
 #define XCB_BA_FP64 0           /* everything in float64: the plain form */
 #define XCB_BA_MIXED 1          /* FP32 linearisation + Schur, FP64 Cholesky, FP64 refinement (to 1e-9, <= 3 steps) */
 #define XCB_BA_LINEARISE 2      /* internal: one float64 linearisation, the reduced system exported (no step) */
+/* per-window status (stats [w][4] of the window solves, stats [w][3] of the Newton calls) when the scratch cannot
+   hold the batch's per-landmark records; the kernel counts the landmarks from the windows themselves (lm_off + L),
+   writes nothing else and leaves the state unchanged */
+#define XCB_BA_STATUS_SCRATCH (-3)
 
 /* Device scratch the batched solve needs for `Lt` landmarks: the work counter, the trial landmark states and, for the
    float64 mode, each landmark's back-substitution record (118 doubles: ~0.95 kB per landmark).  A smaller scratch
@@ -232,7 +241,7 @@ size_t xcb_ba_scratch_bytes(int nw, int Lt);
 /* window.solve (window.py:889-982, purely visual, fixed `iters` LM iterations from lam0) for every window of the batch
    in ONE persistent launch (no reference counterpart as one call; the reference solves one window per call on the
    CPU).  stats [nw][8] = cost0, cost, accepted, lam, status (0 ok, -1 window too large, -2 a landmark touches more
-   than 16 keyframes), iters, -, -;
+   than 16 keyframes, XCB_BA_STATUS_SCRATCH the scratch holds fewer than 3 doubles per landmark), iters, -, -;
    dx0 [nw][dx0_stride] (optional) = the first iteration's pose step.  grid = 0: one CTA per SM. */
 int xcb_ba_solve_windows_dev(const xcb_ba_windows* w, int max_slots, int iters, double lam0, int mode, double* stats,
                              double* dx0, int dx0_stride, void* scratch, size_t scratch_bytes, int grid, void* stream);
@@ -243,8 +252,13 @@ int xcb_ba_solve_windows_dev(const xcb_ba_windows* w, int max_slots, int iters, 
    outputs as for xcb_ba_solve_windows_dev but no scratch: the scratch is a static device array of
    XCB_BA_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until exit, which limits one call to
    xcb_ba_noalloc_max_landmarks() landmarks in total (`Lt`, the batch's landmark count; more -> XCB_ERR_CAPACITY).
-   The first call on a device looks up the array's device address (call it before any stream capture).  Calls share
-   the array: calls that overlap on the GPU race.  No cudaMalloc, cudaFree or allocating library call is made. */
+   The kernel also counts the landmarks from the windows (lm_off + L) and answers XCB_BA_STATUS_SCRATCH for every
+   window, writing nothing else, when they exceed the array whatever `Lt` said.  Up to 4,332 landmarks the array also
+   holds the float64 back-substitution records; above that the solve re-linearises the landmarks for the
+   back-substitution instead (the same results, slower).  The first call on a device looks up the array's device
+   address (call it before any stream capture); the address is kept for the life of the process, so it does not
+   survive cudaDeviceReset or a re-created primary context on that device.  Calls share the array: calls that
+   overlap on the GPU race.  No cudaMalloc, cudaFree or allocating library call is made. */
 #define XCB_BA_NOALLOC_SCRATCH_BYTES ((size_t)4 << 20)
 #define XCB_NOALLOC_MAX_DEVICES 64
 int xcb_ba_noalloc_max_landmarks(void);
@@ -261,7 +275,8 @@ int xcb_ba_solve_windows_noalloc(const xcb_ba_windows* w, int Lt, int max_slots,
    system until the relative residual is below `tol` (at most `maxit` iterations).  stats [nw][4] = iterations,
    final relative residual, final gradient max-norm (polish), status (0 ok, 1 Gauss-Newton system not positive
    definite, 2 non-positive curvature met: the state is not at a strict minimum, so no step is taken, -1 window too
-   large, -2 a landmark touches more than 16 keyframes). */
+   large, -2 a landmark touches more than 16 keyframes, XCB_BA_STATUS_SCRATCH the scratch holds fewer than 19
+   doubles per landmark after its first 256 bytes). */
 #define XCB_BA_NEWTON_POLISH 0
 #define XCB_BA_NEWTON_ADJOINT 1
 #define XCB_BA_NEWTON_POLISH_FIXED 2      /* as XCB_BA_NEWTON_POLISH, flagging no new constant landmarks */

@@ -150,4 +150,6 @@ def main(ref_src):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python %s <the reference's src directory>" % sys.argv[0])
+    main(sys.argv[1])

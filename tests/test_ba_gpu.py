@@ -70,3 +70,43 @@ def test_limits():
     w = S.make_window(0, K=21, L=50)
     with pytest.raises(ValueError):
         pack_windows([w])
+
+
+def test_short_scratch_is_refused_on_the_device():
+    """A scratch that cannot hold the batch's per-landmark records: the kernels count the landmarks from the windows,
+    write nothing past the scratch, leave the state unchanged and answer XCB_BA_STATUS_SCRATCH for every window."""
+    import ctypes
+
+    import torch
+    from xclean_b200 import _lib
+    from xclean_b200.backend.ba import BatchSolver, MAX_SLOTS
+    bs = BatchSolver(windows_small(3, seed=5), "cuda", hold=0)
+    Lt = int(bs.host["lmp"].shape[0])
+    buf = torch.full((256 + 8 * 3 * Lt + 4096,), 0xA5, dtype=torch.uint8, device="cuda")
+    short = 256 + 8 * 3 * (Lt - 1)                      # one landmark's trial state short
+    before = {k: bs.t[k].clone() for k in ("Rwb", "pwb", "lmp")}
+    bs.stats.zero_()
+    for mode in (_lib.XCB_BA_FP64, _lib.XCB_BA_MIXED):
+        rc = _lib.lib().xcb_ba_solve_windows_dev(ctypes.byref(bs.desc), bs.max_slots, 5, 1e-4, mode,
+                                                 bs.stats.data_ptr(), bs.dx0.data_ptr(), 6 * MAX_SLOTS,
+                                                 buf.data_ptr(), short, 0, None)
+        assert rc == _lib.XCB_OK
+        torch.cuda.synchronize()
+        assert (bs.stats[:, 4].cpu().numpy() == _lib.XCB_BA_STATUS_SCRATCH).all()
+        assert bool((buf[256:] == 0xA5).all()), "the kernel wrote into the scratch it refused"
+        for k, v in before.items():
+            assert torch.equal(bs.t[k], v), k
+    # the Newton kernel: 19 doubles per landmark
+    nst = torch.zeros((bs.nw, 4), dtype=torch.float64, device="cuda")
+    nbuf = torch.full((256 + 8 * 19 * Lt + 4096,), 0xA5, dtype=torch.uint8, device="cuda")
+    z = torch.zeros(1, dtype=torch.float64, device="cuda")
+    rc = _lib.lib().xcb_ba_newton_windows_dev(ctypes.byref(bs.desc), bs.max_slots, _lib.XCB_BA_NEWTON_POLISH, 2, 10,
+                                              1e-12, None, ctypes.c_void_p(z.data_ptr()), ctypes.c_void_p(z.data_ptr()),
+                                              ctypes.c_void_p(z.data_ptr()), ctypes.c_void_p(nst.data_ptr()),
+                                              ctypes.c_void_p(nbuf.data_ptr()), 256 + 8 * 19 * (Lt - 1), 0, None)
+    assert rc == _lib.XCB_OK
+    torch.cuda.synchronize()
+    assert (nst[:, 3].cpu().numpy() == _lib.XCB_BA_STATUS_SCRATCH).all()
+    assert bool((nbuf[256:] == 0xA5).all())
+    for k, v in before.items():
+        assert torch.equal(bs.t[k], v), k

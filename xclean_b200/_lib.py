@@ -35,6 +35,7 @@ class FrontBufs(ctypes.Structure):
 _SIGS = {
     "xcb_last_error": (ctypes.c_char_p, []),
     "xcb_version": (c_int, []),
+    "xcb_peak_fma": (c_int, [c_int, c_int, P, P]),
     "xcb_front_create": (c_int, [c_int, c_int, c_int, c_int, ctypes.POINTER(c_void_p)]),
     "xcb_front_destroy": (None, [P]),
     "xcb_front_last_error": (ctypes.c_char_p, [P]),
@@ -74,6 +75,7 @@ XCB_BA_MIXED = 1
 XCB_BA_NEWTON_POLISH = 0
 XCB_BA_NEWTON_ADJOINT = 1
 XCB_BA_NEWTON_POLISH_FIXED = 2
+XCB_BA_STATUS_SCRATCH = -3
 _SIGS.update({
     "xcb_ba_scratch_bytes": (c_size_t, [c_int, c_int]),
     "xcb_ba_solve_windows_dev": (c_int, [ctypes.POINTER(BaWindows), c_int, c_int, c_double, c_int, P, P, c_int, P,

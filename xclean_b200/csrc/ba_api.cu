@@ -27,6 +27,7 @@ extern "C" int xcb_ba_solve_windows_dev(const xcb_ba_windows* w, int max_slots, 
         return ba_fail(XCB_ERR_CAPACITY, "ba_solve_windows: max_slots out of range (1..20)");
     if (mode != XCB_BA_FP64 && mode != XCB_BA_MIXED) return ba_fail(XCB_ERR_ARG, "ba_solve_windows: bad mode");
     if (dx0 && dx0_stride < 6 * max_slots) return ba_fail(XCB_ERR_ARG, "ba_solve_windows: dx0 stride too small");
+    if (scratch_bytes < 256) return ba_fail(XCB_ERR_CAPACITY, "ba_solve_windows: scratch smaller than 256 bytes");
     cudaStream_t st = (cudaStream_t)stream;
     // scratch: [counter (256 B)][trial landmark states]
     int* counter = (int*)scratch;
@@ -55,6 +56,7 @@ extern "C" int xcb_ba_linearise_windows_dev(const xcb_ba_windows* w, int max_slo
         return ba_fail(XCB_ERR_CAPACITY, "ba_linearise_windows: max_slots out of range (1..20)");
     const long long nm = 6LL * max_slots;
     if (out_stride < nm * nm + nm) return ba_fail(XCB_ERR_ARG, "ba_linearise_windows: out stride too small");
+    if (scratch_bytes < 256) return ba_fail(XCB_ERR_CAPACITY, "ba_linearise_windows: scratch smaller than 256 bytes");
     cudaStream_t st = (cudaStream_t)stream;
     int* counter = (int*)scratch;
     double* trial = (double*)((char*)scratch + 256);
@@ -129,10 +131,10 @@ extern "C" int xcb_ba_newton_windows_dev(const xcb_ba_windows* w, int max_slots,
     if (mode == XCB_BA_NEWTON_ADJOINT && (!gpose || !gtheta)) return ba_fail(XCB_ERR_ARG, "ba_newton: adjoint outputs");
     if (steps < 0 || maxit < 1) return ba_fail(XCB_ERR_ARG, "ba_newton: steps / maxit");
     cudaStream_t st = (cudaStream_t)stream;
-    // scratch: [counter (256 B)][19 doubles per landmark]
+    // scratch: [counter (256 B)][19 doubles per landmark]; the kernel checks the batch's landmarks against its size
+    if (scratch_bytes < 256) return ba_fail(XCB_ERR_CAPACITY, "ba_newton: scratch smaller than 256 bytes");
     int* counter = (int*)scratch;
     double* lsc = (double*)((char*)scratch + 256);
-    (void)scratch_bytes;
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), st);
     if (e != cudaSuccess) return ba_fail(XCB_ERR_CUDA, cudaGetErrorString(e));
     if (grid <= 0) {
@@ -143,7 +145,7 @@ extern "C" int xcb_ba_newton_windows_dev(const xcb_ba_windows* w, int max_slots,
     }
     if (grid > w->nw) grid = w->nw;
     e = xcb_launch_ba_newton(*w, max_slots, mode, steps, maxit, tol, gpose, gtheta, gisig, gz, stats, lsc, counter,
-                             grid, st);
+                             grid, st, (scratch_bytes - 256) / sizeof(double));
     if (e != cudaSuccess) return ba_fail(XCB_ERR_CUDA, cudaGetErrorString(e));
     return XCB_OK;
 }

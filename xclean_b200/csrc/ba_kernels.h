@@ -18,4 +18,4 @@ cudaError_t xcb_launch_ba_windows(const XcbBaWindows& d, int max_slots, int iter
 size_t xcb_ba_newton_smem_bytes(int maxP);
 cudaError_t xcb_launch_ba_newton(const XcbBaWindows& d, int max_slots, int mode, int steps, int maxit, double tol,
                                  const double* gpose, double* gtheta, double* gisig, double* gz, double* stats,
-                                 double* lsc, int* counter, int grid, cudaStream_t st);
+                                 double* lsc, int* counter, int grid, cudaStream_t st, size_t lsc_doubles);

@@ -692,12 +692,11 @@ extern "C" int xcb_lba_solve(const xcb_lba_problem* p, int iters, double lam0, d
     const float fx = (float)p->fx, cx = (float)p->cx, cy = (float)p->cy, hk = (float)p->huber;
     const int n = P.n;
     const bool smem = n <= SOLVE_SMEM_MAX_N;
-    static bool attr = false;
-    if (!attr) {
-        const cudaError_t e = cudaFuncSetAttribute(k_lba_solve<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   (int)((size_t)SOLVE_SMEM_MAX_N * (SOLVE_SMEM_MAX_N + 1) / 2 * 8));
+    static XcbAttrOnce attr;
+    {
+        const cudaError_t e = xcb_smem_attr_once(attr, (const void*)k_lba_solve<true>,
+                                                 (int)((size_t)SOLVE_SMEM_MAX_N * (SOLVE_SMEM_MAX_N + 1) / 2 * 8));
         if (e != cudaSuccess) return fail(XCB_ERR_CUDA, std::string("lba_solve: ") + cudaGetErrorString(e));
-        attr = true;
     }
     const size_t solve_smem = smem ? (size_t)n * (n + 1) / 2 * 8 : 0;
     int dev = 0, sms = XCB_B200_SMS;

@@ -631,13 +631,10 @@ extern "C" int xcb_bk_chol_solve(float* H, const float* b, float* x, int n, int*
     if (nthreads > 1024) nthreads = 1024;
     if (n <= CHOL_SMEM_MAX_N) {
         const size_t sm = (size_t)n * n * sizeof(float);
-        static bool attr = false;
-        if (!attr) {
-            const cudaError_t e = cudaFuncSetAttribute(k_chol_solve<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                       (int)(CHOL_SMEM_MAX_N * CHOL_SMEM_MAX_N * sizeof(float)));
-            if (e != cudaSuccess) return fail(XCB_ERR_CUDA, std::string("chol_solve: ") + cudaGetErrorString(e));
-            attr = true;
-        }
+        static XcbAttrOnce attr;
+        const cudaError_t e = xcb_smem_attr_once(attr, (const void*)k_chol_solve<true>,
+                                                 (int)(CHOL_SMEM_MAX_N * CHOL_SMEM_MAX_N * sizeof(float)));
+        if (e != cudaSuccess) return fail(XCB_ERR_CUDA, std::string("chol_solve: ") + cudaGetErrorString(e));
         k_chol_solve<true><<<1, nthreads, sm, (cudaStream_t)stream>>>(H, b, x, n, status);
     } else {
         k_chol_solve<false><<<1, nthreads, 0, (cudaStream_t)stream>>>(H, b, x, n, status);

@@ -782,14 +782,23 @@ __global__ void __launch_bounds__(BA_THREADS, 1) k_ba_windows(XcbBaWindows d, in
     __shared__ BaShared sh;
     __shared__ double s_norm[2];
     __shared__ double* s_bsc;
-    // the back-substitution records follow the trial states when the scratch holds them (float64 mode)
+    __shared__ int s_short;
+    // the back-substitution records follow the trial states when the scratch holds them (float64 mode); the batch's
+    // landmark count is taken from the windows themselves, not from the caller
     if (threadIdx.x == 0) {
         long long Lt = 0;
         for (int w = 0; w < d.nw; ++w) Lt = max(Lt, (long long)d.lm_off[w] + d.L[w]);
         const size_t off = ((size_t)3 * Lt + 31) / 32 * 32;
+        s_short = (size_t)3 * Lt > trial_doubles;
         s_bsc = off + (size_t)Lt * BA_BSC <= trial_doubles ? lmp_trial + off : nullptr;
     }
     __syncthreads();
+    if (s_short) {
+        // the trial states do not fit the scratch: nothing is written but every window's status
+        if (blockIdx.x == 0)
+            for (int w = threadIdx.x; w < d.nw; w += blockDim.x) stats[8 * w + 4] = XCB_BA_STATUS_SCRATCH;
+        return;
+    }
     double* const bsc = s_bsc;
     const int tid = threadIdx.x;
     for (;;) {
@@ -1523,12 +1532,25 @@ __device__ double nt_gmax(BaShared& sh, NtShared& nt, const double* lsc)
 __global__ void __launch_bounds__(BA_THREADS, 1) k_ba_newton(XcbBaWindows d, int mode, int steps, int maxit,
                                                              double tol, const double* gpose, double* gtheta,
                                                              double* gisig, double* gz, double* stats, double* lsc,
-                                                             int* counter)
+                                                             int* counter, size_t lsc_doubles)
 {
     extern __shared__ __align__(16) unsigned char dsm[];
     __shared__ BaShared sh;
     __shared__ NtShared nt;
+    __shared__ int s_short;
     const int tid = threadIdx.x;
+    if (tid == 0) {
+        long long Lt = 0;
+        for (int w = 0; w < d.nw; ++w) Lt = max(Lt, (long long)d.lm_off[w] + d.L[w]);
+        s_short = (size_t)BA_LSC_STRIDE * Lt > lsc_doubles;
+    }
+    __syncthreads();
+    if (s_short) {
+        // the per-landmark records do not fit the scratch: nothing is written but every window's status
+        if (blockIdx.x == 0)
+            for (int w = tid; w < d.nw; w += blockDim.x) stats[4 * w + 3] = XCB_BA_STATUS_SCRATCH;
+        return;
+    }
     for (;;) {
         if (tid == 0) sh.win = atomicAdd(counter, 1);
         __syncthreads();
@@ -1712,17 +1734,14 @@ size_t xcb_ba_newton_smem_bytes(int maxP)
 
 cudaError_t xcb_launch_ba_newton(const XcbBaWindows& d, int max_slots, int mode, int steps, int maxit, double tol,
                                  const double* gpose, double* gtheta, double* gisig, double* gz, double* stats,
-                                 double* lsc, int* counter, int grid, cudaStream_t st)
+                                 double* lsc, int* counter, int grid, cudaStream_t st, size_t lsc_doubles)
 {
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k_ba_newton, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)xcb_ba_newton_smem_bytes(BA_MAXP));
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    static XcbAttrOnce attr;
+    cudaError_t e = xcb_smem_attr_once(attr, (const void*)k_ba_newton, (int)xcb_ba_newton_smem_bytes(BA_MAXP));
+    if (e != cudaSuccess) return e;
     k_ba_newton<<<grid, BA_THREADS, xcb_ba_newton_smem_bytes(max_slots), st>>>(d, mode, steps, maxit, tol, gpose,
-                                                                               gtheta, gisig, gz, stats, lsc, counter);
+                                                                               gtheta, gisig, gz, stats, lsc, counter,
+                                                                               lsc_doubles);
     return cudaGetLastError();
 }
 
@@ -1731,13 +1750,9 @@ cudaError_t xcb_launch_ba_windows(const XcbBaWindows& d, int max_slots, int iter
                                   int grid, cudaStream_t st, const double* frz, size_t trial_doubles)
 {
     size_t sm = xcb_ba_smem_bytes(max_slots);
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k_ba_windows, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)xcb_ba_smem_bytes(BA_MAXP));
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    static XcbAttrOnce attr;
+    cudaError_t e = xcb_smem_attr_once(attr, (const void*)k_ba_windows, (int)xcb_ba_smem_bytes(BA_MAXP));
+    if (e != cudaSuccess) return e;
     k_ba_windows<<<grid, BA_THREADS, sm, st>>>(d, iters, lam0, mode, stats, dx0, dx0_stride, lmp_trial, counter,
                                                frz, trial_doubles);
     return cudaGetLastError();

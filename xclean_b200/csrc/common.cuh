@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <mutex>
 #include "xcb200.h"
 
 typedef unsigned char u8;
@@ -34,3 +35,23 @@ __device__ __forceinline__ int xcb_key_x(u64 k) { return 0xFFFF - (int)(k & 0xFF
 __device__ __forceinline__ int xcb_key_y(u64 k) { return 0xFFFF - (int)((k >> 16) & 0xFFFFull); }
 
 #define XCB_CHECK_LAUNCH() (cudaGetLastError())
+
+// A kernel's dynamic shared-memory opt-in applies to the device that is current when it is set, so it is raised once
+// per device ordinal (one XcbAttrOnce per call site; thread-safe).  The first call on a device sets it: make that
+// call outside any stream capture.
+struct XcbAttrOnce {
+    std::mutex mu;
+    int bytes[XCB_NOALLOC_MAX_DEVICES] = {};
+};
+static inline cudaError_t xcb_smem_attr_once(XcbAttrOnce& s, const void* func, int bytes)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= XCB_NOALLOC_MAX_DEVICES) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(s.mu);
+    if (s.bytes[dev] >= bytes) return cudaSuccess;
+    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) s.bytes[dev] = bytes;
+    return e;
+}

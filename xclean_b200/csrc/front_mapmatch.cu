@@ -419,16 +419,12 @@ extern "C" int xcb_mm_create(int width, int height, int max_frames, int max_kp, 
     m->ncell = (int)(gw * gh);
     m->maxF = max_frames;
     // the shared-memory opt-in is per kernel, not per handle: raise it to the largest grid any handle has asked for
-    static int s_smem_set = 0;
+    static XcbAttrOnce s_attr_f, s_attr_d;
     const int smem = (m->ncell + 1) * (int)sizeof(int);
     int rc = XCB_OK;
-    if (smem > s_smem_set) {
-        if (cudaFuncSetAttribute(k_mm_grid<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess
-            || cudaFuncSetAttribute(k_mm_grid<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
-            rc = mm_fail(m, XCB_ERR_CUDA, "mm_create: shared-memory opt-in failed");
-        else
-            s_smem_set = smem;
-    }
+    if (xcb_smem_attr_once(s_attr_f, (const void*)k_mm_grid<float>, smem) != cudaSuccess
+        || xcb_smem_attr_once(s_attr_d, (const void*)k_mm_grid<double>, smem) != cudaSuccess)
+        rc = mm_fail(m, XCB_ERR_CUDA, "mm_create: shared-memory opt-in failed");
     if (!rc && cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking) != cudaSuccess)
         rc = mm_fail(m, XCB_ERR_CUDA, "mm_create: stream");
     if (!rc) rc = mm_alloc_scratch(m, max_kp, max_lm);
