@@ -64,6 +64,7 @@ def parse():
     ap.add_argument("--no-ba", action="store_true")
     ap.add_argument("--no-mm", action="store_true", help="skip the gated map matcher")
     ap.add_argument("--no-hd", action="store_true", help="skip the 64-frame 1280x720 frontend batch")
+    ap.add_argument("--no-percall", action="store_true", help="skip the per-call drop-in latencies")
     ap.add_argument("--ba-only", action="store_true",
                     help="run only the batched window BA part and print its JSON object (profiling)")
     ap.add_argument("--ba-windows", type=int, default=None, help="BA windows per step (default 256)")
@@ -376,6 +377,7 @@ def run_ours(args, ws, rank, local):
             recheck = recheck_frames(L, R, outs, gf.calib, gf.pattern, BUDGET, HALF, DLO, DHI)
     del L, R
     hd = None if (args.no_hd or ws > 1) else run_front_hd(args, dev, stream, rank, cpu=(rank == 0 and not args.no_cpu))
+    percall = None if (args.no_percall or ws > 1) else run_percall(args)
     ba = None if args.no_ba else run_ba(args, dev, stream, rank, ws, cpu=(rank == 0 and ws == 1 and not args.no_cpu))
     mm = None if (args.no_mm or outs is None) else run_mapmatch(args, dev, stream, ws, outs,
                                                                   cpu=(rank == 0 and ws == 1 and not args.no_cpu))
@@ -389,7 +391,7 @@ def run_ours(args, ws, rank, local):
                                "oracle/time_reference_cpu.py times its numba / cv2 modules where the source is", "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
             "gpu_launches": launches_per_step * args.steps,
             "kp_per_frame_last_batch": float(np.mean(counts)) if len(counts) else None,
-            "bitexact_vs_oracle_all_frames": recheck, "front_hd": hd, "ba": ba, "mapmatch": mm}
+            "bitexact_vs_oracle_all_frames": recheck, "front_hd": hd, "per_call": percall, "ba": ba, "mapmatch": mm}
     if rank == 0:
         print(json.dumps(line), flush=True)
     gf.close()
@@ -529,6 +531,62 @@ def run_front_hd(args, dev, stream, rank, cpu=True):
                                "single_thread_frames_per_s": 2 / dt1}
     gf.close()
     return res
+
+
+def run_percall(args):
+    """The drop-in path as the engine calls it, one frame per call from host arrays (752x480, budget 2,048): the
+    Detector call, disparities at band 0..5 (dy 0, and dy 0.25 at band 5, which takes the shifted float32 image), and
+    match_desc_gpu against the previous frame; p50 / p95 wall time per call, copies and the result read-back included.
+    The reference's only published figure for this path is its stereo call law on an RTX 5090 (budget.py:852-865):
+    (0.5213 + 0.000292 n + 0.000314 n band) ms x 1.281 at the 95th percentile."""
+    from xclean_b200 import synth
+    from xclean_b200.front import gpu_front as G
+
+    class Rig:
+        width, height = 752, 480
+
+    n_frames = 40
+    L, R = synth.sequence(synth.CAM_SMALL, n_frames, seed=5)
+    L, R = L.numpy(), R.numpy()
+    det = G.Detector(Rig(), cap=2048)
+    det.budget = 2048
+
+    def pct(ts):
+        return {"p50_ms": 1e3 * float(np.percentile(ts, 50)), "p95_ms": 1e3 * float(np.percentile(ts, 95))}
+
+    for f in range(3):                   # warm-up (first-call set-up, caches)
+        kp, desc = det(L[f])
+        G.disparities(L[f], R[f], kp.astype(np.float64), band=5)
+    t_det, t_st, t_m = [], {b: [] for b in range(6)}, []
+    t_dy = []
+    prev = None
+    npts = []
+    for f in range(n_frames):
+        t0 = time.perf_counter()
+        kp, desc = det(L[f])
+        t_det.append(time.perf_counter() - t0)
+        kpd = kp.astype(np.float64)
+        npts.append(len(kp))
+        for b in range(6):
+            t0 = time.perf_counter()
+            G.disparities(L[f], R[f], kpd, band=b)
+            t_st[b].append(time.perf_counter() - t0)
+        t0 = time.perf_counter()
+        G.disparities(L[f], R[f], kpd, dy=0.25, band=5)
+        t_dy.append(time.perf_counter() - t0)
+        if prev is not None:
+            t0 = time.perf_counter()
+            G.match_desc_gpu(det.gpu, {"descriptors": prev}, {"descriptors": desc})
+            t_m.append(time.perf_counter() - t0)
+        prev = desc
+    n = float(np.mean(npts))
+    law = {b: (0.5213 + 0.000292 * n + 0.000314 * n * b) * 1.281 for b in range(6)}
+    return {"api": "front.gpu_front: Detector(left), disparities(left, right, kp, band=b), match_desc_gpu; one call "
+                   "per frame from host arrays", "frames": n_frames, "points_per_call": n,
+            "detector": pct(t_det), "match_desc_gpu": pct(t_m),
+            "disparities": {"band%d" % b: pct(t_st[b]) for b in range(6)},
+            "disparities_dy0.25_band5": pct(t_dy),
+            "reference_rtx5090_stereo_law_p95_ms": {"band%d" % b: law[b] for b in range(6)}}
 
 
 MM_LANDMARKS = 1500     # window landmarks projected per frame (the 10-keyframe window's 1,500)

@@ -17,18 +17,42 @@
 
 #define LK_ITERS 6
 #define MAXD 128
-#define ST_WARPS 8       // warps (points) per block; 2 blocks of 256 threads per SM at up to 128 registers measured
-                          // fastest (16 warps: faster than 20 warps at 96 registers or 16 warps in 4-warp blocks)
+#define ST_GROUP 32      // points per warp: searched one after another by the whole warp, then one LK per lane
 #define BAND_MAX 16
+#define LK_MG 4          // LK block columns: d within LK_MG of the integer peak (a sample beyond reads the image)
+
+// warps per block: two blocks per SM at up to 128 registers (8 warps; 6 for the 11x11 window, whose LK blocks are
+// larger)
+static __host__ __device__ constexpr int st_warps(int half) { return half >= 5 ? 6 : 8; }
 
 static __host__ __device__ __forceinline__ int win_w(int half) { return ((MAXD + 2 * half) + 3) & ~3; }
 
-#define LK_TERMS 9      // the LK's sums except sum(1 * 1) = NPIX, which is exact
+// LK block of one point: the right-image rows its samples can touch (PW + 2 rows from vi + js - HALF - 1) and the
+// columns xr - HALF - LK_MG - 1 .. xr + HALF + LK_MG + 1 (u8 rows of lk_rs bytes), then the left image around the
+// keypoint ((PW + 2) x (PW + 2) from row vi - HALF - 1, column ui - HALF - 1; rows of lk_ls bytes) for the template.
+static __host__ __device__ __forceinline__ int lk_rw(int half) { return 2 * half + 1 + 2 * LK_MG + 2; }
+static __host__ __device__ __forceinline__ int lk_rs(int half) { return (lk_rw(half) + 3) & ~3; }
+static __host__ __device__ __forceinline__ int lk_ls(int half) { return (2 * half + 3 + 3) & ~3; }
+static __host__ __device__ __forceinline__ int lk_job_bytes(int half)
+{
+    int words = ((2 * half + 3) * (lk_rs(half) + lk_ls(half)) + 3) / 4;
+    if (!(words & 1)) ++words;       // odd word stride: lanes reading one offset of their own blocks hit distinct banks
+    return 4 * words;
+}
 
-// per-warp shared memory: Td [NPIX] f64 | T2d [NPIX] f64 | sc [MAXD] f64 | jb [MAXD] i8 | U, where U holds the image
-// window (float32 rows of win_w, or u8 rows of U8Win::WWB) during the two searches, then the LK term table
-// (LK_TERMS rows of NPIX f64, rows NPIXP = NPIX rounded up to even apart) and the LK's staged right-image block
-// ((PW + 2) x (PW + 10) f64)
+// a point that passed the searches, waiting for its LK
+struct StJob {
+    double u, v, seed, ts;
+    long long oi;
+    int ui, vi, xr, js, f, pad_;
+};
+
+// per-warp shared memory: jobs [ST_GROUP] | U.  U holds, while a point is searched: Td [NPIX] f64 | T2d [NPIX] f64 |
+// sc [MAXD] f64 | jb [MAXD] i8 | the image window (float32 rows of win_w, or u8 rows of U8Win::WWB); during the LKs:
+// the group's LK blocks (ST_GROUP x lk_job_bytes); during the vertical scans: Td [NPIX] f64 | the scan block
+// ((2 PW - 1) x PW float32).
+static __host__ __device__ __forceinline__ size_t st_jobs_bytes() { return (ST_GROUP * sizeof(StJob) + 15) & ~(size_t)15; }
+
 static __host__ __device__ __forceinline__ size_t stereo_off_u(int half)
 {
     int pw = 2 * half + 1, npix = pw * pw;
@@ -38,9 +62,12 @@ static __host__ __device__ __forceinline__ size_t stereo_off_u(int half)
 static __host__ __device__ __forceinline__ size_t stereo_warp_bytes(int half, int band)
 {
     int pw = 2 * half + 1, npix = pw * pw;
-    size_t win = (size_t)(pw + 2 * band) * win_w(half) * 4;
-    size_t terms = (size_t)LK_TERMS * ((npix + 1) & ~1) * 8 + (size_t)(pw + 2) * (pw + 2 * 4 + 2) * 8;   // + LK block
-    return (stereo_off_u(half) + (win > terms ? win : terms) + 15) & ~(size_t)15;
+    size_t search = stereo_off_u(half) + (size_t)(pw + 2 * band) * win_w(half) * 4;
+    size_t lk = (size_t)ST_GROUP * lk_job_bytes(half);
+    size_t vert = (size_t)npix * 8 + (size_t)(2 * pw - 1) * pw * 4;
+    size_t u = search > lk ? search : lk;
+    if (vert > u) u = vert;
+    return (st_jobs_bytes() + u + 15) & ~(size_t)15;
 }
 
 size_t xcb_stereo_smem_per_warp(int half, int band) { return stereo_warp_bytes(half, band); }
@@ -399,373 +426,431 @@ __device__ __forceinline__ void warp_argmax(double& v, int& idx)
 }
 
 // ---------------------------------------------------------------- the stereo kernel
+// u8 -> float64 on the FP64 pipe: 2^52 + b carries b in its low mantissa bits, so the subtraction is exact
+__device__ __forceinline__ double u8d(unsigned b)
+{
+    return __dsub_rn(__hiloint2double(0x43300000, (int)b), 4503599627370496.0);
+}
+
+// One warp per group of ST_GROUP points.  Phase A: the whole warp takes the group's points one after another through
+// the template statistics, the ZNCC search over the row band, the uniqueness test and the left-right check (lanes
+// split the disparities); each point that passes becomes an LK job.  Phase B: the warp stages every job's right- and
+// left-image neighbourhood, then each lane runs one job's affine LK (LK_ITERS steps and the covariance pass) with its
+// ten sums in the CPU's sequential order and its own 3x3 OpenBLAS solve: the serial float64 chains of 32 points run side
+// by side instead of one point's chains idling 31 lanes.  Phase C: the whole warp takes each accepted job through the
+// vertical scan.
 template <int HALF, bool FLT>
-__global__ void __launch_bounds__(ST_WARPS * 32, 2) k_stereo(
+__global__ void __launch_bounds__(st_warps(HALF) * 32, 2) k_stereo(
     const u8* __restrict__ Lall, const u8* __restrict__ R8all, const float* __restrict__ Rsall, int H, int W,
     const double* __restrict__ kpd, const long long* __restrict__ dlo_a, const long long* __restrict__ dhi_a, int n,
     const float* __restrict__ kpf, const int* __restrict__ counts, int cap, int dlo_s, int dhi_s, int band,
     double* __restrict__ od, double* __restrict__ osig, u8* __restrict__ ook, double* __restrict__ ozn,
     double* __restrict__ ody)
 {
-    constexpr int PW = 2 * HALF + 1, NPIX = PW * PW, NPIXP = (NPIX + 1) & ~1;
+    constexpr int PW = 2 * HALF + 1, NPIX = PW * PW, NW = st_warps(HALF);
+    constexpr int LKR = PW + 2, LKW = PW + 2 * LK_MG + 2;
     static_assert(U8Win<HALF>::WWB <= 4 * (((MAXD + 2 * HALF) + 3) & ~3), "u8 rows fit the float32 window rows");
+    static_assert(sizeof(StJob) == 64, "job record");
+    const int RS = lk_rs(HALF), LS = lk_ls(HALF), JB = lk_job_bytes(HALF);
     const double ZMIN = 0.5, UNIQ1 = 1.0 + 0.05, LRT = 1.0;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int ww = win_w(HALF);
     unsigned char* base = smem_raw + (size_t)wid * stereo_warp_bytes(HALF, band);
-    double* Td = (double*)base;
+    StJob* jobs = (StJob*)base;
+    unsigned char* U = base + st_jobs_bytes();
+    double* Td = (double*)U;
     double* T2d = Td + NPIX;
     double* sc = T2d + NPIX;
     signed char* jb = (signed char*)(sc + MAXD);
-    float* win = (float*)(base + stereo_off_u(HALF));
-    unsigned char* winb = base + stereo_off_u(HALF);          // the u8 windows (U8Win row stride)
-    double* terms = (double*)(base + stereo_off_u(HALF));     // the LK term table, after the searches
+    float* win = (float*)(U + stereo_off_u(HALF));
+    unsigned char* winb = U + stereo_off_u(HALF);          // the u8 windows (U8Win row stride)
+    constexpr int KP = (NPIX + 31) / 32;                   // patch pixels per lane
 
-    const long long p = (long long)blockIdx.x * ST_WARPS + wid;
-    int f = 0;
-    size_t oi;
-    double u, v;
-    long long lo, hi;
-    if (kpd) {
-        if (p >= n) return;
-        oi = (size_t)p;
-        u = kpd[2 * p]; v = kpd[2 * p + 1];
-        lo = dlo_a[p]; hi = dhi_a[p];
-    } else {
-        f = (int)(p / cap);
-        int i = (int)(p % cap);
-        if (f >= n || i >= counts[f]) return;
-        oi = (size_t)f * cap + i;
-        u = (double)kpf[2 * oi]; v = (double)kpf[2 * oi + 1];
-        lo = dlo_s; hi = dhi_s;
-    }
-    const u8* L = Lall + (size_t)f * H * W;
-    RightImg<FLT> R;
-    R.r8 = R8all ? R8all + (size_t)f * H * W : nullptr;
-    R.rf = Rsall ? Rsall + (size_t)f * H * W : nullptr;
-    if (lane == 0) { ook[oi] = 0; od[oi] = 0.0; osig[oi] = XCB_INF; ozn[oi] = -2.0; ody[oi] = XCB_NAN; }
-
-    const int ui = (int)floor(__dadd_rn(u, 0.5)), vi = (int)floor(__dadd_rn(v, 0.5));
-    if (ui - HALF - 2 < 0 || ui + HALF + 2 >= W || vi - HALF - 2 - band < 0 || vi + HALF + 2 + band >= H) return;
-    if (lo < 0) lo = 0;
-    if (hi > MAXD - 1) hi = MAXD - 1;
-    if (hi > ui - HALF - 2) hi = ui - HALF - 2;
-    if (hi < lo) return;
-
-    // template statistics (_patch_stats on u8: integer sums, exact) and T - mean
-    constexpr int KP = (NPIX + 31) / 32;      // patch pixels per lane
-    int tv[KP];
-#pragma unroll
-    for (int i = 0; i < KP; ++i) {
-        const int k = lane + 32 * i;
-        tv[i] = k < NPIX ? (int)L[(size_t)(vi + k / PW - HALF) * W + ui + k % PW - HALF] : 0;
-    }
-    int s = 0, s2 = 0;
-#pragma unroll
-    for (int i = 0; i < KP; ++i) { s += tv[i]; s2 += tv[i] * tv[i]; }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) { s += __shfl_xor_sync(0xffffffffu, s, o); s2 += __shfl_xor_sync(0xffffffffu, s2, o); }
-    const double tm = __ddiv_rn((double)s, (double)NPIX);
-    const double tvar = __dsub_rn(__ddiv_rn((double)s2, (double)NPIX), __dmul_rn(tm, tm));
-    const double ts = __dsqrt_rn(tvar > 0.0 ? tvar : 0.0);
-    if (ts <= 1e-6) return;
-#pragma unroll
-    for (int i = 0; i < KP; ++i)
-        if (lane + 32 * i < NPIX) Td[lane + 32 * i] = __dsub_rn((double)tv[i], tm);
-
-    // right-image window: rows vi-band-HALF .. vi+band+HALF, columns ui-hi-HALF .. ui-lo+HALF (window column = hi - d)
-    const int wr0 = vi - band - HALF, wc0 = ui - (int)hi - HALF;
-    const int nrows = PW + 2 * band, span = (int)(hi - lo), ncols = span + PW;
-    double lbest = -2.0;
-    int lbd = -1;
-    double best[4];
-    int bj[4] = {0, 0, 0, 0}, dq[4];
-    bool val[4];
-    if (FLT) {
-        // shifted float32 right image: disparities lo + lane + 32 q
-        for (int idx = lane; idx < nrows * ncols; idx += 32) {
-            int rr = idx / ncols, cc = idx % ncols;
-            win[rr * ww + cc] = R.at((size_t)(wr0 + rr) * W + wc0 + cc);
-        }
-        __syncwarp();
-        int col[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            dq[q] = (int)lo + lane + 32 * q;
-            val[q] = dq[q] <= hi;
-            col[q] = (int)hi - dq[q];
-        }
-        // rows in the CPU's order: vi, then vi - j, vi + j for j = 1..band; a later row wins only if strictly better
+    // ------------------------------------------------------------------------------------------- phase A: searches
+    const long long g0 = ((long long)blockIdx.x * NW + wid) * ST_GROUP;
+    int njobs = 0;
 #pragma unroll 1
-        for (int t = 0; t <= 2 * band; ++t) {
-            const int j = t == 0 ? 0 : ((t & 1) ? -((t + 1) >> 1) : (t >> 1));
-            double z[4];
-            zncc_q<HALF, FLT, 4>(win, ww, band + j, col, val, Td, ts, z);
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-                if (t == 0 || z[q] > best[q]) { best[q] = z[q]; bj[q] = j; }
+    for (int gi = 0; gi < ST_GROUP; ++gi) {
+        const long long p = g0 + gi;
+        int f = 0;
+        size_t oi;
+        double u, v;
+        long long lo, hi;
+        if (kpd) {
+            if (p >= n) break;
+            oi = (size_t)p;
+            u = kpd[2 * p]; v = kpd[2 * p + 1];
+            lo = dlo_a[p]; hi = dhi_a[p];
+        } else {
+            f = (int)(p / cap);
+            const int i = (int)(p % cap);
+            if (f >= n) break;
+            if (i >= counts[f]) continue;
+            oi = (size_t)f * cap + i;
+            u = (double)kpf[2 * oi]; v = (double)kpf[2 * oi + 1];
+            lo = dlo_s; hi = dhi_s;
         }
-    } else {
-        // u8 right image: lane's disparities lo + 4 lane + q (q = 0..3) are window columns span - 4 lane - q, a block of
-        // four adjacent patches starting at column cb = span - 4 lane - 3.  The pad makes every block start on a 32-bit
-        // word; a lane whose four disparities all exceed hi starts at the lowest column >= -3 of the same residue
-        // mod 4 (pad bytes, results unused).
-        const int pad = 4 + ((3 - span) & 3);
-        stage_u8<HALF>(winb, R.r8, W, wr0, nrows, wc0, ncols, pad, lane);
-        __syncwarp();
-        int cb = span - 4 * lane - 3;
-        if (cb < -3) cb += (-cb) & ~3;
-        const unsigned char* pb = winb + pad + cb;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            dq[q] = (int)lo + 4 * lane + q;
-            val[q] = dq[q] <= hi;
-        }
-#pragma unroll 1
-        for (int t = 0; t <= 2 * band; ++t) {
-            const int j = t == 0 ? 0 : ((t & 1) ? -((t + 1) >> 1) : (t >> 1));
-            double z[4];
-            zncc4_u8<HALF>(pb + (band + j) * U8Win<HALF>::WWB, Td, ts, z);
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-                if (t == 0 || z[3 - q] > best[q]) { best[q] = z[3 - q]; bj[q] = j; }
-        }
-    }
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        if (val[q]) {
-            sc[dq[q]] = best[q];
-            jb[dq[q]] = (signed char)bj[q];
-            if (best[q] > lbest) { lbest = best[q]; lbd = dq[q]; }
-        }
-    }
-    double bs = lbest;
-    int bestd = lbd;
-    warp_argmax(bs, bestd);
-    if (lane == 0) ozn[oi] = bs;
-    if (bestd < 0 || bs < ZMIN) return;
-    __syncwarp();
-    double sec = -2.0;
-    for (int d = (int)lo + lane; d <= hi; d += 32)
-        if (abs(d - bestd) > 1 && sc[d] > sec) sec = sc[d];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) sec = fmax(sec, __shfl_xor_sync(0xffffffffu, sec, o));
-    if (!(__dsub_rn(1.0, sec) > __dmul_rn(__dsub_rn(1.0, bs), UNIQ1))) return;
+        __syncwarp();                                      // the previous point's shared memory is free
+        const u8* L = Lall + (size_t)f * H * W;
+        RightImg<FLT> R;
+        R.r8 = R8all ? R8all + (size_t)f * H * W : nullptr;
+        R.rf = Rsall ? Rsall + (size_t)f * H * W : nullptr;
+        if (lane == 0) { ook[oi] = 0; od[oi] = 0.0; osig[oi] = XCB_INF; ozn[oi] = -2.0; ody[oi] = XCB_NAN; }
 
-    // left-right check: the right patch at the peak searched back along the left row
-    const int js = jb[bestd];
-    const int xr = ui - bestd;
-    double rm, rsd;
-    float rv[KP];
-#pragma unroll
-    for (int i = 0; i < KP; ++i) {
-        const int k = lane + 32 * i;
-        rv[i] = k < NPIX ? R.at((size_t)(vi + js + k / PW - HALF) * W + xr + k % PW - HALF) : 0.f;
-    }
-    if (FLT) {
-        // float32 patch: the CPU's sequential float64 sums (x * x a float32 product)
-        double a = 0.0, a2 = 0.0;
-        if (lane == 0)
-            for (int k = 0; k < NPIX; ++k) {
-                float x = R.at((size_t)(vi + js + k / PW - HALF) * W + xr + k % PW - HALF);
-                a = __dadd_rn(a, (double)x);
-                a2 = __dadd_rn(a2, (double)__fmul_rn(x, x));
-            }
-        a = __shfl_sync(0xffffffffu, a, 0);
-        a2 = __shfl_sync(0xffffffffu, a2, 0);
-        rm = __ddiv_rn(a, (double)NPIX);
-        double var = __dsub_rn(__ddiv_rn(a2, (double)NPIX), __dmul_rn(rm, rm));
-        rsd = __dsqrt_rn(var > 0.0 ? var : 0.0);
-    } else {
-        int a = 0, a2 = 0;
-#pragma unroll
-        for (int i = 0; i < KP; ++i) { const int x = (int)rv[i]; a += x; a2 += x * x; }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) { a += __shfl_xor_sync(0xffffffffu, a, o); a2 += __shfl_xor_sync(0xffffffffu, a2, o); }
-        rm = __ddiv_rn((double)a, (double)NPIX);
-        double var = __dsub_rn(__ddiv_rn((double)a2, (double)NPIX), __dmul_rn(rm, rm));
-        rsd = __dsqrt_rn(var > 0.0 ? var : 0.0);
-    }
-    if (rsd <= 1e-6) return;
-#pragma unroll
-    for (int i = 0; i < KP; ++i)
-        if (lane + 32 * i < NPIX) T2d[lane + 32 * i] = __dsub_rn((double)rv[i], rm);
-    int dmax = MAXD - 1;
-    if (xr + dmax + HALF >= W) dmax = W - 1 - HALF - xr;
-    const int lc0 = xr - HALF, lcols = dmax + PW;
-    __syncwarp();
-    // left-image window, candidate c at column c: lane scores c = 4 lane .. 4 lane + 3 (pad 4: word-aligned blocks)
-    stage_u8<HALF>(winb, L, W, vi - HALF, PW, lc0, lcols, 4, lane);
-    __syncwarp();
-    double lrb = -2.0;
-    int lrd = -1;
-    {
-        double z[4];
-        zncc4_u8<HALF>(winb + 4 + 4 * lane, T2d, rsd, z);
-#pragma unroll
-        for (int k = 0; k < 4; ++k)
-            if (4 * lane + k <= dmax && z[k] > lrb) { lrb = z[k]; lrd = 4 * lane + k; }
-    }
-    warp_argmax(lrb, lrd);
-    if (lrd < 0 || fabs((double)(lrd - bestd)) > LRT) return;
+        const int ui = (int)floor(__dadd_rn(u, 0.5)), vi = (int)floor(__dadd_rn(v, 0.5));
+        if (ui - HALF - 2 < 0 || ui + HALF + 2 >= W || vi - HALF - 2 - band < 0 || vi + HALF + 2 + band >= H) continue;
+        if (lo < 0) lo = 0;
+        if (hi > MAXD - 1) hi = MAXD - 1;
+        if (hi > ui - HALF - 2) hi = ui - HALF - 2;
+        if (hi < lo) continue;
 
-    // parabola seed, then the affine LK from the sub-pixel keypoint position
-    double off = 0.0;
-    if (bestd > lo && bestd < hi) {
-        double y0 = sc[bestd - 1], y2 = sc[bestd + 1];
-        double den = __dadd_rn(__dsub_rn(y0, __dmul_rn(2.0, bs)), y2);
-        if (den < -1e-9) {
-            off = __ddiv_rn(__dmul_rn(0.5, __dsub_rn(y0, y2)), den);
-            if (off > 0.5) off = 0.5;
-            if (off < -0.5) off = -0.5;
-        }
-    }
-    const double seed = __dadd_rn(__dadd_rn((double)bestd, off), __dsub_rn(u, (double)ui));
-    const double voff = (double)js;
-    double* Tl = T2d;     // the LK template (bilinear left samples) reuses T2d
-    __syncwarp();
-    LeftImg Li;
-    Li.p = L;
-    for (int k = lane; k < NPIX; k += 32) {
-        double g_;
-        bil(Li, H, W, __dadd_rn(u, (double)(k % PW - HALF)), __dadd_rn(v, (double)(k / PW - HALF)), &Tl[k], &g_);
-    }
-    __syncwarp();
-    // the LK's right-image samples: x = u + dx - d moves with d, y = v + dy + voff does not (its row and weight are
-    // fixed).  u8 right image: the rows the samples can touch and the columns of d within LK_MG of the integer peak are
-    // staged once as float64 after the term table; a sample outside them (a diverging LK) reads the image.
-    constexpr int LK_MG = 4, LKW = PW + 2 * LK_MG + 2, LKR = PW + 2;
-    double* lks = terms + LK_TERMS * NPIXP;
-    const int xs0 = xr - HALF - LK_MG - 1, ys0 = vi + js - HALF - 1;
-    const int xa = xs0 > 0 ? xs0 : 0, xb = xs0 + LKW - 1 < W - 1 ? xs0 + LKW - 1 : W - 1;
-    double lpx[KP], lay[KP];
-    int lyr[KP];
-#pragma unroll
-    for (int i = 0; i < KP; ++i) {
-        const int k = lane + 32 * i < NPIX ? lane + 32 * i : NPIX - 1;
-        lpx[i] = __dadd_rn(u, (double)(k % PW - HALF));
-        const double y = __dadd_rn(__dadd_rn(v, (double)(k / PW - HALF)), voff);
-        int y0 = (int)floor(y);
-        lay[i] = __dsub_rn(y, (double)y0);
-        if (y0 < 0) y0 = 0;
-        if (y0 > H - 2) y0 = H - 2;
-        lyr[i] = y0;
-    }
-    if (!FLT) {
-#pragma unroll
-        for (int i = 0; i < (LKR * LKW + 31) / 32; ++i) {
-            const int idx = lane + 32 * i;
-            if (idx < LKR * LKW) {
-                const int rr = idx / LKW, col = xs0 + idx - rr * LKW;
-                lks[idx] = (col >= 0 && col < W) ? (double)R.r8[(size_t)(ys0 + rr) * W + col] : 0.0;
-            }
-        }
-    }
-    __syncwarp();
-    double d = seed, a = 1.0, b = 0.0;
-    bool okk = false;
-    double sig = 0.0;
-    for (int it = 0; it <= LK_ITERS; ++it) {
-        // every patch pixel's residual and Jacobian terms, all lanes in parallel (terms[t][k]); then lane t sums term
-        // t over k = 0..NPIX-1 in the CPU's order.  Table rows: J0 r, J1 r, r, J0 J0, J0 J1, J0, J1 J1, J1, r r.
+        // template statistics (_patch_stats on u8: integer sums, exact) and T - mean
+        int tv[KP];
 #pragma unroll
         for (int i = 0; i < KP; ++i) {
             const int k = lane + 32 * i;
-            if (k >= NPIX) break;
-            double rv, rg;
-            if (FLT) {
-                double px = __dadd_rn(u, (double)(k % PW - HALF)), py = __dadd_rn(v, (double)(k / PW - HALF));
-                bil(R, H, W, __dsub_rn(px, d), __dadd_rn(py, voff), &rv, &rg);
-            } else {
-                // bil() on u8 values held as float64 (their float32 differences are exact, so are these)
-                const double x = __dsub_rn(lpx[i], d);
-                int x0 = (int)floor(x);
-                const double ax = __dsub_rn(x, (double)x0);
-                if (x0 < 0) x0 = 0;
-                if (x0 > W - 2) x0 = W - 2;
-                const int y0 = lyr[i];
-                double fa, fb, fc, fd;
-                if (x0 >= xa && x0 + 1 <= xb && y0 >= ys0 && y0 + 1 < ys0 + LKR) {
-                    const double* sp = lks + (y0 - ys0) * LKW + (x0 - xs0);
-                    fa = sp[0]; fb = sp[1]; fc = sp[LKW]; fd = sp[LKW + 1];
-                } else {
-                    const u8* gp = R.r8 + (size_t)y0 * W + x0;
-                    fa = (double)gp[0]; fb = (double)gp[1]; fc = (double)gp[W]; fd = (double)gp[W + 1];
-                }
-                const double ay = lay[i];
-                const double ba = __dsub_rn(fb, fa), dc = __dsub_rn(fd, fc);
-                const double top = __dadd_rn(fa, __dmul_rn(ax, ba));
-                const double bot = __dadd_rn(fc, __dmul_rn(ax, dc));
-                rv = __dadd_rn(top, __dmul_rn(ay, __dsub_rn(bot, top)));
-                rg = __dadd_rn(__dmul_rn(ba, __dsub_rn(1.0, ay)), __dmul_rn(dc, ay));
-            }
-            double r = __dsub_rn(Tl[k], __dadd_rn(__dmul_rn(a, rv), b));
-            double J0 = __dmul_rn(-a, rg), J1 = rv;
-            terms[0 * NPIXP + k] = __dmul_rn(J0, r);
-            terms[1 * NPIXP + k] = __dmul_rn(J1, r);
-            terms[2 * NPIXP + k] = r;
-            terms[3 * NPIXP + k] = __dmul_rn(J0, J0);
-            terms[4 * NPIXP + k] = __dmul_rn(J0, J1);
-            terms[5 * NPIXP + k] = J0;
-            terms[6 * NPIXP + k] = __dmul_rn(J1, J1);
-            terms[7 * NPIXP + k] = J1;
-            terms[8 * NPIXP + k] = __dmul_rn(r, r);
+            tv[i] = k < NPIX ? (int)L[(size_t)(vi + k / PW - HALF) * W + ui + k % PW - HALF] : 0;
         }
-        __syncwarp();
-        double S = 0.0;
-        if (lane < LK_TERMS && (lane < 8 || it == LK_ITERS)) {
-            const double2* tr = (const double2*)(terms + lane * NPIXP);     // rows are 16-byte aligned
-#pragma unroll 8
-            for (int k2 = 0; k2 < NPIX / 2; ++k2) {
-                const double2 t2 = tr[k2];
-                S = __dadd_rn(__dadd_rn(S, t2.x), t2.y);
-            }
-            if (NPIX & 1) S = __dadd_rn(S, terms[lane * NPIXP + NPIX - 1]);
-        }
-        __syncwarp();
-        double Sv[10];
+        int s = 0, s2 = 0;
 #pragma unroll
-        for (int q = 0; q < 8; ++q) Sv[q] = __shfl_sync(0xffffffffu, S, q);
-        Sv[9] = __shfl_sync(0xffffffffu, S, 8);
-        Sv[8] = (double)NPIX;      // sum of 1 x 1 over the patch: exact
-        int go = 1;
+        for (int i = 0; i < KP; ++i) { s += tv[i]; s2 += tv[i] * tv[i]; }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) { s += __shfl_xor_sync(0xffffffffu, s, o); s2 += __shfl_xor_sync(0xffffffffu, s2, o); }
+        const double tm = __ddiv_rn((double)s, (double)NPIX);
+        const double tvar = __dsub_rn(__ddiv_rn((double)s2, (double)NPIX), __dmul_rn(tm, tm));
+        const double ts = __dsqrt_rn(tvar > 0.0 ? tvar : 0.0);
+        if (ts <= 1e-6) continue;
+#pragma unroll
+        for (int i = 0; i < KP; ++i)
+            if (lane + 32 * i < NPIX) Td[lane + 32 * i] = __dsub_rn((double)tv[i], tm);
+
+        // right-image window: rows vi-band-HALF .. vi+band+HALF, columns ui-hi-HALF .. ui-lo+HALF (window column =
+        // hi - d)
+        const int wr0 = vi - band - HALF, wc0 = ui - (int)hi - HALF;
+        const int nrows = PW + 2 * band, span = (int)(hi - lo), ncols = span + PW;
+        double lbest = -2.0;
+        int lbd = -1;
+        double best[4];
+        int bj[4] = {0, 0, 0, 0}, dq[4];
+        bool val[4];
+        if (FLT) {
+            // shifted float32 right image: disparities lo + lane + 32 q
+            for (int idx = lane; idx < nrows * ncols; idx += 32) {
+                int rr = idx / ncols, cc = idx % ncols;
+                win[rr * ww + cc] = R.at((size_t)(wr0 + rr) * W + wc0 + cc);
+            }
+            __syncwarp();
+            int col[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                dq[q] = (int)lo + lane + 32 * q;
+                val[q] = dq[q] <= hi;
+                col[q] = (int)hi - dq[q];
+            }
+            // rows in the CPU's order: vi, then vi - j, vi + j for j = 1..band; a later row wins only if strictly better
+#pragma unroll 1
+            for (int t = 0; t <= 2 * band; ++t) {
+                const int j = t == 0 ? 0 : ((t & 1) ? -((t + 1) >> 1) : (t >> 1));
+                double z[4];
+                zncc_q<HALF, FLT, 4>(win, ww, band + j, col, val, Td, ts, z);
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    if (t == 0 || z[q] > best[q]) { best[q] = z[q]; bj[q] = j; }
+            }
+        } else {
+            // u8 right image: lane's disparities lo + 4 lane + q (q = 0..3) are window columns span - 4 lane - q, a
+            // block of four adjacent patches starting at column cb = span - 4 lane - 3.  The pad makes every block start
+            // on a 32-bit word; a lane whose four disparities all exceed hi starts at the lowest column >= -3 of the
+            // same residue mod 4 (pad bytes, results unused).
+            const int pad = 4 + ((3 - span) & 3);
+            stage_u8<HALF>(winb, R.r8, W, wr0, nrows, wc0, ncols, pad, lane);
+            __syncwarp();
+            int cb = span - 4 * lane - 3;
+            if (cb < -3) cb += (-cb) & ~3;
+            const unsigned char* pb = winb + pad + cb;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                dq[q] = (int)lo + 4 * lane + q;
+                val[q] = dq[q] <= hi;
+            }
+#pragma unroll 1
+            for (int t = 0; t <= 2 * band; ++t) {
+                const int j = t == 0 ? 0 : ((t & 1) ? -((t + 1) >> 1) : (t >> 1));
+                double z[4];
+                zncc4_u8<HALF>(pb + (band + j) * U8Win<HALF>::WWB, Td, ts, z);
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    if (t == 0 || z[3 - q] > best[q]) { best[q] = z[3 - q]; bj[q] = j; }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (val[q]) {
+                sc[dq[q]] = best[q];
+                jb[dq[q]] = (signed char)bj[q];
+                if (best[q] > lbest) { lbest = best[q]; lbd = dq[q]; }
+            }
+        }
+        double bs = lbest;
+        int bestd = lbd;
+        warp_argmax(bs, bestd);
+        if (lane == 0) ozn[oi] = bs;
+        if (bestd < 0 || bs < ZMIN) continue;
+        __syncwarp();
+        double sec = -2.0;
+        for (int d = (int)lo + lane; d <= hi; d += 32)
+            if (abs(d - bestd) > 1 && sc[d] > sec) sec = sc[d];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sec = fmax(sec, __shfl_xor_sync(0xffffffffu, sec, o));
+        if (!(__dsub_rn(1.0, sec) > __dmul_rn(__dsub_rn(1.0, bs), UNIQ1))) continue;
+
+        // left-right check: the right patch at the peak searched back along the left row
+        const int js = jb[bestd];
+        const int xr = ui - bestd;
+        double rm, rsd;
+        float rv[KP];
+#pragma unroll
+        for (int i = 0; i < KP; ++i) {
+            const int k = lane + 32 * i;
+            rv[i] = k < NPIX ? R.at((size_t)(vi + js + k / PW - HALF) * W + xr + k % PW - HALF) : 0.f;
+        }
+        if (FLT) {
+            // float32 patch: the CPU's sequential float64 sums (x * x a float32 product)
+            double a = 0.0, a2 = 0.0;
+            if (lane == 0)
+                for (int k = 0; k < NPIX; ++k) {
+                    float x = R.at((size_t)(vi + js + k / PW - HALF) * W + xr + k % PW - HALF);
+                    a = __dadd_rn(a, (double)x);
+                    a2 = __dadd_rn(a2, (double)__fmul_rn(x, x));
+                }
+            a = __shfl_sync(0xffffffffu, a, 0);
+            a2 = __shfl_sync(0xffffffffu, a2, 0);
+            rm = __ddiv_rn(a, (double)NPIX);
+            double var = __dsub_rn(__ddiv_rn(a2, (double)NPIX), __dmul_rn(rm, rm));
+            rsd = __dsqrt_rn(var > 0.0 ? var : 0.0);
+        } else {
+            int a = 0, a2 = 0;
+#pragma unroll
+            for (int i = 0; i < KP; ++i) { const int x = (int)rv[i]; a += x; a2 += x * x; }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) { a += __shfl_xor_sync(0xffffffffu, a, o); a2 += __shfl_xor_sync(0xffffffffu, a2, o); }
+            rm = __ddiv_rn((double)a, (double)NPIX);
+            double var = __dsub_rn(__ddiv_rn((double)a2, (double)NPIX), __dmul_rn(rm, rm));
+            rsd = __dsqrt_rn(var > 0.0 ? var : 0.0);
+        }
+        if (rsd <= 1e-6) continue;
+#pragma unroll
+        for (int i = 0; i < KP; ++i)
+            if (lane + 32 * i < NPIX) T2d[lane + 32 * i] = __dsub_rn((double)rv[i], rm);
+        int dmax = MAXD - 1;
+        if (xr + dmax + HALF >= W) dmax = W - 1 - HALF - xr;
+        const int lc0 = xr - HALF, lcols = dmax + PW;
+        __syncwarp();
+        // left-image window, candidate c at column c: lane scores c = 4 lane .. 4 lane + 3 (pad 4: word-aligned blocks)
+        stage_u8<HALF>(winb, L, W, vi - HALF, PW, lc0, lcols, 4, lane);
+        __syncwarp();
+        double lrb = -2.0;
+        int lrd = -1;
+        {
+            double z[4];
+            zncc4_u8<HALF>(winb + 4 + 4 * lane, T2d, rsd, z);
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (4 * lane + k <= dmax && z[k] > lrb) { lrb = z[k]; lrd = 4 * lane + k; }
+        }
+        warp_argmax(lrb, lrd);
+        if (lrd < 0 || fabs((double)(lrd - bestd)) > LRT) continue;
+
+        // parabola seed of the LK (from the sub-pixel keypoint position)
+        double off = 0.0;
+        if (bestd > lo && bestd < hi) {
+            double y0 = sc[bestd - 1], y2 = sc[bestd + 1];
+            double den = __dadd_rn(__dsub_rn(y0, __dmul_rn(2.0, bs)), y2);
+            if (den < -1e-9) {
+                off = __ddiv_rn(__dmul_rn(0.5, __dsub_rn(y0, y2)), den);
+                if (off > 0.5) off = 0.5;
+                if (off < -0.5) off = -0.5;
+            }
+        }
         if (lane == 0) {
-            double A[3][3] = {{Sv[3], Sv[4], Sv[5]}, {Sv[4], Sv[6], Sv[7]}, {Sv[5], Sv[7], Sv[8]}};
+            StJob& J = jobs[njobs];
+            J.u = u; J.v = v; J.ts = ts;
+            J.seed = __dadd_rn(__dadd_rn((double)bestd, off), __dsub_rn(u, (double)ui));
+            J.oi = (long long)oi;
+            J.ui = ui; J.vi = vi; J.xr = xr; J.js = js; J.f = f;
+        }
+        ++njobs;
+    }
+    if (njobs == 0) return;
+
+    // ----------------------------------------------------------------------------------------------- phase B: LKs
+    __syncwarp();
+    // every job's blocks, staged by the whole warp job by job (the search window is no longer needed)
+#pragma unroll 1
+    for (int j = 0; j < njobs; ++j) {
+        const StJob& J = jobs[j];
+        unsigned char* blk = U + (size_t)j * JB;
+        if (!FLT) {
+            const u8* Rf = R8all + (size_t)J.f * H * W;
+            const int ys0 = J.vi + J.js - HALF - 1, xs0 = J.xr - HALF - LK_MG - 1;
+            for (int idx = lane; idx < LKR * RS; idx += 32) {
+                const int rr = idx / RS, cc = idx - rr * RS, col = xs0 + cc;
+                blk[idx] = (cc < LKW && col >= 0 && col < W) ? Rf[(size_t)(ys0 + rr) * W + col] : (u8)0;
+            }
+        }
+        const u8* Lf = Lall + (size_t)J.f * H * W;
+        const int ly0 = J.vi - HALF - 1, lx0 = J.ui - HALF - 1;
+        for (int idx = lane; idx < LKR * LS; idx += 32) {
+            const int rr = idx / LS, cc = idx - rr * LS;
+            blk[LKR * RS + idx] = cc < PW + 2 ? Lf[(size_t)(ly0 + rr) * W + lx0 + cc] : (u8)0;
+        }
+    }
+    __syncwarp();
+    bool okl = false;
+    if (lane < njobs) {
+        const StJob J = jobs[lane];
+        const unsigned char* rb = U + (size_t)lane * JB;
+        const unsigned char* lb = rb + LKR * RS;
+        RightImg<FLT> R;
+        R.r8 = R8all ? R8all + (size_t)J.f * H * W : nullptr;
+        R.rf = Rsall ? Rsall + (size_t)J.f * H * W : nullptr;
+        const int ys0 = J.vi + J.js - HALF - 1, xs0 = J.xr - HALF - LK_MG - 1;
+        const int xa = xs0 > 0 ? xs0 : 0, xb = xs0 + LKW - 1 < W - 1 ? xs0 + LKW - 1 : W - 1;
+        const int ly0 = J.vi - HALF - 1, lx0 = J.ui - HALF - 1;
+        const double u = J.u, v = J.v, voff = (double)J.js, seed = J.seed;
+        double d = seed, a = 1.0, b = 0.0, sig = 0.0;
+#pragma unroll 1
+        for (int it = 0; it <= LK_ITERS; ++it) {
+            double S[9];
+#pragma unroll
+            for (int q = 0; q < 9; ++q) S[q] = 0.0;
+#pragma unroll 1
+            for (int dy = 0; dy < PW; ++dy) {
+                const double py = __dadd_rn(v, (double)(dy - HALF));
+                // the right samples' row: y = v + dy - HALF + js, its floor and fraction, for every pixel of the row
+                const double y = __dadd_rn(py, voff);
+                int y0 = (int)floor(y);
+                const double ay = __dsub_rn(y, (double)y0);
+                if (y0 < 0) y0 = 0;
+                if (y0 > H - 2) y0 = H - 2;
+                const double omay = __dsub_rn(1.0, ay);
+                const bool rin = y0 >= ys0 && y0 + 1 < ys0 + LKR;
+                // the template's row (the keypoint's neighbourhood keeps every sample off the image border: no clamp)
+                const int ty0 = (int)floor(py);
+                const double tay = __dsub_rn(py, (double)ty0);
+                int tr = ty0 - ly0;
+                tr = tr < 0 ? 0 : (tr > PW ? PW : tr);
+                const unsigned char* lrow = lb + tr * LS;
+#pragma unroll
+                for (int dx = 0; dx < PW; ++dx) {
+                    const double px = __dadd_rn(u, (double)(dx - HALF));
+                    // template sample: bilinear left at (px, py) (stereo1d._bil); u8 differences are exact
+                    const int tx0 = (int)floor(px);
+                    const double tax = __dsub_rn(px, (double)tx0);
+                    int tc = tx0 - lx0;
+                    tc = tc < 0 ? 0 : (tc > PW ? PW : tc);
+                    const unsigned char* lp = lrow + tc;
+                    const double tfa = u8d(lp[0]), tfb = u8d(lp[1]), tfc = u8d(lp[LS]), tfd = u8d(lp[LS + 1]);
+                    const double tba = __dsub_rn(tfb, tfa), tdc = __dsub_rn(tfd, tfc);
+                    const double ttop = __dadd_rn(tfa, __dmul_rn(tax, tba));
+                    const double tbot = __dadd_rn(tfc, __dmul_rn(tax, tdc));
+                    const double Tl = __dadd_rn(ttop, __dmul_rn(tay, __dsub_rn(tbot, ttop)));
+                    // right sample at (px - d, y)
+                    double rv, rg;
+                    if (FLT) {
+                        bil(R, H, W, __dsub_rn(px, d), y, &rv, &rg);
+                    } else {
+                        const double x = __dsub_rn(px, d);
+                        int x0 = (int)floor(x);
+                        const double ax = __dsub_rn(x, (double)x0);
+                        if (x0 < 0) x0 = 0;
+                        if (x0 > W - 2) x0 = W - 2;
+                        double fa, fb, fc, fd;
+                        if (rin && x0 >= xa && x0 + 1 <= xb) {
+                            const unsigned char* sp = rb + (y0 - ys0) * RS + (x0 - xs0);
+                            fa = u8d(sp[0]); fb = u8d(sp[1]); fc = u8d(sp[RS]); fd = u8d(sp[RS + 1]);
+                        } else {
+                            const u8* gp = R.r8 + (size_t)y0 * W + x0;
+                            fa = u8d(gp[0]); fb = u8d(gp[1]); fc = u8d(gp[W]); fd = u8d(gp[W + 1]);
+                        }
+                        const double ba = __dsub_rn(fb, fa), dc = __dsub_rn(fd, fc);
+                        const double top = __dadd_rn(fa, __dmul_rn(ax, ba));
+                        const double bot = __dadd_rn(fc, __dmul_rn(ax, dc));
+                        rv = __dadd_rn(top, __dmul_rn(ay, __dsub_rn(bot, top)));
+                        rg = __dadd_rn(__dmul_rn(ba, omay), __dmul_rn(dc, ay));
+                    }
+                    const double r = __dsub_rn(Tl, __dadd_rn(__dmul_rn(a, rv), b));
+                    const double J0 = __dmul_rn(-a, rg), J1 = rv;
+                    S[0] = __dadd_rn(S[0], __dmul_rn(J0, r));
+                    S[1] = __dadd_rn(S[1], __dmul_rn(J1, r));
+                    S[2] = __dadd_rn(S[2], r);
+                    S[3] = __dadd_rn(S[3], __dmul_rn(J0, J0));
+                    S[4] = __dadd_rn(S[4], __dmul_rn(J0, J1));
+                    S[5] = __dadd_rn(S[5], J0);
+                    S[6] = __dadd_rn(S[6], __dmul_rn(J1, J1));
+                    S[7] = __dadd_rn(S[7], J1);
+                    if (it == LK_ITERS) S[8] = __dadd_rn(S[8], __dmul_rn(r, r));
+                }
+            }
+            double A[3][3] = {{S[3], S[4], S[5]}, {S[4], S[6], S[7]}, {S[5], S[7], (double)NPIX}};
+#pragma unroll
             for (int i = 0; i < 3; ++i) A[i][i] = __dadd_rn(A[i][i], 1e-9);
             int piv[3];
             ob_getf2(A, piv);
             if (it < LK_ITERS) {
-                double dl[3] = {Sv[0], Sv[1], Sv[2]};
+                double dl[3] = {S[0], S[1], S[2]};
                 ob_getrs(A, piv, dl);
                 d = __dadd_rn(d, dl[0]);
                 a = __dadd_rn(a, dl[1]);
                 b = __dadd_rn(b, dl[2]);
-                if (!(isfinite(d) && isfinite(a))) go = 0;
+                if (!(isfinite(d) && isfinite(a))) break;
             } else {
-                double s2v = __ddiv_rn(Sv[9], (double)(NPIX - 3));
+                const double s2v = __ddiv_rn(S[8], (double)(NPIX - 3));
                 ob_getri(A, piv);
-                double var = __dmul_rn(s2v, A[0][0]);
+                const double var = __dmul_rn(s2v, A[0][0]);
                 sig = var > 0.0 ? __dsqrt_rn(var) : 0.0;
-                bool conv = isfinite(d) && fabs(__dsub_rn(d, seed)) <= 1.0 && a > 0.5 && a < 2.0;
-                okk = conv && !(d < 0.5);
+                const bool conv = isfinite(d) && fabs(__dsub_rn(d, seed)) <= 1.0 && a > 0.5 && a < 2.0;
+                okl = conv && !(d < 0.5);
             }
         }
-        go = __shfl_sync(0xffffffffu, go, 0);
-        d = __shfl_sync(0xffffffffu, d, 0);
-        a = __shfl_sync(0xffffffffu, a, 0);
-        b = __shfl_sync(0xffffffffu, b, 0);
-        if (!go) return;
+        if (okl) { od[J.oi] = d; osig[J.oi] = sig; ook[J.oi] = 1; }
     }
-    okk = __shfl_sync(0xffffffffu, (int)okk, 0);
-    if (!okk) return;
-    if (lane == 0) { od[oi] = d; osig[oi] = sig; ook[oi] = 1; }
 
-    // the point's own vertical offset: column scan of the ZNCC at the matched integer disparity
-    if (vi - 2 * HALF - 1 >= 0 && vi + 2 * HALF + 1 < H) {
-        // image rows vi - 2 HALF .. vi + 2 HALF, columns xr - HALF .. xr + HALF, staged once (the LK table is done)
-        float* vsf = (float*)(base + stereo_off_u(HALF));
+    // --------------------------------------------------------------------------------------- phase C: vertical scans
+    unsigned okm = __ballot_sync(0xffffffffu, okl);
+    double* Tv = (double*)U;                                    // the point's template minus its mean
+    float* vsf = (float*)(U + (size_t)NPIX * 8);                // the scan block
+    while (okm) {
+        const int j = __ffs(okm) - 1;
+        okm &= okm - 1;
+        const StJob J = jobs[j];
+        const int vi = J.vi, xr = J.xr;
+        // the point's own vertical offset: column scan of the ZNCC at the matched integer disparity
+        if (!(vi - 2 * HALF - 1 >= 0 && vi + 2 * HALF + 1 < H)) continue;
         __syncwarp();
+        const u8* L = Lall + (size_t)J.f * H * W;
+        RightImg<FLT> R;
+        R.r8 = R8all ? R8all + (size_t)J.f * H * W : nullptr;
+        R.rf = Rsall ? Rsall + (size_t)J.f * H * W : nullptr;
+        {
+            int tv[KP];
+#pragma unroll
+            for (int i = 0; i < KP; ++i) {
+                const int k = lane + 32 * i;
+                tv[i] = k < NPIX ? (int)L[(size_t)(vi + k / PW - HALF) * W + J.ui + k % PW - HALF] : 0;
+            }
+            int s = 0;
+#pragma unroll
+            for (int i = 0; i < KP; ++i) s += tv[i];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            const double tm = __ddiv_rn((double)s, (double)NPIX);
+#pragma unroll
+            for (int i = 0; i < KP; ++i)
+                if (lane + 32 * i < NPIX) Tv[lane + 32 * i] = __dsub_rn((double)tv[i], tm);
+        }
+        // image rows vi - 2 HALF .. vi + 2 HALF, columns xr - HALF .. xr + HALF
 #pragma unroll
         for (int i = 0; i < ((2 * PW - 1) * PW + 31) / 32; ++i) {
             const int idx = lane + 32 * i;
@@ -786,18 +871,18 @@ __global__ void __launch_bounds__(ST_WARPS * 32, 2) k_stereo(
                 const double r = (double)rf;
                 zs = __dadd_rn(zs, r);
                 zs2 = __dadd_rn(zs2, FLT ? (double)__fmul_rn(rf, rf) : __dmul_rn(r, r));
-                sx = __dadd_rn(sx, __dmul_rn(r, Td[k]));
+                sx = __dadd_rn(sx, __dmul_rn(r, Tv[k]));
             }
-            z = zncc_finish(zs, zs2, sx, ts, NPIX);
+            z = zncc_finish(zs, zs2, sx, J.ts, NPIX);
         }
         double col[PW];
 #pragma unroll
-        for (int j = 0; j < PW; ++j) col[j] = __shfl_sync(0xffffffffu, z, j);
+        for (int jj = 0; jj < PW; ++jj) col[jj] = __shfl_sync(0xffffffffu, z, jj);
         if (lane == 0) {
             int jp = 0;
             double cs = -2.0;
-            for (int j = -HALF; j <= HALF; ++j)
-                if (col[j + HALF] > cs) { cs = col[j + HALF]; jp = j; }
+            for (int jj = -HALF; jj <= HALF; ++jj)
+                if (col[jj + HALF] > cs) { cs = col[jj + HALF]; jp = jj; }
             double offy = 0.0;
             if (jp > -HALF && jp < HALF) {
                 double y0 = col[jp - 1 + HALF], y2 = col[jp + 1 + HALF];
@@ -808,7 +893,7 @@ __global__ void __launch_bounds__(ST_WARPS * 32, 2) k_stereo(
                     if (offy < -0.5) offy = -0.5;
                 }
             }
-            ody[oi] = __dadd_rn((double)jp, offy);
+            ody[J.oi] = __dadd_rn((double)jp, offy);
         }
     }
 }
@@ -820,12 +905,14 @@ static cudaError_t launch_stereo_t(const uint8_t* L, const uint8_t* R8, const fl
                                    double* od, double* osig, uint8_t* ook, double* ozn, double* ody, long long npts,
                                    cudaStream_t st)
 {
+    constexpr int NW = st_warps(HALF);
     size_t pw = (xcb_stereo_smem_per_warp(HALF, band) + 15) & ~(size_t)15;
-    size_t sm = pw * ST_WARPS;
-    long long nb = (npts + ST_WARPS - 1) / ST_WARPS;
+    size_t sm = pw * NW;
+    const long long per_block = (long long)NW * ST_GROUP;
+    long long nb = (npts + per_block - 1) / per_block;
     if (nb <= 0) return cudaSuccess;
-    k_stereo<HALF, FLT><<<(unsigned)nb, ST_WARPS * 32, sm, st>>>(L, R8, Rs, H, W, kpd, dlo_a, dhi_a, n, kpf, counts,
-                                                                  cap, dlo, dhi, band, od, osig, ook, ozn, ody);
+    k_stereo<HALF, FLT><<<(unsigned)nb, NW * 32, sm, st>>>(L, R8, Rs, H, W, kpd, dlo_a, dhi_a, n, kpf, counts, cap,
+                                                            dlo, dhi, band, od, osig, ook, ozn, ody);
     return cudaGetLastError();
 }
 
@@ -836,7 +923,7 @@ cudaError_t xcb_stereo_init_attrs()
 #define XCB_SA(HH, FF)                                                                                            \
     if (e == cudaSuccess)                                                                                         \
         e = cudaFuncSetAttribute(k_stereo<HH, FF>, cudaFuncAttributeMaxDynamicSharedMemorySize,                   \
-                                 (int)(((xcb_stereo_smem_per_warp(HH, BAND_MAX) + 15) & ~(size_t)15) * ST_WARPS));
+                                 (int)(((xcb_stereo_smem_per_warp(HH, BAND_MAX) + 15) & ~(size_t)15) * st_warps(HH)));
     XCB_SA(3, false) XCB_SA(3, true) XCB_SA(4, false) XCB_SA(4, true) XCB_SA(5, false) XCB_SA(5, true)
 #undef XCB_SA
     return e;
