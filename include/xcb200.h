@@ -223,6 +223,21 @@ typedef struct {
     const double* ob_z;         /* [Mt][2] */
     const double* ob_isig;      /* [Mt] */
     const uint8_t* ob_valid;    /* [Mt] */
+    /* Marginal priors over pose blocks (src/xclean/vio/marg.py Prior, added to the system, the gradient and the cost
+       as window.py _full_system / solve do, :865-887, :963-964), or pr_m == NULL for none.  Window w's prior is
+       1/2 |S d + r|^2 with pr_m[w] rows (0 = no prior, at most 6 pr_nb[w]) over pr_nb[w] blocks: block k of the
+       window is entry pr_boff[w] + k of pr_blk (its window-local slot) and of pr_x0 (its first-estimate pose: R0
+       row-major, p0); d = per block [Log(R0^T R), p - p0]; S is pr_m[w] x 6 pr_nb[w] row-major at pr_S + pr_soff[w],
+       r at pr_r + pr_roff[w]. */
+    const int32_t* pr_m;        /* [nw] */
+    const int32_t* pr_nb;       /* [nw] */
+    const int32_t* pr_boff;     /* [nw] */
+    const int32_t* pr_soff;     /* [nw] */
+    const int32_t* pr_roff;     /* [nw] */
+    const int32_t* pr_blk;      /* [blocks] */
+    const double* pr_x0;        /* [blocks][12] */
+    const double* pr_S;
+    const double* pr_r;
 } xcb_ba_windows;
 
 #define XCB_BA_FP64 0           /* everything in float64: the plain form */
@@ -232,6 +247,8 @@ typedef struct {
    hold the batch's per-landmark records; the kernel counts the landmarks from the windows themselves (lm_off + L),
    writes nothing else and leaves the state unchanged */
 #define XCB_BA_STATUS_SCRATCH (-3)
+/* per-window status of the Newton / adjoint calls for a window with a marginal prior (not supported there) */
+#define XCB_BA_STATUS_PRIOR (-4)
 
 /* Device scratch the batched solve needs for `Lt` landmarks: the work counter, the trial landmark states and, for the
    float64 mode, each landmark's back-substitution record (118 doubles: ~0.95 kB per landmark).  A smaller scratch

@@ -67,7 +67,8 @@ FRONT_STAGES = ("response", "noise_floor", "candidates", "greedy", "orb", "stere
 class BaWindows(ctypes.Structure):
     _fields_ = [("nw", c_int)] + [(n, c_void_p) for n in (
         "P", "L", "slot_off", "lm_off", "hold", "order", "cam", "ext", "Rwb", "pwb", "lmp", "lm_host", "lm_mask",
-        "rho_meas", "rho_isig", "lm_ob", "ob_pose", "ob_cam", "ob_z", "ob_isig", "ob_valid")]
+        "rho_meas", "rho_isig", "lm_ob", "ob_pose", "ob_cam", "ob_z", "ob_isig", "ob_valid",
+        "pr_m", "pr_nb", "pr_boff", "pr_soff", "pr_roff", "pr_blk", "pr_x0", "pr_S", "pr_r")]
 
 
 XCB_BA_FP64 = 0
@@ -76,6 +77,7 @@ XCB_BA_NEWTON_POLISH = 0
 XCB_BA_NEWTON_ADJOINT = 1
 XCB_BA_NEWTON_POLISH_FIXED = 2
 XCB_BA_STATUS_SCRATCH = -3
+XCB_BA_STATUS_PRIOR = -4
 _SIGS.update({
     "xcb_ba_scratch_bytes": (c_size_t, [c_int, c_int]),
     "xcb_ba_solve_windows_dev": (c_int, [ctypes.POINTER(BaWindows), c_int, c_int, c_double, c_int, P, P, c_int, P,

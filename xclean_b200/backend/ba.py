@@ -14,7 +14,8 @@ the drop-in of its stage kernels).
     posefree_marginals(w)                   # final_linearisation's pose-free marginals into w.pf.Hinv / w.pf.ok
     systems, costs = final_linearisation_batch(windows);  H, b, off = marg_system_batch(windows, masks)[i]
 
-    # window.py's own single-window signatures (visual windows; prior / IMU raise NotImplementedError)
+    # window.py's own single-window signatures (visual windows, with a marginal prior over pose slots (w.prior, a
+    # bound backend.marg.Prior or the reference's marg.Prior); IMU terms raise NotImplementedError)
     st = solve(pb, iters=5, lam0=1e-4);  final_linearisation(pb);  marg_system(pb, lm_mask)
 
 Every call goes through libxcb200.so's C ABI (xcb_ba_solve_windows_dev); there is no CPU fallback.
@@ -67,6 +68,7 @@ class _Merged:
         n = len(pf.host)
         for k in ("Rwb", "pwb", "Rbc", "pbc", "fx", "fy", "cx", "cy", "B", "huber_k"):
             setattr(self, k, getattr(w, k))
+        self.prior = getattr(w, "prior", None)
         M = int(np.asarray(w.ob_start)[-1])
         self.lmp = np.concatenate([np.asarray(w.lmp, np.float64).reshape(-1, 3), pf.lmp])
         self.lm_host = np.concatenate([np.asarray(w.lm_host, np.int64), pf.host])
@@ -135,7 +137,8 @@ def pack_windows(windows, hold=0):
                     for w in windows], np.float64).reshape(nw, 12)
     work = P.astype(np.int64) ** 2 * 36 + M.astype(np.int64) * 64
     order = np.argsort(-work, kind="stable").astype(np.int32)
-    return dict(P=P, L=L, slot_off=slot_off, lm_off=lm_off, hold=hold_a, order=order, cam=cam, ext=ext,
+    pr = _pack_priors(windows, P)
+    return dict(**pr, P=P, L=L, slot_off=slot_off, lm_off=lm_off, hold=hold_a, order=order, cam=cam, ext=ext,
                 Rwb=cat("Rwb", np.float64).reshape(-1, 9), pwb=cat("pwb", np.float64).reshape(-1, 3),
                 lmp=cat("lmp", np.float64).reshape(-1, 3), lm_host=cat("lm_host", np.int32).ravel(),
                 lm_mask=cat("lm_mask", np.uint8).ravel(), rho_meas=cat("rho_meas", np.float64).ravel(),
@@ -143,6 +146,65 @@ def pack_windows(windows, hold=0):
                 ob_pose=cat("ob_pose", np.int32).ravel(), ob_cam=cat("ob_cam", np.uint8).ravel(),
                 ob_z=cat("ob_z", np.float64).reshape(-1, 2), ob_isig=cat("ob_isig", np.float64).ravel(),
                 ob_valid=cat("ob_valid", np.uint8).ravel(), max_slots=int(P.max(initial=1)), nw=nw)
+
+
+PRIOR_FIELDS = ("pr_m", "pr_nb", "pr_boff", "pr_soff", "pr_roff", "pr_blk", "pr_x0", "pr_S", "pr_r")
+
+
+def _prior_slots(pr, P):
+    """The window slot of each block of a bound prior (window.Problem.prior: marg.Prior after bind(), 6-dim pose
+    blocks with the default 6-per-slot offsets)."""
+    cols = getattr(pr, "cols", None)
+    dims = [int(x) for x in pr.dims]
+    if cols is None:
+        raise ValueError("solve_batch: the window's prior is not bound to its slots (Prior.bind)")
+    if any(x != 6 for x in dims):
+        raise NotImplementedError("solve_batch: prior blocks of 15 dims (visual-inertial) are not on this path")
+    cols = np.asarray(cols, np.int64)
+    slots = cols[0::6] // 6
+    if len(cols) != 6 * len(dims) or (cols != (6 * np.repeat(slots, 6) + np.tile(np.arange(6), len(dims)))).any():
+        raise ValueError("solve_batch: a prior block does not cover one whole pose slot")
+    if (slots < 0).any() or (slots >= P).any() or len(np.unique(slots)) != len(slots):
+        raise ValueError("solve_batch: prior blocks must be distinct slots of the window")
+    return slots
+
+
+def _pack_priors(windows, P):
+    """The marginal priors of the windows (w.prior: None or a bound marg.Prior) in the pr_* layout of xcb_ba_windows;
+    {} when no window has one."""
+    prs = [getattr(w, "prior", None) for w in windows]
+    if all(p is None for p in prs):
+        return {}
+    nw = len(windows)
+    m = np.zeros(nw, np.int32)
+    nb = np.zeros(nw, np.int32)
+    boff = np.zeros(nw, np.int32)
+    soff = np.zeros(nw, np.int32)
+    roff = np.zeros(nw, np.int32)
+    blk, x0, S, r = [], [], [], []
+    nblk = ns = nr = 0
+    for i, pr in enumerate(prs):
+        boff[i], soff[i], roff[i] = nblk, ns, nr
+        if pr is None:
+            continue
+        slots = _prior_slots(pr, int(P[i]))
+        Sw = np.ascontiguousarray(pr.S, np.float64).reshape(-1, 6 * len(slots))
+        rw = np.ascontiguousarray(pr.r, np.float64).reshape(Sw.shape[0])
+        if Sw.shape[0] > 6 * len(slots):
+            raise ValueError("solve_batch: a prior has more rows than columns")
+        m[i], nb[i] = Sw.shape[0], len(slots)
+        blk.append(slots.astype(np.int32))
+        x0.append(np.stack([np.concatenate([np.asarray(x[0], np.float64).ravel(), np.asarray(x[1], np.float64).ravel()])
+                            for x in pr.x0]))
+        S.append(Sw.ravel())
+        r.append(rw)
+        nblk += len(slots)
+        ns += Sw.size
+        nr += len(rw)
+    cat = lambda parts, dt, shape: (np.ascontiguousarray(np.concatenate(parts).astype(dt)).reshape(shape) if parts
+                                    else np.zeros(shape, dt))
+    return dict(pr_m=m, pr_nb=nb, pr_boff=boff, pr_soff=soff, pr_roff=roff, pr_blk=cat(blk, np.int32, (-1,)),
+                pr_x0=cat(x0, np.float64, (-1, 12)), pr_S=cat(S, np.float64, (-1,)), pr_r=cat(r, np.float64, (-1,)))
 
 
 class BatchSolver:
@@ -159,6 +221,10 @@ class BatchSolver:
         self.nw = self.host["nw"]
         self.max_slots = self.host["max_slots"]
         self.t = {k: torch.from_numpy(np.ascontiguousarray(self.host[k])).to(self.dev) for k in self.FIELDS}
+        for k in PRIOR_FIELDS:
+            if k in self.host:
+                a = np.ascontiguousarray(self.host[k])
+                self.t[k] = torch.from_numpy(a if a.size else np.zeros(1, a.dtype)).to(self.dev)
         self.init = {k: self.t[k].clone() for k in ("Rwb", "pwb", "lmp")}
         self.stats = torch.zeros((max(self.nw, 1), 8), dtype=torch.float64, device=self.dev)
         self.dx0 = torch.zeros((max(self.nw, 1), 6 * MAX_SLOTS), dtype=torch.float64, device=self.dev)
@@ -168,8 +234,9 @@ class BatchSolver:
         self.scratch = torch.zeros(nb, dtype=torch.uint8, device=self.dev)
         self.desc = _lib.BaWindows()
         self.desc.nw = self.nw
-        for k in self.FIELDS:
-            setattr(self.desc, k, self.t[k].data_ptr())
+        for k in self.FIELDS + PRIOR_FIELDS:
+            if k in self.t:
+                setattr(self.desc, k, self.t[k].data_ptr())
 
     def reset(self):
         for k in ("Rwb", "pwb", "lmp"):
@@ -375,8 +442,8 @@ def posefree_marginals(w):
 
 
 def final_linearisation_batch(windows, device="cuda"):
-    """window.final_linearisation for a batch of purely visual windows (no prior, no IMU): per window a dict of the
-    reference's outputs for such a window - H, b (the Schur-reduced visual system at lam = 0), ob_chi2 (M), lm_ok (L),
+    """window.final_linearisation for a batch of visual windows (no IMU; a window's marginal prior, w.prior, is added
+    to its system): per window a dict of the reference's outputs - H, b (the Schur-reduced system at lam = 0), ob_chi2 (M), lm_ok (L),
     Hll_inv (L,3,3) of the window's own landmarks and observations - and the pose-free block's marginals into
     w.pf.Hinv / w.pf.ok.  -> (list of dicts, robust costs (the block's cost included))."""
     bs = BatchSolver(windows, device, hold=None)
@@ -391,7 +458,7 @@ def final_linearisation_batch(windows, device="cuda"):
 def marg_system_batch(windows, lm_masks, device="cuda"):
     """window.marg_system (window.py:1011-1031) for a batch of purely visual windows: for each window and its
     landmark mask, the linear system (H, b) of the masked landmarks' visual observations, Schur'd out, at the current
-    state (lam = 0; the reference adds the prior and IMU terms, which this path has none of), and the state offsets.
+    state (lam = 0; a window's marginal prior is added, as the reference adds it; no IMU terms), and the state offsets.
     The pose-free block never enters (the reference's marg_system does not see it).  -> list of (H, b, off)."""
     views = []
     for w, m in zip(windows, lm_masks):
@@ -408,14 +475,15 @@ class _Masked:
         for k in ("Rwb", "pwb", "Rbc", "pbc", "lmp", "lm_host", "rho_meas", "rho_isig", "ob_start", "ob_pose", "ob_cam",
                   "ob_z", "ob_isig", "ob_valid", "fx", "fy", "cx", "cy", "B", "huber_k"):
             setattr(self, k, getattr(w, k))
+        self.prior = getattr(w, "prior", None)
         self.lm_mask = mask
 
 
 # --------------------------------------------------------------------- window.py's single-window signatures
 def _visual_only(pb, what):
-    if getattr(pb, "prior", None) is not None or getattr(pb, "imu", None):
-        raise NotImplementedError("%s: the marginal prior and IMU terms are not on this path (visual windows only)"
-                                  % what)
+    if getattr(pb, "imu", None):
+        raise NotImplementedError("%s: the IMU terms are not on this path (visual windows, with or without a marginal "
+                                  "prior over pose slots)" % what)
     if getattr(pb, "dims", None) is not None and (np.asarray(pb.dims) != 6).any():
         raise NotImplementedError("%s: full-state slots (dims 15) are not on this path" % what)
 

@@ -131,6 +131,8 @@ struct BaShared {
     double g[BA_MAXN], y[BA_MAXN], dx[BA_MAXN], rhs[BA_MAXN], dmp[BA_MAXN];
     float bf[BA_MAXN];
     double red[BA_WARPS];
+    double pr_d[BA_MAXN], pr_res[BA_MAXN];     // marginal prior: block deltas (or S x), residual S d + r
+    double pr_cost;
     double lam;
     int accepted;
     int overflow;
@@ -772,6 +774,121 @@ __device__ double block_sum_red(BaShared& sh)
     return s;
 }
 
+// ------------------------------------------------------------------------------------------------ marginal prior
+// The prior 1/2 |S d + r|^2 of marg.Prior (src/xclean/vio/marg.py:124-140) over pose blocks, added to the reduced
+// system, the gradient and the cost as window._full_system and window.solve add it (window.py:865-887, :963-964).
+__device__ __forceinline__ bool has_prior(const XcbBaWindows& d, int w) { return d.pr_m != nullptr && d.pr_m[w] > 0; }
+
+// window.so3_log_nb (src/xclean/vio/window.py:65-105)
+__device__ void so3_log_dev(const double* R, double* w)
+{
+    double c = (R[0] + R[4] + R[8] - 1.0) * 0.5;
+    c = fmin(fmax(c, -1.0), 1.0);
+    const double th = acos(c);
+    const double v0 = R[7] - R[5], v1 = R[2] - R[6], v2 = R[3] - R[1];
+    if (th < 1e-6) { w[0] = 0.5 * v0; w[1] = 0.5 * v1; w[2] = 0.5 * v2; return; }
+    if (th > 3.141592653589793 - 1e-4) {
+        // near pi: the axis from the symmetric part, its sign from the skew part
+        double B[9];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) B[3 * i + j] = (R[3 * i + j] + R[3 * j + i]) * 0.5;
+        int i = 0;
+        if (B[4] > B[4 * i]) i = 1;
+        if (B[8] > B[4 * i]) i = 2;
+        const double den = sqrt(fmax((B[4 * i] - c) / (1.0 - c), 0.0));
+        double ax[3];
+        for (int j = 0; j < 3; ++j) ax[j] = (B[3 * j + i] - (j == i ? c : 0.0)) / fmax(den * (1.0 - c), 1e-12);
+        ax[i] = den;
+        const double nrm = sqrt(ax[0] * ax[0] + ax[1] * ax[1] + ax[2] * ax[2]);
+        const double sg = ax[0] * v0 + ax[1] * v1 + ax[2] * v2 < 0 ? -1.0 : 1.0;
+        for (int j = 0; j < 3; ++j) w[j] = sg * th * ax[j] / nrm;
+        return;
+    }
+    const double f = th / (2.0 * sin(th));
+    w[0] = f * v0; w[1] = f * v1; w[2] = f * v2;
+}
+
+// residual S d + r at the slot poses (Rwb, pwb) into sh.pr_res; -> 1/2 |S d + r|^2 (every thread)
+__device__ double prior_residual(BaShared& sh, const XcbBaWindows& d, int w, const double* Rwb, const double* pwb)
+{
+    const int m = d.pr_m[w], nb = d.pr_nb[w], nc = 6 * nb, b0 = d.pr_boff[w];
+    const double* S = d.pr_S + d.pr_soff[w];
+    const double* r = d.pr_r + d.pr_roff[w];
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+        const int s = d.pr_blk[b0 + k];
+        const double* x0 = d.pr_x0 + 12 * (size_t)(b0 + k);
+        const double* R = Rwb + 9 * s;
+        double A[9];                                    // R0^T R
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) A[3 * i + j] = x0[i] * R[j] + x0[3 + i] * R[3 + j] + x0[6 + i] * R[6 + j];
+        so3_log_dev(A, sh.pr_d + 6 * k);
+        for (int i = 0; i < 3; ++i) sh.pr_d[6 * k + 3 + i] = pwb[3 * s + i] - x0[9 + i];
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        double acc = 0.0;
+        for (int j = 0; j < nc; ++j) acc += S[(size_t)i * nc + j] * sh.pr_d[j];
+        sh.pr_res[i] = acc + r[i];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double c = 0.0;
+        for (int i = 0; i < m; ++i) c += sh.pr_res[i] * sh.pr_res[i];
+        sh.pr_cost = 0.5 * c;
+    }
+    __syncthreads();
+    return sh.pr_cost;
+}
+
+__device__ __forceinline__ int prior_col(const XcbBaWindows& d, int w, int i)
+{
+    return 6 * d.pr_blk[d.pr_boff[w] + i / 6] + i % 6;
+}
+
+// S^T S into the packed lower reduced system, S^T res (sh.pr_res) into grad (may be null) and into grad2 (may be null)
+__device__ void prior_system(BaShared& sh, const XcbBaWindows& d, int w, double* S64, double* grad, double* grad2)
+{
+    const int m = d.pr_m[w], nc = 6 * d.pr_nb[w];
+    const double* S = d.pr_S + d.pr_soff[w];
+    if (S64)
+        for (int q = threadIdx.x; q < nc * nc; q += blockDim.x) {
+            const int i = q / nc, j = q % nc;
+            if (j > i) continue;
+            double acc = 0.0;
+            for (int k = 0; k < m; ++k) acc += S[(size_t)k * nc + i] * S[(size_t)k * nc + j];
+            int ci = prior_col(d, w, i), cj = prior_col(d, w, j);
+            if (ci < cj) { const int t = ci; ci = cj; cj = t; }
+            S64[tri(ci, cj)] += acc;
+        }
+    for (int i = threadIdx.x; i < nc; i += blockDim.x) {
+        double acc = 0.0;
+        for (int k = 0; k < m; ++k) acc += S[(size_t)k * nc + i] * sh.pr_res[k];
+        const int ci = prior_col(d, w, i);
+        if (grad) grad[ci] += acc;
+        if (grad2) grad2[ci] += acc;
+    }
+    __syncthreads();
+}
+
+// y += S^T S x on the prior's columns (the refinement's matrix-free product; uses sh.pr_d as scratch)
+__device__ void prior_apply(BaShared& sh, const XcbBaWindows& d, int w, const double* x, double* y)
+{
+    const int m = d.pr_m[w], nc = 6 * d.pr_nb[w];
+    const double* S = d.pr_S + d.pr_soff[w];
+    for (int k = threadIdx.x; k < m; k += blockDim.x) {
+        double acc = 0.0;
+        for (int j = 0; j < nc; ++j) acc += S[(size_t)k * nc + j] * x[prior_col(d, w, j)];
+        sh.pr_d[k] = acc;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nc; i += blockDim.x) {
+        double acc = 0.0;
+        for (int k = 0; k < m; ++k) acc += S[(size_t)k * nc + i] * sh.pr_d[k];
+        y[prior_col(d, w, i)] += acc;
+    }
+    __syncthreads();
+}
+
 // ------------------------------------------------------------------------------------------------- the kernel
 __global__ void __launch_bounds__(BA_THREADS, 1) k_ba_windows(XcbBaWindows d, int iters, double lam0, int mode,
                                                               double* stats, double* dx0, int dx0_stride,
@@ -860,6 +977,13 @@ __global__ void __launch_bounds__(BA_THREADS, 1) k_ba_windows(XcbBaWindows d, in
                 for (int q = tid; q < n; q += blockDim.x) sh.rhs[q] = sh.g[q];
             }
             __syncthreads();
+            const bool pri = has_prior(d, w);
+            if (pri) {
+                // the prior at the linearisation point: its information into the system, its gradient into the
+                // right-hand side source (and the float64 gradient), its cost into the iteration's cost
+                c_tot += prior_residual(sh, d, w, sh.Rwb, sh.pwb);
+                prior_system(sh, d, w, S64, sh.rhs, mode == XCB_BA_MIXED ? nullptr : sh.g);
+            }
             if (mode == XCB_BA_LINEARISE) {
                 // final_linearisation's visual part (window.py:985-1008): the reduced system at the current state, no
                 // hold, no step; dx0 receives, for each window, H (n x n, row-major), b (n), the landmark records
@@ -897,7 +1021,7 @@ __global__ void __launch_bounds__(BA_THREADS, 1) k_ba_windows(XcbBaWindows d, in
             if (bad) {
                 if (mode == XCB_BA_MIXED) {
                     pass_cost(sh, d, sh.g64, d.lmp);
-                    c_tot = block_sum_red(sh);
+                    c_tot = block_sum_red(sh) + (pri ? sh.pr_cost : 0.0);
                 }
                 if (it == 0) cost0 = c_tot;
                 cur = c_tot;
@@ -911,7 +1035,11 @@ __global__ void __launch_bounds__(BA_THREADS, 1) k_ba_windows(XcbBaWindows d, in
                 // correction exceeds 1e-9 of the step
                 for (int rf = 0; rf < BA_REFINE_MAX; ++rf) {
                     pass_refine(sh, d, wl64, rf == 0, frz, rf == 0 ? bsc : nullptr);
-                    if (rf == 0) c_tot = block_sum_red(sh);
+                    if (rf == 0) c_tot = block_sum_red(sh) + (pri ? sh.pr_cost : 0.0);
+                    if (pri) {
+                        if (rf == 0) prior_system(sh, d, w, nullptr, sh.g, nullptr);   // pr_res: this state's
+                        prior_apply(sh, d, w, sh.dx, sh.y);
+                    }
                     for (int q = tid; q < n; q += blockDim.x) {
                         double r = -sh.g[q] - sh.y[q] - sh.dmp[q] * sh.dx[q];
                         if (hs >= 0 && q / 6 == hs) r = 0.0;
@@ -949,7 +1077,8 @@ __global__ void __launch_bounds__(BA_THREADS, 1) k_ba_windows(XcbBaWindows d, in
             __syncthreads();
             slot_geo(sh, sh.R2, sh.p2);
             pass_cost(sh, d, sh.g64, lmp_trial);
-            const double c_new = block_sum_red(sh);
+            double c_new = block_sum_red(sh);
+            if (pri) c_new += prior_residual(sh, d, w, sh.R2, sh.p2);
             const bool acc = c_new < c_tot;
             if (acc) {
                 for (int q = tid; q < P * 9; q += blockDim.x) sh.Rwb[q] = sh.R2[q];
@@ -1574,8 +1703,8 @@ __global__ void __launch_bounds__(BA_THREADS, 1) k_ba_newton(XcbBaWindows d, int
         }
         __syncthreads();
         const int P = sh.w.P, n = sh.w.n, s0 = sh.w.s0;
-        if (P > BA_MAXP || P < 1) {
-            if (tid == 0) stats[4 * w + 3] = -1.0;
+        if (P > BA_MAXP || P < 1 || has_prior(d, w)) {
+            if (tid == 0) stats[4 * w + 3] = has_prior(d, w) ? XCB_BA_STATUS_PRIOR : -1.0;
             __syncthreads();
             continue;
         }
