@@ -269,6 +269,12 @@ def run_ours(args, ws, rank, local):
     torch.cuda.set_stream(stream)
     sptr = stream.cuda_stream
     assert sptr != 0
+    # launch shapes: the autotuner's choice for this device and shape (searched once, then read from its cache)
+    from xclean_b200 import tune as TU
+    tuner = TU.Tuner()
+    tune_pick, tune_ent = TU.tune_front(gf, L.data_ptr(), R.data_ptr(), Bt, BUDGET, HALF, DLO, DHI, stream, tuner)
+    tuning = {"front_stereo": {"best": tune_pick, "candidates_ms": tune_ent["ms"],
+                               "candidates": tune_ent["candidates"], "device": tuner.device()}}
     gf.set_stage_timing(True)
 
     def step():
@@ -391,7 +397,8 @@ def run_ours(args, ws, rank, local):
                                "oracle/time_reference_cpu.py times its numba / cv2 modules where the source is", "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
             "gpu_launches": launches_per_step * args.steps,
             "kp_per_frame_last_batch": float(np.mean(counts)) if len(counts) else None,
-            "bitexact_vs_oracle_all_frames": recheck, "front_hd": hd, "per_call": percall, "ba": ba, "mapmatch": mm}
+            "bitexact_vs_oracle_all_frames": recheck, "tuning": tuning, "front_hd": hd, "per_call": percall, "ba": ba,
+            "mapmatch": mm}
     if rank == 0:
         print(json.dumps(line), flush=True)
     gf.close()
@@ -615,6 +622,10 @@ def run_mapmatch(args, dev, stream, ws_world, outs, cpu=True):
                d2=torch.empty((F, MM_LANDMARKS), dtype=torch.float64, device=dev))
     sptr = stream.cuda_stream
     nb = (F + Bt - 1) // Bt
+    from xclean_b200 import tune as TU
+    pick, ent = TU.tune_mapmatch(mm, dict(kp=d["kp"][:Bt], nkp=d["nkp"][:Bt], desc=d["desc"][:Bt], uv=d["uv"][:Bt],
+                                          S=d["S"][:Bt], lm_desc=d["lmd"][:Bt], lm_ndesc=d["lnd"][:Bt],
+                                          nlm=d["nlm"][:Bt], out={k: v[:Bt] for k, v in out.items()}), stream)
 
     def step():
         for b in range(nb):
@@ -654,6 +665,7 @@ def run_mapmatch(args, dev, stream, ws_world, outs, cpu=True):
            "value": F / (ms / 1e3), "unit": "frames/s", "ms_per_step": ms, "frames_per_step": F,
            "matched_per_frame": float((got["kp"] >= 0).sum() / F),
            "gpu_launches_per_step": 3 * nb,
+           "tuning": {"best": pick, "candidates_ms": ent["ms"], "candidates": ent["candidates"]},
            "e2e": {"value": 1.0 / e2e_dt, "unit": "frames/s", "api": "MapMatcher.match per frame (host arrays)",
                    "us_per_frame": 1e6 * e2e_dt, "h2d_bytes_per_frame": h2d, "d2h_bytes_per_frame": d2h}}
     # the engine's tracking step in one call: predict_projection of a 2,000-landmark window + the gated matching

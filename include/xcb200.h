@@ -27,6 +27,13 @@ extern "C" {
 #define XCB_ERR_NOT_CALIBRATED (-4)
 #define XCB_ERR_DEVICE (-5)       /* a kernel reported an error word (bounded loop ran out, overflow) */
 
+/* Launch-shape knobs chosen per (device, workload shape) by the package's autotuner (xclean_b200/tune.py); no
+   reference counterpart (the reference's launch shapes are constants).  0 = the built-in default. */
+#define XCB_TUNE_MM_LANES 1       /* map matcher gate: lanes per landmark, 1, 2, 4 or 8 (default 2) */
+#define XCB_TUNE_STEREO_WARPS 2   /* stereo: warps (point groups) per block, 1..8 (default 8; 6 for the 11x11 window) */
+#define XCB_TUNE_STEREO_GROUP 3   /* stereo: points per warp, searched one after another, LKs one per lane, 1..32 */
+#define XCB_TUNE_KNOBS 4
+
 /* device error word bits (set by kernels, read back by the host after each call) */
 #define XCB_DEVERR_GREEDY_ROUNDS 1u
 #define XCB_DEVERR_STEREO_SMEM 2u
@@ -126,6 +133,9 @@ int xcb_front_pipeline_host_batches(xcb_front* f, const uint8_t* left, const uin
                                     void* stream);
 /* number of kernel launches the last pipeline call issued */
 int xcb_front_last_launches(const xcb_front* f);
+/* Set a launch-shape knob of this front (XCB_TUNE_STEREO_*; no reference counterpart): later calls launch with it;
+   the captured pipeline graphs are dropped and re-captured on their next use.  Results do not depend on it. */
+int xcb_front_set_tuning(xcb_front* f, int knob, int value);
 /* wait for `stream` (NULL = the front's own) and read the device error word -> XCB_OK or XCB_ERR_DEVICE */
 int xcb_front_sync_check(xcb_front* f, void* stream);
 /* Stage timing of the batched pipeline (no reference counterpart; the reference times stages on the host with
@@ -153,6 +163,9 @@ int xcb_mm_create(int width, int height, int max_frames, int max_kp, int max_lm,
 int xcb_mm_destroy(xcb_mm* m);
 const char* xcb_mm_last_error(xcb_mm* m);
 int xcb_mm_grid_dims(xcb_mm* m, int* gw, int* gh);
+/* Set a launch-shape knob of this matcher (XCB_TUNE_MM_LANES; no reference counterpart).  Results do not depend on
+   it. */
+int xcb_mm_set_tuning(xcb_mm* m, int knob, int value);
 /* MapMatcher.match (mapmatch.py:148-169 + _gated :49-131; mapmatch_fast.py:172-184 + _match_fused :113-161) from host
    arrays: kp (N x 2 float64), desc (N x 32), uv (L x 2 float64), S (L x 2 x 2 float64), lm_desc (L x D x 32),
    lm_ndesc (L, int64, each <= D, else XCB_ERR_ARG: the reference would read past the landmark's slots), chi2 (the

@@ -221,3 +221,38 @@ def test_calibrate_against_this_machines_cv2():
     cal = gf.calibrate(cache=False)
     assert cal["noise_floor_equal"] and cal["orb_equal_random"] == 1500
     gf.close()
+
+
+@pytest.mark.parametrize("warps,group", [(1, 1), (4, 8), (6, 16), (8, 32)])
+def test_stereo_launch_shapes_give_identical_results(warps, group):
+    """The tuner's stereo knobs (warps per block, points per warp) change only the time: the pipeline's outputs stay
+    bit-identical to the oracle's for every shape."""
+    from xclean_b200 import _lib, synth
+    from xclean_b200.front.gpu_front import GpuFront
+    c = G.load_case("kitti1241")
+    cal = G.calib_of(c)
+    L, R = synth.sequence(synth.CAM_KITTI, 2, seed=5)
+    L, R = L.numpy(), R.numpy()
+    gf = GpuFront(1241, 376, cap=2048, max_frames=2)
+    try:
+        gf.set_calibration(cal, G.pattern())
+        gf.set_tuning(_lib.XCB_TUNE_STEREO_WARPS, warps)
+        gf.set_tuning(_lib.XCB_TUNE_STEREO_GROUP, group)
+        out = gf.pipeline(L, R, 2000, half=4, dlo=0, dhi=96, match_prev=False)
+        ref = O.frames(L, R, 2000, cal["q99"], cal, G.pattern(), half=4, dlo=0, dhi=96, cap=2048)
+        for f in range(2):
+            n = int(ref["counts"][f])
+            for k in ("d", "sig", "zn"):
+                assert G.same_bits(out[k][f, :n], ref[k][f, :n]), (f, k)
+            assert np.array_equal(out["ok"][f, :n], ref["ok"][f, :n])
+            assert G.same_bits(np.nan_to_num(out["dy"][f, :n], nan=-1e300),
+                               np.nan_to_num(ref["dy"][f, :n], nan=-1e300))
+        kp = c["kp0"].astype(np.float64)
+        lo, hi = np.zeros(len(kp), np.int64), np.full(len(kp), 127, np.int64)
+        d, s, ok, zn, ody = gf.stereo(c["left0"], c["right0"], kp, lo, hi, dy=0.25, band=2, half=5)
+        od, osg, ook, ozn, oody = O.stereo(c["left0"], c["right0"], kp, lo, hi, dy=0.25, band=2, half=5)
+        assert G.same_bits(d, od) and G.same_bits(s, osg) and np.array_equal(ok, ook) and G.same_bits(zn, ozn)
+        with pytest.raises(RuntimeError):
+            gf.set_tuning(_lib.XCB_TUNE_STEREO_GROUP, 33)
+    finally:
+        gf.close()

@@ -223,3 +223,22 @@ def test_predict_match_random_vs_oracle():
     want = O.mapmatch(kp, desc, uv0[sel], S0[sel], lmd[sel], lnd[sel], W, H)
     assert G.same_outputs((k[sel], d[sel], d2[sel]), want)
     assert len(sel) > 1000 and (want[0] >= 0).sum() > 500
+
+
+@pytest.mark.parametrize("lanes", [1, 2, 4, 8])
+def test_gate_lanes_give_identical_results(lanes):
+    """The tuner's knob (lanes per landmark in the gate) changes only the time: bit-identical outputs for every value,
+    on random frames with crowded cells and on the golden fixture's cases."""
+    from xclean_b200 import _lib
+    rng = np.random.default_rng(77)
+    W, H, N, L, D = 1241, 376, 2000, 3000, 3
+    kp, desc, uv, S, lmd, lnd = _random_case(rng, W, H, N, L, D)
+    mm = _mm(W, H)
+    try:
+        mm.set_tuning(_lib.XCB_TUNE_MM_LANES, lanes)
+        got = mm.match(kp, desc, uv, S, lmd, lnd, chi2=50.0)
+        with pytest.raises(RuntimeError):
+            mm.set_tuning(_lib.XCB_TUNE_MM_LANES, 3)
+    finally:
+        mm.close()
+    assert G.same_outputs(got, O.mapmatch(kp, desc, uv, S, lmd, lnd, W, H, 50.0))

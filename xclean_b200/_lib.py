@@ -56,6 +56,7 @@ _SIGS = {
     "xcb_front_pipeline_host_batches": (c_int, [P, P, P, c_int, c_int, c_int, c_int, c_int, c_int, c_int,
                                                 ctypes.POINTER(FrontBufs), P]),
     "xcb_front_last_launches": (c_int, [P]),
+    "xcb_front_set_tuning": (c_int, [P, c_int, c_int]),
     "xcb_front_sync_check": (c_int, [P, P]),
     "xcb_front_set_stage_timing": (c_int, [P, c_int]),
     "xcb_front_stage_times": (c_int, [P, P, P]),
@@ -71,6 +72,9 @@ class BaWindows(ctypes.Structure):
         "pr_m", "pr_nb", "pr_boff", "pr_soff", "pr_roff", "pr_blk", "pr_x0", "pr_S", "pr_r")]
 
 
+XCB_TUNE_MM_LANES = 1
+XCB_TUNE_STEREO_WARPS = 2
+XCB_TUNE_STEREO_GROUP = 3
 XCB_BA_FP64 = 0
 XCB_BA_MIXED = 1
 XCB_BA_NEWTON_POLISH = 0
@@ -128,6 +132,7 @@ class LbaProblem(ctypes.Structure):
 
 _SIGS.update({
     "xcb_mm_create": (c_int, [c_int, c_int, c_int, c_int, c_int, P]),
+    "xcb_mm_set_tuning": (c_int, [P, c_int, c_int]),
     "xcb_mm_destroy": (c_int, [P]),
     "xcb_mm_last_error": (ctypes.c_char_p, [P]),
     "xcb_mm_grid_dims": (c_int, [P, P, P]),

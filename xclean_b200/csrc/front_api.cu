@@ -98,6 +98,8 @@ struct xcb_front {
     };
     std::vector<GraphEntry> graphs;
     unsigned long long graph_clock;
+    // launch shapes chosen by the tuner (xcb_front_set_tuning; 0 = the built-in default)
+    int tune[XCB_TUNE_KNOBS];
     bool stage_timing;
     int last_launches;
 };
@@ -638,7 +640,8 @@ extern "C" int xcb_front_stereo_host(xcb_front* f, const uint8_t* left, const ui
     }
     CK(xcb_launch_stereo(f->d_left, f->d_right, Rs, 1, f->H, f->W, f->d_kpd, (const long long*)f->d_lo,
                          (const long long*)f->d_hi, n, nullptr, nullptr, 0, 0, 0, band, half, f->d_pd, f->d_psig,
-                         f->d_pok, f->d_pzn, f->d_pdy, f->d_err, st), "stereo");
+                         f->d_pok, f->d_pzn, f->d_pdy, f->d_err, f->tune[XCB_TUNE_STEREO_WARPS],
+                         f->tune[XCB_TUNE_STEREO_GROUP], st), "stereo");
     CK(cudaMemcpyAsync(d, f->d_pd, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
     CK(cudaMemcpyAsync(sig, f->d_psig, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
     CK(cudaMemcpyAsync(ok, f->d_pok, (size_t)n, cudaMemcpyDeviceToHost, st), "D2H");
@@ -767,7 +770,8 @@ static int enqueue_pipeline(xcb_front* f, const u8* left, const u8* right, int F
     if (rc) return rc;
     int* counts = f->d_counts_chain + 1;
     CK(xcb_launch_stereo(left, right, nullptr, F, f->H, f->W, nullptr, nullptr, nullptr, F, f->d_kp, counts, f->cap,
-                         dlo, dhi, 0, half, f->d_d, f->d_sig, f->d_ok, f->d_zn, f->d_dy, f->d_err, st), "stereo");
+                         dlo, dhi, 0, half, f->d_d, f->d_sig, f->d_ok, f->d_zn, f->d_dy, f->d_err,
+                         f->tune[XCB_TUNE_STEREO_WARPS], f->tune[XCB_TUNE_STEREO_GROUP], st), "stereo");
     CK(mark(ev, 6, st), "event");
     if (!match_prev) CK(cudaMemsetAsync(f->d_counts_chain, 0, sizeof(int), st), "memset");
     XcbHamPairs p;
@@ -849,6 +853,23 @@ extern "C" int xcb_front_set_stage_timing(xcb_front* f, int on)
     CK(cudaDeviceSynchronize(), "sync");
     if ((bool)on != f->stage_timing) drop_graphs(f);
     f->stage_timing = on != 0;
+    return XCB_OK;
+}
+
+extern "C" int xcb_front_set_tuning(xcb_front* f, int knob, int value)
+{
+    if (!f) return fail(nullptr, XCB_ERR_ARG, "set_tuning: null front");
+    if (knob == XCB_TUNE_STEREO_WARPS) {
+        if (value < 0 || value > 8) return fail(f, XCB_ERR_ARG, "set_tuning: stereo warps per block in 0..8");
+    } else if (knob == XCB_TUNE_STEREO_GROUP) {
+        if (value < 0 || value > 32) return fail(f, XCB_ERR_ARG, "set_tuning: stereo points per warp in 0..32");
+    } else {
+        return fail(f, XCB_ERR_ARG, "set_tuning: not a front knob");
+    }
+    if (f->tune[knob] != value) {
+        f->tune[knob] = value;
+        drop_graphs(f);            // the captured pipelines hold the old launch shapes
+    }
     return XCB_OK;
 }
 

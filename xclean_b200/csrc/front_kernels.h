@@ -53,7 +53,7 @@ cudaError_t xcb_launch_stereo(const uint8_t* L, const uint8_t* R8, const float* 
                               const double* kpd, const long long* dlo_a, const long long* dhi_a, int n,
                               const float* kpf, const int* counts, int cap, int dlo, int dhi, int band, int half,
                               double* od, double* osig, uint8_t* ook, double* ozn, double* ody, unsigned int* err,
-                              cudaStream_t st);
+                              int warps, int grp, cudaStream_t st);
 size_t xcb_stereo_smem_per_warp(int half, int band);
 cudaError_t xcb_launch_lkcheck(const double* As, const double* gs, int n, double* X, double* Inv, cudaStream_t st);
 

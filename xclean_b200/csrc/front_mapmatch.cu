@@ -37,9 +37,9 @@ extern void xcb_set_last_error(const std::string& m);
 #define MM_GRID 16            // mapmatch.py:30
 #define MM_GRID_T 1024        // threads of k_mm_grid
 #define MM_WARPS 8            // warps per CTA of k_mm_gate / k_mm_mutual
-#define MM_GROUP 2            // lanes per landmark in k_mm_gate (2 measured faster than 4 and 8: more landmarks in flight)
+#define MM_GROUP_DEFAULT 2    // lanes per landmark in k_mm_gate (1, 2, 4 or 8: the tuner's choice per device and
+                              // shape; 2 measured faster than 4 and 8 on B200: more landmarks in flight)
 #define MM_SLOTS 4            // claimant ids kept per keypoint (more claimants: the ordered scan of all claims)
-#define MM_LPB (MM_WARPS * 32 / MM_GROUP)   // landmarks per CTA of k_mm_gate
 // x / 16 and x * 0.0625 are the same correctly rounded double for every x (scaling by a power of two)
 #define MM_INV_GRID 0.0625
 #define MM_MAX_CELLS 49152    // cell counts of one frame live in shared memory (192 KB)
@@ -169,9 +169,10 @@ __device__ __forceinline__ int mm_ham(const uint4* p, const uint4* q)
 }
 
 // ----------------------------------------------------------------------------- gate (2 lanes per landmark, 128 per CTA)
-template <typename KT>
+template <typename KT, int MM_GROUP>
 __global__ void __launch_bounds__(MM_WARPS * 32, 4) k_mm_gate(MMArgs a)
 {
+    constexpr int MM_LPB = MM_WARPS * 32 / MM_GROUP;     // landmarks per CTA
     const int lane = threadIdx.x & 31, gl = lane & (MM_GROUP - 1), f = blockIdx.y;
     const int l = blockIdx.x * MM_LPB + (threadIdx.x / MM_GROUP);
     const bool in = l < mm_nlm(a, f);
@@ -346,6 +347,7 @@ __global__ void __launch_bounds__(MM_WARPS * 32) k_mm_mutual(MMArgs a)
 // ================================================================================================== handle + C ABI
 struct xcb_mm {
     int W, H, gw, gh, ncell, maxF, cap_kp, cap_lm;
+    int lanes;                // lanes per landmark in k_mm_gate (XCB_TUNE_MM_LANES)
     cudaStream_t stream;
     int* d_cstart;
     int* d_slot;
@@ -418,6 +420,7 @@ extern "C" int xcb_mm_create(int width, int height, int max_frames, int max_kp, 
     m->gh = (int)gh;
     m->ncell = (int)(gw * gh);
     m->maxF = max_frames;
+    m->lanes = MM_GROUP_DEFAULT;
     // the shared-memory opt-in is per kernel, not per handle: raise it to the largest grid any handle has asked for
     static XcbAttrOnce s_attr_f, s_attr_d;
     const int smem = (m->ncell + 1) * (int)sizeof(int);
@@ -454,6 +457,17 @@ extern "C" int xcb_mm_destroy(xcb_mm* m)
 
 extern "C" const char* xcb_mm_last_error(xcb_mm* m) { return m ? m->err.c_str() : xcb_last_error(); }
 
+extern "C" int xcb_mm_set_tuning(xcb_mm* m, int knob, int value)
+{
+    if (!m) return mm_fail(nullptr, XCB_ERR_ARG, "mm_set_tuning: null matcher");
+    if (knob != XCB_TUNE_MM_LANES) return mm_fail(m, XCB_ERR_ARG, "mm_set_tuning: not a matcher knob");
+    if (value == 0) value = MM_GROUP_DEFAULT;
+    if (value != 1 && value != 2 && value != 4 && value != 8)
+        return mm_fail(m, XCB_ERR_ARG, "mm_set_tuning: lanes per landmark must be 1, 2, 4 or 8");
+    m->lanes = value;
+    return XCB_OK;
+}
+
 extern "C" int xcb_mm_grid_dims(xcb_mm* m, int* gw, int* gh)
 {
     if (!m || !gw || !gh) return mm_fail(m, XCB_ERR_ARG, "mm_grid_dims: null argument");
@@ -476,14 +490,23 @@ static int mm_launch(xcb_mm* m, MMArgs& a, int F, bool kp_f32, cudaStream_t st)
     a.kcnt = m->d_kcnt;
     a.kslot = m->d_kslot;
     const size_t smem = (size_t)(m->ncell + 1) * sizeof(int);
-    const dim3 lg((a.lm_stride + MM_LPB - 1) / MM_LPB, F), lm((a.lm_stride + MM_WARPS * 32 - 1) / (MM_WARPS * 32), F);
+    const int grp = m->lanes, lpb = MM_WARPS * 32 / grp;
+    const dim3 lg((a.lm_stride + lpb - 1) / lpb, F), lm((a.lm_stride + MM_WARPS * 32 - 1) / (MM_WARPS * 32), F);
+#define MM_GATE(KT)                                                                                               \
+    switch (grp) {                                                                                                \
+        case 1: k_mm_gate<KT, 1><<<lg, MM_WARPS * 32, 0, st>>>(a); break;                                         \
+        case 4: k_mm_gate<KT, 4><<<lg, MM_WARPS * 32, 0, st>>>(a); break;                                         \
+        case 8: k_mm_gate<KT, 8><<<lg, MM_WARPS * 32, 0, st>>>(a); break;                                         \
+        default: k_mm_gate<KT, 2><<<lg, MM_WARPS * 32, 0, st>>>(a); break;                                        \
+    }
     if (kp_f32) {
         k_mm_grid<float><<<F, MM_GRID_T, smem, st>>>(a);
-        if (a.lm_stride > 0) k_mm_gate<float><<<lg, MM_WARPS * 32, 0, st>>>(a);
+        if (a.lm_stride > 0) MM_GATE(float)
     } else {
         k_mm_grid<double><<<F, MM_GRID_T, smem, st>>>(a);
-        if (a.lm_stride > 0) k_mm_gate<double><<<lg, MM_WARPS * 32, 0, st>>>(a);
+        if (a.lm_stride > 0) MM_GATE(double)
     }
+#undef MM_GATE
     if (a.lm_stride > 0) k_mm_mutual<<<lm, MM_WARPS * 32, 0, st>>>(a);
     MCK(cudaGetLastError(), "mapmatch launch");
     return XCB_OK;

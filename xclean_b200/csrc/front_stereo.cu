@@ -445,9 +445,10 @@ __global__ void __launch_bounds__(st_warps(HALF) * 32, 2) k_stereo(
     const double* __restrict__ kpd, const long long* __restrict__ dlo_a, const long long* __restrict__ dhi_a, int n,
     const float* __restrict__ kpf, const int* __restrict__ counts, int cap, int dlo_s, int dhi_s, int band,
     double* __restrict__ od, double* __restrict__ osig, u8* __restrict__ ook, double* __restrict__ ozn,
-    double* __restrict__ ody)
+    double* __restrict__ ody, int grp)
 {
-    constexpr int PW = 2 * HALF + 1, NPIX = PW * PW, NW = st_warps(HALF);
+    constexpr int PW = 2 * HALF + 1, NPIX = PW * PW;
+    const int NW = blockDim.x >> 5;                        // warps per block (at most st_warps(HALF))
     constexpr int LKR = PW + 2, LKW = PW + 2 * LK_MG + 2;
     static_assert(U8Win<HALF>::WWB <= 4 * (((MAXD + 2 * HALF) + 3) & ~3), "u8 rows fit the float32 window rows");
     static_assert(sizeof(StJob) == 64, "job record");
@@ -468,10 +469,10 @@ __global__ void __launch_bounds__(st_warps(HALF) * 32, 2) k_stereo(
     constexpr int KP = (NPIX + 31) / 32;                   // patch pixels per lane
 
     // ------------------------------------------------------------------------------------------- phase A: searches
-    const long long g0 = ((long long)blockIdx.x * NW + wid) * ST_GROUP;
+    const long long g0 = ((long long)blockIdx.x * NW + wid) * grp;     // grp <= ST_GROUP points per warp
     int njobs = 0;
 #pragma unroll 1
-    for (int gi = 0; gi < ST_GROUP; ++gi) {
+    for (int gi = 0; gi < grp; ++gi) {
         const long long p = g0 + gi;
         int f = 0;
         size_t oi;
@@ -903,16 +904,17 @@ static cudaError_t launch_stereo_t(const uint8_t* L, const uint8_t* R8, const fl
                                    const double* kpd, const long long* dlo_a, const long long* dhi_a, int n,
                                    const float* kpf, const int* counts, int cap, int dlo, int dhi, int band,
                                    double* od, double* osig, uint8_t* ook, double* ozn, double* ody, long long npts,
-                                   cudaStream_t st)
+                                   int warps, int grp, cudaStream_t st)
 {
-    constexpr int NW = st_warps(HALF);
+    const int NW = warps >= 1 && warps <= st_warps(HALF) ? warps : st_warps(HALF);
+    const int G = grp >= 1 && grp <= ST_GROUP ? grp : ST_GROUP;
     size_t pw = (xcb_stereo_smem_per_warp(HALF, band) + 15) & ~(size_t)15;
     size_t sm = pw * NW;
-    const long long per_block = (long long)NW * ST_GROUP;
+    const long long per_block = (long long)NW * G;
     long long nb = (npts + per_block - 1) / per_block;
     if (nb <= 0) return cudaSuccess;
     k_stereo<HALF, FLT><<<(unsigned)nb, NW * 32, sm, st>>>(L, R8, Rs, H, W, kpd, dlo_a, dhi_a, n, kpf, counts, cap,
-                                                            dlo, dhi, band, od, osig, ook, ozn, ody);
+                                                            dlo, dhi, band, od, osig, ook, ozn, ody, G);
     return cudaGetLastError();
 }
 
@@ -933,7 +935,7 @@ cudaError_t xcb_launch_stereo(const uint8_t* L, const uint8_t* R8, const float* 
                               const double* kpd, const long long* dlo_a, const long long* dhi_a, int n,
                               const float* kpf, const int* counts, int cap, int dlo, int dhi, int band, int half,
                               double* od, double* osig, uint8_t* ook, double* ozn, double* ody, unsigned int* err,
-                              cudaStream_t st)
+                              int warps, int grp, cudaStream_t st)
 {
     if (band < 0 || band > BAND_MAX) return cudaErrorInvalidValue;
     long long npts = kpd ? (long long)n : (long long)F * cap;
@@ -941,9 +943,9 @@ cudaError_t xcb_launch_stereo(const uint8_t* L, const uint8_t* R8, const float* 
     bool flt = Rs != nullptr;
 #define XCB_ST(HH)                                                                                                  \
     return flt ? launch_stereo_t<HH, true>(L, nullptr, Rs, H, W, kpd, dlo_a, dhi_a, nn, kpf, counts, cap, dlo, dhi,  \
-                                           band, od, osig, ook, ozn, ody, npts, st)                                 \
+                                           band, od, osig, ook, ozn, ody, npts, warps, grp, st)                     \
                : launch_stereo_t<HH, false>(L, R8, nullptr, H, W, kpd, dlo_a, dhi_a, nn, kpf, counts, cap, dlo, dhi, \
-                                            band, od, osig, ook, ozn, ody, npts, st);
+                                            band, od, osig, ook, ozn, ody, npts, warps, grp, st);
     switch (half) {
         case 3: XCB_ST(3)
         case 4: XCB_ST(4)

@@ -502,6 +502,10 @@ class GpuFront:
         self._chk(self.L.xcb_front_buffers(self._h, ctypes.byref(b)), "buffers")
         return {n: int(getattr(b, n) or 0) for n, _ in _lib.FrontBufs._fields_}
 
+    def set_tuning(self, knob, value):
+        """A launch-shape knob (xclean_b200.tune / XCB_TUNE_STEREO_*); results do not depend on it."""
+        self._chk(self.L.xcb_front_set_tuning(self._h, int(knob), int(value)), "set_tuning")
+
     def last_launches(self):
         return int(self.L.xcb_front_last_launches(self._h))
 

@@ -145,6 +145,10 @@ class MapMatcher:
         self.stats["matched"] += int((out_kp >= 0).sum())
         return uv, S, ok, depth, out_kp, out_d, out_d2
 
+    def set_tuning(self, knob, value):
+        """A launch-shape knob (xclean_b200.tune / XCB_TUNE_MM_LANES); results do not depend on it."""
+        self._chk(self.L.xcb_mm_set_tuning(self._h, int(knob), int(value)), "mapmatch.set_tuning")
+
     def match_dev(self, kp, nkp, desc, uv, S, lm_desc, lm_ndesc, nlm, chi2=CHI2_2_999, out=None, stream=0):
         """F frames in device memory (torch CUDA tensors): kp (F,Nk,2) float32, nkp (F,) int32, desc (F,Nk,32) uint8,
         uv (F,Nl,2) float64, S (F,Nl,2,2) float64, lm_desc (F,Nl,D,32) uint8, lm_ndesc (F,Nl) int64, nlm (F,) int32.
