@@ -883,16 +883,17 @@ def run_ba_large(args, dev, stream, ws_world, rank):
         bs = BatchSolver(wins, dev, hold=0)
     torch.cuda.synchronize()
     res = {}
-    for prec in ("mixed", "fp64"):
+    for prec, path in (("mixed", "large"), ("fp64", "large"), ("mixed_window", "window"), ("fp64_window", "window")):
+        pr = prec.split("_")[0]
         for _ in range(max(1, args.warmup)):
             bs.reset()
-            bs.solve(BA_ITERS, BA_LAM0, prec, stream=stream)
+            bs.solve(BA_ITERS, BA_LAM0, pr, stream=stream, path=path)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(args.steps):
             bs.reset()
-            bs.solve(BA_ITERS, BA_LAM0, prec, stream=stream)
+            bs.solve(BA_ITERS, BA_LAM0, pr, stream=stream, path=path)
         e1.record(stream)
         torch.cuda.synchronize()
         res[prec] = (D.max_over_ranks(e0.elapsed_time(e1) / args.steps, device=dev), bs.results())
@@ -901,9 +902,20 @@ def run_ba_large(args, dev, stream, ws_world, rank):
         dx_o, _c, _ok = BO.step(w.copy(), BA_LAM0, hold=0)
         n = 6 * w.Rwb.shape[0]
         errs.append(float(np.linalg.norm(res["mixed"][1]["dx0"][i][:n] - dx_o) / max(np.linalg.norm(dx_o), 1e-300)))
+    errs64 = []
+    for i, w in enumerate(wins):
+        dx_o, _c, _ok = BO.step(w.copy(), BA_LAM0, hold=0)
+        n = 6 * w.Rwb.shape[0]
+        errs64.append(float(np.linalg.norm(res["fp64"][1]["dx0"][i][:n] - dx_o) / max(np.linalg.norm(dx_o), 1e-300)))
     return {"value": ws_world * len(wins) / (res["mixed"][0] / 1e3), "unit": "windows/s",
+            "path": "large-window path (landmark passes of all windows on all SMs)",
             "fp64_batched_value": ws_world * len(wins) / (res["fp64"][0] / 1e3),
-            "ms_per_step": {"mixed_batched": res["mixed"][0], "fp64_batched": res["fp64"][0]},
+            "one_cta_per_window": {"mixed_value": ws_world * len(wins) / (res["mixed_window"][0] / 1e3),
+                                   "fp64_value": ws_world * len(wins) / (res["fp64_window"][0] / 1e3)},
+            "fp64_pose_step_rel_err_max": max(errs64),
+            "ms_per_step": {"mixed_batched": res["mixed"][0], "fp64_batched": res["fp64"][0],
+                            "mixed_one_cta_per_window": res["mixed_window"][0],
+                            "fp64_one_cta_per_window": res["fp64_window"][0]},
             "pose_step_rel_err_vs_fp64_oracle": {"mixed_max": max(errs), "mixed_median": float(np.median(errs))},
             "roofline": ba_roofline(wins, BA_ITERS, res["fp64"][0], res["mixed"][0], "k_ba_windows"),
             "config": {"workload": "32 windows x (20 keyframes, 6000 landmarks, 3-15 obs, 10% outliers), 5 LM "

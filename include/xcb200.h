@@ -276,6 +276,17 @@ size_t xcb_ba_scratch_bytes(int nw, int Lt);
 int xcb_ba_solve_windows_dev(const xcb_ba_windows* w, int max_slots, int iters, double lam0, int mode, double* stats,
                              double* dx0, int dx0_stride, void* scratch, size_t scratch_bytes, int grid, void* stream);
 
+/* The same LM iterations as xcb_ba_solve_windows_dev (no reference counterpart as one call: window.solve,
+   window.py:889-982, for every window of the batch), for batches of few, large windows: each iteration is a sequence
+   of launches whose landmark passes run over chunks of every window at once on all SMs (chunks: [nchunks][3] int32 in
+   device memory = window, first landmark, end (window-local); together they cover each window's landmarks once), and
+   whose Cholesky, solves and LM control run one CTA per window.  slots / Lt: the batch's slot and landmark totals.
+   Windows with a marginal prior are refused (XCB_ERR_ARG).  stats / dx0 as xcb_ba_solve_windows_dev. */
+size_t xcb_ba_large_scratch_bytes(int nw, int slots, int Lt);
+int xcb_ba_solve_windows_large_dev(const xcb_ba_windows* w, int slots, int Lt, const int32_t* chunks, int nchunks,
+                                   int max_slots, int iters, double lam0, int mode, double* stats, double* dx0,
+                                   int dx0_stride, void* scratch, size_t scratch_bytes, void* stream);
+
 /* Allocation-free form of xcb_ba_solve_windows_dev.  No counterpart in the reference.  It is for callers that cannot
    call cudaMalloc while running: a real-time loop whose latency budget rules out an allocation (which may synchronise
    the device), or a plugin whose host owns the device memory through its own allocator.  The caller passes inputs and

@@ -277,9 +277,47 @@ class BatchSolver:
         _lib.check(rc, None, "xcb_ba_solve_windows_free_dev")
         return stats[:self.nw]
 
-    def solve(self, iters=5, lam0=1e-4, precision="mixed", stream=None, grid=0):
-        """One persistent launch over every window (asynchronous on `stream`, torch's current stream by default)."""
+    LARGE_CHUNK = 256           # landmarks per chunk of the large-window path (LW_CHUNK in ba_window.cu)
+
+    def use_large(self):
+        """The large-window path pays when the batch has fewer windows than half the SMs and they are large (the
+        persistent kernel gives each window one SM); windows with a marginal prior always take the persistent one."""
+        if "pr_m" in self.host or self.nw == 0:
+            return False
+        sms = self.torch.cuda.get_device_properties(self.dev).multi_processor_count
+        return self.nw * 2 <= sms and int(self.host["L"].mean()) >= 4 * self.LARGE_CHUNK
+
+    def _large_setup(self):
+        if hasattr(self, "lchunks"):
+            return
+        ch = [(w, l0, min(l0 + self.LARGE_CHUNK, int(L))) for w, L in enumerate(self.host["L"])
+              for l0 in range(0, int(L), self.LARGE_CHUNK)]
+        ch.sort(key=lambda c: -(int(self.host["P"][c[0]]) ** 2))     # the windows with the largest systems first
+        self.lchunks = self.torch.tensor(ch if ch else [(0, 0, 0)], dtype=self.torch.int32, device=self.dev)
+        self.nchunks = len(ch)
+        nb = int(_lib.lib().xcb_ba_large_scratch_bytes(self.nw, int(self.host["Rwb"].shape[0]),
+                                                       int(self.host["lmp"].shape[0])))
+        self.lscratch = self.torch.zeros(nb, dtype=self.torch.uint8, device=self.dev)
+
+    def solve_large(self, iters=5, lam0=1e-4, precision="mixed", stream=None):
+        """window.solve for every window with the large-window path (xcb_ba_solve_windows_large_dev): the landmark
+        passes of all windows on all SMs, the per-window steps one CTA per window; asynchronous on `stream`."""
         torch = self.torch
+        self._large_setup()
+        s = stream if stream is not None else torch.cuda.current_stream(self.dev)
+        rc = _lib.lib().xcb_ba_solve_windows_large_dev(
+            ctypes.byref(self.desc), int(self.host["Rwb"].shape[0]), int(self.host["lmp"].shape[0]),
+            self.lchunks.data_ptr(), self.nchunks, self.max_slots, int(iters), float(lam0), PRECISIONS[precision],
+            self.stats.data_ptr(), self.dx0.data_ptr(), 6 * MAX_SLOTS, self.lscratch.data_ptr(),
+            self.lscratch.numel(), ctypes.c_void_p(s.cuda_stream or None))
+        _lib.check(rc, None, "xcb_ba_solve_windows_large_dev")
+
+    def solve(self, iters=5, lam0=1e-4, precision="mixed", stream=None, grid=0, path="window"):
+        """One persistent launch over every window (asynchronous on `stream`, torch's current stream by default).
+        path: "window" (one CTA per window), "large" (solve_large) or "auto" (use_large decides)."""
+        torch = self.torch
+        if path == "large" or (path == "auto" and self.use_large()):
+            return self.solve_large(iters, lam0, precision, stream)
         s = stream if stream is not None else torch.cuda.current_stream(self.dev)
         rc = _lib.lib().xcb_ba_solve_windows_dev(ctypes.byref(self.desc), self.max_slots, int(iters), float(lam0),
                                                  PRECISIONS[precision], self.stats.data_ptr(), self.dx0.data_ptr(),
@@ -374,10 +412,11 @@ class BatchSolver:
                 pf.lmp[:] = lmp[lo[i] + L:lo[i] + L + len(pf.host)]
 
 
-def solve_batch(windows, iters=5, lam0=1e-4, precision="mixed", hold=0, device="cuda"):
-    """window.solve for every window in one persistent device launch; windows are updated in place."""
+def solve_batch(windows, iters=5, lam0=1e-4, precision="mixed", hold=0, device="cuda", path="auto"):
+    """window.solve for every window on the device (one persistent launch, or the large-window path for a few large
+    windows: BatchSolver.solve's `path`); windows are updated in place."""
     bs = BatchSolver(windows, device, hold)
-    bs.solve(iters, lam0, precision)
+    bs.solve(iters, lam0, precision, path=path)
     bs.torch.cuda.synchronize(bs.dev)
     bs.unpack_into(windows)
     res = bs.results()

@@ -206,3 +206,31 @@ extern "C" int xcb_ba_solve_windows_noalloc(const xcb_ba_windows* w, int Lt, int
     return xcb_ba_solve_windows_dev(w, max_slots, iters, lam0, mode, stats, dx0, dx0_stride, base,
                                     XCB_BA_NOALLOC_SCRATCH_BYTES, grid, stream);
 }
+
+// ------------------------------------------------------------------------------------------------------------------
+// Large-window path: every window's landmark passes spread over all SMs in chunks (see ba_window.cu).
+extern "C" size_t xcb_ba_large_scratch_bytes(int nw, int slots, int Lt)
+{
+    return xcb_ba_large_scratch_bytes_impl(nw, slots, Lt);
+}
+
+extern "C" int xcb_ba_solve_windows_large_dev(const xcb_ba_windows* w, int slots, int Lt, const int32_t* chunks,
+                                              int nchunks, int max_slots, int iters, double lam0, int mode,
+                                              double* stats, double* dx0, int dx0_stride, void* scratch,
+                                              size_t scratch_bytes, void* stream)
+{
+    if (!w || !stats || !scratch || (!chunks && nchunks > 0)) return ba_fail(XCB_ERR_ARG, "ba_solve_large: null argument");
+    if (w->nw <= 0) return XCB_OK;
+    if (max_slots < 1 || max_slots > xcb_ba_max_slots())
+        return ba_fail(XCB_ERR_CAPACITY, "ba_solve_large: max_slots out of range (1..20)");
+    if (mode != XCB_BA_FP64 && mode != XCB_BA_MIXED) return ba_fail(XCB_ERR_ARG, "ba_solve_large: bad mode");
+    if (dx0 && dx0_stride < 6 * max_slots) return ba_fail(XCB_ERR_ARG, "ba_solve_large: dx0 stride too small");
+    if (w->pr_m) return ba_fail(XCB_ERR_ARG, "ba_solve_large: windows with a marginal prior take xcb_ba_solve_windows_dev");
+    if (slots < 0 || Lt < 0 || nchunks < 0 || iters < 0) return ba_fail(XCB_ERR_ARG, "ba_solve_large: negative size");
+    if (scratch_bytes < xcb_ba_large_scratch_bytes_impl(w->nw, slots, Lt))
+        return ba_fail(XCB_ERR_CAPACITY, "ba_solve_large: scratch smaller than xcb_ba_large_scratch_bytes");
+    cudaError_t e = xcb_launch_ba_large(*w, slots, Lt, chunks, nchunks, max_slots, iters, lam0, mode, stats, dx0,
+                                        dx0_stride, scratch, scratch_bytes, (cudaStream_t)stream);
+    if (e != cudaSuccess) return ba_fail(XCB_ERR_CUDA, cudaGetErrorString(e));
+    return XCB_OK;
+}

@@ -19,3 +19,11 @@ size_t xcb_ba_newton_smem_bytes(int maxP);
 cudaError_t xcb_launch_ba_newton(const XcbBaWindows& d, int max_slots, int mode, int steps, int maxit, double tol,
                                  const double* gpose, double* gtheta, double* gisig, double* gz, double* stats,
                                  double* lsc, int* counter, int grid, cudaStream_t st, size_t lsc_doubles);
+
+// the large-window path: the same LM iterations as xcb_launch_ba_windows, the landmark passes over chunks of every
+// window on all SMs (chunks: [nchunks][3] int32 on the device: window, first landmark, end), the per-window steps one
+// CTA per window
+size_t xcb_ba_large_scratch_bytes_impl(int nw, int slots, int Lt);
+cudaError_t xcb_launch_ba_large(const XcbBaWindows& d, int slots, int Lt, const int* chunks, int nchunks,
+                                int max_slots, int iters, double lam0, int mode, double* stats, double* dx0,
+                                int dx0_stride, void* scratch, size_t scratch_bytes, cudaStream_t st);

@@ -137,6 +137,7 @@ struct BaShared {
     int accepted;
     int overflow;
     int win;
+    int lb, le;             // the landmarks (window-local) the landmark passes of this CTA visit
 };
 
 // dynamic shared memory: [S64, packed lower, n(n+1)/2 doubles][region: FP32 packed lower S + FP32 warp scratch |
@@ -406,7 +407,7 @@ __device__ void pass_build(BaShared& sh, const XcbBaWindows& d, const SlotGeo<T>
     const int n = sh.w.n;
     WarpLm<T>& wl = wls[wid];
     double c_local = 0.0;
-    for (int l = wid; l < sh.w.L; l += BA_WARPS) {
+    for (int l = sh.lb + wid; l < sh.le; l += BA_WARPS) {
         const int gl = sh.w.lm0 + l;
         if (!d.lm_mask[gl]) continue;
         const int h = d.lm_host[gl];
@@ -501,7 +502,7 @@ __device__ void pass_refine(BaShared& sh, const XcbBaWindows& d, WarpLm<double>*
     }
     __syncthreads();
     double c_local = 0.0;
-    for (int l = wid; l < sh.w.L; l += BA_WARPS) {
+    for (int l = sh.lb + wid; l < sh.le; l += BA_WARPS) {
         const int gl = sh.w.lm0 + l;
         if (!d.lm_mask[gl]) continue;
         const int h = d.lm_host[gl];
@@ -586,7 +587,7 @@ __device__ void pass_backsub(BaShared& sh, const XcbBaWindows& d, WarpLm<double>
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     WarpLm<double>& wl = wls[wid];
     double c_dummy = 0.0;
-    for (int l = wid; l < sh.w.L; l += BA_WARPS) {
+    for (int l = sh.lb + wid; l < sh.le; l += BA_WARPS) {
         const int gl = sh.w.lm0 + l;
         if (!d.lm_mask[gl]) {
             if (lane < 3) lmp_trial[3 * gl + lane] = d.lmp[3 * gl + lane];
@@ -651,7 +652,7 @@ __device__ void pass_cost(BaShared& sh, const XcbBaWindows& d, const SlotGeo<dou
 {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     double c = 0.0;
-    for (int l = wid; l < sh.w.L; l += BA_WARPS) {
+    for (int l = sh.lb + wid; l < sh.le; l += BA_WARPS) {
         const int gl = sh.w.lm0 + l;
         if (!d.lm_mask[gl]) continue;
         const int h = d.lm_host[gl];
@@ -927,6 +928,7 @@ __global__ void __launch_bounds__(BA_THREADS, 1) k_ba_windows(XcbBaWindows d, in
         if (tid == 0) {
             BaWin& W = sh.w;
             W.P = d.P[w]; W.L = d.L[w]; W.n = 6 * W.P; W.hold = d.hold ? d.hold[w] : -1;
+            sh.lb = 0; sh.le = W.L;
             W.lm0 = d.lm_off[w]; W.s0 = d.slot_off[w];
             W.fx = d.cam[6 * w]; W.fy = d.cam[6 * w + 1]; W.cx = d.cam[6 * w + 2]; W.cy = d.cam[6 * w + 3];
             W.B = d.cam[6 * w + 4]; W.hk = d.cam[6 * w + 5];
@@ -1689,6 +1691,7 @@ __global__ void __launch_bounds__(BA_THREADS, 1) k_ba_newton(XcbBaWindows d, int
         if (tid == 0) {
             BaWin& W = sh.w;
             W.P = d.P[w]; W.L = d.L[w]; W.n = 6 * W.P; W.hold = d.hold ? d.hold[w] : -1;
+            sh.lb = 0; sh.le = W.L;
             W.lm0 = d.lm_off[w]; W.s0 = d.slot_off[w];
             W.fx = d.cam[6 * w]; W.fy = d.cam[6 * w + 1]; W.cx = d.cam[6 * w + 2]; W.cy = d.cam[6 * w + 3];
             W.B = d.cam[6 * w + 4]; W.hk = d.cam[6 * w + 5];
@@ -1884,6 +1887,431 @@ cudaError_t xcb_launch_ba_windows(const XcbBaWindows& d, int max_slots, int iter
     if (e != cudaSuccess) return e;
     k_ba_windows<<<grid, BA_THREADS, sm, st>>>(d, iters, lam0, mode, stats, dx0, dx0_stride, lmp_trial, counter,
                                                frz, trial_doubles);
+    return cudaGetLastError();
+}
+
+// =====================================================================================================================
+// Large windows on every SM.  The persistent kernel above gives each window one CTA, which leaves most of the GPU idle
+// when a batch holds fewer windows than SMs (32 windows of 20 keyframes and 6,000 landmarks use 32 of 148 SMs).  This
+// path runs the same LM iteration (the same landmark passes, the same reduced system, Cholesky, refinement, back-
+// substitution and accept / reject) as a sequence of launches: the landmark passes over chunks of LW_CHUNK landmarks
+// of every window at once (each CTA sums its chunk's share of the reduced system, the gradient and the cost in shared
+// memory, then adds it to the window's accumulators in global memory), and the per-window steps (Cholesky, solves,
+// LM control) one CTA per window.  The LM state lives in global memory (LwState) between the launches.
+// =====================================================================================================================
+#define LW_CHUNK 256
+#define LW_NT (BA_MAXN * (BA_MAXN + 1) / 2)
+
+struct LwState {
+    double lam, cost0, cur, ctot;
+    int accepted, status, bad, acc, conv, pad;
+};
+
+struct LwWork {
+    LwState* st;            // [nw]
+    double* S;              // [nw][LW_NT] reduced system (float in the mixed build: the first LW_NT floats)
+    double* g;              // [nw][BA_MAXN] build gradient (float in the mixed build)
+    double* cost;           // [nw] build cost (float64)
+    double* Lf;             // [nw][LW_NT] Cholesky factor
+    double* dx;             // [nw][BA_MAXN]
+    double* dmp;            // [nw][BA_MAXN]
+    double* g64;            // [nw][BA_MAXN] refinement: float64 gradient
+    double* y64;            // [nw][BA_MAXN] refinement: S_true dx
+    double* cost64;         // [nw] refinement: float64 cost
+    double* ctrial;         // [nw] trial cost
+    double* R2;             // [S][9] trial poses
+    double* p2;             // [S][3]
+    double* lmp_trial;      // [Lt][3]
+};
+
+// one chunk: landmarks [l0, l1) (window-local) of window w
+struct LwChunk {
+    int w, l0, l1;
+};
+
+__device__ void lw_load_window(BaShared& sh, const XcbBaWindows& d, int w)
+{
+    BaWin& W = sh.w;
+    W.P = d.P[w]; W.L = d.L[w]; W.n = 6 * W.P; W.hold = d.hold ? d.hold[w] : -1;
+    W.lm0 = d.lm_off[w]; W.s0 = d.slot_off[w];
+    W.fx = d.cam[6 * w]; W.fy = d.cam[6 * w + 1]; W.cx = d.cam[6 * w + 2]; W.cy = d.cam[6 * w + 3];
+    W.B = d.cam[6 * w + 4]; W.hk = d.cam[6 * w + 5];
+    for (int i = 0; i < 9; ++i) W.Rbc[i] = d.ext[12 * w + i];
+    for (int i = 0; i < 3; ++i) W.pbc[i] = d.ext[12 * w + 9 + i];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) W.Rcb[i * 3 + j] = W.Rbc[j * 3 + i];
+    double px[9] = {0.0, -W.pbc[2], W.pbc[1], W.pbc[2], 0.0, -W.pbc[0], -W.pbc[1], W.pbc[0], 0.0};
+    for (int i = 0; i < 9; ++i) W.Px[i] = px[i];
+    sh.overflow = 0;
+}
+
+// CTA set-up of a chunk kernel: the window's parameters, its current poses (or R / p when given) and their geometry.
+// -> false when the window is done (failed status)
+__device__ bool lw_setup(BaShared& sh, const XcbBaWindows& d, const LwWork& lw, const LwChunk& c, const double* R,
+                         const double* p)
+{
+    if (c.w < 0 || c.w >= d.nw) return false;
+    if (threadIdx.x == 0) {
+        lw_load_window(sh, d, c.w);
+        sh.lam = lw.st[c.w].lam;
+        sh.lb = max(c.l0, 0);
+        sh.le = min(c.l1, sh.w.L);          // a chunk never reaches past its window's landmarks
+        sh.win = lw.st[c.w].status;
+    }
+    __syncthreads();
+    if (sh.win != 0) return false;
+    const int P = sh.w.P, s0 = sh.w.s0;
+    for (int q = threadIdx.x; q < P * 9; q += blockDim.x) sh.Rwb[q] = (R ? R : d.Rwb)[9 * s0 + q];
+    for (int q = threadIdx.x; q < P * 3; q += blockDim.x) sh.pwb[q] = (p ? p : d.pwb)[3 * s0 + q];
+    __syncthreads();
+    slot_geo(sh, sh.Rwb, sh.pwb);
+    return true;
+}
+
+// the chunk's share of the reduced system (packed lower), gradient and cost, added to the window's accumulators
+template <typename T>
+__global__ void __launch_bounds__(BA_THREADS, 1) k_lw_build(XcbBaWindows d, LwWork lw, const LwChunk* chunks)
+{
+    extern __shared__ __align__(16) unsigned char dsm[];
+    __shared__ BaShared sh;
+    const LwChunk c = chunks[blockIdx.x];
+    if (!lw_setup(sh, d, lw, c, nullptr, nullptr)) return;
+    const int n = sh.w.n, nt = n * (n + 1) / 2;
+    T* S = (T*)dsm;
+    WarpLm<T>* wl = (WarpLm<T>*)(dsm + ((sizeof(T) * (size_t)nt + 15) & ~(size_t)15));
+    T* gb;
+    if constexpr (sizeof(T) == 4) gb = sh.bf;
+    else gb = sh.g;
+    for (int q = threadIdx.x; q < nt; q += blockDim.x) S[q] = (T)0;
+    for (int q = threadIdx.x; q < n; q += blockDim.x) gb[q] = (T)0;
+    __syncthreads();
+    double cst = 0.0;
+    if constexpr (sizeof(T) == 4)
+        pass_build<T, true>(sh, d, sh.g32, S, gb, wl, &cst);
+    else
+        pass_build<T, true>(sh, d, sh.g64, S, gb, wl, &cst);
+    const double ctot = block_sum_red(sh);
+    T* Sg = (T*)(lw.S + (size_t)c.w * LW_NT);
+    T* gg = (T*)(lw.g + (size_t)c.w * BA_MAXN);
+    for (int q = threadIdx.x; q < nt; q += blockDim.x)
+        if (S[q] != (T)0) atomicAdd(&Sg[q], S[q]);
+    for (int q = threadIdx.x; q < n; q += blockDim.x) atomicAdd(&gg[q], gb[q]);
+    if (threadIdx.x == 0) {
+        atomicAdd(&lw.cost[c.w], ctot);
+        if (sh.overflow) atomicExch(&lw.st[c.w].status, -2);
+    }
+}
+
+// per window: hold, damping, Cholesky, the first solve (the build's float32 right-hand side in the mixed mode)
+template <typename T>
+__global__ void __launch_bounds__(BA_THREADS, 1) k_lw_solve(XcbBaWindows d, LwWork lw, int mode, int it)
+{
+    extern __shared__ __align__(16) unsigned char dsm[];
+    __shared__ BaShared sh;
+    const int w = blockIdx.x, tid = threadIdx.x;
+    LwState& st = lw.st[w];
+    if (tid == 0) { lw_load_window(sh, d, w); sh.lam = st.lam; sh.win = st.status; }
+    __syncthreads();
+    if (sh.win != 0) return;
+    const int n = sh.w.n, nt = n * (n + 1) / 2;
+    double* S64 = (double*)dsm;
+    const T* Sg = (const T*)(lw.S + (size_t)w * LW_NT);
+    const T* gg = (const T*)(lw.g + (size_t)w * BA_MAXN);
+    for (int q = tid; q < nt; q += blockDim.x) S64[q] = (double)Sg[q];
+    for (int q = tid; q < n; q += blockDim.x) sh.rhs[q] = (double)gg[q];
+    __syncthreads();
+    const int hs = sh.w.hold, P = sh.w.P;
+    if (hs >= 0 && hs < P) {
+        for (int q = tid; q < 6 * n; q += blockDim.x) {
+            const int i = 6 * hs + q / n, j = q % n;
+            S64[i >= j ? tri(i, j) : tri(j, i)] = 0.0;
+        }
+        __syncthreads();
+        for (int q = tid; q < 6; q += blockDim.x) { S64[tri(6 * hs + q, 6 * hs + q)] = 1.0; sh.rhs[6 * hs + q] = 0.0; }
+        __syncthreads();
+    }
+    double* dmp = lw.dmp + (size_t)w * BA_MAXN;
+    for (int q = tid; q < n; q += blockDim.x) {
+        const double dg = S64[tri(q, q)];
+        sh.dmp[q] = sh.lam * dg + 1e-9;
+        S64[tri(q, q)] = dg + sh.dmp[q];
+        sh.dx[q] = -sh.rhs[q];
+        dmp[q] = sh.dmp[q];
+    }
+    __syncthreads();
+    const int bad = chol_factor(S64, n);
+    if (!bad) chol_solve(S64, n, sh.dx);
+    double* dx = lw.dx + (size_t)w * BA_MAXN;
+    double* Lf = lw.Lf + (size_t)w * LW_NT;
+    for (int q = tid; q < n; q += blockDim.x) dx[q] = bad ? 0.0 : sh.dx[q];
+    if (!bad)
+        for (int q = tid; q < nt; q += blockDim.x) Lf[q] = S64[q];
+    for (int q = tid; q < n; q += blockDim.x) { lw.g64[(size_t)w * BA_MAXN + q] = 0.0; lw.y64[(size_t)w * BA_MAXN + q] = 0.0; }
+    if (tid == 0) {
+        st.bad = bad ? 1 : 0;
+        st.conv = 0;
+        lw.cost64[w] = 0.0;
+        lw.ctrial[w] = 0.0;
+        if (mode != XCB_BA_MIXED) st.ctot = lw.cost[w];      // the float64 build's cost
+    }
+}
+
+// the float64 refinement pass over a chunk: its share of the gradient (first pass), of S_true dx and of the cost
+__global__ void __launch_bounds__(BA_THREADS, 1) k_lw_refine(XcbBaWindows d, LwWork lw, const LwChunk* chunks, int rf)
+{
+    extern __shared__ __align__(16) unsigned char dsm[];
+    __shared__ BaShared sh;
+    const LwChunk c = chunks[blockIdx.x];
+    if (c.w < 0 || c.w >= d.nw) return;
+    const LwState& st = lw.st[c.w];
+    if (rf > 0 && (st.bad || st.conv)) return;
+    if (!lw_setup(sh, d, lw, c, nullptr, nullptr)) return;
+    const int n = sh.w.n;
+    for (int q = threadIdx.x; q < n; q += blockDim.x) sh.dx[q] = lw.dx[(size_t)c.w * BA_MAXN + q];
+    __syncthreads();
+    WarpLm<double>* wl = (WarpLm<double>*)dsm;
+    pass_refine(sh, d, wl, rf == 0);
+    const double ctot = block_sum_red(sh);
+    for (int q = threadIdx.x; q < n; q += blockDim.x) {
+        if (rf == 0) atomicAdd(&lw.g64[(size_t)c.w * BA_MAXN + q], sh.g[q]);
+        atomicAdd(&lw.y64[(size_t)c.w * BA_MAXN + q], sh.y[q]);
+    }
+    if (rf == 0 && threadIdx.x == 0) atomicAdd(&lw.cost64[c.w], ctot);
+}
+
+// per window: the refinement's correction (residual of the float64 normal equations, solved with the factor)
+__global__ void __launch_bounds__(BA_THREADS, 1) k_lw_refine_solve(XcbBaWindows d, LwWork lw, int rf)
+{
+    extern __shared__ __align__(16) unsigned char dsm[];
+    __shared__ BaShared sh;
+    __shared__ double nrm[2];
+    const int w = blockIdx.x, tid = threadIdx.x;
+    LwState& st = lw.st[w];
+    if (st.status != 0) return;
+    if (tid == 0 && rf == 0) st.ctot = lw.cost64[w];
+    if (st.bad || st.conv) return;
+    const int n = 6 * d.P[w], nt = n * (n + 1) / 2, hs = d.hold ? d.hold[w] : -1;
+    double* L = (double*)dsm;
+    const double* Lf = lw.Lf + (size_t)w * LW_NT;
+    for (int q = tid; q < nt; q += blockDim.x) L[q] = Lf[q];
+    double* dx = lw.dx + (size_t)w * BA_MAXN;
+    double* y = lw.y64 + (size_t)w * BA_MAXN;
+    for (int q = tid; q < n; q += blockDim.x) {
+        double r = -lw.g64[(size_t)w * BA_MAXN + q] - y[q] - lw.dmp[(size_t)w * BA_MAXN + q] * dx[q];
+        if (hs >= 0 && q / 6 == hs) r = 0.0;
+        sh.rhs[q] = r;
+    }
+    __syncthreads();
+    chol_solve(L, n, sh.rhs);
+    if (tid == 0) {
+        double a = 0.0, b = 0.0;
+        for (int q = 0; q < n; ++q) { a += sh.rhs[q] * sh.rhs[q]; b += dx[q] * dx[q]; }
+        nrm[0] = a; nrm[1] = b;
+    }
+    __syncthreads();
+    for (int q = tid; q < n; q += blockDim.x) { dx[q] += sh.rhs[q]; y[q] = 0.0; }
+    if (tid == 0 && !(nrm[0] > 1e-18 * nrm[1])) st.conv = 1;
+}
+
+// per window: the trial poses (R Exp(dphi), p + dp) and the first iteration's step
+__global__ void k_lw_trial(XcbBaWindows d, LwWork lw, int it, double* dx0, int dx0_stride)
+{
+    const int w = blockIdx.x;
+    const LwState& st = lw.st[w];
+    if (st.status != 0 || st.bad) return;
+    const int P = d.P[w], s0 = d.slot_off[w];
+    const double* dx = lw.dx + (size_t)w * BA_MAXN;
+    if (it == 0 && dx0)
+        for (int q = threadIdx.x; q < 6 * P; q += blockDim.x) dx0[(size_t)w * dx0_stride + q] = dx[q];
+    for (int s = threadIdx.x; s < P; s += blockDim.x) {
+        double Re[9];
+        so3_exp(dx + 6 * s, Re);
+        const double* R = d.Rwb + 9 * (s0 + s);
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+                lw.R2[9 * (s0 + s) + 3 * i + j] = R[3 * i] * Re[j] + R[3 * i + 1] * Re[3 + j] + R[3 * i + 2] * Re[6 + j];
+        for (int i = 0; i < 3; ++i) lw.p2[3 * (s0 + s) + i] = d.pwb[3 * (s0 + s) + i] + dx[6 * s + 3 + i];
+    }
+}
+
+// the chunk's back-substitution (trial landmark states) and its share of the trial cost
+__global__ void __launch_bounds__(BA_THREADS, 1) k_lw_backsub(XcbBaWindows d, LwWork lw, const LwChunk* chunks)
+{
+    extern __shared__ __align__(16) unsigned char dsm[];
+    __shared__ BaShared sh;
+    const LwChunk c = chunks[blockIdx.x];
+    if (c.w < 0 || c.w >= d.nw || lw.st[c.w].bad) return;
+    if (!lw_setup(sh, d, lw, c, nullptr, nullptr)) return;
+    const int n = sh.w.n;
+    for (int q = threadIdx.x; q < n; q += blockDim.x) sh.dx[q] = lw.dx[(size_t)c.w * BA_MAXN + q];
+    __syncthreads();
+    WarpLm<double>* wl = (WarpLm<double>*)dsm;
+    pass_backsub(sh, d, wl, lw.lmp_trial);
+    __syncthreads();
+    const int P = sh.w.P, s0 = sh.w.s0;
+    for (int q = threadIdx.x; q < P * 9; q += blockDim.x) sh.R2[q] = lw.R2[9 * s0 + q];
+    for (int q = threadIdx.x; q < P * 3; q += blockDim.x) sh.p2[q] = lw.p2[3 * s0 + q];
+    __syncthreads();
+    slot_geo(sh, sh.R2, sh.p2);
+    pass_cost(sh, d, sh.g64, lw.lmp_trial);
+    const double ct = block_sum_red(sh);
+    if (threadIdx.x == 0) atomicAdd(&lw.ctrial[c.w], ct);
+}
+
+// per window: accept / reject (window.solve's rule), the poses committed, the next iteration's accumulators cleared
+__global__ void k_lw_accept(XcbBaWindows d, LwWork lw, int it)
+{
+    const int w = blockIdx.x;
+    LwState& st = lw.st[w];
+    __shared__ int acc;
+    if (threadIdx.x == 0) {
+        acc = 0;
+        if (st.status == 0) {
+            const double ct = st.ctot;
+            if (it == 0) st.cost0 = ct;
+            if (st.bad) {
+                st.cur = ct;
+                st.lam *= 10.0;
+            } else {
+                const double cn = lw.ctrial[w];
+                acc = cn < ct;
+                st.cur = acc ? cn : ct;
+                if (acc) { st.lam = fmax(st.lam / 10.0, 1e-12); st.accepted += 1; }
+                else st.lam *= 10.0;
+            }
+        }
+        st.acc = acc;
+        lw.cost[w] = 0.0;
+    }
+    __syncthreads();
+    const int P = d.P[w], s0 = d.slot_off[w];
+    if (acc) {
+        for (int q = threadIdx.x; q < P * 9; q += blockDim.x) d.Rwb[9 * s0 + q] = lw.R2[9 * s0 + q];
+        for (int q = threadIdx.x; q < P * 3; q += blockDim.x) d.pwb[3 * s0 + q] = lw.p2[3 * s0 + q];
+    }
+    for (int q = threadIdx.x; q < LW_NT; q += blockDim.x) lw.S[(size_t)w * LW_NT + q] = 0.0;
+    for (int q = threadIdx.x; q < BA_MAXN; q += blockDim.x) lw.g[(size_t)w * BA_MAXN + q] = 0.0;
+}
+
+// the accepted windows' landmarks take their trial states
+__global__ void k_lw_commit(XcbBaWindows d, LwWork lw, const LwChunk* chunks)
+{
+    const LwChunk c = chunks[blockIdx.x];
+    if (c.w < 0 || c.w >= d.nw || !lw.st[c.w].acc) return;
+    const int lm0 = d.lm_off[c.w], l0 = max(c.l0, 0), l1 = min(c.l1, d.L[c.w]);
+    for (int q = 3 * l0 + threadIdx.x; q < 3 * l1; q += blockDim.x)
+        d.lmp[3 * lm0 + q] = lw.lmp_trial[3 * lm0 + q];
+}
+
+__global__ void k_lw_init(XcbBaWindows d, LwWork lw, double lam0)
+{
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= d.nw) return;
+    LwState& st = lw.st[w];
+    st.lam = lam0; st.cost0 = 0.0; st.cur = 0.0; st.ctot = 0.0;
+    st.accepted = 0; st.bad = 0; st.acc = 0; st.conv = 0;
+    st.status = (d.P[w] > BA_MAXP || d.P[w] < 1) ? -1 : 0;
+    lw.cost[w] = 0.0;
+}
+
+__global__ void k_lw_final(XcbBaWindows d, LwWork lw, double* stats, int iters)
+{
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= d.nw) return;
+    const LwState& st = lw.st[w];
+    stats[8 * w + 0] = st.cost0;
+    stats[8 * w + 1] = st.cur;
+    stats[8 * w + 2] = st.accepted;
+    stats[8 * w + 3] = st.lam;
+    stats[8 * w + 4] = st.status;
+    stats[8 * w + 5] = iters;
+}
+
+size_t xcb_ba_large_scratch_bytes_impl(int nw, int S, int Lt)
+{
+    const size_t W = (size_t)(nw > 0 ? nw : 1);
+    size_t b = 0;
+    b += W * sizeof(LwState);
+    b += W * LW_NT * 8 * 2;                     // S, Lf
+    b += W * BA_MAXN * 8 * 5;                   // g, dx, dmp, g64, y64
+    b += W * 8 * 3;                             // cost, cost64, ctrial
+    b += (size_t)(S > 0 ? S : 1) * 12 * 8;      // R2, p2
+    b += (size_t)(Lt > 0 ? Lt : 1) * 3 * 8;     // lmp_trial
+    return b + 16 * 256;
+}
+
+static size_t lw_build_smem(int maxP, bool mixed)
+{
+    const int n = 6 * maxP, nt = n * (n + 1) / 2;
+    return mixed ? ((4 * (size_t)nt + 15) & ~(size_t)15) + sizeof(WarpLm<float>) * BA_WARPS
+                 : ((8 * (size_t)nt + 15) & ~(size_t)15) + sizeof(WarpLm<double>) * BA_WARPS;
+}
+
+cudaError_t xcb_launch_ba_large(const XcbBaWindows& d, int slots, int Lt, const int* chunks, int nchunks,
+                                int max_slots, int iters, double lam0, int mode, double* stats, double* dx0,
+                                int dx0_stride, void* scratch, size_t scratch_bytes, cudaStream_t st)
+{
+    if (scratch_bytes < xcb_ba_large_scratch_bytes_impl(d.nw, slots, Lt)) return cudaErrorInvalidValue;
+    char* p = (char*)scratch;
+    auto take = [&](size_t bytes) {
+        char* r = p;
+        p += (bytes + 255) & ~(size_t)255;
+        return r;
+    };
+    const size_t W = (size_t)d.nw;
+    LwWork lw;
+    lw.st = (LwState*)take(W * sizeof(LwState));
+    lw.S = (double*)take(W * LW_NT * 8);
+    lw.Lf = (double*)take(W * LW_NT * 8);
+    lw.g = (double*)take(W * BA_MAXN * 8);
+    lw.dx = (double*)take(W * BA_MAXN * 8);
+    lw.dmp = (double*)take(W * BA_MAXN * 8);
+    lw.g64 = (double*)take(W * BA_MAXN * 8);
+    lw.y64 = (double*)take(W * BA_MAXN * 8);
+    lw.cost = (double*)take(W * 8);
+    lw.cost64 = (double*)take(W * 8);
+    lw.ctrial = (double*)take(W * 8);
+    lw.R2 = (double*)take((size_t)slots * 9 * 8);
+    lw.p2 = (double*)take((size_t)slots * 3 * 8);
+    lw.lmp_trial = (double*)take((size_t)Lt * 3 * 8);
+    if ((size_t)(p - (char*)scratch) > scratch_bytes) return cudaErrorInvalidValue;
+    const bool mixed = mode == XCB_BA_MIXED;
+    const int n = 6 * max_slots, nt = n * (n + 1) / 2;
+    const size_t sm_build = lw_build_smem(max_slots, mixed), sm_sys = 8 * (size_t)nt;
+    const size_t sm_pass = sizeof(WarpLm<double>) * BA_WARPS;
+    static XcbAttrOnce a_bf, a_bd, a_sf, a_sd, a_rf, a_rs, a_bs;
+    cudaError_t e = cudaSuccess;
+    if (e == cudaSuccess) e = xcb_smem_attr_once(a_bf, (const void*)k_lw_build<float>, (int)lw_build_smem(BA_MAXP, true));
+    if (e == cudaSuccess) e = xcb_smem_attr_once(a_bd, (const void*)k_lw_build<double>, (int)lw_build_smem(BA_MAXP, false));
+    if (e == cudaSuccess) e = xcb_smem_attr_once(a_sf, (const void*)k_lw_solve<float>, 8 * LW_NT);
+    if (e == cudaSuccess) e = xcb_smem_attr_once(a_sd, (const void*)k_lw_solve<double>, 8 * LW_NT);
+    if (e == cudaSuccess) e = xcb_smem_attr_once(a_rf, (const void*)k_lw_refine, (int)sm_pass);
+    if (e == cudaSuccess) e = xcb_smem_attr_once(a_rs, (const void*)k_lw_refine_solve, 8 * LW_NT);
+    if (e == cudaSuccess) e = xcb_smem_attr_once(a_bs, (const void*)k_lw_backsub, (int)sm_pass);
+    if (e != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(lw.S, 0, W * LW_NT * 8, st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(lw.g, 0, W * BA_MAXN * 8, st)) != cudaSuccess) return e;
+    const LwChunk* ch = (const LwChunk*)chunks;
+    const unsigned nw = (unsigned)d.nw, nc = (unsigned)nchunks;
+    k_lw_init<<<(nw + 127) / 128, 128, 0, st>>>(d, lw, lam0);
+    for (int it = 0; it < iters; ++it) {
+        if (mixed) {
+            k_lw_build<float><<<nc, BA_THREADS, sm_build, st>>>(d, lw, ch);
+            k_lw_solve<float><<<nw, BA_THREADS, sm_sys, st>>>(d, lw, mode, it);
+            for (int rf = 0; rf < BA_REFINE_MAX; ++rf) {
+                k_lw_refine<<<nc, BA_THREADS, sm_pass, st>>>(d, lw, ch, rf);
+                k_lw_refine_solve<<<nw, BA_THREADS, sm_sys, st>>>(d, lw, rf);
+            }
+        } else {
+            k_lw_build<double><<<nc, BA_THREADS, sm_build, st>>>(d, lw, ch);
+            k_lw_solve<double><<<nw, BA_THREADS, sm_sys, st>>>(d, lw, mode, it);
+        }
+        k_lw_trial<<<nw, 64, 0, st>>>(d, lw, it, dx0, dx0_stride);
+        k_lw_backsub<<<nc, BA_THREADS, sm_pass, st>>>(d, lw, ch);
+        k_lw_accept<<<nw, 256, 0, st>>>(d, lw, it);
+        k_lw_commit<<<nc, 256, 0, st>>>(d, lw, ch);
+    }
+    k_lw_final<<<(nw + 127) / 128, 128, 0, st>>>(d, lw, stats, iters);
     return cudaGetLastError();
 }
 
