@@ -38,6 +38,7 @@ extern "C" {
 #define XCB_DEVERR_GREEDY_ROUNDS 1u
 #define XCB_DEVERR_STEREO_SMEM 2u
 #define XCB_DEVERR_CHOL_NOT_PD 4u
+#define XCB_DEVERR_TC_WAIT 8u          /* a tensor-core completion wait ran out (the kernel gave up, results invalid) */
 
 const char* xcb_last_error(void);
 int xcb_version(void);
@@ -256,12 +257,16 @@ typedef struct {
 #define XCB_BA_FP64 0           /* everything in float64: the plain form */
 #define XCB_BA_MIXED 1          /* FP32 linearisation + Schur, FP64 Cholesky, FP64 refinement (to 1e-9, <= 3 steps) */
 #define XCB_BA_LINEARISE 2      /* internal: one float64 linearisation, the reduced system exported (no step) */
+#define XCB_BA_MIXED_NOTC 3     /* large-window path only: XCB_BA_MIXED with the Schur term scattered on the CUDA
+                                   cores instead of accumulated on the tensor cores (for comparison) */
 /* per-window status (stats [w][4] of the window solves, stats [w][3] of the Newton calls) when the scratch cannot
    hold the batch's per-landmark records; the kernel counts the landmarks from the windows themselves (lm_off + L),
    writes nothing else and leaves the state unchanged */
 #define XCB_BA_STATUS_SCRATCH (-3)
 /* per-window status of the Newton / adjoint calls for a window with a marginal prior (not supported there) */
 #define XCB_BA_STATUS_PRIOR (-4)
+/* per-window status of the large-window path when a tensor-core completion wait ran out (the window is not solved) */
+#define XCB_BA_STATUS_TC (-5)
 
 /* Device scratch the batched solve needs for `Lt` landmarks: the work counter, the trial landmark states and, for the
    float64 mode, each landmark's back-substitution record (118 doubles: ~0.95 kB per landmark).  A smaller scratch
@@ -286,6 +291,13 @@ size_t xcb_ba_large_scratch_bytes(int nw, int slots, int Lt);
 int xcb_ba_solve_windows_large_dev(const xcb_ba_windows* w, int slots, int Lt, const int32_t* chunks, int nchunks,
                                    int max_slots, int iters, double lam0, int mode, double* stats, double* dx0,
                                    int dx0_stride, void* scratch, size_t scratch_bytes, void* stream);
+
+/* The dense Gram product D = U U^T on the tensor cores (no reference counterpart: the contraction of the Schur term
+   S -= W V^-1 W^T = U U^T, U = W chol(V^-1), that the large-window path's mixed-precision build runs per chunk):
+   U (n x K, row-major float32, device), n <= 128; D (n x n, row-major, device) written.  tcgen05 kind::tf32 MMAs with
+   every operand split into its TF32 rounding and remainder (hi hi^T + hi lo^T + lo hi^T: float32 accuracy), FP32
+   accumulation in tensor memory.  err (device word, may be NULL): XCB_DEVERR_TC_WAIT if a completion wait ran out. */
+int xcb_ba_gram_tc(const float* U, int n, int K, float* D, unsigned int* err, void* stream);
 
 /* Allocation-free form of xcb_ba_solve_windows_dev.  No counterpart in the reference.  It is for callers that cannot
    call cudaMalloc while running: a real-time loop whose latency budget rules out an allocation (which may synchronise

@@ -85,6 +85,7 @@ XCB_BA_STATUS_PRIOR = -4
 _SIGS.update({
     "xcb_ba_scratch_bytes": (c_size_t, [c_int, c_int]),
     "xcb_ba_large_scratch_bytes": (c_size_t, [c_int, c_int, c_int]),
+    "xcb_ba_gram_tc": (c_int, [P, c_int, c_int, P, P, P]),
     "xcb_ba_solve_windows_large_dev": (c_int, [ctypes.POINTER(BaWindows), c_int, c_int, P, c_int, c_int, c_int,
                                                c_double, c_int, P, P, c_int, P, c_size_t, P]),
     "xcb_ba_solve_windows_dev": (c_int, [ctypes.POINTER(BaWindows), c_int, c_int, c_double, c_int, P, P, c_int, P,

@@ -223,7 +223,8 @@ extern "C" int xcb_ba_solve_windows_large_dev(const xcb_ba_windows* w, int slots
     if (w->nw <= 0) return XCB_OK;
     if (max_slots < 1 || max_slots > xcb_ba_max_slots())
         return ba_fail(XCB_ERR_CAPACITY, "ba_solve_large: max_slots out of range (1..20)");
-    if (mode != XCB_BA_FP64 && mode != XCB_BA_MIXED) return ba_fail(XCB_ERR_ARG, "ba_solve_large: bad mode");
+    if (mode != XCB_BA_FP64 && mode != XCB_BA_MIXED && mode != XCB_BA_MIXED_NOTC)
+        return ba_fail(XCB_ERR_ARG, "ba_solve_large: bad mode");
     if (dx0 && dx0_stride < 6 * max_slots) return ba_fail(XCB_ERR_ARG, "ba_solve_large: dx0 stride too small");
     if (w->pr_m) return ba_fail(XCB_ERR_ARG, "ba_solve_large: windows with a marginal prior take xcb_ba_solve_windows_dev");
     if (slots < 0 || Lt < 0 || nchunks < 0 || iters < 0) return ba_fail(XCB_ERR_ARG, "ba_solve_large: negative size");

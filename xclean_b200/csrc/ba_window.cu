@@ -22,6 +22,7 @@
 // round trip per iteration (the reference returns to the host three times per LM iteration).
 #include "common.cuh"
 #include "ba_kernels.h"
+#include "ba_tc.cuh"
 
 #define BA_WARPS 10
 #define BA_THREADS (BA_WARPS * 32)
@@ -2002,6 +2003,227 @@ __global__ void __launch_bounds__(BA_THREADS, 1) k_lw_build(XcbBaWindows d, LwWo
     }
 }
 
+// The mixed build of a chunk with the Schur term on the tensor cores.  The landmarks go through in rounds of BA_WARPS,
+// one per warp: each warp adds its landmark's pose-pose blocks (the same slot, or a target with the host) and gradient
+// to the CTA's packed system with shared-memory atomics, as pass_build does, and writes the landmark's three Schur
+// columns U = Hlp^T C (Hll^-1 = C C^T; rows 6 s .. 6 s + 5 of its touched slots s, zero elsewhere) into the round's
+// TF32 hi / lo tile; one thread then adds U U^T of the tile to the tensor-memory accumulator (tc_issue), which runs
+// while the next round is linearised.  At the end the accumulator is subtracted from the packed system:
+// S = sum of pose-pose blocks - sum_l Hlp_l^T Hll_l^-1 Hlp_l.  A landmark whose Hll^-1 is not numerically positive
+// definite in float64 keeps the scatter of its Schur blocks.  -> false when a tensor-core wait ran out.
+__device__ bool pass_build_tc(BaShared& sh, const XcbBaWindows& d, float* S, float* gb, WarpLm<float>* wls,
+                              float* tiles, uint64_t* bar, uint32_t tmem, int* fail)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, tid = threadIdx.x;
+    WarpLm<float>& wl = wls[wid];
+    const SlotGeo<float>& G = sh.g32;
+    double c_local = 0.0;
+    int rounds = 0;
+    for (int base = sh.lb; base < sh.le; base += BA_WARPS, ++rounds) {
+        const int stg = rounds & 1;
+        float* hi = tiles + stg * 2 * TC_TILE_FLOATS;
+        float* lo = hi + TC_TILE_FLOATS;
+        if (rounds >= 2 && tid == 0 && !*fail && !tc_mbar_wait(&bar[stg], (uint32_t)(((rounds >> 1) - 1) & 1)))
+            *fail = 1;
+        __syncthreads();
+        if (*fail) break;
+        for (int q = tid; q < 2 * TC_TILE_FLOATS; q += blockDim.x) hi[q] = 0.0f;     // hi and lo are adjacent
+        __syncthreads();
+        const int l = base + wid;
+        const int gl = sh.w.lm0 + l;
+        if (l < sh.le && d.lm_mask[gl]) {
+            const int h = d.lm_host[gl];
+            float Hll[9], bl[3];
+            int nt;
+            const bool ok = lin_landmark<float>(sh, d, G, l, sh.lam, d.lmp, wl, Hll, bl, &nt, &c_local);
+            float Hi[9], HiB[3] = {0.0f, 0.0f, 0.0f};
+            double C[9] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+            bool tcl = false;
+            if (ok) {
+                inv3<float>(Hll, Hi);
+#pragma unroll
+                for (int i = 0; i < 3; ++i) HiB[i] = Hi[i * 3] * bl[0] + Hi[i * 3 + 1] * bl[1] + Hi[i * 3 + 2] * bl[2];
+                // C: the lower Cholesky factor of Hll^-1 in float64
+                double H64[9], I64[9];
+#pragma unroll
+                for (int i = 0; i < 9; ++i) H64[i] = (double)Hll[i];
+                inv3<double>(H64, I64);
+                const double a00 = I64[0];
+                if (a00 > 0.0) {
+                    C[0] = sqrt(a00);
+                    C[3] = I64[3] / C[0];
+                    C[6] = I64[6] / C[0];
+                    const double a11 = I64[4] - C[3] * C[3];
+                    if (a11 > 0.0) {
+                        C[4] = sqrt(a11);
+                        C[7] = (I64[7] - C[6] * C[3]) / C[4];
+                        const double a22 = I64[8] - C[6] * C[6] - C[7] * C[7];
+                        if (a22 > 0.0) { C[8] = sqrt(a22); tcl = true; }
+                    }
+                }
+                if (!tcl)
+                    for (int q = lane; q < nt * 18; q += 32) {
+                        const int a = q / 18, e = q % 18, i = e / 6, j = e % 6;
+                        wl.Tb[a][e] = Hi[i * 3] * wl.Hlp[a][j] + Hi[i * 3 + 1] * wl.Hlp[a][6 + j] +
+                                      Hi[i * 3 + 2] * wl.Hlp[a][12 + j];
+                    }
+                __syncwarp();
+            }
+            // gradient: sum_obs w Jx^T e - Hlp^T Hll^-1 bl
+            for (int q = lane; q < nt * 6; q += 32) {
+                const int a = q / 6, i = q % 6, s = wl.ts[a];
+                const int off = s == h ? OB_JH : OB_JT;
+                float acc = 0.0f;
+                for (unsigned m = wl.om[a]; m; m &= m - 1) {
+                    const float* ob = wl.ob[__ffs(m) - 1];
+                    acc += ob[OB_W] * (obj(ob, off, 0, i) * ob[OB_E] + obj(ob, off, 1, i) * ob[OB_E + 1]);
+                }
+                if (ok) acc -= wl.Hlp[a][i] * HiB[0] + wl.Hlp[a][6 + i] * HiB[1] + wl.Hlp[a][12 + i] * HiB[2];
+                atomicAdd(&gb[6 * s + i], acc);
+            }
+            if (ok && tcl) {
+                // the landmark's Schur columns 3 wid .. 3 wid + 2 of the round's tile
+                for (int q = lane; q < nt * 18; q += 32) {
+                    const int a = q / 18, e = q % 18, j = e / 3, c = e % 3;
+                    const float u = (float)(wl.Hlp[a][j] * C[c] + wl.Hlp[a][6 + j] * C[3 + c] +
+                                            wl.Hlp[a][12 + j] * C[6 + c]);
+                    float uh, ul;
+                    tc_split(u, uh, ul);
+                    const int o = tc_off(6 * wl.ts[a] + j, 3 * wid + c);
+                    hi[o] = uh;
+                    lo[o] = ul;
+                }
+            }
+            // the pose-pose blocks: (a, a) for every touched slot, (a, host) for the others; with the Schur blocks of
+            // a landmark that did not take the tensor-core path
+            int hx = 0;
+            for (int a = 0; a < nt; ++a)
+                if (wl.ts[a] == h) hx = a;
+            const bool full = ok && !tcl;
+            const int npair = full ? nt * (nt + 1) / 2 : (nt > 0 ? 2 * nt - 1 : 0);
+            for (int q = lane; q < npair * 36; q += 32) {
+                const int pr = q / 36, e = q % 36, i = e / 6, j = e % 6;
+                int a, b;
+                if (full) {
+                    a = (int)((sqrtf(8.0f * pr + 1.0f) - 1.0f) * 0.5f);
+                    while (a * (a + 1) / 2 > pr) --a;
+                    while ((a + 1) * (a + 2) / 2 <= pr) ++a;
+                    b = pr - a * (a + 1) / 2;
+                } else if (pr < nt) {
+                    a = b = pr;
+                } else {
+                    const int t = pr - nt < hx ? pr - nt : pr - nt + 1;
+                    a = t > hx ? t : hx;
+                    b = t > hx ? hx : t;
+                }
+                if (a == b && j > i) continue;
+                const int sa = wl.ts[a], sb = wl.ts[b];
+                float acc = 0.0f;
+                if (a == b) {
+                    const int off = sa == h ? OB_JH : OB_JT;
+                    for (unsigned m = wl.om[a]; m; m &= m - 1) {
+                        const float* ob = wl.ob[__ffs(m) - 1];
+                        acc += ob[OB_W] * (obj(ob, off, 0, i) * obj(ob, off, 0, j) + obj(ob, off, 1, i) * obj(ob, off, 1, j));
+                    }
+                } else if (sa == h || sb == h) {
+                    const int at = sa == h ? b : a;
+                    const int offa = sa == h ? OB_JH : OB_JT, offb = sb == h ? OB_JH : OB_JT;
+                    for (unsigned m = wl.om[at]; m; m &= m - 1) {
+                        const float* ob = wl.ob[__ffs(m) - 1];
+                        acc += ob[OB_W] * (obj(ob, offa, 0, i) * obj(ob, offb, 0, j) + obj(ob, offa, 1, i) * obj(ob, offb, 1, j));
+                    }
+                }
+                if (full)
+                    acc -= wl.Hlp[a][i] * wl.Tb[b][j] + wl.Hlp[a][6 + i] * wl.Tb[b][6 + j] + wl.Hlp[a][12 + i] * wl.Tb[b][12 + j];
+                atomicAdd(&S[tri(6 * sa + i, 6 * sb + j)], acc);
+            }
+            __syncwarp();
+        }
+        tc_fence_proxy();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            tc_issue(tmem, hi, lo, rounds > 0, &bar[stg]);
+        }
+    }
+    if (tid == 0 && !*fail && rounds >= 1) {
+        if (!tc_mbar_wait(&bar[(rounds - 1) & 1], (uint32_t)(((rounds - 1) >> 1) & 1))) *fail = 1;
+        if (rounds >= 2 && !tc_mbar_wait(&bar[(rounds - 2) & 1], (uint32_t)(((rounds - 2) >> 1) & 1))) *fail = 1;
+    }
+    __syncthreads();
+    tc_fence_after();
+    const int n = sh.w.n;
+    if (!*fail && rounds > 0 && wid < 4) {
+        const int r = 32 * wid + lane;
+        for (int c0 = 0; c0 < TC_M; c0 += 16) {
+            float v[16];
+            tc_ld16(tmem, wid, c0, v);
+            if (r < n)
+#pragma unroll
+                for (int i = 0; i < 16; ++i)
+                    if (c0 + i <= r) S[tri(r, c0 + i)] -= v[i];
+        }
+    }
+    __syncthreads();
+    c_local = warp_sum(c_local);
+    if (lane == 0) sh.red[wid] = c_local;
+    return !*fail;
+}
+
+// dynamic shared memory of k_lw_build_tc: [tiles: 2 stages x (hi, lo)][S packed float][WarpLm<float> per warp]
+static __host__ __device__ __forceinline__ size_t lw_tc_s_off() { return 4 * (size_t)TC_TILE_FLOATS * sizeof(float); }
+static size_t lw_build_tc_smem(int maxP)
+{
+    const int n = 6 * maxP, nt = n * (n + 1) / 2;
+    return lw_tc_s_off() + ((4 * (size_t)nt + 15) & ~(size_t)15) + sizeof(WarpLm<float>) * BA_WARPS;
+}
+
+__global__ void __launch_bounds__(BA_THREADS, 1) k_lw_build_tc(XcbBaWindows d, LwWork lw, const LwChunk* chunks)
+{
+    extern __shared__ __align__(1024) unsigned char dsm[];
+    __shared__ BaShared sh;
+    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ uint32_t tmem_base;
+    __shared__ int fail;
+    const LwChunk c = chunks[blockIdx.x];
+    if (!lw_setup(sh, d, lw, c, nullptr, nullptr)) return;
+    const int tid = threadIdx.x, wid = tid >> 5;
+    if (wid == 0) tc_alloc(&tmem_base, 128);
+    if (tid == 0) {
+        tc_mbar_init(&bar[0]);
+        tc_mbar_init(&bar[1]);
+        fail = 0;
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_base;
+    const int n = sh.w.n, nt = n * (n + 1) / 2;
+    float* tiles = (float*)dsm;
+    float* S = (float*)(dsm + lw_tc_s_off());
+    WarpLm<float>* wl = (WarpLm<float>*)(dsm + lw_tc_s_off() + ((4 * (size_t)nt + 15) & ~(size_t)15));
+    for (int q = tid; q < nt; q += blockDim.x) S[q] = 0.0f;
+    for (int q = tid; q < n; q += blockDim.x) sh.bf[q] = 0.0f;
+    __syncthreads();
+    const bool good = pass_build_tc(sh, d, S, sh.bf, wl, tiles, bar, tmem, &fail);
+    const double ctot = block_sum_red(sh);
+    float* Sg = (float*)(lw.S + (size_t)c.w * LW_NT);
+    float* gg = (float*)(lw.g + (size_t)c.w * BA_MAXN);
+    if (good) {
+        for (int q = tid; q < nt; q += blockDim.x)
+            if (S[q] != 0.0f) atomicAdd(&Sg[q], S[q]);
+        for (int q = tid; q < n; q += blockDim.x) atomicAdd(&gg[q], sh.bf[q]);
+    }
+    if (tid == 0) {
+        atomicAdd(&lw.cost[c.w], ctot);
+        if (sh.overflow) atomicExch(&lw.st[c.w].status, -2);
+        if (!good) atomicExch(&lw.st[c.w].status, XCB_BA_STATUS_TC);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (wid == 0) tc_dealloc(tmem, 128);
+}
+
 // per window: hold, damping, Cholesky, the first solve (the build's float32 right-hand side in the mixed mode)
 template <typename T>
 __global__ void __launch_bounds__(BA_THREADS, 1) k_lw_solve(XcbBaWindows d, LwWork lw, int mode, int it)
@@ -2275,12 +2497,15 @@ cudaError_t xcb_launch_ba_large(const XcbBaWindows& d, int slots, int Lt, const 
     lw.p2 = (double*)take((size_t)slots * 3 * 8);
     lw.lmp_trial = (double*)take((size_t)Lt * 3 * 8);
     if ((size_t)(p - (char*)scratch) > scratch_bytes) return cudaErrorInvalidValue;
-    const bool mixed = mode == XCB_BA_MIXED;
+    const bool mixed = mode == XCB_BA_MIXED || mode == XCB_BA_MIXED_NOTC;
+    const bool tc = mode == XCB_BA_MIXED;
+    const size_t sm_build_tc = lw_build_tc_smem(max_slots);
     const int n = 6 * max_slots, nt = n * (n + 1) / 2;
     const size_t sm_build = lw_build_smem(max_slots, mixed), sm_sys = 8 * (size_t)nt;
     const size_t sm_pass = sizeof(WarpLm<double>) * BA_WARPS;
-    static XcbAttrOnce a_bf, a_bd, a_sf, a_sd, a_rf, a_rs, a_bs;
+    static XcbAttrOnce a_bf, a_bd, a_sf, a_sd, a_rf, a_rs, a_bs, a_tc;
     cudaError_t e = cudaSuccess;
+    if (e == cudaSuccess) e = xcb_smem_attr_once(a_tc, (const void*)k_lw_build_tc, (int)lw_build_tc_smem(BA_MAXP));
     if (e == cudaSuccess) e = xcb_smem_attr_once(a_bf, (const void*)k_lw_build<float>, (int)lw_build_smem(BA_MAXP, true));
     if (e == cudaSuccess) e = xcb_smem_attr_once(a_bd, (const void*)k_lw_build<double>, (int)lw_build_smem(BA_MAXP, false));
     if (e == cudaSuccess) e = xcb_smem_attr_once(a_sf, (const void*)k_lw_solve<float>, 8 * LW_NT);
@@ -2296,7 +2521,10 @@ cudaError_t xcb_launch_ba_large(const XcbBaWindows& d, int slots, int Lt, const 
     k_lw_init<<<(nw + 127) / 128, 128, 0, st>>>(d, lw, lam0);
     for (int it = 0; it < iters; ++it) {
         if (mixed) {
-            k_lw_build<float><<<nc, BA_THREADS, sm_build, st>>>(d, lw, ch);
+            if (tc)
+                k_lw_build_tc<<<nc, BA_THREADS, sm_build_tc, st>>>(d, lw, ch);
+            else
+                k_lw_build<float><<<nc, BA_THREADS, sm_build, st>>>(d, lw, ch);
             k_lw_solve<float><<<nw, BA_THREADS, sm_sys, st>>>(d, lw, mode, it);
             for (int rf = 0; rf < BA_REFINE_MAX; ++rf) {
                 k_lw_refine<<<nc, BA_THREADS, sm_pass, st>>>(d, lw, ch, rf);
