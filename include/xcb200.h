@@ -292,6 +292,57 @@ int xcb_ba_solve_windows_large_dev(const xcb_ba_windows* w, int slots, int Lt, c
                                    int max_slots, int iters, double lam0, int mode, double* stats, double* dx0,
                                    int dx0_stride, void* scratch, size_t scratch_bytes, void* stream);
 
+/* The engine's state from which a window Problem is assembled (P1Engine._problem, src/xclean/vio/engine_live.py
+   :407-530, visual part).  All pointers are device memory.  The slots' observation lists are concatenated in slot
+   order (slot_n[i] observations for slot i). */
+typedef struct {
+    int P;                      /* slots (<= 64) */
+    const int64_t* sids;        /* [P] slot ids */
+    const int64_t* slot_n;      /* [P] observations of each slot */
+    long long M;                /* total observations */
+    const int64_t* lid;         /* [M] observed landmark id */
+    const double* uv;           /* [M][2] pixel */
+    const int64_t* cam;         /* [M] 0 left, 1 right */
+    const uint8_t* valid;       /* [M] */
+    const double* sig;          /* [M] the row's LK sigma */
+    int n_lm;                   /* landmark ids 0 .. n_lm - 1 */
+    const uint8_t* lm_alive;    /* [n_lm] */
+    const uint8_t* select;      /* [n_lm] the selection of alive landmarks (lm_select), or NULL for all */
+    const int64_t* lm_host;     /* [n_lm] host slot id */
+    const double* lm_p;         /* [n_lm][3] (a, b, rho) */
+    const double* lm_rho_meas;  /* [n_lm] */
+    const double* lm_sig_lk;    /* [n_lm] */
+    const double* lm_span;      /* [n_lm] */
+    int prior_mode;             /* 1: the "prior" stereo mode (inverse-depth priors); 0: "ur" */
+    double kappa_d, fB, sig_px;
+} xcb_ba_engine;
+/* The assembled window in the layout of one window of xcb_ba_windows (device memory, capacity n_lm landmarks and M
+   rows): counts [3] = L, the rows kept, and 1 when a landmark's host slot is not in the window (the reference raises
+   there); alive [n_lm] landmark ids in the window order; src [M][2] (slot, index in the slot) of every row. */
+typedef struct {
+    int32_t* counts;
+    int64_t* alive;
+    int32_t* src;
+    double* lmp;                /* [n_lm][3] */
+    int32_t* lm_host;           /* [n_lm] window slot */
+    uint8_t* lm_mask;           /* [n_lm] */
+    double* rho_meas;           /* [n_lm] */
+    double* rho_isig;           /* [n_lm] */
+    int32_t* lm_ob;             /* [n_lm + 1] */
+    int32_t* ob_pose;           /* [M] */
+    uint8_t* ob_cam;            /* [M] */
+    double* ob_z;               /* [M][2] */
+    double* ob_isig;            /* [M] */
+    uint8_t* ob_valid;          /* [M] */
+} xcb_ba_assembled;
+/* Assemble the window on the device (replaces P1Engine._problem's host work, engine_live.py:407-530: the alive and
+   selected landmarks in id order, their observations sorted stably by landmark, host slots, the inverse-depth
+   priors of the "prior" stereo mode, the rows' whitening; no marginal prior, no IMU, the pose-free landmarks kept as
+   ordinary ones).  Launches only (no synchronisation); the outputs feed xcb_ba_solve_windows_dev directly. */
+size_t xcb_ba_assemble_scratch_bytes(int n_lm, int M, int P);
+int xcb_ba_assemble_dev(const xcb_ba_engine* e, xcb_ba_assembled* out, void* scratch, size_t scratch_bytes,
+                        void* stream);
+
 /* The dense Gram product D = U U^T on the tensor cores (no reference counterpart: the contraction of the Schur term
    S -= W V^-1 W^T = U U^T, U = W chol(V^-1), that the large-window path's mixed-precision build runs per chunk):
    U (n x K, row-major float32, device), n <= 128; D (n x n, row-major, device) written.  tcgen05 kind::tf32 MMAs with

@@ -1,0 +1,80 @@
+"""The window Problem assembled on the device (xcb_ba_assemble_dev) against the reference's own P1Engine._problem
+outputs (tests/golden/assemble_golden.npz) bit for bit, and the assembled window solved on the device straight from
+those buffers: the same solve as the host-packed batch of the reference's Problem (first pose step to 1e-8 relative,
+cost to 1e-10, the same accepted count)."""
+import numpy as np
+import pytest
+
+from tests.test_assemble_oracle import CASES, GOLD, case_inputs
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(z, c):
+    import torch
+    from xclean_b200.backend.assemble import DeviceAssembler
+    a = case_inputs(z, c)
+    T = lambda x, dt: torch.as_tensor(np.ascontiguousarray(np.asarray(x).astype(dt)), device="cuda")
+    n_lm = int(a["n_lm"])
+    state = dict(sids=T(a["sids"], np.int64), slot_n=T(a["slot_n"], np.int64), lid=T(a["lid"], np.int64),
+                 uv=T(a["uv"], np.float64), cam=T(a["cam"], np.int64), valid=T(a["valid"], np.uint8),
+                 sig=T(a["sig"], np.float64), lm_alive=T(a["lm_alive"][:n_lm], np.uint8),
+                 lm_host=T(a["lm_host"][:n_lm], np.int64), lm_p=T(a["lm_p"][:n_lm], np.float64),
+                 lm_rho_meas=T(a["lm_rho_meas"][:n_lm], np.float64), lm_sig_lk=T(a["lm_sig_lk"][:n_lm], np.float64),
+                 lm_span=T(a["lm_span"][:n_lm], np.float64))
+    sel = None if a["select"] is None else T(a["select"][:n_lm], np.uint8)
+    asm = DeviceAssembler(len(a["sids"]), n_lm, len(a["lid"]))
+    asm.run(state, a["prior_mode"], a["kappa_d"], a["fB"], a["sig_px"], select=sel)
+    return asm, a
+
+
+@pytest.fixture(scope="module")
+def z():
+    return np.load(GOLD)
+
+
+@pytest.mark.parametrize("c", CASES)
+def test_device_assembly_is_bit_exact(z, c):
+    asm, _a = _run(z, c)
+    got = asm.to_host()
+    p = "c%d_" % c
+    assert np.array_equal(got["alive"], z[p + "alive"])
+    assert np.array_equal(got["src"], z[p + "src"])
+    for k in ("lmp", "lm_host", "lm_mask", "rho_meas", "rho_isig", "ob_start", "ob_pose", "ob_cam", "ob_z", "ob_isig",
+              "ob_valid"):
+        a, b = np.asarray(got[k]), np.asarray(z[p + "pb_" + k])
+        assert a.shape == b.shape and a.dtype == b.dtype, k
+        assert np.array_equal(a.view(np.uint8), np.ascontiguousarray(b).view(np.uint8)), k
+
+
+@pytest.mark.parametrize("c", CASES)
+def test_assembled_window_solves_on_the_device(z, c):
+    import torch
+    from tests.golden.make_golden_assemble import CASES as GEN, engine_state
+    from xclean_b200.backend import synth_ba as S
+    from xclean_b200.backend.ba import solve_batch
+    asm, a = _run(z, c)
+    K, L0, seed, mode, _sel = GEN[c]
+    st = engine_state(K, L0, seed, mode)
+    Rwb = np.stack([s["R"] for s in st.slots])
+    pwb = np.stack([s["p"] for s in st.slots])
+    cam = [st.fx, st.fy, st.cx, st.cy, st.B, 1.345]
+    win = asm.window(Rwb, pwb, st.Rbc, st.pbc, cam, hold=-1)
+    win.solve(iters=5, lam0=1e-4, precision="fp64")
+    torch.cuda.synchronize()
+    # the same Problem packed on the host from the reference's arrays, solved by the batched solve
+    p = "c%d_" % c
+    w = S.Window(Rwb=Rwb.copy(), pwb=pwb.copy(), Rbc=st.Rbc, pbc=st.pbc, lmp=z[p + "pb_lmp"].copy(),
+                 lm_host=z[p + "pb_lm_host"], lm_mask=z[p + "pb_lm_mask"], rho_meas=z[p + "pb_rho_meas"],
+                 rho_isig=z[p + "pb_rho_isig"], ob_start=z[p + "pb_ob_start"], ob_pose=z[p + "pb_ob_pose"],
+                 ob_cam=z[p + "pb_ob_cam"], ob_z=z[p + "pb_ob_z"], ob_isig=z[p + "pb_ob_isig"],
+                 ob_valid=z[p + "pb_ob_valid"], fx=st.fx, fy=st.fy, cx=st.cx, cy=st.cy, B=st.B, huber_k=1.345)
+    ref = solve_batch([w], iters=5, lam0=1e-4, precision="fp64", hold=None)
+    stt = win.stats.cpu().numpy()[0]
+    assert int(stt[4]) == 0 and int(ref["status"][0]) == 0
+    assert int(stt[2]) == int(ref["accepted"][0])
+    assert abs(stt[0] - ref["cost0"][0]) <= 1e-10 * abs(ref["cost0"][0])
+    n = 6 * K
+    d0, r0 = win.dx0.cpu().numpy()[0][:n], ref["dx0_list"][0]
+    assert np.linalg.norm(d0 - r0) <= 1e-8 * np.linalg.norm(r0)
+    assert np.abs(win.pwb.cpu().numpy() - w.pwb).max() < 1e-6

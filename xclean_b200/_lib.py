@@ -65,6 +65,19 @@ _SIGS = {
 FRONT_STAGES = ("response", "noise_floor", "candidates", "greedy", "orb", "stereo", "match")
 
 
+class BaEngine(ctypes.Structure):
+    _fields_ = [("P", c_int), ("sids", c_void_p), ("slot_n", c_void_p), ("M", ctypes.c_longlong), ("lid", c_void_p),
+                ("uv", c_void_p), ("cam", c_void_p), ("valid", c_void_p), ("sig", c_void_p), ("n_lm", c_int),
+                ("lm_alive", c_void_p), ("select", c_void_p), ("lm_host", c_void_p), ("lm_p", c_void_p),
+                ("lm_rho_meas", c_void_p), ("lm_sig_lk", c_void_p), ("lm_span", c_void_p), ("prior_mode", c_int),
+                ("kappa_d", c_double), ("fB", c_double), ("sig_px", c_double)]
+
+
+class BaAssembled(ctypes.Structure):
+    _fields_ = [(n, c_void_p) for n in ("counts", "alive", "src", "lmp", "lm_host", "lm_mask", "rho_meas", "rho_isig",
+                                         "lm_ob", "ob_pose", "ob_cam", "ob_z", "ob_isig", "ob_valid")]
+
+
 class BaWindows(ctypes.Structure):
     _fields_ = [("nw", c_int)] + [(n, c_void_p) for n in (
         "P", "L", "slot_off", "lm_off", "hold", "order", "cam", "ext", "Rwb", "pwb", "lmp", "lm_host", "lm_mask",
@@ -86,6 +99,8 @@ _SIGS.update({
     "xcb_ba_scratch_bytes": (c_size_t, [c_int, c_int]),
     "xcb_ba_large_scratch_bytes": (c_size_t, [c_int, c_int, c_int]),
     "xcb_ba_gram_tc": (c_int, [P, c_int, c_int, P, P, P]),
+    "xcb_ba_assemble_scratch_bytes": (c_size_t, [c_int, c_int, c_int]),
+    "xcb_ba_assemble_dev": (c_int, [ctypes.POINTER(BaEngine), ctypes.POINTER(BaAssembled), P, c_size_t, P]),
     "xcb_ba_solve_windows_large_dev": (c_int, [ctypes.POINTER(BaWindows), c_int, c_int, P, c_int, c_int, c_int,
                                                c_double, c_int, P, P, c_int, P, c_size_t, P]),
     "xcb_ba_solve_windows_dev": (c_int, [ctypes.POINTER(BaWindows), c_int, c_int, c_double, c_int, P, P, c_int, P,
