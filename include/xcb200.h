@@ -155,6 +155,27 @@ int xcb_front_stage_times(xcb_front* f, float* ms, int* ngraphs);
    Mahalanobis d2, then lower landmark index).  Outputs per landmark: keypoint index or -1, Hamming distance (9999 when
    rejected at the gate), Mahalanobis d2 (inf when rejected at the gate); a landmark that loses the one-per-keypoint
    step keeps its distance and d2 and gets index -1, as in the reference. */
+/* ============================================== dense 32-direction SGM ============================================== */
+/* The reference's dense stereo (src/xclean/stereo/sgm32.py SGM32, CuPy kernels :105-266, launches :333-360):
+   census 9x9 -> Hamming cost volume -> one 32-direction aggregation into a uint16 volume -> left winner with
+   uniqueness and parabola -> right winner off the same volume -> left-right check; disp 0 = invalid.  Bit for bit
+   the reference's outputs.  A handle serves one image size (width <= 2048) and owns its volumes (W x H x 384 B). */
+typedef struct xcb_sgm xcb_sgm;
+int xcb_sgm_create(int width, int height, int p1, int p2, float uniqueness, float lr_threshold, float min_disp,
+                   xcb_sgm** out);                              /* SGM32.__init__ (sgm32.py:278-320) */
+void xcb_sgm_destroy(xcb_sgm* s);
+const char* xcb_sgm_last_error(const xcb_sgm* s);
+/* SGM32.compute_gpu (sgm32.py:333-360): left / right (H x W u8) and disp / conf (H x W float32) in device memory;
+   launches on `stream` (NULL = the handle's stream), no synchronisation */
+int xcb_sgm_compute_dev(xcb_sgm* s, const uint8_t* left, const uint8_t* right, float* disp, float* conf, void* stream);
+/* SGM32.compute (sgm32.py:362-368): host arrays in and out, synchronous */
+int xcb_sgm_compute_host(xcb_sgm* s, const uint8_t* left, const uint8_t* right, float* disp, float* conf);
+/* the handle's device volumes after the last call (SGM32.cost_volume / aggregated_volume, sgm32.py:370-376): cost
+   [H][W][128] u8, sum [H][W][128] u16; npaths: the aggregation's paths over the 32 directions */
+int xcb_sgm_buffers(xcb_sgm* s, void** cost, void** sum, int* npaths);
+/* the same volumes copied to host memory (either may be NULL); waits for the handle's stream and the device */
+int xcb_sgm_read_volumes(xcb_sgm* s, uint8_t* cost, uint16_t* sum);
+
 typedef struct xcb_mm xcb_mm;
 
 /* MapMatcher.__init__ (src/xclean/front/mapmatch.py:134-139, mapmatch_fast.py:164-170): a 16-px grid over a

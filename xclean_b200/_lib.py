@@ -152,6 +152,13 @@ class LbaProblem(ctypes.Structure):
 _SIGS.update({
     "xcb_mm_create": (c_int, [c_int, c_int, c_int, c_int, c_int, P]),
     "xcb_mm_set_tuning": (c_int, [P, c_int, c_int]),
+    "xcb_sgm_create": (c_int, [c_int, c_int, c_int, c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float, P]),
+    "xcb_sgm_destroy": (None, [P]),
+    "xcb_sgm_last_error": (ctypes.c_char_p, [P]),
+    "xcb_sgm_compute_dev": (c_int, [P, P, P, P, P, P]),
+    "xcb_sgm_compute_host": (c_int, [P, P, P, P, P]),
+    "xcb_sgm_buffers": (c_int, [P, P, P, P]),
+    "xcb_sgm_read_volumes": (c_int, [P, P, P]),
     "xcb_mm_destroy": (c_int, [P]),
     "xcb_mm_last_error": (ctypes.c_char_p, [P]),
     "xcb_mm_grid_dims": (c_int, [P, P, P]),

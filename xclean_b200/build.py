@@ -25,6 +25,7 @@ SOURCES = {
     "front_api.cu": STRICT,
     "front_mapmatch.cu": STRICT,
     "ba_posefree.cu": STRICT,
+    "stereo_sgm.cu": STRICT,
     "ba_window.cu": [],
     "ba_api.cu": [],
 }
