@@ -176,6 +176,64 @@ int xcb_sgm_buffers(xcb_sgm* s, void** cost, void** sum, int* npaths);
 /* the same volumes copied to host memory (either may be NULL); waits for the handle's stream and the device */
 int xcb_sgm_read_volumes(xcb_sgm* s, uint8_t* cost, uint16_t* sum);
 
+/* ============================ multi-scale oriented ORB: pyramid, FAST, orientation, steered rBRIEF ============================
+   Beyond the reference, whose frontend is single-scale Shi-Tomasi with unoriented ORB (src/xclean/stages/features.py:27-28,
+   :102-103; src/xclean/front/gpu_front.py:1712-1717, where ORB is created with nlevels=1 and KeyPoint.angle 0).  No
+   reference entry point is replaced; the per-level descriptor is the reference's Frontend.describe (features.py:405-421:
+   cv2 ORB on the reflect-101 pad-32 image) with the pattern rotated, and level 0 at bin 0 is that descriptor bit for bit.
+   Every device pointer below is device memory; `stream` NULL = the legacy default stream (primitives) or the handle's. */
+/* FAST 9-of-16 with the score cv2.FastFeatureDetector gives (TYPE_9_16): keypoints (x, y) in row-major order and
+   their scores; with nonmax, only corners whose score beats all 8 neighbours'.  count (device int): the number found,
+   of which the first `cap` are written.  scratch: device bytes, at least xcb_fast_scratch_bytes(width, height). */
+size_t xcb_fast_scratch_bytes(int width, int height);
+int xcb_fast_dev(const uint8_t* img, int width, int height, int threshold, int nonmax, int cap, float* kp, float* resp,
+                 int32_t* count, void* scratch, size_t scratch_bytes, void* stream);
+/* of the first min(*n_in, cap_in) keypoints, those at least `edge` px inside width x height: the `quota` best by score,
+   ties in input order, written in input order; *count = how many */
+int xcb_fast_select_dev(const float* kp_in, const float* resp_in, const int32_t* n_in, int cap_in, int width, int height,
+                        int edge, int quota, float* kp, float* resp, int32_t* count, void* stream);
+/* bilinear downsampling of n_src samples to n_dst = cv2.resize(INTER_LINEAR_EXACT): per destination sample the source
+   index and an 8-bit weight (host arrays of n_dst) */
+int xcb_pyr_tables(int n_src, int n_dst, int32_t* idx, int32_t* w);
+int xcb_pyr_down_dev(const uint8_t* src, int ws, int hs, uint8_t* dst, int wd, int hd, const int32_t* x0,
+                     const int32_t* wx, const int32_t* y0, const int32_t* wy, void* stream);
+/* orientation: the intensity centroid over the disc u^2 + v^2 <= 240 (radius 15) -> bin k of 30 (centre 12 k degrees,
+   image axes); host tables umax[16], boundary directions bdir[30][2] and centres cdir[30][2] */
+int xcb_orient_tables(int32_t* umax, double* bdir, double* cdir);
+int xcb_ic_bins_dev(const uint8_t* img, int width, int height, const float* kp, int n, const int32_t* count,
+                    const int32_t* umax, const double* bdir, const double* cdir, int32_t* bins, int64_t* moments,
+                    void* stream);              /* count: optional device count (min(*count, n) keypoints) */
+/* steered rBRIEF on a blurred image padded by `pad`: patterns [30][256][4] int8 (x1, y1, x2, y2) rotated per bin */
+int xcb_orb_steered_dev(const uint8_t* blur, int wp, int hp, int pad, const float* kp, int n, const int32_t* count,
+                        const int32_t* bins, const int8_t* patterns, uint8_t* desc, void* stream);
+/* the ORB blur of the reference's describe stage (reflect-101 pad 32, 7x7 Gaussian sigma 2 in OpenCV's float
+   arithmetic with the SIMD split points vr / vc of this width): width x height -> (height + 64) x (width + 64); kf7
+   device taps */
+int xcb_blur_dev(const uint8_t* img, int width, int height, const float* kf7, int vr, int vc, uint8_t* out,
+                 void* stream);
+/* the per-frame handle: `levels` levels at `scale` (sizes rint(n / scale^l)), FAST at fast_threshold on each, per
+   level a geometric share of nfeatures (the best by score at least `edge` >= 16 px inside), orientation bins, the level's
+   blur and steered descriptors.  Outputs in nfeatures slots, level l's from its offset (xcb_orbx_level). */
+typedef struct xcb_orbx xcb_orbx;
+int xcb_orbx_create(int width, int height, int levels, double scale, int nfeatures, int fast_threshold, int edge,
+                    int nonmax, xcb_orbx** out);
+void xcb_orbx_destroy(xcb_orbx* h);
+const char* xcb_orbx_last_error(const xcb_orbx* h);
+int xcb_orbx_level(const xcb_orbx* h, int level, int* width, int* height, float* scale, int* quota, int* offset);
+int xcb_orbx_set_blur(xcb_orbx* h, int level, int vr, int vc, const float* kf7);      /* host taps */
+int xcb_orbx_set_patterns(xcb_orbx* h, const int8_t* patterns);                       /* host [30][256][4] */
+int xcb_orbx_detect_dev(xcb_orbx* h, const uint8_t* img, void* stream);              /* asynchronous */
+int xcb_orbx_launches(const xcb_orbx* h);                                              /* kernels per detect */
+int xcb_orbx_outputs(xcb_orbx* h, float** kp, float** kp_level, float** resp, int32_t** level, int32_t** bins,
+                     uint8_t** desc, int32_t** counts);                               /* device pointers */
+int xcb_orbx_detect_host(xcb_orbx* h, const uint8_t* img, float* kp, float* kp_level, float* resp, int32_t* level,
+                         int32_t* bins, uint8_t* desc, int32_t* counts);               /* synchronous */
+/* the slot arrays of the last detect (either entry) copied to the host after a device-wide wait; any may be NULL */
+int xcb_orbx_read(xcb_orbx* h, float* kp, float* kp_level, float* resp, int32_t* level, int32_t* bins, uint8_t* desc,
+                  int32_t* counts);
+/* a pyramid level of the last xcb_orbx_detect_host frame (level 0 = the frame) to the host */
+int xcb_orbx_read_level(xcb_orbx* h, int level, uint8_t* out);
+
 typedef struct xcb_mm xcb_mm;
 
 /* MapMatcher.__init__ (src/xclean/front/mapmatch.py:134-139, mapmatch_fast.py:164-170): a 16-px grid over a

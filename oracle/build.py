@@ -1,4 +1,4 @@
-"""Build recipe for the CPU oracle (test infrastructure): oracle/{front,ba,sgm}_oracle.c -> oracle/liboracle.so.
+"""Build recipe for the CPU oracle (test infrastructure): oracle/{front,ba,sgm,ext}_oracle.c -> oracle/liboracle.so.
 
 Strict IEEE: -ffp-contract=off and no fast-math, so every fused multiply-add in the oracle is an explicit fma()."""
 import os
@@ -6,7 +6,7 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SRCS = [os.path.join(HERE, f) for f in ("front_oracle.c", "ba_oracle.c", "sgm_oracle.c")]
+SRCS = [os.path.join(HERE, f) for f in ("front_oracle.c", "ba_oracle.c", "sgm_oracle.c", "ext_oracle.c")]
 OUT = os.path.join(HERE, "liboracle.so")
 
 

@@ -77,4 +77,8 @@ def test_assembled_window_solves_on_the_device(z, c):
     n = 6 * K
     d0, r0 = win.dx0.cpu().numpy()[0][:n], ref["dx0_list"][0]
     assert np.linalg.norm(d0 - r0) <= 1e-8 * np.linalg.norm(r0)
-    assert np.abs(win.pwb.cpu().numpy() - w.pwb).max() < 1e-6
+    # no pose is held, so the gauge is free and only LM damping fixes it: summation-order differences between the two
+    # packings drift along the gauge directions over the iterations.  The cost is gauge-invariant and must agree
+    # tightly; the poses to 1e-5.
+    assert abs(stt[1] - ref["cost"][0]) <= 1e-9 * abs(ref["cost"][0])
+    assert np.abs(win.pwb.cpu().numpy() - w.pwb).max() < 1e-5

@@ -237,7 +237,7 @@ def test_gate_lanes_give_identical_results(lanes):
     try:
         mm.set_tuning(_lib.XCB_TUNE_MM_LANES, lanes)
         got = mm.match(kp, desc, uv, S, lmd, lnd, chi2=50.0)
-        with pytest.raises(RuntimeError):
+        with pytest.raises(ValueError):                 # XCB_ERR_ARG, as every other bad argument
             mm.set_tuning(_lib.XCB_TUNE_MM_LANES, 3)
     finally:
         mm.close()

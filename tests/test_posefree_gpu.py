@@ -151,6 +151,6 @@ def test_single_window_signatures(G):
     assert imu == [] and np.array_equal(off, np.arange(w.Rwb.shape[0] + 1) * 6) and w.pf.ok.any()
     Hm, bm, offm = ba.marg_system(w, np.asarray(w.lm_mask, np.bool_))      # the window's own mask: its H again
     assert np.allclose(Hm, H, rtol=0, atol=1e-9 * np.abs(H).max())
-    w.prior = object()
-    with pytest.raises(NotImplementedError):
+    w.prior = object()                    # not a marg.Prior (bound priors are solved: tests/test_prior_gpu.py)
+    with pytest.raises(ValueError):
         ba.solve(w)

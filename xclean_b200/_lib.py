@@ -159,6 +159,27 @@ _SIGS.update({
     "xcb_sgm_compute_host": (c_int, [P, P, P, P, P]),
     "xcb_sgm_buffers": (c_int, [P, P, P, P]),
     "xcb_sgm_read_volumes": (c_int, [P, P, P]),
+    "xcb_fast_scratch_bytes": (c_size_t, [c_int, c_int]),
+    "xcb_fast_dev": (c_int, [P, c_int, c_int, c_int, c_int, c_int, P, P, P, P, c_size_t, P]),
+    "xcb_fast_select_dev": (c_int, [P, P, P, c_int, c_int, c_int, c_int, c_int, P, P, P, P]),
+    "xcb_pyr_tables": (c_int, [c_int, c_int, P, P]),
+    "xcb_pyr_down_dev": (c_int, [P, c_int, c_int, P, c_int, c_int, P, P, P, P, P]),
+    "xcb_orient_tables": (c_int, [P, P, P]),
+    "xcb_ic_bins_dev": (c_int, [P, c_int, c_int, P, c_int, P, P, P, P, P, P, P]),
+    "xcb_orb_steered_dev": (c_int, [P, c_int, c_int, c_int, P, c_int, P, P, P, P, P]),
+    "xcb_blur_dev": (c_int, [P, c_int, c_int, P, c_int, c_int, P, P]),
+    "xcb_orbx_create": (c_int, [c_int, c_int, c_int, c_double, c_int, c_int, c_int, c_int, P]),
+    "xcb_orbx_destroy": (None, [P]),
+    "xcb_orbx_last_error": (ctypes.c_char_p, [P]),
+    "xcb_orbx_level": (c_int, [P, c_int, P, P, P, P, P]),
+    "xcb_orbx_set_blur": (c_int, [P, c_int, c_int, c_int, P]),
+    "xcb_orbx_set_patterns": (c_int, [P, P]),
+    "xcb_orbx_detect_dev": (c_int, [P, P, P]),
+    "xcb_orbx_launches": (c_int, [P]),
+    "xcb_orbx_outputs": (c_int, [P, P, P, P, P, P, P, P]),
+    "xcb_orbx_detect_host": (c_int, [P, P, P, P, P, P, P, P, P]),
+    "xcb_orbx_read": (c_int, [P, P, P, P, P, P, P, P]),
+    "xcb_orbx_read_level": (c_int, [P, c_int, P]),
     "xcb_mm_destroy": (c_int, [P]),
     "xcb_mm_last_error": (ctypes.c_char_p, [P]),
     "xcb_mm_grid_dims": (c_int, [P, P, P]),

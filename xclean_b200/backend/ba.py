@@ -154,6 +154,8 @@ PRIOR_FIELDS = ("pr_m", "pr_nb", "pr_boff", "pr_soff", "pr_roff", "pr_blk", "pr_
 def _prior_slots(pr, P):
     """The window slot of each block of a bound prior (window.Problem.prior: marg.Prior after bind(), 6-dim pose
     blocks with the default 6-per-slot offsets)."""
+    if not hasattr(pr, "dims"):
+        raise ValueError("solve_batch: the window's prior is not a marginal prior (marg.Prior)")
     cols = getattr(pr, "cols", None)
     dims = [int(x) for x in pr.dims]
     if cols is None:

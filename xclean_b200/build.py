@@ -26,6 +26,7 @@ SOURCES = {
     "front_mapmatch.cu": STRICT,
     "ba_posefree.cu": STRICT,
     "stereo_sgm.cu": STRICT,
+    "front_ext.cu": STRICT,
     "ba_window.cu": [],
     "ba_api.cu": [],
 }

@@ -81,8 +81,8 @@ __global__ void __launch_bounds__(128, 1) k_gram_tc(const float* __restrict__ U,
 
 extern "C" int xcb_ba_gram_tc(const float* U, int n, int K, float* D, unsigned int* err, void* stream)
 {
-    if (!U || !D || n < 1 || n > TC_M || K < 0) {
-        xcb_set_last_error("ba_gram_tc: U / D null or n outside 1..128 or K negative");
+    if ((!U && K > 0) || !D || n < 1 || n > TC_M || K < 0) {
+        xcb_set_last_error("ba_gram_tc: D null, U null with K > 0, n outside 1..128 or K negative");
         return XCB_ERR_ARG;
     }
     static XcbAttrOnce attr;
