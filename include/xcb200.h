@@ -175,6 +175,11 @@ int xcb_sgm_compute_host(xcb_sgm* s, const uint8_t* left, const uint8_t* right, 
 int xcb_sgm_buffers(xcb_sgm* s, void** cost, void** sum, int* npaths);
 /* the same volumes copied to host memory (either may be NULL); waits for the handle's stream and the device */
 int xcb_sgm_read_volumes(xcb_sgm* s, uint8_t* cost, uint16_t* sum);
+/* in-stream stage timing (no reference counterpart; the bench's per-kernel roofline): when on, each compute records
+   events around the cost kernel, the aggregation (with the zeroing of the sum volume) and the selection;
+   xcb_sgm_stage_times returns ms[3] summed over the calls since its last call (at most the last 256) and waits for them */
+int xcb_sgm_set_stage_timing(xcb_sgm* s, int on);
+int xcb_sgm_stage_times(xcb_sgm* s, float* ms, int* ncalls);
 
 /* ============================ multi-scale oriented ORB: pyramid, FAST, orientation, steered rBRIEF ============================
    Beyond the reference, whose frontend is single-scale Shi-Tomasi with unoriented ORB (src/xclean/stages/features.py:27-28,

@@ -159,6 +159,8 @@ _SIGS.update({
     "xcb_sgm_compute_host": (c_int, [P, P, P, P, P]),
     "xcb_sgm_buffers": (c_int, [P, P, P, P]),
     "xcb_sgm_read_volumes": (c_int, [P, P, P]),
+    "xcb_sgm_set_stage_timing": (c_int, [P, c_int]),
+    "xcb_sgm_stage_times": (c_int, [P, P, P]),
     "xcb_fast_scratch_bytes": (c_size_t, [c_int, c_int]),
     "xcb_fast_dev": (c_int, [P, c_int, c_int, c_int, c_int, c_int, P, P, P, P, c_size_t, P]),
     "xcb_fast_select_dev": (c_int, [P, P, P, c_int, c_int, c_int, c_int, c_int, P, P, P, P]),

@@ -405,8 +405,8 @@ extern "C" int xcb_fast_dev(const uint8_t* img, int width, int height, int thres
                             float* resp, int32_t* count, void* scratch, size_t scratch_bytes, void* stream)
 {
     if (!img || !kp || !resp || !count || !scratch) return ext_fail("fast: null argument", XCB_ERR_ARG);
-    if (width < 1 || height < 1 || height > (1 << 20) || threshold < 0 || threshold > 255 || cap < 0)
-        return ext_fail("fast: bad size, threshold (0..255) or capacity", XCB_ERR_ARG);
+    if (width < 1 || height < 1 || height > 65535 || threshold < 0 || threshold > 255 || cap < 0)
+        return ext_fail("fast: bad size (height <= 65535), threshold (0..255) or capacity", XCB_ERR_ARG);
     if (scratch_bytes < xcb_fast_scratch_bytes(width, height))
         return ext_fail("fast: scratch smaller than xcb_fast_scratch_bytes", XCB_ERR_CAPACITY);
     char* p = (char*)scratch;
@@ -437,8 +437,8 @@ extern "C" int xcb_fast_select_dev(const float* kp_in, const float* resp_in, con
 extern "C" int xcb_pyr_down_dev(const uint8_t* src, int ws, int hs, uint8_t* dst, int wd, int hd, const int32_t* x0,
                                 const int32_t* wx, const int32_t* y0, const int32_t* wy, void* stream)
 {
-    if (!src || !dst || !x0 || !wx || !y0 || !wy || ws < 1 || hs < 1 || wd < 1 || hd < 1)
-        return ext_fail("pyr_down: null argument or empty image", XCB_ERR_ARG);
+    if (!src || !dst || !x0 || !wx || !y0 || !wy || ws < 1 || hs < 1 || wd < 1 || hd < 1 || hd > 65535)
+        return ext_fail("pyr_down: null argument, empty image or height > 65535", XCB_ERR_ARG);
     k_pyr_down<<<dim3((wd + 127) / 128, hd), 128, 0, (cudaStream_t)stream>>>(src, hs, ws, dst, hd, wd, x0, wx, y0, wy);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return ext_fail(std::string("pyr_down: ") + cudaGetErrorString(e), XCB_ERR_CUDA);
@@ -529,7 +529,7 @@ extern "C" int xcb_orbx_create(int width, int height, int levels, double scale, 
     if (!out) return ox_fail(nullptr, XCB_ERR_ARG, "orbx_create: null output");
     *out = nullptr;
     if (levels < 1 || levels > EXT_MAXL || !(scale > 1.0) || scale > 4.0 || nfeatures < 1 || fast_threshold < 0 ||
-        fast_threshold > 255 || edge < EXT_R + 1 || width < 1 || height < 1 || height > (1 << 20))
+        fast_threshold > 255 || edge < EXT_R + 1 || width < 1 || height < 1 || height > 65535)
         return ox_fail(nullptr, XCB_ERR_ARG,
                        "orbx_create: levels 1..8, scale in (1, 4], nfeatures >= 1, threshold 0..255, edge >= 16");
     xcb_orbx* h = new xcb_orbx();

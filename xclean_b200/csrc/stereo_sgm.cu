@@ -16,6 +16,7 @@
 //   k_sgm_select CTA per row: the row's right winners into shared memory, then the left winner, uniqueness, parabola,
 //                confidence and the left-right check per pixel, one pass over the row's volume
 #include <string>
+#include <vector>
 
 #include "common.cuh"
 
@@ -38,7 +39,15 @@ struct xcb_sgm {
     unsigned char *in_l, *in_r;  // host entry's device inputs
     cudaStream_t stream;
     std::string err;
+    // stage timing (xcb_sgm_set_stage_timing): per timed call four events (cost | aggregation incl. the zeroing of the
+    // sum volume | selection), in a ring of SGM_TRING sets; xcb_sgm_stage_times sums the sets recorded since its last
+    // call
+    bool timing;
+    int tn;
+    std::vector<cudaEvent_t> tev;
 };
+
+#define SGM_TRING 256
 
 struct SgmDirs {
     int dx[32], dy[32], p1[32], p2[32];
@@ -331,12 +340,55 @@ extern "C" void xcb_sgm_destroy(xcb_sgm* s)
 {
     if (!s) return;
     cudaStreamSynchronize(s->stream);
+    for (cudaEvent_t e : s->tev) cudaEventDestroy(e);
     cudaFree(s->C); cudaFree(s->S); cudaFree(s->disp); cudaFree(s->conf); cudaFree(s->in_l); cudaFree(s->in_r);
     cudaStreamDestroy(s->stream);
     delete s;
 }
 
 extern "C" const char* xcb_sgm_last_error(const xcb_sgm* s) { return s ? s->err.c_str() : xcb_last_error(); }
+
+extern "C" int xcb_sgm_set_stage_timing(xcb_sgm* s, int on)
+{
+    if (!s) return sgm_fail(nullptr, XCB_ERR_ARG, "sgm_set_stage_timing: null handle");
+    if (on && s->tev.empty()) {
+        s->tev.assign(4 * SGM_TRING, nullptr);
+        for (auto& e : s->tev) {
+            const cudaError_t r = cudaEventCreate(&e);
+            if (r != cudaSuccess) {
+                for (auto& q : s->tev)
+                    if (q) cudaEventDestroy(q);
+                s->tev.clear();
+                return sgm_fail(s, XCB_ERR_CUDA, std::string("sgm_set_stage_timing: ") + cudaGetErrorString(r));
+            }
+        }
+    }
+    s->timing = on != 0;
+    s->tn = 0;
+    return XCB_OK;
+}
+
+// ms[3]: cost, aggregation (with the zeroing of the sum volume), selection, summed over the timed calls since the last
+// read (at most the last SGM_TRING); *ncalls: how many.  Waits for those calls.
+extern "C" int xcb_sgm_stage_times(xcb_sgm* s, float* ms, int* ncalls)
+{
+    if (!s || !ms) return sgm_fail(s, XCB_ERR_ARG, "sgm_stage_times: null argument");
+    ms[0] = ms[1] = ms[2] = 0.0f;
+    const int n = s->tn < SGM_TRING ? s->tn : SGM_TRING;
+    for (int c = 0; c < n; ++c) {
+        cudaEvent_t* ev = &s->tev[4 * c];
+        for (int i = 0; i < 3; ++i) {
+            float t = 0.0f;
+            cudaError_t e = cudaEventSynchronize(ev[i + 1]);
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&t, ev[i], ev[i + 1]);
+            if (e != cudaSuccess) return sgm_fail(s, XCB_ERR_CUDA, std::string("sgm_stage_times: ") + cudaGetErrorString(e));
+            ms[i] += t;
+        }
+    }
+    if (ncalls) *ncalls = n;
+    s->tn = 0;
+    return XCB_OK;
+}
 
 extern "C" int xcb_sgm_compute_dev(xcb_sgm* s, const uint8_t* left, const uint8_t* right, float* disp, float* conf,
                                    void* stream)
@@ -351,13 +403,19 @@ extern "C" int xcb_sgm_compute_dev(xcb_sgm* s, const uint8_t* left, const uint8_
         dirs.off[i] = s->dir_off[i];
     }
     dirs.off[32] = s->dir_off[32];
+    cudaEvent_t* ev = s->timing ? &s->tev[4 * (s->tn % SGM_TRING)] : nullptr;
+    if (ev) ++s->tn;
     const size_t sm_cost = ((18 * (size_t)W + 15) & ~(size_t)15) + (size_t)W * 20;
+    if (ev) cudaEventRecord(ev[0], st);
     k_sgm_cost<<<H, 256, sm_cost, st>>>(left, right, H, W, s->C);
+    if (ev) cudaEventRecord(ev[1], st);
     cudaError_t e = cudaMemsetAsync(s->S, 0, n * SGM_D * 2, st);
     if (e != cudaSuccess) return sgm_fail(s, XCB_ERR_CUDA, std::string("sgm_compute: ") + cudaGetErrorString(e));
     const long long threads = (long long)s->npaths * 32;
     k_sgm_agg<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(s->C, (unsigned*)s->S, H, W, dirs, s->npaths);
+    if (ev) cudaEventRecord(ev[2], st);
     k_sgm_select<<<H, 256, (size_t)W * 4, st>>>(s->S, H, W, s->uniq, s->dmin, s->lr, disp, conf);
+    if (ev) cudaEventRecord(ev[3], st);
     e = cudaGetLastError();
     if (e != cudaSuccess) return sgm_fail(s, XCB_ERR_CUDA, std::string("sgm_compute: ") + cudaGetErrorString(e));
     return XCB_OK;

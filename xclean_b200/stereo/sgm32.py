@@ -128,6 +128,17 @@ class SGM32:
         self.ms.append((time.perf_counter() - t0) * 1e3)
         return disp, conf
 
+    def set_stage_timing(self, on=True):
+        """In-stream events around the cost, aggregation and selection kernels of each compute (for profiling)."""
+        self._chk(self.L.xcb_sgm_set_stage_timing(self._h, 1 if on else 0), "xcb_sgm_set_stage_timing")
+
+    def stage_times(self):
+        """-> ({"cost", "aggregate", "select"} ms summed over the timed calls since the last read, calls); waits."""
+        ms = (ctypes.c_float * 3)()
+        n = ctypes.c_int(0)
+        self._chk(self.L.xcb_sgm_stage_times(self._h, ms, ctypes.byref(n)), "xcb_sgm_stage_times")
+        return {"cost": ms[0], "aggregate": ms[1], "select": ms[2]}, int(n.value)
+
     def _volume(self, which, dtype):
         n = self.H * self.W * MAX_DISP
         out = np.empty(n, dtype)
