@@ -49,3 +49,20 @@ def ref_sgm(left_t, right_t, p1=P1, p2=P2, uniq=UNIQ, lr=LR, dmin=DMIN):
     if rc != 0:
         raise RuntimeError("reference SGM kernels failed (%d)" % rc)
     return disp.cpu().numpy(), conf.cpu().numpy(), S.cpu().numpy().view(np.uint16)
+
+
+def ref_sgm_time(left_t, right_t, passes=3, p1=P1, p2=P2, uniq=UNIQ, lr=LR, dmin=DMIN):
+    """The reference's own kernels timed on F pairs in device memory (torch CUDA uint8 (F, H, W)), buffers allocated
+    once as SGM32 does; one untimed pass, then `passes` passes between CUDA events -> ms per frame."""
+    import torch
+    lib = ctypes.CDLL(REF_LIB)
+    F, H, W = left_t.shape
+    disp = torch.zeros((H, W), dtype=torch.float32, device=left_t.device)
+    conf = torch.zeros((H, W), dtype=torch.float32, device=left_t.device)
+    ms = ctypes.c_float(0.0)
+    v = lambda t: ctypes.c_void_p(t.data_ptr())
+    rc = lib.xr_sgm_time(v(left_t), v(right_t), F, H, W, int(p1), int(p2), ctypes.c_float(uniq), ctypes.c_float(lr),
+                         ctypes.c_float(dmin), v(disp), v(conf), int(passes), ctypes.byref(ms))
+    if rc != 0:
+        raise RuntimeError("reference SGM kernels failed (%d)" % rc)
+    return float(ms.value)

@@ -34,31 +34,55 @@ extern void xcb_set_last_error(const std::string& m);
 #define EXT_PAD 32
 #define EXT_MAXL 8
 
-__constant__ int c_circ[16][2] = {{0, -3}, {1, -3}, {2, -2}, {3, -1}, {3, 0}, {3, 1}, {2, 2}, {1, 3},
-                                  {0, 3}, {-1, 3}, {-2, 2}, {-3, 1}, {-3, 0}, {-3, -1}, {-2, -2}, {-1, -3}};
 
 // ------------------------------------------------------------------------------------------------------------ FAST
+__device__ __forceinline__ int fmin_i(int a, int b) { return a < b ? a : b; }
+__device__ __forceinline__ int fmax_i(int a, int b) { return a > b ? a : b; }
+
 __global__ void k_fast_score(const u8* __restrict__ img, int H, int W, int threshold, int* __restrict__ score)
 {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     if (x >= W) return;
     int s = -1;
     if (x >= 3 && x < W - 3 && y >= 3 && y < H - 3) {
-        const int p = img[(size_t)y * W + x];
+        // the radius-3 Bresenham circle, clockwise from the top
+        const u8* c = img + (size_t)y * W + x;
+        const int p = c[0];
         int d[16];
+        d[0] = (int)c[-3 * W] - p;
+        d[1] = (int)c[-3 * W + 1] - p;
+        d[2] = (int)c[-2 * W + 2] - p;
+        d[3] = (int)c[-W + 3] - p;
+        d[4] = (int)c[3] - p;
+        d[5] = (int)c[W + 3] - p;
+        d[6] = (int)c[2 * W + 2] - p;
+        d[7] = (int)c[3 * W + 1] - p;
+        d[8] = (int)c[3 * W] - p;
+        d[9] = (int)c[3 * W - 1] - p;
+        d[10] = (int)c[2 * W - 2] - p;
+        d[11] = (int)c[W - 3] - p;
+        d[12] = (int)c[-3] - p;
+        d[13] = (int)c[-W - 3] - p;
+        d[14] = (int)c[-2 * W - 2] - p;
+        d[15] = (int)c[-3 * W - 1] - p;
+        // minima of every arc of 9 by doubling (arcs of 2, 4, 8, then the ninth), for d (bright) and -d (dark)
+        int a2[16], b2[16], a4[16], b4[16];
 #pragma unroll
-        for (int k = 0; k < 16; ++k) d[k] = (int)img[(size_t)(y + c_circ[k][1]) * W + x + c_circ[k][0]] - p;
+        for (int k = 0; k < 16; ++k) {
+            a2[k] = fmin_i(d[k], d[(k + 1) & 15]);
+            b2[k] = fmin_i(-d[k], -d[(k + 1) & 15]);
+        }
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            a4[k] = fmin_i(a2[k], a2[(k + 2) & 15]);
+            b4[k] = fmin_i(b2[k], b2[(k + 2) & 15]);
+        }
         int best = -(1 << 20);
 #pragma unroll
         for (int k = 0; k < 16; ++k) {
-            int lo = 1 << 20, hi = 1 << 20;          // smallest d (bright arc) and smallest -d (dark arc)
-#pragma unroll
-            for (int j = 0; j < 9; ++j) {
-                const int v = d[(k + j) & 15];
-                lo = min(lo, v);
-                hi = min(hi, -v);
-            }
-            best = max(best, max(lo, hi));
+            const int a8 = fmin_i(a4[k], a4[(k + 4) & 15]), b8 = fmin_i(b4[k], b4[(k + 4) & 15]);
+            best = fmax_i(best, fmin_i(a8, d[(k + 8) & 15]));
+            best = fmax_i(best, fmin_i(b8, -d[(k + 8) & 15]));
         }
         if (best - 1 >= threshold) s = best - 1;
     }

@@ -48,21 +48,29 @@ struct StJob {
 };
 
 // per-warp shared memory: jobs [ST_GROUP] | U.  U holds, while a point is searched: Td [NPIX] f64 | T2d [NPIX] f64 |
-// sc [MAXD] f64 | jb [MAXD] i8 | the image window (float32 rows of win_w, or u8 rows of U8Win::WWB); during the LKs:
+// sc [MAXD] f64 | jb [MAXD] i8 | the two templates' rows as words (PW x NTW each) | the exact-evaluation scratch |
+// the image window | the exact evaluation's products (EXB x NPIX f64) (float32 rows of win_w, or u8 rows of U8Win::WWB); during the LKs:
 // the group's LK blocks (ST_GROUP x lk_job_bytes); during the vertical scans: Td [NPIX] f64 | the scan block
 // ((2 PW - 1) x PW float32).
 static __host__ __device__ __forceinline__ size_t st_jobs_bytes() { return (ST_GROUP * sizeof(StJob) + 15) & ~(size_t)15; }
 
+#define EXB 4          // patches evaluated exactly at once (their products staged in shared memory)
+#define EZ 48          // exact-evaluation entries per pass (candidates x band rows)
+
+// the search's exact-evaluation scratch: EZ entry offsets (i32), EZ results (f64), the candidate list (EZ i32), the
+// exact flags of the disparities (MAXD u8)
+static __host__ __device__ __forceinline__ size_t st_exact_bytes() { return (size_t)EZ * 16 + MAXD; }
+
 static __host__ __device__ __forceinline__ size_t stereo_off_u(int half)
 {
-    int pw = 2 * half + 1, npix = pw * pw;
-    return ((size_t)npix * 16 + MAXD * 8 + MAXD + 15) & ~(size_t)15;
+    int pw = 2 * half + 1, npix = pw * pw, ntw = (pw + 3) / 4;
+    return ((size_t)npix * 16 + MAXD * 8 + MAXD + 2 * (size_t)pw * 4 * ntw + st_exact_bytes() + 15) & ~(size_t)15;
 }
 
 static __host__ __device__ __forceinline__ size_t stereo_warp_bytes(int half, int band)
 {
     int pw = 2 * half + 1, npix = pw * pw;
-    size_t search = stereo_off_u(half) + (size_t)(pw + 2 * band) * win_w(half) * 4;
+    size_t search = stereo_off_u(half) + (size_t)(pw + 2 * band) * win_w(half) * 4 + (size_t)EXB * npix * 8;
     size_t lk = (size_t)ST_GROUP * lk_job_bytes(half);
     size_t vert = (size_t)npix * 8 + (size_t)(2 * pw - 1) * pw * 4;
     size_t u = search > lk ? search : lk;
@@ -71,6 +79,18 @@ static __host__ __device__ __forceinline__ size_t stereo_warp_bytes(int half, in
 }
 
 size_t xcb_stereo_smem_per_warp(int half, int band) { return stereo_warp_bytes(half, band); }
+
+// the shared-memory opt-in limit of a block (227 KB); a launch whose warps would need more takes fewer warps
+#define ST_SMEM_MAX ((size_t)227 * 1024)
+
+// the dynamic shared memory the kernel is enabled for: the widest band's block, at most the opt-in limit
+static size_t st_smem_attr(int half)
+{
+    const size_t pw = (stereo_warp_bytes(half, BAND_MAX) + 15) & ~(size_t)15;
+    size_t b = pw * st_warps(half);
+    if (b > ST_SMEM_MAX) b = (ST_SMEM_MAX / pw) * pw;
+    return b;
+}
 
 // ---------------------------------------------------------------- OpenBLAS 3x3 arithmetic (as the oracle restates it)
 // Every loop has constant bounds and the pivot rows are applied by comparisons, so the matrix stays in registers (a
@@ -326,8 +346,10 @@ struct U8Win {
     static constexpr int PW = 2 * HALF + 1;
     static constexpr int NV = PW + 3;                 // bytes a lane reads per row
     static constexpr int NWD = (NV + 3) / 4;          // ... as 32-bit words
+    static constexpr int NTW = (PW + 3) / 4;          // a template row as zero-padded 32-bit words
+    static constexpr int NSW = NTW + 1;               // window words a lane reads per row for the byte-shifted products
     static constexpr int PAD = 8;                     // left pad bytes: 4 + the alignment shift (0..3)
-    static constexpr int WWB = (MAXD + 4 * NWD + PAD + 3) & ~3;    // row stride in bytes
+    static constexpr int WWB = (MAXD + 4 * (NSW > NWD ? NSW : NWD) + PAD + 3) & ~3;    // row stride in bytes
 };
 
 // z[k] = ZNCC of the patch whose top-left is byte `p` + k (rows WWB bytes apart); p is 4-byte aligned
@@ -372,6 +394,130 @@ __device__ __forceinline__ void zncc4_u8(const unsigned char* p, const double* T
     }
 #pragma unroll
     for (int k = 0; k < 4; ++k) z[k] = zncc_finish((double)S[k], (double)SQ[k], sx[k], ts, NPIX);
+}
+
+// The search filter (u8 images).  Every ZNCC the searches need is first bounded from exact integers: with the
+// template bytes t, the patch bytes r, St = sum t, S = sum r, SQ = sum r^2, SI = sum r t (dp4a), N = NPIX SI - St S and
+// V = NPIX SQ - S^2, the reference's float64 value is N / (NPIX ts sqrt(V)) up to its own roundings:
+//   numerator   |sx - N / NPIX| <= E = gamma_NPIX 255 sum|T| + 510 u S  (the sequential sum of the rounded products,
+//               and T = fl(t - fl(St / NPIX)) against t - St / NPIX), u = 2^-53
+//   denominator the float64 variance's cancellation error is below 7e-7 relative for any V >= 1 (V is an integer)
+// and the float32 evaluation adds at most 5e-7 relative.  ea = 4e-6 |z| + 1.05 E / den + 1e-9 bounds |z_fp - za|.
+// V = 0 (a flat patch) gives variance exactly 0 in float64 too, so z = -2 exactly (ea = 0); den within 1e-5 of the
+// reference's 1e-6 cut is undecided (ea = inf).  A disparity whose interval lies strictly below another's cannot be
+// the maximum (or the second peak, or the left-right maximum), so only the others are evaluated exactly, in the
+// reference's sequential order (zexact_u8): the decisions and every value that leaves the search are bit for bit the
+// reference's.
+//
+// za[k], ea[k] for the 4 adjacent patches whose top-left is byte p + k (p 4-byte aligned, rows WWB bytes apart);
+// tw: the template's rows as NTW zero-padded words
+template <int HALF>
+__device__ __forceinline__ void zapprox4_u8(const unsigned char* p, const unsigned* tw, int st, float ts32, float at32,
+                                            float za[4], float ea[4])
+{
+    using G = U8Win<HALF>;
+    constexpr int PW = G::PW, NPIX = PW * PW, NV = G::NV, NTW = G::NTW, NSW = G::NSW;
+    unsigned S[4] = {0u, 0u, 0u, 0u}, SQ[4] = {0u, 0u, 0u, 0u}, SI[4] = {0u, 0u, 0u, 0u};
+#pragma unroll 1
+    for (int dy = 0; dy < PW; ++dy) {
+        const unsigned* rp = (const unsigned*)(p + dy * G::WWB);
+        unsigned w[NSW];
+#pragma unroll
+        for (int i = 0; i < NSW; ++i) w[i] = rp[i];
+        unsigned b[NV];
+#pragma unroll
+        for (int i = 0; i < NV; ++i) b[i] = (w[i >> 2] >> (8 * (i & 3))) & 0xffu;
+        unsigned s = 0u, sq = 0u;
+#pragma unroll
+        for (int i = 0; i < PW / 4; ++i) { s = __dp4a(w[i], 0x01010101u, s); sq = __dp4a(w[i], w[i], sq); }
+#pragma unroll
+        for (int i = (PW / 4) * 4; i < PW; ++i) { s += b[i]; sq += b[i] * b[i]; }
+        S[0] += s; SQ[0] += sq;
+#pragma unroll
+        for (int k = 1; k < 4; ++k) {
+            s += b[k - 1 + PW] - b[k - 1];
+            sq += b[k - 1 + PW] * b[k - 1 + PW] - b[k - 1] * b[k - 1];
+            S[k] += s; SQ[k] += sq;
+        }
+        const unsigned* t = tw + dy * NTW;
+#pragma unroll
+        for (int i = 0; i < NTW; ++i) {
+            const unsigned tt = t[i];
+            SI[0] = __dp4a(w[i], tt, SI[0]);
+            SI[1] = __dp4a(__byte_perm(w[i], w[i + 1], 0x4321), tt, SI[1]);
+            SI[2] = __dp4a(__byte_perm(w[i], w[i + 1], 0x5432), tt, SI[2]);
+            SI[3] = __dp4a(__byte_perm(w[i], w[i + 1], 0x6543), tt, SI[3]);
+        }
+    }
+    const float c1 = 4.0f * 1.01f * (float)NPIX * 1.1102230246251565e-16f * 255.0f;
+    const float c2 = 4.0f * 510.0f * 1.1102230246251565e-16f;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int N = NPIX * (int)SI[k] - st * (int)S[k];
+        const int V = NPIX * (int)SQ[k] - (int)S[k] * (int)S[k];
+        if (V <= 0) { za[k] = -2.0f; ea[k] = 0.0f; continue; }
+        const float den = __fmul_rn(ts32, __fsqrt_rn((float)V));
+        if (den < 1e-6f * (1.0f - 1e-5f)) { za[k] = -2.0f; ea[k] = 0.0f; continue; }
+        const float z = __fdiv_rn((float)N, __fmul_rn((float)NPIX, den));
+        za[k] = z;
+        ea[k] = den <= 1e-6f * (1.0f + 1e-5f)
+                    ? INFINITY
+                    : 4e-6f * fabsf(z) + 1.05f * __fdiv_rn(c1 * at32 + c2 * (float)S[k], den) + 1e-9f;
+    }
+}
+
+// The reference's float64 ZNCC of n patches of a u8 window (entry i's top-left byte at winb + eoff[i], rows WWB bytes
+// apart), EXB at a time: the whole warp forms the rounded products r x T into P, then lane i adds its patch's products in
+// the reference's sequential order (with the exact integer sums) and finishes: zncc4_u8's arithmetic and order.  The
+// lanes summing run the same instructions side by side.  Results in ez[i].
+template <int HALF>
+__device__ __noinline__ void zexact_list(const unsigned char* winb, const int* eoff, int n, const double* T, double ts,
+                                         double* P, double* ez, int lane)
+{
+    using G = U8Win<HALF>;
+    constexpr int PW = G::PW, NPIX = PW * PW;
+    for (int b0 = 0; b0 < n; b0 += EXB) {
+        const int m = n - b0 < EXB ? n - b0 : EXB;
+        __syncwarp();
+        for (int idx = lane; idx < m * NPIX; idx += 32) {
+            const int e = idx / NPIX, k = idx - e * NPIX;
+            const int r = winb[eoff[b0 + e] + (k / PW) * G::WWB + (k % PW)];
+            P[e * NPIX + k] = __dmul_rn((double)r, T[k]);
+        }
+        __syncwarp();
+        if (lane < m) {
+            const unsigned char* pb = winb + eoff[b0 + lane];
+            const double* Pe = P + lane * NPIX;
+            double sx = 0.0;
+            int S = 0, S2 = 0;
+#pragma unroll 1
+            for (int dy = 0; dy < PW; ++dy) {
+#pragma unroll
+                for (int dx = 0; dx < PW; ++dx) {
+                    const int r = pb[dy * G::WWB + dx];
+                    S += r;
+                    S2 += r * r;
+                    sx = __dadd_rn(sx, Pe[dy * PW + dx]);
+                }
+            }
+            ez[b0 + lane] = zncc_finish((double)S, (double)S2, sx, ts, NPIX);
+        }
+    }
+    __syncwarp();
+}
+
+__device__ __forceinline__ float warp_max_f(float v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+__device__ __forceinline__ double warp_max_d(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
 }
 
 // stage image rows r0 .. r0 + nrows - 1, columns c0 .. c0 + ncols - 1 of a u8 image into WWB-byte rows (column c at
@@ -530,19 +676,20 @@ __global__ void __launch_bounds__(st_warps(HALF) * 32, 2) k_stereo(
         // hi - d)
         const int wr0 = vi - band - HALF, wc0 = ui - (int)hi - HALF;
         const int nrows = PW + 2 * band, span = (int)(hi - lo), ncols = span + PW;
-        double lbest = -2.0;
-        int lbd = -1;
-        double best[4];
-        int bj[4] = {0, 0, 0, 0}, dq[4];
-        bool val[4];
-        if (FLT) {
-            // shifted float32 right image: disparities lo + lane + 32 q
+        double bs, off = 0.0;
+        int bestd, js, xr;
+        if constexpr (FLT) {
+            // shifted float32 right image: disparities lo + lane + 32 q, every ZNCC evaluated in the reference's order
+            double lbest = -2.0;
+            int lbd = -1;
+            double best[4];
+            int bj[4] = {0, 0, 0, 0}, dq[4], col[4];
+            bool val[4];
             for (int idx = lane; idx < nrows * ncols; idx += 32) {
                 int rr = idx / ncols, cc = idx % ncols;
                 win[rr * ww + cc] = R.at((size_t)(wr0 + rr) * W + wc0 + cc);
             }
             __syncwarp();
-            int col[4];
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 dq[q] = (int)lo + lane + 32 * q;
@@ -559,64 +706,35 @@ __global__ void __launch_bounds__(st_warps(HALF) * 32, 2) k_stereo(
                 for (int q = 0; q < 4; ++q)
                     if (t == 0 || z[q] > best[q]) { best[q] = z[q]; bj[q] = j; }
             }
-        } else {
-            // u8 right image: lane's disparities lo + 4 lane + q (q = 0..3) are window columns span - 4 lane - q, a
-            // block of four adjacent patches starting at column cb = span - 4 lane - 3.  The pad makes every block start
-            // on a 32-bit word; a lane whose four disparities all exceed hi starts at the lowest column >= -3 of the
-            // same residue mod 4 (pad bytes, results unused).
-            const int pad = 4 + ((3 - span) & 3);
-            stage_u8<HALF>(winb, R.r8, W, wr0, nrows, wc0, ncols, pad, lane);
-            __syncwarp();
-            int cb = span - 4 * lane - 3;
-            if (cb < -3) cb += (-cb) & ~3;
-            const unsigned char* pb = winb + pad + cb;
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                dq[q] = (int)lo + 4 * lane + q;
-                val[q] = dq[q] <= hi;
+                if (val[q]) {
+                    sc[dq[q]] = best[q];
+                    jb[dq[q]] = (signed char)bj[q];
+                    if (best[q] > lbest) { lbest = best[q]; lbd = dq[q]; }
+                }
             }
-#pragma unroll 1
-            for (int t = 0; t <= 2 * band; ++t) {
-                const int j = t == 0 ? 0 : ((t & 1) ? -((t + 1) >> 1) : (t >> 1));
-                double z[4];
-                zncc4_u8<HALF>(pb + (band + j) * U8Win<HALF>::WWB, Td, ts, z);
-#pragma unroll
-                for (int q = 0; q < 4; ++q)
-                    if (t == 0 || z[3 - q] > best[q]) { best[q] = z[3 - q]; bj[q] = j; }
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            if (val[q]) {
-                sc[dq[q]] = best[q];
-                jb[dq[q]] = (signed char)bj[q];
-                if (best[q] > lbest) { lbest = best[q]; lbd = dq[q]; }
-            }
-        }
-        double bs = lbest;
-        int bestd = lbd;
-        warp_argmax(bs, bestd);
-        if (lane == 0) ozn[oi] = bs;
-        if (bestd < 0 || bs < ZMIN) continue;
-        __syncwarp();
-        double sec = -2.0;
-        for (int d = (int)lo + lane; d <= hi; d += 32)
-            if (abs(d - bestd) > 1 && sc[d] > sec) sec = sc[d];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) sec = fmax(sec, __shfl_xor_sync(0xffffffffu, sec, o));
-        if (!(__dsub_rn(1.0, sec) > __dmul_rn(__dsub_rn(1.0, bs), UNIQ1))) continue;
+            bs = lbest;
+            bestd = lbd;
+            warp_argmax(bs, bestd);
+            if (lane == 0) ozn[oi] = bs;
+            if (bestd < 0 || bs < ZMIN) continue;
+            __syncwarp();
+            double sec = -2.0;
+            for (int d = (int)lo + lane; d <= hi; d += 32)
+                if (abs(d - bestd) > 1 && sc[d] > sec) sec = sc[d];
+            sec = warp_max_d(sec);
+            if (!(__dsub_rn(1.0, sec) > __dmul_rn(__dsub_rn(1.0, bs), UNIQ1))) continue;
 
-        // left-right check: the right patch at the peak searched back along the left row
-        const int js = jb[bestd];
-        const int xr = ui - bestd;
-        double rm, rsd;
-        float rv[KP];
+            // left-right check: the right patch at the peak searched back along the left row
+            js = jb[bestd];
+            xr = ui - bestd;
+            float rv[KP];
 #pragma unroll
-        for (int i = 0; i < KP; ++i) {
-            const int k = lane + 32 * i;
-            rv[i] = k < NPIX ? R.at((size_t)(vi + js + k / PW - HALF) * W + xr + k % PW - HALF) : 0.f;
-        }
-        if (FLT) {
+            for (int i = 0; i < KP; ++i) {
+                const int k = lane + 32 * i;
+                rv[i] = k < NPIX ? R.at((size_t)(vi + js + k / PW - HALF) * W + xr + k % PW - HALF) : 0.f;
+            }
             // float32 patch: the CPU's sequential float64 sums (x * x a float32 product)
             double a = 0.0, a2 = 0.0;
             if (lane == 0)
@@ -627,44 +745,308 @@ __global__ void __launch_bounds__(st_warps(HALF) * 32, 2) k_stereo(
                 }
             a = __shfl_sync(0xffffffffu, a, 0);
             a2 = __shfl_sync(0xffffffffu, a2, 0);
-            rm = __ddiv_rn(a, (double)NPIX);
-            double var = __dsub_rn(__ddiv_rn(a2, (double)NPIX), __dmul_rn(rm, rm));
-            rsd = __dsqrt_rn(var > 0.0 ? var : 0.0);
+            const double rm = __ddiv_rn(a, (double)NPIX);
+            const double rvar = __dsub_rn(__ddiv_rn(a2, (double)NPIX), __dmul_rn(rm, rm));
+            const double rsd = __dsqrt_rn(rvar > 0.0 ? rvar : 0.0);
+            if (rsd <= 1e-6) continue;
+#pragma unroll
+            for (int i = 0; i < KP; ++i)
+                if (lane + 32 * i < NPIX) T2d[lane + 32 * i] = __dsub_rn((double)rv[i], rm);
+            int dmax = MAXD - 1;
+            if (xr + dmax + HALF >= W) dmax = W - 1 - HALF - xr;
+            const int lc0 = xr - HALF, lcols = dmax + PW;
+            __syncwarp();
+            // left-image window, candidate c at column c: lane scores c = 4 lane .. 4 lane + 3 (pad 4: word-aligned)
+            stage_u8<HALF>(winb, L, W, vi - HALF, PW, lc0, lcols, 4, lane);
+            __syncwarp();
+            double lrb = -2.0;
+            int lrd = -1;
+            {
+                double z[4];
+                zncc4_u8<HALF>(winb + 4 + 4 * lane, T2d, rsd, z);
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    if (4 * lane + k <= dmax && z[k] > lrb) { lrb = z[k]; lrd = 4 * lane + k; }
+            }
+            warp_argmax(lrb, lrd);
+            if (lrd < 0 || fabs((double)(lrd - bestd)) > LRT) continue;
         } else {
+            // u8 right image, the search filter: lane's disparities lo + 4 lane + q (q = 0..3) are window columns
+            // span - 4 lane - q, a block of four adjacent patches starting at column cb = span - 4 lane - 3.  The pad
+            // makes every block start on a 32-bit word; a lane whose four disparities all exceed hi starts at the
+            // lowest column >= -3 of the same residue mod 4 (pad bytes, results unused).
+            using G = U8Win<HALF>;
+            constexpr int RB = 4 * G::NTW;                       // template row bytes
+            unsigned char* twb = (unsigned char*)(jb + MAXD);    // the search template's rows
+            unsigned char* twb2 = twb + PW * RB;                 // the left-right template's rows
+            int* eoff = (int*)(twb2 + PW * RB);                  // exact-evaluation entries
+            double* ez = (double*)(eoff + EZ);                   // ... their values
+            int* clist = (int*)(ez + EZ);                        // candidate disparities (or columns)
+            unsigned char* exf = (unsigned char*)(clist + EZ);   // exact value known, per disparity
+            double* P = (double*)(win + (size_t)(PW + 2 * band) * ww);    // products, after the window
+            const int NR = 2 * band + 1;                         // band rows per disparity
+            double at = 0.0;
+#pragma unroll
+            for (int i = 0; i < KP; ++i) {
+                const int k = lane + 32 * i;
+                if (k < NPIX) {
+                    twb[(k / PW) * RB + k % PW] = (unsigned char)tv[i];
+                    at = __dadd_rn(at, fabs(__dsub_rn((double)tv[i], tm)));
+                }
+            }
+            for (int k = lane; k < PW * RB; k += 32)
+                if (k % RB >= PW) twb[k] = 0;
+            for (int k = lane; k < MAXD; k += 32) exf[k] = 0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) at = __dadd_rn(at, __shfl_xor_sync(0xffffffffu, at, o));
+            const int pad = 4 + ((3 - span) & 3);
+            stage_u8<HALF>(winb, R.r8, W, wr0, nrows, wc0, ncols, pad, lane);
+            __syncwarp();
+            int cb = span - 4 * lane - 3;
+            if (cb < -3) cb += (-cb) & ~3;
+            const unsigned char* pb = winb + pad + cb;
+            int dq[4];
+            bool val[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                dq[q] = (int)lo + 4 * lane + q;
+                val[q] = dq[q] <= hi;
+            }
+            // bounds of every disparity's best row
+            float za[4], ea[4];
+            const float ts32 = (float)ts, at32 = (float)at;
+#pragma unroll 1
+            for (int t = 0; t < NR; ++t) {
+                const int j = t == 0 ? 0 : ((t & 1) ? -((t + 1) >> 1) : (t >> 1));
+                float z4[4], e4[4];
+                zapprox4_u8<HALF>(pb + (band + j) * G::WWB, (const unsigned*)twb, s, ts32, at32, z4, e4);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    za[q] = t == 0 ? z4[3 - q] : fmaxf(za[q], z4[3 - q]);
+                    ea[q] = t == 0 ? e4[3 - q] : fmaxf(ea[q], e4[3 - q]);
+                }
+            }
+            // exact values of the flagged disparities: a disparity certainly -2 (flat patch or a denominator certainly
+            // under the reference's cut in every row) is recorded directly; the others are listed, every band row of
+            // each evaluated, and the best row taken in the reference's row order (a later row only if strictly better)
+            auto exact_flagged = [&](const bool* want) {
+                int nc = 0;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const bool cert = want[q] && !(ea[q] > 0.0f);
+                    if (cert) { sc[dq[q]] = -2.0; jb[dq[q]] = 0; exf[dq[q]] = 1; }
+                    const bool lst = want[q] && ea[q] > 0.0f;
+                    const unsigned m = __ballot_sync(0xffffffffu, lst);
+                    if (lst) {
+                        const int pos = nc + __popc(m & ((1u << lane) - 1u));
+                        if (pos < 32 * 4) clist[pos % EZ] = dq[q];    // (overflow handled below)
+                    }
+                    nc += __popc(m);
+                }
+                __syncwarp();
+                if (nc > EZ) {
+                    // more candidates than one list holds (a patch nearly flat everywhere): take them in passes
+                    // straight from the flags, one disparity at a time
+                    for (int d = (int)lo; d <= hi; ++d) {
+                        bool w = false;
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) w |= (dq[q] == d) && want[q] && ea[q] > 0.0f;
+                        if (!__any_sync(0xffffffffu, w)) continue;
+                        for (int t = lane; t < NR; t += 32) {
+                            const int j = t == 0 ? 0 : ((t & 1) ? -((t + 1) >> 1) : (t >> 1));
+                            eoff[t] = pad + ((int)hi - d) + (band + j) * G::WWB;
+                        }
+                        zexact_list<HALF>(winb, eoff, NR, Td, ts, P, ez, lane);
+                        if (lane == 0) {
+                            double bz = -2.0;
+                            int bjr = 0;
+                            for (int t = 0; t < NR; ++t)
+                                if (t == 0 || ez[t] > bz) { bz = ez[t]; bjr = t == 0 ? 0 : ((t & 1) ? -((t + 1) >> 1) : (t >> 1)); }
+                            sc[d] = bz; jb[d] = (signed char)bjr; exf[d] = 1;
+                        }
+                        __syncwarp();
+                    }
+                    return;
+                }
+                const int per = EZ / NR;                         // candidates per pass
+                for (int c0 = 0; c0 < nc; c0 += per) {
+                    const int m = nc - c0 < per ? nc - c0 : per;
+                    for (int i = lane; i < m * NR; i += 32) {
+                        const int c = i / NR, t = i - c * NR;
+                        const int j = t == 0 ? 0 : ((t & 1) ? -((t + 1) >> 1) : (t >> 1));
+                        eoff[i] = pad + ((int)hi - clist[c0 + c]) + (band + j) * G::WWB;
+                    }
+                    zexact_list<HALF>(winb, eoff, m * NR, Td, ts, P, ez, lane);
+                    if (lane < m) {
+                        double bz = -2.0;
+                        int bjr = 0;
+                        for (int t = 0; t < NR; ++t)
+                            if (t == 0 || ez[lane * NR + t] > bz) {
+                                bz = ez[lane * NR + t];
+                                bjr = t == 0 ? 0 : ((t & 1) ? -((t + 1) >> 1) : (t >> 1));
+                            }
+                        const int d = clist[c0 + lane];
+                        sc[d] = bz; jb[d] = (signed char)bjr; exf[d] = 1;
+                    }
+                    __syncwarp();
+                }
+            };
+            // round A: the candidates for the maximum, the approximate peak's neighbours, the candidates for the second
+            // peak away from it
+            float lbq = -INFINITY, am = -INFINITY;
+            int ad = 0x7fffffff;
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (val[q]) {
+                    lbq = fmaxf(lbq, za[q] - ea[q]);
+                    if (za[q] > am) { am = za[q]; ad = dq[q]; }
+                }
+            const float lb = warp_max_f(lbq);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const float a2 = __shfl_xor_sync(0xffffffffu, am, o);
+                const int d2 = __shfl_xor_sync(0xffffffffu, ad, o);
+                if (a2 > am || (a2 == am && d2 < ad)) { am = a2; ad = d2; }
+            }
+            float l2q = -INFINITY;
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (val[q] && abs(dq[q] - ad) > 1) l2q = fmaxf(l2q, za[q] - ea[q]);
+            const float lb2 = warp_max_f(l2q);
+            {
+                bool want[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int dd = abs(dq[q] - ad);
+                    want[q] = val[q] && (za[q] + ea[q] >= lb || dd == 1 || (dd > 1 && za[q] + ea[q] >= lb2));
+                }
+                exact_flagged(want);
+            }
+            double lbest = -2.0;
+            int lbd = -1;
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (val[q] && exf[dq[q]] && sc[dq[q]] > lbest) { lbest = sc[dq[q]]; lbd = dq[q]; }
+            bs = lbest;
+            bestd = lbd;
+            warp_argmax(bs, bestd);
+            if (lane == 0) ozn[oi] = bs;
+            if (bestd < 0 || bs < ZMIN) continue;
+            if (bestd != ad) {
+                // round B (the exact peak is not the approximate one): the second-peak candidates and neighbours
+                double l2d = -INFINITY;
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    if (val[q] && abs(dq[q] - bestd) > 1)
+                        l2d = fmax(l2d, exf[dq[q]] ? sc[dq[q]] : (double)za[q] - (double)ea[q]);
+                l2d = warp_max_d(l2d);
+                bool want[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int dd = abs(dq[q] - bestd);
+                    want[q] = val[q] && !exf[dq[q]] && (dd == 1 || (dd > 1 && (double)za[q] + (double)ea[q] >= l2d));
+                }
+                exact_flagged(want);
+            }
+            double sec = -2.0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (val[q] && exf[dq[q]] && abs(dq[q] - bestd) > 1 && sc[dq[q]] > sec) sec = sc[dq[q]];
+            sec = warp_max_d(sec);
+            __syncwarp();
+            if (!(__dsub_rn(1.0, sec) > __dmul_rn(__dsub_rn(1.0, bs), UNIQ1))) continue;
+
+            // left-right check: the right patch at the peak searched back along the left row, through the same filter
+            js = jb[bestd];
+            xr = ui - bestd;
+            int rvi[KP];
+#pragma unroll
+            for (int i = 0; i < KP; ++i) {
+                const int k = lane + 32 * i;
+                rvi[i] = k < NPIX ? (int)R.r8[(size_t)(vi + js + k / PW - HALF) * W + xr + k % PW - HALF] : 0;
+            }
             int a = 0, a2 = 0;
 #pragma unroll
-            for (int i = 0; i < KP; ++i) { const int x = (int)rv[i]; a += x; a2 += x * x; }
+            for (int i = 0; i < KP; ++i) { a += rvi[i]; a2 += rvi[i] * rvi[i]; }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) { a += __shfl_xor_sync(0xffffffffu, a, o); a2 += __shfl_xor_sync(0xffffffffu, a2, o); }
-            rm = __ddiv_rn((double)a, (double)NPIX);
-            double var = __dsub_rn(__ddiv_rn((double)a2, (double)NPIX), __dmul_rn(rm, rm));
-            rsd = __dsqrt_rn(var > 0.0 ? var : 0.0);
-        }
-        if (rsd <= 1e-6) continue;
+            const double rm = __ddiv_rn((double)a, (double)NPIX);
+            const double rvar = __dsub_rn(__ddiv_rn((double)a2, (double)NPIX), __dmul_rn(rm, rm));
+            const double rsd = __dsqrt_rn(rvar > 0.0 ? rvar : 0.0);
+            if (rsd <= 1e-6) continue;
+            double at2 = 0.0;
 #pragma unroll
-        for (int i = 0; i < KP; ++i)
-            if (lane + 32 * i < NPIX) T2d[lane + 32 * i] = __dsub_rn((double)rv[i], rm);
-        int dmax = MAXD - 1;
-        if (xr + dmax + HALF >= W) dmax = W - 1 - HALF - xr;
-        const int lc0 = xr - HALF, lcols = dmax + PW;
-        __syncwarp();
-        // left-image window, candidate c at column c: lane scores c = 4 lane .. 4 lane + 3 (pad 4: word-aligned blocks)
-        stage_u8<HALF>(winb, L, W, vi - HALF, PW, lc0, lcols, 4, lane);
-        __syncwarp();
-        double lrb = -2.0;
-        int lrd = -1;
-        {
-            double z[4];
-            zncc4_u8<HALF>(winb + 4 + 4 * lane, T2d, rsd, z);
+            for (int i = 0; i < KP; ++i) {
+                const int k = lane + 32 * i;
+                if (k < NPIX) {
+                    const double tk = __dsub_rn((double)rvi[i], rm);
+                    T2d[k] = tk;
+                    at2 = __dadd_rn(at2, fabs(tk));
+                    twb2[(k / PW) * RB + k % PW] = (unsigned char)rvi[i];
+                }
+            }
+            for (int k = lane; k < PW * RB; k += 32)
+                if (k % RB >= PW) twb2[k] = 0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) at2 = __dadd_rn(at2, __shfl_xor_sync(0xffffffffu, at2, o));
+            int dmax = MAXD - 1;
+            if (xr + dmax + HALF >= W) dmax = W - 1 - HALF - xr;
+            const int lc0 = xr - HALF, lcols = dmax + PW;
+            __syncwarp();
+            // left-image window, candidate c at column c: lane bounds c = 4 lane .. 4 lane + 3 (pad 4: word-aligned)
+            stage_u8<HALF>(winb, L, W, vi - HALF, PW, lc0, lcols, 4, lane);
+            __syncwarp();
+            float z4[4], e4[4];
+            zapprox4_u8<HALF>(winb + 4 + 4 * lane, (const unsigned*)twb2, a, (float)rsd, (float)at2, z4, e4);
+            float lq = -INFINITY;
 #pragma unroll
             for (int k = 0; k < 4; ++k)
-                if (4 * lane + k <= dmax && z[k] > lrb) { lrb = z[k]; lrd = 4 * lane + k; }
+                if (4 * lane + k <= dmax) lq = fmaxf(lq, z4[k] - e4[k]);
+            const float llb = warp_max_f(lq);
+            // the candidates (a column certainly at -2 can never be the maximum, which must exceed -2)
+            int nc = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const bool lst = 4 * lane + k <= dmax && z4[k] + e4[k] >= llb && e4[k] > 0.0f;
+                const unsigned m = __ballot_sync(0xffffffffu, lst);
+                if (lst) {
+                    const int pos = nc + __popc(m & ((1u << lane) - 1u));
+                    if (pos < EZ) { clist[pos] = 4 * lane + k; eoff[pos] = 4 + 4 * lane + k; }
+                }
+                nc += __popc(m);
+            }
+            double lrb = -2.0;
+            int lrd = -1;
+            for (int c0 = 0; c0 < nc; c0 += EZ) {
+                const int m = nc - c0 < EZ ? nc - c0 : EZ;
+                if (c0 > 0) {
+                    // a further pass (more than EZ candidates): list them again from the bounds
+                    int pos = 0;
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const bool lst = 4 * lane + k <= dmax && z4[k] + e4[k] >= llb && e4[k] > 0.0f;
+                        const unsigned mk = __ballot_sync(0xffffffffu, lst);
+                        if (lst) {
+                            const int p2 = pos + __popc(mk & ((1u << lane) - 1u)) - c0;
+                            if (p2 >= 0 && p2 < EZ) { clist[p2] = 4 * lane + k; eoff[p2] = 4 + 4 * lane + k; }
+                        }
+                        pos += __popc(mk);
+                    }
+                }
+                __syncwarp();
+                zexact_list<HALF>(winb, eoff, m, T2d, rsd, P, ez, lane);
+                for (int i = lane; i < m; i += 32) {
+                    const double z = ez[i];
+                    const int c = clist[i];
+                    if (z > lrb || (z == lrb && lrd >= 0 && c < lrd)) { lrb = z; lrd = c; }
+                }
+                __syncwarp();
+            }
+            warp_argmax(lrb, lrd);
+            if (lrd < 0 || fabs((double)(lrd - bestd)) > LRT) continue;
         }
-        warp_argmax(lrb, lrd);
-        if (lrd < 0 || fabs((double)(lrd - bestd)) > LRT) continue;
 
         // parabola seed of the LK (from the sub-pixel keypoint position)
-        double off = 0.0;
         if (bestd > lo && bestd < hi) {
             double y0 = sc[bestd - 1], y2 = sc[bestd + 1];
             double den = __dadd_rn(__dsub_rn(y0, __dmul_rn(2.0, bs)), y2);
@@ -743,7 +1125,8 @@ __global__ void __launch_bounds__(st_warps(HALF) * 32, 2) k_stereo(
                 int tr = ty0 - ly0;
                 tr = tr < 0 ? 0 : (tr > PW ? PW : tr);
                 const unsigned char* lrow = lb + tr * LS;
-#pragma unroll
+                // three pixels per unrolled step: a full unroll of the row spills at the 128-register budget
+#pragma unroll 3
                 for (int dx = 0; dx < PW; ++dx) {
                     const double px = __dadd_rn(u, (double)(dx - HALF));
                     // template sample: bilinear left at (px, py) (stereo1d._bil); u8 differences are exact
@@ -819,75 +1202,69 @@ __global__ void __launch_bounds__(st_warps(HALF) * 32, 2) k_stereo(
     }
 
     // --------------------------------------------------------------------------------------- phase C: vertical scans
-    unsigned okm = __ballot_sync(0xffffffffu, okl);
-    double* Tv = (double*)U;                                    // the point's template minus its mean
-    float* vsf = (float*)(U + (size_t)NPIX * 8);                // the scan block
-    while (okm) {
-        const int j = __ffs(okm) - 1;
-        okm &= okm - 1;
-        const StJob J = jobs[j];
-        const int vi = J.vi, xr = J.xr;
-        // the point's own vertical offset: column scan of the ZNCC at the matched integer disparity
-        if (!(vi - 2 * HALF - 1 >= 0 && vi + 2 * HALF + 1 < H)) continue;
-        __syncwarp();
-        const u8* L = Lall + (size_t)J.f * H * W;
-        RightImg<FLT> R;
-        R.r8 = R8all ? R8all + (size_t)J.f * H * W : nullptr;
-        R.rf = Rsall ? Rsall + (size_t)J.f * H * W : nullptr;
-        {
-            int tv[KP];
+    // one lane per accepted job: the ZNCC of the matched right patch's column neighbourhood (scan offsets -HALF ..
+    // HALF), its PW patches summed side by side, each in the reference's pixel order; then the first maximum and the
+    // parabola.  The template (the left patch minus its mean) and the right pixels come from global memory (L1).
+    if (okl) {
+        const StJob J = jobs[lane];
+        const int vi = J.vi, xr = J.xr, ui = J.ui;
+        if (vi - 2 * HALF - 1 >= 0 && vi + 2 * HALF + 1 < H) {
+            const u8* L = Lall + (size_t)J.f * H * W;
+            RightImg<FLT> R;
+            R.r8 = R8all ? R8all + (size_t)J.f * H * W : nullptr;
+            R.rf = Rsall ? Rsall + (size_t)J.f * H * W : nullptr;
+            int st = 0;
+#pragma unroll 1
+            for (int k = 0; k < NPIX; ++k) st += (int)L[(size_t)(vi + k / PW - HALF) * W + ui + k % PW - HALF];
+            const double tm = __ddiv_rn((double)st, (double)NPIX);
+            double sx[PW], zs[PW], zs2[PW];
+            int is[PW], is2[PW];
 #pragma unroll
-            for (int i = 0; i < KP; ++i) {
-                const int k = lane + 32 * i;
-                tv[i] = k < NPIX ? (int)L[(size_t)(vi + k / PW - HALF) * W + J.ui + k % PW - HALF] : 0;
+            for (int j = 0; j < PW; ++j) { sx[j] = 0.0; zs[j] = 0.0; zs2[j] = 0.0; is[j] = 0; is2[j] = 0; }
+            const size_t r0 = (size_t)(vi - 2 * HALF) * W + (xr - HALF);
+#pragma unroll 1
+            for (int dy = 0; dy < PW; ++dy) {
+#pragma unroll 1
+                for (int dx = 0; dx < PW; ++dx) {
+                    const double T = __dsub_rn((double)L[(size_t)(vi + dy - HALF) * W + ui + dx - HALF], tm);
+                    const size_t o = r0 + (size_t)dy * W + dx;
+#pragma unroll
+                    for (int j = 0; j < PW; ++j) {
+                        const float rf = R.at(o + (size_t)j * W);
+                        const double r = (double)rf;
+                        if (FLT) {
+                            zs[j] = __dadd_rn(zs[j], r);
+                            zs2[j] = __dadd_rn(zs2[j], (double)__fmul_rn(rf, rf));
+                        } else {
+                            const int iv = (int)rf;
+                            is[j] += iv;
+                            is2[j] += iv * iv;
+                        }
+                        sx[j] = __dadd_rn(sx[j], __dmul_rn(r, T));
+                    }
+                }
             }
-            int s = 0;
+            double z[PW];
 #pragma unroll
-            for (int i = 0; i < KP; ++i) s += tv[i];
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            const double tm = __ddiv_rn((double)s, (double)NPIX);
-#pragma unroll
-            for (int i = 0; i < KP; ++i)
-                if (lane + 32 * i < NPIX) Tv[lane + 32 * i] = __dsub_rn((double)tv[i], tm);
-        }
-        // image rows vi - 2 HALF .. vi + 2 HALF, columns xr - HALF .. xr + HALF
-#pragma unroll
-        for (int i = 0; i < ((2 * PW - 1) * PW + 31) / 32; ++i) {
-            const int idx = lane + 32 * i;
-            if (idx < (2 * PW - 1) * PW) {
-                const int rr = idx / PW, cc = idx - rr * PW;
-                vsf[idx] = R.at((size_t)(vi - 2 * HALF + rr) * W + xr - HALF + cc);
+            for (int j = 0; j < PW; ++j) {
+                if (!FLT) { zs[j] = (double)is[j]; zs2[j] = (double)is2[j]; }
+                z[j] = zncc_finish(zs[j], zs2[j], sx[j], J.ts, NPIX);
             }
-        }
-        __syncwarp();
-        double z = -2.0;
-        if (lane < PW) {
-            // lane j scores rows vi + j - 2 HALF .. vi + j (staged rows j .. j + PW - 1).  Sums of u8 values and of
-            // their squares are exact in float64 in any order; the shifted float32 image keeps the CPU's float32 square.
-            double zs = 0.0, zs2 = 0.0, sx = 0.0;
-#pragma unroll 9
-            for (int k = 0; k < NPIX; ++k) {
-                const float rf = vsf[(lane + k / PW) * PW + k % PW];
-                const double r = (double)rf;
-                zs = __dadd_rn(zs, r);
-                zs2 = __dadd_rn(zs2, FLT ? (double)__fmul_rn(rf, rf) : __dmul_rn(r, r));
-                sx = __dadd_rn(sx, __dmul_rn(r, Tv[k]));
-            }
-            z = zncc_finish(zs, zs2, sx, J.ts, NPIX);
-        }
-        double col[PW];
-#pragma unroll
-        for (int jj = 0; jj < PW; ++jj) col[jj] = __shfl_sync(0xffffffffu, z, jj);
-        if (lane == 0) {
+            // the first maximum above -2 (row 0 when none), then the parabola from its neighbours
             int jp = 0;
             double cs = -2.0;
-            for (int jj = -HALF; jj <= HALF; ++jj)
-                if (col[jj + HALF] > cs) { cs = col[jj + HALF]; jp = jj; }
+#pragma unroll
+            for (int j = 0; j < PW; ++j)
+                if (z[j] > cs) { cs = z[j]; jp = j - HALF; }
+            double y0 = 0.0, y2 = 0.0;
+#pragma unroll
+            for (int j = 0; j < PW; ++j) {
+                if (j == jp - 1 + HALF) y0 = z[j];
+                if (j == jp + 1 + HALF) y2 = z[j];
+            }
             double offy = 0.0;
             if (jp > -HALF && jp < HALF) {
-                double y0 = col[jp - 1 + HALF], y2 = col[jp + 1 + HALF];
-                double den = __dadd_rn(__dsub_rn(y0, __dmul_rn(2.0, cs)), y2);
+                const double den = __dadd_rn(__dsub_rn(y0, __dmul_rn(2.0, cs)), y2);
                 if (den < -1e-9) {
                     offy = __ddiv_rn(__dmul_rn(0.5, __dsub_rn(y0, y2)), den);
                     if (offy > 0.5) offy = 0.5;
@@ -906,9 +1283,26 @@ static cudaError_t launch_stereo_t(const uint8_t* L, const uint8_t* R8, const fl
                                    double* od, double* osig, uint8_t* ook, double* ozn, double* ody, long long npts,
                                    int warps, int grp, cudaStream_t st)
 {
-    const int NW = warps >= 1 && warps <= st_warps(HALF) ? warps : st_warps(HALF);
-    const int G = grp >= 1 && grp <= ST_GROUP ? grp : ST_GROUP;
+    int NW = warps >= 1 && warps <= st_warps(HALF) ? warps : st_warps(HALF);
+    // points per warp: the knob, else as many as fill two blocks per SM once (a small call spreads over every SM with
+    // one point per warp; a large batch takes ST_GROUP, which gives the LKs a full warp of lanes)
+    int G = grp;
+    if (!(G >= 1 && G <= ST_GROUP)) {
+        static int sms[64];
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (dev < 0 || dev >= 64) dev = 0;
+        if (!sms[dev]) {
+            int v = 0;
+            cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+            sms[dev] = v > 0 ? v : 148;
+        }
+        const long long slots = (long long)sms[dev] * 2 * NW;
+        const long long g = (npts + slots - 1) / slots;
+        G = g < 1 ? 1 : (g > ST_GROUP ? ST_GROUP : (int)g);
+    }
     size_t pw = (xcb_stereo_smem_per_warp(HALF, band) + 15) & ~(size_t)15;
+    if ((size_t)NW * pw > ST_SMEM_MAX) NW = (int)(ST_SMEM_MAX / pw);    // the widest bands: fewer warps per block
     size_t sm = pw * NW;
     const long long per_block = (long long)NW * G;
     long long nb = (npts + per_block - 1) / per_block;
@@ -925,7 +1319,7 @@ cudaError_t xcb_stereo_init_attrs()
 #define XCB_SA(HH, FF)                                                                                            \
     if (e == cudaSuccess)                                                                                         \
         e = cudaFuncSetAttribute(k_stereo<HH, FF>, cudaFuncAttributeMaxDynamicSharedMemorySize,                   \
-                                 (int)(((xcb_stereo_smem_per_warp(HH, BAND_MAX) + 15) & ~(size_t)15) * st_warps(HH)));
+                                 (int)st_smem_attr(HH));
     XCB_SA(3, false) XCB_SA(3, true) XCB_SA(4, false) XCB_SA(4, true) XCB_SA(5, false) XCB_SA(5, true)
 #undef XCB_SA
     return e;
