@@ -77,6 +77,8 @@ struct xcb_front {
     long long *d_lo, *d_hi;
     double *d_pd, *d_psig, *d_pzn, *d_pdy;
     u8* d_pok;
+    u8* d_pjobs;           // the stereo's job list for the host-API points (xcb_stereo_jobs_bytes(pts_cap))
+    u8* d_jobs;            // the stereo's job list for the batched pipeline (max_frames x cap points)
     // Hamming host-API buffers
     int ham_capL, ham_capN;
     u8 *d_hA, *d_hB;
@@ -397,6 +399,7 @@ extern "C" int xcb_front_create(int width, int height, int cap, int max_frames, 
     AL(f->d_m1, F * cap);
     AL(f->d_nmatch, F);
     AL(f->d_err, 1);
+    AL(f->d_jobs, xcb_stereo_jobs_bytes((long long)F * cap));
 #undef AL
     cudaMemset(f->d_counts_chain, 0, (F + 1) * sizeof(int));
     cudaMemset(f->d_err, 0, sizeof(unsigned int));
@@ -605,6 +608,7 @@ static int grow_points(xcb_front* f, int n)
     CK(dalloc(f, &f->d_pzn, (size_t)c), "alloc points");
     CK(dalloc(f, &f->d_pdy, (size_t)c), "alloc points");
     CK(dalloc(f, &f->d_pok, (size_t)c), "alloc points");
+    CK(dalloc(f, &f->d_pjobs, xcb_stereo_jobs_bytes(c)), "alloc points");
     f->pts_cap = c;
     return XCB_OK;
 }
@@ -640,7 +644,7 @@ extern "C" int xcb_front_stereo_host(xcb_front* f, const uint8_t* left, const ui
     }
     CK(xcb_launch_stereo(f->d_left, f->d_right, Rs, 1, f->H, f->W, f->d_kpd, (const long long*)f->d_lo,
                          (const long long*)f->d_hi, n, nullptr, nullptr, 0, 0, 0, band, half, f->d_pd, f->d_psig,
-                         f->d_pok, f->d_pzn, f->d_pdy, f->d_err, f->tune[XCB_TUNE_STEREO_WARPS],
+                         f->d_pok, f->d_pzn, f->d_pdy, f->d_err, f->d_pjobs, f->tune[XCB_TUNE_STEREO_WARPS],
                          f->tune[XCB_TUNE_STEREO_GROUP], st), "stereo");
     CK(cudaMemcpyAsync(d, f->d_pd, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
     CK(cudaMemcpyAsync(sig, f->d_psig, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
@@ -770,7 +774,7 @@ static int enqueue_pipeline(xcb_front* f, const u8* left, const u8* right, int F
     if (rc) return rc;
     int* counts = f->d_counts_chain + 1;
     CK(xcb_launch_stereo(left, right, nullptr, F, f->H, f->W, nullptr, nullptr, nullptr, F, f->d_kp, counts, f->cap,
-                         dlo, dhi, 0, half, f->d_d, f->d_sig, f->d_ok, f->d_zn, f->d_dy, f->d_err,
+                         dlo, dhi, 0, half, f->d_d, f->d_sig, f->d_ok, f->d_zn, f->d_dy, f->d_err, f->d_jobs,
                          f->tune[XCB_TUNE_STEREO_WARPS], f->tune[XCB_TUNE_STEREO_GROUP], st), "stereo");
     CK(mark(ev, 6, st), "event");
     if (!match_prev) CK(cudaMemsetAsync(f->d_counts_chain, 0, sizeof(int), st), "memset");
@@ -790,7 +794,7 @@ static int enqueue_pipeline(xcb_front* f, const u8* left, const u8* right, int F
     CK(cudaMemcpyAsync(f->d_desc_chain, f->d_desc_chain + (size_t)F * f->cap * 32, (size_t)f->cap * 32,
                        cudaMemcpyDeviceToDevice, st), "carry desc");
     CK(cudaMemcpyAsync(f->d_counts_chain, f->d_counts_chain + F, sizeof(int), cudaMemcpyDeviceToDevice, st), "carry count");
-    *nl += 4;
+    *nl += 5;                        // stereo search + LK, hamming, match epilogue (+ the carry copies)
     return XCB_OK;
 }
 

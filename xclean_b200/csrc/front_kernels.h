@@ -53,8 +53,10 @@ cudaError_t xcb_launch_stereo(const uint8_t* L, const uint8_t* R8, const float* 
                               const double* kpd, const long long* dlo_a, const long long* dhi_a, int n,
                               const float* kpf, const int* counts, int cap, int dlo, int dhi, int band, int half,
                               double* od, double* osig, uint8_t* ook, double* ozn, double* ody, unsigned int* err,
-                              int warps, int grp, cudaStream_t st);
-size_t xcb_stereo_smem_per_warp(int half, int band);
+                              void* jobs, int warps, int grp, cudaStream_t st);
+// the search kernel appends the points that pass to a job list for the LK kernel: xcb_stereo_jobs_bytes(points) of
+// device scratch per launch (one launch at a time per buffer)
+size_t xcb_stereo_jobs_bytes(long long npts);
 cudaError_t xcb_launch_lkcheck(const double* As, const double* gs, int n, double* X, double* Inv, cudaStream_t st);
 
 // Hamming over frame pairs: pair p matches A_p (LA[p] rows at A + p * strideA) with B_p.  Lengths are read on the

@@ -67,26 +67,52 @@ static __host__ __device__ __forceinline__ size_t stereo_off_u(int half)
     return ((size_t)npix * 16 + MAXD * 8 + MAXD + 2 * (size_t)pw * 4 * ntw + st_exact_bytes() + 15) & ~(size_t)15;
 }
 
-static __host__ __device__ __forceinline__ size_t stereo_warp_bytes(int half, int band)
+// the u8 window's row stride (U8Win<HALF>::WWB for a run-time half)
+static __host__ __device__ __forceinline__ int u8_wwb(int half)
 {
-    int pw = 2 * half + 1, npix = pw * pw;
-    size_t search = stereo_off_u(half) + (size_t)(pw + 2 * band) * win_w(half) * 4 + (size_t)EXB * npix * 8;
-    size_t lk = (size_t)ST_GROUP * lk_job_bytes(half);
-    size_t vert = (size_t)npix * 8 + (size_t)(2 * pw - 1) * pw * 4;
-    size_t u = search > lk ? search : lk;
-    if (vert > u) u = vert;
-    return (st_jobs_bytes() + u + 15) & ~(size_t)15;
+    const int pw = 2 * half + 1, nwd = (pw + 3 + 3) / 4, nsw = (pw + 3) / 4 + 1;
+    return (MAXD + 4 * (nsw > nwd ? nsw : nwd) + 8 + 3) & ~3;
 }
 
-size_t xcb_stereo_smem_per_warp(int half, int band) { return stereo_warp_bytes(half, band); }
+// per-warp shared memory of the search kernel: U (see below) with the window sized for its image type, then the
+// exact evaluation's products
+static __host__ __device__ __forceinline__ size_t st_win_bytes(int half, int band, bool flt)
+{
+    const int rows = 2 * half + 1 + 2 * band;
+    const size_t b = flt ? (size_t)rows * win_w(half) * 4 : (size_t)rows * u8_wwb(half);
+    return (b + 15) & ~(size_t)15;
+}
+
+static __host__ __device__ __forceinline__ size_t stereo_search_bytes(int half, int band, bool flt)
+{
+    const int pw = 2 * half + 1, npix = pw * pw;
+    return (stereo_off_u(half) + st_win_bytes(half, band, flt) + (size_t)EXB * npix * 8 + 15) & ~(size_t)15;
+}
+
+// the vertical scan's staged block of a job (u8 images): the right image's 2 PW - 1 rows x PW columns around the
+// match, then the template's PW x PW bytes; an odd word stride, so lanes reading their own jobs hit distinct banks
+static __host__ __device__ __forceinline__ int st_vjob_bytes(int half)
+{
+    const int pw = 2 * half + 1;
+    int words = ((2 * pw - 1) * pw + pw * pw + 3) / 4;
+    if (!(words & 1)) ++words;
+    return 4 * words;
+}
+
+// per-warp shared memory of the LK kernel: its jobs, then the LK blocks (later the vertical-scan blocks)
+static __host__ __device__ __forceinline__ size_t stereo_lk_bytes(int half)
+{
+    const size_t lk = (size_t)ST_GROUP * lk_job_bytes(half), vs = (size_t)ST_GROUP * st_vjob_bytes(half);
+    return (st_jobs_bytes() + (lk > vs ? lk : vs) + 15) & ~(size_t)15;
+}
 
 // the shared-memory opt-in limit of a block (227 KB); a launch whose warps would need more takes fewer warps
 #define ST_SMEM_MAX ((size_t)227 * 1024)
 
-// the dynamic shared memory the kernel is enabled for: the widest band's block, at most the opt-in limit
-static size_t st_smem_attr(int half)
+// the dynamic shared memory the search kernel is enabled for: the widest band's block, at most the opt-in limit
+static size_t st_smem_attr(int half, bool flt)
 {
-    const size_t pw = (stereo_warp_bytes(half, BAND_MAX) + 15) & ~(size_t)15;
+    const size_t pw = stereo_search_bytes(half, BAND_MAX, flt);
     size_t b = pw * st_warps(half);
     if (b > ST_SMEM_MAX) b = (ST_SMEM_MAX / pw) * pw;
     return b;
@@ -578,34 +604,29 @@ __device__ __forceinline__ double u8d(unsigned b)
     return __dsub_rn(__hiloint2double(0x43300000, (int)b), 4503599627370496.0);
 }
 
-// One warp per group of ST_GROUP points.  Phase A: the whole warp takes the group's points one after another through
-// the template statistics, the ZNCC search over the row band, the uniqueness test and the left-right check (lanes
-// split the disparities); each point that passes becomes an LK job.  Phase B: the warp stages every job's right- and
-// left-image neighbourhood, then each lane runs one job's affine LK (LK_ITERS steps and the covariance pass) with its
-// ten sums in the CPU's sequential order and its own 3x3 OpenBLAS solve: the serial float64 chains of 32 points run side
-// by side instead of one point's chains idling 31 lanes.  Phase C: the whole warp takes each accepted job through the
-// vertical scan.
+// The search kernel: one warp per group of points (grp points, one after another).  The whole warp takes each point
+// through the template statistics, the ZNCC search over the row band, the uniqueness test and the left-right check
+// (lanes split the disparities); each point that passes is appended to the job list (gjobs, *gcount) for the LK kernel.
+// Two blocks per SM of up to 128 registers (three blocks at 80 registers spilled and measured slower); the LK's registers
+// and shared memory live in the other kernel.
+#define ST_SEARCH_MINB 2
 template <int HALF, bool FLT>
-__global__ void __launch_bounds__(st_warps(HALF) * 32, 2) k_stereo(
+__global__ void __launch_bounds__(st_warps(HALF) * 32, ST_SEARCH_MINB) k_stereo_search(
     const u8* __restrict__ Lall, const u8* __restrict__ R8all, const float* __restrict__ Rsall, int H, int W,
     const double* __restrict__ kpd, const long long* __restrict__ dlo_a, const long long* __restrict__ dhi_a, int n,
     const float* __restrict__ kpf, const int* __restrict__ counts, int cap, int dlo_s, int dhi_s, int band,
     double* __restrict__ od, double* __restrict__ osig, u8* __restrict__ ook, double* __restrict__ ozn,
-    double* __restrict__ ody, int grp)
+    double* __restrict__ ody, int grp, StJob* __restrict__ gjobs, int* __restrict__ gcount)
 {
     constexpr int PW = 2 * HALF + 1, NPIX = PW * PW;
     const int NW = blockDim.x >> 5;                        // warps per block (at most st_warps(HALF))
-    constexpr int LKR = PW + 2, LKW = PW + 2 * LK_MG + 2;
     static_assert(U8Win<HALF>::WWB <= 4 * (((MAXD + 2 * HALF) + 3) & ~3), "u8 rows fit the float32 window rows");
     static_assert(sizeof(StJob) == 64, "job record");
-    const int RS = lk_rs(HALF), LS = lk_ls(HALF), JB = lk_job_bytes(HALF);
     const double ZMIN = 0.5, UNIQ1 = 1.0 + 0.05, LRT = 1.0;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int ww = win_w(HALF);
-    unsigned char* base = smem_raw + (size_t)wid * stereo_warp_bytes(HALF, band);
-    StJob* jobs = (StJob*)base;
-    unsigned char* U = base + st_jobs_bytes();
+    unsigned char* U = smem_raw + (size_t)wid * stereo_search_bytes(HALF, band, FLT);
     double* Td = (double*)U;
     double* T2d = Td + NPIX;
     double* sc = T2d + NPIX;
@@ -616,7 +637,6 @@ __global__ void __launch_bounds__(st_warps(HALF) * 32, 2) k_stereo(
 
     // ------------------------------------------------------------------------------------------- phase A: searches
     const long long g0 = ((long long)blockIdx.x * NW + wid) * grp;     // grp <= ST_GROUP points per warp
-    int njobs = 0;
 #pragma unroll 1
     for (int gi = 0; gi < grp; ++gi) {
         const long long p = g0 + gi;
@@ -659,6 +679,12 @@ __global__ void __launch_bounds__(st_warps(HALF) * 32, 2) k_stereo(
             const int k = lane + 32 * i;
             tv[i] = k < NPIX ? (int)L[(size_t)(vi + k / PW - HALF) * W + ui + k % PW - HALF] : 0;
         }
+        // right-image window: rows vi-band-HALF .. vi+band+HALF, columns ui-hi-HALF .. ui-lo+HALF (window column =
+        // hi - d); u8 images stage it now, its loads in flight with the template's
+        const int wr0 = vi - band - HALF, wc0 = ui - (int)hi - HALF;
+        const int nrows = PW + 2 * band, span = (int)(hi - lo), ncols = span + PW;
+        const int pad = 4 + ((3 - span) & 3);
+        if (!FLT) stage_u8<HALF>(winb, R.r8, W, wr0, nrows, wc0, ncols, pad, lane);
         int s = 0, s2 = 0;
 #pragma unroll
         for (int i = 0; i < KP; ++i) { s += tv[i]; s2 += tv[i] * tv[i]; }
@@ -672,10 +698,6 @@ __global__ void __launch_bounds__(st_warps(HALF) * 32, 2) k_stereo(
         for (int i = 0; i < KP; ++i)
             if (lane + 32 * i < NPIX) Td[lane + 32 * i] = __dsub_rn((double)tv[i], tm);
 
-        // right-image window: rows vi-band-HALF .. vi+band+HALF, columns ui-hi-HALF .. ui-lo+HALF (window column =
-        // hi - d)
-        const int wr0 = vi - band - HALF, wc0 = ui - (int)hi - HALF;
-        const int nrows = PW + 2 * band, span = (int)(hi - lo), ncols = span + PW;
         double bs, off = 0.0;
         int bestd, js, xr;
         if constexpr (FLT) {
@@ -783,7 +805,7 @@ __global__ void __launch_bounds__(st_warps(HALF) * 32, 2) k_stereo(
             double* ez = (double*)(eoff + EZ);                   // ... their values
             int* clist = (int*)(ez + EZ);                        // candidate disparities (or columns)
             unsigned char* exf = (unsigned char*)(clist + EZ);   // exact value known, per disparity
-            double* P = (double*)(win + (size_t)(PW + 2 * band) * ww);    // products, after the window
+            double* P = (double*)(winb + st_win_bytes(HALF, band, FLT));   // products, after the window
             const int NR = 2 * band + 1;                         // band rows per disparity
             double at = 0.0;
 #pragma unroll
@@ -799,9 +821,7 @@ __global__ void __launch_bounds__(st_warps(HALF) * 32, 2) k_stereo(
             for (int k = lane; k < MAXD; k += 32) exf[k] = 0;
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) at = __dadd_rn(at, __shfl_xor_sync(0xffffffffu, at, o));
-            const int pad = 4 + ((3 - span) & 3);
-            stage_u8<HALF>(winb, R.r8, W, wr0, nrows, wc0, ncols, pad, lane);
-            __syncwarp();
+            __syncwarp();                                        // the window and the template rows
             int cb = span - 4 * lane - 3;
             if (cb < -3) cb += (-cb) & ~3;
             const unsigned char* pb = winb + pad + cb;
@@ -965,6 +985,12 @@ __global__ void __launch_bounds__(st_warps(HALF) * 32, 2) k_stereo(
                 const int k = lane + 32 * i;
                 rvi[i] = k < NPIX ? (int)R.r8[(size_t)(vi + js + k / PW - HALF) * W + xr + k % PW - HALF] : 0;
             }
+            // the left-image window, its loads in flight with the patch's (the right window is no longer read):
+            // candidate c at column c, lane bounds c = 4 lane .. 4 lane + 3 (pad 4: word-aligned)
+            int dmax = MAXD - 1;
+            if (xr + dmax + HALF >= W) dmax = W - 1 - HALF - xr;
+            const int lc0 = xr - HALF, lcols = dmax + PW;
+            stage_u8<HALF>(winb, L, W, vi - HALF, PW, lc0, lcols, 4, lane);
             int a = 0, a2 = 0;
 #pragma unroll
             for (int i = 0; i < KP; ++i) { a += rvi[i]; a2 += rvi[i] * rvi[i]; }
@@ -989,13 +1015,7 @@ __global__ void __launch_bounds__(st_warps(HALF) * 32, 2) k_stereo(
                 if (k % RB >= PW) twb2[k] = 0;
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) at2 = __dadd_rn(at2, __shfl_xor_sync(0xffffffffu, at2, o));
-            int dmax = MAXD - 1;
-            if (xr + dmax + HALF >= W) dmax = W - 1 - HALF - xr;
-            const int lc0 = xr - HALF, lcols = dmax + PW;
-            __syncwarp();
-            // left-image window, candidate c at column c: lane bounds c = 4 lane .. 4 lane + 3 (pad 4: word-aligned)
-            stage_u8<HALF>(winb, L, W, vi - HALF, PW, lc0, lcols, 4, lane);
-            __syncwarp();
+            __syncwarp();                                        // the left window and the template rows
             float z4[4], e4[4];
             zapprox4_u8<HALF>(winb + 4 + 4 * lane, (const unsigned*)twb2, a, (float)rsd, (float)at2, z4, e4);
             float lq = -INFINITY;
@@ -1003,6 +1023,22 @@ __global__ void __launch_bounds__(st_warps(HALF) * 32, 2) k_stereo(
             for (int k = 0; k < 4; ++k)
                 if (4 * lane + k <= dmax) lq = fmaxf(lq, z4[k] - e4[k]);
             const float llb = warp_max_f(lq);
+            // Only the exact maximum's distance from the peak matters, and the maximum is one of the candidates (or
+            // none exceeds -2).  Every candidate within LRT of the peak with a lower bound above -2: the check passes;
+            // none within LRT: it fails; otherwise the candidates are evaluated exactly.
+            bool cin = false, cout = false;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int c = 4 * lane + k;
+                if (c <= dmax && z4[k] + e4[k] >= llb) {
+                    if (fabs((double)(c - bestd)) > LRT) cout = true;
+                    else cin = true;
+                }
+            }
+            cin = __any_sync(0xffffffffu, cin);
+            cout = __any_sync(0xffffffffu, cout);
+            if (!cin) continue;
+            if (cout || !(llb > -2.0f)) {
             // the candidates (a column certainly at -2 can never be the maximum, which must exceed -2)
             int nc = 0;
 #pragma unroll
@@ -1044,6 +1080,7 @@ __global__ void __launch_bounds__(st_warps(HALF) * 32, 2) k_stereo(
             }
             warp_argmax(lrb, lrd);
             if (lrd < 0 || fabs((double)(lrd - bestd)) > LRT) continue;
+            }
         }
 
         // parabola seed of the LK (from the sub-pixel keypoint position)
@@ -1057,15 +1094,41 @@ __global__ void __launch_bounds__(st_warps(HALF) * 32, 2) k_stereo(
             }
         }
         if (lane == 0) {
-            StJob& J = jobs[njobs];
+            StJob J;
             J.u = u; J.v = v; J.ts = ts;
             J.seed = __dadd_rn(__dadd_rn((double)bestd, off), __dsub_rn(u, (double)ui));
             J.oi = (long long)oi;
-            J.ui = ui; J.vi = vi; J.xr = xr; J.js = js; J.f = f;
+            J.ui = ui; J.vi = vi; J.xr = xr; J.js = js; J.f = f; J.pad_ = 0;
+            gjobs[atomicAdd(gcount, 1)] = J;
         }
-        ++njobs;
     }
-    if (njobs == 0) return;
+}
+
+// The LK kernel: jpw jobs of the list per warp (up to 32).  The warp stages every job's right- and left-image
+// neighbourhood, then each lane runs one job's affine LK (LK_ITERS steps and the covariance pass) with its ten sums in
+// the CPU's sequential order and its own 3x3 OpenBLAS solve: the serial float64 chains of the jobs run side by side.
+// Then each lane takes its accepted job through the vertical scan.  Outputs are written by point index, so the list's
+// order (atomic appends) does not matter.
+template <int HALF, bool FLT>
+__global__ void __launch_bounds__(st_warps(HALF) * 32, 2) k_stereo_lk(
+    const u8* __restrict__ Lall, const u8* __restrict__ R8all, const float* __restrict__ Rsall, int H, int W,
+    const StJob* __restrict__ gjobs, const int* __restrict__ gcount, int jpw, double* __restrict__ od,
+    double* __restrict__ osig, u8* __restrict__ ook, double* __restrict__ ody)
+{
+    constexpr int PW = 2 * HALF + 1, NPIX = PW * PW;
+    const int NW = blockDim.x >> 5;
+    constexpr int LKR = PW + 2, LKW = PW + 2 * LK_MG + 2;
+    const int RS = lk_rs(HALF), LS = lk_ls(HALF), JB = lk_job_bytes(HALF);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    unsigned char* base = smem_raw + (size_t)wid * stereo_lk_bytes(HALF);
+    StJob* jobs = (StJob*)base;
+    unsigned char* U = base + st_jobs_bytes();
+    const long long j0 = ((long long)blockIdx.x * NW + wid) * jpw;
+    const int total = *gcount;
+    if (j0 >= total) return;
+    const int njobs = (int)(total - j0 < jpw ? total - j0 : jpw);
+    if (lane < njobs) jobs[lane] = gjobs[j0 + lane];
 
     // ----------------------------------------------------------------------------------------------- phase B: LKs
     __syncwarp();
@@ -1204,7 +1267,30 @@ __global__ void __launch_bounds__(st_warps(HALF) * 32, 2) k_stereo(
     // --------------------------------------------------------------------------------------- phase C: vertical scans
     // one lane per accepted job: the ZNCC of the matched right patch's column neighbourhood (scan offsets -HALF ..
     // HALF), its PW patches summed side by side, each in the reference's pixel order; then the first maximum and the
-    // parabola.  The template (the left patch minus its mean) and the right pixels come from global memory (L1).
+    // parabola.  u8 images: every accepted job's right-image block (2 PW - 1 rows x PW columns) and template are first
+    // staged in shared memory over the LK blocks; the shifted float32 image is read from global memory (L1).
+    const unsigned okm = __ballot_sync(0xffffffffu, okl);
+    constexpr int VR = (2 * PW - 1) * PW;
+    const int VJ = st_vjob_bytes(HALF);
+    if (!FLT) {
+        __syncwarp();
+        for (int t = lane; t < njobs * (VR + NPIX); t += 32) {
+            const int j = t / (VR + NPIX), q = t - j * (VR + NPIX);
+            if (!((okm >> j) & 1u)) continue;
+            const StJob& J = jobs[j];
+            if (!(J.vi - 2 * HALF - 1 >= 0 && J.vi + 2 * HALF + 1 < H)) continue;
+            const size_t fo = (size_t)J.f * H * W;
+            unsigned char* blk = U + (size_t)j * VJ;
+            if (q < VR) {
+                const int rr = q / PW, cc = q - rr * PW;
+                blk[q] = R8all[fo + (size_t)(J.vi - 2 * HALF + rr) * W + J.xr - HALF + cc];
+            } else {
+                const int p2 = q - VR;
+                blk[q] = Lall[fo + (size_t)(J.vi + p2 / PW - HALF) * W + J.ui + p2 % PW - HALF];
+            }
+        }
+        __syncwarp();
+    }
     if (okl) {
         const StJob J = jobs[lane];
         const int vi = J.vi, xr = J.xr, ui = J.ui;
@@ -1213,9 +1299,13 @@ __global__ void __launch_bounds__(st_warps(HALF) * 32, 2) k_stereo(
             RightImg<FLT> R;
             R.r8 = R8all ? R8all + (size_t)J.f * H * W : nullptr;
             R.rf = Rsall ? Rsall + (size_t)J.f * H * W : nullptr;
+            const unsigned char* blk = U + (size_t)lane * VJ;
+            auto tpl = [&](int q) -> int {
+                return FLT ? (int)L[(size_t)(vi + q / PW - HALF) * W + ui + q % PW - HALF] : (int)blk[VR + q];
+            };
             int st = 0;
 #pragma unroll 1
-            for (int k = 0; k < NPIX; ++k) st += (int)L[(size_t)(vi + k / PW - HALF) * W + ui + k % PW - HALF];
+            for (int q = 0; q < NPIX; ++q) st += tpl(q);
             const double tm = __ddiv_rn((double)st, (double)NPIX);
             double sx[PW], zs[PW], zs2[PW];
             int is[PW], is2[PW];
@@ -1226,11 +1316,10 @@ __global__ void __launch_bounds__(st_warps(HALF) * 32, 2) k_stereo(
             for (int dy = 0; dy < PW; ++dy) {
 #pragma unroll 1
                 for (int dx = 0; dx < PW; ++dx) {
-                    const double T = __dsub_rn((double)L[(size_t)(vi + dy - HALF) * W + ui + dx - HALF], tm);
-                    const size_t o = r0 + (size_t)dy * W + dx;
+                    const double T = __dsub_rn((double)tpl(dy * PW + dx), tm);
 #pragma unroll
                     for (int j = 0; j < PW; ++j) {
-                        const float rf = R.at(o + (size_t)j * W);
+                        const float rf = FLT ? R.at(r0 + (size_t)(dy + j) * W + dx) : (float)blk[(dy + j) * PW + dx];
                         const double r = (double)rf;
                         if (FLT) {
                             zs[j] = __dadd_rn(zs[j], r);
@@ -1276,50 +1365,74 @@ __global__ void __launch_bounds__(st_warps(HALF) * 32, 2) k_stereo(
     }
 }
 
+static int st_sm_count()
+{
+    static int sms[64];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) dev = 0;
+    if (!sms[dev]) {
+        int v = 0;
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+        sms[dev] = v > 0 ? v : 148;
+    }
+    return sms[dev];
+}
+
+// units per warp that fill `per_sm` blocks of nw warps on every SM once, at most ST_GROUP
+static int st_per_warp(long long units, int nw, int per_sm)
+{
+    const long long slots = (long long)st_sm_count() * per_sm * nw;
+    const long long g = (units + slots - 1) / slots;
+    return g < 1 ? 1 : (g > ST_GROUP ? ST_GROUP : (int)g);
+}
+
 template <int HALF, bool FLT>
 static cudaError_t launch_stereo_t(const uint8_t* L, const uint8_t* R8, const float* Rs, int H, int W,
                                    const double* kpd, const long long* dlo_a, const long long* dhi_a, int n,
                                    const float* kpf, const int* counts, int cap, int dlo, int dhi, int band,
                                    double* od, double* osig, uint8_t* ook, double* ozn, double* ody, long long npts,
-                                   int warps, int grp, cudaStream_t st)
+                                   int warps, int grp, void* jobs, cudaStream_t st)
 {
+    if (npts <= 0) return cudaSuccess;
+    int* gcount = (int*)jobs;
+    StJob* gjobs = (StJob*)((char*)jobs + 256);
+    cudaError_t e = cudaMemsetAsync(gcount, 0, sizeof(int), st);
+    if (e != cudaSuccess) return e;
+    // the search: the knobs, else st_warps warps and as many points per warp as fill ST_SEARCH_MINB blocks per SM
     int NW = warps >= 1 && warps <= st_warps(HALF) ? warps : st_warps(HALF);
-    // points per warp: the knob, else as many as fill two blocks per SM once (a small call spreads over every SM with
-    // one point per warp; a large batch takes ST_GROUP, which gives the LKs a full warp of lanes)
-    int G = grp;
-    if (!(G >= 1 && G <= ST_GROUP)) {
-        static int sms[64];
-        int dev = 0;
-        cudaGetDevice(&dev);
-        if (dev < 0 || dev >= 64) dev = 0;
-        if (!sms[dev]) {
-            int v = 0;
-            cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
-            sms[dev] = v > 0 ? v : 148;
-        }
-        const long long slots = (long long)sms[dev] * 2 * NW;
-        const long long g = (npts + slots - 1) / slots;
-        G = g < 1 ? 1 : (g > ST_GROUP ? ST_GROUP : (int)g);
-    }
-    size_t pw = (xcb_stereo_smem_per_warp(HALF, band) + 15) & ~(size_t)15;
+    const size_t pw = stereo_search_bytes(HALF, band, FLT);
     if ((size_t)NW * pw > ST_SMEM_MAX) NW = (int)(ST_SMEM_MAX / pw);    // the widest bands: fewer warps per block
-    size_t sm = pw * NW;
-    const long long per_block = (long long)NW * G;
-    long long nb = (npts + per_block - 1) / per_block;
-    if (nb <= 0) return cudaSuccess;
-    k_stereo<HALF, FLT><<<(unsigned)nb, NW * 32, sm, st>>>(L, R8, Rs, H, W, kpd, dlo_a, dhi_a, n, kpf, counts, cap,
-                                                            dlo, dhi, band, od, osig, ook, ozn, ody, G);
+    const int G = grp >= 1 && grp <= ST_GROUP ? grp : st_per_warp(npts, NW, ST_SEARCH_MINB);
+    const long long nb = (npts + (long long)NW * G - 1) / ((long long)NW * G);
+    k_stereo_search<HALF, FLT><<<(unsigned)nb, NW * 32, pw * NW, st>>>(L, R8, Rs, H, W, kpd, dlo_a, dhi_a, n, kpf,
+                                                                         counts, cap, dlo, dhi, band, od, osig, ook,
+                                                                         ozn, ody, G, gjobs, gcount);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    // the LKs and vertical scans of the jobs (at most npts), as many per warp as fill two blocks per SM once
+    const int NW2 = st_warps(HALF);
+    const int JP = st_per_warp(npts, NW2, 2);
+    const long long nb2 = (npts + (long long)NW2 * JP - 1) / ((long long)NW2 * JP);
+    k_stereo_lk<HALF, FLT><<<(unsigned)nb2, NW2 * 32, stereo_lk_bytes(HALF) * NW2, st>>>(L, R8, Rs, H, W, gjobs,
+                                                                                      gcount, JP, od, osig, ook, ody);
     return cudaGetLastError();
 }
 
 // the largest window (band BAND_MAX) of every instantiation, set once before any launch or graph capture
+// bytes of the job list a launch over npts points needs (a counter, then a 64-byte record per point that passes)
+size_t xcb_stereo_jobs_bytes(long long npts) { return 256 + (size_t)(npts > 0 ? npts : 0) * sizeof(StJob); }
+
 cudaError_t xcb_stereo_init_attrs()
 {
     cudaError_t e = cudaSuccess;
 #define XCB_SA(HH, FF)                                                                                            \
     if (e == cudaSuccess)                                                                                         \
-        e = cudaFuncSetAttribute(k_stereo<HH, FF>, cudaFuncAttributeMaxDynamicSharedMemorySize,                   \
-                                 (int)st_smem_attr(HH));
+        e = cudaFuncSetAttribute(k_stereo_search<HH, FF>, cudaFuncAttributeMaxDynamicSharedMemorySize,            \
+                                 (int)st_smem_attr(HH, FF));                                                     \
+    if (e == cudaSuccess)                                                                                         \
+        e = cudaFuncSetAttribute(k_stereo_lk<HH, FF>, cudaFuncAttributeMaxDynamicSharedMemorySize,                \
+                                 (int)(stereo_lk_bytes(HH) * st_warps(HH)));
     XCB_SA(3, false) XCB_SA(3, true) XCB_SA(4, false) XCB_SA(4, true) XCB_SA(5, false) XCB_SA(5, true)
 #undef XCB_SA
     return e;
@@ -1329,7 +1442,7 @@ cudaError_t xcb_launch_stereo(const uint8_t* L, const uint8_t* R8, const float* 
                               const double* kpd, const long long* dlo_a, const long long* dhi_a, int n,
                               const float* kpf, const int* counts, int cap, int dlo, int dhi, int band, int half,
                               double* od, double* osig, uint8_t* ook, double* ozn, double* ody, unsigned int* err,
-                              int warps, int grp, cudaStream_t st)
+                              void* jobs, int warps, int grp, cudaStream_t st)
 {
     if (band < 0 || band > BAND_MAX) return cudaErrorInvalidValue;
     long long npts = kpd ? (long long)n : (long long)F * cap;
@@ -1337,9 +1450,9 @@ cudaError_t xcb_launch_stereo(const uint8_t* L, const uint8_t* R8, const float* 
     bool flt = Rs != nullptr;
 #define XCB_ST(HH)                                                                                                  \
     return flt ? launch_stereo_t<HH, true>(L, nullptr, Rs, H, W, kpd, dlo_a, dhi_a, nn, kpf, counts, cap, dlo, dhi,  \
-                                           band, od, osig, ook, ozn, ody, npts, warps, grp, st)                     \
+                                           band, od, osig, ook, ozn, ody, npts, warps, grp, jobs, st)               \
                : launch_stereo_t<HH, false>(L, R8, nullptr, H, W, kpd, dlo_a, dhi_a, nn, kpf, counts, cap, dlo, dhi, \
-                                            band, od, osig, ook, ozn, ody, npts, warps, grp, st);
+                                            band, od, osig, ook, ozn, ody, npts, warps, grp, jobs, st);
     switch (half) {
         case 3: XCB_ST(3)
         case 4: XCB_ST(4)

@@ -207,69 +207,114 @@ __global__ void __launch_bounds__(256) k_sgm_agg(const unsigned char* __restrict
 }
 
 // ------------------------------------------------------------------------------------------------------ selection
+// CTA per row.  One pass over the row's sum vectors, a warp per pixel (four disparities per lane, 8-byte coalesced
+// loads): the left winner (first minimum), the second best more than one disparity away and the parabola by shuffles;
+// each S[x][d] is also a candidate of the right pixel x - d, whose winner (first minimum over d, as the reference scans
+// it) is a shared-memory atomicMin of (sum << 8 | d).  Then the right winners' parabolas and the left-right check.
+__device__ __forceinline__ unsigned sgm_pick(unsigned c0, unsigned c1, unsigned c2, unsigned c3, int k)
+{
+    return k == 0 ? c0 : (k == 1 ? c1 : (k == 2 ? c2 : c3));
+}
+
 __global__ void __launch_bounds__(256) k_sgm_select(const unsigned short* __restrict__ S, int H, int W, float uniq,
                                                     float dmin, float lr_thr, float* __restrict__ disp,
                                                     float* __restrict__ conf)
 {
-    extern __shared__ float dr[];                   // [W] the row's right winners
-    const int y = blockIdx.x;
+    extern __shared__ unsigned char sraw[];
+    unsigned* rkey = (unsigned*)sraw;              // [W] right winner keys, then the right disparities (float bits)
+    float* ld = (float*)(rkey + W);                // [W] left disparity (0 = invalid)
+    float* lc = ld + W;                            // [W] its confidence
+    const int y = blockIdx.x, lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const unsigned short* Sy = S + (size_t)y * W * SGM_D;
-    for (int x = threadIdx.x; x < W; x += blockDim.x) {
-        const int nd = min(SGM_D, W - x);
-        unsigned best = 0xFFFFFFFFu;
-        int bd = 0;
-        for (int d = 0; d < nd; ++d) {
-            const unsigned c = Sy[(size_t)(x + d) * SGM_D + d];
-            if (c < best) { best = c; bd = d; }
+    for (int x = threadIdx.x; x < W; x += blockDim.x) rkey[x] = 0xFFFFFFFFu;
+    __syncthreads();
+    for (int x = wid; x < W; x += nw) {
+        const uint2 v = *reinterpret_cast<const uint2*>(Sy + (size_t)x * SGM_D + 4 * lane);
+        const unsigned c0 = v.x & 0xffffu, c1 = v.x >> 16, c2 = v.y & 0xffffu, c3 = v.y >> 16;
+        const int nd = min(SGM_D, x + 1);
+        // right-winner candidates: right pixel x - d, d <= x
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int d = 4 * lane + k;
+            if (d <= x) atomicMin(&rkey[x - d], (sgm_pick(c0, c1, c2, c3, k) << 8) | (unsigned)d);
         }
+        // left winner: the first minimum over d < nd
+        unsigned best = 0xFFFFFFFFu;
+        int bd = 0x7fffffff;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int d = 4 * lane + k;
+            const unsigned c = sgm_pick(c0, c1, c2, c3, k);
+            if (d < nd && c < best) { best = c; bd = d; }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned b2 = __shfl_xor_sync(0xffffffffu, best, o);
+            const int d2 = __shfl_xor_sync(0xffffffffu, bd, o);
+            if (b2 < best || (b2 == best && d2 < bd)) { best = b2; bd = d2; }
+        }
+        // the best more than one disparity away
+        unsigned sec = 0xFFFFFFFFu;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int d = 4 * lane + k;
+            const unsigned c = sgm_pick(c0, c1, c2, c3, k);
+            if (d < nd && abs(d - bd) > 1 && c < sec) sec = c;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sec = min(sec, __shfl_xor_sync(0xffffffffu, sec, o));
+        // the neighbours of the winner (for the parabola)
+        const int dm = bd > 0 ? bd - 1 : 0, dp = bd + 1 < SGM_D ? bd + 1 : SGM_D - 1;
+        const unsigned cvl = sgm_pick(c0, c1, c2, c3, dm & 3), cnl = sgm_pick(c0, c1, c2, c3, dp & 3);
+        const int cv = (int)__shfl_sync(0xffffffffu, cvl, dm >> 2);
+        const int cn = (int)__shfl_sync(0xffffffffu, cnl, dp >> 2);
+        if (lane == 0) {
+            float o_d = 0.0f, o_c = 0.0f;
+            if (!(sec != 0xFFFFFFFFu && (float)sec <= __fmul_rn((float)best, __fadd_rn(1.0f, uniq)))) {
+                float sd = (float)bd;
+                if (bd > 0 && bd < nd - 1) {
+                    const int den = cv - 2 * (int)best + cn;
+                    if (den > 0) {
+                        const float off = __fdiv_rn((float)(cv - cn), (float)(2 * den));
+                        sd = __fadd_rn((float)bd, fmaxf(-1.0f, fminf(1.0f, off)));
+                    }
+                }
+                const float cval = (sec != 0xFFFFFFFFu && sec > 0) ? __fsub_rn(1.0f, __fdiv_rn((float)best, (float)sec))
+                                                                   : 0.5f;
+                o_d = sd >= dmin ? sd : 0.0f;
+                o_c = sd >= dmin ? fmaxf(0.0f, fminf(1.0f, cval)) : 0.0f;
+            }
+            ld[x] = o_d;
+            lc[x] = o_c;
+        }
+    }
+    __syncthreads();
+    // the right winners' parabolas (their neighbours read from the volume), in place of the keys
+    for (int x = threadIdx.x; x < W; x += blockDim.x) {
+        const unsigned key = rkey[x];
+        const int bd = (int)(key & 0xffu), best = (int)(key >> 8);
+        const int nd = min(SGM_D, W - x);
         float sd = (float)bd;
         if (bd > 0 && bd < nd - 1) {
             const int cv = (int)Sy[(size_t)(x + bd - 1) * SGM_D + bd - 1];
             const int cn = (int)Sy[(size_t)(x + bd + 1) * SGM_D + bd + 1];
-            const int den = cv - 2 * (int)best + cn;
+            const int den = cv - 2 * best + cn;
             if (den > 0) {
                 const float off = __fdiv_rn((float)(cv - cn), (float)(2 * den));
                 sd = __fadd_rn((float)bd, fmaxf(-1.0f, fminf(1.0f, off)));
             }
         }
-        dr[x] = sd;
+        rkey[x] = __float_as_uint(sd);
     }
     __syncthreads();
+    // the left-right check against the row's right winners
     for (int x = threadIdx.x; x < W; x += blockDim.x) {
+        float o_d = ld[x], o_c = lc[x];
+        if (o_d > 0.0f) {
+            const int xr = x - (int)__fadd_rn(o_d, 0.5f);
+            if (xr < 0 || xr >= W || fabsf(__fsub_rn(o_d, __uint_as_float(rkey[xr]))) > lr_thr) { o_d = 0.0f; o_c = 0.0f; }
+        }
         const size_t p = (size_t)y * W + x;
-        const unsigned short* sp = Sy + (size_t)x * SGM_D;
-        const int nd = min(SGM_D, x + 1);
-        unsigned best = 0xFFFFFFFFu, sec = 0xFFFFFFFFu;
-        int bd = 0;
-        for (int d = 0; d < nd; ++d) {
-            const unsigned c = sp[d];
-            if (c < best) { best = c; bd = d; }
-        }
-        for (int d = 0; d < nd; ++d) {
-            const unsigned c = sp[d];
-            if (abs(d - bd) > 1 && c < sec) sec = c;
-        }
-        float o_d = 0.0f, o_c = 0.0f;
-        if (!(sec != 0xFFFFFFFFu && (float)sec <= __fmul_rn((float)best, __fadd_rn(1.0f, uniq)))) {
-            float sd = (float)bd;
-            if (bd > 0 && bd < nd - 1) {
-                const int cv = sp[bd - 1], cn = sp[bd + 1];
-                const int den = cv - 2 * (int)best + cn;
-                if (den > 0) {
-                    const float off = __fdiv_rn((float)(cv - cn), (float)(2 * den));
-                    sd = __fadd_rn((float)bd, fmaxf(-1.0f, fminf(1.0f, off)));
-                }
-            }
-            const float cval = (sec != 0xFFFFFFFFu && sec > 0) ? __fsub_rn(1.0f, __fdiv_rn((float)best, (float)sec))
-                                                               : 0.5f;
-            o_d = sd >= dmin ? sd : 0.0f;
-            o_c = sd >= dmin ? fmaxf(0.0f, fminf(1.0f, cval)) : 0.0f;
-            // the left-right check against the row's right winners
-            if (o_d > 0.0f) {
-                const int xr = x - (int)__fadd_rn(o_d, 0.5f);
-                if (xr < 0 || xr >= W || fabsf(__fsub_rn(o_d, dr[xr])) > lr_thr) { o_d = 0.0f; o_c = 0.0f; }
-            }
-        }
         disp[p] = o_d;
         conf[p] = o_c;
     }
@@ -414,7 +459,7 @@ extern "C" int xcb_sgm_compute_dev(xcb_sgm* s, const uint8_t* left, const uint8_
     const long long threads = (long long)s->npaths * 32;
     k_sgm_agg<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(s->C, (unsigned*)s->S, H, W, dirs, s->npaths);
     if (ev) cudaEventRecord(ev[2], st);
-    k_sgm_select<<<H, 256, (size_t)W * 4, st>>>(s->S, H, W, s->uniq, s->dmin, s->lr, disp, conf);
+    k_sgm_select<<<H, 256, (size_t)W * 12, st>>>(s->S, H, W, s->uniq, s->dmin, s->lr, disp, conf);
     if (ev) cudaEventRecord(ev[3], st);
     e = cudaGetLastError();
     if (e != cudaSuccess) return sgm_fail(s, XCB_ERR_CUDA, std::string("sgm_compute: ") + cudaGetErrorString(e));
