@@ -48,7 +48,8 @@ DLO, DHI = 0, 96
 METRIC = "frontend frames/s"
 # ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_stereo launch over 8 frames (9.549 MB + 0.222 MB),
 # per frame; traffic grows with the frame count, so a launch of F frames moves F times this
-TRAFFIC_PER_FRAME = {"stereo": (8.183552e6 + 0.163584e6) / 8}      # ncu dram read + write, 8-frame capture
+# ncu dram read + write of the stereo stage (search + LK kernels), 100-frame captures
+TRAFFIC_PER_FRAME = {"stereo": (91.095040e6 + 9.889792e6 + 119.745280e6 + 18.723584e6) / 100}
 
 
 def parse():
@@ -396,8 +397,8 @@ def run_ours(args, ws, rank, local):
             "frac": achieved / peak, "peak_kind": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_kind if peak_kind == "measured"
             else "fallback 6650 GB/s",
             "traffic": (TRAFFIC_PER_FRAME[dom] * (F / nb)) if dom in TRAFFIC_PER_FRAME else None,
-            "traffic_note": "DRAM read+write per launch, ncu capture of 8 frames scaled by frames "
-                            "(profiles/k_stereo_kitti1241_8frames.md)" if dom in TRAFFIC_PER_FRAME else None,
+            "traffic_note": "DRAM read+write per launch, ncu capture of 100 frames scaled by frames "
+                            "(profiles/k_stereo_search_kitti1241_100frames.md, k_stereo_lk_kitti1241_100frames.md)" if dom in TRAFFIC_PER_FRAME else None,
             "algorithmic_bytes_per_launch": bytes_launch,
             "whole_path_frac": frame_bytes * value / ws / 1e9 / peak,
             "stage_ms_per_step": per_step}

@@ -933,41 +933,43 @@ __global__ void __launch_bounds__(st_warps(HALF) * 32, ST_SEARCH_MINB) k_stereo_
             for (int q = 0; q < 4; ++q)
                 if (val[q] && abs(dq[q] - ad) > 1) l2q = fmaxf(l2q, za[q] - ea[q]);
             const float lb2 = warp_max_f(l2q);
-            {
-                bool want[4];
+            // round A, then (only when the exact peak is not the approximate one) round B: the second-peak candidates
+            // and neighbours around the exact peak; one call site for both rounds
+            bool want[4];
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const int dd = abs(dq[q] - ad);
-                    want[q] = val[q] && (za[q] + ea[q] >= lb || dd == 1 || (dd > 1 && za[q] + ea[q] >= lb2));
-                }
-                exact_flagged(want);
+            for (int q = 0; q < 4; ++q) {
+                const int dd = abs(dq[q] - ad);
+                want[q] = val[q] && (za[q] + ea[q] >= lb || dd == 1 || (dd > 1 && za[q] + ea[q] >= lb2));
             }
-            double lbest = -2.0;
-            int lbd = -1;
+            bool dead = false;
+#pragma unroll 1
+            for (int round = 0; round < 2; ++round) {
+                exact_flagged(want);
+                if (round == 1) break;
+                double lbest = -2.0;
+                int lbd = -1;
 #pragma unroll
-            for (int q = 0; q < 4; ++q)
-                if (val[q] && exf[dq[q]] && sc[dq[q]] > lbest) { lbest = sc[dq[q]]; lbd = dq[q]; }
-            bs = lbest;
-            bestd = lbd;
-            warp_argmax(bs, bestd);
-            if (lane == 0) ozn[oi] = bs;
-            if (bestd < 0 || bs < ZMIN) continue;
-            if (bestd != ad) {
-                // round B (the exact peak is not the approximate one): the second-peak candidates and neighbours
+                for (int q = 0; q < 4; ++q)
+                    if (val[q] && exf[dq[q]] && sc[dq[q]] > lbest) { lbest = sc[dq[q]]; lbd = dq[q]; }
+                bs = lbest;
+                bestd = lbd;
+                warp_argmax(bs, bestd);
+                if (lane == 0) ozn[oi] = bs;
+                if (bestd < 0 || bs < ZMIN) { dead = true; break; }
+                if (bestd == ad) break;
                 double l2d = -INFINITY;
 #pragma unroll
                 for (int q = 0; q < 4; ++q)
                     if (val[q] && abs(dq[q] - bestd) > 1)
                         l2d = fmax(l2d, exf[dq[q]] ? sc[dq[q]] : (double)za[q] - (double)ea[q]);
                 l2d = warp_max_d(l2d);
-                bool want[4];
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     const int dd = abs(dq[q] - bestd);
                     want[q] = val[q] && !exf[dq[q]] && (dd == 1 || (dd > 1 && (double)za[q] + (double)ea[q] >= l2d));
                 }
-                exact_flagged(want);
             }
+            if (dead) continue;
             double sec = -2.0;
 #pragma unroll
             for (int q = 0; q < 4; ++q)
@@ -1132,24 +1134,42 @@ __global__ void __launch_bounds__(st_warps(HALF) * 32, 2) k_stereo_lk(
 
     // ----------------------------------------------------------------------------------------------- phase B: LKs
     __syncwarp();
-    // every job's blocks, staged by the whole warp job by job (the search window is no longer needed)
-#pragma unroll 1
-    for (int j = 0; j < njobs; ++j) {
-        const StJob& J = jobs[j];
-        unsigned char* blk = U + (size_t)j * JB;
-        if (!FLT) {
-            const u8* Rf = R8all + (size_t)J.f * H * W;
-            const int ys0 = J.vi + J.js - HALF - 1, xs0 = J.xr - HALF - LK_MG - 1;
-            for (int idx = lane; idx < LKR * RS; idx += 32) {
-                const int rr = idx / RS, cc = idx - rr * RS, col = xs0 + cc;
-                blk[idx] = (cc < LKW && col >= 0 && col < W) ? Rf[(size_t)(ys0 + rr) * W + col] : (u8)0;
+    // every job's blocks (right image, then left image), staged by the whole warp over all jobs at once with eight
+    // loads in flight per lane
+    {
+        const int RB = LKR * RS, PJ = RB + LKR * LS;           // bytes per job
+        constexpr int UB = 8;
+        const int total = njobs * PJ;
+        for (int t0 = lane; t0 < total; t0 += 32 * UB) {
+            u8 v[UB];
+#pragma unroll
+            for (int u = 0; u < UB; ++u) {
+                const int t = t0 + 32 * u;
+                v[u] = 0;
+                if (t < total) {
+                    const int j = t / PJ, q = t - j * PJ;
+                    const StJob& J = jobs[j];
+                    const size_t fo = (size_t)J.f * H * W;
+                    if (q < RB) {
+                        if (!FLT) {
+                            const int rr = q / RS, cc = q - rr * RS, col = J.xr - HALF - LK_MG - 1 + cc;
+                            if (cc < LKW && col >= 0 && col < W)
+                                v[u] = R8all[fo + (size_t)(J.vi + J.js - HALF - 1 + rr) * W + col];
+                        }
+                    } else {
+                        const int q2 = q - RB, rr = q2 / LS, cc = q2 - rr * LS;
+                        if (cc < PW + 2) v[u] = Lall[fo + (size_t)(J.vi - HALF - 1 + rr) * W + J.ui - HALF - 1 + cc];
+                    }
+                }
             }
-        }
-        const u8* Lf = Lall + (size_t)J.f * H * W;
-        const int ly0 = J.vi - HALF - 1, lx0 = J.ui - HALF - 1;
-        for (int idx = lane; idx < LKR * LS; idx += 32) {
-            const int rr = idx / LS, cc = idx - rr * LS;
-            blk[LKR * RS + idx] = cc < PW + 2 ? Lf[(size_t)(ly0 + rr) * W + lx0 + cc] : (u8)0;
+#pragma unroll
+            for (int u = 0; u < UB; ++u) {
+                const int t = t0 + 32 * u;
+                if (t < total) {
+                    const int j = t / PJ, q = t - j * PJ;
+                    U[(size_t)j * JB + q] = v[u];
+                }
+            }
         }
     }
     __syncwarp();
@@ -1274,19 +1294,39 @@ __global__ void __launch_bounds__(st_warps(HALF) * 32, 2) k_stereo_lk(
     const int VJ = st_vjob_bytes(HALF);
     if (!FLT) {
         __syncwarp();
-        for (int t = lane; t < njobs * (VR + NPIX); t += 32) {
-            const int j = t / (VR + NPIX), q = t - j * (VR + NPIX);
-            if (!((okm >> j) & 1u)) continue;
-            const StJob& J = jobs[j];
-            if (!(J.vi - 2 * HALF - 1 >= 0 && J.vi + 2 * HALF + 1 < H)) continue;
-            const size_t fo = (size_t)J.f * H * W;
-            unsigned char* blk = U + (size_t)j * VJ;
-            if (q < VR) {
-                const int rr = q / PW, cc = q - rr * PW;
-                blk[q] = R8all[fo + (size_t)(J.vi - 2 * HALF + rr) * W + J.xr - HALF + cc];
-            } else {
-                const int p2 = q - VR;
-                blk[q] = Lall[fo + (size_t)(J.vi + p2 / PW - HALF) * W + J.ui + p2 % PW - HALF];
+        constexpr int UB = 8;
+        const int total = njobs * (VR + NPIX);
+        for (int t0 = lane; t0 < total; t0 += 32 * UB) {
+            u8 v[UB];
+            bool w[UB];
+#pragma unroll
+            for (int u = 0; u < UB; ++u) {
+                const int t = t0 + 32 * u;
+                v[u] = 0;
+                w[u] = false;
+                if (t < total) {
+                    const int j = t / (VR + NPIX), q = t - j * (VR + NPIX);
+                    const StJob& J = jobs[j];
+                    if (((okm >> j) & 1u) && J.vi - 2 * HALF - 1 >= 0 && J.vi + 2 * HALF + 1 < H) {
+                        const size_t fo = (size_t)J.f * H * W;
+                        w[u] = true;
+                        if (q < VR) {
+                            const int rr = q / PW, cc = q - rr * PW;
+                            v[u] = R8all[fo + (size_t)(J.vi - 2 * HALF + rr) * W + J.xr - HALF + cc];
+                        } else {
+                            const int p2 = q - VR;
+                            v[u] = Lall[fo + (size_t)(J.vi + p2 / PW - HALF) * W + J.ui + p2 % PW - HALF];
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < UB; ++u) {
+                const int t = t0 + 32 * u;
+                if (w[u]) {
+                    const int j = t / (VR + NPIX), q = t - j * (VR + NPIX);
+                    U[(size_t)j * VJ + q] = v[u];
+                }
             }
         }
         __syncwarp();
