@@ -428,7 +428,8 @@ __device__ __forceinline__ void zncc4_u8(const unsigned char* p, const double* T
 //   numerator   |sx - N / NPIX| <= E = gamma_NPIX 255 sum|T| + 510 u S  (the sequential sum of the rounded products,
 //               and T = fl(t - fl(St / NPIX)) against t - St / NPIX), u = 2^-53
 //   denominator the float64 variance's cancellation error is below 7e-7 relative for any V >= 1 (V is an integer)
-// and the float32 evaluation adds at most 5e-7 relative.  ea = 4e-6 |z| + 1.05 E / den + 1e-9 bounds |z_fp - za|.
+// and the float32 evaluation (reciprocal square root, products) adds at most 4e-7 relative.  ea = 4e-6 |z| +
+// 1.05 E / den + 1e-9 bounds |z_fp - za|.
 // V = 0 (a flat patch) gives variance exactly 0 in float64 too, so z = -2 exactly (ea = 0); den within 1e-5 of the
 // reference's 1e-6 cut is undecided (ea = inf).  A disparity whose interval lies strictly below another's cannot be
 // the maximum (or the second peak, or the left-right maximum), so only the others are evaluated exactly, in the
@@ -477,18 +478,22 @@ __device__ __forceinline__ void zapprox4_u8(const unsigned char* p, const unsign
     }
     const float c1 = 4.0f * 1.01f * (float)NPIX * 1.1102230246251565e-16f * 255.0f;
     const float c2 = 4.0f * 510.0f * 1.1102230246251565e-16f;
+    // 1 / sqrt(V) by the hardware reciprocal square root (at most 2 ulp, 2.4e-7 relative) and multiplications by
+    // 1 / ts: the approximation stays within 1e-6 relative of the exact quotient, inside the 4e-6 margin
+    const float its = __fdividef(1.0f, ts32);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         const int N = NPIX * (int)SI[k] - st * (int)S[k];
         const int V = NPIX * (int)SQ[k] - (int)S[k] * (int)S[k];
         if (V <= 0) { za[k] = -2.0f; ea[k] = 0.0f; continue; }
-        const float den = __fmul_rn(ts32, __fsqrt_rn((float)V));
+        const float rs = rsqrtf((float)V);
+        const float den = ts32 * ((float)V * rs);                   // ts sqrt(V): the reference's denominator
         if (den < 1e-6f * (1.0f - 1e-5f)) { za[k] = -2.0f; ea[k] = 0.0f; continue; }
-        const float z = __fdiv_rn((float)N, __fmul_rn((float)NPIX, den));
+        const float irden = rs * its;                               // 1 / den
+        const float z = (float)N * irden * (1.0f / (float)NPIX);
         za[k] = z;
-        ea[k] = den <= 1e-6f * (1.0f + 1e-5f)
-                    ? INFINITY
-                    : 4e-6f * fabsf(z) + 1.05f * __fdiv_rn(c1 * at32 + c2 * (float)S[k], den) + 1e-9f;
+        ea[k] = den <= 1e-6f * (1.0f + 1e-5f) ? INFINITY
+                                              : 4e-6f * fabsf(z) + 1.05f * (c1 * at32 + c2 * (float)S[k]) * irden + 1e-9f;
     }
 }
 
