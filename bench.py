@@ -1157,8 +1157,8 @@ ADJ_NEWTON = 30
 
 def run_adjoint(args, dev, stream, ws_world, rank):
     """Differentiable BA: 64 windows of 10 keyframes and 2,000 landmarks; forward = 20 LM iterations, two rounds of 40
-    LM iterations with the landmarks the LM cannot move held constant, up to 30 trust-region Newton steps on the exact
-    Hessian; loss = sum of squared translation errors against the ground truth, backward = the implicit adjoint
+    LM iterations with the landmarks the LM cannot move held constant, up to 30 landmark-eliminated Newton steps on the
+    exact Hessian; loss = sum of squared translation errors against the ground truth, backward = the implicit adjoint
     (gradients to fx, fy, cx, cy, baseline, left-right extrinsic, per-row weights and pixels)."""
     import torch
     from xclean_b200.backend import synth_ba as S
@@ -1194,7 +1194,7 @@ def run_adjoint(args, dev, stream, ws_world, rank):
             "final_gradient_max_quartiles": [float(x) for x in np.percentile(st[:, 2], [25, 75])],
             "config": {"workload": "64 windows x (10 keyframes, 2000 landmarks, 2-6 obs, 5%% outliers); forward 20 LM "
                                    "iterations, 2 x 40 LM iterations with the landmarks the LM cannot move held "
-                                   "constant, up to %d trust-region Newton steps; implicit adjoint of "
+                                   "constant, up to %d landmark-eliminated Newton steps; implicit adjoint of "
                                    "sum |t - t_gt|^2" % ADJ_NEWTON}}
 
 

@@ -454,17 +454,25 @@ int xcb_ba_solve_windows_noalloc(const xcb_ba_windows* w, int Lt, int max_slots,
                                  double* stats, double* dx0, int dx0_stride, int grid, void* stream);
 
 /* Exact second-order steps on the window cost (no reference counterpart: the differentiable BA of the north-star API).
-   XCB_BA_NEWTON_POLISH: `steps` Newton steps with the exact Hessian (window.solve's LM converges only linearly when
-   Huber weights are active), the state updated in place.  XCB_BA_NEWTON_ADJOINT: at the converged state, solves
-   H x = dL/dstate (gpose: [slots][6] = dL/d(dphi, dp) per slot of the batch, landmarks 0) and writes
+   XCB_BA_NEWTON_POLISH: at most `steps` Newton steps with the exact Hessian (window.solve's LM converges only
+   linearly when Huber weights are active), the state updated in place.  Each step moves every landmark to the
+   minimum of its own cost with the poses fixed (Newton on its exact 3x3 block), then takes a Newton step on the poses
+   with the exact reduced Hessian Hpp - Hpl Hll^-1 Hlp (Cholesky; Levenberg-Marquardt damped while it is not positive
+   definite or the cost does not decrease), the landmarks following to first order; landmarks whose minimum lies at
+   infinity (inverse depth below 1e-7, or their own Newton step taking it to <= 1e-9) are flagged constant (not in
+   XCB_BA_NEWTON_POLISH_FIXED); it stops early at a gradient max-norm of 1e-10 or when a step at the cost's rounding
+   level no longer halves it.  XCB_BA_NEWTON_ADJOINT: at the converged
+   state, solves H x = dL/dstate (gpose: [slots][6] = dL/d(dphi, dp) per slot of the batch, landmarks 0) and writes
    dL/dtheta = -(d2C / dtheta dstate) x: gtheta [nw][11] = fx, fy, cx, cy, B, omega (3), t (3) of the left-to-right
    extrinsic at the rectified rig; gisig [M] = per-row weight 1/sigma; gz [M][2] = per-row pixels.  H is applied
    exactly (dual numbers) and the system solved by conjugate gradients preconditioned with the Gauss-Newton Schur
-   system until the relative residual is below `tol` (at most `maxit` iterations).  stats [nw][4] = iterations,
-   final relative residual, final gradient max-norm (polish), status (0 ok, 1 Gauss-Newton system not positive
-   definite, 2 non-positive curvature met: the state is not at a strict minimum, so no step is taken, -1 window too
-   large, -2 a landmark touches more than 16 keyframes, XCB_BA_STATUS_SCRATCH the scratch holds fewer than 19
-   doubles per landmark after its first 256 bytes). */
+   system until the relative residual is below `tol` (at most `maxit` iterations).  stats [nw][4]: polish = Newton
+   steps taken, final damping, final gradient max-norm, status; adjoint = iterations, final relative residual, -,
+   status.  Status: 0 ok, 1 Gauss-Newton system not positive definite, 2 (polish) no damping gave a decrease /
+   (adjoint) non-positive curvature met: the state is not at a strict minimum, -1 window too large, -2 a landmark
+   touches more than 16 keyframes, XCB_BA_STATUS_SCRATCH the scratch, less its last xcb_ba_newton_scratch_bytes(nw, 0)
+   - 512 bytes (the copies of the reduced systems), holds fewer than 19 doubles per landmark after its first 256
+   bytes. */
 #define XCB_BA_NEWTON_POLISH 0
 #define XCB_BA_NEWTON_ADJOINT 1
 #define XCB_BA_NEWTON_POLISH_FIXED 2      /* as XCB_BA_NEWTON_POLISH, flagging no new constant landmarks */

@@ -83,8 +83,8 @@ def test_adjoint_matches_the_autodiff_reference(run):
 
 def test_newton_polish_reaches_a_stationary_point_where_the_lm_solve_stalls():
     """This seed's window.solve stalls with an indefinite Hessian (a landmark whose outlier host pixel pins it, and
-    steps that the positive-depth rule rejects); the trust-region Newton polish still reaches a stationary point of
-    the cost in the remaining variables, with a lower cost."""
+    steps that the positive-depth rule rejects); the landmark-eliminated Newton polish still reaches a stationary
+    point of the cost in the remaining variables, with a lower cost."""
     import torch
     from oracle import ba_oracle as BO
     from xclean_b200.backend import synth_ba as S

@@ -96,14 +96,16 @@ def test_short_scratch_is_refused_on_the_device():
         assert bool((buf[256:] == 0xA5).all()), "the kernel wrote into the scratch it refused"
         for k, v in before.items():
             assert torch.equal(bs.t[k], v), k
-    # the Newton kernel: 19 doubles per landmark
+    # the Newton kernel: 19 doubles per landmark, then the reduced-system copies
+    ncopy = int(_lib.lib().xcb_ba_newton_scratch_bytes(bs.nw, 0)) - 512
     nst = torch.zeros((bs.nw, 4), dtype=torch.float64, device="cuda")
-    nbuf = torch.full((256 + 8 * 19 * Lt + 4096,), 0xA5, dtype=torch.uint8, device="cuda")
+    nbuf = torch.full((256 + 8 * 19 * Lt + ncopy + 4096,), 0xA5, dtype=torch.uint8, device="cuda")
     z = torch.zeros(1, dtype=torch.float64, device="cuda")
     rc = _lib.lib().xcb_ba_newton_windows_dev(ctypes.byref(bs.desc), bs.max_slots, _lib.XCB_BA_NEWTON_POLISH, 2, 10,
                                               1e-12, None, ctypes.c_void_p(z.data_ptr()), ctypes.c_void_p(z.data_ptr()),
                                               ctypes.c_void_p(z.data_ptr()), ctypes.c_void_p(nst.data_ptr()),
-                                              ctypes.c_void_p(nbuf.data_ptr()), 256 + 8 * 19 * (Lt - 1), 0, None)
+                                              ctypes.c_void_p(nbuf.data_ptr()), 256 + 8 * 19 * (Lt - 1) + ncopy, 0,
+                                              None)
     assert rc == _lib.XCB_OK
     torch.cuda.synchronize()
     assert (nst[:, 3].cpu().numpy() == _lib.XCB_BA_STATUS_SCRATCH).all()

@@ -14,9 +14,10 @@ converged poses to de-rectifying it), weights [M] (the per-row weight 1/sigma in
 Forward: `iters` LM iterations of window.solve (float64, batched, one launch); then the landmarks whose
 Gauss-Newton step would take the inverse depth to <= 1e-9 (window.solve keeps them where they are, while its Schur
 complement assumes they move, so its fixed point is not stationary) are flagged constant and two rounds of
-`free_iters` LM iterations run with them held; then at most `newton_steps` trust-region Newton steps on the exact
-Hessian (the LM converges only linearly where Huber weights are active, and the adjoint is exact only at a stationary
-point).  Backward: one solve H x = dL/dstate (H applied exactly through dual numbers, conjugate gradients
+`free_iters` LM iterations run with them held; then at most `newton_steps` landmark-eliminated Newton steps on the
+exact Hessian (the LM converges only linearly where Huber weights are active, and the adjoint is exact only at a
+stationary point): each moves every landmark to the minimum of its own cost with the poses fixed, then solves the exact
+reduced pose system; landmarks whose minimum lies at infinity (rho < 1e-7) are flagged constant on the way.  Backward: one solve H x = dL/dstate (H applied exactly through dual numbers, conjugate gradients
 preconditioned with the Gauss-Newton Cholesky factor, Jacobians recomputed from the state rather than stored), then dL/dtheta = -(d2C / dtheta dstate) x, scattered to the window parameters and to every observation row.
 The solver keeps the converged state between forward and backward: do not reuse it for another forward before
 backward.  ctx.newton_stats / ctx.adjoint_stats keep the per-window stats (column 2: the gradient max-norm at the
@@ -51,7 +52,7 @@ class BAAdjoint(torch.autograd.Function):
             for _ in range(2):
                 solver.newton(0)                                    # flag the landmarks the LM cannot move
                 solver.solve_free(int(free_iters), float(lam0))
-            st = solver.newton(int(newton_steps), tol=float(tol), flag=False)
+            st = solver.newton(int(newton_steps), tol=float(tol))
         ctx.solver = solver
         ctx.tol = float(tol)
         ctx.dtypes = (intrinsics.dtype, baseline.dtype, extrinsic.dtype, weights.dtype, pixels.dtype)

@@ -82,7 +82,9 @@ static int ba_fail(int code, const char* msg)
 extern "C" size_t xcb_ba_newton_scratch_bytes(int nw, int Lt)
 {
     (void)nw;
-    return ((size_t)(Lt > 0 ? Lt : 1) * 22 * sizeof(double) + 255) / 256 * 256 + 256;
+    // [counter 256 B][19 + 3 doubles per landmark][the polish's copies of the reduced systems]
+    return ((size_t)(Lt > 0 ? Lt : 1) * 22 * sizeof(double) + 255) / 256 * 256 + 256 +
+           xcb_ba_newton_copy_doubles(nw) * sizeof(double);
 }
 
 static int ba_grid(int grid, int nw)
@@ -131,10 +133,15 @@ extern "C" int xcb_ba_newton_windows_dev(const xcb_ba_windows* w, int max_slots,
     if (mode == XCB_BA_NEWTON_ADJOINT && (!gpose || !gtheta)) return ba_fail(XCB_ERR_ARG, "ba_newton: adjoint outputs");
     if (steps < 0 || maxit < 1) return ba_fail(XCB_ERR_ARG, "ba_newton: steps / maxit");
     cudaStream_t st = (cudaStream_t)stream;
-    // scratch: [counter (256 B)][19 doubles per landmark]; the kernel checks the batch's landmarks against its size
-    if (scratch_bytes < 256) return ba_fail(XCB_ERR_CAPACITY, "ba_newton: scratch smaller than 256 bytes");
+    // scratch: [counter (256 B)][19 doubles per landmark ...][the reduced-system copies at the end]; the kernel
+    // checks the batch's landmarks against the part before the copies
+    const size_t ncopy = xcb_ba_newton_copy_doubles(w->nw);
+    if (scratch_bytes < 256 + ncopy * sizeof(double))
+        return ba_fail(XCB_ERR_CAPACITY, "ba_newton: scratch smaller than xcb_ba_newton_scratch_bytes(nw, 0)");
     int* counter = (int*)scratch;
     double* lsc = (double*)((char*)scratch + 256);
+    const size_t lsc_doubles = (scratch_bytes - 256) / sizeof(double) - ncopy;
+    double* scopy = lsc + lsc_doubles;
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), st);
     if (e != cudaSuccess) return ba_fail(XCB_ERR_CUDA, cudaGetErrorString(e));
     if (grid <= 0) {
@@ -145,7 +152,7 @@ extern "C" int xcb_ba_newton_windows_dev(const xcb_ba_windows* w, int max_slots,
     }
     if (grid > w->nw) grid = w->nw;
     e = xcb_launch_ba_newton(*w, max_slots, mode, steps, maxit, tol, gpose, gtheta, gisig, gz, stats, lsc, counter,
-                             grid, st, (scratch_bytes - 256) / sizeof(double));
+                             grid, st, lsc_doubles, scopy);
     if (e != cudaSuccess) return ba_fail(XCB_ERR_CUDA, cudaGetErrorString(e));
     return XCB_OK;
 }

@@ -16,9 +16,12 @@ cudaError_t xcb_launch_ba_windows(const XcbBaWindows& d, int max_slots, int iter
                                   double* stats, double* dx0, int dx0_stride, double* lmp_trial, int* counter,
                                   int grid, cudaStream_t st, const double* frz = nullptr, size_t trial_doubles = 0);
 size_t xcb_ba_newton_smem_bytes(int maxP);
+// the Newton polish keeps a copy of each window's reduced system in global memory (scopy: this many doubles)
+size_t xcb_ba_newton_copy_doubles(int nw);
 cudaError_t xcb_launch_ba_newton(const XcbBaWindows& d, int max_slots, int mode, int steps, int maxit, double tol,
                                  const double* gpose, double* gtheta, double* gisig, double* gz, double* stats,
-                                 double* lsc, int* counter, int grid, cudaStream_t st, size_t lsc_doubles);
+                                 double* lsc, int* counter, int grid, cudaStream_t st, size_t lsc_doubles,
+                                 double* scopy);
 
 // the large-window path: the same LM iterations as xcb_launch_ba_windows, the landmark passes over chunks of every
 // window on all SMs (chunks: [nchunks][3] int32 on the device: window, first landmark, end), the per-window steps one

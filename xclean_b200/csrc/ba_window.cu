@@ -173,10 +173,11 @@ __device__ __forceinline__ bool lm_const(const double* frz, int gl)
 
 // ---------------------------------------------------------------------------------------------- observations
 // One observation row group: whitened residual and Jacobians into ob (window.obs_residual / obs_jacobians_ws,
-// window.py:126-263).  -> 0 when q2 <= 1e-9 (not evaluable).
+// window.py:126-263).  jac: 0 the residual only, 1 every Jacobian, 2 the landmark Jacobian only (the pose blocks are
+// left unwritten).  -> 0 when q2 <= 1e-9 (not evaluable).
 template <typename T>
 __device__ __forceinline__ int obs_lin(const BaWin& w, const SlotGeo<T>& G, const T lm[3], int h, int t, int cam,
-                                       const double* z, T isg, T* ob, bool want_jac)
+                                       const double* z, T isg, T* ob, int jac)
 {
     const T a = lm[0], b = lm[1], rho = lm[2];
     const T* Rh = G.Rwc + 9 * h;
@@ -197,7 +198,7 @@ __device__ __forceinline__ int obs_lin(const BaWin& w, const SlotGeo<T>& G, cons
         ob[OB_E] = (fx * (q0 - rho * B) / q2 + (T)w.cx - (T)z[0]) * isg;
         ob[OB_E + 1] = 0;
     }
-    if (!want_jac) return 1;
+    if (!jac) return 1;
     const T iq = (T)1 / q2;
     T Dp[2][3];
     if (cam == 0) {
@@ -222,6 +223,7 @@ __device__ __forceinline__ int obs_lin(const BaWin& w, const SlotGeo<T>& G, cons
         ob[OB_JL + 3 * r + 1] = Dp[r][0] * RcR[1] + Dp[r][1] * RcR[4] + Dp[r][2] * RcR[7];
         ob[OB_JL + 3 * r + 2] = Dp[r][0] * r0 + Dp[r][1] * r1 + Dp[r][2] * r2;
     }
+    if (jac == 2) return 1;
     if (t == h) {
 #pragma unroll
         for (int j = 0; j < 18; ++j) ob[OB_JT + j] = 0;
@@ -289,7 +291,7 @@ __device__ __forceinline__ bool lin_landmark(BaShared& sh, const XcbBaWindows& d
         const int t = d.ob_pose[k];
         double chi2 = XCB_INF;
         if (d.ob_valid[k] && h_ok && (unsigned)t < (unsigned)w.P) {
-            if (obs_lin<T>(w, G, lm, h, t, d.ob_cam[k], d.ob_z + 2 * k, (T)d.ob_isig[k], ob, true)) {
+            if (obs_lin<T>(w, G, lm, h, t, d.ob_cam[k], d.ob_z + 2 * k, (T)d.ob_isig[k], ob, 1)) {
                 const T e2 = ob[OB_E] * ob[OB_E] + ob[OB_E + 1] * ob[OB_E + 1];
                 T en = sqrt(e2), wt, cc;
                 huber_w<T>(en, (T)w.hk, &wt, &cc);
@@ -662,7 +664,7 @@ __device__ void pass_cost(BaShared& sh, const XcbBaWindows& d, const SlotGeo<dou
         for (int k = d.lm_ob[gl] + lane; k < d.lm_ob[gl + 1]; k += 32) {
             if (!d.ob_valid[k] || (unsigned)d.ob_pose[k] >= (unsigned)sh.w.P) continue;
             double ob[OB_N];
-            if (!obs_lin<double>(sh.w, G, lm, h, d.ob_pose[k], d.ob_cam[k], d.ob_z + 2 * k, d.ob_isig[k], ob, false)) {
+            if (!obs_lin<double>(sh.w, G, lm, h, d.ob_pose[k], d.ob_cam[k], d.ob_z + 2 * k, d.ob_isig[k], ob, 0)) {
                 c += 1e6;
                 continue;
             }
@@ -1297,7 +1299,7 @@ __device__ void pass_dual(BaShared& sh, NtShared& nt, const XcbBaWindows& d, con
             const int t = d.ob_pose[k];
             Dual ob[OB_N];
             if (d.ob_valid[k] && (unsigned)t < (unsigned)sh.w.P &&
-                obs_lin<Dual>(sh.w, G, lm, h, t, d.ob_cam[k], d.ob_z + 2 * k, Dual(d.ob_isig[k]), ob, true)) {
+                obs_lin<Dual>(sh.w, G, lm, h, t, d.ob_cam[k], d.ob_z + 2 * k, Dual(d.ob_isig[k]), ob, 1)) {
                 const Dual en = sqrt(ob[OB_E] * ob[OB_E] + ob[OB_E + 1] * ob[OB_E + 1]);
                 Dual wt, cc;
                 huber_w<Dual>(en, Dual(sh.w.hk), &wt, &cc);
@@ -1661,10 +1663,641 @@ __device__ double nt_gmax(BaShared& sh, NtShared& nt, const double* lsc)
     return r;
 }
 
+// =====================================================================================================================
+// Landmark-eliminated Newton (the polish).  Near the LM's fixed point the exact Hessian is indefinite in a few landmark
+// blocks (landmarks with an outlier row: the second-order term of k|e| outweighs the block's Gauss-Newton curvature),
+// and a Newton or trust-region iteration on the joint system stalls there.  Each step therefore
+//   (1) moves every variable landmark to the minimum of its own cost with the poses fixed (Newton on its exact 3x3
+//       block with Levenberg-Marquardt damping);
+//   (2) builds the exact reduced system S = Hpp - Hpl Hll^-1 Hlp over the landmarks whose exact block is positive
+//       definite and solves S dp = -g_p (the gradient of the cost with every landmark at its own minimum) by Cholesky,
+//       Levenberg-Marquardt damped (mu |S_ii|) while S is not positive definite or the cost does not decrease;
+//   (3) moves those landmarks to first order with the poses (dl = -Hll^-1 Hlp dp), runs (1) at the trial poses, and
+//       keeps the trial if the cost decreased.
+// Second derivatives come from dual numbers: Hll and Hlp from three landmark directions per landmark, Hpp from one pass
+// per pose direction over the row groups that have that slot as host or target.
+// =====================================================================================================================
+#define NT_INNER 8              // Newton iterations per landmark in (1)
+#define NT_RETRY 10             // damping increases per step
+#define NT_SC (BA_MAXN * (BA_MAXN + 1) / 2)     // doubles per window of the reduced-system copy
+#define NT_RHO_INF 1e-7         // a landmark whose inverse depth falls below this has its minimum at infinity
+// polish records in the landmark scratch (the conjugate-gradient slots are free during the polish)
+#define NR_HI 0                 // Hll^-1, symmetric: 00 01 02 11 12 22; entry 0 is 0 for a landmark held this step
+#define NR_BK 9                 // the landmark before the trial step
+
+// dynamic shared memory of the Newton kernel: [S, packed lower][WarpLm<double> x BA_WARPS | SlotGeo<Dual> of a
+// direction][SlotGeo<Dual> with zero tangents]
+static __host__ __device__ __forceinline__ size_t nt_x_bytes(int n)
+{
+    size_t x = ba_x_bytes(n);
+    if (sizeof(SlotGeo<Dual>) > x) x = sizeof(SlotGeo<Dual>);
+    return (x + 15) & ~(size_t)15;
+}
+
+// the Huber cost of landmark gl's row groups at landmark state lm (the geometry G), as pass_cost counts it (1e6 for a
+// row group whose point is not in front of its camera), plus its inverse-depth prior; identical on every lane
+__device__ double lm_cost(const BaShared& sh, const XcbBaWindows& d, const SlotGeo<double>& G, int gl, int h,
+                          const double lm[3])
+{
+    const int lane = threadIdx.x & 31;
+    double c = 0.0;
+    for (int k = d.lm_ob[gl] + lane; k < d.lm_ob[gl + 1]; k += 32) {
+        if (!d.ob_valid[k] || (unsigned)d.ob_pose[k] >= (unsigned)sh.w.P) continue;
+        double ob[OB_N];
+        if (!obs_lin<double>(sh.w, G, lm, h, d.ob_pose[k], d.ob_cam[k], d.ob_z + 2 * k, d.ob_isig[k], ob, 0)) {
+            c += 1e6;
+            continue;
+        }
+        double wt, cc;
+        huber_w<double>(sqrt(ob[0] * ob[0] + ob[1] * ob[1]), sh.w.hk, &wt, &cc);
+        c += cc;
+    }
+    c = warp_sum(c);
+    if (d.rho_isig[gl] > 0.0) {
+        double r0 = (lm[2] - d.rho_meas[gl]) * d.rho_isig[gl], wt, cc;
+        huber_w<double>(fabs(r0), sh.w.hk, &wt, &cc);
+        c += cc;
+    }
+    return c;
+}
+
+// the exact landmark block of landmark gl at lm, the poses fixed (G0: the geometry with zero tangents): g (3) the
+// gradient, H (9) the exact Hessian block (symmetrised), hv (9) its Gauss-Newton block (the variable test of
+// pass_dual), *nobs the evaluable row groups; prior included; identical on every lane
+__device__ void lm_exact(const BaShared& sh, const XcbBaWindows& d, const SlotGeo<Dual>& G0, int gl, int h,
+                         const double lm[3], double g[3], double H[9], double hv[9], int* nobs)
+{
+    const int lane = threadIdx.x & 31;
+    const int k0 = d.lm_ob[gl], nob = lm_rows(d, gl);
+    for (int i = 0; i < 3; ++i) g[i] = 0.0;
+    for (int i = 0; i < 9; ++i) { H[i] = 0.0; hv[i] = 0.0; }
+    int ok = 0;
+    if (lane < nob) {
+        const int k = k0 + lane, t = d.ob_pose[k];
+        if (d.ob_valid[k] && (unsigned)t < (unsigned)sh.w.P) {
+            for (int i = 0; i < 3; ++i) {
+                const Dual lmd[3] = {Dual(lm[0], i == 0 ? 1.0 : 0.0), Dual(lm[1], i == 1 ? 1.0 : 0.0),
+                                     Dual(lm[2], i == 2 ? 1.0 : 0.0)};
+                Dual ob[OB_N];
+                if (!obs_lin<Dual>(sh.w, G0, lmd, h, t, d.ob_cam[k], d.ob_z + 2 * k, Dual(d.ob_isig[k]), ob, 2)) break;
+                const Dual en = sqrt(ob[OB_E] * ob[OB_E] + ob[OB_E + 1] * ob[OB_E + 1]);
+                Dual wt, cc;
+                huber_w<Dual>(en, Dual(sh.w.hk), &wt, &cc);
+                for (int r = 0; r < 3; ++r) {
+                    const Dual gr = wt * (ob[OB_JL + r] * ob[OB_E] + ob[OB_JL + 3 + r] * ob[OB_E + 1]);
+                    H[r * 3 + i] = gr.e;
+                    if (i == 0) g[r] = gr.v;
+                }
+                if (i == 0) {
+                    ok = 1;
+                    for (int p = 0; p < 3; ++p)
+                        for (int q = 0; q < 3; ++q)
+                            hv[p * 3 + q] = wt.v * (ob[OB_JL + p].v * ob[OB_JL + q].v +
+                                                    ob[OB_JL + 3 + p].v * ob[OB_JL + 3 + q].v);
+                }
+            }
+        }
+    }
+    *nobs = __popc(__ballot_sync(0xffffffffu, ok != 0));
+    for (int i = 0; i < 3; ++i) g[i] = warp_sum(g[i]);
+    for (int i = 0; i < 9; ++i) { H[i] = warp_sum(H[i]); hv[i] = warp_sum(hv[i]); }
+    if (d.rho_isig[gl] > 0.0) {
+        // prior huber(|(rho - rho_meas) ris|): gradient wt ris r0, exact curvature ris^2 inside the kink, 0 outside
+        const double ris = d.rho_isig[gl], r0 = (lm[2] - d.rho_meas[gl]) * ris;
+        double wt, cc;
+        huber_w<double>(fabs(r0), sh.w.hk, &wt, &cc);
+        g[2] += wt * ris * r0;
+        if (fabs(r0) <= sh.w.hk) H[8] += ris * ris;
+        hv[8] += wt * ris * ris;
+    }
+    for (int p = 0; p < 3; ++p)
+        for (int q = p + 1; q < 3; ++q) {
+            const double m = 0.5 * (H[p * 3 + q] + H[q * 3 + p]);
+            H[p * 3 + q] = m;
+            H[q * 3 + p] = m;
+        }
+}
+
+// pass_dual's variable test on the Gauss-Newton block
+__device__ __forceinline__ bool lm_var(const double hv0[9], int nobs)
+{
+    double hv[9];
+    for (int i = 0; i < 9; ++i) hv[i] = hv0[i];
+    for (int i = 0; i < 3; ++i) hv[i * 4] += 1e-12;
+    const double det = hv[0] * (hv[4] * hv[8] - hv[5] * hv[7]) - hv[1] * (hv[3] * hv[8] - hv[5] * hv[6]) +
+                       hv[2] * (hv[3] * hv[7] - hv[4] * hv[6]);
+    const double tr = hv[0] + hv[4] + hv[8];
+    return nobs > 0 && det > 1e-18 * tr * tr * tr && isfinite(det);
+}
+
+// (H + tau I)^-1 of a symmetric 3x3 block for the first tau of tau0, 1e-9 tr, 1e-8 tr, ... (none below tau0, none
+// above 1e3 tr) that makes it positive definite by Cholesky (pivots above 1e-13 tr); the inverse as 00 01 02 11 12 22.
+// -> tau, or -1 when none does
+__device__ double spd_inv3(const double H[9], double tau0, double Hi[6])
+{
+    const double tr = fabs(H[0]) + fabs(H[4]) + fabs(H[8]);
+    if (!(tr > 0.0) || !isfinite(tr) || !(tau0 >= 0.0)) return -1.0;
+    double tau = tau0;
+    for (int a = 0; a < 16 && tau <= 1e3 * tr; ++a) {
+        const double eps = 1e-13 * tr;
+        const double d0 = H[0] + tau;
+        if (d0 > eps) {
+            const double l00 = sqrt(d0), l10 = H[3] / l00, l20 = H[6] / l00;
+            const double d1 = H[4] + tau - l10 * l10;
+            if (d1 > eps) {
+                const double l11 = sqrt(d1), l21 = (H[7] - l20 * l10) / l11;
+                const double d2 = H[8] + tau - l20 * l20 - l21 * l21;
+                if (d2 > eps) {
+                    const double l22 = sqrt(d2);
+                    // L^-1 (lower), then (L L^T)^-1 = L^-T L^-1
+                    const double m00 = 1.0 / l00, m11 = 1.0 / l11, m22 = 1.0 / l22;
+                    const double m10 = -l10 * m00 * m11;
+                    const double m21 = -l21 * m11 * m22;
+                    const double m20 = -(l20 * m00 + l21 * m10) * m22;
+                    Hi[0] = m00 * m00 + m10 * m10 + m20 * m20;
+                    Hi[1] = m10 * m11 + m20 * m21;
+                    Hi[2] = m20 * m22;
+                    Hi[3] = m11 * m11 + m21 * m21;
+                    Hi[4] = m21 * m22;
+                    Hi[5] = m22 * m22;
+                    return tau;
+                }
+            }
+        }
+        tau = tau > 0.0 ? 10.0 * tau : 1e-9 * tr;
+    }
+    return -1.0;
+}
+
+__device__ __forceinline__ void sym3_mv(const double Hi[6], const double v[3], double o[3])
+{
+    o[0] = Hi[0] * v[0] + Hi[1] * v[1] + Hi[2] * v[2];
+    o[1] = Hi[1] * v[0] + Hi[3] * v[1] + Hi[4] * v[2];
+    o[2] = Hi[2] * v[0] + Hi[4] * v[1] + Hi[5] * v[2];
+}
+
+// (1) every variable landmark that is not held constant to the minimum of its own cost, the poses fixed (the state in
+// sh.Rwb / sh.pwb: sh.g64 and G0 built from it).  Newton on the exact block with Levenberg-Marquardt damping: the
+// shift is the smallest of the spd_inv3 sequence that makes the block positive definite (0 where it is) plus mu tr,
+// mu / 10 after a decrease and x 10 after none; a step at the cost's rounding level is kept unless the cost rose.
+// The cost of every landmark at its final state -> sh.red (per warp: block_sum_red gives the window's).
+__device__ void pass_inner(BaShared& sh, const XcbBaWindows& d, const SlotGeo<Dual>& G0, const double* lsc)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    double ctot = 0.0;
+    for (int l = sh.lb + wid; l < sh.le; l += BA_WARPS) {
+        const int gl = sh.w.lm0 + l;
+        if (!d.lm_mask[gl]) continue;
+        const int h = d.lm_host[gl];
+        if ((unsigned)h >= (unsigned)sh.w.P) continue;
+        double lm[3] = {d.lmp[3 * gl], d.lmp[3 * gl + 1], d.lmp[3 * gl + 2]};
+        double c = lm_cost(sh, d, sh.g64, gl, h, lm);
+        const bool frozen = lsc[(size_t)gl * NT_LM_STRIDE + NT_FROZEN] != 0.0;
+        bool moved = false;
+        double mu = 0.0;
+        for (int it = 0; it < NT_INNER && !frozen; ++it) {
+            double g[3], H[9], hv[9], Hi[6], dl[3];
+            int nobs;
+            lm_exact(sh, d, G0, gl, h, lm, g, H, hv, &nobs);
+            if (!lm_var(hv, nobs)) break;
+            const double tr = fabs(H[0]) + fabs(H[4]) + fabs(H[8]);
+            const double tau0 = spd_inv3(H, 0.0, Hi);
+            if (tau0 < 0.0) break;
+            bool acc = false;
+            double dec = 0.0;
+            for (int att = 0; att < 12 && !acc; ++att) {
+                if (spd_inv3(H, tau0 + mu * tr, Hi) < 0.0) break;
+                sym3_mv(Hi, g, dl);
+                dec = g[0] * dl[0] + g[1] * dl[1] + g[2] * dl[2];      // -(g.step), the step being -dl
+                double tr3[3];
+                for (int i = 0; i < 3; ++i) tr3[i] = lm[i] - dl[i];
+                if (dec > 0.0 && tr3[2] > 1e-9 && isfinite(tr3[0]) && isfinite(tr3[1]) && isfinite(tr3[2])) {
+                    const double c1 = lm_cost(sh, d, sh.g64, gl, h, tr3);
+                    const double noise = 1e-12 * fabs(c);
+                    acc = c1 <= c - 1e-4 * dec || (0.5 * dec <= noise && c1 <= c + noise);
+                    if (acc) {
+                        for (int i = 0; i < 3; ++i) lm[i] = tr3[i];
+                        c = c1;
+                        moved = true;
+                    }
+                }
+                if (acc) mu = mu > 1e-9 ? 0.1 * mu : 0.0;
+                else mu = mu > 0.0 ? 10.0 * mu : 1e-6;
+            }
+            if (!acc || 0.5 * dec <= 1e-12 * fabs(c)) break;      // no decrease, or converged to rounding level
+        }
+        if (moved && lane < 3) d.lmp[3 * gl + lane] = lm[lane];
+        __syncwarp();
+        if (lane == 0) ctot += c;
+    }
+    ctot = warp_sum(ctot);
+    if (lane == 0) sh.red[wid] = ctot;
+}
+
+// Hpp column c = 6 s + j (G: the geometry moved along e_c): every row group with slot s as its host or its target
+// adds the dual part of its pose gradient, d(w J^T e)/dx_c, to the rows >= c of S (packed lower)
+__device__ void pass_hpp_col(BaShared& sh, const XcbBaWindows& d, const SlotGeo<Dual>& G, int s, int c, double* S)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int l = sh.lb + wid; l < sh.le; l += BA_WARPS) {
+        const int gl = sh.w.lm0 + l;
+        if (!d.lm_mask[gl]) continue;
+        const int h = d.lm_host[gl];
+        if ((unsigned)h >= (unsigned)sh.w.P) continue;
+        const int k0 = d.lm_ob[gl], nob = lm_rows(d, gl);
+        int t = -1;
+        bool ev = false;
+        if (lane < nob) {
+            const int k = k0 + lane;
+            t = d.ob_pose[k];
+            ev = d.ob_valid[k] && (unsigned)t < (unsigned)sh.w.P && t != h && (h == s || t == s);
+        }
+        if (!__any_sync(0xffffffffu, ev)) continue;
+        if (ev) {
+            const int k = k0 + lane;
+            const Dual lm[3] = {Dual(d.lmp[3 * gl]), Dual(d.lmp[3 * gl + 1]), Dual(d.lmp[3 * gl + 2])};
+            Dual ob[OB_N];
+            if (obs_lin<Dual>(sh.w, G, lm, h, t, d.ob_cam[k], d.ob_z + 2 * k, Dual(d.ob_isig[k]), ob, 1)) {
+                const Dual en = sqrt(ob[OB_E] * ob[OB_E] + ob[OB_E + 1] * ob[OB_E + 1]);
+                Dual wt, cc;
+                huber_w<Dual>(en, Dual(sh.w.hk), &wt, &cc);
+                for (int i = 0; i < 6; ++i) {
+                    const Dual gt = wt * (ob[OB_JT + i] * ob[OB_E] + ob[OB_JT + 6 + i] * ob[OB_E + 1]);
+                    const Dual gh = wt * (obj(ob, OB_JH, 0, i) * ob[OB_E] + obj(ob, OB_JH, 1, i) * ob[OB_E + 1]);
+                    const int rt = 6 * t + i, rh = 6 * h + i;
+                    if (rt >= c) atomicAdd(&S[tri(rt, c)], gt.e);
+                    if (rh >= c) atomicAdd(&S[tri(rh, c)], gh.e);
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// (2) the landmark terms of the exact reduced system at the current state (G0: zero tangents): per landmark whose exact
+// block is positive definite (a landmark whose block is not is not at a minimum of its own cost, and this step holds
+// it where it is: no Schur term, no step, its rows still in Hpp and the pose gradient), its Hlp blocks from the three
+// landmark directions, S -= Hpl Hll^-1 Hlp (S holds Hpp from the column passes); for every landmark nt.gp += its pose
+// gradient; records Hll^-1 in the scratch.  upd: a variable landmark whose minimum lies at infinity (rho below
+// NT_RHO_INF, or its own Newton step taking rho to <= 1e-9) is flagged constant here (builds run at accepted states).
+// -> the warp's max |g_l| over the variable landmarks (held this step or not) in sh.red.
+__device__ void pass_xbuild(BaShared& sh, NtShared& nt, const XcbBaWindows& d, const SlotGeo<Dual>& G0, double* S,
+                            WarpLm<double>* wls, double* lsc, bool upd)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    WarpLm<double>& wl = wls[wid];
+    double gmax = 0.0;
+    for (int l = sh.lb + wid; l < sh.le; l += BA_WARPS) {
+        const int gl = sh.w.lm0 + l;
+        if (!d.lm_mask[gl]) continue;
+        const int h = d.lm_host[gl];
+        if ((unsigned)h >= (unsigned)sh.w.P) continue;
+        double* sc = lsc + (size_t)gl * NT_LM_STRIDE;
+        const int k0 = d.lm_ob[gl], nob = lm_rows(d, gl);
+        const double lmv[3] = {d.lmp[3 * gl], d.lmp[3 * gl + 1], d.lmp[3 * gl + 2]};
+        int mt = -1, ok = 0;
+        double g[3] = {0.0, 0.0, 0.0}, hv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int i = 0; i < 3; ++i) {
+            // lane = row group: the dual parts of its gradient along landmark direction i -> wl.ob[lane][0..15)
+            // (landmark 3, host pose 6, target pose 6); the value parts on the first direction
+            double* st = wl.ob[lane];
+            for (int q = 0; q < 15; ++q) st[q] = 0.0;
+            if (lane < nob) {
+                const int k = k0 + lane, t = d.ob_pose[k];
+                if (d.ob_valid[k] && (unsigned)t < (unsigned)sh.w.P) {
+                    const Dual lmd[3] = {Dual(lmv[0], i == 0 ? 1.0 : 0.0), Dual(lmv[1], i == 1 ? 1.0 : 0.0),
+                                         Dual(lmv[2], i == 2 ? 1.0 : 0.0)};
+                    Dual ob[OB_N];
+                    if (obs_lin<Dual>(sh.w, G0, lmd, h, t, d.ob_cam[k], d.ob_z + 2 * k, Dual(d.ob_isig[k]), ob, 1)) {
+                        const Dual en = sqrt(ob[OB_E] * ob[OB_E] + ob[OB_E + 1] * ob[OB_E + 1]);
+                        Dual wt, cc;
+                        huber_w<Dual>(en, Dual(sh.w.hk), &wt, &cc);
+                        for (int r = 0; r < 3; ++r) {
+                            const Dual gr = wt * (ob[OB_JL + r] * ob[OB_E] + ob[OB_JL + 3 + r] * ob[OB_E + 1]);
+                            st[r] = gr.e;
+                            if (i == 0) g[r] = gr.v;
+                        }
+                        if (t != h)
+                            for (int q = 0; q < 6; ++q) {
+                                const Dual gh = wt * (obj(ob, OB_JH, 0, q) * ob[OB_E] + obj(ob, OB_JH, 1, q) * ob[OB_E + 1]);
+                                const Dual gt = wt * (ob[OB_JT + q] * ob[OB_E] + ob[OB_JT + 6 + q] * ob[OB_E + 1]);
+                                st[3 + q] = gh.e;
+                                st[9 + q] = gt.e;
+                                if (i == 0) {
+                                    atomicAdd(&nt.gp[6 * h + q], gh.v);
+                                    atomicAdd(&nt.gp[6 * t + q], gt.v);
+                                }
+                            }
+                        if (i == 0) {
+                            ok = 1;
+                            mt = t;
+                            for (int p = 0; p < 3; ++p)
+                                for (int q = 0; q < 3; ++q)
+                                    hv[p * 3 + q] = wt.v * (ob[OB_JL + p].v * ob[OB_JL + q].v +
+                                                            ob[OB_JL + 3 + p].v * ob[OB_JL + 3 + q].v);
+                        }
+                    }
+                }
+            }
+            if (i == 0) {
+                // touched slots: the observing keyframes other than the host, plus the host when any exists
+                const bool pose = mt >= 0 && mt != h;
+                unsigned mine = pose ? (1u << mt) : 0u;
+                for (int o = 16; o > 0; o >>= 1) mine |= __shfl_xor_sync(0xffffffffu, mine, o);
+                const unsigned tm = mine ? (mine | (1u << h)) : 0u;
+                int nt_ = 0;
+                for (unsigned m = tm; m; m &= m - 1) {
+                    const int s = __ffs(m) - 1;
+                    const unsigned om = __ballot_sync(0xffffffffu, pose && (s == h || mt == s));
+                    if (lane == 0 && nt_ < BA_MAXT) { wl.ts[nt_] = s; wl.om[nt_] = om; }
+                    ++nt_;
+                }
+                if (nt_ > BA_MAXT) {
+                    if (lane == 0) sh.overflow = 1;
+                    nt_ = BA_MAXT;
+                }
+                if (lane == 0) wl.hl[9] = (double)nt_;
+            }
+            __syncwarp();
+            const int ntc = (int)wl.hl[9];
+            // column i of Hll (lanes 0..2) and row i of every Hlp block
+            if (lane < 3) {
+                double acc = 0.0;
+                for (int m = 0; m < nob; ++m) acc += wl.ob[m][lane];
+                wl.hl[lane * 3 + i] = acc;
+            }
+            for (int q = lane; q < ntc * 6; q += 32) {
+                const int a = q / 6, j = q % 6;
+                const int off = wl.ts[a] == h ? 3 : 9;
+                double acc = 0.0;
+                for (unsigned m = wl.om[a]; m; m &= m - 1) acc += wl.ob[__ffs(m) - 1][off + j];
+                wl.Hlp[a][i * 6 + j] = acc;
+            }
+            __syncwarp();
+        }
+        const int ntc = (int)wl.hl[9];
+        const int nobs = __popc(__ballot_sync(0xffffffffu, ok != 0));
+        double H[9];
+        for (int q = 0; q < 9; ++q) H[q] = wl.hl[q];
+        for (int r = 0; r < 3; ++r) g[r] = warp_sum(g[r]);
+        for (int q = 0; q < 9; ++q) hv[q] = warp_sum(hv[q]);
+        if (d.rho_isig[gl] > 0.0) {
+            const double ris = d.rho_isig[gl], r0 = (lmv[2] - d.rho_meas[gl]) * ris;
+            double wt, cc;
+            huber_w<double>(fabs(r0), sh.w.hk, &wt, &cc);
+            g[2] += wt * ris * r0;
+            if (fabs(r0) <= sh.w.hk) H[8] += ris * ris;
+            hv[8] += wt * ris * ris;
+        }
+        for (int p = 0; p < 3; ++p)
+            for (int q = p + 1; q < 3; ++q) {
+                const double m = 0.5 * (H[p * 3 + q] + H[q * 3 + p]);
+                H[p * 3 + q] = m;
+                H[q * 3 + p] = m;
+            }
+        double Hi[6];
+        const bool fz = sc[NT_FROZEN] != 0.0, lv = lm_var(hv, nobs);
+        const bool pd = spd_inv3(H, 0.0, Hi) == 0.0;
+        double u[3] = {0.0, 0.0, 0.0};
+        if (pd) sym3_mv(Hi, g, u);                                    // Hll^-1 g_l: the landmark's own Newton step is -u
+        const bool inf = upd && !fz && lv && (lmv[2] < NT_RHO_INF || (pd && !(lmv[2] - u[2] > 1e-9)));
+        const bool var = !fz && !inf && lv && pd;
+        __syncwarp();
+        if (inf && lane == 0) sc[NT_FROZEN] = 1.0;
+        if (!fz && !inf && lv) gmax = fmax(gmax, fmax(fabs(g[0]), fmax(fabs(g[1]), fabs(g[2]))));
+        if (var) {
+            for (int q = lane; q < ntc * 18; q += 32) {              // Tb = Hll^-1 Hlp
+                const int a = q / 18, e = q % 18, i = e / 6, j = e % 6;
+                const double* Hl = wl.Hlp[a];
+                const double r0 = i == 0 ? Hi[0] : (i == 1 ? Hi[1] : Hi[2]);
+                const double r1 = i == 0 ? Hi[1] : (i == 1 ? Hi[3] : Hi[4]);
+                const double r2 = i == 0 ? Hi[2] : (i == 1 ? Hi[4] : Hi[5]);
+                wl.Tb[a][e] = r0 * Hl[j] + r1 * Hl[6 + j] + r2 * Hl[12 + j];
+            }
+            __syncwarp();
+            const int npair = ntc * (ntc + 1) / 2;
+            for (int q = lane; q < npair * 36; q += 32) {
+                const int pr = q / 36, e = q % 36, i = e / 6, j = e % 6;
+                int a = (int)((sqrtf(8.0f * pr + 1.0f) - 1.0f) * 0.5f);
+                while (a * (a + 1) / 2 > pr) --a;
+                while ((a + 1) * (a + 2) / 2 <= pr) ++a;
+                const int b = pr - a * (a + 1) / 2;
+                if (a == b && j > i) continue;
+                const double acc = wl.Hlp[a][i] * wl.Tb[b][j] + wl.Hlp[a][6 + i] * wl.Tb[b][6 + j] +
+                                   wl.Hlp[a][12 + i] * wl.Tb[b][12 + j];
+                atomicAdd(&S[tri(6 * wl.ts[a] + i, 6 * wl.ts[b] + j)], -acc);
+            }
+            if (lane < 6) sc[NR_HI + lane] = Hi[lane];
+        } else if (lane < 9) {
+            sc[lane] = 0.0;
+        }
+        __syncwarp();
+    }
+    for (int o = 16; o > 0; o >>= 1) gmax = fmax(gmax, __shfl_xor_sync(0xffffffffu, gmax, o));
+    if (lane == 0) sh.red[wid] = gmax;
+}
+
+// (3) the landmarks' first-order step with the poses, dl = -Hll^-1 Hlp dp (G: the geometry at the current
+// state moved along dp; Hlp dp is the dual part of the landmark gradient), for the landmarks the build kept; every
+// landmark's state is saved to the scratch first (restored when the trial is rejected)
+__device__ void pass_lstep(BaShared& sh, const XcbBaWindows& d, const SlotGeo<Dual>& G, double* lsc)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int l = sh.lb + wid; l < sh.le; l += BA_WARPS) {
+        const int gl = sh.w.lm0 + l;
+        if (!d.lm_mask[gl]) continue;
+        const int h = d.lm_host[gl];
+        if ((unsigned)h >= (unsigned)sh.w.P) continue;
+        double* sc = lsc + (size_t)gl * NT_LM_STRIDE;
+        const double lmv[3] = {d.lmp[3 * gl], d.lmp[3 * gl + 1], d.lmp[3 * gl + 2]};
+        if (lane < 3) sc[NR_BK + lane] = lmv[lane];
+        if (!(sc[NR_HI] > 0.0)) { __syncwarp(); continue; }
+        const int k0 = d.lm_ob[gl], nob = lm_rows(d, gl);
+        double u[3] = {0.0, 0.0, 0.0};
+        if (lane < nob) {
+            const int k = k0 + lane, t = d.ob_pose[k];
+            if (d.ob_valid[k] && (unsigned)t < (unsigned)sh.w.P && t != h) {
+                const Dual lm[3] = {Dual(lmv[0]), Dual(lmv[1]), Dual(lmv[2])};
+                Dual ob[OB_N];
+                if (obs_lin<Dual>(sh.w, G, lm, h, t, d.ob_cam[k], d.ob_z + 2 * k, Dual(d.ob_isig[k]), ob, 2)) {
+                    const Dual en = sqrt(ob[OB_E] * ob[OB_E] + ob[OB_E + 1] * ob[OB_E + 1]);
+                    Dual wt, cc;
+                    huber_w<Dual>(en, Dual(sh.w.hk), &wt, &cc);
+                    for (int r = 0; r < 3; ++r)
+                        u[r] = (wt * (ob[OB_JL + r] * ob[OB_E] + ob[OB_JL + 3 + r] * ob[OB_E + 1])).e;
+                }
+            }
+        }
+        for (int r = 0; r < 3; ++r) u[r] = warp_sum(u[r]);
+        double Hi[6], dl[3];
+        for (int q = 0; q < 6; ++q) Hi[q] = sc[NR_HI + q];
+        sym3_mv(Hi, u, dl);
+        const double nr = lmv[2] - dl[2];
+        if (nr > 1e-9 && isfinite(nr) && isfinite(dl[0]) && isfinite(dl[1]) && lane < 3)
+            d.lmp[3 * gl + lane] = lmv[lane] - dl[lane];
+        __syncwarp();
+    }
+}
+
+// restore every landmark the last pass_lstep saved
+__device__ void pass_lrestore(BaShared& sh, const XcbBaWindows& d, const double* lsc)
+{
+    for (int l = threadIdx.x; l < sh.w.L; l += blockDim.x) {
+        const int gl = sh.w.lm0 + l;
+        if (!d.lm_mask[gl] || (unsigned)d.lm_host[gl] >= (unsigned)sh.w.P) continue;
+        const double* sc = lsc + (size_t)gl * NT_LM_STRIDE;
+        for (int i = 0; i < 3; ++i) d.lmp[3 * gl + i] = sc[NR_BK + i];
+    }
+    __syncthreads();
+}
+
+__device__ double block_max_red(BaShared& sh)
+{
+    __syncthreads();
+    double s = 0.0;
+    for (int i = 0; i < BA_WARPS; ++i) s = fmax(s, sh.red[i]);
+    __syncthreads();
+    return s;
+}
+
+// the geometry of the state in sh.Rwb / sh.pwb: sh.g64 and the zero-tangent dual copy G0
+__device__ void nt_geo(BaShared& sh, SlotGeo<Dual>& G0)
+{
+    slot_geo(sh, sh.Rwb, sh.pwb);
+    for (int q = threadIdx.x; q < sh.w.n; q += blockDim.x) sh.dx[q] = 0.0;
+    __syncthreads();
+    slot_geo_dual(sh, sh.dx, G0);
+}
+
+// the landmark-eliminated Newton polish of one window (the state in sh.Rwb / sh.pwb and d.lmp); `steps` bounds the
+// Newton steps; it stops early at a gradient max-norm of 1e-10, or when a step at the cost's rounding level did not
+// halve it.  upd: landmarks whose minimum lies at infinity are flagged constant (pass_xbuild).  -> status (0, or 2 when
+// no damping gave a decrease); *steps_out, *mu_out the steps taken and the final damping
+__device__ int nt_polish(BaShared& sh, NtShared& nt, const XcbBaWindows& d, unsigned char* dsm, double* lsc,
+                         double* Sc, int steps, bool upd, int* steps_out, double* mu_out)
+{
+    const int n = sh.w.n, P = sh.w.P, tid = threadIdx.x;
+    double* S = (double*)dsm;
+    WarpLm<double>* wl64 = (WarpLm<double>*)(dsm + ba_off_x(n));
+    SlotGeo<Dual>* Gd = (SlotGeo<Dual>*)(dsm + ba_off_x(n));           // aliases wl64: never live together
+    SlotGeo<Dual>* G0 = (SlotGeo<Dual>*)(dsm + ba_off_x(n) + nt_x_bytes(n));
+    const int ntri = n * (n + 1) / 2;
+    nt_geo(sh, *G0);
+    pass_inner(sh, d, *G0, lsc);
+    double c0 = block_sum_red(sh);
+    double mu = 0.0, gm_prev = 0.0;
+    int st = 0, status = 0;
+    bool tiny = false;
+    while (st < steps) {
+        // the exact reduced system at the current state
+        for (int q = tid; q < ntri; q += blockDim.x) S[q] = 0.0;
+        for (int q = tid; q < n; q += blockDim.x) nt.gp[q] = 0.0;
+        __syncthreads();
+        for (int c = 0; c < n; ++c) {
+            if (held(sh, c)) continue;
+            for (int q = tid; q < n; q += blockDim.x) sh.dx[q] = q == c ? 1.0 : 0.0;
+            __syncthreads();
+            slot_geo_dual(sh, sh.dx, *Gd);
+            pass_hpp_col(sh, d, *Gd, c / 6, c, S);
+            __syncthreads();
+        }
+        pass_xbuild(sh, nt, d, *G0, S, wl64, lsc, upd);
+        const double gml = block_max_red(sh);
+        const int hs = sh.w.hold;
+        if (hs >= 0 && hs < P) {
+            for (int q = tid; q < 6 * n; q += blockDim.x) {
+                const int i = 6 * hs + q / n, j = q % n;
+                S[i >= j ? tri(i, j) : tri(j, i)] = 0.0;
+            }
+            __syncthreads();
+            for (int q = tid; q < 6; q += blockDim.x) S[tri(6 * hs + q, 6 * hs + q)] = 1.0;
+        }
+        // the pose gradient (sh.g) and the largest |g| over the poses and the variable landmarks
+        double gm = 0.0;
+        for (int q = tid; q < n; q += blockDim.x) {
+            const bool hq = held(sh, q);
+            sh.g[q] = hq ? 0.0 : nt.gp[q];
+            if (!hq) gm = fmax(gm, fabs(nt.gp[q]));
+        }
+        for (int o = 16; o > 0; o >>= 1) gm = fmax(gm, __shfl_xor_sync(0xffffffffu, gm, o));
+        __syncthreads();
+        if ((tid & 31) == 0) sh.red[tid >> 5] = gm;
+        gm = fmax(block_max_red(sh), gml);
+        if (gm <= 1e-10 || (tiny && gm > 0.5 * gm_prev)) break;
+        gm_prev = gm;
+        for (int q = tid; q < ntri; q += blockDim.x) Sc[q] = S[q];
+        __syncthreads();
+        bool acc = false;
+        for (int r = 0; r < NT_RETRY && !acc; ++r) {
+            if (r > 0 || mu > 0.0) {
+                for (int q = tid; q < ntri; q += blockDim.x) S[q] = Sc[q];
+                __syncthreads();
+                for (int q = tid; q < n; q += blockDim.x)
+                    if (!held(sh, q)) S[tri(q, q)] += mu * fabs(Sc[tri(q, q)]) + 1e-12;
+                __syncthreads();
+            }
+            if (chol_factor(S, n)) {
+                mu = mu > 0.0 ? 10.0 * mu : 1e-6;
+                continue;
+            }
+            for (int q = tid; q < n; q += blockDim.x) sh.dmp[q] = -sh.g[q];
+            __syncthreads();
+            chol_solve(S, n, sh.dmp);
+            // the model's decrease -g.dp / 2 (exact for the undamped step)
+            double pr = 0.0;
+            for (int q = tid; q < n; q += blockDim.x) pr -= sh.g[q] * sh.dmp[q];
+            pr = warp_sum(pr);
+            __syncthreads();
+            if ((tid & 31) == 0) sh.red[tid >> 5] = pr;
+            const double pred = 0.5 * block_sum_red(sh);
+            // landmarks to first order (geometry at the current state along dp), then the trial poses
+            slot_geo_dual(sh, sh.dmp, *Gd);
+            pass_lstep(sh, d, *Gd, lsc);
+            __syncthreads();
+            for (int s = tid; s < P; s += blockDim.x) {
+                double Re[9], R[9];
+                for (int i = 0; i < 9; ++i) { R[i] = sh.Rwb[9 * s + i]; sh.R2[9 * s + i] = R[i]; }
+                for (int i = 0; i < 3; ++i) sh.p2[3 * s + i] = sh.pwb[3 * s + i];
+                if (sh.w.hold == s) continue;
+                so3_exp(sh.dmp + 6 * s, Re);
+                for (int i = 0; i < 3; ++i)
+                    for (int j = 0; j < 3; ++j)
+                        sh.Rwb[9 * s + 3 * i + j] = R[3 * i] * Re[j] + R[3 * i + 1] * Re[3 + j] + R[3 * i + 2] * Re[6 + j];
+                for (int i = 0; i < 3; ++i) sh.pwb[3 * s + i] += sh.dmp[6 * s + 3 + i];
+            }
+            __syncthreads();
+            nt_geo(sh, *G0);
+            pass_inner(sh, d, *G0, lsc);
+            const double c1 = block_sum_red(sh);
+            // the cost is a float64 sum of ~1e4 terms: below ~1e-10 of it a decrease is rounding noise, so a step whose
+            // predicted decrease is that small is kept unless the cost visibly rose
+            const double noise = 1e-10 * fabs(c0);
+            tiny = pred <= noise;
+            acc = (c1 <= c0 - 1e-4 * pred && pred > 0.0) || (tiny && c1 <= c0 + noise);
+            if (acc) {
+                c0 = c1;
+                mu = mu > 1e-9 ? 0.1 * mu : 0.0;
+            } else {
+                for (int q = tid; q < P * 9; q += blockDim.x) sh.Rwb[q] = sh.R2[q];
+                for (int q = tid; q < P * 3; q += blockDim.x) sh.pwb[q] = sh.p2[q];
+                __syncthreads();
+                pass_lrestore(sh, d, lsc);
+                nt_geo(sh, *G0);
+                mu = mu > 0.0 ? 10.0 * mu : 1e-6;
+            }
+        }
+        ++st;
+        if (!acc) { status = 2; break; }
+    }
+    *steps_out = st;
+    *mu_out = mu;
+    return status;
+}
+
 __global__ void __launch_bounds__(BA_THREADS, 1) k_ba_newton(XcbBaWindows d, int mode, int steps, int maxit,
                                                              double tol, const double* gpose, double* gtheta,
                                                              double* gisig, double* gz, double* stats, double* lsc,
-                                                             int* counter, size_t lsc_doubles)
+                                                             int* counter, size_t lsc_doubles, double* scopy)
 {
     extern __shared__ __align__(16) unsigned char dsm[];
     __shared__ BaShared sh;
@@ -1721,101 +2354,14 @@ __global__ void __launch_bounds__(BA_THREADS, 1) k_ba_newton(XcbBaWindows d, int
         double rel = 0.0, gmax = 0.0;
         const bool upd = mode == XCB_BA_NEWTON_POLISH;      // may flag new constant landmarks
         if (mode != XCB_BA_NEWTON_ADJOINT) {
-            // Trust-region Newton on the exact Hessian: Steihaug's truncated CG in the Gauss-Newton metric, the step
-            // kept when the cost decreases by more than 1e-4 of the model's prediction (or the prediction is at
-            // rounding level: a converged state); the radius shrinks x4 on a poor step and doubles on a good step that
-            // reached it.  The first radius is unbounded, so a state in the Newton basin takes pure Newton steps.
-            // `steps` bounds the linear solves.
-            double delta = 1e300;
-            slot_geo(sh, sh.Rwb, sh.pwb);
-            pass_cost(sh, d, sh.g64, d.lmp);
-            double c0 = block_sum_red(sh);
-            bool last_ok = true;
-            int st = 0;
-            SlotGeo<Dual>* Gd = (SlotGeo<Dual>*)(dsm + ba_off_x(n));
-            double g0 = -1.0;
-            while (st < steps) {
-                if (nt_gn_factor(sh, d, S64, wl64, lsc)) { status = 1; break; }
-                nt_grad(sh, nt, d, dsm, lsc, upd);
-                // inexact Newton: the CG solves to a relative residual eta = min(0.1, sqrt(|g| / |g_0|)) (at least
-                // `tol`), so early steps take few iterations and the last ones converge superlinearly; a gradient at
-                // rounding level ends the polish
-                const double gm = nt_gmax(sh, nt, lsc);
-                if (g0 < 0.0) g0 = gm;
-                if (gm <= 1e-10) break;
-                const double eta = fmax(tol, fmin(0.1, sqrt(gm / fmax(g0, 1e-300))));
-                bool moved = false;
-                while (st < steps && !moved) {
-                    ++st;
-                    int bnd = 0;
-                    double xMx = 0.0;
-                    rel = nt_solve_exact(sh, nt, d, S64, dsm, lsc, maxit, eta, &iters, &neg, 0.0, delta, &bnd, &xMx);
-                    // the model's decrease b.x - x.Hx / 2 (b = -gradient), H x from one more dual pass
-                    for (int q = tid; q < n; q += blockDim.x) { sh.dx[q] = sh.dmp[q]; nt.gp[q] = 0.0; nt.hp[q] = 0.0; }
-                    for (int l = tid; l < sh.w.L; l += blockDim.x) {
-                        double* sc = lsc + (size_t)(sh.w.lm0 + l) * NT_LM_STRIDE;
-                        for (int i = 0; i < 3; ++i) sc[NT_P + i] = sc[NT_X + i];
-                    }
-                    __syncthreads();
-                    slot_geo_dual(sh, sh.dx, *Gd);
-                    pass_dual(sh, nt, d, *Gd, NT_MODE_HV, lsc, nullptr, nullptr);
-                    __syncthreads();
-                    const double xHx = nt_dot(sh, nt, sh.dmp, nt.hp, lsc, NT_X, NT_HP);
-                    const double bx = nt_dot(sh, nt, sh.rhs, sh.dmp, lsc, NT_B, NT_X);
-                    const double pred = bx - 0.5 * xHx;
-                    // the trial state: poses R Exp(dphi), p + dp (held slot unchanged), landmarks + x_l
-                    for (int s = tid; s < P; s += blockDim.x) {
-                        double Re[9], R[9];
-                        for (int i = 0; i < 9; ++i) R[i] = sh.Rwb[9 * s + i];
-                        if (sh.w.hold == s) {
-                            for (int i = 0; i < 9; ++i) sh.R2[9 * s + i] = R[i];
-                            for (int i = 0; i < 3; ++i) sh.p2[3 * s + i] = sh.pwb[3 * s + i];
-                            continue;
-                        }
-                        so3_exp(sh.dmp + 6 * s, Re);
-                        for (int i = 0; i < 3; ++i)
-                            for (int j = 0; j < 3; ++j)
-                                sh.R2[9 * s + 3 * i + j] = R[3 * i] * Re[j] + R[3 * i + 1] * Re[3 + j] + R[3 * i + 2] * Re[6 + j];
-                        for (int i = 0; i < 3; ++i) sh.p2[3 * s + i] = sh.pwb[3 * s + i] + sh.dmp[6 * s + 3 + i];
-                    }
-                    for (int l = tid; l < sh.w.L; l += blockDim.x) {
-                        const int gl = sh.w.lm0 + l;
-                        const double* sc = lsc + (size_t)gl * NT_LM_STRIDE;
-                        for (int i = 0; i < 3; ++i) d.lmp[3 * gl + i] += sc[NT_X + i];
-                    }
-                    __syncthreads();
-                    slot_geo(sh, sh.R2, sh.p2);
-                    pass_cost(sh, d, sh.g64, d.lmp);
-                    const double c1 = block_sum_red(sh);
-                    // the cost is a float64 sum of ~1e4 terms: below ~1e-10 of it a decrease is rounding noise, so a
-                    // step whose predicted decrease is that small is kept unless the cost visibly rose
-                    const double noise = 1e-10 * fabs(c0);
-                    const bool tiny = fabs(pred) <= noise;
-                    const double ratio = pred > 0.0 ? (c0 - c1) / pred : -1.0;
-                    if ((tiny && c1 <= c0 + noise) || ratio > 1e-4) {
-                        for (int q = tid; q < P * 9; q += blockDim.x) sh.Rwb[q] = sh.R2[q];
-                        for (int q = tid; q < P * 3; q += blockDim.x) sh.pwb[q] = sh.p2[q];
-                        c0 = c1;
-                        moved = true;
-                        last_ok = true;
-                        if (ratio > 0.75 && bnd) delta *= 2.0;
-                        else if (ratio < 0.25 && !tiny) delta = 0.25 * sqrt(xMx);
-                    } else {
-                        for (int l = tid; l < sh.w.L; l += blockDim.x) {
-                            const int gl = sh.w.lm0 + l;
-                            const double* sc = lsc + (size_t)gl * NT_LM_STRIDE;
-                            for (int i = 0; i < 3; ++i) d.lmp[3 * gl + i] -= sc[NT_X + i];
-                        }
-                        delta = 0.25 * sqrt(xMx);
-                        last_ok = false;
-                    }
-                    __syncthreads();
-                    slot_geo(sh, sh.Rwb, sh.pwb);
-                    if (!(delta > 0.0)) { status = 2; st = steps; }
-                }
-            }
-            if (!last_ok && status == 0) status = 2;
-            // the gradient at the final state
+            // the landmark-eliminated Newton polish (nt_polish), then the gradient at the final state (flagging the
+            // landmarks the LM cannot move when `upd`)
+            int taken = 0;
+            double mu = 0.0;
+            if (steps > 0)
+                status = nt_polish(sh, nt, d, dsm, lsc, scopy + (size_t)w * NT_SC, steps, upd, &taken, &mu);
+            iters = taken;
+            rel = mu;
             slot_geo(sh, sh.Rwb, sh.pwb);
             nt_grad(sh, nt, d, dsm, lsc, upd);
             gmax = nt_gmax(sh, nt, lsc);
@@ -1860,21 +2406,22 @@ __global__ void __launch_bounds__(BA_THREADS, 1) k_ba_newton(XcbBaWindows d, int
 size_t xcb_ba_newton_smem_bytes(int maxP)
 {
     const int n = 6 * maxP;
-    size_t x = ba_x_bytes(n);
-    if (sizeof(SlotGeo<Dual>) > x) x = sizeof(SlotGeo<Dual>);
-    return ba_off_x(n) + x;
+    return ba_off_x(n) + nt_x_bytes(n) + sizeof(SlotGeo<Dual>);
 }
+
+size_t xcb_ba_newton_copy_doubles(int nw) { return (size_t)(nw > 0 ? nw : 1) * NT_SC; }
 
 cudaError_t xcb_launch_ba_newton(const XcbBaWindows& d, int max_slots, int mode, int steps, int maxit, double tol,
                                  const double* gpose, double* gtheta, double* gisig, double* gz, double* stats,
-                                 double* lsc, int* counter, int grid, cudaStream_t st, size_t lsc_doubles)
+                                 double* lsc, int* counter, int grid, cudaStream_t st, size_t lsc_doubles,
+                                 double* scopy)
 {
     static XcbAttrOnce attr;
     cudaError_t e = xcb_smem_attr_once(attr, (const void*)k_ba_newton, (int)xcb_ba_newton_smem_bytes(BA_MAXP));
     if (e != cudaSuccess) return e;
     k_ba_newton<<<grid, BA_THREADS, xcb_ba_newton_smem_bytes(max_slots), st>>>(d, mode, steps, maxit, tol, gpose,
                                                                                gtheta, gisig, gz, stats, lsc, counter,
-                                                                               lsc_doubles);
+                                                                               lsc_doubles, scopy);
     return cudaGetLastError();
 }
 
