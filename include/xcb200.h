@@ -461,7 +461,7 @@ int xcb_ba_solve_windows_noalloc(const xcb_ba_windows* w, int Lt, int max_slots,
    definite or the cost does not decrease), the landmarks following to first order; landmarks whose minimum lies at
    infinity (inverse depth below 1e-7, or their own Newton step taking it to <= 1e-9) are flagged constant (not in
    XCB_BA_NEWTON_POLISH_FIXED); it stops early at a gradient max-norm of 1e-10 or when a step at the cost's rounding
-   level no longer halves it.  XCB_BA_NEWTON_ADJOINT: at the converged
+   level in a row no longer halve it (three times).  XCB_BA_NEWTON_ADJOINT: at the converged
    state, solves H x = dL/dstate (gpose: [slots][6] = dL/d(dphi, dp) per slot of the batch, landmarks 0) and writes
    dL/dtheta = -(d2C / dtheta dstate) x: gtheta [nw][11] = fx, fy, cx, cy, B, omega (3), t (3) of the left-to-right
    extrinsic at the rectified rig; gisig [M] = per-row weight 1/sigma; gz [M][2] = per-row pixels.  H is applied

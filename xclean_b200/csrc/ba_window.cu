@@ -1677,7 +1677,7 @@ __device__ double nt_gmax(BaShared& sh, NtShared& nt, const double* lsc)
 // Second derivatives come from dual numbers: Hll and Hlp from three landmark directions per landmark, Hpp from one pass
 // per pose direction over the row groups that have that slot as host or target.
 // =====================================================================================================================
-#define NT_INNER 8              // Newton iterations per landmark in (1)
+#define NT_INNER 32             // Newton iterations per landmark in (1)
 #define NT_RETRY 10             // damping increases per step
 #define NT_SC (BA_MAXN * (BA_MAXN + 1) / 2)     // doubles per window of the reduced-system copy
 #define NT_RHO_INF 1e-7         // a landmark whose inverse depth falls below this has its minimum at infinity
@@ -2170,8 +2170,8 @@ __device__ void nt_geo(BaShared& sh, SlotGeo<Dual>& G0)
 }
 
 // the landmark-eliminated Newton polish of one window (the state in sh.Rwb / sh.pwb and d.lmp); `steps` bounds the
-// Newton steps; it stops early at a gradient max-norm of 1e-10, or when a step at the cost's rounding level did not
-// halve it.  upd: landmarks whose minimum lies at infinity are flagged constant (pass_xbuild).  -> status (0, or 2 when
+// Newton steps; it stops early at a gradient max-norm of 1e-10, or after three steps in a row at the cost's rounding
+// level that did not halve it.  upd: landmarks whose minimum lies at infinity are flagged constant (pass_xbuild).  -> status (0, or 2 when
 // no damping gave a decrease); *steps_out, *mu_out the steps taken and the final damping
 __device__ int nt_polish(BaShared& sh, NtShared& nt, const XcbBaWindows& d, unsigned char* dsm, double* lsc,
                          double* Sc, int steps, bool upd, int* steps_out, double* mu_out)
@@ -2186,7 +2186,7 @@ __device__ int nt_polish(BaShared& sh, NtShared& nt, const XcbBaWindows& d, unsi
     pass_inner(sh, d, *G0, lsc);
     double c0 = block_sum_red(sh);
     double mu = 0.0, gm_prev = 0.0;
-    int st = 0, status = 0;
+    int st = 0, status = 0, stall = 0;
     bool tiny = false;
     while (st < steps) {
         // the exact reduced system at the current state
@@ -2223,7 +2223,9 @@ __device__ int nt_polish(BaShared& sh, NtShared& nt, const XcbBaWindows& d, unsi
         __syncthreads();
         if ((tid & 31) == 0) sh.red[tid >> 5] = gm;
         gm = fmax(block_max_red(sh), gml);
-        if (gm <= 1e-10 || (tiny && gm > 0.5 * gm_prev)) break;
+        // three steps in a row at the cost's rounding level that did not halve the gradient: no further progress
+        stall = tiny && gm > 0.5 * gm_prev ? stall + 1 : 0;
+        if (gm <= 1e-10 || stall >= 3) break;
         gm_prev = gm;
         for (int q = tid; q < ntri; q += blockDim.x) Sc[q] = S[q];
         __syncthreads();
