@@ -1156,9 +1156,9 @@ ADJ_NEWTON = 30
 
 
 def run_adjoint(args, dev, stream, ws_world, rank):
-    """Differentiable BA: 64 windows of 10 keyframes and 2,000 landmarks; forward = 20 LM iterations, two rounds of 40
-    LM iterations with the landmarks the LM cannot move held constant, up to 30 landmark-eliminated Newton steps on the
-    exact Hessian; loss = sum of squared translation errors against the ground truth, backward = the implicit adjoint
+    """Differentiable BA: 64 windows of 10 keyframes and 2,000 landmarks; forward = 20 LM iterations, 20 LM iterations
+    with the landmarks the LM cannot move held constant, up to 30 landmark-eliminated Newton steps on the exact Hessian;
+    loss = sum of squared translation errors against the ground truth, backward = the implicit adjoint
     (gradients to fx, fy, cx, cy, baseline, left-right extrinsic, per-row weights and pixels)."""
     import torch
     from xclean_b200.backend import synth_ba as S
@@ -1193,9 +1193,9 @@ def run_adjoint(args, dev, stream, ws_world, rank):
             "final_gradient_max_median": float(np.median(st[:, 2])),
             "final_gradient_max_quartiles": [float(x) for x in np.percentile(st[:, 2], [25, 75])],
             "config": {"workload": "64 windows x (10 keyframes, 2000 landmarks, 2-6 obs, 5%% outliers); forward 20 LM "
-                                   "iterations, 2 x 40 LM iterations with the landmarks the LM cannot move held "
+                                   "iterations, 20 LM iterations with the landmarks the LM cannot move held "
                                    "constant, up to %d landmark-eliminated Newton steps; implicit adjoint of "
-                                   "sum |t - t_gt|^2" % ADJ_NEWTON}}
+                                   "sum |t - t_gt|^2 by the exact reduced system" % ADJ_NEWTON}}
 
 
 def cpu_baseline(L, R, args):

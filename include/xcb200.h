@@ -465,9 +465,11 @@ int xcb_ba_solve_windows_noalloc(const xcb_ba_windows* w, int Lt, int max_slots,
    state, solves H x = dL/dstate (gpose: [slots][6] = dL/d(dphi, dp) per slot of the batch, landmarks 0) and writes
    dL/dtheta = -(d2C / dtheta dstate) x: gtheta [nw][11] = fx, fy, cx, cy, B, omega (3), t (3) of the left-to-right
    extrinsic at the rectified rig; gisig [M] = per-row weight 1/sigma; gz [M][2] = per-row pixels.  H is applied
-   exactly (dual numbers) and the system solved by conjugate gradients preconditioned with the Gauss-Newton Schur
-   system until the relative residual is below `tol` (at most `maxit` iterations).  stats [nw][4]: polish = Newton
-   steps taken, final damping, final gradient max-norm, status; adjoint = iterations, final relative residual, -,
+   exactly (dual numbers); the system is solved with the Cholesky factor of the exact reduced system (the landmarks
+   by back-substitution) and at most two refinement steps while the relative residual is above `tol`, or, where the
+   reduced system is not positive definite, by conjugate gradients preconditioned with the Gauss-Newton Schur
+   system (at most `maxit` iterations).  stats [nw][4]: polish = Newton steps taken, final damping, final gradient
+   max-norm, status; adjoint = refinement steps (or conjugate-gradient iterations), final relative residual, -,
    status.  Status: 0 ok, 1 Gauss-Newton system not positive definite, 2 (polish) no damping gave a decrease /
    (adjoint) non-positive curvature met: the state is not at a strict minimum, -1 window too large, -2 a landmark
    touches more than 16 keyframes, XCB_BA_STATUS_SCRATCH the scratch, less its last xcb_ba_newton_scratch_bytes(nw, 0)

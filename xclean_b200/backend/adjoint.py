@@ -13,12 +13,15 @@ converged poses to de-rectifying it), weights [M] (the per-row weight 1/sigma in
 
 Forward: `iters` LM iterations of window.solve (float64, batched, one launch); then the landmarks whose
 Gauss-Newton step would take the inverse depth to <= 1e-9 (window.solve keeps them where they are, while its Schur
-complement assumes they move, so its fixed point is not stationary) are flagged constant and two rounds of
-`free_iters` LM iterations run with them held; then at most `newton_steps` landmark-eliminated Newton steps on the
+complement assumes they move, so its fixed point is not stationary) are flagged constant and `free_iters` LM
+iterations run with them held; then at most `newton_steps` landmark-eliminated Newton steps on the
 exact Hessian (the LM converges only linearly where Huber weights are active, and the adjoint is exact only at a
 stationary point): each moves every landmark to the minimum of its own cost with the poses fixed, then solves the exact
-reduced pose system; landmarks whose minimum lies at infinity (rho < 1e-7) are flagged constant on the way.  Backward: one solve H x = dL/dstate (H applied exactly through dual numbers, conjugate gradients
-preconditioned with the Gauss-Newton Cholesky factor, Jacobians recomputed from the state rather than stored), then dL/dtheta = -(d2C / dtheta dstate) x, scattered to the window parameters and to every observation row.
+reduced pose system; landmarks whose minimum lies at infinity (rho < 1e-7) are flagged constant on the way.  Backward: one solve H x = dL/dstate with the exact reduced system (its Cholesky factor for the poses,
+the landmarks by back-substitution, at most two refinement steps on the exact residual; H applied through dual numbers,
+Jacobians recomputed from the state rather than stored; conjugate gradients preconditioned with the Gauss-Newton
+system where the reduced system is not positive definite), then dL/dtheta = -(d2C / dtheta dstate) x, scattered to
+the window parameters and to every observation row.
 The solver keeps the converged state between forward and backward: do not reuse it for another forward before
 backward.  ctx.newton_stats / ctx.adjoint_stats keep the per-window stats (column 2: the gradient max-norm at the
 returned state; a window that did not reach a stationary point within `newton_steps` has an approximate gradient).
@@ -32,7 +35,7 @@ import torch
 class BAAdjoint(torch.autograd.Function):
     @staticmethod
     def forward(ctx, intrinsics, baseline, extrinsic, weights, pixels, solver, iters=20, newton_steps=40,
-                lam0=1e-4, tol=1e-12, free_iters=40):
+                lam0=1e-4, tol=1e-12, free_iters=20):
         if float(extrinsic.detach().abs().max()) != 0.0:
             raise ValueError("BAAdjoint: the left-to-right extrinsic is the rectified rig (zero); only its gradient "
                              "is returned")
@@ -49,9 +52,8 @@ class BAAdjoint(torch.autograd.Function):
             t["ob_z"].copy_(pixels.detach().to(torch.float64))
             solver.reset()
             solver.solve(int(iters), float(lam0), "fp64")
-            for _ in range(2):
-                solver.newton(0)                                    # flag the landmarks the LM cannot move
-                solver.solve_free(int(free_iters), float(lam0))
+            solver.newton(0)                                        # flag the landmarks the LM cannot move
+            solver.solve_free(int(free_iters), float(lam0))
             st = solver.newton(int(newton_steps), tol=float(tol))
         ctx.solver = solver
         ctx.tol = float(tol)

@@ -2097,9 +2097,61 @@ __device__ void pass_xbuild(BaShared& sh, NtShared& nt, const XcbBaWindows& d, c
     if (lane == 0) sh.red[wid] = gmax;
 }
 
-// (3) the landmarks' first-order step with the poses, dl = -Hll^-1 Hlp dp (G: the geometry at the current
-// state moved along dp; Hlp dp is the dual part of the landmark gradient), for the landmarks the build kept; every
-// landmark's state is saved to the scratch first (restored when the trial is rejected)
+// Hlp dp of landmark gl (G: the geometry moved along dp, the landmark's tangent zero): the dual part of its gradient,
+// summed over its row groups; identical on every lane
+__device__ void lm_hlp(const BaShared& sh, const XcbBaWindows& d, const SlotGeo<Dual>& G, int gl, int h,
+                       const double lmv[3], double u[3])
+{
+    const int lane = threadIdx.x & 31;
+    const int k0 = d.lm_ob[gl], nob = lm_rows(d, gl);
+    for (int r = 0; r < 3; ++r) u[r] = 0.0;
+    if (lane < nob) {
+        const int k = k0 + lane, t = d.ob_pose[k];
+        if (d.ob_valid[k] && (unsigned)t < (unsigned)sh.w.P && t != h) {
+            const Dual lm[3] = {Dual(lmv[0]), Dual(lmv[1]), Dual(lmv[2])};
+            Dual ob[OB_N];
+            if (obs_lin<Dual>(sh.w, G, lm, h, t, d.ob_cam[k], d.ob_z + 2 * k, Dual(d.ob_isig[k]), ob, 2)) {
+                const Dual en = sqrt(ob[OB_E] * ob[OB_E] + ob[OB_E + 1] * ob[OB_E + 1]);
+                Dual wt, cc;
+                huber_w<Dual>(en, Dual(sh.w.hk), &wt, &cc);
+                for (int r = 0; r < 3; ++r)
+                    u[r] = (wt * (ob[OB_JL + r] * ob[OB_E] + ob[OB_JL + 3 + r] * ob[OB_E + 1])).e;
+            }
+        }
+    }
+    for (int r = 0; r < 3; ++r) u[r] = warp_sum(u[r]);
+}
+
+// Hpl v of landmark gl for a landmark tangent v (G0: zero pose tangents), added to acc (poses; shared atomics)
+__device__ void lm_hpl(const BaShared& sh, const XcbBaWindows& d, const SlotGeo<Dual>& G0, int gl, int h,
+                       const double lmv[3], const double v[3], double* acc)
+{
+    const int lane = threadIdx.x & 31;
+    const int k0 = d.lm_ob[gl], nob = lm_rows(d, gl);
+    if (lane < nob) {
+        const int k = k0 + lane, t = d.ob_pose[k];
+        if (d.ob_valid[k] && (unsigned)t < (unsigned)sh.w.P && t != h) {
+            const Dual lm[3] = {Dual(lmv[0], v[0]), Dual(lmv[1], v[1]), Dual(lmv[2], v[2])};
+            Dual ob[OB_N];
+            if (obs_lin<Dual>(sh.w, G0, lm, h, t, d.ob_cam[k], d.ob_z + 2 * k, Dual(d.ob_isig[k]), ob, 1)) {
+                const Dual en = sqrt(ob[OB_E] * ob[OB_E] + ob[OB_E + 1] * ob[OB_E + 1]);
+                Dual wt, cc;
+                huber_w<Dual>(en, Dual(sh.w.hk), &wt, &cc);
+                for (int q = 0; q < 6; ++q) {
+                    const Dual gh = wt * (obj(ob, OB_JH, 0, q) * ob[OB_E] + obj(ob, OB_JH, 1, q) * ob[OB_E + 1]);
+                    const Dual gt = wt * (ob[OB_JT + q] * ob[OB_E] + ob[OB_JT + 6 + q] * ob[OB_E + 1]);
+                    atomicAdd(&acc[6 * h + q], gh.e);
+                    atomicAdd(&acc[6 * t + q], gt.e);
+                }
+            }
+        }
+    }
+    __syncwarp();
+}
+
+// (3) the landmarks' first-order step with the poses, dl = -Hll^-1 Hlp dp (G: the geometry at the current state moved
+// along dp), for the landmarks the build kept; every landmark's state is saved to the scratch first (restored when the
+// trial is rejected)
 __device__ void pass_lstep(BaShared& sh, const XcbBaWindows& d, const SlotGeo<Dual>& G, double* lsc)
 {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -2112,30 +2164,60 @@ __device__ void pass_lstep(BaShared& sh, const XcbBaWindows& d, const SlotGeo<Du
         const double lmv[3] = {d.lmp[3 * gl], d.lmp[3 * gl + 1], d.lmp[3 * gl + 2]};
         if (lane < 3) sc[NR_BK + lane] = lmv[lane];
         if (!(sc[NR_HI] > 0.0)) { __syncwarp(); continue; }
-        const int k0 = d.lm_ob[gl], nob = lm_rows(d, gl);
-        double u[3] = {0.0, 0.0, 0.0};
-        if (lane < nob) {
-            const int k = k0 + lane, t = d.ob_pose[k];
-            if (d.ob_valid[k] && (unsigned)t < (unsigned)sh.w.P && t != h) {
-                const Dual lm[3] = {Dual(lmv[0]), Dual(lmv[1]), Dual(lmv[2])};
-                Dual ob[OB_N];
-                if (obs_lin<Dual>(sh.w, G, lm, h, t, d.ob_cam[k], d.ob_z + 2 * k, Dual(d.ob_isig[k]), ob, 2)) {
-                    const Dual en = sqrt(ob[OB_E] * ob[OB_E] + ob[OB_E + 1] * ob[OB_E + 1]);
-                    Dual wt, cc;
-                    huber_w<Dual>(en, Dual(sh.w.hk), &wt, &cc);
-                    for (int r = 0; r < 3; ++r)
-                        u[r] = (wt * (ob[OB_JL + r] * ob[OB_E] + ob[OB_JL + 3 + r] * ob[OB_E + 1])).e;
-                }
-            }
-        }
-        for (int r = 0; r < 3; ++r) u[r] = warp_sum(u[r]);
-        double Hi[6], dl[3];
+        double u[3], Hi[6], dl[3];
+        lm_hlp(sh, d, G, gl, h, lmv, u);
         for (int q = 0; q < 6; ++q) Hi[q] = sc[NR_HI + q];
         sym3_mv(Hi, u, dl);
         const double nr = lmv[2] - dl[2];
         if (nr > 1e-9 && isfinite(nr) && isfinite(dl[0]) && isfinite(dl[1]) && lane < 3)
             d.lmp[3 * gl + lane] = lmv[lane] - dl[lane];
         __syncwarp();
+    }
+}
+
+// the adjoint's landmark part from a pose part (G: the geometry moved along it): first = true, x_l = -Hll^-1 Hlp x_p
+// -> NT_P (0 for the landmarks the build did not keep); false, the refinement x_l += Hll^-1 (r_l - Hlp dx_p) (r_l in
+// NT_Z)
+__device__ void pass_adj_l(BaShared& sh, const XcbBaWindows& d, const SlotGeo<Dual>& G, double* lsc, bool first)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int l = sh.lb + wid; l < sh.le; l += BA_WARPS) {
+        const int gl = sh.w.lm0 + l;
+        double* sc = lsc + (size_t)gl * NT_LM_STRIDE;
+        const int h = d.lm_host[gl];
+        if (!d.lm_mask[gl] || (unsigned)h >= (unsigned)sh.w.P || !(sc[NR_HI] > 0.0)) {
+            if (first && lane < 3) sc[NT_P + lane] = 0.0;
+            __syncwarp();
+            continue;
+        }
+        const double lmv[3] = {d.lmp[3 * gl], d.lmp[3 * gl + 1], d.lmp[3 * gl + 2]};
+        double u[3], Hi[6], x[3];
+        lm_hlp(sh, d, G, gl, h, lmv, u);
+        if (!first)
+            for (int r = 0; r < 3; ++r) u[r] -= sc[NT_Z + r];
+        for (int q = 0; q < 6; ++q) Hi[q] = sc[NR_HI + q];
+        sym3_mv(Hi, u, x);
+        __syncwarp();
+        if (lane < 3) sc[NT_P + lane] = (first ? 0.0 : sc[NT_P + lane]) - x[lane];
+        __syncwarp();
+    }
+}
+
+// acc (poses) += sum over the kept landmarks of Hpl Hll^-1 r_l (r_l in NT_Z)
+__device__ void pass_adj_y(BaShared& sh, const XcbBaWindows& d, const SlotGeo<Dual>& G0, const double* lsc,
+                           double* acc)
+{
+    const int wid = threadIdx.x >> 5;
+    for (int l = sh.lb + wid; l < sh.le; l += BA_WARPS) {
+        const int gl = sh.w.lm0 + l;
+        const double* sc = lsc + (size_t)gl * NT_LM_STRIDE;
+        const int h = d.lm_host[gl];
+        if (!d.lm_mask[gl] || (unsigned)h >= (unsigned)sh.w.P || !(sc[NR_HI] > 0.0)) continue;
+        const double lmv[3] = {d.lmp[3 * gl], d.lmp[3 * gl + 1], d.lmp[3 * gl + 2]};
+        double Hi[6], v[3];
+        for (int q = 0; q < 6; ++q) Hi[q] = sc[NR_HI + q];
+        sym3_mv(Hi, sc + NT_Z, v);
+        lm_hpl(sh, d, G0, gl, h, lmv, v, acc);
     }
 }
 
@@ -2169,17 +2251,63 @@ __device__ void nt_geo(BaShared& sh, SlotGeo<Dual>& G0)
     slot_geo_dual(sh, sh.dx, G0);
 }
 
-// the landmark-eliminated Newton polish of one window (the state in sh.Rwb / sh.pwb and d.lmp); `steps` bounds the
-// Newton steps; it stops early at a gradient max-norm of 1e-10, or after three steps in a row at the cost's rounding
-// level that did not halve it.  upd: landmarks whose minimum lies at infinity are flagged constant (pass_xbuild).  -> status (0, or 2 when
-// no damping gave a decrease); *steps_out, *mu_out the steps taken and the final damping
-__device__ int nt_polish(BaShared& sh, NtShared& nt, const XcbBaWindows& d, unsigned char* dsm, double* lsc,
-                         double* Sc, int steps, bool upd, int* steps_out, double* mu_out)
+// the exact reduced system at the state in sh.Rwb / sh.pwb (G0 built from it): S (packed lower, the held slot's rows
+// and columns the identity) from the column passes and pass_xbuild, sh.g the pose gradient (held slot 0).  -> the
+// largest |g| over the poses and the variable landmarks
+__device__ double nt_xsystem(BaShared& sh, NtShared& nt, const XcbBaWindows& d, unsigned char* dsm, double* lsc,
+                             bool upd)
 {
     const int n = sh.w.n, P = sh.w.P, tid = threadIdx.x;
     double* S = (double*)dsm;
     WarpLm<double>* wl64 = (WarpLm<double>*)(dsm + ba_off_x(n));
     SlotGeo<Dual>* Gd = (SlotGeo<Dual>*)(dsm + ba_off_x(n));           // aliases wl64: never live together
+    SlotGeo<Dual>* G0 = (SlotGeo<Dual>*)(dsm + ba_off_x(n) + nt_x_bytes(n));
+    const int ntri = n * (n + 1) / 2;
+    for (int q = tid; q < ntri; q += blockDim.x) S[q] = 0.0;
+    for (int q = tid; q < n; q += blockDim.x) nt.gp[q] = 0.0;
+    __syncthreads();
+    for (int c = 0; c < n; ++c) {
+        if (held(sh, c)) continue;
+        for (int q = tid; q < n; q += blockDim.x) sh.dx[q] = q == c ? 1.0 : 0.0;
+        __syncthreads();
+        slot_geo_dual(sh, sh.dx, *Gd);
+        pass_hpp_col(sh, d, *Gd, c / 6, c, S);
+        __syncthreads();
+    }
+    pass_xbuild(sh, nt, d, *G0, S, wl64, lsc, upd);
+    const double gml = block_max_red(sh);
+    const int hs = sh.w.hold;
+    if (hs >= 0 && hs < P) {
+        for (int q = tid; q < 6 * n; q += blockDim.x) {
+            const int i = 6 * hs + q / n, j = q % n;
+            S[i >= j ? tri(i, j) : tri(j, i)] = 0.0;
+        }
+        __syncthreads();
+        for (int q = tid; q < 6; q += blockDim.x) S[tri(6 * hs + q, 6 * hs + q)] = 1.0;
+    }
+    // the pose gradient (sh.g) and the largest |g| over the poses and the variable landmarks
+    double gm = 0.0;
+    for (int q = tid; q < n; q += blockDim.x) {
+        const bool hq = held(sh, q);
+        sh.g[q] = hq ? 0.0 : nt.gp[q];
+        if (!hq) gm = fmax(gm, fabs(nt.gp[q]));
+    }
+    for (int o = 16; o > 0; o >>= 1) gm = fmax(gm, __shfl_xor_sync(0xffffffffu, gm, o));
+    __syncthreads();
+    if ((tid & 31) == 0) sh.red[tid >> 5] = gm;
+    return fmax(block_max_red(sh), gml);
+}
+
+// the landmark-eliminated Newton polish of one window (the state in sh.Rwb / sh.pwb and d.lmp); `steps` bounds the
+// Newton steps; it stops early at a gradient max-norm of 1e-10, or after three steps in a row at the cost's rounding
+// level that did not halve it.  upd: landmarks whose minimum lies at infinity are flagged constant (pass_xbuild).
+// -> status (0, or 2 when no damping gave a decrease); *steps_out, *mu_out the steps taken and the final damping
+__device__ int nt_polish(BaShared& sh, NtShared& nt, const XcbBaWindows& d, unsigned char* dsm, double* lsc,
+                         double* Sc, int steps, bool upd, int* steps_out, double* mu_out)
+{
+    const int n = sh.w.n, P = sh.w.P, tid = threadIdx.x;
+    double* S = (double*)dsm;
+    SlotGeo<Dual>* Gd = (SlotGeo<Dual>*)(dsm + ba_off_x(n));           // aliases the warp scratch of the build
     SlotGeo<Dual>* G0 = (SlotGeo<Dual>*)(dsm + ba_off_x(n) + nt_x_bytes(n));
     const int ntri = n * (n + 1) / 2;
     nt_geo(sh, *G0);
@@ -2189,40 +2317,7 @@ __device__ int nt_polish(BaShared& sh, NtShared& nt, const XcbBaWindows& d, unsi
     int st = 0, status = 0, stall = 0;
     bool tiny = false;
     while (st < steps) {
-        // the exact reduced system at the current state
-        for (int q = tid; q < ntri; q += blockDim.x) S[q] = 0.0;
-        for (int q = tid; q < n; q += blockDim.x) nt.gp[q] = 0.0;
-        __syncthreads();
-        for (int c = 0; c < n; ++c) {
-            if (held(sh, c)) continue;
-            for (int q = tid; q < n; q += blockDim.x) sh.dx[q] = q == c ? 1.0 : 0.0;
-            __syncthreads();
-            slot_geo_dual(sh, sh.dx, *Gd);
-            pass_hpp_col(sh, d, *Gd, c / 6, c, S);
-            __syncthreads();
-        }
-        pass_xbuild(sh, nt, d, *G0, S, wl64, lsc, upd);
-        const double gml = block_max_red(sh);
-        const int hs = sh.w.hold;
-        if (hs >= 0 && hs < P) {
-            for (int q = tid; q < 6 * n; q += blockDim.x) {
-                const int i = 6 * hs + q / n, j = q % n;
-                S[i >= j ? tri(i, j) : tri(j, i)] = 0.0;
-            }
-            __syncthreads();
-            for (int q = tid; q < 6; q += blockDim.x) S[tri(6 * hs + q, 6 * hs + q)] = 1.0;
-        }
-        // the pose gradient (sh.g) and the largest |g| over the poses and the variable landmarks
-        double gm = 0.0;
-        for (int q = tid; q < n; q += blockDim.x) {
-            const bool hq = held(sh, q);
-            sh.g[q] = hq ? 0.0 : nt.gp[q];
-            if (!hq) gm = fmax(gm, fabs(nt.gp[q]));
-        }
-        for (int o = 16; o > 0; o >>= 1) gm = fmax(gm, __shfl_xor_sync(0xffffffffu, gm, o));
-        __syncthreads();
-        if ((tid & 31) == 0) sh.red[tid >> 5] = gm;
-        gm = fmax(block_max_red(sh), gml);
+        const double gm = nt_xsystem(sh, nt, d, dsm, lsc, upd);
         // three steps in a row at the cost's rounding level that did not halve the gradient: no further progress
         stall = tiny && gm > 0.5 * gm_prev ? stall + 1 : 0;
         if (gm <= 1e-10 || stall >= 3) break;
@@ -2294,6 +2389,74 @@ __device__ int nt_polish(BaShared& sh, NtShared& nt, const XcbBaWindows& d, unsi
     *steps_out = st;
     *mu_out = mu;
     return status;
+}
+
+// The implicit adjoint's solve H x = b (b: gpose for the poses, 0 for the landmarks) through the exact reduced system at
+// the state in sh.Rwb / sh.pwb: x_p = S^-1 b_p, x_l = -Hll^-1 Hlp x_p, then at most two refinement steps on the residual
+// b - H x (H x exactly, one dual pass).  -> false when S is not positive definite (then nothing is solved); else x in
+// sh.dmp (poses) and NT_P (landmarks), *rel the final relative residual, *iters the refinement steps taken
+__device__ bool nt_adjoint_direct(BaShared& sh, NtShared& nt, const XcbBaWindows& d, unsigned char* dsm, double* lsc,
+                                  const double* b, double tol, double* rel, int* iters)
+{
+    const int n = sh.w.n, tid = threadIdx.x;
+    double* S = (double*)dsm;
+    SlotGeo<Dual>* Gd = (SlotGeo<Dual>*)(dsm + ba_off_x(n));
+    SlotGeo<Dual>* G0 = (SlotGeo<Dual>*)(dsm + ba_off_x(n) + nt_x_bytes(n));
+    nt_geo(sh, *G0);
+    nt_xsystem(sh, nt, d, dsm, lsc, false);
+    if (chol_factor(S, n)) return false;
+    double b2 = 0.0;
+    for (int q = tid; q < n; q += blockDim.x) {
+        sh.rhs[q] = held(sh, q) ? 0.0 : b[q];
+        sh.dmp[q] = sh.rhs[q];
+        b2 += sh.rhs[q] * sh.rhs[q];
+    }
+    b2 = warp_sum(b2);
+    __syncthreads();
+    if ((tid & 31) == 0) sh.red[tid >> 5] = b2;
+    const double bn = sqrt(block_sum_red(sh));
+    chol_solve(S, n, sh.dmp);
+    for (int q = tid; q < n; q += blockDim.x) sh.dx[q] = sh.dmp[q];
+    __syncthreads();
+    slot_geo_dual(sh, sh.dx, *Gd);
+    pass_adj_l(sh, d, *Gd, lsc, true);
+    __syncthreads();
+    int it = 0;
+    *rel = 0.0;
+    while (bn > 0.0) {
+        // r = b - H x: poses -> sh.g, landmarks -> NT_Z
+        for (int q = tid; q < n; q += blockDim.x) { nt.gp[q] = 0.0; nt.hp[q] = 0.0; sh.dx[q] = sh.dmp[q]; }
+        __syncthreads();
+        slot_geo_dual(sh, sh.dx, *Gd);
+        pass_dual(sh, nt, d, *Gd, NT_MODE_HV, lsc, nullptr, nullptr);
+        __syncthreads();
+        for (int q = tid; q < n; q += blockDim.x) sh.g[q] = held(sh, q) ? 0.0 : sh.rhs[q] - nt.hp[q];
+        for (int l = tid; l < sh.w.L; l += blockDim.x) {
+            double* sc = lsc + (size_t)(sh.w.lm0 + l) * NT_LM_STRIDE;
+            for (int i = 0; i < 3; ++i) sc[NT_Z + i] = -sc[NT_HP + i];
+        }
+        __syncthreads();
+        *rel = sqrt(nt_dot(sh, nt, sh.g, sh.g, lsc, NT_Z, NT_Z)) / bn;
+        if (!(*rel > tol) || it >= 2) break;
+        ++it;
+        // dx_p = S^-1 (r_p - sum Hpl Hll^-1 r_l), dx_l = Hll^-1 (r_l - Hlp dx_p)
+        for (int q = tid; q < n; q += blockDim.x) nt.gp[q] = 0.0;
+        __syncthreads();
+        pass_adj_y(sh, d, *G0, lsc, nt.gp);
+        __syncthreads();
+        for (int q = tid; q < n; q += blockDim.x) sh.y[q] = held(sh, q) ? 0.0 : sh.g[q] - nt.gp[q];
+        __syncthreads();
+        chol_solve(S, n, sh.y);
+        for (int q = tid; q < n; q += blockDim.x) sh.dx[q] = sh.y[q];
+        __syncthreads();
+        slot_geo_dual(sh, sh.dx, *Gd);
+        pass_adj_l(sh, d, *Gd, lsc, false);
+        __syncthreads();
+        for (int q = tid; q < n; q += blockDim.x) sh.dmp[q] += sh.y[q];
+        __syncthreads();
+    }
+    *iters = it;
+    return true;
 }
 
 __global__ void __launch_bounds__(BA_THREADS, 1) k_ba_newton(XcbBaWindows d, int mode, int steps, int maxit,
@@ -2370,25 +2533,35 @@ __global__ void __launch_bounds__(BA_THREADS, 1) k_ba_newton(XcbBaWindows d, int
             for (int q = tid; q < P * 9; q += blockDim.x) d.Rwb[9 * s0 + q] = sh.Rwb[q];
             for (int q = tid; q < P * 3; q += blockDim.x) d.pwb[3 * s0 + q] = sh.pwb[q];
         } else {
-            // implicit adjoint: H x = dL/dx (poses from gpose, landmarks 0), then -(d2C / dtheta dx) x
-            slot_geo(sh, sh.Rwb, sh.pwb);
-            if (nt_gn_factor(sh, d, S64, wl64, lsc)) status = 1;
-            else {
-                nt_grad(sh, nt, d, dsm, lsc, false);       // the gradient; constant landmarks as flagged
-                for (int q = tid; q < n; q += blockDim.x) sh.rhs[q] = held(sh, q) ? 0.0 : gpose[6 * (size_t)s0 + q];
-                for (int l = tid; l < sh.w.L; l += blockDim.x)
-                    for (int i = 0; i < NT_FROZEN; ++i) lsc[(size_t)(sh.w.lm0 + l) * NT_LM_STRIDE + i] = 0.0;
-                __syncthreads();
-                rel = nt_solve_exact(sh, nt, d, S64, dsm, lsc, maxit, tol, &iters, &neg);
-                if (neg) status = 2;
-                // the theta pass moves the state along the solution x
-                for (int q = tid; q < n; q += blockDim.x) sh.dx[q] = sh.dmp[q];
-                for (int l = tid; l < sh.w.L; l += blockDim.x) {
-                    double* sc = lsc + (size_t)(sh.w.lm0 + l) * NT_LM_STRIDE;
-                    for (int i = 0; i < 3; ++i) sc[NT_P + i] = sc[NT_X + i];
+            // implicit adjoint: H x = dL/dx (poses from gpose, landmarks 0), then -(d2C / dtheta dx) x.  The exact
+            // reduced system solves it directly (nt_adjoint_direct); where that is not positive definite, conjugate
+            // gradients preconditioned with the Gauss-Newton system
+            if (!nt_adjoint_direct(sh, nt, d, dsm, lsc, gpose + 6 * (size_t)s0, tol, &rel, &iters)) {
+                slot_geo(sh, sh.Rwb, sh.pwb);
+                if (nt_gn_factor(sh, d, S64, wl64, lsc)) status = 1;
+                else {
+                    nt_grad(sh, nt, d, dsm, lsc, false);       // the gradient; constant landmarks as flagged
+                    for (int q = tid; q < n; q += blockDim.x)
+                        sh.rhs[q] = held(sh, q) ? 0.0 : gpose[6 * (size_t)s0 + q];
+                    for (int l = tid; l < sh.w.L; l += blockDim.x)
+                        for (int i = 0; i < NT_FROZEN; ++i) lsc[(size_t)(sh.w.lm0 + l) * NT_LM_STRIDE + i] = 0.0;
+                    __syncthreads();
+                    rel = nt_solve_exact(sh, nt, d, S64, dsm, lsc, maxit, tol, &iters, &neg);
+                    if (neg) status = 2;
+                    for (int l = tid; l < sh.w.L; l += blockDim.x) {
+                        double* sc = lsc + (size_t)(sh.w.lm0 + l) * NT_LM_STRIDE;
+                        for (int i = 0; i < 3; ++i) sc[NT_P + i] = sc[NT_X + i];
+                    }
+                    __syncthreads();
                 }
+            }
+            if (status != 1) {
+                // the theta pass moves the state along the solution x (poses sh.dmp, landmarks NT_P)
+                for (int q = tid; q < n; q += blockDim.x) { sh.dx[q] = sh.dmp[q]; nt.gp[q] = 0.0; nt.hp[q] = 0.0; }
+                if (tid < NT_THETA) nt.th[tid] = 0.0;
                 __syncthreads();
                 SlotGeo<Dual>* Gd = (SlotGeo<Dual>*)(dsm + ba_off_x(n));
+                slot_geo(sh, sh.Rwb, sh.pwb);
                 slot_geo_dual(sh, sh.dx, *Gd);
                 pass_dual(sh, nt, d, *Gd, NT_MODE_THETA, lsc, gisig, gz);
                 __syncthreads();
