@@ -47,9 +47,10 @@ def _huber(en):
 
 
 class Window:
-    """A window's arrays as float64 torch tensors (a synth_ba.Window or anything with its fields)."""
+    """A window's arrays as float64 torch tensors (a synth_ba.Window or anything with its fields).  const (optional,
+    bool per landmark): landmarks held constant (not variables) whose rows stay in the cost."""
 
-    def __init__(self, w, hold=0):
+    def __init__(self, w, hold=0, const=None):
         g = lambda k: torch.as_tensor(np.array(getattr(w, k), np.float64))
         self.R0, self.p0 = g("Rwb"), g("pwb")
         self.Rbc, self.pbc = g("Rbc"), g("pbc")
@@ -68,7 +69,7 @@ class Window:
         self.prior = torch.as_tensor(mask & (np.asarray(w.rho_isig) > 0))
         has = np.zeros(self.L, bool)
         has[lm_of[valid]] = True
-        self.lvar = torch.as_tensor(mask & has)
+        self.lvar = torch.as_tensor(mask & has & (~np.asarray(const, bool) if const is not None else True))
         self.pvar = torch.as_tensor(np.array([s != hold for s in range(self.P)]))
         self.theta0 = torch.tensor([w.fx, w.fy, w.cx, w.cy, w.B, 0, 0, 0, 0, 0, 0], dtype=f64)
         self.isig0 = g("ob_isig")
@@ -160,6 +161,44 @@ def implicit_grad(win, theta, isig, z, dLdp):
     _, vjp = torch.func.vjp(gx, theta, isig, z)
     gt, gs, gz = vjp(lam_)
     return (-gt).numpy(), (-gs).numpy(), (-gz).numpy()
+
+
+def implicit_grad_schur(win, theta, isig, z, dLdp):
+    """implicit_grad for windows too large for a dense Hessian (thousands of landmarks).  The Hessian's pose columns
+    come from one Hessian-vector product per pose variable; its landmark blocks are 3x3 and independent, so the
+    product along component i of every landmark at once gives column i of all of them.  H lam = v (v on the poses
+    only) is solved through the Schur complement on the poses: lam_p = S^-1 v_p with S = Hpp - Hpl Hll^-1 Hlp, then
+    lam_l = -Hll^-1 Hlp lam_p.  -> as implicit_grad, and the largest |gradient| over the variables at the state."""
+    n = win.n_x()
+    npv = 6 * int(win.pvar.sum())
+    nl = (n - npv) // 3
+    x = torch.zeros(n, dtype=f64)
+    gfun = torch.func.grad(lambda xx: win.cost(xx, theta, isig, z))
+    g = gfun(x)
+    hvp = lambda v: torch.func.jvp(gfun, (x,), (v,))[1]
+    Hp = torch.func.vmap(hvp)(torch.eye(n, dtype=f64)[:npv])          # row j = H e_j (pose variable j)
+    Hpp = Hp[:, :npv]
+    Hlp = Hp[:, npv:].T.reshape(nl, 3, npv)                          # landmark rows, pose columns
+    Hll = torch.zeros(nl, 3, 3, dtype=f64)
+    for i in range(3):
+        v = torch.zeros(n, dtype=f64)
+        v[npv + i::3] = 1.0
+        Hll[:, :, i] = hvp(v)[npv:].reshape(nl, 3)
+    Hll = 0.5 * (Hll + Hll.transpose(1, 2))
+    T = torch.linalg.solve(Hll, Hlp)                                 # Hll^-1 Hlp per landmark
+    S = Hpp - torch.einsum("lip,liq->pq", Hlp, T)
+    S = 0.5 * (S + S.T)
+    vp = torch.zeros(npv, dtype=f64)
+    piv = torch.nonzero(win.pvar)[:, 0]
+    for j, s in enumerate(piv.tolist()):
+        vp[6 * j + 3:6 * j + 6] = torch.as_tensor(np.asarray(dLdp[s], np.float64))
+    lam_p = torch.linalg.solve(S, vp)
+    lam_l = -torch.einsum("lip,p->li", T, lam_p).reshape(-1)
+    lam = torch.cat([lam_p, lam_l])
+    gx = lambda th, si, zz: torch.func.grad(lambda xx: win.cost(xx, th, si, zz))(x)
+    _, vjp = torch.func.vjp(gx, theta, isig, z)
+    gt, gs, gz = vjp(lam)
+    return (-gt).numpy(), (-gs).numpy(), (-gz).numpy(), float(g.abs().max())
 
 
 def fd_grad(start, theta, isig, z, loss, step=1e-6, idx=None):
