@@ -454,36 +454,46 @@ __device__ void pass_build(BaShared& sh, const XcbBaWindows& d, const SlotGeo<T>
             if (ok) acc -= wl.Hlp[a][i] * HiB[0] + wl.Hlp[a][6 + i] * HiB[1] + wl.Hlp[a][12 + i] * HiB[2];
             atomicAdd(&gb[6 * s + i], acc);
         }
-        // reduced system, lower triangle: block (ts[a], ts[b]) with a >= b (ts ascending)
+        // reduced system, lower triangle: block (ts[a], ts[b]) with a >= b (ts ascending).  A lane per (pair, row i)
+        // takes the row's entries, so the pair decode, the row's Jacobian entries and its Hlp column are read once per
+        // row instead of once per entry
         const int npair = nt * (nt + 1) / 2;
-        for (int q = lane; q < npair * 36; q += 32) {
-            const int pr = q / 36, e = q % 36, i = e / 6, j = e % 6;
+        for (int q = lane; q < npair * 6; q += 32) {
+            const int pr = q / 6, i = q % 6;
             int a = (int)((sqrtf(8.0f * pr + 1.0f) - 1.0f) * 0.5f);
             while (a * (a + 1) / 2 > pr) --a;
             while ((a + 1) * (a + 2) / 2 <= pr) ++a;
             const int b = pr - a * (a + 1) / 2;
-            if (a == b && j > i) continue;
             const int sa = wl.ts[a], sb = wl.ts[b];
-            T acc = 0;
+            const int jn = a == b ? i + 1 : 6;
+            T acc[6];
+#pragma unroll
+            for (int j = 0; j < 6; ++j) acc[j] = 0;
             // pose-pose: the same slot, or the (target, host) pair of the target's observations
-            if (a == b) {
-                const int off = sa == h ? OB_JH : OB_JT;
-                for (unsigned m = wl.om[a]; m; m &= m - 1) {
-                    const T* ob = wl.ob[__ffs(m) - 1];
-                    acc += ob[OB_W] * (obj(ob, off, 0, i) * obj(ob, off, 0, j) + obj(ob, off, 1, i) * obj(ob, off, 1, j));
-                }
-            } else if (sa == h || sb == h) {
-                const int at = sa == h ? b : a;           // the target slot's index
+            const bool pp = a == b || sa == h || sb == h;
+            if (pp) {
+                const int at = a == b ? a : (sa == h ? b : a);    // the observations: the slot's, or the target's
                 const int offa = sa == h ? OB_JH : OB_JT, offb = sb == h ? OB_JH : OB_JT;
                 for (unsigned m = wl.om[at]; m; m &= m - 1) {
                     const T* ob = wl.ob[__ffs(m) - 1];
-                    acc += ob[OB_W] * (obj(ob, offa, 0, i) * obj(ob, offb, 0, j) + obj(ob, offa, 1, i) * obj(ob, offb, 1, j));
+                    const T ri0 = obj(ob, offa, 0, i), ri1 = obj(ob, offa, 1, i), wt = ob[OB_W];
+#pragma unroll
+                    for (int j = 0; j < 6; ++j) acc[j] += wt * (ri0 * obj(ob, offb, 0, j) + ri1 * obj(ob, offb, 1, j));
                 }
             }
-            if (ok) acc -= wl.Hlp[a][i] * wl.Tb[b][j] + wl.Hlp[a][6 + i] * wl.Tb[b][6 + j] + wl.Hlp[a][12 + i] * wl.Tb[b][12 + j];
-            const int r = 6 * sa + i, c = 6 * sb + j;
-            if (PACKED) atomicAdd(&S[tri(r, c)], acc);
-            else atomicAdd(&S[r * n + c], acc);
+            if (ok) {
+                const T h0 = wl.Hlp[a][i], h1 = wl.Hlp[a][6 + i], h2 = wl.Hlp[a][12 + i];
+#pragma unroll
+                for (int j = 0; j < 6; ++j) acc[j] -= h0 * wl.Tb[b][j] + h1 * wl.Tb[b][6 + j] + h2 * wl.Tb[b][12 + j];
+            }
+            const int r = 6 * sa + i;
+#pragma unroll
+            for (int j = 0; j < 6; ++j) {
+                if (j >= jn) break;
+                const int c = 6 * sb + j;
+                if (PACKED) atomicAdd(&S[tri(r, c)], acc[j]);
+                else atomicAdd(&S[r * n + c], acc[j]);
+            }
         }
         __syncwarp();
     }
@@ -584,69 +594,95 @@ __device__ void pass_refine(BaShared& sh, const XcbBaWindows& d, WarpLm<double>*
 }
 
 // ------------------------------------------------------------------ pass C: back-substitution (FP64) -> trial lmp
+// one landmark re-linearised by the whole warp (no record, or none kept): dl = -Hll^-1 (bl + sum_a Hlp_a dx_{slot a})
+__device__ void backsub_relin(BaShared& sh, const XcbBaWindows& d, WarpLm<double>& wl, int l, double* lmp_trial,
+                              const double* frz)
+{
+    const int lane = threadIdx.x & 31;
+    const int gl = sh.w.lm0 + l;
+    double Hll[9], bl[3], c_dummy = 0.0;
+    int nt;
+    const bool ok = lin_landmark<double>(sh, d, sh.g64, l, sh.lam, d.lmp, wl, Hll, bl, &nt, &c_dummy) &&
+                    !lm_const(frz, gl);
+    if (lane < 3) {
+        double out = d.lmp[3 * gl + lane];
+        if (ok) {
+            double Hi[9];
+            inv3<double>(Hll, Hi);
+            double v[3] = {bl[0], bl[1], bl[2]};
+            for (int a = 0; a < nt; ++a) {
+                const int s = wl.ts[a];
+                for (int i = 0; i < 3; ++i) {
+                    double acc = 0.0;
+                    for (int j = 0; j < 6; ++j) acc += wl.Hlp[a][i * 6 + j] * sh.dx[6 * s + j];
+                    v[i] += acc;
+                }
+            }
+            double dl[3];
+            for (int i = 0; i < 3; ++i) dl[i] = -(Hi[i * 3] * v[0] + Hi[i * 3 + 1] * v[1] + Hi[i * 3 + 2] * v[2]);
+            const double r = d.lmp[3 * gl + 2] + dl[2];
+            if (r > 1e-9 && isfinite(r)) out = lane == 2 ? r : d.lmp[3 * gl + lane] + dl[lane];
+        }
+        lmp_trial[3 * gl + lane] = out;
+    }
+    __syncwarp();
+}
+
 __device__ void pass_backsub(BaShared& sh, const XcbBaWindows& d, WarpLm<double>* wls, double* lmp_trial,
                              const double* frz = nullptr, const double* bsc = nullptr)
 {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     WarpLm<double>& wl = wls[wid];
-    double c_dummy = 0.0;
-    for (int l = sh.lb + wid; l < sh.le; l += BA_WARPS) {
-        const int gl = sh.w.lm0 + l;
-        if (!d.lm_mask[gl]) {
-            if (lane < 3) lmp_trial[3 * gl + lane] = d.lmp[3 * gl + lane];
-            continue;
-        }
-        if (bsc) {
-            // the build's record: dl = -(Hll^-1 bl + sum_a (Hll^-1 Hlp_a) dx_{slot a})
-            const double* rec = bsc + (size_t)gl * BA_BSC;
-            const int nt = (int)rec[0];
-            if (nt >= -2 && nt != -1) {
-                if (lane < 3) {
-                    double out = d.lmp[3 * gl + lane];
-                    if (nt >= 0) {
-                        double v = rec[1 + lane];
-                        for (int a = 0; a < nt; ++a) {
-                            const int sl = (int)rec[4 + a];
-                            const double* tb = rec + 10 + 18 * a + 6 * lane;
-#pragma unroll
-                            for (int j = 0; j < 6; ++j) v += tb[j] * sh.dx[6 * sl + j];
-                        }
-                        const double dl2 = __shfl_sync(0x7u, -v, 2);
-                        const double r = d.lmp[3 * gl + 2] + dl2;
-                        if (r > 1e-9 && isfinite(r)) out = lane == 2 ? r : d.lmp[3 * gl + lane] - v;
-                    }
-                    lmp_trial[3 * gl + lane] = out;
-                }
-                __syncwarp();
+    if (!bsc) {
+        for (int l = sh.lb + wid; l < sh.le; l += BA_WARPS) {
+            const int gl = sh.w.lm0 + l;
+            if (!d.lm_mask[gl]) {
+                if (lane < 3) lmp_trial[3 * gl + lane] = d.lmp[3 * gl + lane];
                 continue;
             }
+            backsub_relin(sh, d, wl, l, lmp_trial, frz);
         }
-        double Hll[9], bl[3];
-        int nt;
-        const bool ok = lin_landmark<double>(sh, d, sh.g64, l, sh.lam, d.lmp, wl, Hll, bl, &nt, &c_dummy) &&
-                        !lm_const(frz, gl);
-        if (lane < 3) {
-            double out = d.lmp[3 * gl + lane];
-            if (ok) {
-                double Hi[9];
-                inv3<double>(Hll, Hi);
-                double v[3] = {bl[0], bl[1], bl[2]};
-                for (int a = 0; a < nt; ++a) {
-                    const int s = wl.ts[a];
-                    for (int i = 0; i < 3; ++i) {
-                        double acc = 0.0;
-                        for (int j = 0; j < 6; ++j) acc += wl.Hlp[a][i * 6 + j] * sh.dx[6 * s + j];
-                        v[i] += acc;
+        return;
+    }
+    // the build's records: dl = -(Hll^-1 bl + sum_a (Hll^-1 Hlp_a) dx_{slot a}).  Ten landmarks per warp, a lane per
+    // landmark component, so that the record loads of ten landmarks are in flight together; a landmark without a
+    // record (more than BA_BSC_NT touched slots) is re-linearised by the whole warp afterwards
+    const int sub = lane / 3, comp = lane - 3 * sub;
+    for (int l0 = sh.lb + wid * 10; l0 < sh.le; l0 += BA_WARPS * 10) {
+        const int l = l0 + sub;
+        const bool mine = lane < 30 && l < sh.le;
+        const int gl = sh.w.lm0 + (mine ? l : l0);
+        bool masked = false;
+        int nt = -2;
+        double v = 0.0;
+        if (mine) {
+            masked = !d.lm_mask[gl];
+            if (!masked) {
+                const double* rec = bsc + (size_t)gl * BA_BSC;
+                nt = (int)rec[0];
+                if (nt >= 0) {
+                    v = rec[1 + comp];
+                    for (int a = 0; a < nt; ++a) {
+                        const int sl = (int)rec[4 + a];
+                        const double* tb = rec + 10 + 18 * a + 6 * comp;
+#pragma unroll
+                        for (int j = 0; j < 6; ++j) v += tb[j] * sh.dx[6 * sl + j];
                     }
                 }
-                double dl[3];
-                for (int i = 0; i < 3; ++i) dl[i] = -(Hi[i * 3] * v[0] + Hi[i * 3 + 1] * v[1] + Hi[i * 3 + 2] * v[2]);
-                const double r = d.lmp[3 * gl + 2] + dl[2];
-                if (r > 1e-9 && isfinite(r)) out = lane == 2 ? r : d.lmp[3 * gl + lane] + dl[lane];
             }
-            lmp_trial[3 * gl + lane] = out;
         }
-        __syncwarp();
+        const double dl2 = __shfl_sync(0xffffffffu, -v, min(3 * sub + 2, 31));
+        const bool redo = mine && !masked && (nt == -1 || nt < -2);
+        if (mine && !redo) {
+            double out = d.lmp[3 * gl + comp];
+            if (!masked && nt >= 0) {
+                const double r = d.lmp[3 * gl + 2] + dl2;
+                if (r > 1e-9 && isfinite(r)) out = comp == 2 ? r : d.lmp[3 * gl + comp] - v;
+            }
+            lmp_trial[3 * gl + comp] = out;
+        }
+        for (unsigned m = __ballot_sync(0xffffffffu, redo && comp == 0); m; m &= m - 1)
+            backsub_relin(sh, d, wl, l0 + (__ffs(m) - 1) / 3, lmp_trial, frz);
     }
 }
 
