@@ -1098,6 +1098,7 @@ def run_ba(args, dev, stream, rank, ws_world, cpu=True):
     if not args.no_ba_large:
         out["large_windows"] = run_ba_large(args, dev, stream, ws_world, rank)
         out["adjoint"] = run_adjoint(args, dev, stream, ws_world, rank)
+        out["large_windows"]["adjoint"] = run_adjoint(args, dev, stream, ws_world, rank, large=True)
     return out
 
 
@@ -1158,23 +1159,24 @@ def run_ba_large(args, dev, stream, ws_world, rank):
 ADJ_NEWTON = 30
 
 
-def run_adjoint(args, dev, stream, ws_world, rank):
+def run_adjoint(args, dev, stream, ws_world, rank, large=False):
     """Differentiable BA: 64 windows of 10 keyframes and 2,000 landmarks; forward = 20 LM iterations, 20 LM iterations
     with the landmarks the LM cannot move held constant, up to 30 landmark-eliminated Newton steps on the exact Hessian;
     loss = sum of squared translation errors against the ground truth, backward = the implicit adjoint
-    (gradients to fx, fy, cx, cy, baseline, left-right extrinsic, per-row weights and pixels)."""
+    (gradients to fx, fy, cx, cy, baseline, left-right extrinsic, per-row weights and pixels).  large: the same pass on
+    the large stress case's windows (32 x 20 keyframes, 6,000 landmarks, 3-15 observing keyframes, 10 % outliers)."""
     import torch
     from xclean_b200.backend import synth_ba as S
     from xclean_b200.backend.adjoint import BAAdjoint, inputs_of
     from xclean_b200.backend.ba import BatchSolver
-    wins = S.config3_windows(64, seed=3 + rank)
+    wins = S.config4_windows(args.large_windows, seed=4 + rank) if large else S.config3_windows(64, seed=3 + rank)
     with torch.cuda.stream(stream):
         solver = BatchSolver(wins, dev, hold=0)
         ptrue = torch.as_tensor(np.concatenate([w.pwb_true for w in wins]), device=dev)
     torch.cuda.synchronize()
     fwd, bwd = [], []
     with torch.cuda.stream(stream):
-        n_warm, n_timed = 1, min(2, args.steps)          # bounded: a step is seconds long
+        n_warm, n_timed = 1, (1 if large else min(2, args.steps))      # bounded: a step is seconds long
         for it in range(n_warm + n_timed):
             inp = inputs_of(solver)
             ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
@@ -1195,7 +1197,9 @@ def run_adjoint(args, dev, stream, ws_world, rank):
             "windows_stationary": int(((st[:, 3] == 0) & (st[:, 2] < 1e-6)).sum()),
             "final_gradient_max_median": float(np.median(st[:, 2])),
             "final_gradient_max_quartiles": [float(x) for x in np.percentile(st[:, 2], [25, 75])],
-            "config": {"workload": "64 windows x (10 keyframes, 2000 landmarks, 2-6 obs, 5%% outliers); forward 20 LM "
+            "config": {"workload": ("%d windows x (20 keyframes, 6000 landmarks, 3-15 obs, 10%% outliers)" % len(wins)
+                                    if large else "64 windows x (10 keyframes, 2000 landmarks, 2-6 obs, 5% outliers)") +
+                                   "; forward 20 LM "
                                    "iterations, 20 LM iterations with the landmarks the LM cannot move held "
                                    "constant, up to %d landmark-eliminated Newton steps; implicit adjoint of "
                                    "sum |t - t_gt|^2 by the exact reduced system" % ADJ_NEWTON}}
