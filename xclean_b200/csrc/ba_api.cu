@@ -150,7 +150,7 @@ extern "C" int xcb_ba_newton_windows_dev(const xcb_ba_windows* w, int max_slots,
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         grid = sms;
     }
-    if (grid > w->nw) grid = w->nw;
+    // at most `grid` CTAs in all, up to 4 per window (a thread-block cluster) when there are fewer windows than CTAs
     e = xcb_launch_ba_newton(*w, max_slots, mode, steps, maxit, tol, gpose, gtheta, gisig, gz, stats, lsc, counter,
                              grid, st, lsc_doubles, scopy);
     if (e != cudaSuccess) return ba_fail(XCB_ERR_CUDA, cudaGetErrorString(e));

@@ -23,6 +23,8 @@
 #include "common.cuh"
 #include "ba_kernels.h"
 #include "ba_tc.cuh"
+#include <cooperative_groups.h>
+namespace cg = cooperative_groups;
 
 #define BA_WARPS 10
 #define BA_THREADS (BA_WARPS * 32)
@@ -1211,7 +1213,52 @@ struct NtShared {
     double hp[BA_MAXN];         // dual accumulators (H p)
     double th[NT_THETA];
     double red2;
+    double cred;                // this CTA's partial of a cluster reduction
 };
+
+// ---------------------------------------------------------------------------------------------------------------------
+// Reductions over the CTAs of a thread-block cluster (distributed shared memory).  The Newton kernel gives each window a
+// cluster whose CTAs take slices of the window's landmarks; these sums run in rank order, so every CTA holds the same
+// bits afterwards and every CTA takes the same branches.  Every thread of every CTA calls them, with a block-uniform
+// partial; with one CTA per cluster they return at once.
+__device__ double cl_reduce(NtShared& nt, double v, bool mx)
+{
+    cg::cluster_group cl = cg::this_cluster();
+    const unsigned C = cl.num_blocks();
+    if (C == 1) return v;
+    if (threadIdx.x == 0) nt.cred = v;
+    cl.sync();
+    double s = 0.0;
+    for (unsigned r = 0; r < C; ++r) {
+        const double x = *cl.map_shared_rank(&nt.cred, r);
+        s = mx ? (r == 0 ? x : fmax(s, x)) : s + x;
+    }
+    cl.sync();
+    return s;
+}
+
+// a[0, len) in shared memory summed over the cluster's CTAs into every CTA: each CTA totals its slice in rank order,
+// then copies the others' slices from their owners
+__device__ void cl_sum_array(double* a, int len)
+{
+    cg::cluster_group cl = cg::this_cluster();
+    const int C = (int)cl.num_blocks(), r = (int)cl.block_rank();
+    if (C == 1) return;
+    cl.sync();
+    const int b0 = (int)((long long)len * r / C), b1 = (int)((long long)len * (r + 1) / C);
+    for (int q = b0 + threadIdx.x; q < b1; q += blockDim.x) {
+        double t = 0.0;
+        for (int k = 0; k < C; ++k) t += *cl.map_shared_rank(a + q, k);
+        a[q] = t;
+    }
+    cl.sync();
+    for (int q = threadIdx.x; q < len; q += blockDim.x) {
+        int o = 0;
+        while (o + 1 < C && q >= (int)((long long)len * (o + 1) / C)) ++o;
+        if (o != r) a[q] = *cl.map_shared_rank(a + q, o);
+    }
+    cl.sync();
+}
 
 __device__ __forceinline__ bool held(const BaShared& sh, int q) { return sh.w.hold >= 0 && q / 6 == sh.w.hold; }
 
@@ -1314,7 +1361,7 @@ __device__ void pass_dual(BaShared& sh, NtShared& nt, const XcbBaWindows& d, con
                           double* lsc, double* gisig, double* gz, double mu = 0.0, bool upd = false)
 {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    for (int l = wid; l < sh.w.L; l += BA_WARPS) {
+    for (int l = sh.lb + wid; l < sh.le; l += BA_WARPS) {
         const int gl = sh.w.lm0 + l;
         if (!d.lm_mask[gl]) continue;
         const int h = d.lm_host[gl];
@@ -1525,14 +1572,15 @@ __device__ int nt_gn_factor(BaShared& sh, const XcbBaWindows& d, double* S64, Wa
 }
 
 // sum over the window's variables of a_p b_p (poses, the held slot excluded) + a_l b_l (scratch offsets oa, ob)
+// (poses = false: the landmark part only; the landmarks of this CTA's slice lb..le)
 __device__ double nt_dot(BaShared& sh, NtShared& nt, const double* pa, const double* pb, const double* lsc, int oa,
-                         int ob)
+                         int ob, bool poses = true)
 {
     const int tid = threadIdx.x, n = sh.w.n;
     double s = 0.0;
-    for (int q = tid; q < n; q += blockDim.x)
+    for (int q = tid; q < n && poses; q += blockDim.x)
         if (!held(sh, q)) s += pa[q] * pb[q];
-    for (int l = tid; l < sh.w.L; l += blockDim.x) {
+    for (int l = sh.lb + tid; l < sh.le; l += blockDim.x) {
         const double* sc = lsc + (size_t)(sh.w.lm0 + l) * NT_LM_STRIDE;
         s += sc[oa] * sc[ob] + sc[oa + 1] * sc[ob + 1] + sc[oa + 2] * sc[ob + 2];
     }
@@ -1664,18 +1712,20 @@ __device__ double nt_solve_exact(BaShared& sh, NtShared& nt, const XcbBaWindows&
 }
 
 // the exact gradient at the current state: -gradient -> sh.rhs (poses, held slot 0) and NT_B (landmarks)
+// (the landmarks of this CTA's slice; cl: the pose gradient summed over the cluster)
 __device__ void nt_grad(BaShared& sh, NtShared& nt, const XcbBaWindows& d, unsigned char* dsm, double* lsc,
-                        bool upd)
+                        bool upd, bool cl = false)
 {
     const int n = sh.w.n, tid = threadIdx.x;
     SlotGeo<Dual>* Gd = (SlotGeo<Dual>*)(dsm + ba_off_x(n));
     for (int q = tid; q < n; q += blockDim.x) { sh.dx[q] = 0.0; nt.gp[q] = 0.0; nt.hp[q] = 0.0; }
-    for (int l = tid; l < sh.w.L; l += blockDim.x)
+    for (int l = sh.lb + tid; l < sh.le; l += blockDim.x)
         for (int i = 0; i < NT_FROZEN; ++i) lsc[(size_t)(sh.w.lm0 + l) * NT_LM_STRIDE + i] = 0.0;
     __syncthreads();
     slot_geo_dual(sh, sh.dx, *Gd);
     pass_dual(sh, nt, d, *Gd, NT_MODE_GRAD, lsc, nullptr, nullptr, 0.0, upd);
     __syncthreads();
+    if (cl) cl_sum_array(nt.gp, n);
     for (int q = tid; q < n; q += blockDim.x) sh.rhs[q] = held(sh, q) ? 0.0 : -nt.gp[q];
     __syncthreads();
 }
@@ -1686,7 +1736,7 @@ __device__ double nt_gmax(BaShared& sh, NtShared& nt, const double* lsc)
     const int tid = threadIdx.x, n = sh.w.n;
     double gm = 0.0;
     for (int q = tid; q < n; q += blockDim.x) gm = fmax(gm, fabs(sh.rhs[q]));
-    for (int l = tid; l < sh.w.L; l += blockDim.x)
+    for (int l = sh.lb + tid; l < sh.le; l += blockDim.x)
         for (int i = 0; i < 3; ++i) gm = fmax(gm, fabs(lsc[(size_t)(sh.w.lm0 + l) * NT_LM_STRIDE + NT_B + i]));
     for (int o = 16; o > 0; o >>= 1) gm = fmax(gm, __shfl_xor_sync(0xffffffffu, gm, o));
     __syncthreads();
@@ -1715,7 +1765,8 @@ __device__ double nt_gmax(BaShared& sh, NtShared& nt, const double* lsc)
 // =====================================================================================================================
 #define NT_INNER 32             // Newton iterations per landmark in (1)
 #define NT_RETRY 10             // damping increases per step
-#define NT_SC (BA_MAXN * (BA_MAXN + 1) / 2)     // doubles per window of the reduced-system copy
+#define NT_SC (BA_MAXN * (BA_MAXN + 1) / 2)     // doubles of one reduced-system copy
+#define NT_CL_MAX 4             // CTAs per window (thread-block cluster); each keeps its own copy
 #define NT_RHO_INF 1e-7         // a landmark whose inverse depth falls below this has its minimum at infinity
 // polish records in the landmark scratch (the conjugate-gradient slots are free during the polish)
 #define NR_HI 0                 // Hll^-1, symmetric: 00 01 02 11 12 22; entry 0 is 0 for a landmark held this step
@@ -2260,7 +2311,7 @@ __device__ void pass_adj_y(BaShared& sh, const XcbBaWindows& d, const SlotGeo<Du
 // restore every landmark the last pass_lstep saved
 __device__ void pass_lrestore(BaShared& sh, const XcbBaWindows& d, const double* lsc)
 {
-    for (int l = threadIdx.x; l < sh.w.L; l += blockDim.x) {
+    for (int l = sh.lb + threadIdx.x; l < sh.le; l += blockDim.x) {
         const int gl = sh.w.lm0 + l;
         if (!d.lm_mask[gl] || (unsigned)d.lm_host[gl] >= (unsigned)sh.w.P) continue;
         const double* sc = lsc + (size_t)gl * NT_LM_STRIDE;
@@ -2311,7 +2362,11 @@ __device__ double nt_xsystem(BaShared& sh, NtShared& nt, const XcbBaWindows& d, 
         __syncthreads();
     }
     pass_xbuild(sh, nt, d, *G0, S, wl64, lsc, upd);
-    const double gml = block_max_red(sh);
+    double gml = block_max_red(sh);
+    // each CTA of the window's cluster built the terms of its landmark slice
+    cl_sum_array(S, ntri);
+    cl_sum_array(nt.gp, n);
+    gml = cl_reduce(nt, gml, true);
     const int hs = sh.w.hold;
     if (hs >= 0 && hs < P) {
         for (int q = tid; q < 6 * n; q += blockDim.x) {
@@ -2348,7 +2403,7 @@ __device__ int nt_polish(BaShared& sh, NtShared& nt, const XcbBaWindows& d, unsi
     const int ntri = n * (n + 1) / 2;
     nt_geo(sh, *G0);
     pass_inner(sh, d, *G0, lsc);
-    double c0 = block_sum_red(sh);
+    double c0 = cl_reduce(nt, block_sum_red(sh), false);
     double mu = 0.0, gm_prev = 0.0;
     int st = 0, status = 0, stall = 0;
     bool tiny = false;
@@ -2401,7 +2456,7 @@ __device__ int nt_polish(BaShared& sh, NtShared& nt, const XcbBaWindows& d, unsi
             __syncthreads();
             nt_geo(sh, *G0);
             pass_inner(sh, d, *G0, lsc);
-            const double c1 = block_sum_red(sh);
+            const double c1 = cl_reduce(nt, block_sum_red(sh), false);
             // the cost is a float64 sum of ~1e4 terms: below ~1e-10 of it a decrease is rounding noise, so a step whose
             // predicted decrease is that small is kept unless the cost visibly rose
             const double noise = 1e-10 * fabs(c0);
@@ -2466,13 +2521,16 @@ __device__ bool nt_adjoint_direct(BaShared& sh, NtShared& nt, const XcbBaWindows
         slot_geo_dual(sh, sh.dx, *Gd);
         pass_dual(sh, nt, d, *Gd, NT_MODE_HV, lsc, nullptr, nullptr);
         __syncthreads();
+        cl_sum_array(nt.hp, n);
         for (int q = tid; q < n; q += blockDim.x) sh.g[q] = held(sh, q) ? 0.0 : sh.rhs[q] - nt.hp[q];
-        for (int l = tid; l < sh.w.L; l += blockDim.x) {
+        for (int l = sh.lb + tid; l < sh.le; l += blockDim.x) {
             double* sc = lsc + (size_t)(sh.w.lm0 + l) * NT_LM_STRIDE;
             for (int i = 0; i < 3; ++i) sc[NT_Z + i] = -sc[NT_HP + i];
         }
         __syncthreads();
-        *rel = sqrt(nt_dot(sh, nt, sh.g, sh.g, lsc, NT_Z, NT_Z)) / bn;
+        // the pose part counted by the cluster's rank 0, the landmark part by every CTA for its slice
+        const bool r0 = cg::this_cluster().block_rank() == 0;
+        *rel = sqrt(cl_reduce(nt, nt_dot(sh, nt, sh.g, sh.g, lsc, NT_Z, NT_Z, r0), false)) / bn;
         if (!(*rel > tol) || it >= 2) break;
         ++it;
         // dx_p = S^-1 (r_p - sum Hpl Hll^-1 r_l), dx_l = Hll^-1 (r_l - Hlp dx_p)
@@ -2480,6 +2538,7 @@ __device__ bool nt_adjoint_direct(BaShared& sh, NtShared& nt, const XcbBaWindows
         __syncthreads();
         pass_adj_y(sh, d, *G0, lsc, nt.gp);
         __syncthreads();
+        cl_sum_array(nt.gp, n);
         for (int q = tid; q < n; q += blockDim.x) sh.y[q] = held(sh, q) ? 0.0 : sh.g[q] - nt.gp[q];
         __syncthreads();
         chol_solve(S, n, sh.y);
@@ -2517,8 +2576,18 @@ __global__ void __launch_bounds__(BA_THREADS, 1) k_ba_newton(XcbBaWindows d, int
             for (int w = tid; w < d.nw; w += blockDim.x) stats[4 * w + 3] = XCB_BA_STATUS_SCRATCH;
         return;
     }
+    // a window per thread-block cluster: its CTAs take slices of the window's landmarks and reduce their sums through
+    // distributed shared memory (cl_reduce, cl_sum_array); poses, reduced systems and decisions are the same bits on
+    // every CTA, so every CTA takes the same branches
+    cg::cluster_group cl = cg::this_cluster();
+    const int crank = (int)cl.block_rank(), csize = (int)cl.num_blocks();
     for (;;) {
-        if (tid == 0) sh.win = atomicAdd(counter, 1);
+        if (crank == 0 && tid == 0) sh.win = atomicAdd(counter, 1);
+        if (csize > 1) {
+            cl.sync();
+            if (crank != 0 && tid == 0) sh.win = *cl.map_shared_rank(&sh.win, 0);
+            cl.sync();
+        }
         __syncthreads();
         const int wi = sh.win;
         if (wi >= d.nw) break;
@@ -2526,7 +2595,8 @@ __global__ void __launch_bounds__(BA_THREADS, 1) k_ba_newton(XcbBaWindows d, int
         if (tid == 0) {
             BaWin& W = sh.w;
             W.P = d.P[w]; W.L = d.L[w]; W.n = 6 * W.P; W.hold = d.hold ? d.hold[w] : -1;
-            sh.lb = 0; sh.le = W.L;
+            sh.lb = (int)((long long)W.L * crank / csize);
+            sh.le = (int)((long long)W.L * (crank + 1) / csize);
             W.lm0 = d.lm_off[w]; W.s0 = d.slot_off[w];
             W.fx = d.cam[6 * w]; W.fy = d.cam[6 * w + 1]; W.cx = d.cam[6 * w + 2]; W.cy = d.cam[6 * w + 3];
             W.B = d.cam[6 * w + 4]; W.hk = d.cam[6 * w + 5];
@@ -2542,7 +2612,7 @@ __global__ void __launch_bounds__(BA_THREADS, 1) k_ba_newton(XcbBaWindows d, int
         __syncthreads();
         const int P = sh.w.P, n = sh.w.n, s0 = sh.w.s0;
         if (P > BA_MAXP || P < 1 || has_prior(d, w)) {
-            if (tid == 0) stats[4 * w + 3] = has_prior(d, w) ? XCB_BA_STATUS_PRIOR : -1.0;
+            if (tid == 0 && crank == 0) stats[4 * w + 3] = has_prior(d, w) ? XCB_BA_STATUS_PRIOR : -1.0;
             __syncthreads();
             continue;
         }
@@ -2560,39 +2630,50 @@ __global__ void __launch_bounds__(BA_THREADS, 1) k_ba_newton(XcbBaWindows d, int
             int taken = 0;
             double mu = 0.0;
             if (steps > 0)
-                status = nt_polish(sh, nt, d, dsm, lsc, scopy + (size_t)w * NT_SC, steps, upd, &taken, &mu);
+                status = nt_polish(sh, nt, d, dsm, lsc, scopy + ((size_t)w * NT_CL_MAX + crank) * NT_SC, steps, upd,
+                                   &taken, &mu);
             iters = taken;
             rel = mu;
             slot_geo(sh, sh.Rwb, sh.pwb);
-            nt_grad(sh, nt, d, dsm, lsc, upd);
-            gmax = nt_gmax(sh, nt, lsc);
-            for (int q = tid; q < P * 9; q += blockDim.x) d.Rwb[9 * s0 + q] = sh.Rwb[q];
-            for (int q = tid; q < P * 3; q += blockDim.x) d.pwb[3 * s0 + q] = sh.pwb[q];
-        } else {
-            // implicit adjoint: H x = dL/dx (poses from gpose, landmarks 0), then -(d2C / dtheta dx) x.  The exact
-            // reduced system solves it directly (nt_adjoint_direct); where that is not positive definite, conjugate
-            // gradients preconditioned with the Gauss-Newton system
-            if (!nt_adjoint_direct(sh, nt, d, dsm, lsc, gpose + 6 * (size_t)s0, tol, &rel, &iters)) {
-                slot_geo(sh, sh.Rwb, sh.pwb);
-                if (nt_gn_factor(sh, d, S64, wl64, lsc)) status = 1;
-                else {
-                    nt_grad(sh, nt, d, dsm, lsc, false);       // the gradient; constant landmarks as flagged
-                    for (int q = tid; q < n; q += blockDim.x)
-                        sh.rhs[q] = held(sh, q) ? 0.0 : gpose[6 * (size_t)s0 + q];
-                    for (int l = tid; l < sh.w.L; l += blockDim.x)
-                        for (int i = 0; i < NT_FROZEN; ++i) lsc[(size_t)(sh.w.lm0 + l) * NT_LM_STRIDE + i] = 0.0;
-                    __syncthreads();
-                    rel = nt_solve_exact(sh, nt, d, S64, dsm, lsc, maxit, tol, &iters, &neg);
-                    if (neg) status = 2;
-                    for (int l = tid; l < sh.w.L; l += blockDim.x) {
-                        double* sc = lsc + (size_t)(sh.w.lm0 + l) * NT_LM_STRIDE;
-                        for (int i = 0; i < 3; ++i) sc[NT_P + i] = sc[NT_X + i];
-                    }
-                    __syncthreads();
-                }
+            nt_grad(sh, nt, d, dsm, lsc, upd, true);
+            gmax = cl_reduce(nt, nt_gmax(sh, nt, lsc), true);
+            if (crank == 0) {
+                for (int q = tid; q < P * 9; q += blockDim.x) d.Rwb[9 * s0 + q] = sh.Rwb[q];
+                for (int q = tid; q < P * 3; q += blockDim.x) d.pwb[3 * s0 + q] = sh.pwb[q];
             }
-            if (status != 1) {
-                // the theta pass moves the state along the solution x (poses sh.dmp, landmarks NT_P)
+        } else if (nt_adjoint_direct(sh, nt, d, dsm, lsc, gpose + 6 * (size_t)s0, tol, &rel, &iters)) {
+            // implicit adjoint: H x = dL/dx (poses from gpose, landmarks 0) solved through the exact reduced system,
+            // then -(d2C / dtheta dx) x: the theta pass moves the state along x (poses sh.dmp, landmarks NT_P)
+            for (int q = tid; q < n; q += blockDim.x) { sh.dx[q] = sh.dmp[q]; nt.gp[q] = 0.0; nt.hp[q] = 0.0; }
+            if (tid < NT_THETA) nt.th[tid] = 0.0;
+            __syncthreads();
+            SlotGeo<Dual>* Gd = (SlotGeo<Dual>*)(dsm + ba_off_x(n));
+            slot_geo(sh, sh.Rwb, sh.pwb);
+            slot_geo_dual(sh, sh.dx, *Gd);
+            pass_dual(sh, nt, d, *Gd, NT_MODE_THETA, lsc, gisig, gz);
+            __syncthreads();
+            cl_sum_array(nt.th, NT_THETA);
+            if (tid < NT_THETA && crank == 0) gtheta[(size_t)w * NT_THETA + tid] = nt.th[tid];
+        } else if (crank == 0) {
+            // the exact reduced system is not positive definite: conjugate gradients preconditioned with the Gauss-
+            // Newton system, by the cluster's rank 0 over every landmark (no cluster barrier on this path)
+            if (tid == 0) { sh.lb = 0; sh.le = sh.w.L; }
+            __syncthreads();
+            slot_geo(sh, sh.Rwb, sh.pwb);
+            if (nt_gn_factor(sh, d, S64, wl64, lsc)) status = 1;
+            else {
+                nt_grad(sh, nt, d, dsm, lsc, false);       // the gradient; constant landmarks as flagged
+                for (int q = tid; q < n; q += blockDim.x)
+                    sh.rhs[q] = held(sh, q) ? 0.0 : gpose[6 * (size_t)s0 + q];
+                for (int l = tid; l < sh.w.L; l += blockDim.x)
+                    for (int i = 0; i < NT_FROZEN; ++i) lsc[(size_t)(sh.w.lm0 + l) * NT_LM_STRIDE + i] = 0.0;
+                __syncthreads();
+                rel = nt_solve_exact(sh, nt, d, S64, dsm, lsc, maxit, tol, &iters, &neg);
+                if (neg) status = 2;
+                for (int l = tid; l < sh.w.L; l += blockDim.x) {
+                    double* sc = lsc + (size_t)(sh.w.lm0 + l) * NT_LM_STRIDE;
+                    for (int i = 0; i < 3; ++i) sc[NT_P + i] = sc[NT_X + i];
+                }
                 for (int q = tid; q < n; q += blockDim.x) { sh.dx[q] = sh.dmp[q]; nt.gp[q] = 0.0; nt.hp[q] = 0.0; }
                 if (tid < NT_THETA) nt.th[tid] = 0.0;
                 __syncthreads();
@@ -2604,11 +2685,12 @@ __global__ void __launch_bounds__(BA_THREADS, 1) k_ba_newton(XcbBaWindows d, int
                 if (tid < NT_THETA) gtheta[(size_t)w * NT_THETA + tid] = nt.th[tid];
             }
         }
-        if (tid == 0) {
+        const double ovf = cl_reduce(nt, sh.overflow ? 1.0 : 0.0, true);
+        if (tid == 0 && crank == 0) {
             stats[4 * w + 0] = iters;
             stats[4 * w + 1] = rel;
             stats[4 * w + 2] = gmax;
-            stats[4 * w + 3] = status ? (double)status : (sh.overflow ? -2.0 : 0.0);
+            stats[4 * w + 3] = status ? (double)status : (ovf != 0.0 ? -2.0 : 0.0);
         }
         __syncthreads();
     }
@@ -2620,7 +2702,7 @@ size_t xcb_ba_newton_smem_bytes(int maxP)
     return ba_off_x(n) + nt_x_bytes(n) + sizeof(SlotGeo<Dual>);
 }
 
-size_t xcb_ba_newton_copy_doubles(int nw) { return (size_t)(nw > 0 ? nw : 1) * NT_SC; }
+size_t xcb_ba_newton_copy_doubles(int nw) { return (size_t)(nw > 0 ? nw : 1) * NT_CL_MAX * NT_SC; }
 
 cudaError_t xcb_launch_ba_newton(const XcbBaWindows& d, int max_slots, int mode, int steps, int maxit, double tol,
                                  const double* gpose, double* gtheta, double* gisig, double* gz, double* stats,
@@ -2630,10 +2712,36 @@ cudaError_t xcb_launch_ba_newton(const XcbBaWindows& d, int max_slots, int mode,
     static XcbAttrOnce attr;
     cudaError_t e = xcb_smem_attr_once(attr, (const void*)k_ba_newton, (int)xcb_ba_newton_smem_bytes(BA_MAXP));
     if (e != cudaSuccess) return e;
-    k_ba_newton<<<grid, BA_THREADS, xcb_ba_newton_smem_bytes(max_slots), st>>>(d, mode, steps, maxit, tol, gpose,
-                                                                               gtheta, gisig, gz, stats, lsc, counter,
-                                                                               lsc_doubles, scopy);
-    return cudaGetLastError();
+    // CTAs per window: the SMs that one CTA per window would leave idle, at most NT_CL_MAX (grid: the SM count)
+    int C = d.nw > 0 ? grid / d.nw : 1;
+    C = C < 1 ? 1 : (C > NT_CL_MAX ? NT_CL_MAX : C);
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    cfg.blockDim = dim3(BA_THREADS);
+    cfg.dynamicSmemBytes = xcb_ba_newton_smem_bytes(max_slots);
+    cfg.stream = st;
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    for (; C >= 1; --C) {
+        // as many clusters as the GPU holds at once (persistent: windows from the work counter), at most one per window
+        at[0].val.clusterDim.x = C;
+        cfg.gridDim = dim3(C);
+        int ncl = 0;
+        if (cudaOccupancyMaxActiveClusters(&ncl, (const void*)k_ba_newton, &cfg) != cudaSuccess || ncl < 1) {
+            cudaGetLastError();
+            continue;
+        }
+        int nc = ncl < d.nw ? ncl : d.nw;
+        if (grid / C < nc) nc = grid / C > 1 ? grid / C : 1;
+        cfg.gridDim = dim3(nc * C);
+        e = cudaLaunchKernelEx(&cfg, k_ba_newton, d, mode, steps, maxit, tol, gpose, gtheta, gisig, gz, stats, lsc,
+                               counter, lsc_doubles, scopy);
+        return e != cudaSuccess ? e : cudaGetLastError();
+    }
+    return cudaErrorInvalidConfiguration;
 }
 
 cudaError_t xcb_launch_ba_windows(const XcbBaWindows& d, int max_slots, int iters, double lam0, int mode,
