@@ -11,7 +11,8 @@ converged poses to de-rectifying it), weights [M] (the per-row weight 1/sigma in
 [M, 2] (observed pixels per row; the right rows use column 0).  Output: the converged body translations [slots, 3]
 (float64; the batch's slots in window order).
 
-Forward: `iters` LM iterations of window.solve (float64, batched, one launch); then the landmarks whose
+Forward: `iters` LM iterations of window.solve (float64, batched: one launch, or the large-window path when the
+batch holds few large windows); then the landmarks whose
 Gauss-Newton step would take the inverse depth to <= 1e-9 (window.solve keeps them where they are, while its Schur
 complement assumes they move, so its fixed point is not stationary) are flagged constant and `free_iters` LM
 iterations run with them held; then at most `newton_steps` landmark-eliminated Newton steps on the
@@ -51,7 +52,7 @@ class BAAdjoint(torch.autograd.Function):
             t["ob_isig"].copy_(weights.detach().to(torch.float64))
             t["ob_z"].copy_(pixels.detach().to(torch.float64))
             solver.reset()
-            solver.solve(int(iters), float(lam0), "fp64")
+            solver.solve(int(iters), float(lam0), "fp64", path="auto")    # the large-window path for few large windows
             solver.newton(0)                                        # flag the landmarks the LM cannot move
             solver.solve_free(int(free_iters), float(lam0))
             st = solver.newton(int(newton_steps), tol=float(tol))
