@@ -402,6 +402,19 @@ def run_ours(args, ws, rank, local):
             "algorithmic_bytes_per_launch": bytes_launch,
             "whole_path_frac": frame_bytes * value / ws / 1e9 / peak,
             "stage_ms_per_step": per_step}
+    if dom == "stereo" and per_step["stereo"] > 0:
+        # the search's compute roofline in the reference's float32 formulation: per feature, the forward search and
+        # the left-right check each take sum R, sum R^2 and sum L R over the window at every disparity (3 FMAs per
+        # pixel and disparity); this path does the same search in exact integer sums plus float64 for the
+        # candidates that can decide, so the figure is algorithmic work per second, not the instructions issued
+        npix, nd = (2 * HALF + 1) ** 2, DHI - DLO + 1
+        flops_frame = BUDGET * 2 * nd * npix * 3 * 2
+        ach_tf = flops_frame * F / (per_step["stereo"] / 1e3) / 1e12
+        p32 = fma_peak(False)
+        roof["compute"] = {"bound": "fp32 (the reference's formulation)", "achieved": ach_tf, "peak": p32,
+                           "unit": "TFLOP/s", "frac": ach_tf / p32,
+                           "peak_kind": "measured FP32 FMA loop on this GPU (xcb_peak_fma)",
+                           "algorithmic_flops_per_frame": flops_frame}
     cpu = None
     recheck = None
     if rank == 0 and ws == 1 and not args.no_cpu:
