@@ -114,3 +114,33 @@ def test_config3_adjoint_matches_central_finite_differences(c3):
     fd = central("ob_isig", torch.as_tensor(wrows, device="cuda"), 1e-4)
     for i in range(NW):
         assert abs(fd[i] - gw[wrows[i]]) < TOL * np.abs(gw[ro[i]:ro[i + 1]]).max(), i
+
+
+def test_config3_clusters_and_one_cta_per_window_agree(c3):
+    """The Newton kernel gives a window a thread-block cluster of up to four CTAs when there are fewer windows than SMs
+    (here 4 CTAs each) and reduces across them in rank order; with `grid` equal to the window count it runs one CTA
+    per window.  Both forward states and adjoints agree to rounding (the sums run in another order)."""
+    import torch
+    from xclean_b200.backend.ba import BatchSolver
+    s1, ws = c3["solver"], c3["ws"]
+    s2 = BatchSolver(ws, "cuda", hold=0)
+    for k in ("cam", "ob_isig", "ob_z"):
+        s2.t[k].copy_(s1.t[k])
+    s2.reset()
+    s2.solve(20, 1e-4, "fp64", path="auto")
+    s2.newton(0, grid=NW)
+    s2.solve_free(20, 1e-4)
+    st = s2.newton(40, grid=NW).cpu().numpy()
+    assert float(st[:, 2].max()) < 1e-6, st
+    for k in ("Rwb", "pwb", "lmp"):
+        a, b = c3["state"][k].cpu().numpy(), s2.t[k].cpu().numpy()
+        assert np.abs(a - b).max() < 1e-9 * max(1.0, np.abs(a).max()), k
+    ptrue = torch.as_tensor(np.concatenate([w.pwb_true for w in ws]), device="cuda")
+    gpose = torch.zeros((s2.t["pwb"].shape[0], 6), dtype=torch.float64, device="cuda")
+    gpose[:, 3:] = 2 * (s2.t["pwb"] - ptrue)
+    _st, gth, gis, gz = s2.adjoint(gpose, grid=NW)
+    gi, gb, ge, gw, gp = c3["grads"]
+    dev_theta = np.concatenate([gi, gb[:, None], ge], axis=1)
+    assert _rel(gth.cpu().numpy(), dev_theta) < 1e-7
+    assert _rel(gis.cpu().numpy(), gw) < 1e-7
+    assert _rel(gz.cpu().numpy(), gp) < 1e-7

@@ -1777,7 +1777,8 @@ __device__ double nt_gmax(BaShared& sh, NtShared& nt, const double* lsc)
 static __host__ __device__ __forceinline__ size_t nt_x_bytes(int n)
 {
     size_t x = ba_x_bytes(n);
-    if (sizeof(SlotGeo<Dual>) > x) x = sizeof(SlotGeo<Dual>);
+    const size_t q = ((sizeof(SlotGeo<Dual>) + 15) & ~(size_t)15) + (size_t)BA_WARPS * 256 * sizeof(int);
+    if (q > x) x = q;                   // a direction's geometry and the column passes' row queues
     return (x + 15) & ~(size_t)15;
 }
 
@@ -1982,10 +1983,36 @@ __device__ void pass_inner(BaShared& sh, const XcbBaWindows& d, const SlotGeo<Du
 }
 
 // Hpp column c = 6 s + j (G: the geometry moved along e_c): every row group with slot s as its host or its target
-// adds the dual part of its pose gradient, d(w J^T e)/dx_c, to the rows >= c of S (packed lower)
-__device__ void pass_hpp_col(BaShared& sh, const XcbBaWindows& d, const SlotGeo<Dual>& G, int s, int c, double* S)
+// adds the dual part of its pose gradient, d(w J^T e)/dx_c, to the rows >= c of S (packed lower).  A row group's
+// terms need no sum over its landmark, so the warp queues the row groups that touch slot s (2-4 of a landmark's
+// rows) in wq (this warp's 4 x 64 ints) and evaluates them 32 at a time, a lane each.
+__device__ __forceinline__ void hpp_row(const BaShared& sh, const XcbBaWindows& d, const SlotGeo<Dual>& G, int c,
+                                        double* S, int k, int gl, int h, int t)
+{
+    const Dual lm[3] = {Dual(d.lmp[3 * gl]), Dual(d.lmp[3 * gl + 1]), Dual(d.lmp[3 * gl + 2])};
+    Dual ob[OB_N];
+    if (!obs_lin<Dual>(sh.w, G, lm, h, t, d.ob_cam[k], d.ob_z + 2 * k, Dual(d.ob_isig[k]), ob, 1)) return;
+    const Dual en = sqrt(ob[OB_E] * ob[OB_E] + ob[OB_E + 1] * ob[OB_E + 1]);
+    Dual wt, cc;
+    huber_w<Dual>(en, Dual(sh.w.hk), &wt, &cc);
+    for (int i = 0; i < 6; ++i) {
+        const Dual gt = wt * (ob[OB_JT + i] * ob[OB_E] + ob[OB_JT + 6 + i] * ob[OB_E + 1]);
+        const Dual gh = wt * (obj(ob, OB_JH, 0, i) * ob[OB_E] + obj(ob, OB_JH, 1, i) * ob[OB_E + 1]);
+        const int rt = 6 * t + i, rh = 6 * h + i;
+        if (rt >= c) atomicAdd(&S[tri(rt, c)], gt.e);
+        if (rh >= c) atomicAdd(&S[tri(rh, c)], gh.e);
+    }
+}
+
+__device__ void pass_hpp_col(BaShared& sh, const XcbBaWindows& d, const SlotGeo<Dual>& G, int s, int c, double* S,
+                             int* wq)
 {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int* qk = wq;
+    int* ql = wq + 64;
+    int* qh = wq + 128;
+    int* qt = wq + 192;
+    int nq = 0;                                          // queued row groups (the same on every lane)
     for (int l = sh.lb + wid; l < sh.le; l += BA_WARPS) {
         const int gl = sh.w.lm0 + l;
         if (!d.lm_mask[gl]) continue;
@@ -1995,30 +2022,31 @@ __device__ void pass_hpp_col(BaShared& sh, const XcbBaWindows& d, const SlotGeo<
         int t = -1;
         bool ev = false;
         if (lane < nob) {
-            const int k = k0 + lane;
-            t = d.ob_pose[k];
-            ev = d.ob_valid[k] && (unsigned)t < (unsigned)sh.w.P && t != h && (h == s || t == s);
+            t = d.ob_pose[k0 + lane];
+            ev = d.ob_valid[k0 + lane] && (unsigned)t < (unsigned)sh.w.P && t != h && (h == s || t == s);
         }
-        if (!__any_sync(0xffffffffu, ev)) continue;
+        const unsigned m = __ballot_sync(0xffffffffu, ev);
+        if (!m) continue;
         if (ev) {
-            const int k = k0 + lane;
-            const Dual lm[3] = {Dual(d.lmp[3 * gl]), Dual(d.lmp[3 * gl + 1]), Dual(d.lmp[3 * gl + 2])};
-            Dual ob[OB_N];
-            if (obs_lin<Dual>(sh.w, G, lm, h, t, d.ob_cam[k], d.ob_z + 2 * k, Dual(d.ob_isig[k]), ob, 1)) {
-                const Dual en = sqrt(ob[OB_E] * ob[OB_E] + ob[OB_E + 1] * ob[OB_E + 1]);
-                Dual wt, cc;
-                huber_w<Dual>(en, Dual(sh.w.hk), &wt, &cc);
-                for (int i = 0; i < 6; ++i) {
-                    const Dual gt = wt * (ob[OB_JT + i] * ob[OB_E] + ob[OB_JT + 6 + i] * ob[OB_E + 1]);
-                    const Dual gh = wt * (obj(ob, OB_JH, 0, i) * ob[OB_E] + obj(ob, OB_JH, 1, i) * ob[OB_E + 1]);
-                    const int rt = 6 * t + i, rh = 6 * h + i;
-                    if (rt >= c) atomicAdd(&S[tri(rt, c)], gt.e);
-                    if (rh >= c) atomicAdd(&S[tri(rh, c)], gh.e);
-                }
-            }
+            const int pos = nq + __popc(m & ((1u << lane) - 1u));
+            qk[pos] = k0 + lane; ql[pos] = gl; qh[pos] = h; qt[pos] = t;
         }
+        nq += __popc(m);
         __syncwarp();
+        if (nq >= 32) {
+            hpp_row(sh, d, G, c, S, qk[lane], ql[lane], qh[lane], qt[lane]);
+            __syncwarp();
+            const int rest = nq - 32;
+            int a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+            if (lane < rest) { a0 = qk[32 + lane]; a1 = ql[32 + lane]; a2 = qh[32 + lane]; a3 = qt[32 + lane]; }
+            __syncwarp();
+            if (lane < rest) { qk[lane] = a0; ql[lane] = a1; qh[lane] = a2; qt[lane] = a3; }
+            __syncwarp();
+            nq = rest;
+        }
     }
+    if (lane < nq) hpp_row(sh, d, G, c, S, qk[lane], ql[lane], qh[lane], qt[lane]);
+    __syncwarp();
 }
 
 // (2) the landmark terms of the exact reduced system at the current state (G0: zero tangents): per landmark whose exact
@@ -2349,6 +2377,8 @@ __device__ double nt_xsystem(BaShared& sh, NtShared& nt, const XcbBaWindows& d, 
     WarpLm<double>* wl64 = (WarpLm<double>*)(dsm + ba_off_x(n));
     SlotGeo<Dual>* Gd = (SlotGeo<Dual>*)(dsm + ba_off_x(n));           // aliases wl64: never live together
     SlotGeo<Dual>* G0 = (SlotGeo<Dual>*)(dsm + ba_off_x(n) + nt_x_bytes(n));
+    // the column passes' row queues (256 ints per warp) after the direction's geometry, in the warp-scratch region
+    int* wq = (int*)(dsm + ba_off_x(n) + ((sizeof(SlotGeo<Dual>) + 15) & ~(size_t)15)) + (tid >> 5) * 256;
     const int ntri = n * (n + 1) / 2;
     for (int q = tid; q < ntri; q += blockDim.x) S[q] = 0.0;
     for (int q = tid; q < n; q += blockDim.x) nt.gp[q] = 0.0;
@@ -2358,7 +2388,7 @@ __device__ double nt_xsystem(BaShared& sh, NtShared& nt, const XcbBaWindows& d, 
         for (int q = tid; q < n; q += blockDim.x) sh.dx[q] = q == c ? 1.0 : 0.0;
         __syncthreads();
         slot_geo_dual(sh, sh.dx, *Gd);
-        pass_hpp_col(sh, d, *Gd, c / 6, c, S);
+        pass_hpp_col(sh, d, *Gd, c / 6, c, S, wq);
         __syncthreads();
     }
     pass_xbuild(sh, nt, d, *G0, S, wl64, lsc, upd);
