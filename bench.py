@@ -77,6 +77,9 @@ def parse():
     ap.add_argument("--ba-large-only", action="store_true",
                     help="only the 20-keyframe windows (large-window path and one CTA per window), printed as one line")
     ap.add_argument("--large-windows", type=int, default=32, help="20-keyframe windows per step (default 32)")
+    ap.add_argument("--adjoint-only", action="store_true",
+                    help="only the differentiable-BA adjoint (forward + backward), printed as one line (profiling)")
+    ap.add_argument("--adj-windows", type=int, default=64, help="differentiable-BA windows per step (default 64)")
     return ap.parse_args()
 
 
@@ -270,10 +273,12 @@ def run_ours(args, ws, rank, local):
     dev = torch.device("cuda", local)
     if ws > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
-    if args.ba_only or args.ba_large_only:
+    if args.ba_only or args.ba_large_only or args.adjoint_only:
         stream = torch.cuda.Stream(device=dev)
         torch.cuda.set_stream(stream)
-        if args.ba_large_only:
+        if args.adjoint_only:
+            ba = run_adjoint(args, dev, stream, ws, rank)
+        elif args.ba_large_only:
             ba = run_ba_large(args, dev, stream, ws, rank)
         else:
             ba = run_ba(args, dev, stream, rank, ws, cpu=(rank == 0 and ws == 1 and not args.no_cpu))
@@ -1182,7 +1187,8 @@ def run_adjoint(args, dev, stream, ws_world, rank, large=False):
     from xclean_b200.backend import synth_ba as S
     from xclean_b200.backend.adjoint import BAAdjoint, inputs_of
     from xclean_b200.backend.ba import BatchSolver
-    wins = S.config4_windows(args.large_windows, seed=4 + rank) if large else S.config3_windows(64, seed=3 + rank)
+    wins = (S.config4_windows(args.large_windows, seed=4 + rank) if large
+            else S.config3_windows(args.adj_windows, seed=3 + rank))
     with torch.cuda.stream(stream):
         solver = BatchSolver(wins, dev, hold=0)
         ptrue = torch.as_tensor(np.concatenate([w.pwb_true for w in wins]), device=dev)
@@ -1211,7 +1217,8 @@ def run_adjoint(args, dev, stream, ws_world, rank, large=False):
             "final_gradient_max_median": float(np.median(st[:, 2])),
             "final_gradient_max_quartiles": [float(x) for x in np.percentile(st[:, 2], [25, 75])],
             "config": {"workload": ("%d windows x (20 keyframes, 6000 landmarks, 3-15 obs, 10%% outliers)" % len(wins)
-                                    if large else "64 windows x (10 keyframes, 2000 landmarks, 2-6 obs, 5% outliers)") +
+                                    if large else "%d windows x (10 keyframes, 2000 landmarks, 2-6 obs, 5%% outliers)"
+                                    % len(wins)) +
                                    "; forward 20 LM "
                                    "iterations, 20 LM iterations with the landmarks the LM cannot move held "
                                    "constant, up to %d landmark-eliminated Newton steps; implicit adjoint of "

@@ -375,6 +375,14 @@ size_t xcb_ba_large_scratch_bytes(int nw, int slots, int Lt);
 int xcb_ba_solve_windows_large_dev(const xcb_ba_windows* w, int slots, int Lt, const int32_t* chunks, int nchunks,
                                    int max_slots, int iters, double lam0, int mode, double* stats, double* dx0,
                                    int dx0_stride, void* scratch, size_t scratch_bytes, void* stream);
+/* xcb_ba_solve_windows_free_dev (float64, the landmarks that the Newton calls on `newton_scratch` flagged held
+   constant) on the large-window path (no reference counterpart: the differentiable BA's forward on few large
+   windows).  Arguments as xcb_ba_solve_windows_large_dev; newton_scratch / newton_scratch_bytes: the scratch of those
+   Newton calls (its flags: 19 doubles per landmark after its first 256 bytes). */
+int xcb_ba_solve_windows_large_free_dev(const xcb_ba_windows* w, int slots, int Lt, const int32_t* chunks, int nchunks,
+                                        int max_slots, int iters, double lam0, double* stats, void* scratch,
+                                        size_t scratch_bytes, const void* newton_scratch, size_t newton_scratch_bytes,
+                                        void* stream);
 
 /* The engine's state from which a window Problem is assembled (P1Engine._problem, src/xclean/vio/engine_live.py
    :407-530, visual part).  All pointers are device memory.  The slots' observation lists are concatenated in slot

@@ -26,6 +26,31 @@ def _rel(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
 
+def test_large_path_constant_landmarks_match_the_window_kernel():
+    """The constant-landmark LM (the differentiable-BA forward: landmarks the Newton call flagged are held constant,
+    their rows kept) on the large-window path against the one-CTA-per-window kernel, float64, the same flags."""
+    import torch
+    from xclean_b200.backend.ba import BatchSolver
+    ws = _windows()
+    a = BatchSolver(ws, "cuda", hold=0)
+    b = BatchSolver(ws, "cuda", hold=0)
+    for s in (a, b):
+        s.solve(10, 1e-4, "fp64", path="window")
+        s.newton(0)                                      # the flags
+    assert torch.equal(a.frozen(), b.frozen()) and bool(a.frozen().any())
+    held = b.t["lmp"][b.frozen()].clone()
+    fa = a.solve_free(10, 1e-4, path="window").cpu().numpy()
+    fb = b.solve_free(10, 1e-4, path="large").cpu().numpy()
+    torch.cuda.synchronize()
+    assert (fa[:, 4] == 0).all() and (fb[:, 4] == 0).all()
+    assert np.array_equal(fa[:, 2], fb[:, 2])                               # accepted steps
+    np.testing.assert_allclose(fb[:, 1], fa[:, 1], rtol=1e-9)               # final cost
+    assert torch.equal(b.t["lmp"][b.frozen()], held)                         # the flagged landmarks did not move
+    for k in ("Rwb", "pwb"):
+        assert float((a.t[k] - b.t[k]).abs().max()) < 1e-6, k
+    assert float((a.t["lmp"] - b.t["lmp"]).abs().max()) < 1e-5 * max(1.0, float(a.t["lmp"].abs().max()))
+
+
 def test_large_path_matches_the_window_kernel_float64():
     import torch
     from xclean_b200.backend.ba import BatchSolver

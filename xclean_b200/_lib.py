@@ -103,6 +103,8 @@ _SIGS.update({
     "xcb_ba_assemble_dev": (c_int, [ctypes.POINTER(BaEngine), ctypes.POINTER(BaAssembled), P, c_size_t, P]),
     "xcb_ba_solve_windows_large_dev": (c_int, [ctypes.POINTER(BaWindows), c_int, c_int, P, c_int, c_int, c_int,
                                                c_double, c_int, P, P, c_int, P, c_size_t, P]),
+    "xcb_ba_solve_windows_large_free_dev": (c_int, [ctypes.POINTER(BaWindows), c_int, c_int, P, c_int, c_int, c_int,
+                                                    c_double, P, P, c_size_t, P, c_size_t, P]),
     "xcb_ba_solve_windows_dev": (c_int, [ctypes.POINTER(BaWindows), c_int, c_int, c_double, c_int, P, P, c_int, P,
                                          c_size_t, c_int, P]),
     "xcb_ba_newton_scratch_bytes": (c_size_t, [c_int, c_int]),

@@ -54,7 +54,7 @@ class BAAdjoint(torch.autograd.Function):
             solver.reset()
             solver.solve(int(iters), float(lam0), "fp64", path="auto")    # the large-window path for few large windows
             solver.newton(0)                                        # flag the landmarks the LM cannot move
-            solver.solve_free(int(free_iters), float(lam0))
+            solver.solve_free(int(free_iters), float(lam0), path="auto")
             st = solver.newton(int(newton_steps), tol=float(tol))
         ctx.solver = solver
         ctx.tol = float(tol)

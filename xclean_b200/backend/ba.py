@@ -264,14 +264,24 @@ class BatchSolver:
             self.nscratch = self.torch.zeros(nb, dtype=self.torch.uint8, device=self.dev)
         return self.nscratch
 
-    def solve_free(self, iters=20, lam0=1e-4, stream=None, grid=0):
+    def solve_free(self, iters=20, lam0=1e-4, stream=None, grid=0, path="window"):
         """window.solve (float64) with the landmarks that earlier newton() calls found frozen held constant, so that
-        the LM converges to a stationary point of the cost in the other variables.  -> stats [nw, 8] (cost0, cost,
+        the LM converges to a stationary point of the cost in the other variables.  path: "window" (one CTA per
+        window), "large" (the large-window path) or "auto" (use_large decides).  -> stats [nw, 8] (cost0, cost,
         accepted, lam, status, iters, -, -)."""
         torch = self.torch
         s = stream if stream is not None else torch.cuda.current_stream(self.dev)
         sc = self._nscratch()
         stats = torch.zeros((max(self.nw, 1), 8), dtype=torch.float64, device=self.dev)
+        if path == "large" or (path == "auto" and self.use_large()):
+            self._large_setup()
+            rc = _lib.lib().xcb_ba_solve_windows_large_free_dev(
+                ctypes.byref(self.desc), int(self.host["Rwb"].shape[0]), int(self.host["lmp"].shape[0]),
+                self.lchunks.data_ptr(), self.nchunks, self.max_slots, int(iters), float(lam0), stats.data_ptr(),
+                self.lscratch.data_ptr(), self.lscratch.numel(), sc.data_ptr(), sc.numel(),
+                ctypes.c_void_p(s.cuda_stream or None))
+            _lib.check(rc, None, "xcb_ba_solve_windows_large_free_dev")
+            return stats[:self.nw]
         rc = _lib.lib().xcb_ba_solve_windows_free_dev(ctypes.byref(self.desc), int(self.host["lmp"].shape[0]),
                                                       self.max_slots, int(iters), float(lam0), stats.data_ptr(),
                                                       sc.data_ptr(), sc.numel(), int(grid),

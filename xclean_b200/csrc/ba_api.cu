@@ -242,3 +242,27 @@ extern "C" int xcb_ba_solve_windows_large_dev(const xcb_ba_windows* w, int slots
     if (e != cudaSuccess) return ba_fail(XCB_ERR_CUDA, cudaGetErrorString(e));
     return XCB_OK;
 }
+
+extern "C" int xcb_ba_solve_windows_large_free_dev(const xcb_ba_windows* w, int slots, int Lt, const int32_t* chunks,
+                                                   int nchunks, int max_slots, int iters, double lam0, double* stats,
+                                                   void* scratch, size_t scratch_bytes, const void* newton_scratch,
+                                                   size_t newton_scratch_bytes, void* stream)
+{
+    if (!w || !stats || !scratch || !newton_scratch || (!chunks && nchunks > 0))
+        return ba_fail(XCB_ERR_ARG, "ba_solve_large_free: null argument");
+    if (w->nw <= 0) return XCB_OK;
+    if (max_slots < 1 || max_slots > xcb_ba_max_slots())
+        return ba_fail(XCB_ERR_CAPACITY, "ba_solve_large_free: max_slots out of range (1..20)");
+    if (w->pr_m) return ba_fail(XCB_ERR_ARG, "ba_solve_large_free: windows with a marginal prior take xcb_ba_solve_windows_free_dev");
+    if (slots < 0 || Lt < 0 || nchunks < 0 || iters < 0) return ba_fail(XCB_ERR_ARG, "ba_solve_large_free: negative size");
+    if (scratch_bytes < xcb_ba_large_scratch_bytes_impl(w->nw, slots, Lt))
+        return ba_fail(XCB_ERR_CAPACITY, "ba_solve_large_free: scratch smaller than xcb_ba_large_scratch_bytes");
+    // the flags: 19 doubles per landmark after the Newton scratch's first 256 bytes
+    if (newton_scratch_bytes < 256 + (size_t)19 * (size_t)(Lt > 0 ? Lt : 1) * sizeof(double))
+        return ba_fail(XCB_ERR_CAPACITY, "ba_solve_large_free: Newton scratch smaller than 19 doubles per landmark");
+    const double* frz = (const double*)((const char*)newton_scratch + 256);
+    cudaError_t e = xcb_launch_ba_large(*w, slots, Lt, chunks, nchunks, max_slots, iters, lam0, XCB_BA_FP64, stats,
+                                        nullptr, 0, scratch, scratch_bytes, (cudaStream_t)stream, frz);
+    if (e != cudaSuccess) return ba_fail(XCB_ERR_CUDA, cudaGetErrorString(e));
+    return XCB_OK;
+}

@@ -27,6 +27,8 @@ cudaError_t xcb_launch_ba_newton(const XcbBaWindows& d, int max_slots, int mode,
 // window on all SMs (chunks: [nchunks][3] int32 on the device: window, first landmark, end), the per-window steps one
 // CTA per window
 size_t xcb_ba_large_scratch_bytes_impl(int nw, int slots, int Lt);
+// frz (optional): constant-landmark flags as xcb_launch_ba_windows takes them
 cudaError_t xcb_launch_ba_large(const XcbBaWindows& d, int slots, int Lt, const int* chunks, int nchunks,
                                 int max_slots, int iters, double lam0, int mode, double* stats, double* dx0,
-                                int dx0_stride, void* scratch, size_t scratch_bytes, cudaStream_t st);
+                                int dx0_stride, void* scratch, size_t scratch_bytes, cudaStream_t st,
+                                const double* frz = nullptr);

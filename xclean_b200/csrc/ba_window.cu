@@ -2819,6 +2819,7 @@ struct LwWork {
     double* R2;             // [S][9] trial poses
     double* p2;             // [S][3]
     double* lmp_trial;      // [Lt][3]
+    const double* frz;      // the Newton scratch's constant-landmark flags (19 doubles per landmark), or null
 };
 
 // one chunk: landmarks [l0, l1) (window-local) of window w
@@ -2884,9 +2885,9 @@ __global__ void __launch_bounds__(BA_THREADS, 1) k_lw_build(XcbBaWindows d, LwWo
     __syncthreads();
     double cst = 0.0;
     if constexpr (sizeof(T) == 4)
-        pass_build<T, true>(sh, d, sh.g32, S, gb, wl, &cst);
+        pass_build<T, true>(sh, d, sh.g32, S, gb, wl, &cst, lw.frz);
     else
-        pass_build<T, true>(sh, d, sh.g64, S, gb, wl, &cst);
+        pass_build<T, true>(sh, d, sh.g64, S, gb, wl, &cst, lw.frz);
     const double ctot = block_sum_red(sh);
     T* Sg = (T*)(lw.S + (size_t)c.w * LW_NT);
     T* gg = (T*)(lw.g + (size_t)c.w * BA_MAXN);
@@ -2908,7 +2909,7 @@ __global__ void __launch_bounds__(BA_THREADS, 1) k_lw_build(XcbBaWindows d, LwWo
 // S = sum of pose-pose blocks - sum_l Hlp_l^T Hll_l^-1 Hlp_l.  A landmark whose Hll^-1 is not numerically positive
 // definite in float64 keeps the scatter of its Schur blocks.  -> false when a tensor-core wait ran out.
 __device__ bool pass_build_tc(BaShared& sh, const XcbBaWindows& d, float* S, float* gb, WarpLm<float>* wls,
-                              float* tiles, uint64_t* bar, uint32_t tmem, int* fail)
+                              float* tiles, uint64_t* bar, uint32_t tmem, int* fail, const double* frz)
 {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, tid = threadIdx.x;
     WarpLm<float>& wl = wls[wid];
@@ -2931,7 +2932,8 @@ __device__ bool pass_build_tc(BaShared& sh, const XcbBaWindows& d, float* S, flo
             const int h = d.lm_host[gl];
             float Hll[9], bl[3];
             int nt;
-            const bool ok = lin_landmark<float>(sh, d, G, l, sh.lam, d.lmp, wl, Hll, bl, &nt, &c_local);
+            const bool ok = lin_landmark<float>(sh, d, G, l, sh.lam, d.lmp, wl, Hll, bl, &nt, &c_local) &&
+                            !lm_const(frz, gl);
             float Hi[9], HiB[3] = {0.0f, 0.0f, 0.0f};
             double C[9] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
             bool tcl = false;
@@ -3101,7 +3103,7 @@ __global__ void __launch_bounds__(BA_THREADS, 1) k_lw_build_tc(XcbBaWindows d, L
     for (int q = tid; q < nt; q += blockDim.x) S[q] = 0.0f;
     for (int q = tid; q < n; q += blockDim.x) sh.bf[q] = 0.0f;
     __syncthreads();
-    const bool good = pass_build_tc(sh, d, S, sh.bf, wl, tiles, bar, tmem, &fail);
+    const bool good = pass_build_tc(sh, d, S, sh.bf, wl, tiles, bar, tmem, &fail, lw.frz);
     const double ctot = block_sum_red(sh);
     float* Sg = (float*)(lw.S + (size_t)c.w * LW_NT);
     float* gg = (float*)(lw.g + (size_t)c.w * BA_MAXN);
@@ -3188,7 +3190,7 @@ __global__ void __launch_bounds__(BA_THREADS, 1) k_lw_refine(XcbBaWindows d, LwW
     for (int q = threadIdx.x; q < n; q += blockDim.x) sh.dx[q] = lw.dx[(size_t)c.w * BA_MAXN + q];
     __syncthreads();
     WarpLm<double>* wl = (WarpLm<double>*)dsm;
-    pass_refine(sh, d, wl, rf == 0);
+    pass_refine(sh, d, wl, rf == 0, lw.frz);
     const double ctot = block_sum_red(sh);
     for (int q = threadIdx.x; q < n; q += blockDim.x) {
         if (rf == 0) atomicAdd(&lw.g64[(size_t)c.w * BA_MAXN + q], sh.g[q]);
@@ -3264,7 +3266,7 @@ __global__ void __launch_bounds__(BA_THREADS, 1) k_lw_backsub(XcbBaWindows d, Lw
     for (int q = threadIdx.x; q < n; q += blockDim.x) sh.dx[q] = lw.dx[(size_t)c.w * BA_MAXN + q];
     __syncthreads();
     WarpLm<double>* wl = (WarpLm<double>*)dsm;
-    pass_backsub(sh, d, wl, lw.lmp_trial);
+    pass_backsub(sh, d, wl, lw.lmp_trial, lw.frz);
     __syncthreads();
     const int P = sh.w.P, s0 = sh.w.s0;
     for (int q = threadIdx.x; q < P * 9; q += blockDim.x) sh.R2[q] = lw.R2[9 * s0 + q];
@@ -3367,7 +3369,7 @@ static size_t lw_build_smem(int maxP, bool mixed)
 
 cudaError_t xcb_launch_ba_large(const XcbBaWindows& d, int slots, int Lt, const int* chunks, int nchunks,
                                 int max_slots, int iters, double lam0, int mode, double* stats, double* dx0,
-                                int dx0_stride, void* scratch, size_t scratch_bytes, cudaStream_t st)
+                                int dx0_stride, void* scratch, size_t scratch_bytes, cudaStream_t st, const double* frz)
 {
     if (scratch_bytes < xcb_ba_large_scratch_bytes_impl(d.nw, slots, Lt)) return cudaErrorInvalidValue;
     char* p = (char*)scratch;
@@ -3392,6 +3394,7 @@ cudaError_t xcb_launch_ba_large(const XcbBaWindows& d, int slots, int Lt, const 
     lw.R2 = (double*)take((size_t)slots * 9 * 8);
     lw.p2 = (double*)take((size_t)slots * 3 * 8);
     lw.lmp_trial = (double*)take((size_t)Lt * 3 * 8);
+    lw.frz = frz;
     if ((size_t)(p - (char*)scratch) > scratch_bytes) return cudaErrorInvalidValue;
     const bool mixed = mode == XCB_BA_MIXED || mode == XCB_BA_MIXED_NOTC;
     const bool tc = mode == XCB_BA_MIXED;
