@@ -78,11 +78,10 @@ static int ba_fail(int code, const char* msg)
 }
 
 // Newton / adjoint scratch: [counter (256 B)][19 doubles per landmark][3 doubles per landmark: trial states of the
-// constant-landmark window solve]
+// constant-landmark window solve][the polish's copies of the reduced systems: 4 per window, one per CTA of its
+// cluster]
 extern "C" size_t xcb_ba_newton_scratch_bytes(int nw, int Lt)
 {
-    (void)nw;
-    // [counter 256 B][19 + 3 doubles per landmark][the polish's copies of the reduced systems]
     return ((size_t)(Lt > 0 ? Lt : 1) * 22 * sizeof(double) + 255) / 256 * 256 + 256 +
            xcb_ba_newton_copy_doubles(nw) * sizeof(double);
 }

@@ -1604,32 +1604,12 @@ __device__ void nt_precond(BaShared& sh, const XcbBaWindows& d, double* S64, War
     pass_pre_b(sh, d, wl64, lsc);
 }
 
-// (H + mu H_GN) x = b (b_p = sh.rhs, b_l = NT_B) by conjugate gradients preconditioned with the Gauss-Newton system
-// (its factor in S64; H_GN p comes from the same dual pass: the dual part of e is J p).  delta > 0: Steihaug's
-// truncated CG for the trust region |x|_M <= delta (M the Gauss-Newton preconditioner): a step that would leave the
-// region, or a direction of non-positive curvature, ends at its boundary (*boundary = 1).  -> x (sh.dmp, NT_X); the final relative residual; *iters_out the iterations; *neg set if a non-positive
-// curvature p^T H p was met (the state is not a strict minimum).
-__device__ void nt_axpy_p(BaShared& sh, double* lsc, double a)        // x += a p (poses sh.dmp / sh.dx, NT_X / NT_P)
-{
-    for (int q = threadIdx.x; q < sh.w.n; q += blockDim.x)
-        if (!held(sh, q)) sh.dmp[q] += a * sh.dx[q];
-    for (int l = threadIdx.x; l < sh.w.L; l += blockDim.x) {
-        double* sc = lsc + (size_t)(sh.w.lm0 + l) * NT_LM_STRIDE;
-        for (int i = 0; i < 3; ++i) sc[NT_X + i] += a * sc[NT_P + i];
-    }
-    __syncthreads();
-}
-
-// tau >= 0 with |x + tau p|_M = delta, from x^T M x, x^T M p, p^T M p
-__device__ __forceinline__ double nt_to_boundary(double xMx, double xMp, double pMp, double delta)
-{
-    const double disc = fmax(xMp * xMp + pMp * (delta * delta - xMx), 0.0);
-    return (-xMp + sqrt(disc)) / fmax(pMp, 1e-300);
-}
-
+// H x = b (b_p = sh.rhs, b_l = NT_B) by conjugate gradients preconditioned with the Gauss-Newton system (its factor in
+// S64): the adjoint's fallback where the exact reduced system is not positive definite.  -> x (sh.dmp, NT_X); the
+// final relative residual; *iters_out the iterations; *neg set if a non-positive curvature p^T H p was met (the state
+// is not a strict minimum).  The landmarks of the slice lb..le (the whole window on the fallback's single CTA).
 __device__ double nt_solve_exact(BaShared& sh, NtShared& nt, const XcbBaWindows& d, double* S64, unsigned char* dsm,
-                                 double* lsc, int maxit, double tol, int* iters_out, int* neg, double mu = 0.0,
-                                 double delta = 0.0, int* boundary = nullptr, double* xMx_out = nullptr)
+                                 double* lsc, int maxit, double tol, int* iters_out, int* neg)
 {
     const int n = sh.w.n, tid = threadIdx.x;
     WarpLm<double>* wl64 = (WarpLm<double>*)(dsm + ba_off_x(n));
@@ -1642,8 +1622,7 @@ __device__ double nt_solve_exact(BaShared& sh, NtShared& nt, const XcbBaWindows&
     __syncthreads();
     const double bnorm = sqrt(nt_dot(sh, nt, sh.g, sh.g, lsc, NT_R, NT_R));
     *neg = 0;
-    if (boundary) *boundary = 0;
-    double rel = 0.0, pMp = 0.0, xMp = 0.0, xMx = 0.0;
+    double rel = 0.0;
     int it = 0;
     if (bnorm > 0.0) {
         nt_precond(sh, d, S64, wl64, lsc);
@@ -1654,29 +1633,16 @@ __device__ double nt_solve_exact(BaShared& sh, NtShared& nt, const XcbBaWindows&
         }
         __syncthreads();
         double rz = nt_dot(sh, nt, sh.g, sh.y, lsc, NT_R, NT_Z);
-        pMp = rz;                                       // M-norm terms of the iterates (CG recursions)
-        if (delta >= 1e100) delta = 10.0 * sqrt(fmax(rz, 0.0));   // unbounded: 10x the Gauss-Newton step's M-norm
         rel = 1.0;
         for (it = 0; it < maxit; ++it) {
             for (int q = tid; q < n; q += blockDim.x) { nt.gp[q] = 0.0; nt.hp[q] = 0.0; }
             __syncthreads();
             slot_geo_dual(sh, sh.dx, *Gd);
-            pass_dual(sh, nt, d, *Gd, NT_MODE_HV, lsc, nullptr, nullptr, mu);
+            pass_dual(sh, nt, d, *Gd, NT_MODE_HV, lsc, nullptr, nullptr);
             __syncthreads();
             const double pAp = nt_dot(sh, nt, sh.dx, nt.hp, lsc, NT_P, NT_HP);
-            if (delta > 0.0) {
-                const double a0 = pAp > 0.0 ? rz / pAp : 0.0;
-                if (!(pAp > 0.0) || xMx + 2.0 * a0 * xMp + a0 * a0 * pMp >= delta * delta) {
-                    nt_axpy_p(sh, lsc, nt_to_boundary(xMx, xMp, pMp, delta));
-                    xMx = delta * delta;
-                    if (boundary) *boundary = 1;
-                    ++it;
-                    break;
-                }
-            }
             if (!(pAp > 0.0)) { *neg = 1; break; }
             const double alpha = rz / pAp;
-            xMx += 2.0 * alpha * xMp + alpha * alpha * pMp;
             for (int q = tid; q < n; q += blockDim.x) {
                 if (held(sh, q)) continue;
                 sh.dmp[q] += alpha * sh.dx[q];
@@ -1696,8 +1662,6 @@ __device__ double nt_solve_exact(BaShared& sh, NtShared& nt, const XcbBaWindows&
             const double rz_new = nt_dot(sh, nt, sh.g, sh.y, lsc, NT_R, NT_Z);
             const double beta = rz_new / rz;
             rz = rz_new;
-            xMp = beta * (xMp + alpha * pMp);
-            pMp = rz_new + beta * beta * pMp;
             for (int q = tid; q < n; q += blockDim.x) sh.dx[q] = held(sh, q) ? 0.0 : sh.y[q] + beta * sh.dx[q];
             for (int l = tid; l < sh.w.L; l += blockDim.x) {
                 double* sc = lsc + (size_t)(sh.w.lm0 + l) * NT_LM_STRIDE;
@@ -1707,7 +1671,6 @@ __device__ double nt_solve_exact(BaShared& sh, NtShared& nt, const XcbBaWindows&
         }
     }
     *iters_out = it;
-    if (xMx_out) *xMx_out = xMx;
     return rel;
 }
 
