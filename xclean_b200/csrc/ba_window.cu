@@ -26,7 +26,7 @@
 #include <cooperative_groups.h>
 namespace cg = cooperative_groups;
 
-#define BA_WARPS 10
+#define BA_WARPS 11
 #define BA_THREADS (BA_WARPS * 32)
 #define BA_MAXP 20
 #define BA_MAXN (6 * BA_MAXP)
@@ -2863,14 +2863,16 @@ __global__ void __launch_bounds__(BA_THREADS, 1) k_lw_build(XcbBaWindows d, LwWo
     }
 }
 
-// The mixed build of a chunk with the Schur term on the tensor cores.  The landmarks go through in rounds of BA_WARPS,
-// one per warp: each warp adds its landmark's pose-pose blocks (the same slot, or a target with the host) and gradient
+// The mixed build of a chunk with the Schur term on the tensor cores.  The landmarks go through in rounds of TC_LMS
+// (the tile's TC_KT columns hold three per landmark), one per warp, the CTA's other warps idle: each warp adds its landmark's pose-pose blocks (the same slot, or a target with the host) and gradient
 // to the CTA's packed system with shared-memory atomics, as pass_build does, and writes the landmark's three Schur
 // columns U = Hlp^T C (Hll^-1 = C C^T; rows 6 s .. 6 s + 5 of its touched slots s, zero elsewhere) into the round's
 // TF32 hi / lo tile; one thread then adds U U^T of the tile to the tensor-memory accumulator (tc_issue), which runs
 // while the next round is linearised.  At the end the accumulator is subtracted from the packed system:
 // S = sum of pose-pose blocks - sum_l Hlp_l^T Hll_l^-1 Hlp_l.  A landmark whose Hll^-1 is not numerically positive
 // definite in float64 keeps the scatter of its Schur blocks.  -> false when a tensor-core wait ran out.
+#define TC_LMS (TC_KT / 3)                      // landmarks per tensor-core round: three tile columns each
+static_assert(TC_LMS <= BA_WARPS, "a tensor-core round takes one landmark per warp");
 __device__ bool pass_build_tc(BaShared& sh, const XcbBaWindows& d, float* S, float* gb, WarpLm<float>* wls,
                               float* tiles, uint64_t* bar, uint32_t tmem, int* fail, const double* frz)
 {
@@ -2879,7 +2881,7 @@ __device__ bool pass_build_tc(BaShared& sh, const XcbBaWindows& d, float* S, flo
     const SlotGeo<float>& G = sh.g32;
     double c_local = 0.0;
     int rounds = 0;
-    for (int base = sh.lb; base < sh.le; base += BA_WARPS, ++rounds) {
+    for (int base = sh.lb; base < sh.le; base += TC_LMS, ++rounds) {
         const int stg = rounds & 1;
         float* hi = tiles + stg * 2 * TC_TILE_FLOATS;
         float* lo = hi + TC_TILE_FLOATS;
@@ -2891,7 +2893,7 @@ __device__ bool pass_build_tc(BaShared& sh, const XcbBaWindows& d, float* S, flo
         __syncthreads();
         const int l = base + wid;
         const int gl = sh.w.lm0 + l;
-        if (l < sh.le && d.lm_mask[gl]) {
+        if (wid < TC_LMS && l < sh.le && d.lm_mask[gl]) {
             const int h = d.lm_host[gl];
             float Hll[9], bl[3];
             int nt;
