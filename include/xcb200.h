@@ -461,7 +461,7 @@ int xcb_ba_noalloc_max_landmarks(void);
 int xcb_ba_solve_windows_noalloc(const xcb_ba_windows* w, int Lt, int max_slots, int iters, double lam0, int mode,
                                  double* stats, double* dx0, int dx0_stride, int grid, void* stream);
 
-/* Exact second-order steps on the window cost (no reference counterpart: the differentiable BA of the north-star API).
+/* Exact second-order steps on the window cost (no reference counterpart: the differentiable-BA API behind BAAdjoint).
    XCB_BA_NEWTON_POLISH: at most `steps` Newton steps with the exact Hessian (window.solve's LM converges only
    linearly when Huber weights are active), the state updated in place.  Each step moves every landmark to the
    minimum of its own cost with the poses fixed (Newton on its exact 3x3 block), then takes a Newton step on the poses

@@ -1369,7 +1369,7 @@ __device__ void pass_dual(BaShared& sh, NtShared& nt, const XcbBaWindows& d, con
         double* sc = lsc + (size_t)gl * NT_LM_STRIDE;
         const int k0 = d.lm_ob[gl], nob = lm_rows(d, gl);
         // the landmark moves along p only if it is a variable (its Gauss-Newton block passes the conditioning test,
-        // judged below on the same sums; a landmark that is not a variable has p_l = 0 in the scratch)
+        // decided below on the same sums; a landmark that is not a variable has p_l = 0 in the scratch)
         const Dual lm[3] = {Dual(d.lmp[3 * gl], sc[NT_P]), Dual(d.lmp[3 * gl + 1], sc[NT_P + 1]),
                             Dual(d.lmp[3 * gl + 2], sc[NT_P + 2])};
         Dual gl3[3] = {Dual(0.0), Dual(0.0), Dual(0.0)}, gh[6];
