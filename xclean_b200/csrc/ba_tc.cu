@@ -13,7 +13,7 @@ __global__ void __launch_bounds__(128, 1) k_gram_tc(const float* __restrict__ U,
                                                    unsigned int* err)
 {
     extern __shared__ __align__(1024) float tsm[];
-    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ __align__(8) uint64_t bar[3];          // two tile stages, the final drain
     __shared__ uint32_t tmem_base;
     __shared__ int fail;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -21,6 +21,7 @@ __global__ void __launch_bounds__(128, 1) k_gram_tc(const float* __restrict__ U,
     if (tid == 0) {
         tc_mbar_init(&bar[0]);
         tc_mbar_init(&bar[1]);
+        tc_mbar_init(&bar[2]);
         fail = 0;
     }
     tc_fence_before();
@@ -54,6 +55,7 @@ __global__ void __launch_bounds__(128, 1) k_gram_tc(const float* __restrict__ U,
         if (ntile >= 1 && !tc_mbar_wait(&bar[(ntile - 1) & 1], (uint32_t)(((ntile - 1) >> 1) & 1))) fail = 1;
         if (ntile >= 2 && !tc_mbar_wait(&bar[(ntile - 2) & 1], (uint32_t)(((ntile - 2) >> 1) & 1))) fail = 1;
     }
+    if (tid == 0 && ntile >= 1 && !tc_drain(&bar[2])) fail = 1;
     __syncthreads();
     tc_fence_after();
     if (!fail) {

@@ -6,7 +6,8 @@
 // tile).  The tile uses the canonical no-swizzle K-major layout of the shared-memory descriptors: core matrices of
 // 8 rows x 16 bytes (4 floats), the core matrices of one 8-row group consecutive along K (LBO = 128 B), the 8-row
 // groups TC_KT / 4 core matrices apart (SBO = TC_KT * 32 B).  The accumulator is one 128-lane x 128-column FP32 block
-// of tensor memory; one thread issues the MMAs and commits them to an mbarrier per tile stage; every wait is bounded.
+// of tensor memory; one thread issues the MMAs and commits them to an mbarrier per tile stage, and at the end to a
+// third one that drains them all; every wait is bounded.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -86,6 +87,13 @@ __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence:
 // generic-proxy writes of this thread to shared memory become visible to the tensor core's reads
 __device__ __forceinline__ void tc_fence_proxy() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
+// one thread: arrive on bar once every tcgen05 operation the thread issued before has completed
+__device__ __forceinline__ void tc_commit(uint64_t* bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(tc_smem_addr(bar))
+                 : "memory");
+}
+
 // one thread: D (+)= hi hi^T + hi lo^T + lo hi^T over the TC_KT columns of the tile pair, then commit to bar
 __device__ __forceinline__ void tc_issue(uint32_t tmem, const float* hi, const float* lo, bool accumulate,
                                          uint64_t* bar)
@@ -106,8 +114,16 @@ __device__ __forceinline__ void tc_issue(uint32_t tmem, const float* hi, const f
                          : "memory");
         }
     }
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(tc_smem_addr(bar))
-                 : "memory");
+    tc_commit(bar);
+}
+
+// one thread, after the stage waits (or after one of them ran out): commit to a barrier of its own (`fin`, initialised,
+// used once) and wait, bounded, until every tcgen05 operation the thread issued has completed (tcgen05.commit tracks
+// all of the thread's earlier ones), so that tensor memory is freed with nothing in flight; false when it ran out
+__device__ __forceinline__ bool tc_drain(uint64_t* fin)
+{
+    tc_commit(fin);
+    return tc_mbar_wait(fin, 0);
 }
 
 // warp w (0..3) reads accumulator rows 32 w .. 32 w + 31 (its lane's row), columns c0 .. c0 + 15

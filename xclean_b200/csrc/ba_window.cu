@@ -3013,6 +3013,7 @@ __device__ bool pass_build_tc(BaShared& sh, const XcbBaWindows& d, float* S, flo
         if (!tc_mbar_wait(&bar[(rounds - 1) & 1], (uint32_t)(((rounds - 1) >> 1) & 1))) *fail = 1;
         if (rounds >= 2 && !tc_mbar_wait(&bar[(rounds - 2) & 1], (uint32_t)(((rounds - 2) >> 1) & 1))) *fail = 1;
     }
+    if (tid == 0 && rounds >= 1 && !tc_drain(&bar[2])) *fail = 1;
     __syncthreads();
     tc_fence_after();
     const int n = sh.w.n;
@@ -3045,7 +3046,7 @@ __global__ void __launch_bounds__(BA_THREADS, 1) k_lw_build_tc(XcbBaWindows d, L
 {
     extern __shared__ __align__(1024) unsigned char dsm[];
     __shared__ BaShared sh;
-    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ __align__(8) uint64_t bar[3];          // two tile stages, the final drain
     __shared__ uint32_t tmem_base;
     __shared__ int fail;
     const LwChunk c = chunks[blockIdx.x];
@@ -3055,6 +3056,7 @@ __global__ void __launch_bounds__(BA_THREADS, 1) k_lw_build_tc(XcbBaWindows d, L
     if (tid == 0) {
         tc_mbar_init(&bar[0]);
         tc_mbar_init(&bar[1]);
+        tc_mbar_init(&bar[2]);
         fail = 0;
     }
     tc_fence_before();
