@@ -9,6 +9,8 @@ q_r = Exp(omega) q + rho (t - B e_x) (the rectified model is omega = t = 0).  It
   * solve(win, ...)        Newton with the exact Hessian to a gradient of ~1e-13 (the converged state x*), from a
                            start inside the basin of the minimum (e.g. the state window.solve converged to);
   * implicit_grad(...)     dL/dtheta = -(d2C/dtheta dx)^T (d2C/dx2)^-1 dL/dx* by autograd (the FP64 autodiff reference);
+  * implicit_grad_schur(...) the same through the Schur complement on the poses, for windows of thousands of
+                           landmarks (Hessian-vector products, no dense Hessian), with the gradient's max-norm;
   * fd_grad(...)           central finite differences of L(x*(theta)) with step 1e-6.
 The held slot is not a variable; landmarks outside lm_mask or without a valid observation are constants.
 """
