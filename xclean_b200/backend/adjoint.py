@@ -12,21 +12,22 @@ converged poses to de-rectifying it), weights [M] (the per-row weight 1/sigma in
 (float64; the batch's slots in window order).
 
 Forward: `iters` LM iterations of window.solve (float64, batched: one launch, or the large-window path when the
-batch holds few large windows); then the landmarks whose
-Gauss-Newton step would take the inverse depth to <= 1e-9 (window.solve keeps them where they are, while its Schur
-complement assumes they move, so its fixed point is not stationary) are flagged constant and `free_iters` LM
-iterations run with them held; then at most `newton_steps` landmark-eliminated Newton steps on the
-exact Hessian (the LM converges only linearly where Huber weights are active, and the adjoint is exact only at a
-stationary point): each moves every landmark to the minimum of its own cost with the poses fixed, then solves the exact
-reduced pose system; landmarks whose minimum lies at infinity (rho < 1e-7) are flagged constant on the way.  Backward: one solve H x = dL/dstate with the exact reduced system (its Cholesky factor for the poses,
-the landmarks by back-substitution, at most two refinement steps on the exact residual; H applied through dual numbers,
-Jacobians recomputed from the state rather than stored; conjugate gradients preconditioned with the Gauss-Newton
-system where the reduced system is not positive definite), then dL/dtheta = -(d2C / dtheta dstate) x, scattered to
-the window parameters and to every observation row.
-The solver keeps the converged state between forward and backward: do not reuse it for another forward before
-backward.  ctx.newton_stats / ctx.adjoint_stats keep the per-window stats (column 2: the gradient max-norm at the
-returned state; a window that did not reach a stationary point within `newton_steps` has an approximate gradient).
-The flagged landmarks are constants of the forward and of the adjoint.
+batch holds few large windows); then the landmarks whose Gauss-Newton step would take the inverse depth to <= 1e-9
+(window.solve keeps them where they are, while its Schur complement assumes they move, so its fixed point is not
+stationary) are flagged constant and `free_iters` LM iterations run with them held; then at most `newton_steps`
+landmark-eliminated Newton steps on the exact Hessian (the LM converges only linearly where Huber weights are active,
+and the adjoint is exact only at a stationary point): each moves every landmark to the minimum of its own cost with
+the poses fixed, then solves the exact reduced pose system; landmarks whose minimum lies at infinity (rho < 1e-7) are
+flagged constant on the way.  Backward: one solve H x = dL/dstate with the exact reduced system (its Cholesky factor
+for the poses, the landmarks by back-substitution, at most two refinement steps on the exact residual; H applied
+through dual numbers, Jacobians recomputed from the state rather than stored; conjugate gradients preconditioned with
+the Gauss-Newton system where the reduced system is not positive definite), then dL/dtheta = -(d2C / dtheta dstate) x,
+scattered to the window parameters and to every observation row.
+The solver keeps the converged state between forward and backward: backward raises RuntimeError when a solver call
+changed it in between (another forward, solve, solve_free, newton, reset; the solver's `generation` counts them;
+writes into solver.t are the caller's to avoid).  ctx.newton_stats / ctx.adjoint_stats keep the per-window stats
+(column 2: the gradient max-norm at the returned state; a window that did not reach a stationary point within
+`newton_steps` has an approximate gradient).  The flagged landmarks are constants of the forward and of the adjoint.
 """
 from __future__ import annotations
 
@@ -57,6 +58,7 @@ class BAAdjoint(torch.autograd.Function):
             solver.solve_free(int(free_iters), float(lam0), path="auto")
             st = solver.newton(int(newton_steps), tol=float(tol))
         ctx.solver = solver
+        ctx.generation = solver.generation
         ctx.tol = float(tol)
         ctx.dtypes = (intrinsics.dtype, baseline.dtype, extrinsic.dtype, weights.dtype, pixels.dtype)
         ctx.newton_stats = st
@@ -65,6 +67,9 @@ class BAAdjoint(torch.autograd.Function):
     @staticmethod
     def backward(ctx, grad_p):
         solver = ctx.solver
+        if solver.generation != ctx.generation:
+            raise RuntimeError("BAAdjoint: the solver's state changed between forward and backward (a solve, newton, "
+                               "reset or another forward on the same solver); run backward first")
         gpose = torch.zeros((grad_p.shape[0], 6), dtype=torch.float64, device=grad_p.device)
         gpose[:, 3:] = grad_p.to(torch.float64)
         stats, gtheta, gisig, gz = solver.adjoint(gpose, tol=ctx.tol)

@@ -228,6 +228,7 @@ class BatchSolver:
                 a = np.ascontiguousarray(self.host[k])
                 self.t[k] = torch.from_numpy(a if a.size else np.zeros(1, a.dtype)).to(self.dev)
         self.init = {k: self.t[k].clone() for k in ("Rwb", "pwb", "lmp")}
+        self.generation = 0         # bumped by every call that changes the state or the constant-landmark flags
         self.stats = torch.zeros((max(self.nw, 1), 8), dtype=torch.float64, device=self.dev)
         self.dx0 = torch.zeros((max(self.nw, 1), 6 * MAX_SLOTS), dtype=torch.float64, device=self.dev)
         Lt = int(self.host["lmp"].shape[0])
@@ -241,12 +242,14 @@ class BatchSolver:
                 setattr(self.desc, k, self.t[k].data_ptr())
 
     def reset(self):
+        self.generation += 1
         for k in ("Rwb", "pwb", "lmp"):
             self.t[k].copy_(self.init[k])
         self.clear_frozen()
 
     def clear_frozen(self):
         """Forget the constant-landmark flags of the Newton calls (they belong to the state they were found at)."""
+        self.generation += 1
         if hasattr(self, "nscratch"):
             self.nscratch.zero_()
 
@@ -272,6 +275,7 @@ class BatchSolver:
         torch = self.torch
         s = stream if stream is not None else torch.cuda.current_stream(self.dev)
         sc = self._nscratch()
+        self.generation += 1
         stats = torch.zeros((max(self.nw, 1), 8), dtype=torch.float64, device=self.dev)
         if path == "large" or (path == "auto" and self.use_large()):
             self._large_setup()
@@ -317,6 +321,7 @@ class BatchSolver:
         torch = self.torch
         self._large_setup()
         s = stream if stream is not None else torch.cuda.current_stream(self.dev)
+        self.generation += 1
         rc = _lib.lib().xcb_ba_solve_windows_large_dev(
             ctypes.byref(self.desc), int(self.host["Rwb"].shape[0]), int(self.host["lmp"].shape[0]),
             self.lchunks.data_ptr(), self.nchunks, self.max_slots, int(iters), float(lam0), PRECISIONS[precision],
@@ -331,6 +336,7 @@ class BatchSolver:
         if path == "large" or (path == "auto" and self.use_large()):
             return self.solve_large(iters, lam0, precision, stream)
         s = stream if stream is not None else torch.cuda.current_stream(self.dev)
+        self.generation += 1
         rc = _lib.lib().xcb_ba_solve_windows_dev(ctypes.byref(self.desc), self.max_slots, int(iters), float(lam0),
                                                  PRECISIONS[precision], self.stats.data_ptr(), self.dx0.data_ptr(),
                                                  6 * MAX_SLOTS, self.scratch.data_ptr(), self.scratch.numel(),
@@ -395,6 +401,8 @@ class BatchSolver:
             gp = gpose.to(self.dev, torch.float64).contiguous()
             if tuple(gp.shape) != (int(self.host["Rwb"].shape[0]), 6):
                 raise ValueError("adjoint: gpose must be [slots, 6]")
+        if mode != _lib.XCB_BA_NEWTON_ADJOINT:
+            self.generation += 1
         rc = _lib.lib().xcb_ba_newton_windows_dev(
             ctypes.byref(self.desc), self.max_slots, int(mode), int(steps), int(maxit), float(tol),
             ctypes.c_void_p(gp.data_ptr() if gp is not None else None), ctypes.c_void_p(gtheta.data_ptr()),
